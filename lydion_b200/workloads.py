@@ -1,0 +1,168 @@
+"""Synthetic static-cloud workloads for the Lyman-alpha step.
+
+The cloud set-up restates SetupStaticCloudTest (src/StaticCloudTest.jl:117-306): a uniform
+cylindrical (r, Z) box of side 1.1 R_cl with R_cl = 1 pc, a uniform sphere of H I at
+temperature T0 with line-centre optical depth tau0, gray continuum absorption tau_abs,
+constant destruction probability, a Hubble-like outflow inside the cloud
+(GetHubbleFlow, src/StaticCloudTest.jl:34-59), and either a uniform-sphere source of radius
+rs*R_cl or (rs = 0) a point source in the axis cell at the cloud centre. The time step is
+the CFL step of GetRHDCFLTimeStep (src/AdvectJandH.jl:29-68) with CFL = 0.4 and c~ = c.
+
+Arrays use the reference's memory order: a Julia array A[k, i, j] (column-major) is the
+numpy C-order array A[j, i, k]; a per-cell array A[i, j] is numpy A[j, i].
+
+No public dataset is involved: every input is generated here from seeded parameters.
+"""
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import constants as K
+from .grid import FreqGrid, CylGeometry, symmetric_frequency_grid, uniform_cylindrical_geometry, alpha_floor
+
+BC_REFLECT, BC_OUTFLOW = 0, 1
+FLUX_GLF, FLUX_HLL = 0, 1
+
+
+@dataclass
+class StaticCloud:
+    """All inputs of one static-cloud run (everything the step reads except H_voigt)."""
+    name: str
+    geom: CylGeometry
+    freq: FreqGrid
+    T: np.ndarray            # [j, i]
+    alpha: np.ndarray        # line-centre opacity n_HI sigma0
+    alpha_c: np.ndarray      # continuum absorption opacity (J)
+    alpha_cF: np.ndarray     # continuum flux opacity added to alpha*H_voigt (0 for static clouds)
+    pd: np.ndarray
+    js: np.ndarray           # frequency-integrated emissivity
+    u_r: np.ndarray          # cell-centred velocities (for the CFL step)
+    u_Z: np.ndarray
+    u_r_star: np.ndarray     # [j, f] f = 0..nr
+    u_Z_star: np.ndarray     # [f, i] f = 0..nz
+    dur_dr: np.ndarray
+    dur_dZ: np.ndarray
+    duZ_dr: np.ndarray
+    duZ_dZ: np.ndarray
+    ur_over_r: np.ndarray
+    c_tilde: float
+    dt: float
+    z_center: float
+    bc_r_right: int
+    bc_z_bot: int
+    bc_z_top: int
+    recoil: bool
+    flux_method: int
+    alpha_floor: float
+    tau0: float
+    L_source: float
+
+    @property
+    def n_nu(self):
+        return self.freq.n_nu
+
+    @property
+    def nr(self):
+        return self.geom.nr
+
+    @property
+    def nz(self):
+        return self.geom.nz
+
+    @property
+    def cell_bins(self):
+        return self.n_nu * self.nr * self.nz
+
+
+def hubble_flow(r, Z, umax, Rcl, Zc):
+    """GetHubbleFlow, src/StaticCloudTest.jl:34-59 (vectorised)."""
+    R = np.hypot(r, Z - Zc)
+    inside = R <= Rcl
+    H = umax / Rcl
+    u_r = np.where(inside, H * r, 0.0)
+    u_Z = np.where(inside, H * (Z - Zc), 0.0)
+    g = np.where(inside, H, 0.0)
+    return u_r, u_Z, g
+
+
+def cfl_dt(geom, c_tilde, u_r, u_Z, cfl):
+    """GetRHDCFLTimeStep, src/AdvectJandH.jl:29-68."""
+    dr = geom.r[1:] - geom.r[:-1]
+    dZ = geom.Z[1:] - geom.Z[:-1]
+    u = np.hypot(u_r, u_Z)
+    dt = 0.5 * np.minimum(dr[None, :], dZ[:, None]) / (c_tilde + u)
+    return cfl * float(dt.min())
+
+
+def static_cloud(nr, nz, n_nu, tau0, T0=1e4, tau_abs=0.0, pd0=0.0, rs=0.0, umax_kms=0.0,
+                 recoil=True, bc_z_bot=BC_REFLECT, flux_method=FLUX_GLF, freq=None, name="cloud",
+                 cfl=0.4, x_max=600.0):
+    """Fields of SetupStaticCloudTest (src/StaticCloudTest.jl:117-306), uniform grid, no cone."""
+    L = 1e5 * K.Lsun
+    Rcl = K.pc
+    Rmax = 1.1 * Rcl
+    Zmax = Rmax
+    Zc = 0.0 if bc_z_bot == BC_REFLECT else 0.5 * Zmax
+    c_tilde = K.c
+    geom = uniform_cylindrical_geometry(Rmax, Zmax, nr, nz)
+    if freq is None:
+        freq = symmetric_frequency_grid(n_nu, x_max=x_max, T_ref=T0)
+    rC, ZC = np.meshgrid(geom.rCoM, geom.ZCoM)            # [j, i]
+    T = np.full((nz, nr), float(T0))
+    Rs = rs * Rcl
+    dL = Rcl
+    sigma0 = K.compute_sigma0(T0)
+    nHI0 = tau0 / (sigma0 * dL)
+    ac0 = tau_abs / Rcl
+    RCoM = np.sqrt(rC ** 2 + (ZC - Zc) ** 2)
+    inside_cloud = RCoM < Rcl
+    inside_source = RCoM < Rs
+    alpha = np.where(inside_cloud, nHI0 * sigma0, 0.0)
+    alpha_c = np.where(inside_cloud, ac0, 0.0)
+    pd = np.where(inside_cloud, pd0, 0.0)
+    js = np.where(inside_cloud & inside_source, 3 * L / ((4 * np.pi) * (4 * np.pi) * (Rs * Rs * Rs)) if Rs > 0 else 0.0, 0.0)
+    umax = umax_kms * K.kms
+    u_r, u_Z, g = hubble_flow(rC, ZC, umax, Rcl, Zc)
+    rf, Zrow = np.meshgrid(geom.r, geom.ZCoM)             # [j, f]
+    u_r_star, _, _ = hubble_flow(rf, Zrow, umax, Rcl, Zc)
+    rcol, Zf = np.meshgrid(geom.rCoM, geom.Z)             # [f, i]
+    _, u_Z_star, _ = hubble_flow(rcol, Zf, umax, Rcl, Zc)
+    if js.max() <= 0.0:
+        i0 = int(np.argmin(np.abs(geom.rCoM - 0.0)))
+        j0 = int(np.argmin(np.abs(geom.ZCoM - Zc)))
+        js[j0, i0] = L / (4 * np.pi * geom.dV[j0, i0])
+    zeros = np.zeros((nz, nr))
+    dt = cfl_dt(geom, c_tilde, u_r, u_Z, cfl)
+    return StaticCloud(name=name, geom=geom, freq=freq, T=T, alpha=alpha, alpha_c=alpha_c,
+                       alpha_cF=zeros.copy(), pd=pd, js=js, u_r=u_r, u_Z=u_Z,
+                       u_r_star=np.ascontiguousarray(u_r_star), u_Z_star=np.ascontiguousarray(u_Z_star),
+                       dur_dr=g.copy(), dur_dZ=zeros.copy(), duZ_dr=zeros.copy(), duZ_dZ=g.copy(),
+                       ur_over_r=g.copy(), c_tilde=c_tilde, dt=dt, z_center=Zc,
+                       bc_r_right=BC_OUTFLOW, bc_z_bot=bc_z_bot, bc_z_top=BC_OUTFLOW,
+                       recoil=bool(recoil), flux_method=flux_method, alpha_floor=alpha_floor(geom),
+                       tau0=tau0, L_source=L)
+
+
+def config_c1(scale=1):
+    """Plain FP64, 64x64 cells x 64 bins, tau0 = 1e6, T = 1e4 K, no dust, static, point source."""
+    n = 64 // scale
+    return static_cloud(n, n, 64 if scale == 1 else max(8, 64 // scale), tau0=1e6, T0=1e4, rs=0.0,
+                        name="c1_static_point_64x64x64")
+
+
+def config_c2(scale=1):
+    """256x256 cells x 64 bins, tau0 = 1e8, T = 1e4 K, gray dust tau_abs = 1, uniform source of
+    radius 0.5 R_cl, Hubble outflow with v_max = 200 km/s."""
+    n = 256 // scale
+    return static_cloud(n, n, 64 if scale == 1 else max(8, 64 // scale), tau0=1e8, T0=1e4, tau_abs=1.0,
+                        rs=0.5, umax_kms=200.0, name="c2_dusty_outflow_256x256x64")
+
+
+def small_cloud(nr=12, nz=10, n_nu=16, **kw):
+    """A cheap cloud for parity tests (the oracle finishes it in milliseconds)."""
+    kw.setdefault("tau0", 1e5)
+    kw.setdefault("rs", 0.5)
+    kw.setdefault("umax_kms", 150.0)
+    kw.setdefault("tau_abs", 0.5)
+    kw.setdefault("x_max", 60.0)
+    return static_cloud(nr, nz, n_nu, name="small", **kw)

@@ -1,0 +1,284 @@
+"""ctypes front end of the CPU FP64 oracle (oracle/lydion_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, by __graft_entry__.smoke() as the checker, and by
+bench.py's CPU-baseline leg. The product library never imports this module.
+
+Parity status: the step is "parity unpinned" (the Julia reference cannot run in this
+environment and no J/H golden vectors exist); the LAPACK dgtsv and the erf/Dawson Voigt
+tables are pinned against scipy fixtures under tests/golden/.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "build", "liblydion_oracle.so")
+_lib = None
+
+P = C.POINTER(C.c_double)
+
+
+def build():
+    """Compile the oracle with its Makefile (gcc, OpenMP, no fast-math)."""
+    subprocess.check_call(["make", "-s", "-C", _HERE])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = C.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+class Geom(C.Structure):
+    _fields_ = [("nr", C.c_int), ("nz", C.c_int), ("r", P), ("Z", P), ("rCoM", P), ("ZCoM", P),
+                ("dV", P), ("inv_dV", P), ("A_r", P), ("A_Z", P), ("inv_r_cell", P),
+                ("dr_L", P), ("dr_R", P), ("inv_dr_i_im1", P), ("inv_dr_ip1_i", P), ("inv_dr_ip2_ip1", P),
+                ("dr_b", C.c_double * 10),
+                ("dZ_L", P), ("dZ_R", P), ("inv_dZ_j_jm1", P), ("inv_dZ_jp1_j", P), ("inv_dZ_jp2_jp1", P),
+                ("dZ_b", C.c_double * 10)]
+
+
+class Lya(C.Structure):
+    _fields_ = [("nnu", C.c_int), ("nr", C.c_int), ("nz", C.c_int),
+                ("J", P), ("J_old", P), ("H_r", P), ("H_Z", P), ("H_r_old", P), ("H_Z_old", P),
+                ("alpha_F", P), ("Hvoigt", P), ("phi_nu", P),
+                ("alpha", P), ("alpha_c", P), ("pd", P), ("js", P), ("T", P),
+                ("dru_r", P), ("dru_Z", P), ("f_r", P), ("f_Z", P),
+                ("nu", P), ("nuC", P), ("dnu", P), ("inv_dnu", P), ("inv_nuC", P),
+                ("kcore_min", C.c_int), ("kcore_max", C.c_int), ("recoil", C.c_int), ("flux_method", C.c_int),
+                ("alpha_floor", C.c_double),
+                ("F_r", P), ("F_Z", P), ("F_r_Hr", P), ("F_Z_Hr", P), ("F_r_HZ", P), ("F_Z_HZ", P),
+                ("K_iph", P), ("K_imh", P), ("Fkp", P), ("Fk", P), ("Fkm", P)]
+
+
+class Vel(C.Structure):
+    _fields_ = [("u_r_star", P), ("u_Z_star", P), ("dur_dr", P), ("dur_dZ", P), ("duZ_dr", P),
+                ("duZ_dZ", P), ("ur_over_r", P)]
+
+
+class VoigtLUT(C.Structure):
+    _fields_ = [("xmax", C.c_double), ("xmin", C.c_double), ("inv_dx", C.c_double), ("nx", C.c_int),
+                ("erf_y", P), ("dawson_y", P), ("gauss_y", P), ("xgauss_y", P), ("omx2gauss_y", P)]
+
+
+def _declare(L):
+    I, D = C.c_int, C.c_double
+    sig = {
+        "orc_minmod": (D, [D, D]), "orc_chi_L84": (D, [D]),
+        "orc_D_edd": (None, [D, D, D, P]), "orc_D_edd_from_f_n": (None, [D, D, D, P]),
+        "orc_hll_eigenvalues": (None, [D, D, P]),
+        "orc_dgtsv": (I, [I, P, P, P, P]),
+        "orc_pd_lya": (D, [D] * 7),
+        "orc_compute_b": (D, [D]), "orc_compute_dnuD": (D, [D]), "orc_compute_a": (D, [D]),
+        "orc_compute_sigma0": (D, [D]),
+        "orc_voigt_H": (D, [C.c_void_p, D, D]), "orc_voigt_intH": (D, [C.c_void_p, D, D]),
+        "orc_voigt_tophat": (D, [C.c_void_p, D, D, D, D]),
+        "orc_update_hvoigt": (None, [C.c_void_p, C.c_void_p]),
+        "orc_update_phi_nu": (None, [C.c_void_p, I, I]),
+        "orc_find_active_bins": (None, [C.c_void_p, C.c_void_p, C.POINTER(I), C.POINTER(I)]),
+        "orc_advect_jh": (None, [C.c_void_p, C.c_void_p, C.c_void_p, D, I, I, I, I, I, I]),
+        "orc_advect_lya": (None, [C.c_void_p, C.c_void_p, C.c_void_p, D, I, I, I, C.POINTER(I), C.POINTER(I)]),
+        "orc_emission_absorption": (None, [C.c_void_p, D, D]),
+        "orc_update_freq_factors": (None, [C.c_void_p, C.c_void_p]),
+        "orc_frequency_update_all_cells": (I, [C.c_void_p, C.c_void_p, D, I, C.POINTER(C.c_long)]),
+        "orc_update_f_mf": (None, [C.c_void_p, C.c_void_p, D, D, I, P]),
+        "orc_f_esc_lya": (D, [C.c_void_p, C.c_void_p, D, I]),
+        "orc_reset_dru": (None, [C.c_void_p]),
+        "orc_cfl_dt": (D, [C.c_void_p, D, P, P, D]),
+        "orc_edge_count": (I, [I, I]),
+        "orc_edge_spectra": (None, [C.c_void_p, P, P, C.POINTER(I), C.POINTER(I)]),
+        "orc_static_step": (None, [C.c_void_p, C.c_void_p, C.c_void_p, D, D, D, I, I, I, P]),
+        "orc_static_run": (None, [C.c_void_p, C.c_void_p, C.c_void_p, D, D, D, I, I, I, I, P]),
+        "orc_num_threads": (I, []), "orc_set_num_threads": (None, [I]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+
+
+def _p(a):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(P)
+
+
+# ---- Voigt look-up tables (src/FastInterpolations.jl:175-197) ----------------------------
+XMAX_VOIGT = 1000.0
+NX_VOIGT = 200001
+_voigt_cache = {}
+
+
+def voigt_tables(xmax=XMAX_VOIGT, nx=NX_VOIGT):
+    """The five tables of CreateVoigtLUTs, tabulated with scipy's erf and Dawson integral
+    (the stand-ins for SpecialFunctions.jl's erf/dawson)."""
+    key = (xmax, nx)
+    if key not in _voigt_cache:
+        from scipy.special import erf, dawsn
+        xmin = -xmax
+        dx = (xmax - xmin) / (nx - 1)
+        x = xmin + np.arange(nx, dtype=np.float64) * dx
+        g = np.exp(-x * x)
+        _voigt_cache[key] = dict(xmax=xmax, xmin=xmin, inv_dx=1.0 / dx, nx=nx,
+                                 erf=np.ascontiguousarray(erf(x)), dawson=np.ascontiguousarray(dawsn(x)),
+                                 gauss=g, xgauss=x * np.exp(-x * x), omx2gauss=(1.0 - 2.0 * (x * x)) * np.exp(-x * x))
+    return _voigt_cache[key]
+
+
+class OracleLUT:
+    def __init__(self, xmax=XMAX_VOIGT, nx=NX_VOIGT):
+        t = voigt_tables(xmax, nx)
+        self._t = t
+        self.s = VoigtLUT(t["xmax"], t["xmin"], t["inv_dx"], t["nx"], _p(t["erf"]), _p(t["dawson"]),
+                          _p(t["gauss"]), _p(t["xgauss"]), _p(t["omx2gauss"]))
+
+    @property
+    def ref(self):
+        return C.byref(self.s)
+
+
+def geom_struct(geom):
+    keep = []
+
+    def q(a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        keep.append(a)
+        return _p(a)
+
+    g = Geom(geom.nr, geom.nz, q(geom.r), q(geom.Z), q(geom.rCoM), q(geom.ZCoM), q(geom.dV), q(geom.inv_dV),
+             q(geom.A_r), q(geom.A_Z), q(geom.inv_r_cell), q(geom.dr_L), q(geom.dr_R), q(geom.inv_dr_i_im1),
+             q(geom.inv_dr_ip1_i), q(geom.inv_dr_ip2_ip1), (C.c_double * 10)(*geom.dr_b),
+             q(geom.dZ_L), q(geom.dZ_R), q(geom.inv_dZ_j_jm1), q(geom.inv_dZ_jp1_j), q(geom.inv_dZ_jp2_jp1),
+             (C.c_double * 10)(*geom.dZ_b))
+    return g, keep
+
+
+class OracleState:
+    """A LyaArrays restatement whose arrays are numpy buffers shared with the oracle.
+
+    Arrays follow the reference's memory order: 3-D fields are numpy [j, i, k]."""
+
+    FIELDS3 = ("J", "J_old", "H_r", "H_Z", "H_r_old", "H_Z_old", "alpha_F", "Hvoigt", "phi_nu",
+               "Fkp", "Fk", "Fkm", "K_iph", "K_imh")
+
+    def __init__(self, cloud, lut=None):
+        lib()
+        self.cloud = cloud
+        nnu, nr, nz = cloud.n_nu, cloud.nr, cloud.nz
+        z3 = lambda: np.zeros((nz, nr, nnu))
+        for f in self.FIELDS3:
+            setattr(self, f, z3())
+        self.F_r = np.zeros((nz, nr + 1, nnu)); self.F_r_Hr = np.zeros_like(self.F_r); self.F_r_HZ = np.zeros_like(self.F_r)
+        self.F_Z = np.zeros((nz + 1, nr, nnu)); self.F_Z_Hr = np.zeros_like(self.F_Z); self.F_Z_HZ = np.zeros_like(self.F_Z)
+        self.alpha = np.ascontiguousarray(cloud.alpha, dtype=np.float64)
+        self.alpha_c = np.ascontiguousarray(cloud.alpha_c, dtype=np.float64)
+        self.pd = np.ascontiguousarray(cloud.pd, dtype=np.float64)
+        self.js = np.ascontiguousarray(cloud.js, dtype=np.float64)
+        self.T = np.ascontiguousarray(cloud.T, dtype=np.float64)
+        self.dru_r = np.zeros((nz, nr)); self.dru_Z = np.zeros((nz, nr))
+        self.f_r = np.zeros((nz, nr)); self.f_Z = np.zeros((nz, nr))
+        fq = cloud.freq
+        self._fq = [np.ascontiguousarray(a) for a in (fq.nu, fq.nuC, fq.dnu, fq.inv_dnu, fq.inv_nuC)]
+        self.s = Lya(nnu, nr, nz, _p(self.J), _p(self.J_old), _p(self.H_r), _p(self.H_Z), _p(self.H_r_old),
+                     _p(self.H_Z_old), _p(self.alpha_F), _p(self.Hvoigt), _p(self.phi_nu), _p(self.alpha),
+                     _p(self.alpha_c), _p(self.pd), _p(self.js), _p(self.T), _p(self.dru_r), _p(self.dru_Z),
+                     _p(self.f_r), _p(self.f_Z), *[_p(a) for a in self._fq], fq.kcore_min, fq.kcore_max,
+                     int(cloud.recoil), int(cloud.flux_method), float(cloud.alpha_floor),
+                     _p(self.F_r), _p(self.F_Z), _p(self.F_r_Hr), _p(self.F_Z_Hr), _p(self.F_r_HZ), _p(self.F_Z_HZ),
+                     _p(self.K_iph), _p(self.K_imh), _p(self.Fkp), _p(self.Fk), _p(self.Fkm))
+        self.g, self._gkeep = geom_struct(cloud.geom)
+        self._vel = [np.ascontiguousarray(a, dtype=np.float64) for a in
+                     (cloud.u_r_star, cloud.u_Z_star, cloud.dur_dr, cloud.dur_dZ, cloud.duZ_dr, cloud.duZ_dZ,
+                      cloud.ur_over_r)]
+        self.v = Vel(*[_p(a) for a in self._vel])
+        self.lut = lut
+
+    # setup: src/FreqFactors.jl:24-51 and src/StaticCloudTest.jl:283-285
+    def setup_profiles(self, lut=None):
+        lut = lut or self.lut or OracleLUT()
+        self.lut = lut
+        lib().orc_update_hvoigt(lut.ref, C.byref(self.s))
+        fq = self.cloud.freq
+        lib().orc_update_phi_nu(C.byref(self.s), fq.kcore_min, fq.kcore_max)
+        if np.any(self.cloud.alpha_cF):
+            # RHD form, PhotoThermoChemistry.jl:2151
+            self.alpha_F[...] = self.alpha[:, :, None] * self.Hvoigt + self.cloud.alpha_cF[:, :, None]
+        else:
+            # static-cloud form, src/StaticCloudTest.jl:283-285
+            self.alpha_F[...] = self.alpha[:, :, None] * self.Hvoigt
+        # UpdateFreqFactors! once at set-up, as the static driver does (src/StaticCloudTest.jl:309)
+        lib().orc_update_freq_factors(C.byref(self.s), C.byref(self.v))
+
+    def ref(self):
+        return C.byref(self.s), C.byref(self.g), C.byref(self.v)
+
+    def find_active_bins(self):
+        a, b = C.c_int(), C.c_int()
+        lib().orc_find_active_bins(C.byref(self.s), C.byref(self.g), C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def advect(self, ctdt):
+        c = self.cloud
+        a, b = C.c_int(), C.c_int()
+        lib().orc_advect_lya(C.byref(self.s), C.byref(self.g), C.byref(self.v), ctdt, c.bc_r_right, c.bc_z_bot,
+                             c.bc_z_top, C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def emission_absorption(self, c_tilde, dt):
+        lib().orc_emission_absorption(C.byref(self.s), c_tilde, dt)
+
+    def frequency_update(self, ctdt, update_ff=True):
+        npiv = C.c_long(0)
+        nfail = lib().orc_frequency_update_all_cells(C.byref(self.s), C.byref(self.v), ctdt, int(update_ff),
+                                                     C.byref(npiv))
+        return nfail, npiv.value
+
+    def force_multiplier(self, dt):
+        out = np.zeros(4)
+        lib().orc_update_f_mf(C.byref(self.s), C.byref(self.g), dt, self.cloud.z_center, self.cloud.bc_z_bot, _p(out))
+        return out
+
+    def f_esc(self, L_all):
+        return lib().orc_f_esc_lya(C.byref(self.s), C.byref(self.g), L_all, self.cloud.bc_z_bot)
+
+    def step(self):
+        c = self.cloud
+        d = np.zeros(7)
+        lib().orc_static_step(C.byref(self.s), C.byref(self.g), C.byref(self.v), c.c_tilde, c.dt, c.z_center,
+                              c.bc_r_right, c.bc_z_bot, c.bc_z_top, _p(d))
+        return d
+
+    def run(self, n_steps):
+        c = self.cloud
+        d = np.zeros((n_steps, 7))
+        lib().orc_static_run(C.byref(self.s), C.byref(self.g), C.byref(self.v), c.c_tilde, c.dt, c.z_center,
+                             c.bc_r_right, c.bc_z_bot, c.bc_z_top, n_steps, _p(d))
+        return d
+
+    def edge_spectra(self):
+        n = lib().orc_edge_count(self.cloud.nr, self.cloud.nz)
+        raw = np.zeros((n, self.cloud.n_nu)); norm = np.zeros_like(raw)
+        ri = (C.c_int * n)(); zi = (C.c_int * n)()
+        lib().orc_edge_spectra(C.byref(self.s), _p(raw), _p(norm), ri, zi)
+        return raw, norm, np.array(ri[:]), np.array(zi[:])
+
+
+def dgtsv(dl, d, du, b):
+    dl, d, du, b = (np.array(a, dtype=np.float64) for a in (dl, d, du, b))
+    info = lib().orc_dgtsv(d.size, _p(dl), _p(d), _p(du), _p(b))
+    return b, info
+
+
+def scalar(name, *args):
+    return getattr(lib(), name)(*args)
+
+
+def vec_fn(name, *args, n=3):
+    out = np.zeros(n)
+    getattr(lib(), name)(*args, _p(out))
+    return out

@@ -1,0 +1,190 @@
+"""CPU tests of the FP64 oracle: pins against the committed golden fixtures, known answers of
+the closure and line-profile functions, and conservation properties of the step."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from lydion_b200 import constants as K
+from lydion_b200 import grid as G
+from lydion_b200 import workloads as W
+
+
+def test_dgtsv_matches_lapack_fixture(oracle_mod):
+    z = np.load(os.path.join(GOLDEN, "dgtsv_cases.npz"))
+    n = int(z["n"])
+    assert n > 30
+    for q in range(n):
+        dl, d, du, b = z[f"dl{q}"], z[f"d{q}"], z[f"du{q}"], z[f"b{q}"]
+        x_ref, info_ref = z[f"x{q}"], int(z[f"info{q}"])
+        x, info = oracle_mod.dgtsv(dl, d, du, b)
+        assert info == info_ref, q
+        if info == 0:
+            # same algorithm, same operation order: agreement to a few ulps
+            np.testing.assert_allclose(x, x_ref, rtol=1e-13, atol=0, err_msg=f"case {q}")
+
+
+def test_dgtsv_single_row(oracle_mod):
+    x, info = oracle_mod.dgtsv(np.zeros(0), [4.0], np.zeros(0), [2.0])
+    assert info == 0 and x[0] == 0.5
+    _, info = oracle_mod.dgtsv(np.zeros(0), [0.0], np.zeros(0), [2.0])
+    assert info == 1
+
+
+def test_voigt_tables_match_fixture(oracle_mod):
+    z = np.load(os.path.join(GOLDEN, "voigt_samples.npz"))
+    t = oracle_mod.voigt_tables()
+    np.testing.assert_array_equal(t["erf"][z["idx"]], z["erf"])
+    np.testing.assert_array_equal(t["dawson"][z["idx"]], z["dawson"])
+    # node coordinates of CreateLUT: x_i = xmin + i*dx
+    x = t["xmin"] + z["idx"] * (1 / t["inv_dx"])
+    np.testing.assert_allclose(x, z["x"], rtol=0, atol=1e-12)
+
+
+def test_closure_known_answers(oracle_mod):
+    L = oracle_mod.lib()
+    assert L.orc_chi_L84(0.0) == pytest.approx(1 / 3, abs=1e-16)
+    assert L.orc_chi_L84(1.0) == pytest.approx(1.0, abs=1e-16)
+    # isotropic limit
+    D = oracle_mod.vec_fn("orc_D_edd", 0.0, 0.0, 1.0)
+    np.testing.assert_allclose(D, [1 / 3, 1 / 3, 0.0])
+    # free streaming along r: D_rr -> 1
+    D = oracle_mod.vec_fn("orc_D_edd", 1.0 - 1e-12, 0.0, 1.0)
+    assert D[0] == pytest.approx(1.0, abs=1e-6) and abs(D[1]) < 1e-6
+    # trace of the r-Z block plus phi-phi part is one for the f,n form
+    for f in [0.0, 0.2, 0.7, 1.0]:
+        for th in np.linspace(0, 2 * np.pi, 7):
+            D = oracle_mod.vec_fn("orc_D_edd_from_f_n", f, np.cos(th), np.sin(th))
+            chi = L.orc_chi_L84(min(max(f, 1e-10), 1 - 1e-10)) if f > 1e-10 else 1 / 3
+            assert D[0] + D[1] == pytest.approx((1 - chi) * 0.5 * 2 + (3 * chi - 1) * 0.5 if f > 1e-10 else 2 / 3)
+    # HLL eigenvalues at vanishing flux are +-1/sqrt(3)
+    e = oracle_mod.vec_fn("orc_hll_eigenvalues", 0.0, 1.0, n=2)
+    np.testing.assert_allclose(e, [-1 / np.sqrt(3), 1 / np.sqrt(3)], rtol=1e-6)
+    e = oracle_mod.vec_fn("orc_hll_eigenvalues", 1.0, 1.0, n=2)
+    assert e[1] == pytest.approx(1.0, abs=1e-4)
+    assert L.orc_minmod(1.0, -2.0) == 0.0 and L.orc_minmod(1.0, 2.0) == 1.0 and L.orc_minmod(-3.0, -2.0) == -2.0
+
+
+def test_thermal_constants(oracle_mod):
+    L = oracle_mod.lib()
+    for T in [10.0, 1e2, 1e4]:
+        assert L.orc_compute_dnuD(T) == K.compute_dnuD(T)
+        assert L.orc_compute_a(T) == K.compute_a(T)
+        assert L.orc_compute_sigma0(T) == pytest.approx(K.compute_sigma0(T), rel=1e-15)
+    # a ~ 4.7e-4 at 1e4 K and sigma0 ~ 5.9e-14 cm^2 (src/ConstantsAndFunctions.jl:222-223)
+    assert 4.5e-4 < K.compute_a(1e4) < 4.9e-4
+    assert 5.5e-14 < K.compute_sigma0(1e4) < 6.2e-14
+
+
+def test_voigt_profile_normalisation(oracle_mod):
+    """Bin-averaged H times bin width sums to sqrt(pi) dnuD over a wide grid."""
+    cl = W.small_cloud(nr=4, nz=4, n_nu=64, x_max=600.0, tau0=1e4)
+    st = oracle_mod.OracleState(cl)
+    st.setup_profiles()
+    dnuD = K.compute_dnuD(1e4)
+    s = np.sum(st.Hvoigt[0, 0] * cl.freq.dnu)
+    assert s == pytest.approx(np.sqrt(np.pi) * dnuD, rel=2e-3)
+    # phi_nu is normalised over the core bins and zero outside
+    fq = cl.freq
+    phi = st.phi_nu[0, 0]
+    assert np.sum(phi[fq.kcore_min:fq.kcore_max + 1] * fq.dnu[fq.kcore_min:fq.kcore_max + 1]) == pytest.approx(1.0, rel=1e-13)
+    assert np.all(phi[:fq.kcore_min] == 0) and np.all(phi[fq.kcore_max + 1:] == 0)
+
+
+def test_voigt_tophat_small_bin_uses_H(oracle_mod):
+    lut = oracle_mod.OracleLUT()
+    L = oracle_mod.lib()
+    a = K.compute_a(1e4)
+    for x in [0.0, 0.3, 2.0, 7.5]:
+        th = L.orc_voigt_tophat(lut.ref, x, x + 5e-6, x - 4e-6, a)
+        assert th == L.orc_voigt_H(lut.ref, x, a)
+
+
+def test_pd_lya_range(oracle_mod):
+    L = oracle_mod.lib()
+    vals = [L.orc_pd_lya(nh, nh, 1e-4 * nh, 0.1 * nh, 0.0, T, 0.0) for nh in [1e-2, 1e2, 1e6] for T in [1e2, 1e4, 1e5]]
+    assert all(0.0 <= v <= 1.0 for v in vals)
+    # more ions -> more 2s-2p mixing -> larger destruction probability
+    assert L.orc_pd_lya(1e6, 1e6, 1.0, 0.0, 0.0, 1e4, 0.0) > L.orc_pd_lya(1.0, 1.0, 1.0, 0.0, 0.0, 1e4, 0.0)
+    # the H2 line-absorption term (src/LymanAlphaDestruction.jl:85-91) needs H I present
+    assert L.orc_pd_lya(0.0, 0.0, 1.0, 0.0, 1.0, 3e3, 0.0) > 1e-4
+    assert L.orc_pd_lya(0.0, 0.0, 0.0, 0.0, 1.0, 3e3, 0.0) < 1e-10
+
+
+def test_geometry_uniform_grid():
+    g = G.uniform_cylindrical_geometry(3.0, 2.0, 6, 4)
+    assert g.dV.shape == (4, 6) and g.A_r.shape == (4, 7) and g.A_Z.shape == (5, 6)
+    assert g.dV.sum() == pytest.approx(np.pi * 9.0 * 2.0, rel=1e-14)
+    assert np.all(g.A_r[:, 0] == 0.0)
+    assert g.dZ_L == pytest.approx(np.full(4, 0.25)) and g.dZ_R == pytest.approx(np.full(4, 0.25))
+    # the inner Z ghost centroid mirrors ZCoM[1] about Z = 0
+    assert g.dZ_b[0] == pytest.approx(0.25) and g.dZ_b[3] == pytest.approx(2.0)
+    with pytest.raises(ValueError):
+        G.uniform_cylindrical_geometry(1.0, 1.0, 2, 5)
+
+
+def test_frequency_grids():
+    fq = G.symmetric_frequency_grid(64)
+    assert fq.n_nu == 64
+    x = (fq.nu - K.nu_lya) / K.compute_dnuD(1e4)
+    assert x[0] == pytest.approx(-600.0) and x[-1] == pytest.approx(600.0)
+    np.testing.assert_allclose(fq.dnu, fq.dnu[::-1], rtol=1e-9)
+    assert 0 < fq.kcore_min < 32 <= fq.kcore_max < 63
+    ref = G.reference_frequency_grid()
+    assert ref.n_nu == 194  # default grid of GenerateLyaArrays with Tmin = 30 K, q = 1.1
+
+
+def test_find_active_bins_empty_field_is_core(oracle_mod):
+    cl = W.small_cloud()
+    st = oracle_mod.OracleState(cl)
+    st.setup_profiles()
+    assert st.find_active_bins() == (cl.freq.kcore_min, cl.freq.kcore_max)
+
+
+def _closed_box(oracle_mod, steps, **kw):
+    cl = W.small_cloud(nr=10, nz=9, n_nu=16, umax_kms=0.0, tau_abs=0.0, **kw)
+    cl.bc_r_right = W.BC_REFLECT
+    cl.bc_z_top = W.BC_REFLECT
+    st = oracle_mod.OracleState(cl)
+    st.setup_profiles()
+    rng = np.random.default_rng(1)
+    J = 1e-12 * (1 + rng.uniform(size=st.J.shape))
+    st.J[...] = J; st.J_old[...] = J
+    st.H_r[...] = 0.3 * J * rng.uniform(-1, 1, J.shape); st.H_Z[...] = 0.3 * J * rng.uniform(-1, 1, J.shape)
+    st.H_r[:, 0, :] = 0.0
+    return cl, st
+
+
+def test_advection_conserves_energy_in_closed_box(oracle_mod):
+    cl, st = _closed_box(oracle_mod, 1)
+    dV = cl.geom.dV[:, :, None]
+    e0 = np.sum(st.J * dV)
+    for _ in range(5):
+        st.advect(0.3 * cl.c_tilde * cl.dt)
+    assert np.sum(st.J * dV) == pytest.approx(e0, rel=1e-12)
+
+
+def test_frequency_step_conserves_photons(oracle_mod):
+    cl, st = _closed_box(oracle_mod, 1)
+    dnu = cl.freq.dnu
+    n0 = np.sum(st.J[..., 1:-1] * dnu[1:-1], axis=-1)
+    nf, _ = st.frequency_update(cl.c_tilde * cl.dt)
+    assert nf == 0
+    n1 = np.sum(st.J[..., 1:-1] * dnu[1:-1], axis=-1)
+    # edge bins are outside the system, so only leakage into bins 0 and N-1 changes the sum
+    np.testing.assert_allclose(n1, n0, rtol=1e-6)
+
+
+def test_static_run_is_finite_and_emits(oracle_mod):
+    cl = W.small_cloud()
+    st = oracle_mod.OracleState(cl)
+    st.setup_profiles()
+    d = st.run(60)
+    assert np.all(np.isfinite(d)) and np.all(np.isfinite(st.J))
+    assert d[-1, 0] > d[5, 0] > 0  # force multiplier builds up
+    assert d[-1, 3] == pytest.approx(d[0, 3])  # luminosity is constant
+    raw, norm, ri, zi = st.edge_spectra()
+    assert raw.shape[0] == (cl.nz - 2) + 2 * (cl.nr - 3)
+    assert np.all(ri[: cl.nz - 2] == cl.nr - 2)
