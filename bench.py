@@ -1,0 +1,290 @@
+"""Benchmark of the Lyman-alpha M1 step: cell-bin updates per second on the 256x256 x 64-bin
+dusty outflowing cloud (tau0 = 1e8, tau_abs = 1, uniform source r_s = 0.5 R_cl, Hubble
+outflow v_max = 200 km/s), one static-cloud driver iteration per step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One unit of work is one (cell, frequency bin) advanced through one full step: advection of
+the active bins, emission/absorption, frequency factors + FP64 tridiagonal solve, flux
+correction and the per-step reductions (N_r N_Z N_nu per step regardless of the active
+window). With N > 1 (torchrun) every rank advances its own copy of the cloud: the clouds are
+independent, so the step has no data-path collective and the scaling is weak.
+
+`--impl reference` times the reference algorithm on the host cores instead: the Julia
+reference cannot run on this machine, so its FP64 C restatement under oracle/ stands in.
+"""
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Lyα M1 cell·bin updates/s at 256²×64, mixed vs FP64 GPU; adjoint/forward cost"
+UNIT = "cell·bin updates/s"
+WORKLOAD = "c2_dusty_outflow_256x256x64_tau1e8"
+
+
+def rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0}, "fallback"
+
+
+def profile_traffic(kernel, precision):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_c2_{precision}.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if len(r) > 5 + q and r[5 + q].strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def algorithmic_bytes(n_nu, s):
+    """Algorithmic HBM bytes per cell-bin of each kernel: the four streams read (J, H_r, H_Z,
+    H_voigt) and three written (J, H_r, H_Z) of storage size s, plus the per-cell inputs
+    amortised over the bins (advection: 11 doubles -- velocity-gradient terms, u*_r, u*_Z,
+    areas, 1/dV, alpha, <1/r>; frequency step: 15 doubles -- alpha, alpha_c, pd, js, T, the
+    five gradient terms, dV, the phi normalisation, rCoM/ZCoM, f_r, f_Z)."""
+    return {"advect": 7 * s + 11 * 8 / n_nu, "freq": 7 * s + 15 * 8 / n_nu}
+
+
+def cpu_baseline(cloud, budget_s=15.0, max_steps=40):
+    """The FP64 oracle (a C restatement of the reference path, OpenMP on every host core)
+    on the same cloud, for a bounded number of steps."""
+    from oracle import oracle as O
+    st = O.OracleState(cloud)
+    st.setup_profiles()
+    st.step()  # warm-up (first touch of the scratch arrays)
+    t0 = time.perf_counter()
+    n = 0
+    while n < max_steps and (time.perf_counter() - t0) < budget_s:
+        st.step()
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": n * cloud.cell_bins / dt, "unit": UNIT, "cores": int(O.lib().orc_num_threads()),
+            "kind": "port", "sample": f"{n} full steps of the {cloud.nr}x{cloud.nz}x{cloud.n_nu} cloud, FP64"}
+
+
+def run_reference(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return 0
+    from lydion_b200 import workloads as W
+    from oracle import oracle as O
+    cloud = W.config_c2()
+    st = O.OracleState(cloud)
+    st.setup_profiles()
+    # one step of the reference arm is one full FP64 step of the whole cloud on the host;
+    # the timed count is capped so the run stays within a few minutes of wall clock
+    for _ in range(min(args.warmup, 2)):
+        st.step()
+    t0 = time.perf_counter()
+    n = 0
+    while n < args.steps and (n == 0 or time.perf_counter() - t0 < 90.0):
+        st.step()
+        n += 1
+    el = time.perf_counter() - t0
+    args.steps = n
+    v = n * cloud.cell_bins / el
+    cores = int(O.lib().orc_num_threads())
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded static cloud set-up)",
+            "config": {"workload": WORKLOAD, "cells": [cloud.nr, cloud.nz], "bins": cloud.n_nu, "tau0": 1e8},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} full FP64 steps of the {cloud.nr}x{cloud.nz}x{cloud.n_nu} cloud "
+                                       "(C restatement of the Julia reference; Julia is not installed)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gpu(args):
+    import torch
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from lydion_b200 import workloads as W
+    from lydion_b200.m1 import context_for_cloud
+    from lydion_b200._lib import PREC_FP64
+    cloud = W.config_c2()
+    prec = PREC_FP64
+    ctx = context_for_cloud(cloud, precision=prec, device=local)
+    p = (cloud.c_tilde, cloud.dt, cloud.z_center, cloud.bc_r_right, cloud.bc_z_bot, cloud.bc_z_top)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ctx.synchronize()
+
+    # warm-up (also instantiates the step graph)
+    ctx.static_steps(args.warmup, *p, history=False)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        e0.record(stream)
+        ctx.static_steps(args.steps, *p, history=False)
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+    ms = e0.elapsed_time(e1)
+    clocks = clk.summary()
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    units = world * args.steps * cloud.cell_bins
+    value = units / (ms_max * 1e-3)
+
+    # per-kernel device time over a separate pass (events around every launch)
+    ctx.set_timing(True)
+    kt_steps = min(args.steps, 200)
+    ctx.static_steps(kt_steps, *p, history=False)
+    ctx.synchronize()
+    kms = ctx.timing() / kt_steps
+    ctx.set_timing(False)
+    names = ["advect", "freq", "reduce"]
+    dom = int(np.argmax(kms[:2]))
+    s = 8 if prec == PREC_FP64 else 4
+    ab = algorithmic_bytes(cloud.n_nu, s)[names[dom]] * cloud.cell_bins
+    peaks, src = measured_peaks()
+    achieved = ab / (kms[dom] * 1e-3) / 1e9
+    traffic = profile_traffic("k_" + names[dom], "fp64" if prec == PREC_FP64 else "mixed")
+
+    # end to end through the public API with host buffers: per step, J/H_r/H_Z up from pinned
+    # host memory, one step, J/H_r/H_Z and the diagnostics back
+    e2e_steps = max(3, min(20, args.steps // 50))
+    pinned = [torch.empty((cloud.nz, cloud.nr, cloud.n_nu), dtype=torch.float64, pin_memory=True).numpy()
+              for _ in range(3)]
+    for a, name in zip(pinned, ("J", "H_r", "H_Z")):
+        a[...] = ctx.download(name)
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        for a, name in zip(pinned, ("J", "H_r", "H_Z")):
+            ctx.upload(name, a)
+        ctx.static_steps(1, *p, history=True)
+        for a, name in zip(pinned, ("J", "H_r", "H_Z")):
+            a[...] = ctx.download(name)
+    f1.record(stream)
+    f1.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * e2e_steps * cloud.cell_bins / (e2e_ms * 1e-3)
+    nbytes = 3 * cloud.cell_bins * 8
+
+    cpu = cpu_baseline(cloud) if (rank == 0 and world == 1 and not args.no_cpu) else None
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded static cloud set-up, no dataset)",
+                "config": {"workload": WORKLOAD, "cells": [cloud.nr, cloud.nz], "bins": cloud.n_nu, "tau0": 1e8,
+                           "tau_abs": 1.0, "source_radius": 0.5, "v_max_kms": 200.0, "precision": "fp64",
+                           "parallelism": f"{world} independent clouds (one per GPU)" if world > 1 else "single GPU",
+                           "l2": "inputs larger than L2: 7 FP64 fields x 33.5 MB resident, 56 B/cell-bin streamed per kernel"},
+                "roofline": {"bound": "hbm", "kernel": "k_" + names[dom], "achieved": achieved,
+                             "peak": peaks["hbm_gbs"], "peak_source": src, "unit": "GB/s",
+                             "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                             "algorithmic_bytes_per_launch": ab, "ms_per_launch": float(kms[dom]),
+                             "kernel_ms_per_step": {n: float(v) for n, v in zip(names, kms)}},
+                "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                        "d2h_bytes_per_step": nbytes + 7 * 8, "steps": e2e_steps},
+                "gpu_launches": 3 * args.steps,
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="lydion", choices=["lydion", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,204 @@
+/*
+ * lydion_m1.h -- C ABI of the B200 Lyman-alpha M1 transport step.
+ *
+ * One context holds one (frequency x r x Z) Lyman-alpha state on one GPU, in the memory
+ * order of the Julia LyaArrays: a field F[k, i, j] (column-major, k fastest) is the flat
+ * array F[k + n_nu*(i + n_r*j)]; per-cell arrays are [i + n_r*j]; r-face arrays are
+ * [f + (n_r+1)*j], Z-face arrays [i + n_r*f]. All host pointers are borrowed for the
+ * duration of the call; device memory is owned by the context. Indices are 0-based.
+ *
+ * Every entry point returns LYD_OK (0) or a negative status; lyd_last_error() returns a
+ * description of the last failure on that context. A context is not re-entrant: calls on
+ * one context must come from one host thread at a time. Work is issued on the context's
+ * own CUDA stream; lyd_download* and the diagnostic calls return after the stream drains.
+ *
+ * Each step entry point names the Julia function of LYDION it replaces (path:line within
+ * the LYDION source tree). The Julia ccall bindings are given in INTEGRATION.md.
+ */
+#ifndef LYDION_M1_H
+#define LYDION_M1_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LYD_ABI_VERSION 1
+
+/* status codes */
+#define LYD_OK              0
+#define LYD_ERR_ARG        -1   /* bad argument (size, pointer, enum)                  */
+#define LYD_ERR_CUDA       -2   /* CUDA runtime error                                   */
+#define LYD_ERR_NONFINITE  -3   /* a NaN/Inf appeared in J or H                          */
+#define LYD_ERR_SOLVE      -4   /* a frequency tridiagonal system had a zero pivot      */
+#define LYD_ERR_STATE      -5   /* call needs an input that was never provided           */
+#define LYD_ERR_NOMEM      -6   /* device allocation failed                              */
+
+/* boundary conditions (Symbol :Reflect / :Outflow in the reference) */
+#define LYD_BC_REFLECT 0
+#define LYD_BC_OUTFLOW 1
+/* flux methods (LyaArrays{FluxMethod}, Val(:GLF) / Val(:HLL)) */
+#define LYD_FLUX_GLF 0
+#define LYD_FLUX_HLL 1
+/* precision of the step */
+#define LYD_PREC_FP64   0   /* everything in FP64 (the reference's arithmetic)             */
+#define LYD_PREC_MIXED  1   /* FP32 storage and bulk arithmetic; FP64 tridiagonal solve,
+                               FP64 reductions                                              */
+
+typedef struct lyd_ctx lyd_ctx;
+
+typedef struct lyd_dims {
+    int32_t n_nu;   /* frequency bins (N_nu), 4 <= n_nu <= 256 */
+    int32_t n_r;    /* radial cells, >= 3                      */
+    int32_t n_z;    /* vertical cells, >= 3                    */
+    int32_t reserved;
+} lyd_dims;
+
+typedef struct lyd_config {
+    int32_t flux_method;        /* LYD_FLUX_GLF or LYD_FLUX_HLL                           */
+    int32_t recoil;             /* LyaArrays.Recoil                                        */
+    int32_t precision;          /* LYD_PREC_*                                              */
+    int32_t kcore_min;          /* LyaArrays.kcore_min - 1 (0-based, inclusive)            */
+    int32_t kcore_max;          /* LyaArrays.kcore_max - 1                                 */
+    int32_t keep_freq_factors;  /* keep F+/F/F- on the device so that a later frequency
+                                   update may pass update_freq_factors = 0                 */
+    double alpha_floor;         /* LyaArrays.alpha_Lya_floor                               */
+    double j_scale;             /* LYD_PREC_MIXED: J and H are stored as value / j_scale;
+                                   0 selects 1e-12                                         */
+    int32_t device;             /* CUDA device ordinal                                     */
+    int32_t reserved[7];
+} lyd_config;
+
+/* Cylindrical geometry: the fields of GeometryCylindrical read by AdvectJandH!
+ * (src/AdvectJandH.jl:2272-2319). Arrays as described at the top of this file. */
+typedef struct lyd_geometry {
+    const double *r, *Z;                 /* interfaces, n_r+1 and n_z+1   */
+    const double *rCoM, *ZCoM;           /* centroids, n_r and n_z         */
+    const double *dV, *inv_dV;           /* n_r*n_z                        */
+    const double *A_r;                   /* (n_r+1)*n_z                    */
+    const double *A_Z;                   /* n_r*(n_z+1)                    */
+    const double *inv_r_cell;            /* n_r                            */
+    const double *dr_L, *dr_R, *inv_dr_i_im1, *inv_dr_ip1_i, *inv_dr_ip2_ip1;   /* n_r each */
+    double dr_bnd[10];  /* inner: dr_L, dr_R, inv_i_im1, inv_ip1_i, inv_ip2_ip1; then outer */
+    const double *dZ_L, *dZ_R, *inv_dZ_j_jm1, *inv_dZ_jp1_j, *inv_dZ_jp2_jp1;   /* n_z each */
+    double dZ_bnd[10];
+} lyd_geometry;
+
+/* Frequency grid of LyaArrays: interfaces nu (n_nu+1), centres nuC, widths dnu, and the
+ * stored inverses inv_dnu, inv_nuC (n_nu each). */
+typedef struct lyd_freq_grid {
+    const double *nu, *nuC, *dnu, *inv_dnu, *inv_nuC;
+} lyd_freq_grid;
+
+/* Fields that can be uploaded / downloaded (FP64 host arrays in the layouts above). */
+enum lyd_field {
+    /* (n_nu, n_r, n_z) */
+    LYD_F_J = 0, LYD_F_J_OLD = 1, LYD_F_H_R = 2, LYD_F_H_Z = 3, LYD_F_H_R_OLD = 4, LYD_F_H_Z_OLD = 5,
+    LYD_F_HVOIGT = 6,
+    LYD_F_PHI_NU = 7,    /* uploading phi_nu makes the step read it; otherwise phi_nu is
+                            derived from H_voigt by lyd_update_phi_nu                        */
+    LYD_F_ALPHA_F = 8,   /* uploading alpha_F makes the step read it; otherwise
+                            alpha_F = alpha*H_voigt (+ alpha_cF if uploaded)                 */
+    /* (n_r, n_z) */
+    LYD_F_ALPHA = 16, LYD_F_ALPHA_C = 17, LYD_F_ALPHA_CF = 18, LYD_F_PD = 19, LYD_F_JS = 20,
+    LYD_F_T = 21, LYD_F_DUR_DR = 22, LYD_F_DUR_DZ = 23, LYD_F_DUZ_DR = 24, LYD_F_DUZ_DZ = 25,
+    LYD_F_UR_OVER_R = 26, LYD_F_DRU_R = 27, LYD_F_DRU_Z = 28, LYD_F_F_R = 29, LYD_F_F_Z = 30,
+    /* faces */
+    LYD_F_U_R_STAR = 40,  /* (n_r+1, n_z) */
+    LYD_F_U_Z_STAR = 41   /* (n_r, n_z+1) */
+};
+
+/* Diagnostics of one static-driver step. */
+typedef struct lyd_diag {
+    double M_F, M_F_radial_net, M_F_radial_out, L_tot, f_esc;
+    int32_t kmin, kmax;   /* active window used by this step's advection (0-based) */
+} lyd_diag;
+
+/* Parameters of lyd_static_steps: one static-cloud driver iteration is
+ * AdvectLya! -> LyaEmissionAbsorptionUpdate! -> FrequencyUpdateJLya_AllCells!(true)
+ * -> Update_f_Lya_MF_L_Lya! -> Compute_f_esc_Lya_Cylindrical -> Reset_Delta_rho_u!
+ * (src/StaticCloudTest.jl:357-392). */
+typedef struct lyd_step_params {
+    double c_tilde;        /* reduced speed of light                  */
+    double dt;             /* time step                               */
+    double z_center;       /* cloud centre for the radial M_F         */
+    int32_t bc_r_right, bc_z_bot, bc_z_top;   /* r = 0 is always reflecting */
+    int32_t n_steps;
+} lyd_step_params;
+
+/* ---- context -------------------------------------------------------------------------- */
+int  lyd_create(lyd_ctx **out, const lyd_dims *dims, const lyd_config *cfg);
+int  lyd_destroy(lyd_ctx *ctx);
+const char *lyd_last_error(const lyd_ctx *ctx);
+int  lyd_abi_version(void);
+int  lyd_set_geometry(lyd_ctx *ctx, const lyd_geometry *g);
+int  lyd_set_freq_grid(lyd_ctx *ctx, const lyd_freq_grid *f);
+int  lyd_upload(lyd_ctx *ctx, int32_t field, const double *host, size_t count);
+int  lyd_download(lyd_ctx *ctx, int32_t field, double *host, size_t count);
+int  lyd_synchronize(lyd_ctx *ctx);
+/* The CUDA stream (cudaStream_t) all work of this context is issued on. */
+int  lyd_get_stream(lyd_ctx *ctx, void **stream);
+
+/* ---- the Lyman-alpha step (drop-in replacements) -------------------------------------- */
+/* FindActiveBins, src/UpdateLyaJandH.jl:47-97 */
+int  lyd_find_active_bins(lyd_ctx *ctx, int32_t *kmin, int32_t *kmax);
+/* AdvectLya!, src/UpdateLyaJandH.jl:107-171 (FindActiveBins + AdvectJandH! with
+ * UpdateJold = true + H_old = H); bc_r_left must be LYD_BC_REFLECT (cylindrical axis). */
+int  lyd_advect(lyd_ctx *ctx, double ctdt, int32_t bc_r_left, int32_t bc_r_right,
+                int32_t bc_z_bot, int32_t bc_z_top);
+/* LyaEmissionAbsorptionUpdate!, src/ConstantsAndFunctions.jl:483-573 (reads the uploaded
+ * alpha, alpha_c, pd, js, H_voigt, phi_nu, alpha_F; accumulates into Delta rho u). */
+int  lyd_emission_absorption(lyd_ctx *ctx, double c_tilde, double dt);
+/* FrequencyUpdateJLya_AllCells!, src/UpdateLyaJandH.jl:231-391 with UpdateFreqFactors!
+ * (src/FreqFactors.jl:142-278) and the per-cell tridiagonal solve
+ * (src/TridiagonalSolver.jl:33-58). */
+int  lyd_frequency_update(lyd_ctx *ctx, double ctdt, int32_t update_freq_factors);
+/* UpdateLyaJandH!, src/UpdateLyaJandH.jl:409-486 (advection then frequency update). */
+int  lyd_update_J_and_H(lyd_ctx *ctx, double dt, double c_tilde, int32_t update_freq_factors,
+                        int32_t bc_r_left, int32_t bc_r_right, int32_t bc_z_bot, int32_t bc_z_top);
+/* Update_f_Lya_MF_L_Lya!, src/ConstantsAndFunctions.jl:588-674: fills f_r, f_Z on the
+ * device and returns {M_F, M_F_radial_net, M_F_radial_out, L_tot} in out[4]. */
+int  lyd_force_multiplier(lyd_ctx *ctx, double dt, double z_center, int32_t bc_z_bot, double out[4]);
+/* Compute_f_esc_Lya_Cylindrical, src/ConstantsAndFunctions.jl:969-993 */
+int  lyd_f_esc(lyd_ctx *ctx, double L_allspace, int32_t bc_z_bot, double *f_esc);
+/* Reset_Delta_rho_u!, src/ConstantsAndFunctions.jl:809-816 */
+int  lyd_reset_dru(lyd_ctx *ctx);
+/* n_steps iterations of the static-cloud driver loop, src/StaticCloudTest.jl:357-392, as
+ * fused kernels replayed from a CUDA graph. diag_hist (may be NULL) receives one lyd_diag
+ * per step; with diag_hist == NULL the call returns once the steps are enqueued and any
+ * error is reported by the next synchronising call. */
+int  lyd_static_steps(lyd_ctx *ctx, const lyd_step_params *p, lyd_diag *diag_hist);
+/* Per-kernel device time of the last lyd_static_steps call that had timing enabled:
+ * ms[0] = advection kernel, ms[1] = frequency kernel, ms[2] = reductions (totals). */
+int  lyd_set_timing(lyd_ctx *ctx, int32_t enable);
+int  lyd_get_timing(lyd_ctx *ctx, double ms[3]);
+
+/* ---- set-up and output helpers --------------------------------------------------------- */
+/* Update_Hvoigt! from the uploaded temperature, src/ConstantsAndFunctions.jl:319-357, using
+ * the Voigt look-up tables of src/FastInterpolations.jl:175-275 built on the device. */
+int  lyd_update_hvoigt(lyd_ctx *ctx);
+/* Update_phi_nu!, src/ConstantsAndFunctions.jl:362-393 (normalised over bins kmin..kmax) */
+int  lyd_update_phi_nu(lyd_ctx *ctx, int32_t kmin, int32_t kmax);
+/* pd_Lya, src/LymanAlphaDestruction.jl:43-97, evaluated on the device for n cells; inputs
+ * and output are host arrays of length n. */
+int  lyd_pd_lya(lyd_ctx *ctx, size_t n, const double *nHII, const double *ne, const double *nHI,
+                const double *nHeI, const double *nH2, const double *T, double z, double *pd_out);
+/* GetRHDCFLTimeStep, src/AdvectJandH.jl:29-68, with cell-centred u_r, u_Z (host arrays). */
+int  lyd_cfl_dt(lyd_ctx *ctx, double c_tilde, const double *u_r, const double *u_Z, double cfl,
+                double *dt_out);
+/* Edge-ring spectra of src/SaveHDF5Data_StaticCloudTests.jl:152-199, 392-420:
+ * n_edge = (n_z-2) + 2*(n_r-3) cells; raw and normalised are (n_edge, n_nu) row-major. */
+int  lyd_edge_count(int32_t n_r, int32_t n_z);
+int  lyd_edge_spectra(lyd_ctx *ctx, double *raw, double *norm, int32_t *r_index, int32_t *z_index);
+/* The five Voigt look-up tables the device evaluates (CreateVoigtLUTs,
+ * src/FastInterpolations.jl:178-197): erf, Dawson's integral, exp(-x^2), x exp(-x^2) and
+ * (1-2x^2) exp(-x^2) at x_i = -xmax + 2 xmax i/(n-1), written to out[5*n] table after table.
+ * Host-only; needs no GPU. */
+int  lyd_voigt_tables(double *out, int32_t n, double xmax);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LYDION_M1_H */

@@ -1,0 +1,116 @@
+"""ctypes binding of liblydion_m1.so (the C ABI declared in include/lydion_m1.h).
+
+There is no fallback: if the CUDA library is missing this module raises, and every step
+call goes through the CUDA kernels."""
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "liblydion_m1.so")
+
+LYD_OK = 0
+LYD_ERR_ARG, LYD_ERR_CUDA, LYD_ERR_NONFINITE, LYD_ERR_SOLVE, LYD_ERR_STATE, LYD_ERR_NOMEM = -1, -2, -3, -4, -5, -6
+BC_REFLECT, BC_OUTFLOW = 0, 1
+FLUX_GLF, FLUX_HLL = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+
+F = dict(J=0, J_old=1, H_r=2, H_Z=3, H_r_old=4, H_Z_old=5, Hvoigt=6, phi_nu=7, alpha_F=8,
+         alpha=16, alpha_c=17, alpha_cF=18, pd=19, js=20, T=21, dur_dr=22, dur_dZ=23, duZ_dr=24, duZ_dZ=25,
+         ur_over_r=26, dru_r=27, dru_Z=28, f_r=29, f_Z=30, u_r_star=40, u_Z_star=41)
+
+P = C.POINTER(C.c_double)
+
+
+class LydionError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"lydion_m1 error {code}: {msg}")
+        self.code = code
+
+
+class Dims(C.Structure):
+    _fields_ = [("n_nu", C.c_int32), ("n_r", C.c_int32), ("n_z", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Config(C.Structure):
+    _fields_ = [("flux_method", C.c_int32), ("recoil", C.c_int32), ("precision", C.c_int32),
+                ("kcore_min", C.c_int32), ("kcore_max", C.c_int32), ("keep_freq_factors", C.c_int32),
+                ("alpha_floor", C.c_double), ("j_scale", C.c_double), ("device", C.c_int32),
+                ("reserved", C.c_int32 * 7)]
+
+
+class Geometry(C.Structure):
+    _fields_ = [("r", P), ("Z", P), ("rCoM", P), ("ZCoM", P), ("dV", P), ("inv_dV", P), ("A_r", P), ("A_Z", P),
+                ("inv_r_cell", P), ("dr_L", P), ("dr_R", P), ("inv_dr_i_im1", P), ("inv_dr_ip1_i", P),
+                ("inv_dr_ip2_ip1", P), ("dr_bnd", C.c_double * 10), ("dZ_L", P), ("dZ_R", P),
+                ("inv_dZ_j_jm1", P), ("inv_dZ_jp1_j", P), ("inv_dZ_jp2_jp1", P), ("dZ_bnd", C.c_double * 10)]
+
+
+class FreqGrid(C.Structure):
+    _fields_ = [("nu", P), ("nuC", P), ("dnu", P), ("inv_dnu", P), ("inv_nuC", P)]
+
+
+class StepParams(C.Structure):
+    _fields_ = [("c_tilde", C.c_double), ("dt", C.c_double), ("z_center", C.c_double), ("bc_r_right", C.c_int32),
+                ("bc_z_bot", C.c_int32), ("bc_z_top", C.c_int32), ("n_steps", C.c_int32)]
+
+
+class Diag(C.Structure):
+    _fields_ = [("M_F", C.c_double), ("M_F_radial_net", C.c_double), ("M_F_radial_out", C.c_double),
+                ("L_tot", C.c_double), ("f_esc", C.c_double), ("kmin", C.c_int32), ("kmax", C.c_int32)]
+
+
+# name -> (restype, argtypes); this list is the ABI surface checked by the CPU tests
+I32, D, SZ, VP = C.c_int32, C.c_double, C.c_size_t, C.c_void_p
+SIGNATURES = {
+    "lyd_create": (C.c_int, [C.POINTER(VP), C.POINTER(Dims), C.POINTER(Config)]),
+    "lyd_destroy": (C.c_int, [VP]),
+    "lyd_last_error": (C.c_char_p, [VP]),
+    "lyd_abi_version": (C.c_int, []),
+    "lyd_set_geometry": (C.c_int, [VP, C.POINTER(Geometry)]),
+    "lyd_set_freq_grid": (C.c_int, [VP, C.POINTER(FreqGrid)]),
+    "lyd_upload": (C.c_int, [VP, I32, P, SZ]),
+    "lyd_download": (C.c_int, [VP, I32, P, SZ]),
+    "lyd_synchronize": (C.c_int, [VP]),
+    "lyd_get_stream": (C.c_int, [VP, C.POINTER(VP)]),
+    "lyd_find_active_bins": (C.c_int, [VP, C.POINTER(I32), C.POINTER(I32)]),
+    "lyd_advect": (C.c_int, [VP, D, I32, I32, I32, I32]),
+    "lyd_emission_absorption": (C.c_int, [VP, D, D]),
+    "lyd_frequency_update": (C.c_int, [VP, D, I32]),
+    "lyd_update_J_and_H": (C.c_int, [VP, D, D, I32, I32, I32, I32, I32]),
+    "lyd_force_multiplier": (C.c_int, [VP, D, D, I32, P]),
+    "lyd_f_esc": (C.c_int, [VP, D, I32, P]),
+    "lyd_reset_dru": (C.c_int, [VP]),
+    "lyd_static_steps": (C.c_int, [VP, C.POINTER(StepParams), C.POINTER(Diag)]),
+    "lyd_set_timing": (C.c_int, [VP, I32]),
+    "lyd_get_timing": (C.c_int, [VP, P]),
+    "lyd_update_hvoigt": (C.c_int, [VP]),
+    "lyd_update_phi_nu": (C.c_int, [VP, I32, I32]),
+    "lyd_pd_lya": (C.c_int, [VP, SZ, P, P, P, P, P, P, D, P]),
+    "lyd_cfl_dt": (C.c_int, [VP, D, P, P, D, P]),
+    "lyd_edge_count": (C.c_int, [I32, I32]),
+    "lyd_edge_spectra": (C.c_int, [VP, P, P, C.POINTER(I32), C.POINTER(I32)]),
+    "lyd_voigt_tables": (C.c_int, [P, I32, D]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load liblydion_m1.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m lydion_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc, ctx=None):
+    if rc != LYD_OK:
+        msg = lib().lyd_last_error(ctx).decode() if ctx else ""
+        raise LydionError(rc, msg)

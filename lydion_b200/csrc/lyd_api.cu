@@ -1,0 +1,826 @@
+// lyd_api.cu -- the C ABI (include/lydion_m1.h): context, device state, and the drop-in
+// entry points of the Lyman-alpha M1 step.
+//
+// Device state. J, H_r, H_Z live in two buffer sets. `cur` holds the current values; the
+// other set holds J_old, H_r_old, H_Z_old unless `old_alias` is set, in which case the old
+// values equal the current ones (true after every step phase of the reference:
+// AdvectLya! copies J_old = J and H_old = H, the emission and frequency updates end by
+// setting the old arrays to the new ones). The advection writes into the spare set and the
+// sets swap; the emission and frequency kernels work per cell in place. The fused
+// static-cloud step advects cur -> spare and then runs emission + frequency spare -> cur,
+// so a step starts and ends in the same set and one CUDA graph replays every step.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "lyd_internal.h"
+#include "lyd_physics.cuh"
+#include "lydion_m1.h"
+
+using namespace lyd;
+
+namespace {
+constexpr int kLutN = 200001;        // src/FastInterpolations.jl:175-176
+constexpr double kLutXmax = 1000.0;
+}
+
+struct lyd_ctx {
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    int nnu = 0, nr = 0, nz = 0;
+    size_t ncell = 0, n3 = 0;
+    lyd_config cfg{};
+    int prec = 0;
+    size_t ssz = 8;
+    double jscale = 1.0, jeps_s = kJeps, heps2_s = kHeps * kHeps;
+    void *set[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+    int cur = 0;
+    bool old_alias = true;
+    void *Hv = nullptr;
+    bool hv_set = false;
+    void *phi = nullptr;
+    bool phi_explicit = false;
+    double *phi_inv = nullptr;
+    int phi_kmin = 0, phi_kmax = -1;
+    bool phi_ready = false;
+    void *aF = nullptr;
+    bool aF_explicit = false;
+    double *Ff[3] = {nullptr, nullptr, nullptr};
+    bool ff_valid = false;
+    double *cellf[16] = {};        // per-cell fields, index = field - 16
+    bool cell_set[16] = {};
+    double *u_r_star = nullptr, *u_Z_star = nullptr;
+    double *dV = nullptr, *inv_dV = nullptr, *A_r = nullptr, *A_Z = nullptr, *inv_r_cell = nullptr;
+    double *rCoM = nullptr, *ZCoM = nullptr, *rint = nullptr, *zint = nullptr, *r_if = nullptr, *Z_if = nullptr;
+    bool geom_set = false;
+    double *nu = nullptr, *nuC = nullptr, *dnu = nullptr, *inv_dnu = nullptr, *inv_nuC = nullptr;
+    bool freq_set = false;
+    int fblocks = 0;
+    double *partials = nullptr;
+    int *kwin = nullptr;
+    bool active_valid = false;
+    double *hist = nullptr;
+    int hist_cap = 0;
+    int *step_ctr = nullptr;
+    double *last = nullptr;
+    int *err = nullptr;
+    double *lut = nullptr;
+    double *stage = nullptr;       // device FP64 staging buffer (n3 doubles)
+    double *small = nullptr;       // device scratch (256 doubles)
+    cudaGraphExec_t gexec = nullptr;
+    double gkey[3] = {0, 0, 0};
+    int gkey_i[4] = {-1, -1, -1, -1};
+    bool timing = false;
+    cudaEvent_t ev[8] = {};
+    double ms[3] = {0, 0, 0};
+    std::string msg;
+};
+
+enum { CF_ALPHA = 0, CF_ALPHA_C, CF_ALPHA_CF, CF_PD, CF_JS, CF_T, CF_DUR_DR, CF_DUR_DZ, CF_DUZ_DR, CF_DUZ_DZ,
+       CF_UR_OVER_R, CF_DRU_R, CF_DRU_Z, CF_F_R, CF_F_Z, CF_N };
+
+static int fail(lyd_ctx *c, int code, const std::string &m) {
+    if (c) c->msg = m;
+    return code;
+}
+
+#define LYD_CU(ctx, call)                                                                          \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(ctx, LYD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
+    } while (0)
+
+static int dalloc(lyd_ctx *c, void **p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+    if (e != cudaSuccess) return fail(c, LYD_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    e = cudaMemsetAsync(*p, 0, bytes ? bytes : 16, c->st);
+    if (e != cudaSuccess) return fail(c, LYD_ERR_CUDA, cudaGetErrorString(e));
+    return LYD_OK;
+}
+#define LYD_TRY(x)              \
+    do {                        \
+        int r_ = (x);           \
+        if (r_ != LYD_OK) return r_; \
+    } while (0)
+
+static void *Jc(lyd_ctx *c, int q) { return c->set[c->cur][q]; }
+static void *Jold(lyd_ctx *c, int q) { return c->old_alias ? c->set[c->cur][q] : c->set[1 - c->cur][q]; }
+
+static int check_err(lyd_ctx *c) {
+    int h = 0;
+    LYD_CU(c, cudaMemcpyAsync(&h, c->err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    LYD_CU(c, cudaStreamSynchronize(c->st));
+    if (h) {
+        LYD_CU(c, cudaMemsetAsync(c->err, 0, sizeof(int), c->st));
+        if (h & ERRB_NONFINITE) return fail(c, LYD_ERR_NONFINITE, "non-finite value in J or H");
+        return fail(c, LYD_ERR_SOLVE, "zero pivot in a frequency tridiagonal system");
+    }
+    return LYD_OK;
+}
+
+// Every lyd_* definition below has C linkage through its declaration in lydion_m1.h.
+
+int lyd_abi_version(void) { return LYD_ABI_VERSION; }
+
+const char *lyd_last_error(const lyd_ctx *c) { return c ? c->msg.c_str() : "null context"; }
+
+int lyd_edge_count(int32_t n_r, int32_t n_z) { return (n_z - 2) + 2 * (n_r - 3); }
+
+int lyd_create(lyd_ctx **out, const lyd_dims *d, const lyd_config *cfg) {
+    if (!out || !d || !cfg) return LYD_ERR_ARG;
+    *out = nullptr;
+    if (d->n_nu < 4 || d->n_nu > 256 || d->n_r < 3 || d->n_z < 3) return LYD_ERR_ARG;
+    if (cfg->precision != LYD_PREC_FP64 && cfg->precision != LYD_PREC_MIXED) return LYD_ERR_ARG;
+    if (cfg->flux_method != LYD_FLUX_GLF && cfg->flux_method != LYD_FLUX_HLL) return LYD_ERR_ARG;
+    if (cfg->kcore_min < 0 || cfg->kcore_max >= d->n_nu || cfg->kcore_min > cfg->kcore_max) return LYD_ERR_ARG;
+    lyd_ctx *c = new lyd_ctx();
+    c->cfg = *cfg;
+    c->dev = cfg->device;
+    if (cudaSetDevice(c->dev) != cudaSuccess) { delete c; return LYD_ERR_CUDA; }
+    if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) { delete c; return LYD_ERR_CUDA; }
+    c->nnu = d->n_nu; c->nr = d->n_r; c->nz = d->n_z;
+    c->ncell = (size_t)c->nr * c->nz;
+    c->n3 = c->ncell * c->nnu;
+    c->prec = cfg->precision;
+    c->ssz = c->prec == LYD_PREC_FP64 ? sizeof(double) : sizeof(float);
+    if (c->prec == LYD_PREC_MIXED) {
+        c->jscale = cfg->j_scale > 0.0 ? cfg->j_scale : 1e-12;
+        c->jeps_s = 1e-30;
+        c->heps2_s = 0.0;
+    }
+    int r = LYD_OK;
+    auto A = [&](void **p, size_t b) { if (r == LYD_OK) r = dalloc(c, p, b); };
+    for (int s = 0; s < 2; s++)
+        for (int q = 0; q < 3; q++) A(&c->set[s][q], c->n3 * c->ssz);
+    A(&c->Hv, c->n3 * c->ssz);
+    A((void **)&c->phi_inv, c->ncell * 8);
+    for (int q = 0; q < CF_N; q++) A((void **)&c->cellf[q], c->ncell * 8);
+    A((void **)&c->u_r_star, (size_t)(c->nr + 1) * c->nz * 8);
+    A((void **)&c->u_Z_star, (size_t)c->nr * (c->nz + 1) * 8);
+    A((void **)&c->dV, c->ncell * 8); A((void **)&c->inv_dV, c->ncell * 8);
+    A((void **)&c->A_r, (size_t)(c->nr + 1) * c->nz * 8); A((void **)&c->A_Z, (size_t)c->nr * (c->nz + 1) * 8);
+    A((void **)&c->inv_r_cell, c->nr * 8); A((void **)&c->rCoM, c->nr * 8); A((void **)&c->ZCoM, c->nz * 8);
+    A((void **)&c->rint, (size_t)(c->nr + 1) * 5 * 8); A((void **)&c->zint, (size_t)(c->nz + 1) * 5 * 8);
+    A((void **)&c->r_if, (c->nr + 1) * 8); A((void **)&c->Z_if, (c->nz + 1) * 8);
+    A((void **)&c->nu, (c->nnu + 1) * 8); A((void **)&c->nuC, c->nnu * 8); A((void **)&c->dnu, c->nnu * 8);
+    A((void **)&c->inv_dnu, c->nnu * 8); A((void **)&c->inv_nuC, c->nnu * 8);
+    c->fblocks = freq_blocks((int)c->ncell, c->dev);
+    A((void **)&c->partials, (size_t)c->fblocks * (c->nnu + kExtraCols) * 8);
+    A((void **)&c->kwin, 2 * sizeof(int));
+    A((void **)&c->step_ctr, sizeof(int));
+    A((void **)&c->last, 8 * sizeof(double));
+    A((void **)&c->err, sizeof(int));
+    A((void **)&c->stage, c->n3 * 8);
+    A((void **)&c->small, 512 * 8);
+    if (cfg->keep_freq_factors)
+        for (int q = 0; q < 3; q++) A((void **)&c->Ff[q], c->n3 * 8);
+    if (r != LYD_OK) {
+        lyd_destroy(c);
+        return r;
+    }
+    for (int q = 0; q < 8; q++) cudaEventCreate(&c->ev[q]);
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) { lyd_destroy(c); return LYD_ERR_CUDA; }
+    *out = c;
+    return LYD_OK;
+}
+
+int lyd_destroy(lyd_ctx *c) {
+    if (!c) return LYD_OK;
+    cudaSetDevice(c->dev);
+    if (c->st) cudaStreamSynchronize(c->st);
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    for (int s = 0; s < 2; s++)
+        for (int q = 0; q < 3; q++) cudaFree(c->set[s][q]);
+    void *ps[] = {c->Hv, c->phi, c->phi_inv, c->aF, c->Ff[0], c->Ff[1], c->Ff[2], c->u_r_star, c->u_Z_star, c->dV,
+                  c->inv_dV, c->A_r, c->A_Z, c->inv_r_cell, c->rCoM, c->ZCoM, c->rint, c->zint, c->r_if, c->Z_if,
+                  c->nu, c->nuC, c->dnu, c->inv_dnu, c->inv_nuC, c->partials, c->kwin, c->hist, c->step_ctr,
+                  c->last, c->err, c->lut, c->stage, c->small};
+    for (void *p : ps) cudaFree(p);
+    for (int q = 0; q < CF_N; q++) cudaFree(c->cellf[q]);
+    for (int q = 0; q < 8; q++)
+        if (c->ev[q]) cudaEventDestroy(c->ev[q]);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+    return LYD_OK;
+}
+
+int lyd_get_stream(lyd_ctx *c, void **s) {
+    if (!c || !s) return LYD_ERR_ARG;
+    *s = (void *)c->st;
+    return LYD_OK;
+}
+
+int lyd_synchronize(lyd_ctx *c) {
+    if (!c) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    return check_err(c);
+}
+
+static int h2d(lyd_ctx *c, void *dst, const double *src, size_t n) {
+    if (!src) return fail(c, LYD_ERR_ARG, "null host pointer");
+    LYD_CU(c, cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyHostToDevice, c->st));
+    return LYD_OK;
+}
+
+int lyd_set_geometry(lyd_ctx *c, const lyd_geometry *g) {
+    if (!c || !g) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    const int nr = c->nr, nz = c->nz;
+    LYD_TRY(h2d(c, c->dV, g->dV, c->ncell));
+    LYD_TRY(h2d(c, c->inv_dV, g->inv_dV, c->ncell));
+    LYD_TRY(h2d(c, c->A_r, g->A_r, (size_t)(nr + 1) * nz));
+    LYD_TRY(h2d(c, c->A_Z, g->A_Z, (size_t)nr * (nz + 1)));
+    LYD_TRY(h2d(c, c->inv_r_cell, g->inv_r_cell, nr));
+    LYD_TRY(h2d(c, c->rCoM, g->rCoM, nr));
+    LYD_TRY(h2d(c, c->ZCoM, g->ZCoM, nz));
+    LYD_TRY(h2d(c, c->r_if, g->r, nr + 1));
+    LYD_TRY(h2d(c, c->Z_if, g->Z, nz + 1));
+    // PLM intervals per face: face 0 = inner boundary, face n = outer boundary, face f in
+    // between uses the cell arrays at f-1 (src/AdvectJandH.jl:628-638, 775-779, 884-887).
+    auto pack = [](int n, const double *L, const double *R, const double *a, const double *b, const double *cc,
+                   const double *bnd, std::vector<double> &o) {
+        o.assign((size_t)(n + 1) * 5, 0.0);
+        for (int t = 0; t < 5; t++) o[t] = bnd[t];
+        for (int f = 1; f < n; f++) {
+            o[5 * f + 0] = L[f - 1]; o[5 * f + 1] = R[f - 1]; o[5 * f + 2] = a[f - 1];
+            o[5 * f + 3] = b[f - 1]; o[5 * f + 4] = cc[f - 1];
+        }
+        for (int t = 0; t < 5; t++) o[5 * n + t] = bnd[5 + t];
+    };
+    if (!g->dr_L || !g->dr_R || !g->inv_dr_i_im1 || !g->inv_dr_ip1_i || !g->inv_dr_ip2_ip1 || !g->dZ_L ||
+        !g->dZ_R || !g->inv_dZ_j_jm1 || !g->inv_dZ_jp1_j || !g->inv_dZ_jp2_jp1)
+        return fail(c, LYD_ERR_ARG, "missing interval arrays");
+    std::vector<double> pr, pz;
+    pack(nr, g->dr_L, g->dr_R, g->inv_dr_i_im1, g->inv_dr_ip1_i, g->inv_dr_ip2_ip1, g->dr_bnd, pr);
+    pack(nz, g->dZ_L, g->dZ_R, g->inv_dZ_j_jm1, g->inv_dZ_jp1_j, g->inv_dZ_jp2_jp1, g->dZ_bnd, pz);
+    LYD_CU(c, cudaMemcpyAsync(c->rint, pr.data(), pr.size() * 8, cudaMemcpyHostToDevice, c->st));
+    LYD_CU(c, cudaMemcpyAsync(c->zint, pz.data(), pz.size() * 8, cudaMemcpyHostToDevice, c->st));
+    LYD_CU(c, cudaStreamSynchronize(c->st));
+    c->geom_set = true;
+    return LYD_OK;
+}
+
+int lyd_set_freq_grid(lyd_ctx *c, const lyd_freq_grid *f) {
+    if (!c || !f) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    LYD_TRY(h2d(c, c->nu, f->nu, c->nnu + 1));
+    LYD_TRY(h2d(c, c->nuC, f->nuC, c->nnu));
+    LYD_TRY(h2d(c, c->dnu, f->dnu, c->nnu));
+    LYD_TRY(h2d(c, c->inv_dnu, f->inv_dnu, c->nnu));
+    LYD_TRY(h2d(c, c->inv_nuC, f->inv_nuC, c->nnu));
+    LYD_CU(c, cudaStreamSynchronize(c->st));
+    c->freq_set = true;
+    c->active_valid = false;
+    return LYD_OK;
+}
+
+// Make the old set a real copy before one of J/H or J_old/H_old is overwritten alone.
+static int materialize_old(lyd_ctx *c) {
+    if (!c->old_alias) return LYD_OK;
+    for (int q = 0; q < 3; q++)
+        LYD_CU(c, cudaMemcpyAsync(c->set[1 - c->cur][q], c->set[c->cur][q], c->n3 * c->ssz, cudaMemcpyDeviceToDevice,
+                                  c->st));
+    c->old_alias = false;
+    return LYD_OK;
+}
+
+static int upload3(lyd_ctx *c, void *dst, const double *host, double scale) {
+    LYD_CU(c, cudaMemcpyAsync(c->stage, host, c->n3 * 8, cudaMemcpyHostToDevice, c->st));
+    launch_convert_in(c->prec, c->stage, dst, c->n3, scale, c->st);
+    LYD_CU(c, cudaGetLastError());
+    return LYD_OK;
+}
+
+int lyd_upload(lyd_ctx *c, int32_t field, const double *host, size_t count) {
+    if (!c) return LYD_ERR_ARG;
+    if (!host) return fail(c, LYD_ERR_ARG, "null host pointer");
+    cudaSetDevice(c->dev);
+    const size_t n3 = c->n3, nc = c->ncell;
+    if (field <= LYD_F_H_Z_OLD) {
+        if (count != n3) return fail(c, LYD_ERR_ARG, "wrong element count for a (n_nu, n_r, n_z) field");
+        LYD_TRY(materialize_old(c));
+        int q = (field == LYD_F_J || field == LYD_F_J_OLD) ? 0 : ((field == LYD_F_H_R || field == LYD_F_H_R_OLD) ? 1 : 2);
+        bool old = field == LYD_F_J_OLD || field == LYD_F_H_R_OLD || field == LYD_F_H_Z_OLD;
+        void *dst = old ? c->set[1 - c->cur][q] : c->set[c->cur][q];
+        LYD_TRY(upload3(c, dst, host, c->jscale));
+        if (q == 0 && !old) c->active_valid = false;
+    } else if (field == LYD_F_HVOIGT) {
+        if (count != n3) return fail(c, LYD_ERR_ARG, "wrong element count for H_voigt");
+        LYD_TRY(upload3(c, c->Hv, host, 1.0));
+        c->hv_set = true;
+        if (!c->phi_explicit) c->phi_ready = false;
+    } else if (field == LYD_F_PHI_NU || field == LYD_F_ALPHA_F) {
+        if (count != n3) return fail(c, LYD_ERR_ARG, "wrong element count");
+        void **p = field == LYD_F_PHI_NU ? &c->phi : &c->aF;
+        if (!*p) LYD_TRY(dalloc(c, p, n3 * c->ssz));
+        LYD_TRY(upload3(c, *p, host, 1.0));
+        if (field == LYD_F_PHI_NU) { c->phi_explicit = true; c->phi_ready = true; }
+        else c->aF_explicit = true;
+    } else if (field >= LYD_F_ALPHA && field <= LYD_F_F_Z) {
+        if (count != nc) return fail(c, LYD_ERR_ARG, "wrong element count for a per-cell field");
+        int q = field - LYD_F_ALPHA;
+        LYD_TRY(h2d(c, c->cellf[q], host, nc));
+        c->cell_set[q] = true;
+    } else if (field == LYD_F_U_R_STAR) {
+        if (count != (size_t)(c->nr + 1) * c->nz) return fail(c, LYD_ERR_ARG, "wrong element count for u_r_star");
+        LYD_TRY(h2d(c, c->u_r_star, host, count));
+    } else if (field == LYD_F_U_Z_STAR) {
+        if (count != (size_t)c->nr * (c->nz + 1)) return fail(c, LYD_ERR_ARG, "wrong element count for u_Z_star");
+        LYD_TRY(h2d(c, c->u_Z_star, host, count));
+    } else {
+        return fail(c, LYD_ERR_ARG, "unknown field");
+    }
+    LYD_CU(c, cudaStreamSynchronize(c->st));
+    return LYD_OK;
+}
+
+int lyd_download(lyd_ctx *c, int32_t field, double *host, size_t count) {
+    if (!c) return LYD_ERR_ARG;
+    if (!host) return fail(c, LYD_ERR_ARG, "null host pointer");
+    cudaSetDevice(c->dev);
+    const size_t n3 = c->n3, nc = c->ncell;
+    const void *src = nullptr;
+    size_t n = 0;
+    double scale = 1.0;
+    bool is3 = false;
+    if (field <= LYD_F_H_Z_OLD) {
+        int q = (field == LYD_F_J || field == LYD_F_J_OLD) ? 0 : ((field == LYD_F_H_R || field == LYD_F_H_R_OLD) ? 1 : 2);
+        bool old = field == LYD_F_J_OLD || field == LYD_F_H_R_OLD || field == LYD_F_H_Z_OLD;
+        src = old ? Jold(c, q) : Jc(c, q);
+        n = n3; scale = c->jscale; is3 = true;
+    } else if (field == LYD_F_HVOIGT) {
+        src = c->Hv; n = n3; is3 = true;
+    } else if (field == LYD_F_PHI_NU || field == LYD_F_ALPHA_F) {
+        src = field == LYD_F_PHI_NU ? c->phi : c->aF;
+        if (!src) return fail(c, LYD_ERR_STATE, "field is derived on the device and was never uploaded");
+        n = n3; is3 = true;
+    } else if (field >= LYD_F_ALPHA && field <= LYD_F_F_Z) {
+        src = c->cellf[field - LYD_F_ALPHA]; n = nc;
+    } else if (field == LYD_F_U_R_STAR) {
+        src = c->u_r_star; n = (size_t)(c->nr + 1) * c->nz;
+    } else if (field == LYD_F_U_Z_STAR) {
+        src = c->u_Z_star; n = (size_t)c->nr * (c->nz + 1);
+    } else {
+        return fail(c, LYD_ERR_ARG, "unknown field");
+    }
+    if (count != n) return fail(c, LYD_ERR_ARG, "wrong element count");
+    if (is3) {
+        launch_convert_out(c->prec, src, c->stage, n, scale, c->st);
+        LYD_CU(c, cudaGetLastError());
+        LYD_CU(c, cudaMemcpyAsync(host, c->stage, n * 8, cudaMemcpyDeviceToHost, c->st));
+    } else {
+        LYD_CU(c, cudaMemcpyAsync(host, src, n * 8, cudaMemcpyDeviceToHost, c->st));
+    }
+    return check_err(c);
+}
+
+// ---- argument blocks -------------------------------------------------------------------------
+template <typename S>
+static void fill_adv(lyd_ctx *c, AdvArgs<S> &a, int in_set, int out_set, double ctdt, int bcr, int bzb, int bzt) {
+    a.J = (const S *)c->set[in_set][0]; a.Hr = (const S *)c->set[in_set][1]; a.HZ = (const S *)c->set[in_set][2];
+    a.Jo = (S *)c->set[out_set][0]; a.Hro = (S *)c->set[out_set][1]; a.HZo = (S *)c->set[out_set][2];
+    a.aF = c->aF_explicit ? (const S *)c->aF : nullptr;
+    a.Hv = (const S *)c->Hv;
+    a.alpha = c->cellf[CF_ALPHA];
+    a.alpha_cF = c->cell_set[CF_ALPHA_CF] ? c->cellf[CF_ALPHA_CF] : nullptr;
+    a.A_r = c->A_r; a.A_Z = c->A_Z; a.inv_dV = c->inv_dV; a.inv_r_cell = c->inv_r_cell;
+    a.rint = c->rint; a.zint = c->zint;
+    a.u_r_star = c->u_r_star; a.u_Z_star = c->u_Z_star;
+    a.dur_dr = c->cellf[CF_DUR_DR]; a.dur_dZ = c->cellf[CF_DUR_DZ]; a.duZ_dr = c->cellf[CF_DUZ_DR];
+    a.duZ_dZ = c->cellf[CF_DUZ_DZ]; a.ur_over_r = c->cellf[CF_UR_OVER_R];
+    a.kwin = c->kwin;
+    a.nnu = c->nnu; a.nr = c->nr; a.nz = c->nz;
+    a.ctdt = ctdt; a.jeps = c->jeps_s; a.heps2 = c->heps2_s;
+    a.bc_r_right = bcr; a.bc_z_bot = bzb; a.bc_z_top = bzt;
+}
+
+template <typename S>
+static void fill_freq(lyd_ctx *c, FreqArgs<S> &a, const void *Jin, const void *Hrin, const void *HZin, const void *Jo,
+                      void *Jout, void *Hrout, void *HZout) {
+    memset(&a, 0, sizeof(a));
+    a.Jin = (const S *)Jin; a.Hrin = (const S *)Hrin; a.HZin = (const S *)HZin; a.Jold = (const S *)Jo;
+    a.Jout = (S *)Jout; a.Hrout = (S *)Hrout; a.HZout = (S *)HZout;
+    a.Hv = (const S *)c->Hv;
+    a.phi = c->phi_explicit ? (const S *)c->phi : nullptr;
+    a.phi_inv = c->phi_inv; a.phi_kmin = c->phi_kmin; a.phi_kmax = c->phi_kmax;
+    a.aF = c->aF_explicit ? (const S *)c->aF : nullptr;
+    a.alpha = c->cellf[CF_ALPHA]; a.alpha_c = c->cellf[CF_ALPHA_C];
+    a.alpha_cF = c->cell_set[CF_ALPHA_CF] ? c->cellf[CF_ALPHA_CF] : nullptr;
+    a.pd = c->cellf[CF_PD]; a.js = c->cellf[CF_JS]; a.T = c->cellf[CF_T];
+    a.dur_dr = c->cellf[CF_DUR_DR]; a.dur_dZ = c->cellf[CF_DUR_DZ]; a.duZ_dr = c->cellf[CF_DUZ_DR];
+    a.duZ_dZ = c->cellf[CF_DUZ_DZ]; a.ur_over_r = c->cellf[CF_UR_OVER_R];
+    a.nu = c->nu; a.nuC = c->nuC; a.dnu = c->dnu; a.inv_dnu = c->inv_dnu; a.inv_nuC = c->inv_nuC;
+    a.dV = c->dV; a.A_r = c->A_r; a.A_Z = c->A_Z; a.rCoM = c->rCoM; a.ZCoM = c->ZCoM;
+    a.alpha_floor = c->cfg.alpha_floor;
+    a.jeps = c->jeps_s; a.heps2 = c->heps2_s; a.j_scale = c->jscale;
+    a.recoil = c->cfg.recoil;
+    a.partials = c->partials; a.err = c->err;
+    a.nnu = c->nnu; a.nr = c->nr; a.nz = c->nz;
+}
+
+static int need_inputs(lyd_ctx *c, bool emission, bool freq) {
+    if (!c->geom_set) return fail(c, LYD_ERR_STATE, "geometry not set (lyd_set_geometry)");
+    if (!c->freq_set) return fail(c, LYD_ERR_STATE, "frequency grid not set (lyd_set_freq_grid)");
+    if ((emission || freq) && !c->hv_set) return fail(c, LYD_ERR_STATE, "H_voigt not set");
+    if (emission && !c->phi_ready)
+        return fail(c, LYD_ERR_STATE, "phi_nu not set (upload it or call lyd_update_phi_nu)");
+    if (freq && !c->cell_set[CF_T]) return fail(c, LYD_ERR_STATE, "temperature T not uploaded");
+    return LYD_OK;
+}
+
+static RedArgs red_args(lyd_ctx *c, int parts) {
+    RedArgs r;
+    memset(&r, 0, sizeof(r));
+    r.partials = c->partials; r.nblocks = c->fblocks; r.nnu = c->nnu; r.parts = parts;
+    r.kcore_min = c->cfg.kcore_min; r.kcore_max = c->cfg.kcore_max;
+    r.j_scale = c->jscale; r.kwin = c->kwin; r.err = c->err; r.last = c->last;
+    return r;
+}
+
+static int run_find_active(lyd_ctx *c) {
+    launch_find_active(c->prec, Jc(c, 0), c->nnu, c->nr, c->nz, c->dnu, c->dV, c->jeps_s, c->partials, c->fblocks,
+                       c->st);
+    RedArgs r = red_args(c, PART_ACTIVE);
+    launch_reduce(r, c->st);
+    LYD_CU(c, cudaGetLastError());
+    c->active_valid = true;
+    return LYD_OK;
+}
+
+int lyd_find_active_bins(lyd_ctx *c, int32_t *kmin, int32_t *kmax) {
+    if (!c || !kmin || !kmax) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    LYD_TRY(need_inputs(c, false, false));
+    LYD_TRY(run_find_active(c));
+    int h[2];
+    LYD_CU(c, cudaMemcpyAsync(h, c->kwin, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+    LYD_TRY(check_err(c));
+    *kmin = h[0];
+    *kmax = h[1];
+    return LYD_OK;
+}
+
+static int check_bcs(lyd_ctx *c, int l, int r, int b, int t) {
+    if (l != LYD_BC_REFLECT) return fail(c, LYD_ERR_ARG, "the r = 0 boundary of a cylindrical grid is always reflecting");
+    auto ok = [](int v) { return v == LYD_BC_REFLECT || v == LYD_BC_OUTFLOW; };
+    if (!ok(r) || !ok(b) || !ok(t)) return fail(c, LYD_ERR_ARG, "unknown boundary condition");
+    return LYD_OK;
+}
+
+static int do_advect(lyd_ctx *c, double ctdt, int bcr, int bzb, int bzt) {
+    if (!c->active_valid) LYD_TRY(run_find_active(c));
+    int in = c->cur, out = 1 - c->cur;
+    if (c->prec == 0) {
+        AdvArgs<double> a;
+        fill_adv<double>(c, a, in, out, ctdt, bcr, bzb, bzt);
+        launch_advect(0, c->cfg.flux_method, &a, c->nnu, c->nr, c->nz, c->st);
+    } else {
+        AdvArgs<float> a;
+        fill_adv<float>(c, a, in, out, ctdt, bcr, bzb, bzt);
+        launch_advect(1, c->cfg.flux_method, &a, c->nnu, c->nr, c->nz, c->st);
+    }
+    LYD_CU(c, cudaGetLastError());
+    c->cur = out;
+    c->old_alias = true;
+    c->active_valid = false;
+    return LYD_OK;
+}
+
+int lyd_advect(lyd_ctx *c, double ctdt, int32_t bl, int32_t br, int32_t bb, int32_t bt) {
+    if (!c) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    LYD_TRY(check_bcs(c, bl, br, bb, bt));
+    LYD_TRY(need_inputs(c, false, false));
+    if (!(ctdt > 0.0)) return fail(c, LYD_ERR_ARG, "c~ dt must be positive");
+    return do_advect(c, ctdt, br, bb, bt);
+}
+
+template <typename S>
+static int freq_call(lyd_ctx *c, bool emission, bool freq, double ct, double dt, double ctdt, int update_ff,
+                     int parts) {
+    FreqArgs<S> a;
+    fill_freq<S>(c, a, Jc(c, 0), Jc(c, 1), Jc(c, 2), Jold(c, 0), Jc(c, 0), Jc(c, 1), Jc(c, 2));
+    a.do_emission = emission; a.do_freq = freq; a.update_ff = update_ff;
+    a.c_tilde = ct; a.dt = dt; a.ctdt = ctdt;
+    a.dru_r = c->cellf[CF_DRU_R]; a.dru_Z = c->cellf[CF_DRU_Z];
+    if (c->cfg.keep_freq_factors) { a.Fkp = c->Ff[0]; a.Fk = c->Ff[1]; a.Fkm = c->Ff[2]; }
+    a.parts = parts;
+    launch_freq(c->prec, &a, c->nnu, (int)c->ncell, c->fblocks, c->st);
+    LYD_CU(c, cudaGetLastError());
+    return LYD_OK;
+}
+
+int lyd_emission_absorption(lyd_ctx *c, double ct, double dt) {
+    if (!c) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    LYD_TRY(need_inputs(c, true, false));
+    if (!(ct > 0.0) || !(dt > 0.0)) return fail(c, LYD_ERR_ARG, "c~ and dt must be positive");
+    int r = c->prec == 0 ? freq_call<double>(c, true, false, ct, dt, ct * dt, 1, 0)
+                         : freq_call<float>(c, true, false, ct, dt, ct * dt, 1, 0);
+    if (r != LYD_OK) return r;
+    c->old_alias = true;
+    c->active_valid = false;
+    return LYD_OK;
+}
+
+int lyd_frequency_update(lyd_ctx *c, double ctdt, int32_t update_ff) {
+    if (!c) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    LYD_TRY(need_inputs(c, false, true));
+    if (!(ctdt > 0.0)) return fail(c, LYD_ERR_ARG, "c~ dt must be positive");
+    if (!update_ff && !(c->cfg.keep_freq_factors && c->ff_valid))
+        return fail(c, LYD_ERR_STATE, "update_freq_factors = 0 needs keep_freq_factors and a previous update");
+    int r = c->prec == 0 ? freq_call<double>(c, false, true, 1.0, 1.0, ctdt, update_ff ? 1 : 0, PART_ACTIVE)
+                         : freq_call<float>(c, false, true, 1.0, 1.0, ctdt, update_ff ? 1 : 0, PART_ACTIVE);
+    if (r != LYD_OK) return r;
+    launch_reduce(red_args(c, PART_ACTIVE), c->st);
+    LYD_CU(c, cudaGetLastError());
+    if (update_ff && c->cfg.keep_freq_factors) c->ff_valid = true;
+    c->old_alias = true;
+    c->active_valid = true;
+    return LYD_OK;
+}
+
+int lyd_update_J_and_H(lyd_ctx *c, double dt, double ct, int32_t update_ff, int32_t bl, int32_t br, int32_t bb,
+                       int32_t bt) {
+    if (!c) return LYD_ERR_ARG;
+    double ctdt = ct * dt;
+    LYD_TRY(lyd_advect(c, ctdt, bl, br, bb, bt));
+    return lyd_frequency_update(c, ctdt, update_ff);
+}
+
+int lyd_reset_dru(lyd_ctx *c) {
+    if (!c) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_R], 0, c->ncell * 8, c->st));
+    LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_Z], 0, c->ncell * 8, c->st));
+    return LYD_OK;
+}
+
+int lyd_force_multiplier(lyd_ctx *c, double dt, double zc, int32_t bc_z_bot, double out[4]) {
+    if (!c || !out) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    if (!c->geom_set) return fail(c, LYD_ERR_STATE, "geometry not set");
+    if (!(dt > 0.0)) return fail(c, LYD_ERR_ARG, "dt must be positive");
+    launch_mf(c->cellf[CF_DRU_R], c->cellf[CF_DRU_Z], c->cellf[CF_F_R], c->cellf[CF_F_Z], c->cellf[CF_JS], c->dV,
+              c->rCoM, c->ZCoM, c->nr, c->nz, dt, zc, c->partials, c->fblocks, c->st);
+    launch_column_sums(c->partials, 4, c->fblocks, c->small, c->st);
+    LYD_CU(c, cudaGetLastError());
+    double h[4];
+    LYD_CU(c, cudaMemcpyAsync(h, c->small, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+    LYD_TRY(check_err(c));
+    c->cell_set[CF_F_R] = c->cell_set[CF_F_Z] = true;
+    // normalisation, src/ConstantsAndFunctions.jl:652-673
+    double MF = h[0], net = h[1], outw = h[2], L = h[3];
+    if (L > 0.0) {
+        double k = 1.0 / (L / kC);
+        MF *= k; net *= k; outw *= k;
+    } else {
+        MF = net = outw = 0.0;
+    }
+    out[0] = MF; out[1] = net; out[2] = outw;
+    out[3] = (bc_z_bot == LYD_BC_REFLECT) ? 2.0 * L : L;
+    return LYD_OK;
+}
+
+int lyd_f_esc(lyd_ctx *c, double L_all, int32_t bc_z_bot, double *f) {
+    if (!c || !f) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    if (!c->geom_set || !c->freq_set) return fail(c, LYD_ERR_STATE, "geometry / frequency grid not set");
+    if (L_all <= 0.0) { *f = 0.0; return LYD_OK; }
+    launch_fesc(c->prec, Jc(c, 1), Jc(c, 2), c->A_r, c->A_Z, c->dnu, c->nnu, c->nr, c->nz, bc_z_bot, c->jscale,
+                c->small, c->st);
+    LYD_CU(c, cudaGetLastError());
+    double num;
+    LYD_CU(c, cudaMemcpyAsync(&num, c->small, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    LYD_TRY(check_err(c));
+    double Lsim = (bc_z_bot == LYD_BC_REFLECT) ? 0.5 * L_all : L_all;
+    *f = Lsim > 0.0 ? num / Lsim : 0.0;
+    return LYD_OK;
+}
+
+// ---- fused static-cloud step -----------------------------------------------------------------
+template <typename S>
+static int enqueue_step(lyd_ctx *c, const lyd_step_params *p, bool timed) {
+    const double ctdt = p->c_tilde * p->dt;
+    const int A = c->cur, B = 1 - c->cur;
+    AdvArgs<S> aa;
+    fill_adv<S>(c, aa, A, B, ctdt, p->bc_r_right, p->bc_z_bot, p->bc_z_top);
+    FreqArgs<S> fa;
+    fill_freq<S>(c, fa, c->set[B][0], c->set[B][1], c->set[B][2], c->set[B][0], c->set[A][0], c->set[A][1],
+                 c->set[A][2]);
+    fa.do_emission = 1; fa.do_freq = 1; fa.update_ff = 1;
+    fa.c_tilde = p->c_tilde; fa.dt = p->dt; fa.ctdt = ctdt; fa.z_center = p->z_center;
+    fa.bc_z_bot = p->bc_z_bot;
+    fa.parts = PART_ACTIVE | PART_DIAG;
+    fa.f_r = c->cellf[CF_F_R]; fa.f_Z = c->cellf[CF_F_Z];
+    RedArgs ra = red_args(c, PART_ACTIVE | PART_DIAG);
+    ra.dt = p->dt; ra.c_tilde = p->c_tilde; ra.bc_z_bot = p->bc_z_bot;
+    ra.diag = c->hist; ra.step_counter = c->step_ctr; ra.hist_capacity = c->hist_cap;
+    const int prec = sizeof(S) == 8 ? 0 : 1;
+    if (timed) cudaEventRecord(c->ev[0], c->st);
+    launch_advect(prec, c->cfg.flux_method, &aa, c->nnu, c->nr, c->nz, c->st);
+    if (timed) cudaEventRecord(c->ev[1], c->st);
+    launch_freq(prec, &fa, c->nnu, (int)c->ncell, c->fblocks, c->st);
+    if (timed) cudaEventRecord(c->ev[2], c->st);
+    launch_reduce(ra, c->st);
+    if (timed) cudaEventRecord(c->ev[3], c->st);
+    LYD_CU(c, cudaGetLastError());
+    return LYD_OK;
+}
+
+int lyd_set_timing(lyd_ctx *c, int32_t enable) {
+    if (!c) return LYD_ERR_ARG;
+    c->timing = enable != 0;
+    return LYD_OK;
+}
+
+int lyd_get_timing(lyd_ctx *c, double ms[3]) {
+    if (!c || !ms) return LYD_ERR_ARG;
+    for (int q = 0; q < 3; q++) ms[q] = c->ms[q];
+    return LYD_OK;
+}
+
+int lyd_static_steps(lyd_ctx *c, const lyd_step_params *p, lyd_diag *hist_out) {
+    if (!c || !p) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    LYD_TRY(check_bcs(c, LYD_BC_REFLECT, p->bc_r_right, p->bc_z_bot, p->bc_z_top));
+    LYD_TRY(need_inputs(c, true, true));
+    if (!(p->c_tilde > 0.0) || !(p->dt > 0.0) || p->n_steps < 0) return fail(c, LYD_ERR_ARG, "bad step parameters");
+    if (p->n_steps == 0) return LYD_OK;
+    if (p->n_steps > c->hist_cap) {
+        cudaFree(c->hist);
+        c->hist = nullptr;
+        int cap = p->n_steps < 1024 ? 1024 : p->n_steps;
+        LYD_TRY(dalloc(c, (void **)&c->hist, (size_t)cap * 7 * 8));
+        c->hist_cap = cap;
+        if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
+    }
+    LYD_CU(c, cudaMemsetAsync(c->step_ctr, 0, sizeof(int), c->st));
+    // the fused step keeps no Delta rho u between steps (Reset_Delta_rho_u! ends each step)
+    LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_R], 0, c->ncell * 8, c->st));
+    LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_Z], 0, c->ncell * 8, c->st));
+    if (!c->active_valid) LYD_TRY(run_find_active(c));
+    if (c->timing) {
+        double acc[3] = {0, 0, 0};
+        for (int n = 0; n < p->n_steps; n++) {
+            int r = c->prec == 0 ? enqueue_step<double>(c, p, true) : enqueue_step<float>(c, p, true);
+            if (r != LYD_OK) return r;
+            LYD_CU(c, cudaEventSynchronize(c->ev[3]));
+            for (int q = 0; q < 3; q++) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, c->ev[q], c->ev[q + 1]);
+                acc[q] += ms;
+            }
+        }
+        for (int q = 0; q < 3; q++) c->ms[q] = acc[q];
+    } else {
+        bool same = c->gexec && c->gkey[0] == p->c_tilde && c->gkey[1] == p->dt && c->gkey[2] == p->z_center &&
+                    c->gkey_i[0] == p->bc_r_right && c->gkey_i[1] == p->bc_z_bot && c->gkey_i[2] == p->bc_z_top &&
+                    c->gkey_i[3] == c->cur;
+        if (!same) {
+            if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
+            cudaGraph_t g;
+            LYD_CU(c, cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+            int r = c->prec == 0 ? enqueue_step<double>(c, p, false) : enqueue_step<float>(c, p, false);
+            cudaError_t e = cudaStreamEndCapture(c->st, &g);
+            if (r != LYD_OK) return r;
+            if (e != cudaSuccess) return fail(c, LYD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&c->gexec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return fail(c, LYD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            c->gkey[0] = p->c_tilde; c->gkey[1] = p->dt; c->gkey[2] = p->z_center;
+            c->gkey_i[0] = p->bc_r_right; c->gkey_i[1] = p->bc_z_bot; c->gkey_i[2] = p->bc_z_top;
+            c->gkey_i[3] = c->cur;
+        }
+        for (int n = 0; n < p->n_steps; n++) LYD_CU(c, cudaGraphLaunch(c->gexec, c->st));
+    }
+    c->old_alias = true;
+    c->active_valid = true;
+    if (hist_out) {
+        std::vector<double> h((size_t)p->n_steps * 7);
+        LYD_CU(c, cudaMemcpyAsync(h.data(), c->hist, h.size() * 8, cudaMemcpyDeviceToHost, c->st));
+        LYD_TRY(check_err(c));
+        for (int n = 0; n < p->n_steps; n++) {
+            const double *r = &h[(size_t)n * 7];
+            hist_out[n].M_F = r[0]; hist_out[n].M_F_radial_net = r[1]; hist_out[n].M_F_radial_out = r[2];
+            hist_out[n].L_tot = r[3]; hist_out[n].f_esc = r[4];
+            hist_out[n].kmin = (int32_t)r[5]; hist_out[n].kmax = (int32_t)r[6];
+        }
+        return LYD_OK;
+    }
+    // without a history buffer the call only enqueues; errors surface at the next
+    // synchronising call (lyd_synchronize, a download or a diagnostic)
+    LYD_CU(c, cudaGetLastError());
+    return LYD_OK;
+}
+
+// ---- set-up helpers ------------------------------------------------------------------------------
+int lyd_update_hvoigt(lyd_ctx *c) {
+    if (!c) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    if (!c->freq_set) return fail(c, LYD_ERR_STATE, "frequency grid not set");
+    if (!c->cell_set[CF_T]) return fail(c, LYD_ERR_STATE, "temperature T not uploaded");
+    if (!c->lut) {
+        std::vector<double> h((size_t)5 * kLutN);
+        build_voigt_lut(h.data(), kLutN, kLutXmax);
+        LYD_TRY(dalloc(c, (void **)&c->lut, h.size() * 8));
+        LYD_CU(c, cudaMemcpyAsync(c->lut, h.data(), h.size() * 8, cudaMemcpyHostToDevice, c->st));
+        LYD_CU(c, cudaStreamSynchronize(c->st));
+    }
+    launch_hvoigt(c->prec, c->Hv, c->cellf[CF_T], c->nu, c->nuC, c->nnu, (int)c->ncell, c->lut, kLutN, kLutXmax, c->st);
+    LYD_CU(c, cudaGetLastError());
+    c->hv_set = true;
+    if (!c->phi_explicit) c->phi_ready = false;
+    return check_err(c);
+}
+
+int lyd_update_phi_nu(lyd_ctx *c, int32_t kmin, int32_t kmax) {
+    if (!c) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    if (kmin < 0 || kmax >= c->nnu || kmin > kmax) return fail(c, LYD_ERR_ARG, "bad bin range");
+    if (!c->hv_set || !c->freq_set) return fail(c, LYD_ERR_STATE, "H_voigt / frequency grid not set");
+    launch_phi_inv(c->prec, c->Hv, c->dnu, c->nnu, (int)c->ncell, kmin, kmax, c->phi_inv, c->st);
+    LYD_CU(c, cudaGetLastError());
+    c->phi_kmin = kmin;
+    c->phi_kmax = kmax;
+    c->phi_explicit = false;
+    c->phi_ready = true;
+    return check_err(c);
+}
+
+int lyd_pd_lya(lyd_ctx *c, size_t n, const double *nHII, const double *ne, const double *nHI, const double *nHeI,
+               const double *nH2, const double *T, double z, double *out) {
+    if (!c || !out || !nHII || !ne || !nHI || !nHeI || !nH2 || !T) return LYD_ERR_ARG;
+    if (n == 0) return LYD_OK;
+    cudaSetDevice(c->dev);
+    double *d = nullptr;
+    LYD_TRY(dalloc(c, (void **)&d, n * 7 * 8));
+    const double *src[6] = {nHII, ne, nHI, nHeI, nH2, T};
+    int r = LYD_OK;
+    for (int q = 0; q < 6 && r == LYD_OK; q++) r = h2d(c, d + q * n, src[q], n);
+    if (r == LYD_OK) {
+        launch_pd(n, d, d + n, d + 2 * n, d + 3 * n, d + 4 * n, d + 5 * n, z, d + 6 * n, c->st);
+        cudaError_t e = cudaMemcpyAsync(out, d + 6 * n, n * 8, cudaMemcpyDeviceToHost, c->st);
+        if (e != cudaSuccess) r = fail(c, LYD_ERR_CUDA, cudaGetErrorString(e));
+        e = cudaStreamSynchronize(c->st);
+        if (e != cudaSuccess && r == LYD_OK) r = fail(c, LYD_ERR_CUDA, cudaGetErrorString(e));
+    }
+    cudaFree(d);
+    return r;
+}
+
+int lyd_cfl_dt(lyd_ctx *c, double ct, const double *u_r, const double *u_Z, double cfl, double *dt_out) {
+    if (!c || !u_r || !u_Z || !dt_out) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    if (!c->geom_set) return fail(c, LYD_ERR_STATE, "geometry not set");
+    double *d = nullptr;
+    LYD_TRY(dalloc(c, (void **)&d, c->ncell * 2 * 8));
+    int r = h2d(c, d, u_r, c->ncell);
+    if (r == LYD_OK) r = h2d(c, d + c->ncell, u_Z, c->ncell);
+    double m = 0.0;
+    if (r == LYD_OK) {
+        launch_cfl(c->r_if, c->Z_if, d, d + c->ncell, c->nr, c->nz, ct, c->small, c->st);
+        cudaError_t e = cudaMemcpyAsync(&m, c->small, 8, cudaMemcpyDeviceToHost, c->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+        if (e != cudaSuccess) r = fail(c, LYD_ERR_CUDA, cudaGetErrorString(e));
+    }
+    cudaFree(d);
+    if (r == LYD_OK) *dt_out = cfl * m;
+    return r;
+}
+
+int lyd_edge_spectra(lyd_ctx *c, double *raw, double *norm, int32_t *ridx, int32_t *zidx) {
+    if (!c || !raw || !norm) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    if (!c->freq_set) return fail(c, LYD_ERR_STATE, "frequency grid not set");
+    int ne = lyd_edge_count(c->nr, c->nz);
+    if (ne <= 0) return fail(c, LYD_ERR_ARG, "grid too small for the edge ring");
+    size_t n = (size_t)ne * c->nnu;
+    double *d = nullptr;
+    LYD_TRY(dalloc(c, (void **)&d, 2 * n * 8));
+    launch_edge(c->prec, Jc(c, 0), c->dnu, c->nnu, c->nr, c->nz, c->jscale, d, d + n, c->st);
+    int r = LYD_OK;
+    cudaError_t e = cudaMemcpyAsync(raw, d, n * 8, cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(norm, d + n, n * 8, cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) r = fail(c, LYD_ERR_CUDA, cudaGetErrorString(e));
+    cudaFree(d);
+    if (r != LYD_OK) return r;
+    int q = 0;
+    for (int j = 1; j <= c->nz - 2; j++, q++) { if (ridx) ridx[q] = c->nr - 2; if (zidx) zidx[q] = j; }
+    for (int i = 1; i <= c->nr - 3; i++, q++) { if (ridx) ridx[q] = i; if (zidx) zidx[q] = c->nz - 2; }
+    for (int i = 1; i <= c->nr - 3; i++, q++) { if (ridx) ridx[q] = i; if (zidx) zidx[q] = 1; }
+    return check_err(c);
+}
+
+int lyd_voigt_tables(double *out, int32_t n, double xmax) {
+    if (!out || n < 2 || !(xmax > 0.0)) return LYD_ERR_ARG;
+    build_voigt_lut(out, n, xmax);
+    return LYD_OK;
+}
+

@@ -1,0 +1,819 @@
+// lyd_kernels.cu -- the hot kernels of the Lyman-alpha M1 step on sm_100a.
+//
+//  k_advect   AdvectJandH_Cylindrical! (src/AdvectJandH.jl:526-1390) as ONE kernel: a CTA
+//             owns an 8x4 (r x Z) tile of cells and a 32-bin slice of frequencies (one bin
+//             per lane, k innermost so every warp load is a contiguous 256 B / 128 B run).
+//             Face fluxes of the tile are computed once into shared memory, then each cell
+//             is updated from them: the six face-flux arrays and the two K_phiphi arrays
+//             of the reference never touch HBM. Ghost cells of the four boundaries are
+//             produced on the fly from the boundary conditions.
+//  k_freq     LyaEmissionAbsorptionUpdate! + UpdateFreqFactors! + the per-cell tridiagonal
+//             solve + the flux correction of FrequencyUpdateJLya_AllCells! fused per cell:
+//             one warp owns one cell's whole spectrum (M contiguous bins per lane), the
+//             k +- 1 couplings travel by warp shuffles, and the tridiagonal system is solved
+//             in FP64 by parallel cyclic reduction across the warp. The epilogue
+//             accumulates the next step's FindActiveBins energies and the step diagnostics
+//             into per-CTA partials (fixed order, so results are run-to-run deterministic).
+//  k_reduce   sums the partials (one warp per column) and derives kmin/kmax, M_F, L, f_esc.
+#include <cuda_runtime.h>
+
+#include "lyd_internal.h"
+#include "lyd_physics.cuh"
+
+namespace lyd {
+
+constexpr int TI = 8;          // tile width in r
+constexpr int TJ = 4;          // tile height in Z
+constexpr int ADV_THREADS = 256;
+constexpr int FREQ_THREADS = 256;
+
+template <typename S, typename R>
+__device__ __forceinline__ Cell<R> ld_cell(const AdvArgs<S> &a, int i, int j, int k) {
+    size_t x = (size_t)k + (size_t)a.nnu * ((size_t)i + (size_t)a.nr * (size_t)j);
+    Cell<R> c;
+    c.J = R(__ldg(a.J + x));
+    c.Hr = R(__ldg(a.Hr + x));
+    c.HZ = R(__ldg(a.HZ + x));
+    return c;
+}
+
+// Radial stencil cell with the ghost cells of src/AdvectJandH.jl:662-673 (axis, always
+// reflecting) and 853-871 (outer boundary, reflecting or outflow).
+template <typename S, typename R>
+__device__ __forceinline__ Cell<R> r_cell(const AdvArgs<S> &a, int idx, int j, int k) {
+    if (idx < 0) {
+        Cell<R> c = ld_cell<S, R>(a, -1 - idx, j, k);
+        c.Hr = -c.Hr;
+        return c;
+    }
+    if (idx >= a.nr) {
+        if (a.bc_r_right == 0) {
+            Cell<R> c = ld_cell<S, R>(a, 2 * a.nr - 1 - idx, j, k);
+            c.Hr = -c.Hr;
+            return c;
+        }
+        Cell<R> c = ld_cell<S, R>(a, a.nr - 1, j, k);
+        c.Hr = c.Hr > R(0) ? c.Hr : R(0);
+        return c;
+    }
+    return ld_cell<S, R>(a, idx, j, k);
+}
+
+// Vertical stencil cell with the ghost cells of src/AdvectJandH.jl:1000-1018 (bottom) and
+// 1185-1203 (top).
+template <typename S, typename R>
+__device__ __forceinline__ Cell<R> z_cell(const AdvArgs<S> &a, int i, int idx, int k) {
+    if (idx < 0) {
+        if (a.bc_z_bot == 0) {
+            Cell<R> c = ld_cell<S, R>(a, i, -1 - idx, k);
+            c.HZ = -c.HZ;
+            return c;
+        }
+        Cell<R> c = ld_cell<S, R>(a, i, 0, k);
+        c.HZ = c.HZ < R(0) ? c.HZ : R(0);
+        return c;
+    }
+    if (idx >= a.nz) {
+        if (a.bc_z_top == 0) {
+            Cell<R> c = ld_cell<S, R>(a, i, 2 * a.nz - 1 - idx, k);
+            c.HZ = -c.HZ;
+            return c;
+        }
+        Cell<R> c = ld_cell<S, R>(a, i, a.nz - 1, k);
+        c.HZ = c.HZ > R(0) ? c.HZ : R(0);
+        return c;
+    }
+    return ld_cell<S, R>(a, i, idx, k);
+}
+
+// alpha_F of an in-grid cell: explicit array, or alpha*H_voigt (+ alpha_cF) as set up by
+// src/StaticCloudTest.jl:283-285 and PhotoThermoChemistry.jl:2151.
+template <typename S, typename R>
+__device__ __forceinline__ R alpha_F(const AdvArgs<S> &a, int i, int j, int k) {
+    size_t c = (size_t)i + (size_t)a.nr * (size_t)j;
+    size_t x = (size_t)k + (size_t)a.nnu * c;
+    if (a.aF) return R(__ldg(a.aF + x));
+    R v = R(__ldg(a.alpha + c)) * R(__ldg(a.Hv + x));
+    if (a.alpha_cF) v = v + R(__ldg(a.alpha_cF + c));
+    return v;
+}
+
+// One r interface f (between cells f-1 and f) in row j: the three fluxes plus the
+// K_phiphi of both sides (src/AdvectJandH.jl:641-968).
+template <typename S, typename R, int FLUX>
+__device__ __forceinline__ void face_r(const AdvArgs<S> &a, int f, int j, int k, R jeps, R *F, R &kL, R &kR) {
+    Cell<R> cm1 = r_cell<S, R>(a, f - 2, j, k);
+    Cell<R> ci = r_cell<S, R>(a, f - 1, j, k);
+    Cell<R> cp1 = r_cell<S, R>(a, f, j, k);
+    Cell<R> cp2 = r_cell<S, R>(a, f + 1, j, k);
+    R iv[5];
+#pragma unroll
+    for (int t = 0; t < 5; t++) iv[t] = R(__ldg(a.rint + 5 * f + t));
+    R aFi = alpha_F<S, R>(a, f - 1 > 0 ? f - 1 : 0, j, k);
+    R aFp = alpha_F<S, R>(a, f < a.nr - 1 ? f : a.nr - 1, j, k);
+    Recon<R> q = reconstruct<R>(cm1, ci, cp1, cp2, iv, aFi, aFp, jeps);
+    R DrrL, DZZL, DrZL, DrrR, DZZR, DrZR;
+    D_from_f_n<R>(q.f_L, q.nr_L, q.nZ_L, DrrL, DZZL, DrZL);
+    D_from_f_n<R>(q.f_R, q.nr_R, q.nZ_R, DrrR, DZZR, DrZR);
+    R FJ, FHr, FHZ;
+    m1_flux<R, FLUX, false>(q.Hr_L, q.Hr_R, DrrL * q.J_L, DrrR * q.J_R, DrZL * q.J_L, DrZR * q.J_R, q, ci.J, cp1.J,
+                            FJ, FHr, FHZ);
+    R uc = R(__ldg(a.u_r_star + f + (size_t)(a.nr + 1) * j) * kInvC);
+    F[0] = FJ + adv_flux(uc, q.J_L, q.J_R);
+    F[1] = FHr + adv_flux(uc, q.Hr_L, q.Hr_R);
+    F[2] = FHZ + adv_flux(uc, q.HZ_L, q.HZ_R);
+    kL = clamp01(R(1) - DrrL - DZZL) * q.J_L;
+    kR = (f == 0) ? k_phiphi_axis<R>(q.J_R, q.HZ_R, jeps) : clamp01(R(1) - DrrR - DZZR) * q.J_R;
+}
+
+// One Z interface f (between cells f-1 and f) in column i (src/AdvectJandH.jl:978-1289).
+template <typename S, typename R, int FLUX>
+__device__ __forceinline__ void face_z(const AdvArgs<S> &a, int i, int f, int k, R jeps, R *F) {
+    Cell<R> cm1 = z_cell<S, R>(a, i, f - 2, k);
+    Cell<R> ci = z_cell<S, R>(a, i, f - 1, k);
+    Cell<R> cp1 = z_cell<S, R>(a, i, f, k);
+    Cell<R> cp2 = z_cell<S, R>(a, i, f + 1, k);
+    R iv[5];
+#pragma unroll
+    for (int t = 0; t < 5; t++) iv[t] = R(__ldg(a.zint + 5 * f + t));
+    R aFi = alpha_F<S, R>(a, i, f - 1 > 0 ? f - 1 : 0, k);
+    R aFp = alpha_F<S, R>(a, i, f < a.nz - 1 ? f : a.nz - 1, k);
+    Recon<R> q = reconstruct<R>(cm1, ci, cp1, cp2, iv, aFi, aFp, jeps);
+    R DrrL, DZZL, DrZL, DrrR, DZZR, DrZR;
+    D_from_f_n<R>(q.f_L, q.nr_L, q.nZ_L, DrrL, DZZL, DrZL);
+    D_from_f_n<R>(q.f_R, q.nr_R, q.nZ_R, DrrR, DZZR, DrZR);
+    R FJ, FHr, FHZ;
+    m1_flux<R, FLUX, true>(q.HZ_L, q.HZ_R, DrZL * q.J_L, DrZR * q.J_R, DZZL * q.J_L, DZZR * q.J_R, q, ci.J, cp1.J,
+                           FJ, FHr, FHZ);
+    R uc = R(__ldg(a.u_Z_star + i + (size_t)a.nr * f) * kInvC);
+    F[0] = FJ + adv_flux(uc, q.J_L, q.J_R);
+    F[1] = FHr + adv_flux(uc, q.Hr_L, q.Hr_R);
+    F[2] = FHZ + adv_flux(uc, q.HZ_L, q.HZ_R);
+}
+
+template <typename S, typename R, int FLUX>
+__global__ void __launch_bounds__(ADV_THREADS, 2) k_advect(AdvArgs<S> a) {
+    extern __shared__ __align__(16) unsigned char adv_smem[];
+    R *sFr = reinterpret_cast<R *>(adv_smem);        // [TJ][TI+1][3][32]
+    R *sKr = sFr + TJ * (TI + 1) * 3 * 32;            // [TJ][TI+1][2][32]
+    R *sFz = sKr + TJ * (TI + 1) * 2 * 32;            // [TJ+1][TI][3][32]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = ADV_THREADS / 32;
+    const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ, kb = blockIdx.z * 32;
+    const int k = kb + lane;
+    const int kmin = a.kwin[0], kmax = a.kwin[1];
+    const bool kact = (k >= kmin) && (k <= kmax) && (k < a.nnu);
+    const bool chunk_act = (kb <= kmax) && (kb + 31 >= kmin);
+    const R jeps = R(a.jeps);
+
+    if (chunk_act) {
+        const int nRF = (TI + 1) * TJ, nZF = TI * (TJ + 1);
+        for (int t = warp; t < nRF + nZF; t += nwarps) {
+            if (t < nRF) {
+                int fl = t % (TI + 1), jl = t / (TI + 1);
+                int f = i0 + fl, j = j0 + jl;
+                if (kact && f <= a.nr && j < a.nz) {
+                    R F[3], kL, kR;
+                    face_r<S, R, FLUX>(a, f, j, k, jeps, F, kL, kR);
+                    R *p = sFr + ((jl * (TI + 1) + fl) * 3) * 32 + lane;
+                    p[0] = F[0]; p[32] = F[1]; p[64] = F[2];
+                    R *q = sKr + ((jl * (TI + 1) + fl) * 2) * 32 + lane;
+                    q[0] = kL; q[32] = kR;
+                }
+            } else {
+                int u = t - nRF;
+                int il = u % TI, fl = u / TI;
+                int i = i0 + il, f = j0 + fl;
+                if (kact && i < a.nr && f <= a.nz) {
+                    R F[3];
+                    face_z<S, R, FLUX>(a, i, f, k, jeps, F);
+                    R *p = sFz + ((fl * TI + il) * 3) * 32 + lane;
+                    p[0] = F[0]; p[32] = F[1]; p[64] = F[2];
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    const double ctdt = a.ctdt;
+    const double ctdt_c = ctdt * kInvC;
+    for (int t = warp; t < TI * TJ; t += nwarps) {
+        int il = t % TI, jl = t / TI;
+        int i = i0 + il, j = j0 + jl;
+        if (i >= a.nr || j >= a.nz || k >= a.nnu) continue;
+        size_t c = (size_t)i + (size_t)a.nr * (size_t)j;
+        size_t x = (size_t)k + (size_t)a.nnu * c;
+        if (!kact) {
+            a.Jo[x] = a.J[x];
+            a.Hro[x] = a.Hr[x];
+            a.HZo[x] = a.HZ[x];
+            continue;
+        }
+        Cell<R> s = ld_cell<S, R>(a, i, j, k);
+        R Drr, DZZ, DrZ;
+        D_edd<R>(s.Hr, s.HZ, s.J, jeps, R(a.heps2), Drr, DZZ, DrZ);
+        const R *FrL = sFr + ((jl * (TI + 1) + il) * 3) * 32 + lane;
+        const R *FrR = FrL + 3 * 32;
+        const R *FzL = sFz + ((jl * TI + il) * 3) * 32 + lane;
+        const R *FzR = FzL + TI * 3 * 32;
+        const R *KL = sKr + ((jl * (TI + 1) + il) * 2) * 32 + lane;
+        R kimh = KL[32];          // right side of face i   (K_phiphi at i-1/2)
+        R kiph = KL[2 * 32];      // left side of face i+1  (K_phiphi at i+1/2)
+        double ArL = __ldg(a.A_r + i + (size_t)(a.nr + 1) * j), ArR = __ldg(a.A_r + i + 1 + (size_t)(a.nr + 1) * j);
+        double AZL = __ldg(a.A_Z + c), AZR = __ldg(a.A_Z + c + a.nr);
+        double fac = ctdt * __ldg(a.inv_dV + c);
+        R Jn, Hrn, HZn;
+        if (sizeof(R) == 8) {
+            // UpdateConservativeQuantity in the reference's operation order
+            R f = R(fac);
+            Jn = s.J - f * ((R(ArR) * FrR[0] - R(ArL) * FrL[0]) + (R(AZR) * FzR[0] - R(AZL) * FzL[0]));
+            HZn = s.HZ - f * ((R(ArR) * FrR[64] - R(ArL) * FrL[64]) + (R(AZR) * FzR[64] - R(AZL) * FzL[64]));
+            Hrn = s.Hr - f * ((R(ArR) * FrR[32] - R(ArL) * FrL[32]) + (R(AZR) * FzR[32] - R(AZL) * FzL[32]));
+        } else {
+            // FP32: fold c~dt/dV into the areas in FP64 first (dimensionless weights)
+            R wrL = R(fac * ArL), wrR = R(fac * ArR), wzL = R(fac * AZL), wzR = R(fac * AZR);
+            Jn = s.J - ((wrR * FrR[0] - wrL * FrL[0]) + (wzR * FzR[0] - wzL * FzL[0]));
+            HZn = s.HZ - ((wrR * FrR[64] - wrL * FrL[64]) + (wzR * FzR[64] - wzL * FzL[64]));
+            Hrn = s.Hr - ((wrR * FrR[32] - wrL * FrL[32]) + (wzR * FzR[32] - wzL * FzL[32]));
+        }
+        Jn = Jn > jeps ? Jn : jeps;
+        R ga = R(__ldg(a.dur_dr + c)), gb = R(__ldg(a.dur_dZ + c)), gc = R(__ldg(a.duZ_dr + c));
+        R gd = R(__ldg(a.duZ_dZ + c)), ge = R(__ldg(a.ur_over_r + c));
+        R DdU = d_colon_grad_u<R>(Drr, DrZ, DZZ, ga, gb, gc, gd, ge);
+        R Kav = R(0.5) * (kimh + kiph);
+        if (sizeof(R) == 8)
+            Hrn += R(ctdt) * Kav * R(__ldg(a.inv_r_cell + i));
+        else
+            Hrn += R(ctdt * __ldg(a.inv_r_cell + i)) * Kav;
+        R cc = R(ctdt_c);
+        R dHr = -cc * (s.Hr * ga + s.HZ * gb);
+        R dHZ = -cc * (s.Hr * gc + s.HZ * gd);
+        Hrn = Hrn + dHr;
+        HZn = HZn + dHZ;
+        Jn = Jn - cc * DdU * s.J;
+        Jn = Jn > jeps ? Jn : jeps;
+        R H2 = Hrn * Hrn + HZn * HZn;
+        if (H2 > Jn * Jn) {
+            R fsc = Jn / rsq(H2);
+            Hrn *= fsc;
+            HZn *= fsc;
+        }
+        a.Jo[x] = S(Jn);
+        a.Hro[x] = S(Hrn);
+        a.HZo[x] = S(HZn);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Frequency kernel helpers
+// ------------------------------------------------------------------------------------------
+template <int M>
+struct Row {
+    double a[M], b[M], c[M], d[M];
+};
+
+// Fetch, for every owned row r = lane*M + m, the quantity v of row r - s (dir = -1) or r + s
+// (dir = +1). Rows outside [0, 32M) read the identity-row value `idv`.
+template <int M>
+__device__ __forceinline__ void nbr(const double (&v)[M], double (&out)[M], int s, int dir, int lane, double idv) {
+    if (s < M) {
+#pragma unroll
+        for (int m = 0; m < M; m++) {
+            int mm = m + dir * s;
+            if (mm >= 0 && mm < M) {
+                out[m] = v[mm];
+            } else {
+                int src = mm < 0 ? mm + M : mm - M;
+                // src is a compile-time index after unrolling of m and s
+                double w = 0.0;
+#pragma unroll
+                for (int q = 0; q < M; q++)
+                    if (q == src) w = v[q];
+                double got = dir < 0 ? __shfl_up_sync(0xffffffffu, w, 1) : __shfl_down_sync(0xffffffffu, w, 1);
+                bool oob = dir < 0 ? (lane == 0) : (lane == 31);
+                out[m] = oob ? idv : got;
+            }
+        }
+    } else {
+        int t = s / M;
+#pragma unroll
+        for (int m = 0; m < M; m++) {
+            double got = dir < 0 ? __shfl_up_sync(0xffffffffu, v[m], t) : __shfl_down_sync(0xffffffffu, v[m], t);
+            bool oob = dir < 0 ? (lane < t) : (lane + t > 31);
+            out[m] = oob ? idv : got;
+        }
+    }
+}
+
+// Parallel cyclic reduction of the 32*M-row tridiagonal system held by the warp
+// (row r = lane*M + m; a = sub-, b = main-, c = super-diagonal, d = right-hand side).
+// Decoupled rows are identity rows. Returns x in d.
+template <int M>
+__device__ __forceinline__ void pcr_solve(Row<M> &R_, int lane) {
+#pragma unroll
+    for (int s = 1; s < 32 * M; s <<= 1) {
+        double ib[M];
+#pragma unroll
+        for (int m = 0; m < M; m++) ib[m] = 1.0 / R_.b[m];
+        double am[M], cm[M], dm[M], ibm[M], ap[M], cp[M], dp[M], ibp[M];
+        nbr<M>(R_.a, am, s, -1, lane, 0.0);
+        nbr<M>(R_.c, cm, s, -1, lane, 0.0);
+        nbr<M>(R_.d, dm, s, -1, lane, 0.0);
+        nbr<M>(ib, ibm, s, -1, lane, 1.0);
+        nbr<M>(R_.a, ap, s, +1, lane, 0.0);
+        nbr<M>(R_.c, cp, s, +1, lane, 0.0);
+        nbr<M>(R_.d, dp, s, +1, lane, 0.0);
+        nbr<M>(ib, ibp, s, +1, lane, 1.0);
+#pragma unroll
+        for (int m = 0; m < M; m++) {
+            double al = -R_.a[m] * ibm[m];
+            double ga = -R_.c[m] * ibp[m];
+            double nb = R_.b[m] + al * cm[m] + ga * ap[m];
+            double nd = R_.d[m] + al * dm[m] + ga * dp[m];
+            R_.a[m] = al * am[m];
+            R_.c[m] = ga * cp[m];
+            R_.b[m] = nb;
+            R_.d[m] = nd;
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < M; m++) R_.d[m] = R_.d[m] / R_.b[m];
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Per-k constants of UpdateFreqFactors! staged in shared memory once per CTA.
+enum { KC_NCK, KC_NCKP, KC_NCKM, KC_DNKP, KC_DNK, KC_DNKM, KC_IDNU, KC_ICK, KC_ICKP, KC_ICKM, KC_DNU, KC_N };
+
+template <typename S, typename R, int M>
+__global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
+    extern __shared__ __align__(16) double fsm[];
+    constexpr int NP = 32 * M;
+    double *kc = fsm;                              // [KC_N][NP]
+    double *red = fsm + KC_N * NP;                 // [nwarps][NP + 8]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    const int nnu = a.nnu;
+    for (int t = threadIdx.x; t < NP; t += blockDim.x) {
+        bool in = (t >= 1 && t <= nnu - 2);
+        kc[KC_NCK * NP + t] = in ? a.nuC[t] : 0.0;
+        kc[KC_NCKP * NP + t] = in ? a.nuC[t + 1] : 0.0;
+        kc[KC_NCKM * NP + t] = in ? a.nuC[t - 1] : 0.0;
+        kc[KC_DNKP * NP + t] = in ? a.nuC[t + 1] - a.nu[t + 1] : 0.0;
+        kc[KC_DNK * NP + t] = in ? a.nu[t + 1] - a.nuC[t] : 0.0;
+        kc[KC_DNKM * NP + t] = in ? a.nu[t] - a.nuC[t - 1] : 0.0;
+        kc[KC_IDNU * NP + t] = in ? a.inv_dnu[t] : 0.0;
+        kc[KC_ICK * NP + t] = in ? a.inv_nuC[t] : 0.0;
+        kc[KC_ICKP * NP + t] = in ? a.inv_nuC[t + 1] : 0.0;
+        kc[KC_ICKM * NP + t] = in ? a.inv_nuC[t - 1] : 0.0;
+        kc[KC_DNU * NP + t] = (t < nnu) ? a.dnu[t] : 0.0;
+    }
+    __syncthreads();
+
+    const int ncell = a.nr * a.nz;
+    const double jeps = a.jeps;
+    const double dw = 1.0 / a.ctdt;
+    double acc_e[M];
+#pragma unroll
+    for (int m = 0; m < M; m++) acc_e[m] = 0.0;
+    double acc_tot = 0.0, acc_mf = 0.0, acc_net = 0.0, acc_out = 0.0, acc_L = 0.0, acc_esc = 0.0;
+    int bad = 0;
+
+    for (int c = blockIdx.x * nw + warp; c < ncell; c += gridDim.x * nw) {
+        const int i = c % a.nr, j = c / a.nr;
+        const size_t base = (size_t)c * nnu;
+        R J[M], Hr[M], HZ[M], Hv[M];
+        double Jo[M];
+#pragma unroll
+        for (int m = 0; m < M; m++) {
+            int k = lane * M + m;
+            bool v = k < nnu;
+            J[m] = v ? R(a.Jin[base + k]) : R(0);
+            Hr[m] = v ? R(a.Hrin[base + k]) : R(0);
+            HZ[m] = v ? R(a.HZin[base + k]) : R(0);
+            Hv[m] = v ? R(__ldg(a.Hv + base + k)) : R(0);
+            Jo[m] = v ? double(a.Jold[base + k]) : 0.0;
+        }
+        double dr_sum = 0.0, dz_sum = 0.0;
+        // ---- LyaEmissionAbsorptionUpdate! (src/ConstantsAndFunctions.jl:526-567) ----
+        if (a.do_emission) {
+            const R al = R(__ldg(a.alpha + c)), acv = R(__ldg(a.alpha_c + c));
+            const R al_pd = al * R(__ldg(a.pd + c));
+            const R js_ct = R(__ldg(a.js + c) * a.c_tilde / a.j_scale);
+            const R ct = R(a.c_tilde), dtr = R(a.dt);
+            const R pinv = a.phi ? R(0) : R(__ldg(a.phi_inv + c));
+            const R acF = a.alpha_cF ? R(__ldg(a.alpha_cF + c)) : R(0);
+#pragma unroll
+            for (int m = 0; m < M; m++) {
+                int k = lane * M + m;
+                if (k >= nnu) continue;
+                R phi = a.phi ? R(__ldg(a.phi + base + k))
+                              : ((k >= a.phi_kmin && k <= a.phi_kmax) ? Hv[m] * pinv : R(0));
+                R aabs = acv + al_pd * Hv[m];
+                R dJdt = js_ct * phi;
+                R Jn = (R(Jo[m]) + dJdt * dtr) / (R(1) + aabs * ct * dtr);
+                R aH = a.aF ? R(__ldg(a.aF + base + k)) : (a.alpha_cF ? al * Hv[m] + acF : al * Hv[m]);
+                R den = R(1) + aH * ct * dtr;
+                R hr = (Hr[m] + R(0) * dtr) / den;
+                R hz = (HZ[m] + R(0) * dtr) / den;
+                double dn = kc[KC_DNU * NP + k];
+                dr_sum += dn * (double(Hr[m]) - double(hr));
+                dz_sum += dn * (double(HZ[m]) - double(hz));
+                Hr[m] = hr;
+                HZ[m] = hz;
+                J[m] = Jn;
+                Jo[m] = double(Jn);
+            }
+            dr_sum = warp_sum(dr_sum);
+            dz_sum = warp_sum(dz_sum);
+            if (lane == 0 && a.dru_r) {
+                const double k4 = kFourPiOverC * (1.0 / a.c_tilde) * a.j_scale;
+                a.dru_r[c] += k4 * dr_sum;
+                a.dru_Z[c] += k4 * dz_sum;
+            }
+        }
+        // ---- FrequencyUpdateJLya_AllCells! (src/UpdateLyaJandH.jl:231-391) ----
+        if (a.do_freq) {
+            Row<M> sys;
+            double Fp[M], F0[M], Fm[M];
+            if (a.update_ff) {
+                // UpdateFreqFactors!, src/FreqFactors.jl:181-275
+                const double T = __ldg(a.T + c);
+                const double dnuD = compute_dnuD(T);
+                const double alv = __ldg(a.alpha + c);
+                const double pref = 0.5 * (alv > a.alpha_floor ? alv : a.alpha_floor) * (dnuD * dnuD);
+                const double rec0 = kHOverKB / T;
+                const R ga = R(__ldg(a.dur_dr + c)), gb = R(__ldg(a.dur_dZ + c)), gc = R(__ldg(a.duZ_dr + c));
+                const R gd = R(__ldg(a.duZ_dZ + c)), ge = R(__ldg(a.ur_over_r + c));
+                // neighbours H_voigt[k-1], H_voigt[k+1]
+                double hv_up = __shfl_up_sync(0xffffffffu, double(Hv[M - 1]), 1);
+                double hv_dn = __shfl_down_sync(0xffffffffu, double(Hv[0]), 1);
+#pragma unroll
+                for (int m = 0; m < M; m++) {
+                    int k = lane * M + m;
+                    Fp[m] = 0.0; F0[m] = 0.0; Fm[m] = 0.0;
+                    if (k < 1 || k > nnu - 2) continue;
+                    double hkm = (m > 0) ? double(Hv[m - 1]) : hv_up;
+                    double hkp = (m < M - 1) ? double(Hv[m + 1]) : hv_dn;
+                    R Drr, DZZ, DrZ;
+                    D_edd<R>(Hr[m], HZ[m], J[m], R(jeps), R(a.heps2), Drr, DZZ, DrZ);
+                    double vel = double(d_colon_grad_u<R>(Drr, DrZ, DZZ, ga, gb, gc, gd, ge)) * kInvC;
+                    double Kkp = pref * hkp, Kk = pref * double(Hv[m]), Kkm = pref * hkm;
+                    double nCk = kc[KC_NCK * NP + k], nCkp = kc[KC_NCKP * NP + k], nCkm = kc[KC_NCKM * NP + k];
+                    double Ckp = vel * nCkp, Ck = vel * nCk, Ckm = vel * nCkm;
+                    if (a.recoil) {
+                        Ckp += Kkp * (rec0 - 2.0 * kc[KC_ICKP * NP + k]);
+                        Ck += Kk * (rec0 - 2.0 * kc[KC_ICK * NP + k]);
+                        Ckm += Kkm * (rec0 - 2.0 * kc[KC_ICKM * NP + k]);
+                    }
+                    double rkp = kc[KC_DNKP * NP + k] * (1.0 / Kkp);
+                    double rk = kc[KC_DNK * NP + k] * (1.0 / Kk);
+                    double rkm = kc[KC_DNKM * NP + k] * (1.0 / Kkm);
+                    double Pkp = fmin(fmax(Ckp * rkp, -kPmax), kPmax);
+                    double Pk = fmin(fmax(Ck * rk, -kPmax), kPmax);
+                    double Pkm = fmin(fmax(Ckm * rkm, -kPmax), kPmax);
+                    double oRkp, xRkp, oLk, xLk, oRk, xRk, oLkm, xLkm;
+                    omphi_R(Pkp, oRkp, xRkp);
+                    omphi_L(Pk, oLk, xLk);
+                    omphi_R(Pk, oRk, xRk);
+                    omphi_L(Pkm, oLkm, xLkm);
+                    double idn = kc[KC_IDNU * NP + k];
+                    double dkp = idn * (1.0 / (xLk * rk - xRkp * rkp));
+                    double dkm = idn * (1.0 / (xLkm * rkm - xRk * rk));
+                    Fp[m] = oRkp * dkp;
+                    Fm[m] = oLkm * dkm;
+                    F0[m] = oLk * dkp + oRk * dkm;
+                }
+                if (a.Fkp) {
+#pragma unroll
+                    for (int m = 0; m < M; m++) {
+                        int k = lane * M + m;
+                        if (k < nnu) { a.Fkp[base + k] = Fp[m]; a.Fk[base + k] = F0[m]; a.Fkm[base + k] = Fm[m]; }
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int m = 0; m < M; m++) {
+                    int k = lane * M + m;
+                    bool in = (k >= 1 && k <= nnu - 2);
+                    Fp[m] = in ? a.Fkp[base + k] : 0.0;
+                    F0[m] = in ? a.Fk[base + k] : 0.0;
+                    Fm[m] = in ? a.Fkm[base + k] : 0.0;
+                }
+            }
+            // rows k = 1 .. nnu-2 of src/UpdateLyaJandH.jl:200-214; the couplings of the
+            // first and last rows to k = 0 and k = nnu-1 are dropped (TridiagonalSolver.jl:45-46)
+#pragma unroll
+            for (int m = 0; m < M; m++) {
+                int k = lane * M + m;
+                bool in = (k >= 1 && k <= nnu - 2);
+                sys.a[m] = (in && k >= 2) ? Fm[m] : 0.0;
+                sys.b[m] = in ? -(F0[m] + dw) : 1.0;
+                sys.c[m] = (in && k <= nnu - 3) ? Fp[m] : 0.0;
+                sys.d[m] = in ? -dw * Jo[m] : 0.0;
+            }
+            pcr_solve<M>(sys, lane);
+            // flux correction, src/UpdateLyaJandH.jl:341-377
+#pragma unroll
+            for (int m = 0; m < M; m++) {
+                int k = lane * M + m;
+                if (k >= nnu) continue;
+                bool in = (k >= 1 && k <= nnu - 2);
+                double Jn = in ? sys.d[m] : double(J[m]);
+                if (!(sys.b[m] != 0.0)) bad |= ERRB_SOLVE;
+                double Jf = Jn > jeps ? Jn : jeps;
+                double ratio = Jf * (1.0 / (Jo[m] > jeps ? Jo[m] : jeps));
+                double hr = double(Hr[m]) * ratio, hz = double(HZ[m]) * ratio;
+                double H2 = hr * hr + hz * hz;
+                if (H2 > Jf * Jf) {
+                    double fsc = Jf / sqrt(H2);
+                    hr *= fsc;
+                    hz *= fsc;
+                }
+                J[m] = R(Jf);
+                Hr[m] = R(hr);
+                HZ[m] = R(hz);
+            }
+        }
+        // ---- store ----
+#pragma unroll
+        for (int m = 0; m < M; m++) {
+            int k = lane * M + m;
+            if (k >= nnu) continue;
+            S js = S(J[m]), hs = S(Hr[m]), zs = S(HZ[m]);
+            if (!isfinite(double(js)) || !isfinite(double(hs)) || !isfinite(double(zs))) bad |= ERRB_NONFINITE;
+            a.Jout[base + k] = js;
+            a.Hrout[base + k] = hs;
+            a.HZout[base + k] = zs;
+        }
+        // ---- epilogue partials ----
+        if (a.parts & PART_ACTIVE) {
+            const double dV = __ldg(a.dV + c);
+#pragma unroll
+            for (int m = 0; m < M; m++) {
+                int k = lane * M + m;
+                if (k >= nnu) continue;
+                double dn = kc[KC_DNU * NP + k];
+                double Jv = double(S(J[m]));
+                double e1 = Jv - 10.0 * jeps, e0 = Jv - jeps;
+                acc_e[m] += dn * (e1 > 0.0 ? e1 : 0.0) * dV;
+                acc_tot += dn * (e0 > 0.0 ? e0 : 0.0) * dV;
+            }
+        }
+        if (a.parts & PART_DIAG) {
+            // escaping flux through the outer r face, the top face and (outflow) the bottom face
+            double esc = 0.0;
+            const bool rb = (i == a.nr - 1), zt = (j == a.nz - 1), zb = (j == 0 && a.bc_z_bot == 1);
+            if (rb || zt || zb) {
+                const double Arr = rb ? __ldg(a.A_r + a.nr + (size_t)(a.nr + 1) * j) * kFourPi : 0.0;
+                const double AZt = zt ? __ldg(a.A_Z + i + (size_t)a.nr * a.nz) * kFourPi : 0.0;
+                const double AZb = zb ? __ldg(a.A_Z + i) * kFourPi : 0.0;
+#pragma unroll
+                for (int m = 0; m < M; m++) {
+                    int k = lane * M + m;
+                    if (k >= nnu) continue;
+                    double dn = kc[KC_DNU * NP + k];
+                    double hr = double(S(Hr[m])) * a.j_scale, hz = double(S(HZ[m])) * a.j_scale;
+                    if (rb) esc += dn * (Arr * (hr > 0.0 ? hr : 0.0));
+                    if (zt) esc += dn * (AZt * (hz > 0.0 ? hz : 0.0));
+                    if (zb) esc += dn * (AZb * (-hz > 0.0 ? -hz : 0.0));
+                }
+            }
+            acc_esc += esc;
+            if (lane == 0) {
+                const double dV = __ldg(a.dV + c);
+                const double k4 = kFourPiOverC * (1.0 / a.c_tilde) * a.j_scale;
+                const double inv_dt = 1.0 / a.dt;
+                double fr = (k4 * dr_sum) * inv_dt, fz = (k4 * dz_sum) * inv_dt;
+                if (a.f_r) { a.f_r[c] = fr; a.f_Z[c] = fz; }
+                acc_mf += dV * sqrt(fr * fr + fz * fz);
+                acc_L += kFourPi * dV * __ldg(a.js + c);
+                double drr = __ldg(a.rCoM + i), dzz = __ldg(a.ZCoM + j) - a.z_center;
+                double dist = sqrt(drr * drr + dzz * dzz);
+                double frad = 0.0;
+                if (dist > 0.0) {
+                    double id = 1.0 / dist;
+                    frad = fr * (drr * id) + fz * (dzz * id);
+                }
+                acc_net += dV * frad;
+                acc_out += dV * (frad > 0.0 ? frad : 0.0);
+            }
+        }
+    }
+    if (bad) atomicOr(a.err, bad);
+    if (!a.parts) return;
+    // ---- CTA reduction of the partials, fixed order ----
+    const int stride = NP + 8;
+#pragma unroll
+    for (int m = 0; m < M; m++) red[warp * stride + lane * M + m] = acc_e[m];
+    acc_tot = warp_sum(acc_tot);
+    acc_esc = warp_sum(acc_esc);
+    if (lane == 0) {
+        red[warp * stride + NP + 0] = acc_tot;
+        red[warp * stride + NP + 1] = acc_mf;
+        red[warp * stride + NP + 2] = acc_net;
+        red[warp * stride + NP + 3] = acc_out;
+        red[warp * stride + NP + 4] = acc_L;
+        red[warp * stride + NP + 5] = acc_esc;
+    }
+    __syncthreads();
+    const int ncols = nnu + kExtraCols;
+    for (int col = threadIdx.x; col < ncols; col += blockDim.x) {
+        int src = col < nnu ? col : NP + (col - nnu);
+        double s = 0.0;
+        for (int w = 0; w < nw; w++) s += red[w * stride + src];
+        a.partials[(size_t)col * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// FindActiveBins partials of the current J (src/UpdateLyaJandH.jl:47-97): one warp per cell.
+template <typename S, int M>
+__global__ void __launch_bounds__(FREQ_THREADS) k_find_active(const S *J, int nnu, int ncell, const double *dnu,
+                                                              const double *dV, double jeps, double *partials) {
+    extern __shared__ __align__(16) double fsm[];
+    constexpr int NP = 32 * M;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double acc_e[M];
+#pragma unroll
+    for (int m = 0; m < M; m++) acc_e[m] = 0.0;
+    double acc_tot = 0.0;
+    for (int c = blockIdx.x * nw + warp; c < ncell; c += gridDim.x * nw) {
+        const double v = __ldg(dV + c);
+#pragma unroll
+        for (int m = 0; m < M; m++) {
+            int k = lane * M + m;
+            if (k >= nnu) continue;
+            double Jv = double(__ldg(J + (size_t)c * nnu + k));
+            double dn = __ldg(dnu + k);
+            double e1 = Jv - 10.0 * jeps, e0 = Jv - jeps;
+            acc_e[m] += dn * (e1 > 0.0 ? e1 : 0.0) * v;
+            acc_tot += dn * (e0 > 0.0 ? e0 : 0.0) * v;
+        }
+    }
+    const int stride = NP + 8;
+#pragma unroll
+    for (int m = 0; m < M; m++) fsm[warp * stride + lane * M + m] = acc_e[m];
+    acc_tot = warp_sum(acc_tot);
+    if (lane == 0) fsm[warp * stride + NP] = acc_tot;
+    __syncthreads();
+    for (int col = threadIdx.x; col <= nnu; col += blockDim.x) {
+        int src = col < nnu ? col : NP;
+        double s = 0.0;
+        for (int w = 0; w < nw; w++) s += fsm[w * stride + src];
+        partials[(size_t)col * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// Column sums of the partials (one warp per column, fixed order), then FindActiveBins'
+// decision and the diagnostics of Update_f_Lya_MF_L_Lya! / Compute_f_esc_Lya_Cylindrical.
+__global__ void __launch_bounds__(1024) k_reduce(RedArgs a) {
+    __shared__ double col[256 + kExtraCols];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int ncols = a.nnu + kExtraCols;
+    for (int cc = warp; cc < ncols; cc += nw) {
+        bool need = (cc < a.nnu + 1) ? (a.parts & PART_ACTIVE) : (a.parts & PART_DIAG);
+        double s = 0.0;
+        if (need)
+            for (int b = lane; b < a.nblocks; b += 32) s += a.partials[(size_t)cc * a.nblocks + b];
+        s = warp_sum(s);
+        if (lane == 0) col[cc] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    int used_kmin = a.kwin[0], used_kmax = a.kwin[1];
+    if (a.parts & PART_ACTIVE) {
+        double Etot = col[a.nnu];
+        int kmin = a.nnu - 1, kmax = 0;
+        for (int k = 0; k < a.nnu; k++) {
+            if (col[k] > kEpsActive * Etot) {
+                kmin = k < kmin ? k : kmin;
+                kmax = k > kmax ? k : kmax;
+            }
+        }
+        kmax = kmax > a.kcore_max ? kmax : a.kcore_max;
+        kmin = kmin < a.kcore_min ? kmin : a.kcore_min;
+        a.kwin[0] = kmin;
+        a.kwin[1] = kmax;
+    }
+    if (a.parts & PART_DIAG) {
+        double MF = col[a.nnu + 1], net = col[a.nnu + 2], outw = col[a.nnu + 3];
+        double L = col[a.nnu + 4];
+        if (L > 0.0) {
+            double kk = 1.0 / (L / kC);
+            MF *= kk; net *= kk; outw *= kk;
+        } else {
+            MF = 0.0; net = 0.0; outw = 0.0;
+        }
+        double Ltot = (a.bc_z_bot == 0) ? 2.0 * L : L;
+        double Lsim = (a.bc_z_bot == 0) ? 0.5 * Ltot : Ltot;
+        double fesc = (Ltot > 0.0 && Lsim > 0.0) ? col[a.nnu + 5] / Lsim : 0.0;
+        double rec[7] = {MF, net, outw, Ltot, fesc, (double)used_kmin, (double)used_kmax};
+        if (a.last)
+            for (int q = 0; q < 7; q++) a.last[q] = rec[q];
+        if (a.diag && a.step_counter) {
+            int idx = *a.step_counter;
+            if (idx < a.hist_capacity)
+                for (int q = 0; q < 7; q++) a.diag[(size_t)idx * 7 + q] = rec[q];
+            *a.step_counter = idx + 1;
+        }
+    }
+}
+
+// ---- launch wrappers ----------------------------------------------------------------------
+static size_t adv_smem_bytes(int prec) {
+    size_t per = (prec == 0) ? sizeof(double) : sizeof(float);
+    return per * 32 * (TJ * (TI + 1) * 3 + TJ * (TI + 1) * 2 + (TJ + 1) * TI * 3);
+}
+
+template <typename S, typename R, int FLUX>
+static void adv_launch(const void *args, int nnu, int nr, int nz, cudaStream_t st, int prec) {
+    static bool attr = false;
+    size_t sm = adv_smem_bytes(prec);
+    if (!attr) {
+        cudaFuncSetAttribute(k_advect<S, R, FLUX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        attr = true;
+    }
+    dim3 grid((nr + TI - 1) / TI, (nz + TJ - 1) / TJ, (nnu + 31) / 32);
+    k_advect<S, R, FLUX><<<grid, ADV_THREADS, sm, st>>>(*static_cast<const AdvArgs<S> *>(args));
+}
+
+void launch_advect(int prec, int flux, const void *args, int nnu, int nr, int nz, cudaStream_t st) {
+    if (prec == 0) {
+        if (flux == 0) adv_launch<double, double, 0>(args, nnu, nr, nz, st, prec);
+        else adv_launch<double, double, 1>(args, nnu, nr, nz, st, prec);
+    } else {
+        if (flux == 0) adv_launch<float, float, 0>(args, nnu, nr, nz, st, prec);
+        else adv_launch<float, float, 1>(args, nnu, nr, nz, st, prec);
+    }
+}
+
+static int bins_per_lane(int nnu) { return nnu <= 32 ? 1 : nnu <= 64 ? 2 : nnu <= 128 ? 4 : 8; }
+
+int freq_blocks(int ncell, int dev) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int want = (ncell + (FREQ_THREADS / 32) - 1) / (FREQ_THREADS / 32);
+    int cap = sms * 4;
+    return want < cap ? (want > 0 ? want : 1) : cap;
+}
+
+template <typename S, typename R, int M>
+static void freq_launch(const void *args, int nblocks, cudaStream_t st) {
+    size_t sm = sizeof(double) * (KC_N * 32 * M + (FREQ_THREADS / 32) * (32 * M + 8));
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_freq<S, R, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        attr = true;
+    }
+    k_freq<S, R, M><<<nblocks, FREQ_THREADS, sm, st>>>(*static_cast<const FreqArgs<S> *>(args));
+}
+
+void launch_freq(int prec, const void *args, int nnu, int ncell, int nblocks, cudaStream_t st) {
+    (void)ncell;
+    int M = bins_per_lane(nnu);
+    if (prec == 0) {
+        switch (M) {
+        case 1: freq_launch<double, double, 1>(args, nblocks, st); break;
+        case 2: freq_launch<double, double, 2>(args, nblocks, st); break;
+        case 4: freq_launch<double, double, 4>(args, nblocks, st); break;
+        default: freq_launch<double, double, 8>(args, nblocks, st); break;
+        }
+    } else {
+        switch (M) {
+        case 1: freq_launch<float, float, 1>(args, nblocks, st); break;
+        case 2: freq_launch<float, float, 2>(args, nblocks, st); break;
+        case 4: freq_launch<float, float, 4>(args, nblocks, st); break;
+        default: freq_launch<float, float, 8>(args, nblocks, st); break;
+        }
+    }
+}
+
+template <typename S, int M>
+static void active_launch(const S *J, int nnu, int ncell, const double *dnu, const double *dV, double jeps,
+                          double *partials, int nblocks, cudaStream_t st) {
+    size_t sm = sizeof(double) * (FREQ_THREADS / 32) * (32 * M + 8);
+    k_find_active<S, M><<<nblocks, FREQ_THREADS, sm, st>>>(J, nnu, ncell, dnu, dV, jeps, partials);
+}
+
+void launch_find_active(int prec, const void *J, int nnu, int nr, int nz, const double *dnu, const double *dV,
+                        double jeps, double *partials, int nblocks, cudaStream_t st) {
+    int ncell = nr * nz;
+    int M = bins_per_lane(nnu);
+#define LYD_ACT(T, MM) active_launch<T, MM>(static_cast<const T *>(J), nnu, ncell, dnu, dV, jeps, partials, nblocks, st)
+    if (prec == 0) {
+        switch (M) { case 1: LYD_ACT(double, 1); break; case 2: LYD_ACT(double, 2); break;
+                     case 4: LYD_ACT(double, 4); break; default: LYD_ACT(double, 8); break; }
+    } else {
+        switch (M) { case 1: LYD_ACT(float, 1); break; case 2: LYD_ACT(float, 2); break;
+                     case 4: LYD_ACT(float, 4); break; default: LYD_ACT(float, 8); break; }
+    }
+#undef LYD_ACT
+}
+
+void launch_reduce(const RedArgs &a, cudaStream_t st) { k_reduce<<<1, 1024, 0, st>>>(a); }
+
+}  // namespace lyd

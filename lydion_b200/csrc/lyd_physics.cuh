@@ -1,0 +1,292 @@
+// lyd_physics.cuh -- device arithmetic of the Lyman-alpha M1 step, templated on the
+// arithmetic type R (double for the FP64 step, float for the bulk of the mixed step).
+//
+// Each function restates one piece of the LYDION reference (paths inside its source tree):
+// the M1 closure (src/M1Closure.jl), PLM reconstruction and the GLF/HLL fluxes
+// (src/AdvectJandH.jl), and the exponentially fitted frequency leakage coefficients
+// (src/FreqFactors.jl). Thresholds that depend on the storage scale of J (the floors
+// Jeps, Heps^2) are passed in at run time.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+namespace lyd {
+
+// ---- constants (src/ConstantsAndFunctions.jl:46-170) -------------------------------------
+constexpr double kC = 2.99792458e10;
+constexpr double kInvC = 1.0 / kC;
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kFourPi = 4.0 * kPi;
+constexpr double kFourPiOverC = kFourPi / kC;
+constexpr double kHPlanck = 6.626069573e-27;
+constexpr double kKBoltz = 1.380648813e-16;
+constexpr double kHOverKB = kHPlanck / kKBoltz;
+constexpr double kNuLya = 2.466068e15;
+constexpr double kMH = 1.0080 * 1.660539069e-24;
+constexpr double kALya = 6.265e8;
+constexpr double kA2g = 8.2206;
+constexpr double kA2p2s = 8.78e-7;
+constexpr double kA2s2p = 1.597e-9;
+// src/M1Closure.jl:36-41
+constexpr double kFmin = 1e-10;
+constexpr double kFmax = 1.0 - 1e-10;
+constexpr double kJeps = 1e-60;
+constexpr double kHeps = 1e-100;
+// src/FreqFactors.jl:16-18
+constexpr double kPmin = 1e-3;
+constexpr double kPmax = 40.0;
+// src/UpdateLyaJandH.jl:43
+constexpr double kEpsActive = 1e-10;
+
+template <typename R> struct Num;
+template <> struct Num<double> {
+    static __device__ __forceinline__ double third() { return 1.0 / 3.0; }
+    static __device__ __forceinline__ double fmin() { return kFmin; }
+    static __device__ __forceinline__ double fmax() { return kFmax; }
+    static __device__ __forceinline__ double tiny() { return 1e-300; }
+};
+template <> struct Num<float> {
+    static __device__ __forceinline__ float third() { return 1.0f / 3.0f; }
+    static __device__ __forceinline__ float fmin() { return 1e-10f; }
+    static __device__ __forceinline__ float fmax() { return 1.0f - 1e-7f; }
+    static __device__ __forceinline__ float tiny() { return 1e-37f; }
+};
+
+__device__ __forceinline__ double rsq(double x) { return sqrt(x); }
+__device__ __forceinline__ float rsq(float x) { return sqrtf(x); }
+
+// MinMod, src/ConstantsAndFunctions.jl:1571-1582
+template <typename R>
+__device__ __forceinline__ R minmod(R a, R b) {
+    return (a * b <= R(0)) ? R(0) : (fabs(a) < fabs(b) ? a : b);
+}
+
+// Levermore closure chi(f), src/M1Closure.jl:28-33
+template <typename R>
+__device__ __forceinline__ R chi_L84(R f) {
+    R f2 = f * f;
+    return (R(3) + R(4) * f2) / (R(5) + R(2) * rsq(R(4) - R(3) * f2));
+}
+
+// Compute_D_Edd_from_f_n, src/M1Closure.jl:91-119
+template <typename R>
+__device__ __forceinline__ void D_from_f_n(R f, R nr, R nZ, R &Drr, R &DZZ, R &DrZ) {
+    if (f > Num<R>::fmin()) {
+        f = f < Num<R>::fmax() ? f : Num<R>::fmax();
+        R chi = chi_L84(f);
+        R a = (R(1) - chi) * R(0.5);
+        R b = (R(3) * chi - R(1)) * R(0.5);
+        R b_nr = b * nr;
+        Drr = a + b_nr * nr;
+        DZZ = a + b * nZ * nZ;
+        DrZ = b_nr * nZ;
+    } else {
+        Drr = Num<R>::third(); DZZ = Num<R>::third(); DrZ = R(0);
+    }
+}
+
+// Compute_D_Edd, src/M1Closure.jl:46-83. jeps / heps2 are the floors in storage units.
+template <typename R>
+__device__ __forceinline__ void D_edd(R Hr, R HZ, R J, R jeps, R heps2, R &Drr, R &DZZ, R &DrZ) {
+    R H2 = Hr * Hr + HZ * HZ;
+    const R fmin2 = Num<R>::fmin() * Num<R>::fmin();
+    if (J <= jeps || H2 <= heps2 || H2 <= fmin2 * J * J) {
+        Drr = Num<R>::third(); DZZ = Num<R>::third(); DrZ = R(0);
+        return;
+    }
+    R Hmag = rsq(H2);
+    R f = Hmag / J;
+    f = f < Num<R>::fmin() ? Num<R>::fmin() : (f > Num<R>::fmax() ? Num<R>::fmax() : f);
+    R chi = chi_L84(f);
+    R inv_H = R(1) / Hmag;
+    R a = (R(1) - chi) * R(0.5);
+    R b = (R(3) * chi - R(1)) * R(0.5);
+    R nr = Hr * inv_H, nZ = HZ * inv_H;
+    R b_nr = b * nr;
+    Drr = a + b_nr * nr;
+    DZZ = a + b * nZ * nZ;
+    DrZ = b_nr * nZ;
+}
+
+// HLL_Eigenvalues, src/M1Closure.jl:273-296
+template <typename R>
+__device__ __forceinline__ void hll_eigen(R f, R mu, R &l1, R &l3) {
+    f = f < Num<R>::fmin() ? Num<R>::fmin() : (f > Num<R>::fmax() ? Num<R>::fmax() : f);
+    mu = mu < R(-1) ? R(-1) : (mu > R(1) ? R(1) : mu);
+    R f2 = f * f, mu2 = mu * mu, muf = mu * f;
+    R t = R(4) - R(3) * f2;
+    R sq = rsq(t > R(0) ? t : R(0));
+    R inv_sq = R(1) / sq;
+    R g = R(2) / R(3) * (R(4) - R(3) * f2 - sq) + R(2) * mu2 * (R(2) - f2 - sq);
+    R fac = rsq(g > R(0) ? g : R(0));
+    R x1 = (muf - fac) * inv_sq, x3 = (muf + fac) * inv_sq;
+    l1 = x1 < R(-1) ? R(-1) : (x1 > R(1) ? R(1) : x1);
+    l3 = x3 < R(-1) ? R(-1) : (x3 > R(1) ? R(1) : x3);
+}
+
+// One cell of the reconstruction stencil.
+template <typename R> struct Cell { R J, Hr, HZ; };
+
+// ReconstructInterface output, src/AdvectJandH.jl:359-473
+template <typename R> struct Recon {
+    R J_L, J_R, Hr_L, Hr_R, HZ_L, HZ_R, tau_L, tau_R, f_L, f_R, nr_L, nr_R, nZ_L, nZ_R;
+};
+
+// ReconstructInterface, src/AdvectJandH.jl:359-473. Cells: im1, i, ip1, ip2 around the
+// interface between i and ip1; iv = {dL, dR, inv_i_im1, inv_ip1_i, inv_ip2_ip1}.
+template <typename R>
+__device__ __forceinline__ Recon<R> reconstruct(const Cell<R> &cm1, const Cell<R> &ci, const Cell<R> &cp1,
+                                                const Cell<R> &cp2, const R iv[5], R aF_i, R aF_ip1, R jeps) {
+    Recon<R> o;
+    const R dL = iv[0], dR = iv[1];
+    o.tau_L = aF_i * dL;
+    o.tau_R = aF_ip1 * dR;
+    R iJ_i = R(1) / (ci.J > jeps ? ci.J : jeps);
+    R iJ_p1 = R(1) / (cp1.J > jeps ? cp1.J : jeps);
+    R iJ_p2 = R(1) / (cp2.J > jeps ? cp2.J : jeps);
+    R iJ_m1 = R(1) / (cm1.J > jeps ? cm1.J : jeps);
+    R fr_i = ci.Hr * iJ_i, fr_p1 = cp1.Hr * iJ_p1, fr_p2 = cp2.Hr * iJ_p2, fr_m1 = cm1.Hr * iJ_m1;
+    R fZ_i = ci.HZ * iJ_i, fZ_p1 = cp1.HZ * iJ_p1, fZ_p2 = cp2.HZ * iJ_p2, fZ_m1 = cm1.HZ * iJ_m1;
+
+    R dJc = (cp1.J - ci.J) * iv[3];
+    R dJL = minmod((ci.J - cm1.J) * iv[2], dJc);
+    R dJR = minmod((cp2.J - cp1.J) * iv[4], dJc);
+    R dfrc = (fr_p1 - fr_i) * iv[3];
+    R dfrL = minmod((fr_i - fr_m1) * iv[2], dfrc);
+    R dfrR = minmod((fr_p2 - fr_p1) * iv[4], dfrc);
+    R dfZc = (fZ_p1 - fZ_i) * iv[3];
+    R dfZL = minmod((fZ_i - fZ_m1) * iv[2], dfZc);
+    R dfZR = minmod((fZ_p2 - fZ_p1) * iv[4], dfZc);
+
+    R JL = ci.J + dJL * dL;
+    R JR = cp1.J - dJR * dR;
+    o.J_L = JL > jeps ? JL : jeps;
+    o.J_R = JR > jeps ? JR : jeps;
+    R frL = fr_i + dfrL * dL, frR = fr_p1 - dfrR * dR;
+    R fZL = fZ_i + dfZL * dL, fZR = fZ_p1 - dfZR * dR;
+
+    R fL = rsq(frL * frL + fZL * fZL);
+    if (fL > R(1)) { R inv = R(1) / fL; frL *= inv; fZL *= inv; fL = R(1); }
+    R fR = rsq(frR * frR + fZR * fZR);
+    if (fR > R(1)) { R inv = R(1) / fR; frR *= inv; fZR *= inv; fR = R(1); }
+
+    o.Hr_L = frL * o.J_L; o.Hr_R = frR * o.J_R;
+    o.HZ_L = fZL * o.J_L; o.HZ_R = fZR * o.J_R;
+    if (fL > R(0)) { R inv = R(1) / fL; o.nr_L = frL * inv; o.nZ_L = fZL * inv; }
+    else { o.nr_L = R(0); o.nZ_L = R(0); }
+    if (fR > R(0)) { R inv = R(1) / fR; o.nr_R = frR * inv; o.nZ_R = fZR * inv; }
+    else { o.nr_R = R(0); o.nZ_R = R(0); }
+    o.f_L = fL; o.f_R = fR;
+    return o;
+}
+
+// GetFluxGLF / GetFluxHLL, src/AdvectJandH.jl:81-118, 155-204, with the wave speeds of
+// M1WaveSpeeds_r/Z (src/M1Closure.jl:301-326). F{J,Hr,HZ}_{L,R} are the physical fluxes of
+// the three conserved quantities on either side; Ji/Jip1 the cell values for the
+// diffusion-limit term. ZDIR selects n_Z (true) or n_r (false) for the HLL eigenvalues.
+template <typename R, int FLUX, bool ZDIR>
+__device__ __forceinline__ void m1_flux(R FJ_L, R FJ_R, R FHr_L, R FHr_R, R FHZ_L, R FHZ_R,
+                                        const Recon<R> &q, R Ji, R Jip1, R &FJ, R &FHr, R &FHZ) {
+    R tau = q.tau_L + q.tau_R;
+    R num = R(0.2) + tau;
+    R eps = num / (num + tau * tau);
+    R ome = R(1) - eps;
+    R tau_eff = tau > Num<R>::tiny() ? tau : Num<R>::tiny();
+    R FJ_diff = -Num<R>::third() * (Jip1 - Ji) / tau_eff;
+    if (FLUX == 0) {
+        R FJ_glf = R(0.5) * (FJ_L + FJ_R) - R(0.5) * (q.J_R - q.J_L);
+        FJ = eps * FJ_glf + ome * FJ_diff;
+        R he = R(0.5) * eps;
+        FHr = R(0.5) * (FHr_L + FHr_R) - he * (q.Hr_R - q.Hr_L);
+        FHZ = R(0.5) * (FHZ_L + FHZ_R) - he * (q.HZ_R - q.HZ_L);
+    } else {
+        R l1L, l3L, l1R, l3R;
+        hll_eigen<R>(q.f_L, ZDIR ? q.nZ_L : q.nr_L, l1L, l3L);
+        hll_eigen<R>(q.f_R, ZDIR ? q.nZ_R : q.nr_R, l1R, l3R);
+        R SR = fmax(fmax(l3L, l3R), R(0));
+        R SL = fmin(fmin(l1L, l1R), R(0));
+        R dS = SR - SL;
+        R inv_dS = R(1) / (dS > Num<R>::tiny() ? dS : Num<R>::tiny());
+        R SRSL = SR * SL;
+        R FJh = (SR * FJ_L - SL * FJ_R + SRSL * (q.J_R - q.J_L)) * inv_dS;
+        R FHrh = (SR * FHr_L - SL * FHr_R + SRSL * (q.Hr_R - q.Hr_L)) * inv_dS;
+        R FHZh = (SR * FHZ_L - SL * FHZ_R + SRSL * (q.HZ_R - q.HZ_L)) * inv_dS;
+        R hom = R(0.5) * ome;
+        FJ = eps * FJh + ome * FJ_diff;
+        FHr = eps * FHrh + hom * (FHr_L + FHr_R);
+        FHZ = eps * FHZh + hom * (FHZ_L + FHZ_R);
+    }
+}
+
+// GetAdvectionFlux, src/AdvectJandH.jl:276-282
+template <typename R>
+__device__ __forceinline__ R adv_flux(R uc, R L, R Rv) { return uc * (uc < R(0) ? Rv : L); }
+
+// Compute_K_phiphi_InnerAxis, src/AdvectJandH.jl:499-522
+template <typename R>
+__device__ __forceinline__ R k_phiphi_axis(R J, R HZ, R jeps) {
+    J = J > jeps ? J : jeps;
+    R fZ = HZ / J;
+    fZ = fZ < R(-1) ? R(-1) : (fZ > R(1) ? R(1) : fZ);
+    R f = fabs(fZ);
+    R nZ = f > R(0) ? (fZ > R(0) ? R(1) : R(-1)) : R(0);
+    R Drr, DZZ, DrZ;
+    D_from_f_n<R>(f, R(0), nZ, Drr, DZZ, DrZ);
+    R k = R(1) - Drr - DZZ;
+    k = k < R(0) ? R(0) : (k > R(1) ? R(1) : k);
+    return k * J;
+}
+
+template <typename R>
+__device__ __forceinline__ R clamp01(R x) { return x < R(0) ? R(0) : (x > R(1) ? R(1) : x); }
+
+// D_colon_grad_u_Cylindrical, src/ConstantsAndFunctions.jl:883-895
+template <typename R>
+__device__ __forceinline__ R d_colon_grad_u(R Drr, R DrZ, R DZZ, R a, R b, R c, R d, R e) {
+    R Dpp = R(1) - Drr - DZZ;
+    Dpp = Dpp > R(0) ? Dpp : R(0);
+    return Drr * a + DrZ * (b + c) + DZZ * d + Dpp * e;
+}
+
+// OneMinusphi_L_and_chi_L / OneMinusphi_R_and_chi_R, src/FreqFactors.jl:54-133, in FP64.
+__device__ __forceinline__ void omphi_L(double P, double &omp, double &chi) {
+    if (P >= kPmax) { omp = exp(-kPmax); chi = (1.0 - omp) / kPmax; return; }
+    if (P <= -kPmax) { omp = exp(kPmax); chi = (1.0 - omp) / (-kPmax); return; }
+    if (fabs(P) < kPmin) { omp = 1.0 - P + 0.5 * (P * P); chi = 1.0 - 0.5 * P; return; }
+    omp = exp(-P);
+    chi = (1.0 - omp) / P;
+}
+__device__ __forceinline__ void omphi_R(double P, double &omp, double &chi) {
+    if (P >= kPmax) { omp = exp(kPmax); chi = (1.0 - omp) / kPmax; return; }
+    if (P <= -kPmax) { omp = exp(-kPmax); chi = (1.0 - omp) / (-kPmax); return; }
+    if (fabs(P) < kPmin) { omp = 1.0 + P + 0.5 * (P * P); chi = -1.0 - 0.5 * P; return; }
+    omp = exp(P);
+    chi = (1.0 - omp) / P;
+}
+// FP32 variants for the mixed step (same branches, float arithmetic)
+__device__ __forceinline__ void omphi_L(float P, float &omp, float &chi) {
+    const float Pm = 40.0f;
+    if (P >= Pm) { omp = expf(-Pm); chi = (1.0f - omp) / Pm; return; }
+    if (P <= -Pm) { omp = expf(Pm); chi = (1.0f - omp) / (-Pm); return; }
+    if (fabsf(P) < 1e-3f) { omp = 1.0f - P + 0.5f * (P * P); chi = 1.0f - 0.5f * P; return; }
+    omp = expf(-P);
+    chi = (1.0f - omp) / P;
+}
+__device__ __forceinline__ void omphi_R(float P, float &omp, float &chi) {
+    const float Pm = 40.0f;
+    if (P >= Pm) { omp = expf(Pm); chi = (1.0f - omp) / Pm; return; }
+    if (P <= -Pm) { omp = expf(-Pm); chi = (1.0f - omp) / (-Pm); return; }
+    if (fabsf(P) < 1e-3f) { omp = 1.0f + P + 0.5f * (P * P); chi = -1.0f - 0.5f * P; return; }
+    omp = expf(P);
+    chi = (1.0f - omp) / P;
+}
+
+// Thermal velocity, Doppler width, Voigt parameter (src/ConstantsAndFunctions.jl:282-314)
+__host__ __device__ __forceinline__ double compute_b(double T) { return sqrt(2.0 * kKBoltz / kMH) * sqrt(T); }
+__host__ __device__ __forceinline__ double compute_dnuD(double T) { return compute_b(T) * (kNuLya / kC); }
+__host__ __device__ __forceinline__ double compute_a(double T) {
+    return (kALya / (kFourPi * kNuLya * 1.0 / kC)) / compute_b(T);
+}
+
+}  // namespace lyd

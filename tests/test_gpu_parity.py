@@ -1,0 +1,246 @@
+"""GPU parity of the CUDA step against the FP64 oracle, through the C ABI.
+
+Tolerances (FP64 path): the kernels follow the reference's operation order, but the GPU
+contracts multiply-adds into FMAs and solves the frequency systems by cyclic reduction
+instead of dgtsv's pivoted elimination; both solvers are backward stable and agree to the
+conditioning of the system (~1e-9 relative at F/dw ~ 4e8, tau0 = 1e8, measured against a
+50-digit solve). Element-wise bounds below are relative to the field's maximum.
+"""
+import numpy as np
+import pytest
+
+from helpers import CLOUDS, matched_pair, max_rel, norm_err, random_state
+from lydion_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+BC_CASES = [("glf_outflow", 1, 1), ("glf_outflow", 0, 0), ("hll_outflow", 1, 0), ("glf_zout_48", 1, 1),
+            ("hll_point_64", 0, 1), ("glf_20bins", 1, 1)]
+
+
+def _set_bcs(cloud, r_right, z_top):
+    cloud.bc_r_right = r_right
+    cloud.bc_z_top = z_top
+    return cloud
+
+
+@pytest.mark.parametrize("name,bcr,bzt", BC_CASES)
+def test_advect_matches_oracle(oracle_mod, name, bcr, bzt):
+    cl = _set_bcs(CLOUDS[name](), bcr, bzt)
+    st, ctx = matched_pair(oracle_mod, cl, seed=11)
+    ctdt = cl.c_tilde * cl.dt
+    for _ in range(3):
+        km_o = st.advect(ctdt)
+        km_g = ctx.find_active_bins()
+        assert km_g == km_o
+        ctx.advect(ctdt, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+    for f in ("J", "H_r", "H_Z"):
+        e = norm_err(ctx.download(f), getattr(st, f))
+        assert e < 1e-12, (f, e)
+    # AdvectLya! leaves J_old = J and H_old = H
+    np.testing.assert_array_equal(ctx.download("J_old"), ctx.download("J"))
+    np.testing.assert_array_equal(ctx.download("H_Z_old"), ctx.download("H_Z"))
+
+
+def test_advect_partial_active_window(oracle_mod):
+    """Bins outside FindActiveBins' window are passed through untouched."""
+    cl = CLOUDS["hll_point_64"]()
+    st, ctx = matched_pair(oracle_mod, cl, seed=3)
+    J, Hr, HZ = random_state(cl, 3)
+    J[..., :6] = 1e-58
+    J[..., -6:] = 1e-58
+    for name, a in (("J", J), ("H_r", Hr * 0), ("H_Z", HZ * 0)):
+        getattr(st, name)[...] = a
+        ctx.upload(name, a)
+    k = st.advect(cl.c_tilde * cl.dt)
+    assert k[0] > 0 and k[1] < cl.n_nu - 1
+    ctx.advect(cl.c_tilde * cl.dt, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+    assert norm_err(ctx.download("J"), st.J) < 1e-12
+    np.testing.assert_array_equal(ctx.download("J")[..., : k[0]], J[..., : k[0]])
+
+
+@pytest.mark.parametrize("name", ["glf_outflow", "glf_zout_48", "glf_20bins"])
+def test_emission_absorption_matches_oracle(oracle_mod, name):
+    cl = CLOUDS[name]()
+    st, ctx = matched_pair(oracle_mod, cl, seed=5)
+    for _ in range(2):
+        st.emission_absorption(cl.c_tilde, cl.dt)
+        ctx.emission_absorption(cl.c_tilde, cl.dt)
+    for f in ("J", "H_r", "H_Z", "J_old", "H_r_old"):
+        assert norm_err(ctx.download(f), getattr(st, f)) < 1e-14, f
+    for f in ("dru_r", "dru_Z"):
+        assert norm_err(ctx.download(f), getattr(st, f)) < 1e-12, f
+
+
+@pytest.mark.parametrize("name", ["glf_outflow", "hll_point_64", "glf_zout_48", "glf_20bins"])
+def test_frequency_update_matches_oracle(oracle_mod, name):
+    cl = CLOUDS[name]()
+    st, ctx = matched_pair(oracle_mod, cl, seed=7)
+    ctdt = cl.c_tilde * cl.dt
+    nf, _ = st.frequency_update(ctdt)
+    assert nf == 0
+    ctx.frequency_update(ctdt)
+    for f in ("J", "H_r", "H_Z"):
+        e = norm_err(ctx.download(f), getattr(st, f))
+        assert e < 1e-9, (f, e)
+    assert max_rel(ctx.download("J"), st.J, floor=1e-6 * st.J.max()) < 1e-8
+
+
+def test_frequency_update_keep_factors(oracle_mod):
+    cl = CLOUDS["glf_outflow"]()
+    st, ctx = matched_pair(oracle_mod, cl, seed=9, keep_ff=True)
+    ctdt = cl.c_tilde * cl.dt
+    st.frequency_update(ctdt, True)
+    ctx.frequency_update(ctdt, True)
+    st.frequency_update(ctdt, False)
+    ctx.frequency_update(ctdt, False)
+    assert norm_err(ctx.download("J"), st.J) < 1e-9
+
+
+def test_frequency_update_without_kept_factors_is_an_error(oracle_mod):
+    from lydion_b200._lib import LydionError, LYD_ERR_STATE
+    cl = CLOUDS["glf_outflow"]()
+    _, ctx = matched_pair(oracle_mod, cl, seed=9)
+    with pytest.raises(LydionError) as e:
+        ctx.frequency_update(cl.c_tilde * cl.dt, False)
+    assert e.value.code == LYD_ERR_STATE
+
+
+@pytest.mark.parametrize("name", ["glf_outflow", "hll_outflow", "glf_zout_48", "hll_point_64"])
+def test_static_steps_match_oracle(oracle_mod, name):
+    cl = CLOUDS[name]()
+    st, ctx = matched_pair(oracle_mod, cl)
+    n = 40
+    d_o = st.run(n)
+    d_g = ctx.static_steps(n, cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+    np.testing.assert_array_equal(d_g[:, 5:7], d_o[:, 5:7])       # active windows
+    np.testing.assert_allclose(d_g[:, 3], d_o[:, 3], rtol=1e-13)   # L
+    for col in (0, 1, 2):
+        assert max_rel(d_g[5:, col], d_o[5:, col]) < 1e-9, col
+    assert max_rel(d_g[10:, 4], d_o[10:, 4], floor=1e-6 * np.abs(d_o[:, 4]).max()) < 1e-8
+    for f in ("J", "H_r", "H_Z"):
+        assert norm_err(ctx.download(f), getattr(st, f)) < 1e-9, f
+    np.testing.assert_allclose(ctx.download("f_r"), st.f_r, rtol=1e-8, atol=1e-9 * np.abs(st.f_r).max())
+    assert np.all(ctx.download("dru_r") == 0.0)
+
+
+def test_per_phase_calls_equal_fused_step(oracle_mod):
+    cl = CLOUDS["glf_outflow"]()
+    _, a = matched_pair(oracle_mod, cl, seed=21)
+    _, b = matched_pair(oracle_mod, cl, seed=21)
+    ctdt = cl.c_tilde * cl.dt
+    for _ in range(3):
+        a.advect(ctdt, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+        a.emission_absorption(cl.c_tilde, cl.dt)
+        a.frequency_update(ctdt)
+        a.reset_dru()
+    b.static_steps(3, cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+    for f in ("J", "H_r", "H_Z"):
+        np.testing.assert_array_equal(a.download(f), b.download(f))
+
+
+def test_update_J_and_H_matches_oracle(oracle_mod):
+    cl = CLOUDS["glf_zout_48"]()
+    st, ctx = matched_pair(oracle_mod, cl, seed=13)
+    ctdt = cl.c_tilde * cl.dt
+    st.advect(ctdt)
+    st.frequency_update(ctdt)
+    ctx.update_J_and_H(cl.dt, cl.c_tilde, True, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+    assert norm_err(ctx.download("J"), st.J) < 1e-9
+
+
+def test_diagnostics_match_oracle(oracle_mod):
+    cl = CLOUDS["glf_zout_48"]()
+    st, ctx = matched_pair(oracle_mod, cl, seed=17)
+    st.emission_absorption(cl.c_tilde, cl.dt)
+    ctx.emission_absorption(cl.c_tilde, cl.dt)
+    mo = st.force_multiplier(cl.dt)
+    mg = ctx.force_multiplier(cl.dt, cl.z_center, cl.bc_z_bot)
+    np.testing.assert_allclose(mg, mo, rtol=1e-12)
+    np.testing.assert_allclose(ctx.download("f_Z"), st.f_Z, rtol=1e-12, atol=1e-300)
+    fo = st.f_esc(mo[3])
+    fg = ctx.f_esc(mg[3], cl.bc_z_bot)
+    assert fg == pytest.approx(fo, rel=1e-12)
+    ro, no, rio, zio = st.edge_spectra()
+    rg, ng, rig, zig = ctx.edge_spectra()
+    np.testing.assert_array_equal(rig, rio)
+    np.testing.assert_array_equal(zig, zio)
+    np.testing.assert_allclose(rg, ro, rtol=1e-14, atol=0)   # FMA rounding of the emission update
+    np.testing.assert_allclose(ng, no, rtol=1e-13)
+
+
+def test_device_hvoigt_and_phi_match_oracle(oracle_mod):
+    cl = W.small_cloud(nr=6, nz=5, n_nu=64, x_max=600.0)
+    cl.T = np.linspace(30.0, 3e4, cl.nr * cl.nz).reshape(cl.nz, cl.nr)
+    st, ctx = matched_pair(oracle_mod, cl, device_hvoigt=True)
+    hv = ctx.download("Hvoigt")
+    assert max_rel(hv, st.Hvoigt, floor=1e-300) < 1e-9
+    assert norm_err(hv, st.Hvoigt) < 1e-13
+
+
+def test_pd_and_cfl_on_device(oracle_mod):
+    from lydion_b200.m1 import M1Context
+    rng = np.random.default_rng(2)
+    n = 500
+    nH = 10 ** rng.uniform(-2, 6, n)
+    xi = rng.uniform(0, 1, n)
+    T = 10 ** rng.uniform(1, 5, n)
+    args = (xi * nH, xi * nH, (1 - xi) * nH, 0.08 * nH, 0.1 * rng.uniform(size=n) * nH, T)
+    cl = CLOUDS["glf_outflow"]()
+    st, ctx = matched_pair(oracle_mod, cl)
+    got = ctx.pd_lya(*args, z=3.0)
+    L = oracle_mod.lib()
+    ref = np.array([L.orc_pd_lya(*(a[q] for a in args), 3.0) for q in range(n)])
+    np.testing.assert_allclose(got, ref, rtol=1e-13)
+    dt = ctx.cfl_dt(cl.c_tilde, cl.u_r, cl.u_Z, 0.4)
+    assert dt == pytest.approx(W.cfl_dt(cl.geom, cl.c_tilde, cl.u_r, cl.u_Z, 0.4), rel=1e-15)
+
+
+def test_nonfinite_input_is_reported(oracle_mod):
+    """An infinite J_old makes the emission update produce a non-finite J, which the kernel
+    flags; the flag is reported at the next synchronising call and then cleared."""
+    from lydion_b200._lib import LydionError, LYD_ERR_NONFINITE
+    cl = CLOUDS["glf_outflow"]()
+    _, ctx = matched_pair(oracle_mod, cl, seed=1)
+    J = ctx.download("J_old")
+    J[2, 3, 5] = np.inf
+    ctx.upload("J_old", J)
+    ctx.emission_absorption(cl.c_tilde, cl.dt)
+    with pytest.raises(LydionError) as e:
+        ctx.synchronize()
+    assert e.value.code == LYD_ERR_NONFINITE
+    J, Hr, HZ = random_state(cl, 2)
+    for name, a in (("J", J), ("H_r", Hr), ("H_Z", HZ), ("J_old", J)):
+        ctx.upload(name, a)
+    ctx.emission_absorption(cl.c_tilde, cl.dt)
+    ctx.frequency_update(cl.c_tilde * cl.dt)
+    ctx.synchronize()
+
+
+def test_bad_arguments_are_rejected(oracle_mod):
+    from lydion_b200._lib import LydionError, LYD_ERR_ARG, LYD_ERR_STATE
+    from lydion_b200.m1 import M1Context
+    cl = CLOUDS["glf_outflow"]()
+    _, ctx = matched_pair(oracle_mod, cl, seed=1)
+    with pytest.raises(LydionError) as e:
+        ctx.advect(cl.c_tilde * cl.dt, bc_r_left=1)
+    assert e.value.code == LYD_ERR_ARG
+    with pytest.raises(LydionError):
+        ctx.upload("J", np.zeros(7))
+    bare = M1Context(cl.n_nu, cl.nr, cl.nz, cl.freq.kcore_min, cl.freq.kcore_max, cl.alpha_floor)
+    with pytest.raises(LydionError) as e:
+        bare.advect(1.0)
+    assert e.value.code == LYD_ERR_STATE
+    bare.close()
+
+
+def test_full_size_c2_steps_match_oracle(oracle_mod):
+    """The headline 256x256x64 cloud: 6 fused steps against the oracle."""
+    cl = W.config_c2()
+    st, ctx = matched_pair(oracle_mod, cl)
+    d_o = st.run(6)
+    d_g = ctx.static_steps(6, cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+    np.testing.assert_array_equal(d_g[:, 5:7], d_o[:, 5:7])
+    assert max_rel(d_g[1:, 0], d_o[1:, 0]) < 1e-9
+    for f in ("J", "H_r", "H_Z"):
+        assert norm_err(ctx.download(f), getattr(st, f)) < 1e-9, f
