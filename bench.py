@@ -166,6 +166,7 @@ def run_gpu(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from lydion_b200 import sharding
     from lydion_b200 import workloads as W
     from lydion_b200.m1 import context_for_cloud
     from lydion_b200._lib import PREC_FP64
@@ -194,13 +195,8 @@ def run_gpu(args):
         barrier()
     ms = e0.elapsed_time(e1)
     clocks = clk.summary()
-    ms_max = ms
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    units = world * args.steps * cloud.cell_bins
-    value = units / (ms_max * 1e-3)
+    ms_max = sharding.max_over_ranks(ms, device="cuda")
+    value = sharding.weak_scaling_throughput(args.steps * cloud.cell_bins, world, ms_max)
 
     # per-kernel device time over a separate pass (events around every launch)
     ctx.set_timing(True)
@@ -235,12 +231,8 @@ def run_gpu(args):
             a[...] = ctx.download(name)
     f1.record(stream)
     f1.synchronize()
-    e2e_ms = f0.elapsed_time(f1)
-    if dist:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * e2e_steps * cloud.cell_bins / (e2e_ms * 1e-3)
+    e2e_ms = sharding.max_over_ranks(f0.elapsed_time(f1), device="cuda")
+    e2e_value = sharding.weak_scaling_throughput(e2e_steps * cloud.cell_bins, world, e2e_ms)
     nbytes = 3 * cloud.cell_bins * 8
 
     cpu = cpu_baseline(cloud) if (rank == 0 and world == 1 and not args.no_cpu) else None
