@@ -198,6 +198,23 @@ int  lyd_edge_spectra(lyd_ctx *ctx, double *raw, double *norm, int32_t *r_index,
  * Host-only; needs no GPU. */
 int  lyd_voigt_tables(double *out, int32_t n, double xmax);
 
+/* ---- FindActiveBins without any device allocation ----------------------------------------
+ * No counterpart in the reference. For callers that may not allocate device memory (a host
+ * framework that owns every allocation through its own pool, a plugin inside a fixed memory
+ * budget, a time loop that must not allocate): computes the active-bin window of
+ * FindActiveBins from caller-owned device arrays J (n_nu*n_r*n_z, FP64, [k,i,j]), dnu (n_nu)
+ * and dV (n_r*n_z), on `stream` (a cudaStream_t; NULL is the legacy default stream), and
+ * returns kmin/kmax (0-based) to the host after synchronising that stream. It creates no
+ * context and calls no cudaMalloc/cudaFree: its scratch is a file-scope 1 MiB device array
+ * (131072 FP64 partial sums) that every GPU loading the library holds until exit. The first
+ * call on each device looks up that array's address, so make the first call before any
+ * stream capture. All calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. Returns LYD_ERR_ARG for n_nu > 256 (or n_nu < 4, n_r < 3,
+ * n_z < 3, a bad core range, a null pointer). */
+int  lyd_find_active_bins_noalloc(const double *J, const double *dnu, const double *dV, int32_t n_nu,
+                                  int32_t n_r, int32_t n_z, int32_t kcore_min, int32_t kcore_max,
+                                  void *stream, int32_t *kmin, int32_t *kmax);
+
 #ifdef __cplusplus
 }
 #endif

@@ -90,6 +90,8 @@ SIGNATURES = {
     "lyd_edge_count": (C.c_int, [I32, I32]),
     "lyd_edge_spectra": (C.c_int, [VP, P, P, C.POINTER(I32), C.POINTER(I32)]),
     "lyd_voigt_tables": (C.c_int, [P, I32, D]),
+    "lyd_find_active_bins_noalloc": (C.c_int, [VP, VP, VP, I32, I32, I32, I32, I32, VP, C.POINTER(I32),
+                                               C.POINTER(I32)]),
 }
 
 _lib = None
