@@ -22,9 +22,6 @@
 
 namespace lyd {
 
-constexpr int TI = 8;          // tile width in r
-constexpr int TJ = 4;          // tile height in Z
-constexpr int ADV_THREADS = 256;
 constexpr int FREQ_THREADS = 256;
 
 template <typename S, typename R>
@@ -98,20 +95,70 @@ __device__ __forceinline__ R alpha_F(const AdvArgs<S> &a, int i, int j, int k) {
     return v;
 }
 
-// One r interface f (between cells f-1 and f) in row j: the three fluxes plus the
-// K_phiphi of both sides (src/AdvectJandH.jl:641-968).
+// ---- k_advect: one CTA = 8 columns (r) x ROWS rows (Z) x 32 bins, marching up in Z ----------
+//
+// A ring of four rows holds, for the 8 own columns and the 2 + 2 halo columns of each row,
+// the cell values every face needs: J, the reduced fluxes H/max(J, Jeps) and alpha_F (so the
+// reciprocal of J is taken once per cell, not once per face), plus the raw H of the own
+// columns for the cell update. Warp w (0..7) owns column i0+w; warp 8 stages the halo
+// columns and computes the tile's rightmost r face. Per row: stage row j+2 -> sync -> every
+// warp computes the r face on its left (warp 8: the right edge) into shared memory and its
+// Z face j+1/2 into registers -> sync -> the cell update of row j uses the two r faces from
+// shared memory and the Z faces j-1/2 (carried from the previous row) and j+1/2.
+constexpr int MT = 8;                  // own columns per CTA
+constexpr int MWARPS = MT + 1;
+constexpr int MTHREADS = 32 * MWARPS;
+constexpr int MCOL = MT + 4;           // staged columns i0-2 .. i0+MT+1
+constexpr int RING = 4;
+constexpr int MROWS = 16;              // rows per CTA
+
+template <typename S, typename R>
+__device__ __forceinline__ Cell<R> raw_cell(const AdvArgs<S> &a, int col, int row, int k) {
+    if (col < 0 || col >= a.nr) return r_cell<S, R>(a, col, row, k);
+    if (row < 0 || row >= a.nz) return z_cell<S, R>(a, col, row, k);
+    return ld_cell<S, R>(a, col, row, k);
+}
+
+// Stage cell (col, row) into ring slot `slot`, staged column lc (= col - i0 + 2).
+template <typename S, typename R>
+__device__ __forceinline__ void stage_cell(const AdvArgs<S> &a, R *A, R *Hh, int slot, int lc, int col, int row,
+                                           int k, int lane, R jeps) {
+    Cell<R> c = raw_cell<S, R>(a, col, row, k);
+    CellF<R> f = cell_f<R>(c.J, c.Hr, c.HZ, jeps);
+    int cc = col < 0 ? 0 : (col >= a.nr ? a.nr - 1 : col);
+    int rr = row < 0 ? 0 : (row >= a.nz ? a.nz - 1 : row);
+    R aF = alpha_F<S, R>(a, cc, rr, k);
+    R *p = A + ((slot * MCOL + lc) * 4) * 32 + lane;
+    p[0] = f.J; p[32] = f.fr; p[64] = f.fZ; p[96] = aF;
+    if (lc >= 2 && lc < 2 + MT) {
+        R *q = Hh + ((slot * MT + (lc - 2)) * 2) * 32 + lane;
+        q[0] = c.Hr; q[32] = c.HZ;
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ CellF<R> staged(const R *A, int slot, int lc, int lane, R &aF) {
+    const R *p = A + ((slot * MCOL + lc) * 4) * 32 + lane;
+    CellF<R> c;
+    c.J = p[0]; c.fr = p[32]; c.fZ = p[64];
+    aF = p[96];
+    return c;
+}
+
+// r face f (between cells f-1 and f) of row j held in ring slot `slot`; wl = f - i0 is the
+// staged column of the stencil's first cell (src/AdvectJandH.jl:641-968).
 template <typename S, typename R, int FLUX>
-__device__ __forceinline__ void face_r(const AdvArgs<S> &a, int f, int j, int k, R jeps, R *F, R &kL, R &kR) {
-    Cell<R> cm1 = r_cell<S, R>(a, f - 2, j, k);
-    Cell<R> ci = r_cell<S, R>(a, f - 1, j, k);
-    Cell<R> cp1 = r_cell<S, R>(a, f, j, k);
-    Cell<R> cp2 = r_cell<S, R>(a, f + 1, j, k);
+__device__ __forceinline__ void face_r_staged(const AdvArgs<S> &a, const R *A, int slot, int wl, int f, int j,
+                                              int lane, R jeps, R *F, R &kL, R &kR) {
+    R d0, aFi, aFp, d3;
+    CellF<R> cm1 = staged<R>(A, slot, wl, lane, d0);
+    CellF<R> ci = staged<R>(A, slot, wl + 1, lane, aFi);
+    CellF<R> cp1 = staged<R>(A, slot, wl + 2, lane, aFp);
+    CellF<R> cp2 = staged<R>(A, slot, wl + 3, lane, d3);
     R iv[5];
 #pragma unroll
     for (int t = 0; t < 5; t++) iv[t] = R(__ldg(a.rint + 5 * f + t));
-    R aFi = alpha_F<S, R>(a, f - 1 > 0 ? f - 1 : 0, j, k);
-    R aFp = alpha_F<S, R>(a, f < a.nr - 1 ? f : a.nr - 1, j, k);
-    Recon<R> q = reconstruct<R>(cm1, ci, cp1, cp2, iv, aFi, aFp, jeps);
+    Recon<R> q = reconstruct_f<R>(cm1, ci, cp1, cp2, iv, aFi, aFp, jeps);
     R DrrL, DZZL, DrZL, DrrR, DZZR, DrZR;
     D_from_f_n<R>(q.f_L, q.nr_L, q.nZ_L, DrrL, DZZL, DrZL);
     D_from_f_n<R>(q.f_R, q.nr_R, q.nZ_R, DrrR, DZZR, DrZR);
@@ -126,19 +173,19 @@ __device__ __forceinline__ void face_r(const AdvArgs<S> &a, int f, int j, int k,
     kR = (f == 0) ? k_phiphi_axis<R>(q.J_R, q.HZ_R, jeps) : clamp01(R(1) - DrrR - DZZR) * q.J_R;
 }
 
-// One Z interface f (between cells f-1 and f) in column i (src/AdvectJandH.jl:978-1289).
+// Z face f (between rows f-1 and f) of column i, staged column lc (src/AdvectJandH.jl:978-1289).
 template <typename S, typename R, int FLUX>
-__device__ __forceinline__ void face_z(const AdvArgs<S> &a, int i, int f, int k, R jeps, R *F) {
-    Cell<R> cm1 = z_cell<S, R>(a, i, f - 2, k);
-    Cell<R> ci = z_cell<S, R>(a, i, f - 1, k);
-    Cell<R> cp1 = z_cell<S, R>(a, i, f, k);
-    Cell<R> cp2 = z_cell<S, R>(a, i, f + 1, k);
+__device__ __forceinline__ void face_z_staged(const AdvArgs<S> &a, const R *A, int lc, int i, int f, int lane,
+                                              R jeps, R *F) {
+    R d0, aFi, aFp, d3;
+    CellF<R> cm1 = staged<R>(A, (f + 2) & (RING - 1), lc, lane, d0);     // row f-2
+    CellF<R> ci = staged<R>(A, (f + 3) & (RING - 1), lc, lane, aFi);     // row f-1
+    CellF<R> cp1 = staged<R>(A, f & (RING - 1), lc, lane, aFp);          // row f
+    CellF<R> cp2 = staged<R>(A, (f + 1) & (RING - 1), lc, lane, d3);     // row f+1
     R iv[5];
 #pragma unroll
     for (int t = 0; t < 5; t++) iv[t] = R(__ldg(a.zint + 5 * f + t));
-    R aFi = alpha_F<S, R>(a, i, f - 1 > 0 ? f - 1 : 0, k);
-    R aFp = alpha_F<S, R>(a, i, f < a.nz - 1 ? f : a.nz - 1, k);
-    Recon<R> q = reconstruct<R>(cm1, ci, cp1, cp2, iv, aFi, aFp, jeps);
+    Recon<R> q = reconstruct_f<R>(cm1, ci, cp1, cp2, iv, aFi, aFp, jeps);
     R DrrL, DZZL, DrZL, DrrR, DZZR, DrZR;
     D_from_f_n<R>(q.f_L, q.nr_L, q.nZ_L, DrrL, DZZL, DrZL);
     D_from_f_n<R>(q.f_R, q.nr_R, q.nZ_R, DrrR, DZZR, DrZR);
@@ -152,115 +199,133 @@ __device__ __forceinline__ void face_z(const AdvArgs<S> &a, int i, int f, int k,
 }
 
 template <typename S, typename R, int FLUX>
-__global__ void __launch_bounds__(ADV_THREADS, 2) k_advect(AdvArgs<S> a) {
+__global__ void __launch_bounds__(MTHREADS, 2) k_advect(AdvArgs<S> a) {
     extern __shared__ __align__(16) unsigned char adv_smem[];
-    R *sFr = reinterpret_cast<R *>(adv_smem);        // [TJ][TI+1][3][32]
-    R *sKr = sFr + TJ * (TI + 1) * 3 * 32;            // [TJ][TI+1][2][32]
-    R *sFz = sKr + TJ * (TI + 1) * 2 * 32;            // [TJ+1][TI][3][32]
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nwarps = ADV_THREADS / 32;
-    const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ, kb = blockIdx.z * 32;
+    R *A = reinterpret_cast<R *>(adv_smem);              // [RING][MCOL][4][32]
+    R *Hh = A + RING * MCOL * 4 * 32;                     // [RING][MT][2][32]
+    R *Fr = Hh + RING * MT * 2 * 32;                      // [MT+1][5][32]
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int i0 = blockIdx.x * MT, j0 = blockIdx.y * MROWS, kb = blockIdx.z * 32;
+    const int j1 = (j0 + MROWS < a.nz) ? j0 + MROWS : a.nz;
     const int k = kb + lane;
     const int kmin = a.kwin[0], kmax = a.kwin[1];
     const bool kact = (k >= kmin) && (k <= kmax) && (k < a.nnu);
     const bool chunk_act = (kb <= kmax) && (kb + 31 >= kmin);
     const R jeps = R(a.jeps);
+    const int col = i0 + w;                      // own column (warps 0..7)
+    const bool own = (w < MT);
 
-    if (chunk_act) {
-        const int nRF = (TI + 1) * TJ, nZF = TI * (TJ + 1);
-        for (int t = warp; t < nRF + nZF; t += nwarps) {
-            if (t < nRF) {
-                int fl = t % (TI + 1), jl = t / (TI + 1);
-                int f = i0 + fl, j = j0 + jl;
-                if (kact && f <= a.nr && j < a.nz) {
-                    R F[3], kL, kR;
-                    face_r<S, R, FLUX>(a, f, j, k, jeps, F, kL, kR);
-                    R *p = sFr + ((jl * (TI + 1) + fl) * 3) * 32 + lane;
-                    p[0] = F[0]; p[32] = F[1]; p[64] = F[2];
-                    R *q = sKr + ((jl * (TI + 1) + fl) * 2) * 32 + lane;
-                    q[0] = kL; q[32] = kR;
-                }
-            } else {
-                int u = t - nRF;
-                int il = u % TI, fl = u / TI;
-                int i = i0 + il, f = j0 + fl;
-                if (kact && i < a.nr && f <= a.nz) {
-                    R F[3];
-                    face_z<S, R, FLUX>(a, i, f, k, jeps, F);
-                    R *p = sFz + ((fl * TI + il) * 3) * 32 + lane;
-                    p[0] = F[0]; p[32] = F[1]; p[64] = F[2];
-                }
+    if (!chunk_act) {
+        if (own && col < a.nr && k < a.nnu) {
+            for (int j = j0; j < j1; j++) {
+                size_t x = (size_t)k + (size_t)a.nnu * ((size_t)col + (size_t)a.nr * j);
+                a.Jo[x] = a.J[x]; a.Hro[x] = a.Hr[x]; a.HZo[x] = a.HZ[x];
             }
+        }
+        return;
+    }
+
+    // prologue: own columns, rows j0-2 .. j0+1
+    if (own && kact && col <= a.nr + 1) {
+        for (int r = j0 - 2; r <= j0 + 1; r++) {
+            bool gcol = col >= a.nr, grow = (r < 0 || r >= a.nz);
+            if (r < -2 || r > a.nz + 1 || (gcol && grow)) continue;
+            stage_cell<S, R>(a, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps);
         }
     }
     __syncthreads();
+    R zL[3] = {R(0), R(0), R(0)};
+    if (own && kact && col < a.nr) face_z_staged<S, R, FLUX>(a, A, w + 2, col, j0, lane, jeps, zL);
 
     const double ctdt = a.ctdt;
     const double ctdt_c = ctdt * kInvC;
-    for (int t = warp; t < TI * TJ; t += nwarps) {
-        int il = t % TI, jl = t / TI;
-        int i = i0 + il, j = j0 + jl;
-        if (i >= a.nr || j >= a.nz || k >= a.nnu) continue;
-        size_t c = (size_t)i + (size_t)a.nr * (size_t)j;
-        size_t x = (size_t)k + (size_t)a.nnu * c;
-        if (!kact) {
-            a.Jo[x] = a.J[x];
-            a.Hro[x] = a.Hr[x];
-            a.HZo[x] = a.HZ[x];
-            continue;
+    for (int j = j0; j < j1; j++) {
+        // (A) stage row j+2 of the own column; warp 8 stages the halo columns of row j
+        if (kact) {
+            if (own) {
+                int r = j + 2;
+                bool gcol = col >= a.nr, grow = r >= a.nz;
+                if (col <= a.nr + 1 && r <= a.nz + 1 && !(gcol && grow))
+                    stage_cell<S, R>(a, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps);
+            } else {
+                const int hl[4] = {0, 1, MT + 2, MT + 3};
+#pragma unroll
+                for (int t = 0; t < 4; t++) {
+                    int c2 = i0 - 2 + hl[t];
+                    if (c2 <= a.nr + 1) stage_cell<S, R>(a, A, Hh, j & (RING - 1), hl[t], c2, j, k, lane, jeps);
+                }
+            }
         }
-        Cell<R> s = ld_cell<S, R>(a, i, j, k);
-        R Drr, DZZ, DrZ;
-        D_edd<R>(s.Hr, s.HZ, s.J, jeps, R(a.heps2), Drr, DZZ, DrZ);
-        const R *FrL = sFr + ((jl * (TI + 1) + il) * 3) * 32 + lane;
-        const R *FrR = FrL + 3 * 32;
-        const R *FzL = sFz + ((jl * TI + il) * 3) * 32 + lane;
-        const R *FzR = FzL + TI * 3 * 32;
-        const R *KL = sKr + ((jl * (TI + 1) + il) * 2) * 32 + lane;
-        R kimh = KL[32];          // right side of face i   (K_phiphi at i-1/2)
-        R kiph = KL[2 * 32];      // left side of face i+1  (K_phiphi at i+1/2)
-        double ArL = __ldg(a.A_r + i + (size_t)(a.nr + 1) * j), ArR = __ldg(a.A_r + i + 1 + (size_t)(a.nr + 1) * j);
-        double AZL = __ldg(a.A_Z + c), AZR = __ldg(a.A_Z + c + a.nr);
-        double fac = ctdt * __ldg(a.inv_dV + c);
-        R Jn, Hrn, HZn;
-        if (sizeof(R) == 8) {
-            // UpdateConservativeQuantity in the reference's operation order
-            R f = R(fac);
-            Jn = s.J - f * ((R(ArR) * FrR[0] - R(ArL) * FrL[0]) + (R(AZR) * FzR[0] - R(AZL) * FzL[0]));
-            HZn = s.HZ - f * ((R(ArR) * FrR[64] - R(ArL) * FrL[64]) + (R(AZR) * FzR[64] - R(AZL) * FzL[64]));
-            Hrn = s.Hr - f * ((R(ArR) * FrR[32] - R(ArL) * FrL[32]) + (R(AZR) * FzR[32] - R(AZL) * FzL[32]));
-        } else {
-            // FP32: fold c~dt/dV into the areas in FP64 first (dimensionless weights)
-            R wrL = R(fac * ArL), wrR = R(fac * ArR), wzL = R(fac * AZL), wzR = R(fac * AZR);
-            Jn = s.J - ((wrR * FrR[0] - wrL * FrL[0]) + (wzR * FzR[0] - wzL * FzL[0]));
-            HZn = s.HZ - ((wrR * FrR[64] - wrL * FrL[64]) + (wzR * FzR[64] - wzL * FzL[64]));
-            Hrn = s.Hr - ((wrR * FrR[32] - wrL * FrL[32]) + (wzR * FzR[32] - wzL * FzL[32]));
+        __syncthreads();
+        // (B) the r face left of the own column (warp 8: the tile's right face), the Z face j+1/2
+        const int f = i0 + w;
+        R zR[3] = {R(0), R(0), R(0)};
+        if (kact && f <= a.nr) {
+            R F[3], kL, kR;
+            face_r_staged<S, R, FLUX>(a, A, j & (RING - 1), w, f, j, lane, jeps, F, kL, kR);
+            R *p = Fr + (w * 5) * 32 + lane;
+            p[0] = F[0]; p[32] = F[1]; p[64] = F[2]; p[96] = kL; p[128] = kR;
         }
-        Jn = Jn > jeps ? Jn : jeps;
-        R ga = R(__ldg(a.dur_dr + c)), gb = R(__ldg(a.dur_dZ + c)), gc = R(__ldg(a.duZ_dr + c));
-        R gd = R(__ldg(a.duZ_dZ + c)), ge = R(__ldg(a.ur_over_r + c));
-        R DdU = d_colon_grad_u<R>(Drr, DrZ, DZZ, ga, gb, gc, gd, ge);
-        R Kav = R(0.5) * (kimh + kiph);
-        if (sizeof(R) == 8)
-            Hrn += R(ctdt) * Kav * R(__ldg(a.inv_r_cell + i));
-        else
-            Hrn += R(ctdt * __ldg(a.inv_r_cell + i)) * Kav;
-        R cc = R(ctdt_c);
-        R dHr = -cc * (s.Hr * ga + s.HZ * gb);
-        R dHZ = -cc * (s.Hr * gc + s.HZ * gd);
-        Hrn = Hrn + dHr;
-        HZn = HZn + dHZ;
-        Jn = Jn - cc * DdU * s.J;
-        Jn = Jn > jeps ? Jn : jeps;
-        R H2 = Hrn * Hrn + HZn * HZn;
-        if (H2 > Jn * Jn) {
-            R fsc = Jn / rsq(H2);
-            Hrn *= fsc;
-            HZn *= fsc;
+        if (own && kact && col < a.nr) face_z_staged<S, R, FLUX>(a, A, w + 2, col, j + 1, lane, jeps, zR);
+        __syncthreads();
+        // (C) cell update, src/AdvectJandH.jl:1302-1382
+        if (own && col < a.nr && k < a.nnu) {
+            const int i = col;
+            size_t c = (size_t)i + (size_t)a.nr * (size_t)j;
+            size_t x = (size_t)k + (size_t)a.nnu * c;
+            if (!kact) {
+                a.Jo[x] = a.J[x]; a.Hro[x] = a.Hr[x]; a.HZo[x] = a.HZ[x];
+            } else {
+                const R *pA = A + (((j & (RING - 1)) * MCOL + w + 2) * 4) * 32 + lane;
+                const R *pH = Hh + (((j & (RING - 1)) * MT + w) * 2) * 32 + lane;
+                R sJ = pA[0], sHr = pH[0], sHZ = pH[32];
+                R Drr, DZZ, DrZ;
+                D_edd<R>(sHr, sHZ, sJ, jeps, R(a.heps2), Drr, DZZ, DrZ);
+                const R *FL = Fr + (w * 5) * 32 + lane;
+                const R *FR = FL + 5 * 32;
+                double ArL = __ldg(a.A_r + i + (size_t)(a.nr + 1) * j), ArR = __ldg(a.A_r + i + 1 + (size_t)(a.nr + 1) * j);
+                double AZL = __ldg(a.A_Z + c), AZR = __ldg(a.A_Z + c + a.nr);
+                double fac = ctdt * __ldg(a.inv_dV + c);
+                R Jn, Hrn, HZn;
+                if (sizeof(R) == 8) {
+                    R fr_ = R(fac);
+                    Jn = sJ - fr_ * ((R(ArR) * FR[0] - R(ArL) * FL[0]) + (R(AZR) * zR[0] - R(AZL) * zL[0]));
+                    HZn = sHZ - fr_ * ((R(ArR) * FR[64] - R(ArL) * FL[64]) + (R(AZR) * zR[2] - R(AZL) * zL[2]));
+                    Hrn = sHr - fr_ * ((R(ArR) * FR[32] - R(ArL) * FL[32]) + (R(AZR) * zR[1] - R(AZL) * zL[1]));
+                } else {
+                    R wrL = R(fac * ArL), wrR = R(fac * ArR), wzL = R(fac * AZL), wzR = R(fac * AZR);
+                    Jn = sJ - ((wrR * FR[0] - wrL * FL[0]) + (wzR * zR[0] - wzL * zL[0]));
+                    HZn = sHZ - ((wrR * FR[64] - wrL * FL[64]) + (wzR * zR[2] - wzL * zL[2]));
+                    Hrn = sHr - ((wrR * FR[32] - wrL * FL[32]) + (wzR * zR[1] - wzL * zL[1]));
+                }
+                Jn = Jn > jeps ? Jn : jeps;
+                R ga = R(__ldg(a.dur_dr + c)), gb = R(__ldg(a.dur_dZ + c)), gc = R(__ldg(a.duZ_dr + c));
+                R gd = R(__ldg(a.duZ_dZ + c)), ge = R(__ldg(a.ur_over_r + c));
+                R DdU = d_colon_grad_u<R>(Drr, DrZ, DZZ, ga, gb, gc, gd, ge);
+                R Kav = R(0.5) * (FL[128] + FR[96]);
+                if (sizeof(R) == 8)
+                    Hrn += R(ctdt) * Kav * R(__ldg(a.inv_r_cell + i));
+                else
+                    Hrn += R(ctdt * __ldg(a.inv_r_cell + i)) * Kav;
+                R cc = R(ctdt_c);
+                R dHr = -cc * (sHr * ga + sHZ * gb);
+                R dHZ = -cc * (sHr * gc + sHZ * gd);
+                Hrn = Hrn + dHr;
+                HZn = HZn + dHZ;
+                Jn = Jn - cc * DdU * sJ;
+                Jn = Jn > jeps ? Jn : jeps;
+                R H2 = Hrn * Hrn + HZn * HZn;
+                if (H2 > Jn * Jn) {
+                    R fsc = Jn / rsq(H2);
+                    Hrn *= fsc;
+                    HZn *= fsc;
+                }
+                a.Jo[x] = S(Jn);
+                a.Hro[x] = S(Hrn);
+                a.HZo[x] = S(HZn);
+            }
         }
-        a.Jo[x] = S(Jn);
-        a.Hro[x] = S(Hrn);
-        a.HZo[x] = S(HZn);
+        zL[0] = zR[0]; zL[1] = zR[1]; zL[2] = zR[2];
     }
 }
 
@@ -417,9 +482,9 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
                 R dJdt = js_ct * phi;
                 R Jn = (R(Jo[m]) + dJdt * dtr) / (R(1) + aabs * ct * dtr);
                 R aH = a.aF ? R(__ldg(a.aF + base + k)) : (a.alpha_cF ? al * Hv[m] + acF : al * Hv[m]);
-                R den = R(1) + aH * ct * dtr;
-                R hr = (Hr[m] + R(0) * dtr) / den;
-                R hz = (HZ[m] + R(0) * dtr) / den;
+                R iden = R(1) / (R(1) + aH * ct * dtr);
+                R hr = Hr[m] * iden;
+                R hz = HZ[m] * iden;
                 double dn = kc[KC_DNU * NP + k];
                 dr_sum += dn * (double(Hr[m]) - double(hr));
                 dz_sum += dn * (double(HZ[m]) - double(hz));
@@ -449,20 +514,31 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
                 const double rec0 = kHOverKB / T;
                 const R ga = R(__ldg(a.dur_dr + c)), gb = R(__ldg(a.dur_dZ + c)), gc = R(__ldg(a.duZ_dr + c));
                 const R gd = R(__ldg(a.duZ_dZ + c)), ge = R(__ldg(a.ur_over_r + c));
-                // neighbours H_voigt[k-1], H_voigt[k+1]
-                double hv_up = __shfl_up_sync(0xffffffffu, double(Hv[M - 1]), 1);
-                double hv_dn = __shfl_down_sync(0xffffffffu, double(Hv[0]), 1);
+                // K_k = pref H_voigt[k] and 1/K_k once per bin; the k+-1 neighbours come by
+                // shuffle (the same products the reference forms at k-1 and k+1)
+                double Kb[M], iK[M];
+#pragma unroll
+                for (int m = 0; m < M; m++) {
+                    Kb[m] = pref * double(Hv[m]);
+                    iK[m] = 1.0 / Kb[m];
+                }
+                double K_up = __shfl_up_sync(0xffffffffu, Kb[M - 1], 1);
+                double K_dn = __shfl_down_sync(0xffffffffu, Kb[0], 1);
+                double iK_up = __shfl_up_sync(0xffffffffu, iK[M - 1], 1);
+                double iK_dn = __shfl_down_sync(0xffffffffu, iK[0], 1);
 #pragma unroll
                 for (int m = 0; m < M; m++) {
                     int k = lane * M + m;
                     Fp[m] = 0.0; F0[m] = 0.0; Fm[m] = 0.0;
                     if (k < 1 || k > nnu - 2) continue;
-                    double hkm = (m > 0) ? double(Hv[m - 1]) : hv_up;
-                    double hkp = (m < M - 1) ? double(Hv[m + 1]) : hv_dn;
                     R Drr, DZZ, DrZ;
                     D_edd<R>(Hr[m], HZ[m], J[m], R(jeps), R(a.heps2), Drr, DZZ, DrZ);
                     double vel = double(d_colon_grad_u<R>(Drr, DrZ, DZZ, ga, gb, gc, gd, ge)) * kInvC;
-                    double Kkp = pref * hkp, Kk = pref * double(Hv[m]), Kkm = pref * hkm;
+                    double Kk = Kb[m];
+                    double Kkm = (m > 0) ? Kb[m - 1] : K_up;
+                    double Kkp = (m < M - 1) ? Kb[m + 1] : K_dn;
+                    double iKkm = (m > 0) ? iK[m - 1] : iK_up;
+                    double iKkp = (m < M - 1) ? iK[m + 1] : iK_dn;
                     double nCk = kc[KC_NCK * NP + k], nCkp = kc[KC_NCKP * NP + k], nCkm = kc[KC_NCKM * NP + k];
                     double Ckp = vel * nCkp, Ck = vel * nCk, Ckm = vel * nCkm;
                     if (a.recoil) {
@@ -470,16 +546,15 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
                         Ck += Kk * (rec0 - 2.0 * kc[KC_ICK * NP + k]);
                         Ckm += Kkm * (rec0 - 2.0 * kc[KC_ICKM * NP + k]);
                     }
-                    double rkp = kc[KC_DNKP * NP + k] * (1.0 / Kkp);
-                    double rk = kc[KC_DNK * NP + k] * (1.0 / Kk);
-                    double rkm = kc[KC_DNKM * NP + k] * (1.0 / Kkm);
+                    double rkp = kc[KC_DNKP * NP + k] * iKkp;
+                    double rk = kc[KC_DNK * NP + k] * iK[m];
+                    double rkm = kc[KC_DNKM * NP + k] * iKkm;
                     double Pkp = fmin(fmax(Ckp * rkp, -kPmax), kPmax);
                     double Pk = fmin(fmax(Ck * rk, -kPmax), kPmax);
                     double Pkm = fmin(fmax(Ckm * rkm, -kPmax), kPmax);
                     double oRkp, xRkp, oLk, xLk, oRk, xRk, oLkm, xLkm;
                     omphi_R(Pkp, oRkp, xRkp);
-                    omphi_L(Pk, oLk, xLk);
-                    omphi_R(Pk, oRk, xRk);
+                    omphi_LR(Pk, oLk, xLk, oRk, xRk);
                     omphi_L(Pkm, oLkm, xLkm);
                     double idn = kc[KC_IDNU * NP + k];
                     double dkp = idn * (1.0 / (xLk * rk - xRkp * rkp));
@@ -726,7 +801,7 @@ __global__ void __launch_bounds__(1024) k_reduce(RedArgs a) {
 // ---- launch wrappers ----------------------------------------------------------------------
 static size_t adv_smem_bytes(int prec) {
     size_t per = (prec == 0) ? sizeof(double) : sizeof(float);
-    return per * 32 * (TJ * (TI + 1) * 3 + TJ * (TI + 1) * 2 + (TJ + 1) * TI * 3);
+    return per * 32 * (RING * MCOL * 4 + RING * MT * 2 + (MT + 1) * 5);
 }
 
 template <typename S, typename R, int FLUX>
@@ -737,8 +812,8 @@ static void adv_launch(const void *args, int nnu, int nr, int nz, cudaStream_t s
         cudaFuncSetAttribute(k_advect<S, R, FLUX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         attr = true;
     }
-    dim3 grid((nr + TI - 1) / TI, (nz + TJ - 1) / TJ, (nnu + 31) / 32);
-    k_advect<S, R, FLUX><<<grid, ADV_THREADS, sm, st>>>(*static_cast<const AdvArgs<S> *>(args));
+    dim3 grid((nr + MT - 1) / MT, (nz + MROWS - 1) / MROWS, (nnu + 31) / 32);
+    k_advect<S, R, FLUX><<<grid, MTHREADS, sm, st>>>(*static_cast<const AdvArgs<S> *>(args));
 }
 
 void launch_advect(int prec, int flux, const void *args, int nnu, int nr, int nz, cudaStream_t st) {

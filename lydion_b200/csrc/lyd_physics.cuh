@@ -133,38 +133,44 @@ template <typename R> struct Recon {
     R J_L, J_R, Hr_L, Hr_R, HZ_L, HZ_R, tau_L, tau_R, f_L, f_R, nr_L, nr_R, nZ_L, nZ_R;
 };
 
-// ReconstructInterface, src/AdvectJandH.jl:359-473. Cells: im1, i, ip1, ip2 around the
-// interface between i and ip1; iv = {dL, dR, inv_i_im1, inv_ip1_i, inv_ip2_ip1}.
+// A stencil cell in the form ReconstructInterface works on: J and the reduced flux
+// f = H / max(J, Jeps) (src/AdvectJandH.jl:373-386). Computing it once per cell lets every
+// face that uses the cell share one reciprocal.
+template <typename R> struct CellF { R J, fr, fZ; };
+
 template <typename R>
-__device__ __forceinline__ Recon<R> reconstruct(const Cell<R> &cm1, const Cell<R> &ci, const Cell<R> &cp1,
-                                                const Cell<R> &cp2, const R iv[5], R aF_i, R aF_ip1, R jeps) {
+__device__ __forceinline__ CellF<R> cell_f(R J, R Hr, R HZ, R jeps) {
+    R iJ = R(1) / (J > jeps ? J : jeps);
+    CellF<R> c;
+    c.J = J; c.fr = Hr * iJ; c.fZ = HZ * iJ;
+    return c;
+}
+
+// ReconstructInterface, src/AdvectJandH.jl:359-473, on prepared cells im1, i, ip1, ip2
+// around the interface between i and ip1; iv = {dL, dR, inv_i_im1, inv_ip1_i, inv_ip2_ip1}.
+template <typename R>
+__device__ __forceinline__ Recon<R> reconstruct_f(const CellF<R> &cm1, const CellF<R> &ci, const CellF<R> &cp1,
+                                                  const CellF<R> &cp2, const R iv[5], R aF_i, R aF_ip1, R jeps) {
     Recon<R> o;
     const R dL = iv[0], dR = iv[1];
     o.tau_L = aF_i * dL;
     o.tau_R = aF_ip1 * dR;
-    R iJ_i = R(1) / (ci.J > jeps ? ci.J : jeps);
-    R iJ_p1 = R(1) / (cp1.J > jeps ? cp1.J : jeps);
-    R iJ_p2 = R(1) / (cp2.J > jeps ? cp2.J : jeps);
-    R iJ_m1 = R(1) / (cm1.J > jeps ? cm1.J : jeps);
-    R fr_i = ci.Hr * iJ_i, fr_p1 = cp1.Hr * iJ_p1, fr_p2 = cp2.Hr * iJ_p2, fr_m1 = cm1.Hr * iJ_m1;
-    R fZ_i = ci.HZ * iJ_i, fZ_p1 = cp1.HZ * iJ_p1, fZ_p2 = cp2.HZ * iJ_p2, fZ_m1 = cm1.HZ * iJ_m1;
-
     R dJc = (cp1.J - ci.J) * iv[3];
     R dJL = minmod((ci.J - cm1.J) * iv[2], dJc);
     R dJR = minmod((cp2.J - cp1.J) * iv[4], dJc);
-    R dfrc = (fr_p1 - fr_i) * iv[3];
-    R dfrL = minmod((fr_i - fr_m1) * iv[2], dfrc);
-    R dfrR = minmod((fr_p2 - fr_p1) * iv[4], dfrc);
-    R dfZc = (fZ_p1 - fZ_i) * iv[3];
-    R dfZL = minmod((fZ_i - fZ_m1) * iv[2], dfZc);
-    R dfZR = minmod((fZ_p2 - fZ_p1) * iv[4], dfZc);
+    R dfrc = (cp1.fr - ci.fr) * iv[3];
+    R dfrL = minmod((ci.fr - cm1.fr) * iv[2], dfrc);
+    R dfrR = minmod((cp2.fr - cp1.fr) * iv[4], dfrc);
+    R dfZc = (cp1.fZ - ci.fZ) * iv[3];
+    R dfZL = minmod((ci.fZ - cm1.fZ) * iv[2], dfZc);
+    R dfZR = minmod((cp2.fZ - cp1.fZ) * iv[4], dfZc);
 
     R JL = ci.J + dJL * dL;
     R JR = cp1.J - dJR * dR;
     o.J_L = JL > jeps ? JL : jeps;
     o.J_R = JR > jeps ? JR : jeps;
-    R frL = fr_i + dfrL * dL, frR = fr_p1 - dfrR * dR;
-    R fZL = fZ_i + dfZL * dL, fZR = fZ_p1 - dfZR * dR;
+    R frL = ci.fr + dfrL * dL, frR = cp1.fr - dfrR * dR;
+    R fZL = ci.fZ + dfZL * dL, fZR = cp1.fZ - dfZR * dR;
 
     R fL = rsq(frL * frL + fZL * fZL);
     if (fL > R(1)) { R inv = R(1) / fL; frL *= inv; fZL *= inv; fL = R(1); }
@@ -179,6 +185,15 @@ __device__ __forceinline__ Recon<R> reconstruct(const Cell<R> &cm1, const Cell<R
     else { o.nr_R = R(0); o.nZ_R = R(0); }
     o.f_L = fL; o.f_R = fR;
     return o;
+}
+
+// ReconstructInterface from raw cells (J, H_r, H_Z).
+template <typename R>
+__device__ __forceinline__ Recon<R> reconstruct(const Cell<R> &cm1, const Cell<R> &ci, const Cell<R> &cp1,
+                                                const Cell<R> &cp2, const R iv[5], R aF_i, R aF_ip1, R jeps) {
+    return reconstruct_f<R>(cell_f<R>(cm1.J, cm1.Hr, cm1.HZ, jeps), cell_f<R>(ci.J, ci.Hr, ci.HZ, jeps),
+                            cell_f<R>(cp1.J, cp1.Hr, cp1.HZ, jeps), cell_f<R>(cp2.J, cp2.Hr, cp2.HZ, jeps), iv,
+                            aF_i, aF_ip1, jeps);
 }
 
 // GetFluxGLF / GetFluxHLL, src/AdvectJandH.jl:81-118, 155-204, with the wave speeds of
@@ -263,6 +278,22 @@ __device__ __forceinline__ void omphi_R(double P, double &omp, double &chi) {
     if (fabs(P) < kPmin) { omp = 1.0 + P + 0.5 * (P * P); chi = -1.0 - 0.5 * P; return; }
     omp = exp(P);
     chi = (1.0 - omp) / P;
+}
+// Both of the above at once for the same P (used for P_k, which needs phi^L and phi^R):
+// one exponential and one reciprocal of P serve the two branches.
+__device__ __forceinline__ void omphi_LR(double P, double &oL, double &xL, double &oR, double &xR) {
+    if (P >= kPmax || P <= -kPmax || fabs(P) < kPmin) {
+        omphi_L(P, oL, xL);
+        omphi_R(P, oR, xR);
+        return;
+    }
+    double e = exp(-P);
+    double ie = 1.0 / e;
+    double iP = 1.0 / P;
+    oL = e;
+    xL = (1.0 - e) * iP;
+    oR = ie;
+    xR = (1.0 - ie) * iP;
 }
 // FP32 variants for the mixed step (same branches, float arithmetic)
 __device__ __forceinline__ void omphi_L(float P, float &omp, float &chi) {
