@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define LYD_ABI_VERSION 1
+#define LYD_ABI_VERSION 2
 
 /* status codes */
 #define LYD_OK              0
@@ -174,6 +174,48 @@ int  lyd_static_steps(lyd_ctx *ctx, const lyd_step_params *p, lyd_diag *diag_his
  * ms[0] = advection kernel, ms[1] = frequency kernel, ms[2] = reductions (totals). */
 int  lyd_set_timing(lyd_ctx *ctx, int32_t enable);
 int  lyd_get_timing(lyd_ctx *ctx, double ms[3]);
+
+/* ---- batches of independent clouds ------------------------------------------------------ */
+/* A context may hold many independent clouds of different (n_r, n_z) sharing one frequency
+ * grid and one configuration: the batched form of the static-cloud run (512 clouds of
+ * uneven size advancing together). Every step kernel covers all clouds in one launch (a work
+ * list of per-cloud tiles), each cloud with its own time step and boundary conditions, and
+ * the step is replayed from one CUDA graph. lyd_create is a batch of one cloud.
+ *
+ * On a context of several clouds: lyd_upload / lyd_download move every cloud's values,
+ * concatenated cloud after cloud; lyd_find_active_bins writes n_clouds entries to each of
+ * kmin and kmax; lyd_static_steps runs every cloud with the same parameters and writes
+ * n_steps * n_clouds records; the step phases (lyd_advect ... lyd_update_J_and_H) apply one
+ * c_tilde, dt and boundary set to all clouds; lyd_set_geometry, lyd_force_multiplier,
+ * lyd_f_esc, lyd_cfl_dt and lyd_edge_spectra return LYD_ERR_STATE (use the per-cloud forms
+ * and the lyd_batch_steps records). An explicitly uploaded phi_nu or alpha_F must be
+ * uploaded for every cloud. */
+int  lyd_batch_create(lyd_ctx **out, int32_t n_clouds, const int32_t *n_r, const int32_t *n_z, int32_t n_nu,
+                      const lyd_config *cfg);
+int  lyd_batch_info(lyd_ctx *ctx, int32_t *n_clouds, int64_t *cell_bins);
+int  lyd_set_geometry_cloud(lyd_ctx *ctx, int32_t cloud, const lyd_geometry *g);
+int  lyd_upload_cloud(lyd_ctx *ctx, int32_t cloud, int32_t field, const double *host, size_t count);
+int  lyd_download_cloud(lyd_ctx *ctx, int32_t cloud, int32_t field, double *host, size_t count);
+int  lyd_edge_spectra_cloud(lyd_ctx *ctx, int32_t cloud, double *raw, double *norm, int32_t *r_index,
+                            int32_t *z_index);
+
+typedef struct lyd_cloud_params {
+    double c_tilde, dt, z_center;
+    int32_t bc_r_right, bc_z_bot, bc_z_top, reserved;
+} lyd_cloud_params;
+/* n_steps static-driver iterations of every cloud, cloud q with params[q]; hist (may be NULL)
+ * receives n_steps * n_clouds records, step-major. */
+int  lyd_batch_steps(lyd_ctx *ctx, const lyd_cloud_params *params, int32_t n_steps, lyd_diag *hist);
+
+/* Launch-shape knobs chosen by the autotuner (lydion_b200/autotune.py): rows of the
+ * advection tile (4..64), cells per frequency-kernel block (8..1024, or 0 for automatic), and
+ * the frequency solver (0: parallel cyclic reduction across the warp; 1: lane-serial
+ * elimination). */
+typedef struct lyd_tuning {
+    int32_t rows_per_tile, cells_per_block, solver, reserved;
+} lyd_tuning;
+int  lyd_set_tuning(lyd_ctx *ctx, const lyd_tuning *t);
+int  lyd_get_tuning(lyd_ctx *ctx, lyd_tuning *t);
 
 /* ---- set-up and output helpers --------------------------------------------------------- */
 /* Update_Hvoigt! from the uploaded temperature, src/ConstantsAndFunctions.jl:319-357, using

@@ -59,6 +59,18 @@ class Diag(C.Structure):
                 ("L_tot", C.c_double), ("f_esc", C.c_double), ("kmin", C.c_int32), ("kmax", C.c_int32)]
 
 
+class CloudParams(C.Structure):
+    _fields_ = [("c_tilde", C.c_double), ("dt", C.c_double), ("z_center", C.c_double), ("bc_r_right", C.c_int32),
+                ("bc_z_bot", C.c_int32), ("bc_z_top", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("rows_per_tile", C.c_int32), ("cells_per_block", C.c_int32), ("solver", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+SOLVER_PCR, SOLVER_THOMAS = 0, 1
+
 # name -> (restype, argtypes); this list is the ABI surface checked by the CPU tests
 I32, D, SZ, VP = C.c_int32, C.c_double, C.c_size_t, C.c_void_p
 SIGNATURES = {
@@ -83,6 +95,15 @@ SIGNATURES = {
     "lyd_static_steps": (C.c_int, [VP, C.POINTER(StepParams), C.POINTER(Diag)]),
     "lyd_set_timing": (C.c_int, [VP, I32]),
     "lyd_get_timing": (C.c_int, [VP, P]),
+    "lyd_batch_create": (C.c_int, [C.POINTER(VP), I32, C.POINTER(I32), C.POINTER(I32), I32, C.POINTER(Config)]),
+    "lyd_batch_info": (C.c_int, [VP, C.POINTER(I32), C.POINTER(C.c_int64)]),
+    "lyd_set_geometry_cloud": (C.c_int, [VP, I32, C.POINTER(Geometry)]),
+    "lyd_upload_cloud": (C.c_int, [VP, I32, I32, P, SZ]),
+    "lyd_download_cloud": (C.c_int, [VP, I32, I32, P, SZ]),
+    "lyd_edge_spectra_cloud": (C.c_int, [VP, I32, P, P, C.POINTER(I32), C.POINTER(I32)]),
+    "lyd_batch_steps": (C.c_int, [VP, C.POINTER(CloudParams), I32, C.POINTER(Diag)]),
+    "lyd_set_tuning": (C.c_int, [VP, C.POINTER(Tuning)]),
+    "lyd_get_tuning": (C.c_int, [VP, C.POINTER(Tuning)]),
     "lyd_update_hvoigt": (C.c_int, [VP]),
     "lyd_update_phi_nu": (C.c_int, [VP, I32, I32]),
     "lyd_pd_lya": (C.c_int, [VP, SZ, P, P, P, P, P, P, D, P]),

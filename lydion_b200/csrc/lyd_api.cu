@@ -1,6 +1,12 @@
 // lyd_api.cu -- the C ABI (include/lydion_m1.h): context, device state, and the drop-in
 // entry points of the Lyman-alpha M1 step.
 //
+// A context holds a batch of independent clouds (one cloud for lyd_create). Every field of
+// every cloud lives in one concatenated device array per field, cloud after cloud; the
+// per-cloud offsets, sizes, boundary conditions and time step are CloudDesc records in
+// device memory that the kernels read, so changing a time step is a 100-byte copy and the
+// captured step graph stays valid.
+//
 // Device state. J, H_r, H_Z live in two buffer sets. `cur` holds the current values; the
 // other set holds J_old, H_r_old, H_Z_old unless `old_alias` is set, in which case the old
 // values equal the current ones (true after every step phase of the reference:
@@ -11,6 +17,7 @@
 // so a step starts and ends in the same set and one CUDA graph replays every step.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -25,13 +32,25 @@ using namespace lyd;
 namespace {
 constexpr int kLutN = 200001;        // src/FastInterpolations.jl:175-176
 constexpr double kLutXmax = 1000.0;
-}
+constexpr int kTileCols = 8;         // columns per advection tile (the kernel's MT)
+constexpr int kDefaultRows = 16;
+
+// per-cloud "was provided" bits: per-cell fields use their index (field - LYD_F_ALPHA)
+enum { CF_ALPHA = 0, CF_ALPHA_C, CF_ALPHA_CF, CF_PD, CF_JS, CF_T, CF_DUR_DR, CF_DUR_DZ, CF_DUZ_DR, CF_DUZ_DZ,
+       CF_UR_OVER_R, CF_DRU_R, CF_DRU_Z, CF_F_R, CF_F_Z, CF_N };
+enum : unsigned { BIT_HV = 1u << 16, BIT_PHI = 1u << 17, BIT_AF = 1u << 18, BIT_GEOM = 1u << 19 };
+}  // namespace
 
 struct lyd_ctx {
     int dev = 0;
     cudaStream_t st = nullptr;
-    int nnu = 0, nr = 0, nz = 0;
-    size_t ncell = 0, n3 = 0;
+    int nnu = 0, ncl = 0, sms = 148;
+    std::vector<int> nr, nz;
+    std::vector<CloudDesc> desc;       // host copy of the descriptors
+    std::vector<CloudDesc> desc_dev;   // what the device holds (to skip unchanged uploads)
+    CloudDesc *cl = nullptr;
+    std::vector<unsigned> have;        // per-cloud provided bits
+    size_t ncell = 0, n3 = 0, nrf = 0, nzf = 0, ncol = 0, nrow = 0, nrint = 0, nzint = 0, nrif = 0, nzif = 0;
     lyd_config cfg{};
     int prec = 0;
     size_t ssz = 8;
@@ -40,47 +59,42 @@ struct lyd_ctx {
     int cur = 0;
     bool old_alias = true;
     void *Hv = nullptr;
-    bool hv_set = false;
     void *phi = nullptr;
-    bool phi_explicit = false;
     double *phi_inv = nullptr;
     int phi_kmin = 0, phi_kmax = -1;
-    bool phi_ready = false;
+    bool phi_inv_ready = false;
     void *aF = nullptr;
-    bool aF_explicit = false;
     double *Ff[3] = {nullptr, nullptr, nullptr};
     bool ff_valid = false;
-    double *cellf[16] = {};        // per-cell fields, index = field - 16
-    bool cell_set[16] = {};
+    double *cellf[CF_N] = {};
     double *u_r_star = nullptr, *u_Z_star = nullptr;
     double *dV = nullptr, *inv_dV = nullptr, *A_r = nullptr, *A_Z = nullptr, *inv_r_cell = nullptr;
     double *rCoM = nullptr, *ZCoM = nullptr, *rint = nullptr, *zint = nullptr, *r_if = nullptr, *Z_if = nullptr;
-    bool geom_set = false;
     double *nu = nullptr, *nuC = nullptr, *dnu = nullptr, *inv_dnu = nullptr, *inv_nuC = nullptr;
     bool freq_set = false;
-    int fblocks = 0;
+    // work lists
+    lyd_tuning tune{kDefaultRows, 0, SOLVER_PCR, 0};
+    int4 *tiles = nullptr, *items = nullptr;
+    int ntiles = 0, nitems = 0;
     double *partials = nullptr;
     int *kwin = nullptr;
     bool active_valid = false;
     double *hist = nullptr;
-    int hist_cap = 0;
-    int *step_ctr = nullptr;
+    int hist_cap = 0;                  // steps
+    int *step_ctr = nullptr;           // [0] record index, [1] completion counter
     double *last = nullptr;
     int *err = nullptr;
     double *lut = nullptr;
-    double *stage = nullptr;       // device FP64 staging buffer (n3 doubles)
-    double *small = nullptr;       // device scratch (256 doubles)
+    double *stage = nullptr;           // device FP64 staging buffer
+    size_t stage_n = 0;
+    double *small = nullptr;           // device scratch (512 doubles)
     cudaGraphExec_t gexec = nullptr;
-    double gkey[3] = {0, 0, 0};
-    int gkey_i[4] = {-1, -1, -1, -1};
+    int gkey_cur = -1;
     bool timing = false;
     cudaEvent_t ev[8] = {};
     double ms[3] = {0, 0, 0};
     std::string msg;
 };
-
-enum { CF_ALPHA = 0, CF_ALPHA_C, CF_ALPHA_CF, CF_PD, CF_JS, CF_T, CF_DUR_DR, CF_DUR_DZ, CF_DUZ_DR, CF_DUZ_DZ,
-       CF_UR_OVER_R, CF_DRU_R, CF_DRU_Z, CF_F_R, CF_F_Z, CF_N };
 
 static int fail(lyd_ctx *c, int code, const std::string &m) {
     if (c) c->msg = m;
@@ -96,7 +110,10 @@ static int fail(lyd_ctx *c, int code, const std::string &m) {
 
 static int dalloc(lyd_ctx *c, void **p, size_t bytes) {
     cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
-    if (e != cudaSuccess) return fail(c, LYD_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(c, LYD_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
     e = cudaMemsetAsync(*p, 0, bytes ? bytes : 16, c->st);
     if (e != cudaSuccess) return fail(c, LYD_ERR_CUDA, cudaGetErrorString(e));
     return LYD_OK;
@@ -109,6 +126,21 @@ static int dalloc(lyd_ctx *c, void **p, size_t bytes) {
 
 static void *Jc(lyd_ctx *c, int q) { return c->set[c->cur][q]; }
 static void *Jold(lyd_ctx *c, int q) { return c->old_alias ? c->set[c->cur][q] : c->set[1 - c->cur][q]; }
+static char *at(void *p, size_t elems, size_t esz) { return static_cast<char *>(p) + elems * esz; }
+
+static bool all_have(const lyd_ctx *c, unsigned bit) {
+    for (unsigned h : c->have)
+        if (!(h & bit)) return false;
+    return true;
+}
+static bool any_have(const lyd_ctx *c, unsigned bit) {
+    for (unsigned h : c->have)
+        if (h & bit) return true;
+    return false;
+}
+static void set_all(lyd_ctx *c, unsigned bit) {
+    for (unsigned &h : c->have) h |= bit;
+}
 
 static int check_err(lyd_ctx *c) {
     int h = 0;
@@ -122,6 +154,77 @@ static int check_err(lyd_ctx *c) {
     return LYD_OK;
 }
 
+// Copy the host descriptors to the device when they changed. A pageable host-to-device
+// cudaMemcpyAsync returns once the source is staged, so the host copy may change right after.
+static int sync_desc(lyd_ctx *c) {
+    if (c->desc_dev.size() == c->desc.size() &&
+        memcmp(c->desc_dev.data(), c->desc.data(), c->desc.size() * sizeof(CloudDesc)) == 0)
+        return LYD_OK;
+    LYD_CU(c, cudaMemcpyAsync(c->cl, c->desc.data(), c->desc.size() * sizeof(CloudDesc), cudaMemcpyHostToDevice,
+                              c->st));
+    c->desc_dev = c->desc;
+    return LYD_OK;
+}
+
+static void drop_graph(lyd_ctx *c) {
+    if (c->gexec) {
+        cudaGraphExecDestroy(c->gexec);
+        c->gexec = nullptr;
+    }
+}
+
+// Work lists. Advection: tiles of 8 columns x rows x 32 bins, column tile fastest, per cloud.
+// Frequency kernel: runs of `cpb` consecutive cells of one cloud per block.
+static int cells_per_block(const lyd_ctx *c) {
+    if (c->tune.cells_per_block > 0) return c->tune.cells_per_block;
+    long long want = (long long)(c->ncell + 4 * c->sms - 1) / (4 * c->sms);
+    want = (want + 7) / 8 * 8;
+    return (int)std::min<long long>(1024, std::max<long long>(8, want));
+}
+
+static int build_work(lyd_ctx *c) {
+    const int rows = c->tune.rows_per_tile;
+    std::vector<int4> t, it;
+    const int nkb = (c->nnu + 31) / 32;
+    for (int q = 0; q < c->ncl; q++)
+        for (int kb = 0; kb < nkb; kb++)
+            for (int j0 = 0; j0 < c->nz[q]; j0 += rows)
+                for (int i0 = 0; i0 < c->nr[q]; i0 += kTileCols) t.push_back(make_int4(q, i0, j0, 32 * kb));
+    const int cpb = cells_per_block(c);
+    for (int q = 0; q < c->ncl; q++) {
+        const int nc = c->nr[q] * c->nz[q];
+        c->desc[q].pb0 = (int)it.size();
+        for (int b = 0; b < nc; b += cpb) it.push_back(make_int4(q, b, std::min(nc, b + cpb), 0));
+        c->desc[q].npb = (int)it.size() - c->desc[q].pb0;
+    }
+    cudaFree(c->tiles);
+    cudaFree(c->items);
+    cudaFree(c->partials);
+    c->tiles = c->items = nullptr;
+    c->partials = nullptr;
+    LYD_TRY(dalloc(c, (void **)&c->tiles, t.size() * sizeof(int4)));
+    LYD_TRY(dalloc(c, (void **)&c->items, it.size() * sizeof(int4)));
+    LYD_TRY(dalloc(c, (void **)&c->partials, it.size() * (size_t)(c->nnu + kExtraCols) * 8));
+    LYD_CU(c, cudaMemcpyAsync(c->tiles, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice, c->st));
+    LYD_CU(c, cudaMemcpyAsync(c->items, it.data(), it.size() * sizeof(int4), cudaMemcpyHostToDevice, c->st));
+    LYD_CU(c, cudaStreamSynchronize(c->st));
+    c->ntiles = (int)t.size();
+    c->nitems = (int)it.size();
+    drop_graph(c);
+    return sync_desc(c);
+}
+
+static int ensure_stage(lyd_ctx *c, size_t n) {
+    if (n <= c->stage_n) return LYD_OK;
+    LYD_CU(c, cudaStreamSynchronize(c->st));
+    cudaFree(c->stage);
+    c->stage = nullptr;
+    c->stage_n = 0;
+    LYD_TRY(dalloc(c, (void **)&c->stage, n * 8));
+    c->stage_n = n;
+    return LYD_OK;
+}
+
 // Every lyd_* definition below has C linkage through its declaration in lydion_m1.h.
 
 int lyd_abi_version(void) { return LYD_ABI_VERSION; }
@@ -130,21 +233,49 @@ const char *lyd_last_error(const lyd_ctx *c) { return c ? c->msg.c_str() : "null
 
 int lyd_edge_count(int32_t n_r, int32_t n_z) { return (n_z - 2) + 2 * (n_r - 3); }
 
-int lyd_create(lyd_ctx **out, const lyd_dims *d, const lyd_config *cfg) {
-    if (!out || !d || !cfg) return LYD_ERR_ARG;
+int lyd_batch_create(lyd_ctx **out, int32_t ncl, const int32_t *n_r, const int32_t *n_z, int32_t n_nu,
+                     const lyd_config *cfg) {
+    if (!out || !cfg || !n_r || !n_z) return LYD_ERR_ARG;
     *out = nullptr;
-    if (d->n_nu < 4 || d->n_nu > 256 || d->n_r < 3 || d->n_z < 3) return LYD_ERR_ARG;
+    if (ncl < 1 || n_nu < 4 || n_nu > 256) return LYD_ERR_ARG;
+    for (int q = 0; q < ncl; q++) {
+        if (n_r[q] < 3 || n_z[q] < 3) return LYD_ERR_ARG;
+        if ((long long)n_r[q] * n_z[q] * n_nu >= (1LL << 31)) return LYD_ERR_ARG;   // per-cloud int indices
+    }
     if (cfg->precision != LYD_PREC_FP64 && cfg->precision != LYD_PREC_MIXED) return LYD_ERR_ARG;
     if (cfg->flux_method != LYD_FLUX_GLF && cfg->flux_method != LYD_FLUX_HLL) return LYD_ERR_ARG;
-    if (cfg->kcore_min < 0 || cfg->kcore_max >= d->n_nu || cfg->kcore_min > cfg->kcore_max) return LYD_ERR_ARG;
+    if (cfg->kcore_min < 0 || cfg->kcore_max >= n_nu || cfg->kcore_min > cfg->kcore_max) return LYD_ERR_ARG;
     lyd_ctx *c = new lyd_ctx();
     c->cfg = *cfg;
     c->dev = cfg->device;
     if (cudaSetDevice(c->dev) != cudaSuccess) { delete c; return LYD_ERR_CUDA; }
     if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) { delete c; return LYD_ERR_CUDA; }
-    c->nnu = d->n_nu; c->nr = d->n_r; c->nz = d->n_z;
-    c->ncell = (size_t)c->nr * c->nz;
-    c->n3 = c->ncell * c->nnu;
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->dev);
+    c->nnu = n_nu;
+    c->ncl = ncl;
+    c->nr.assign(n_r, n_r + ncl);
+    c->nz.assign(n_z, n_z + ncl);
+    c->have.assign(ncl, 0u);
+    c->desc.assign(ncl, CloudDesc{});
+    for (int q = 0; q < ncl; q++) {
+        CloudDesc &d = c->desc[q];
+        const int nr = n_r[q], nz = n_z[q];
+        d.o3 = (long long)c->n3; d.oc = (long long)c->ncell;
+        d.orf = (long long)c->nrf; d.ozf = (long long)c->nzf;
+        d.ocol = (int)c->ncol; d.orow = (int)c->nrow;
+        d.orint = (int)c->nrint; d.ozint = (int)c->nzint;
+        d.orif = (int)c->nrif; d.ozif = (int)c->nzif;
+        d.nr = nr; d.nz = nz;
+        d.ctdt = d.dt = d.c_tilde = 1.0;
+        c->ncell += (size_t)nr * nz;
+        c->n3 += (size_t)nr * nz * n_nu;
+        c->nrf += (size_t)(nr + 1) * nz;
+        c->nzf += (size_t)nr * (nz + 1);
+        c->ncol += nr; c->nrow += nz;
+        c->nrint += (size_t)(nr + 1) * 5; c->nzint += (size_t)(nz + 1) * 5;
+        c->nrif += nr + 1; c->nzif += nz + 1;
+    }
+    if (c->nrint >= (1u << 31) || c->nzint >= (1u << 31)) { lyd_destroy(c); return LYD_ERR_ARG; }
     c->prec = cfg->precision;
     c->ssz = c->prec == LYD_PREC_FP64 ? sizeof(double) : sizeof(float);
     if (c->prec == LYD_PREC_MIXED) {
@@ -159,25 +290,24 @@ int lyd_create(lyd_ctx **out, const lyd_dims *d, const lyd_config *cfg) {
     A(&c->Hv, c->n3 * c->ssz);
     A((void **)&c->phi_inv, c->ncell * 8);
     for (int q = 0; q < CF_N; q++) A((void **)&c->cellf[q], c->ncell * 8);
-    A((void **)&c->u_r_star, (size_t)(c->nr + 1) * c->nz * 8);
-    A((void **)&c->u_Z_star, (size_t)c->nr * (c->nz + 1) * 8);
+    A((void **)&c->u_r_star, c->nrf * 8);
+    A((void **)&c->u_Z_star, c->nzf * 8);
     A((void **)&c->dV, c->ncell * 8); A((void **)&c->inv_dV, c->ncell * 8);
-    A((void **)&c->A_r, (size_t)(c->nr + 1) * c->nz * 8); A((void **)&c->A_Z, (size_t)c->nr * (c->nz + 1) * 8);
-    A((void **)&c->inv_r_cell, c->nr * 8); A((void **)&c->rCoM, c->nr * 8); A((void **)&c->ZCoM, c->nz * 8);
-    A((void **)&c->rint, (size_t)(c->nr + 1) * 5 * 8); A((void **)&c->zint, (size_t)(c->nz + 1) * 5 * 8);
-    A((void **)&c->r_if, (c->nr + 1) * 8); A((void **)&c->Z_if, (c->nz + 1) * 8);
+    A((void **)&c->A_r, c->nrf * 8); A((void **)&c->A_Z, c->nzf * 8);
+    A((void **)&c->inv_r_cell, c->ncol * 8); A((void **)&c->rCoM, c->ncol * 8); A((void **)&c->ZCoM, c->nrow * 8);
+    A((void **)&c->rint, c->nrint * 8); A((void **)&c->zint, c->nzint * 8);
+    A((void **)&c->r_if, c->nrif * 8); A((void **)&c->Z_if, c->nzif * 8);
     A((void **)&c->nu, (c->nnu + 1) * 8); A((void **)&c->nuC, c->nnu * 8); A((void **)&c->dnu, c->nnu * 8);
     A((void **)&c->inv_dnu, c->nnu * 8); A((void **)&c->inv_nuC, c->nnu * 8);
-    c->fblocks = freq_blocks((int)c->ncell, c->dev);
-    A((void **)&c->partials, (size_t)c->fblocks * (c->nnu + kExtraCols) * 8);
-    A((void **)&c->kwin, 2 * sizeof(int));
-    A((void **)&c->step_ctr, sizeof(int));
-    A((void **)&c->last, 8 * sizeof(double));
+    A((void **)&c->cl, (size_t)ncl * sizeof(CloudDesc));
+    A((void **)&c->kwin, (size_t)2 * ncl * sizeof(int));
+    A((void **)&c->step_ctr, 2 * sizeof(int));
+    A((void **)&c->last, (size_t)7 * ncl * sizeof(double));
     A((void **)&c->err, sizeof(int));
-    A((void **)&c->stage, c->n3 * 8);
     A((void **)&c->small, 512 * 8);
     if (cfg->keep_freq_factors)
         for (int q = 0; q < 3; q++) A((void **)&c->Ff[q], c->n3 * 8);
+    if (r == LYD_OK) r = build_work(c);
     if (r != LYD_OK) {
         lyd_destroy(c);
         return r;
@@ -188,23 +318,38 @@ int lyd_create(lyd_ctx **out, const lyd_dims *d, const lyd_config *cfg) {
     return LYD_OK;
 }
 
+int lyd_create(lyd_ctx **out, const lyd_dims *d, const lyd_config *cfg) {
+    if (!out || !d || !cfg) return LYD_ERR_ARG;
+    *out = nullptr;
+    if (d->n_nu < 4 || d->n_nu > 256 || d->n_r < 3 || d->n_z < 3) return LYD_ERR_ARG;
+    int32_t nr = d->n_r, nz = d->n_z;
+    return lyd_batch_create(out, 1, &nr, &nz, d->n_nu, cfg);
+}
+
 int lyd_destroy(lyd_ctx *c) {
     if (!c) return LYD_OK;
     cudaSetDevice(c->dev);
     if (c->st) cudaStreamSynchronize(c->st);
-    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    drop_graph(c);
     for (int s = 0; s < 2; s++)
         for (int q = 0; q < 3; q++) cudaFree(c->set[s][q]);
     void *ps[] = {c->Hv, c->phi, c->phi_inv, c->aF, c->Ff[0], c->Ff[1], c->Ff[2], c->u_r_star, c->u_Z_star, c->dV,
                   c->inv_dV, c->A_r, c->A_Z, c->inv_r_cell, c->rCoM, c->ZCoM, c->rint, c->zint, c->r_if, c->Z_if,
                   c->nu, c->nuC, c->dnu, c->inv_dnu, c->inv_nuC, c->partials, c->kwin, c->hist, c->step_ctr,
-                  c->last, c->err, c->lut, c->stage, c->small};
+                  c->last, c->err, c->lut, c->stage, c->small, c->cl, c->tiles, c->items};
     for (void *p : ps) cudaFree(p);
     for (int q = 0; q < CF_N; q++) cudaFree(c->cellf[q]);
     for (int q = 0; q < 8; q++)
         if (c->ev[q]) cudaEventDestroy(c->ev[q]);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
+    return LYD_OK;
+}
+
+int lyd_batch_info(lyd_ctx *c, int32_t *ncl, int64_t *cell_bins) {
+    if (!c) return LYD_ERR_ARG;
+    if (ncl) *ncl = c->ncl;
+    if (cell_bins) *cell_bins = (int64_t)c->n3;
     return LYD_OK;
 }
 
@@ -220,25 +365,52 @@ int lyd_synchronize(lyd_ctx *c) {
     return check_err(c);
 }
 
+int lyd_set_tuning(lyd_ctx *c, const lyd_tuning *t) {
+    if (!c || !t) return LYD_ERR_ARG;
+    if (t->rows_per_tile < 4 || t->rows_per_tile > 64) return fail(c, LYD_ERR_ARG, "rows_per_tile outside 4..64");
+    if (t->cells_per_block != 0 && (t->cells_per_block < 8 || t->cells_per_block > 1024))
+        return fail(c, LYD_ERR_ARG, "cells_per_block outside 8..1024");
+    if (t->solver != SOLVER_PCR && t->solver != SOLVER_THOMAS) return fail(c, LYD_ERR_ARG, "unknown solver");
+    cudaSetDevice(c->dev);
+    LYD_CU(c, cudaStreamSynchronize(c->st));
+    c->tune = *t;
+    c->tune.reserved = 0;
+    return build_work(c);
+}
+
+int lyd_get_tuning(lyd_ctx *c, lyd_tuning *t) {
+    if (!c || !t) return LYD_ERR_ARG;
+    *t = c->tune;
+    if (t->cells_per_block == 0) t->cells_per_block = -cells_per_block(c);   // negative: chosen automatically
+    return LYD_OK;
+}
+
 static int h2d(lyd_ctx *c, void *dst, const double *src, size_t n) {
     if (!src) return fail(c, LYD_ERR_ARG, "null host pointer");
     LYD_CU(c, cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyHostToDevice, c->st));
     return LYD_OK;
 }
 
-int lyd_set_geometry(lyd_ctx *c, const lyd_geometry *g) {
+static int bad_cloud(lyd_ctx *c, int q) {
+    return (q < 0 || q >= c->ncl) ? fail(c, LYD_ERR_ARG, "cloud index out of range") : LYD_OK;
+}
+
+int lyd_set_geometry_cloud(lyd_ctx *c, int32_t q, const lyd_geometry *g) {
     if (!c || !g) return LYD_ERR_ARG;
+    LYD_TRY(bad_cloud(c, q));
     cudaSetDevice(c->dev);
-    const int nr = c->nr, nz = c->nz;
-    LYD_TRY(h2d(c, c->dV, g->dV, c->ncell));
-    LYD_TRY(h2d(c, c->inv_dV, g->inv_dV, c->ncell));
-    LYD_TRY(h2d(c, c->A_r, g->A_r, (size_t)(nr + 1) * nz));
-    LYD_TRY(h2d(c, c->A_Z, g->A_Z, (size_t)nr * (nz + 1)));
-    LYD_TRY(h2d(c, c->inv_r_cell, g->inv_r_cell, nr));
-    LYD_TRY(h2d(c, c->rCoM, g->rCoM, nr));
-    LYD_TRY(h2d(c, c->ZCoM, g->ZCoM, nz));
-    LYD_TRY(h2d(c, c->r_if, g->r, nr + 1));
-    LYD_TRY(h2d(c, c->Z_if, g->Z, nz + 1));
+    const CloudDesc &d = c->desc[q];
+    const int nr = d.nr, nz = d.nz;
+    const size_t nc = (size_t)nr * nz;
+    LYD_TRY(h2d(c, c->dV + d.oc, g->dV, nc));
+    LYD_TRY(h2d(c, c->inv_dV + d.oc, g->inv_dV, nc));
+    LYD_TRY(h2d(c, c->A_r + d.orf, g->A_r, (size_t)(nr + 1) * nz));
+    LYD_TRY(h2d(c, c->A_Z + d.ozf, g->A_Z, (size_t)nr * (nz + 1)));
+    LYD_TRY(h2d(c, c->inv_r_cell + d.ocol, g->inv_r_cell, nr));
+    LYD_TRY(h2d(c, c->rCoM + d.ocol, g->rCoM, nr));
+    LYD_TRY(h2d(c, c->ZCoM + d.orow, g->ZCoM, nz));
+    LYD_TRY(h2d(c, c->r_if + d.orif, g->r, nr + 1));
+    LYD_TRY(h2d(c, c->Z_if + d.ozif, g->Z, nz + 1));
     // PLM intervals per face: face 0 = inner boundary, face n = outer boundary, face f in
     // between uses the cell arrays at f-1 (src/AdvectJandH.jl:628-638, 775-779, 884-887).
     auto pack = [](int n, const double *L, const double *R, const double *a, const double *b, const double *cc,
@@ -257,11 +429,17 @@ int lyd_set_geometry(lyd_ctx *c, const lyd_geometry *g) {
     std::vector<double> pr, pz;
     pack(nr, g->dr_L, g->dr_R, g->inv_dr_i_im1, g->inv_dr_ip1_i, g->inv_dr_ip2_ip1, g->dr_bnd, pr);
     pack(nz, g->dZ_L, g->dZ_R, g->inv_dZ_j_jm1, g->inv_dZ_jp1_j, g->inv_dZ_jp2_jp1, g->dZ_bnd, pz);
-    LYD_CU(c, cudaMemcpyAsync(c->rint, pr.data(), pr.size() * 8, cudaMemcpyHostToDevice, c->st));
-    LYD_CU(c, cudaMemcpyAsync(c->zint, pz.data(), pz.size() * 8, cudaMemcpyHostToDevice, c->st));
+    LYD_CU(c, cudaMemcpyAsync(c->rint + d.orint, pr.data(), pr.size() * 8, cudaMemcpyHostToDevice, c->st));
+    LYD_CU(c, cudaMemcpyAsync(c->zint + d.ozint, pz.data(), pz.size() * 8, cudaMemcpyHostToDevice, c->st));
     LYD_CU(c, cudaStreamSynchronize(c->st));
-    c->geom_set = true;
+    c->have[q] |= BIT_GEOM;
     return LYD_OK;
+}
+
+int lyd_set_geometry(lyd_ctx *c, const lyd_geometry *g) {
+    if (!c || !g) return LYD_ERR_ARG;
+    if (c->ncl != 1) return fail(c, LYD_ERR_STATE, "a batch context takes lyd_set_geometry_cloud");
+    return lyd_set_geometry_cloud(c, 0, g);
 }
 
 int lyd_set_freq_grid(lyd_ctx *c, const lyd_freq_grid *f) {
@@ -288,49 +466,59 @@ static int materialize_old(lyd_ctx *c) {
     return LYD_OK;
 }
 
-static int upload3(lyd_ctx *c, void *dst, const double *host, double scale) {
-    LYD_CU(c, cudaMemcpyAsync(c->stage, host, c->n3 * 8, cudaMemcpyHostToDevice, c->st));
-    launch_convert_in(c->prec, c->stage, dst, c->n3, scale, c->st);
+static int upload3(lyd_ctx *c, void *dst, const double *host, size_t n, double scale) {
+    LYD_TRY(ensure_stage(c, n));
+    LYD_CU(c, cudaMemcpyAsync(c->stage, host, n * 8, cudaMemcpyHostToDevice, c->st));
+    launch_convert_in(c->prec, c->stage, dst, n, scale, c->st);
     LYD_CU(c, cudaGetLastError());
     return LYD_OK;
 }
 
-int lyd_upload(lyd_ctx *c, int32_t field, const double *host, size_t count) {
-    if (!c) return LYD_ERR_ARG;
+// One field of cloud q (q < 0: every cloud, concatenated).
+static int upload_field(lyd_ctx *c, int q, int32_t field, const double *host, size_t count) {
     if (!host) return fail(c, LYD_ERR_ARG, "null host pointer");
     cudaSetDevice(c->dev);
-    const size_t n3 = c->n3, nc = c->ncell;
-    if (field <= LYD_F_H_Z_OLD) {
+    const bool one = q >= 0;
+    const CloudDesc d0{};
+    const CloudDesc &d = one ? c->desc[q] : d0;
+    const size_t n3 = one ? (size_t)d.nr * d.nz * c->nnu : c->n3;
+    const size_t nc = one ? (size_t)d.nr * d.nz : c->ncell;
+    auto mark = [&](unsigned bit) {
+        if (one) c->have[q] |= bit;
+        else set_all(c, bit);
+    };
+    if (field <= LYD_F_H_Z_OLD && field >= 0) {
         if (count != n3) return fail(c, LYD_ERR_ARG, "wrong element count for a (n_nu, n_r, n_z) field");
         LYD_TRY(materialize_old(c));
-        int q = (field == LYD_F_J || field == LYD_F_J_OLD) ? 0 : ((field == LYD_F_H_R || field == LYD_F_H_R_OLD) ? 1 : 2);
+        int k = (field == LYD_F_J || field == LYD_F_J_OLD) ? 0 : ((field == LYD_F_H_R || field == LYD_F_H_R_OLD) ? 1 : 2);
         bool old = field == LYD_F_J_OLD || field == LYD_F_H_R_OLD || field == LYD_F_H_Z_OLD;
-        void *dst = old ? c->set[1 - c->cur][q] : c->set[c->cur][q];
-        LYD_TRY(upload3(c, dst, host, c->jscale));
-        if (q == 0 && !old) c->active_valid = false;
+        void *dst = old ? c->set[1 - c->cur][k] : c->set[c->cur][k];
+        LYD_TRY(upload3(c, at(dst, d.o3, c->ssz), host, n3, c->jscale));
+        if (k == 0 && !old) c->active_valid = false;
     } else if (field == LYD_F_HVOIGT) {
         if (count != n3) return fail(c, LYD_ERR_ARG, "wrong element count for H_voigt");
-        LYD_TRY(upload3(c, c->Hv, host, 1.0));
-        c->hv_set = true;
-        if (!c->phi_explicit) c->phi_ready = false;
+        LYD_TRY(upload3(c, at(c->Hv, d.o3, c->ssz), host, n3, 1.0));
+        mark(BIT_HV);
+        c->phi_inv_ready = false;
     } else if (field == LYD_F_PHI_NU || field == LYD_F_ALPHA_F) {
         if (count != n3) return fail(c, LYD_ERR_ARG, "wrong element count");
         void **p = field == LYD_F_PHI_NU ? &c->phi : &c->aF;
-        if (!*p) LYD_TRY(dalloc(c, p, n3 * c->ssz));
-        LYD_TRY(upload3(c, *p, host, 1.0));
-        if (field == LYD_F_PHI_NU) { c->phi_explicit = true; c->phi_ready = true; }
-        else c->aF_explicit = true;
+        if (!*p) LYD_TRY(dalloc(c, p, c->n3 * c->ssz));
+        LYD_TRY(upload3(c, at(*p, d.o3, c->ssz), host, n3, 1.0));
+        mark(field == LYD_F_PHI_NU ? BIT_PHI : BIT_AF);
     } else if (field >= LYD_F_ALPHA && field <= LYD_F_F_Z) {
         if (count != nc) return fail(c, LYD_ERR_ARG, "wrong element count for a per-cell field");
-        int q = field - LYD_F_ALPHA;
-        LYD_TRY(h2d(c, c->cellf[q], host, nc));
-        c->cell_set[q] = true;
+        int k = field - LYD_F_ALPHA;
+        LYD_TRY(h2d(c, c->cellf[k] + d.oc, host, nc));
+        mark(1u << k);
     } else if (field == LYD_F_U_R_STAR) {
-        if (count != (size_t)(c->nr + 1) * c->nz) return fail(c, LYD_ERR_ARG, "wrong element count for u_r_star");
-        LYD_TRY(h2d(c, c->u_r_star, host, count));
+        size_t n = one ? (size_t)(d.nr + 1) * d.nz : c->nrf;
+        if (count != n) return fail(c, LYD_ERR_ARG, "wrong element count for u_r_star");
+        LYD_TRY(h2d(c, c->u_r_star + d.orf, host, n));
     } else if (field == LYD_F_U_Z_STAR) {
-        if (count != (size_t)c->nr * (c->nz + 1)) return fail(c, LYD_ERR_ARG, "wrong element count for u_Z_star");
-        LYD_TRY(h2d(c, c->u_Z_star, host, count));
+        size_t n = one ? (size_t)d.nr * (d.nz + 1) : c->nzf;
+        if (count != n) return fail(c, LYD_ERR_ARG, "wrong element count for u_Z_star");
+        LYD_TRY(h2d(c, c->u_Z_star + d.ozf, host, n));
     } else {
         return fail(c, LYD_ERR_ARG, "unknown field");
     }
@@ -338,19 +526,22 @@ int lyd_upload(lyd_ctx *c, int32_t field, const double *host, size_t count) {
     return LYD_OK;
 }
 
-int lyd_download(lyd_ctx *c, int32_t field, double *host, size_t count) {
-    if (!c) return LYD_ERR_ARG;
+static int download_field(lyd_ctx *c, int q, int32_t field, double *host, size_t count) {
     if (!host) return fail(c, LYD_ERR_ARG, "null host pointer");
     cudaSetDevice(c->dev);
-    const size_t n3 = c->n3, nc = c->ncell;
+    const bool one = q >= 0;
+    const CloudDesc d0{};
+    const CloudDesc &d = one ? c->desc[q] : d0;
+    const size_t n3 = one ? (size_t)d.nr * d.nz * c->nnu : c->n3;
+    const size_t nc = one ? (size_t)d.nr * d.nz : c->ncell;
     const void *src = nullptr;
     size_t n = 0;
     double scale = 1.0;
     bool is3 = false;
-    if (field <= LYD_F_H_Z_OLD) {
-        int q = (field == LYD_F_J || field == LYD_F_J_OLD) ? 0 : ((field == LYD_F_H_R || field == LYD_F_H_R_OLD) ? 1 : 2);
+    if (field <= LYD_F_H_Z_OLD && field >= 0) {
+        int k = (field == LYD_F_J || field == LYD_F_J_OLD) ? 0 : ((field == LYD_F_H_R || field == LYD_F_H_R_OLD) ? 1 : 2);
         bool old = field == LYD_F_J_OLD || field == LYD_F_H_R_OLD || field == LYD_F_H_Z_OLD;
-        src = old ? Jold(c, q) : Jc(c, q);
+        src = old ? Jold(c, k) : Jc(c, k);
         n = n3; scale = c->jscale; is3 = true;
     } else if (field == LYD_F_HVOIGT) {
         src = c->Hv; n = n3; is3 = true;
@@ -359,17 +550,18 @@ int lyd_download(lyd_ctx *c, int32_t field, double *host, size_t count) {
         if (!src) return fail(c, LYD_ERR_STATE, "field is derived on the device and was never uploaded");
         n = n3; is3 = true;
     } else if (field >= LYD_F_ALPHA && field <= LYD_F_F_Z) {
-        src = c->cellf[field - LYD_F_ALPHA]; n = nc;
+        src = c->cellf[field - LYD_F_ALPHA] + d.oc; n = nc;
     } else if (field == LYD_F_U_R_STAR) {
-        src = c->u_r_star; n = (size_t)(c->nr + 1) * c->nz;
+        src = c->u_r_star + d.orf; n = one ? (size_t)(d.nr + 1) * d.nz : c->nrf;
     } else if (field == LYD_F_U_Z_STAR) {
-        src = c->u_Z_star; n = (size_t)c->nr * (c->nz + 1);
+        src = c->u_Z_star + d.ozf; n = one ? (size_t)d.nr * (d.nz + 1) : c->nzf;
     } else {
         return fail(c, LYD_ERR_ARG, "unknown field");
     }
     if (count != n) return fail(c, LYD_ERR_ARG, "wrong element count");
     if (is3) {
-        launch_convert_out(c->prec, src, c->stage, n, scale, c->st);
+        LYD_TRY(ensure_stage(c, n));
+        launch_convert_out(c->prec, at(const_cast<void *>(src), d.o3, c->ssz), c->stage, n, scale, c->st);
         LYD_CU(c, cudaGetLastError());
         LYD_CU(c, cudaMemcpyAsync(host, c->stage, n * 8, cudaMemcpyDeviceToHost, c->st));
     } else {
@@ -378,24 +570,46 @@ int lyd_download(lyd_ctx *c, int32_t field, double *host, size_t count) {
     return check_err(c);
 }
 
+int lyd_upload(lyd_ctx *c, int32_t field, const double *host, size_t count) {
+    if (!c) return LYD_ERR_ARG;
+    return upload_field(c, -1, field, host, count);
+}
+int lyd_download(lyd_ctx *c, int32_t field, double *host, size_t count) {
+    if (!c) return LYD_ERR_ARG;
+    return download_field(c, -1, field, host, count);
+}
+int lyd_upload_cloud(lyd_ctx *c, int32_t q, int32_t field, const double *host, size_t count) {
+    if (!c) return LYD_ERR_ARG;
+    LYD_TRY(bad_cloud(c, q));
+    return upload_field(c, q, field, host, count);
+}
+int lyd_download_cloud(lyd_ctx *c, int32_t q, int32_t field, double *host, size_t count) {
+    if (!c) return LYD_ERR_ARG;
+    LYD_TRY(bad_cloud(c, q));
+    return download_field(c, q, field, host, count);
+}
+
 // ---- argument blocks -------------------------------------------------------------------------
 template <typename S>
-static void fill_adv(lyd_ctx *c, AdvArgs<S> &a, int in_set, int out_set, double ctdt, int bcr, int bzb, int bzt) {
+static void fill_adv(lyd_ctx *c, AdvArgs<S> &a, int in_set, int out_set) {
+    memset(&a, 0, sizeof(a));
     a.J = (const S *)c->set[in_set][0]; a.Hr = (const S *)c->set[in_set][1]; a.HZ = (const S *)c->set[in_set][2];
     a.Jo = (S *)c->set[out_set][0]; a.Hro = (S *)c->set[out_set][1]; a.HZo = (S *)c->set[out_set][2];
-    a.aF = c->aF_explicit ? (const S *)c->aF : nullptr;
+    a.aF = c->aF ? (const S *)c->aF : nullptr;
     a.Hv = (const S *)c->Hv;
     a.alpha = c->cellf[CF_ALPHA];
-    a.alpha_cF = c->cell_set[CF_ALPHA_CF] ? c->cellf[CF_ALPHA_CF] : nullptr;
+    a.alpha_cF = any_have(c, 1u << CF_ALPHA_CF) ? c->cellf[CF_ALPHA_CF] : nullptr;
     a.A_r = c->A_r; a.A_Z = c->A_Z; a.inv_dV = c->inv_dV; a.inv_r_cell = c->inv_r_cell;
     a.rint = c->rint; a.zint = c->zint;
     a.u_r_star = c->u_r_star; a.u_Z_star = c->u_Z_star;
     a.dur_dr = c->cellf[CF_DUR_DR]; a.dur_dZ = c->cellf[CF_DUR_DZ]; a.duZ_dr = c->cellf[CF_DUZ_DR];
     a.duZ_dZ = c->cellf[CF_DUZ_DZ]; a.ur_over_r = c->cellf[CF_UR_OVER_R];
     a.kwin = c->kwin;
-    a.nnu = c->nnu; a.nr = c->nr; a.nz = c->nz;
-    a.ctdt = ctdt; a.jeps = c->jeps_s; a.heps2 = c->heps2_s;
-    a.bc_r_right = bcr; a.bc_z_bot = bzb; a.bc_z_top = bzt;
+    a.cl = c->cl;
+    a.tiles = c->tiles;
+    a.rows = c->tune.rows_per_tile;
+    a.nnu = c->nnu;
+    a.jeps = c->jeps_s; a.heps2 = c->heps2_s;
 }
 
 template <typename S>
@@ -405,47 +619,54 @@ static void fill_freq(lyd_ctx *c, FreqArgs<S> &a, const void *Jin, const void *H
     a.Jin = (const S *)Jin; a.Hrin = (const S *)Hrin; a.HZin = (const S *)HZin; a.Jold = (const S *)Jo;
     a.Jout = (S *)Jout; a.Hrout = (S *)Hrout; a.HZout = (S *)HZout;
     a.Hv = (const S *)c->Hv;
-    a.phi = c->phi_explicit ? (const S *)c->phi : nullptr;
+    a.phi = c->phi ? (const S *)c->phi : nullptr;
     a.phi_inv = c->phi_inv; a.phi_kmin = c->phi_kmin; a.phi_kmax = c->phi_kmax;
-    a.aF = c->aF_explicit ? (const S *)c->aF : nullptr;
+    a.aF = c->aF ? (const S *)c->aF : nullptr;
     a.alpha = c->cellf[CF_ALPHA]; a.alpha_c = c->cellf[CF_ALPHA_C];
-    a.alpha_cF = c->cell_set[CF_ALPHA_CF] ? c->cellf[CF_ALPHA_CF] : nullptr;
+    a.alpha_cF = any_have(c, 1u << CF_ALPHA_CF) ? c->cellf[CF_ALPHA_CF] : nullptr;
     a.pd = c->cellf[CF_PD]; a.js = c->cellf[CF_JS]; a.T = c->cellf[CF_T];
     a.dur_dr = c->cellf[CF_DUR_DR]; a.dur_dZ = c->cellf[CF_DUR_DZ]; a.duZ_dr = c->cellf[CF_DUZ_DR];
     a.duZ_dZ = c->cellf[CF_DUZ_DZ]; a.ur_over_r = c->cellf[CF_UR_OVER_R];
     a.nu = c->nu; a.nuC = c->nuC; a.dnu = c->dnu; a.inv_dnu = c->inv_dnu; a.inv_nuC = c->inv_nuC;
     a.dV = c->dV; a.A_r = c->A_r; a.A_Z = c->A_Z; a.rCoM = c->rCoM; a.ZCoM = c->ZCoM;
+    a.cl = c->cl;
+    a.items = c->items;
     a.alpha_floor = c->cfg.alpha_floor;
     a.jeps = c->jeps_s; a.heps2 = c->heps2_s; a.j_scale = c->jscale;
     a.recoil = c->cfg.recoil;
     a.partials = c->partials; a.err = c->err;
-    a.nnu = c->nnu; a.nr = c->nr; a.nz = c->nz;
+    a.nnu = c->nnu;
+    a.solver = c->tune.solver;
 }
 
 static int need_inputs(lyd_ctx *c, bool emission, bool freq) {
-    if (!c->geom_set) return fail(c, LYD_ERR_STATE, "geometry not set (lyd_set_geometry)");
+    if (!all_have(c, BIT_GEOM)) return fail(c, LYD_ERR_STATE, "geometry not set (lyd_set_geometry)");
     if (!c->freq_set) return fail(c, LYD_ERR_STATE, "frequency grid not set (lyd_set_freq_grid)");
-    if ((emission || freq) && !c->hv_set) return fail(c, LYD_ERR_STATE, "H_voigt not set");
-    if (emission && !c->phi_ready)
+    if ((emission || freq) && !all_have(c, BIT_HV)) return fail(c, LYD_ERR_STATE, "H_voigt not set");
+    if (c->phi && !all_have(c, BIT_PHI))
+        return fail(c, LYD_ERR_STATE, "phi_nu was uploaded for some clouds only");
+    if (c->aF && !all_have(c, BIT_AF))
+        return fail(c, LYD_ERR_STATE, "alpha_F was uploaded for some clouds only");
+    if (emission && !c->phi && !c->phi_inv_ready)
         return fail(c, LYD_ERR_STATE, "phi_nu not set (upload it or call lyd_update_phi_nu)");
-    if (freq && !c->cell_set[CF_T]) return fail(c, LYD_ERR_STATE, "temperature T not uploaded");
+    if (freq && !all_have(c, 1u << CF_T)) return fail(c, LYD_ERR_STATE, "temperature T not uploaded");
     return LYD_OK;
 }
 
 static RedArgs red_args(lyd_ctx *c, int parts) {
     RedArgs r;
     memset(&r, 0, sizeof(r));
-    r.partials = c->partials; r.nblocks = c->fblocks; r.nnu = c->nnu; r.parts = parts;
+    r.partials = c->partials; r.nblocks = c->nitems; r.nnu = c->nnu; r.nclouds = c->ncl; r.parts = parts;
     r.kcore_min = c->cfg.kcore_min; r.kcore_max = c->cfg.kcore_max;
-    r.j_scale = c->jscale; r.kwin = c->kwin; r.err = c->err; r.last = c->last;
+    r.j_scale = c->jscale; r.cl = c->cl; r.kwin = c->kwin; r.last = c->last;
     return r;
 }
 
 static int run_find_active(lyd_ctx *c) {
-    launch_find_active(c->prec, Jc(c, 0), c->nnu, c->nr, c->nz, c->dnu, c->dV, c->jeps_s, c->partials, c->fblocks,
+    LYD_TRY(sync_desc(c));
+    launch_find_active(c->prec, Jc(c, 0), c->nnu, c->dnu, c->dV, c->cl, c->items, c->nitems, c->jeps_s, c->partials,
                        c->st);
-    RedArgs r = red_args(c, PART_ACTIVE);
-    launch_reduce(r, c->st);
+    launch_reduce(red_args(c, PART_ACTIVE), c->st);
     LYD_CU(c, cudaGetLastError());
     c->active_valid = true;
     return LYD_OK;
@@ -456,11 +677,13 @@ int lyd_find_active_bins(lyd_ctx *c, int32_t *kmin, int32_t *kmax) {
     cudaSetDevice(c->dev);
     LYD_TRY(need_inputs(c, false, false));
     LYD_TRY(run_find_active(c));
-    int h[2];
-    LYD_CU(c, cudaMemcpyAsync(h, c->kwin, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+    std::vector<int> h((size_t)2 * c->ncl);
+    LYD_CU(c, cudaMemcpyAsync(h.data(), c->kwin, h.size() * sizeof(int), cudaMemcpyDeviceToHost, c->st));
     LYD_TRY(check_err(c));
-    *kmin = h[0];
-    *kmax = h[1];
+    for (int q = 0; q < c->ncl; q++) {
+        kmin[q] = h[2 * q];
+        kmax[q] = h[2 * q + 1];
+    }
     return LYD_OK;
 }
 
@@ -471,17 +694,30 @@ static int check_bcs(lyd_ctx *c, int l, int r, int b, int t) {
     return LYD_OK;
 }
 
-static int do_advect(lyd_ctx *c, double ctdt, int bcr, int bzb, int bzt) {
+// Parameters of every cloud for the per-phase calls (one c~, dt and boundary set for all).
+static void params_all(lyd_ctx *c, double ct, double dt, double ctdt) {
+    for (CloudDesc &d : c->desc) {
+        d.c_tilde = ct; d.dt = dt; d.ctdt = ctdt;
+    }
+}
+static void bcs_all(lyd_ctx *c, int bcr, int bzb, int bzt) {
+    for (CloudDesc &d : c->desc) {
+        d.bc_r_right = bcr; d.bc_z_bot = bzb; d.bc_z_top = bzt;
+    }
+}
+
+static int do_advect(lyd_ctx *c) {
     if (!c->active_valid) LYD_TRY(run_find_active(c));
+    LYD_TRY(sync_desc(c));
     int in = c->cur, out = 1 - c->cur;
     if (c->prec == 0) {
         AdvArgs<double> a;
-        fill_adv<double>(c, a, in, out, ctdt, bcr, bzb, bzt);
-        launch_advect(0, c->cfg.flux_method, &a, c->nnu, c->nr, c->nz, c->st);
+        fill_adv<double>(c, a, in, out);
+        launch_advect(0, c->cfg.flux_method, &a, c->ntiles, c->st);
     } else {
         AdvArgs<float> a;
-        fill_adv<float>(c, a, in, out, ctdt, bcr, bzb, bzt);
-        launch_advect(1, c->cfg.flux_method, &a, c->nnu, c->nr, c->nz, c->st);
+        fill_adv<float>(c, a, in, out);
+        launch_advect(1, c->cfg.flux_method, &a, c->ntiles, c->st);
     }
     LYD_CU(c, cudaGetLastError());
     c->cur = out;
@@ -496,20 +732,21 @@ int lyd_advect(lyd_ctx *c, double ctdt, int32_t bl, int32_t br, int32_t bb, int3
     LYD_TRY(check_bcs(c, bl, br, bb, bt));
     LYD_TRY(need_inputs(c, false, false));
     if (!(ctdt > 0.0)) return fail(c, LYD_ERR_ARG, "c~ dt must be positive");
-    return do_advect(c, ctdt, br, bb, bt);
+    for (CloudDesc &d : c->desc) d.ctdt = ctdt;
+    bcs_all(c, br, bb, bt);
+    return do_advect(c);
 }
 
 template <typename S>
-static int freq_call(lyd_ctx *c, bool emission, bool freq, double ct, double dt, double ctdt, int update_ff,
-                     int parts) {
+static int freq_call(lyd_ctx *c, bool emission, bool freq, int update_ff, int parts) {
+    LYD_TRY(sync_desc(c));
     FreqArgs<S> a;
     fill_freq<S>(c, a, Jc(c, 0), Jc(c, 1), Jc(c, 2), Jold(c, 0), Jc(c, 0), Jc(c, 1), Jc(c, 2));
     a.do_emission = emission; a.do_freq = freq; a.update_ff = update_ff;
-    a.c_tilde = ct; a.dt = dt; a.ctdt = ctdt;
     a.dru_r = c->cellf[CF_DRU_R]; a.dru_Z = c->cellf[CF_DRU_Z];
     if (c->cfg.keep_freq_factors) { a.Fkp = c->Ff[0]; a.Fk = c->Ff[1]; a.Fkm = c->Ff[2]; }
     a.parts = parts;
-    launch_freq(c->prec, &a, c->nnu, (int)c->ncell, c->fblocks, c->st);
+    launch_freq(c->prec, &a, c->nnu, c->nitems, c->st);
     LYD_CU(c, cudaGetLastError());
     return LYD_OK;
 }
@@ -519,8 +756,8 @@ int lyd_emission_absorption(lyd_ctx *c, double ct, double dt) {
     cudaSetDevice(c->dev);
     LYD_TRY(need_inputs(c, true, false));
     if (!(ct > 0.0) || !(dt > 0.0)) return fail(c, LYD_ERR_ARG, "c~ and dt must be positive");
-    int r = c->prec == 0 ? freq_call<double>(c, true, false, ct, dt, ct * dt, 1, 0)
-                         : freq_call<float>(c, true, false, ct, dt, ct * dt, 1, 0);
+    params_all(c, ct, dt, ct * dt);
+    int r = c->prec == 0 ? freq_call<double>(c, true, false, 1, 0) : freq_call<float>(c, true, false, 1, 0);
     if (r != LYD_OK) return r;
     c->old_alias = true;
     c->active_valid = false;
@@ -534,8 +771,10 @@ int lyd_frequency_update(lyd_ctx *c, double ctdt, int32_t update_ff) {
     if (!(ctdt > 0.0)) return fail(c, LYD_ERR_ARG, "c~ dt must be positive");
     if (!update_ff && !(c->cfg.keep_freq_factors && c->ff_valid))
         return fail(c, LYD_ERR_STATE, "update_freq_factors = 0 needs keep_freq_factors and a previous update");
-    int r = c->prec == 0 ? freq_call<double>(c, false, true, 1.0, 1.0, ctdt, update_ff ? 1 : 0, PART_ACTIVE)
-                         : freq_call<float>(c, false, true, 1.0, 1.0, ctdt, update_ff ? 1 : 0, PART_ACTIVE);
+    for (CloudDesc &d : c->desc) d.ctdt = ctdt;
+    int uf = update_ff ? 1 : 0;
+    int r = c->prec == 0 ? freq_call<double>(c, false, true, uf, PART_ACTIVE)
+                         : freq_call<float>(c, false, true, uf, PART_ACTIVE);
     if (r != LYD_OK) return r;
     launch_reduce(red_args(c, PART_ACTIVE), c->st);
     LYD_CU(c, cudaGetLastError());
@@ -561,19 +800,28 @@ int lyd_reset_dru(lyd_ctx *c) {
     return LYD_OK;
 }
 
+static int single_cloud(lyd_ctx *c, const char *what) {
+    if (c->ncl != 1)
+        return fail(c, LYD_ERR_STATE, std::string(what) + " acts on a single-cloud context; a batch reports it per cloud");
+    return LYD_OK;
+}
+
 int lyd_force_multiplier(lyd_ctx *c, double dt, double zc, int32_t bc_z_bot, double out[4]) {
     if (!c || !out) return LYD_ERR_ARG;
+    LYD_TRY(single_cloud(c, "lyd_force_multiplier"));
     cudaSetDevice(c->dev);
-    if (!c->geom_set) return fail(c, LYD_ERR_STATE, "geometry not set");
+    if (!all_have(c, BIT_GEOM)) return fail(c, LYD_ERR_STATE, "geometry not set");
     if (!(dt > 0.0)) return fail(c, LYD_ERR_ARG, "dt must be positive");
+    const int nr = c->nr[0], nz = c->nz[0];
+    const int nb = std::min(c->nitems, 4 * c->sms);
     launch_mf(c->cellf[CF_DRU_R], c->cellf[CF_DRU_Z], c->cellf[CF_F_R], c->cellf[CF_F_Z], c->cellf[CF_JS], c->dV,
-              c->rCoM, c->ZCoM, c->nr, c->nz, dt, zc, c->partials, c->fblocks, c->st);
-    launch_column_sums(c->partials, 4, c->fblocks, c->small, c->st);
+              c->rCoM, c->ZCoM, nr, nz, dt, zc, c->partials, nb, c->st);
+    launch_column_sums(c->partials, 4, nb, c->small, c->st);
     LYD_CU(c, cudaGetLastError());
     double h[4];
     LYD_CU(c, cudaMemcpyAsync(h, c->small, sizeof(h), cudaMemcpyDeviceToHost, c->st));
     LYD_TRY(check_err(c));
-    c->cell_set[CF_F_R] = c->cell_set[CF_F_Z] = true;
+    set_all(c, (1u << CF_F_R) | (1u << CF_F_Z));
     // normalisation, src/ConstantsAndFunctions.jl:652-673
     double MF = h[0], net = h[1], outw = h[2], L = h[3];
     if (L > 0.0) {
@@ -589,10 +837,11 @@ int lyd_force_multiplier(lyd_ctx *c, double dt, double zc, int32_t bc_z_bot, dou
 
 int lyd_f_esc(lyd_ctx *c, double L_all, int32_t bc_z_bot, double *f) {
     if (!c || !f) return LYD_ERR_ARG;
+    LYD_TRY(single_cloud(c, "lyd_f_esc"));
     cudaSetDevice(c->dev);
-    if (!c->geom_set || !c->freq_set) return fail(c, LYD_ERR_STATE, "geometry / frequency grid not set");
+    if (!all_have(c, BIT_GEOM) || !c->freq_set) return fail(c, LYD_ERR_STATE, "geometry / frequency grid not set");
     if (L_all <= 0.0) { *f = 0.0; return LYD_OK; }
-    launch_fesc(c->prec, Jc(c, 1), Jc(c, 2), c->A_r, c->A_Z, c->dnu, c->nnu, c->nr, c->nz, bc_z_bot, c->jscale,
+    launch_fesc(c->prec, Jc(c, 1), Jc(c, 2), c->A_r, c->A_Z, c->dnu, c->nnu, c->nr[0], c->nz[0], bc_z_bot, c->jscale,
                 c->small, c->st);
     LYD_CU(c, cudaGetLastError());
     double num;
@@ -605,27 +854,23 @@ int lyd_f_esc(lyd_ctx *c, double L_all, int32_t bc_z_bot, double *f) {
 
 // ---- fused static-cloud step -----------------------------------------------------------------
 template <typename S>
-static int enqueue_step(lyd_ctx *c, const lyd_step_params *p, bool timed) {
-    const double ctdt = p->c_tilde * p->dt;
+static int enqueue_step(lyd_ctx *c, bool timed) {
     const int A = c->cur, B = 1 - c->cur;
     AdvArgs<S> aa;
-    fill_adv<S>(c, aa, A, B, ctdt, p->bc_r_right, p->bc_z_bot, p->bc_z_top);
+    fill_adv<S>(c, aa, A, B);
     FreqArgs<S> fa;
     fill_freq<S>(c, fa, c->set[B][0], c->set[B][1], c->set[B][2], c->set[B][0], c->set[A][0], c->set[A][1],
                  c->set[A][2]);
     fa.do_emission = 1; fa.do_freq = 1; fa.update_ff = 1;
-    fa.c_tilde = p->c_tilde; fa.dt = p->dt; fa.ctdt = ctdt; fa.z_center = p->z_center;
-    fa.bc_z_bot = p->bc_z_bot;
     fa.parts = PART_ACTIVE | PART_DIAG;
     fa.f_r = c->cellf[CF_F_R]; fa.f_Z = c->cellf[CF_F_Z];
     RedArgs ra = red_args(c, PART_ACTIVE | PART_DIAG);
-    ra.dt = p->dt; ra.c_tilde = p->c_tilde; ra.bc_z_bot = p->bc_z_bot;
-    ra.diag = c->hist; ra.step_counter = c->step_ctr; ra.hist_capacity = c->hist_cap;
+    ra.diag = c->hist; ra.step_counter = c->step_ctr; ra.done = c->step_ctr + 1; ra.hist_capacity = c->hist_cap;
     const int prec = sizeof(S) == 8 ? 0 : 1;
     if (timed) cudaEventRecord(c->ev[0], c->st);
-    launch_advect(prec, c->cfg.flux_method, &aa, c->nnu, c->nr, c->nz, c->st);
+    launch_advect(prec, c->cfg.flux_method, &aa, c->ntiles, c->st);
     if (timed) cudaEventRecord(c->ev[1], c->st);
-    launch_freq(prec, &fa, c->nnu, (int)c->ncell, c->fblocks, c->st);
+    launch_freq(prec, &fa, c->nnu, c->nitems, c->st);
     if (timed) cudaEventRecord(c->ev[2], c->st);
     launch_reduce(ra, c->st);
     if (timed) cudaEventRecord(c->ev[3], c->st);
@@ -645,30 +890,30 @@ int lyd_get_timing(lyd_ctx *c, double ms[3]) {
     return LYD_OK;
 }
 
-int lyd_static_steps(lyd_ctx *c, const lyd_step_params *p, lyd_diag *hist_out) {
-    if (!c || !p) return LYD_ERR_ARG;
-    cudaSetDevice(c->dev);
-    LYD_TRY(check_bcs(c, LYD_BC_REFLECT, p->bc_r_right, p->bc_z_bot, p->bc_z_top));
+// n_steps fused steps with the parameters already in the host descriptors.
+static int run_steps(lyd_ctx *c, int n_steps, lyd_diag *hist_out) {
     LYD_TRY(need_inputs(c, true, true));
-    if (!(p->c_tilde > 0.0) || !(p->dt > 0.0) || p->n_steps < 0) return fail(c, LYD_ERR_ARG, "bad step parameters");
-    if (p->n_steps == 0) return LYD_OK;
-    if (p->n_steps > c->hist_cap) {
+    if (n_steps == 0) return LYD_OK;
+    if (n_steps > c->hist_cap) {
+        LYD_CU(c, cudaStreamSynchronize(c->st));
         cudaFree(c->hist);
         c->hist = nullptr;
-        int cap = p->n_steps < 1024 ? 1024 : p->n_steps;
-        LYD_TRY(dalloc(c, (void **)&c->hist, (size_t)cap * 7 * 8));
+        c->hist_cap = 0;
+        int cap = n_steps < 1024 ? 1024 : n_steps;
+        LYD_TRY(dalloc(c, (void **)&c->hist, (size_t)cap * c->ncl * 7 * 8));
         c->hist_cap = cap;
-        if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
+        drop_graph(c);
     }
-    LYD_CU(c, cudaMemsetAsync(c->step_ctr, 0, sizeof(int), c->st));
+    LYD_TRY(sync_desc(c));
+    LYD_CU(c, cudaMemsetAsync(c->step_ctr, 0, 2 * sizeof(int), c->st));
     // the fused step keeps no Delta rho u between steps (Reset_Delta_rho_u! ends each step)
     LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_R], 0, c->ncell * 8, c->st));
     LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_Z], 0, c->ncell * 8, c->st));
     if (!c->active_valid) LYD_TRY(run_find_active(c));
     if (c->timing) {
         double acc[3] = {0, 0, 0};
-        for (int n = 0; n < p->n_steps; n++) {
-            int r = c->prec == 0 ? enqueue_step<double>(c, p, true) : enqueue_step<float>(c, p, true);
+        for (int n = 0; n < n_steps; n++) {
+            int r = c->prec == 0 ? enqueue_step<double>(c, true) : enqueue_step<float>(c, true);
             if (r != LYD_OK) return r;
             LYD_CU(c, cudaEventSynchronize(c->ev[3]));
             for (int q = 0; q < 3; q++) {
@@ -679,34 +924,29 @@ int lyd_static_steps(lyd_ctx *c, const lyd_step_params *p, lyd_diag *hist_out) {
         }
         for (int q = 0; q < 3; q++) c->ms[q] = acc[q];
     } else {
-        bool same = c->gexec && c->gkey[0] == p->c_tilde && c->gkey[1] == p->dt && c->gkey[2] == p->z_center &&
-                    c->gkey_i[0] == p->bc_r_right && c->gkey_i[1] == p->bc_z_bot && c->gkey_i[2] == p->bc_z_top &&
-                    c->gkey_i[3] == c->cur;
-        if (!same) {
-            if (c->gexec) { cudaGraphExecDestroy(c->gexec); c->gexec = nullptr; }
+        if (!c->gexec || c->gkey_cur != c->cur) {
+            drop_graph(c);
             cudaGraph_t g;
             LYD_CU(c, cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-            int r = c->prec == 0 ? enqueue_step<double>(c, p, false) : enqueue_step<float>(c, p, false);
+            int r = c->prec == 0 ? enqueue_step<double>(c, false) : enqueue_step<float>(c, false);
             cudaError_t e = cudaStreamEndCapture(c->st, &g);
             if (r != LYD_OK) return r;
             if (e != cudaSuccess) return fail(c, LYD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
             e = cudaGraphInstantiate(&c->gexec, g, 0);
             cudaGraphDestroy(g);
             if (e != cudaSuccess) return fail(c, LYD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-            c->gkey[0] = p->c_tilde; c->gkey[1] = p->dt; c->gkey[2] = p->z_center;
-            c->gkey_i[0] = p->bc_r_right; c->gkey_i[1] = p->bc_z_bot; c->gkey_i[2] = p->bc_z_top;
-            c->gkey_i[3] = c->cur;
+            c->gkey_cur = c->cur;
         }
-        for (int n = 0; n < p->n_steps; n++) LYD_CU(c, cudaGraphLaunch(c->gexec, c->st));
+        for (int n = 0; n < n_steps; n++) LYD_CU(c, cudaGraphLaunch(c->gexec, c->st));
     }
     c->old_alias = true;
     c->active_valid = true;
     if (hist_out) {
-        std::vector<double> h((size_t)p->n_steps * 7);
+        std::vector<double> h((size_t)n_steps * c->ncl * 7);
         LYD_CU(c, cudaMemcpyAsync(h.data(), c->hist, h.size() * 8, cudaMemcpyDeviceToHost, c->st));
         LYD_TRY(check_err(c));
-        for (int n = 0; n < p->n_steps; n++) {
-            const double *r = &h[(size_t)n * 7];
+        for (size_t n = 0; n < (size_t)n_steps * c->ncl; n++) {
+            const double *r = &h[n * 7];
             hist_out[n].M_F = r[0]; hist_out[n].M_F_radial_net = r[1]; hist_out[n].M_F_radial_out = r[2];
             hist_out[n].L_tot = r[3]; hist_out[n].f_esc = r[4];
             hist_out[n].kmin = (int32_t)r[5]; hist_out[n].kmax = (int32_t)r[6];
@@ -719,12 +959,39 @@ int lyd_static_steps(lyd_ctx *c, const lyd_step_params *p, lyd_diag *hist_out) {
     return LYD_OK;
 }
 
+int lyd_static_steps(lyd_ctx *c, const lyd_step_params *p, lyd_diag *hist_out) {
+    if (!c || !p) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    LYD_TRY(check_bcs(c, LYD_BC_REFLECT, p->bc_r_right, p->bc_z_bot, p->bc_z_top));
+    if (!(p->c_tilde > 0.0) || !(p->dt > 0.0) || p->n_steps < 0) return fail(c, LYD_ERR_ARG, "bad step parameters");
+    params_all(c, p->c_tilde, p->dt, p->c_tilde * p->dt);
+    for (CloudDesc &d : c->desc) d.z_center = p->z_center;
+    bcs_all(c, p->bc_r_right, p->bc_z_bot, p->bc_z_top);
+    return run_steps(c, p->n_steps, hist_out);
+}
+
+int lyd_batch_steps(lyd_ctx *c, const lyd_cloud_params *p, int32_t n_steps, lyd_diag *hist_out) {
+    if (!c || !p) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    if (n_steps < 0) return fail(c, LYD_ERR_ARG, "bad step count");
+    for (int q = 0; q < c->ncl; q++) {
+        LYD_TRY(check_bcs(c, LYD_BC_REFLECT, p[q].bc_r_right, p[q].bc_z_bot, p[q].bc_z_top));
+        if (!(p[q].c_tilde > 0.0) || !(p[q].dt > 0.0)) return fail(c, LYD_ERR_ARG, "bad step parameters");
+    }
+    for (int q = 0; q < c->ncl; q++) {
+        CloudDesc &d = c->desc[q];
+        d.c_tilde = p[q].c_tilde; d.dt = p[q].dt; d.ctdt = p[q].c_tilde * p[q].dt; d.z_center = p[q].z_center;
+        d.bc_r_right = p[q].bc_r_right; d.bc_z_bot = p[q].bc_z_bot; d.bc_z_top = p[q].bc_z_top;
+    }
+    return run_steps(c, n_steps, hist_out);
+}
+
 // ---- set-up helpers ------------------------------------------------------------------------------
 int lyd_update_hvoigt(lyd_ctx *c) {
     if (!c) return LYD_ERR_ARG;
     cudaSetDevice(c->dev);
     if (!c->freq_set) return fail(c, LYD_ERR_STATE, "frequency grid not set");
-    if (!c->cell_set[CF_T]) return fail(c, LYD_ERR_STATE, "temperature T not uploaded");
+    if (!all_have(c, 1u << CF_T)) return fail(c, LYD_ERR_STATE, "temperature T not uploaded");
     if (!c->lut) {
         std::vector<double> h((size_t)5 * kLutN);
         build_voigt_lut(h.data(), kLutN, kLutXmax);
@@ -732,10 +999,10 @@ int lyd_update_hvoigt(lyd_ctx *c) {
         LYD_CU(c, cudaMemcpyAsync(c->lut, h.data(), h.size() * 8, cudaMemcpyHostToDevice, c->st));
         LYD_CU(c, cudaStreamSynchronize(c->st));
     }
-    launch_hvoigt(c->prec, c->Hv, c->cellf[CF_T], c->nu, c->nuC, c->nnu, (int)c->ncell, c->lut, kLutN, kLutXmax, c->st);
+    launch_hvoigt(c->prec, c->Hv, c->cellf[CF_T], c->nu, c->nuC, c->nnu, c->ncell, c->lut, kLutN, kLutXmax, c->st);
     LYD_CU(c, cudaGetLastError());
-    c->hv_set = true;
-    if (!c->phi_explicit) c->phi_ready = false;
+    set_all(c, BIT_HV);
+    c->phi_inv_ready = false;
     return check_err(c);
 }
 
@@ -743,13 +1010,16 @@ int lyd_update_phi_nu(lyd_ctx *c, int32_t kmin, int32_t kmax) {
     if (!c) return LYD_ERR_ARG;
     cudaSetDevice(c->dev);
     if (kmin < 0 || kmax >= c->nnu || kmin > kmax) return fail(c, LYD_ERR_ARG, "bad bin range");
-    if (!c->hv_set || !c->freq_set) return fail(c, LYD_ERR_STATE, "H_voigt / frequency grid not set");
-    launch_phi_inv(c->prec, c->Hv, c->dnu, c->nnu, (int)c->ncell, kmin, kmax, c->phi_inv, c->st);
+    if (!all_have(c, BIT_HV) || !c->freq_set) return fail(c, LYD_ERR_STATE, "H_voigt / frequency grid not set");
+    launch_phi_inv(c->prec, c->Hv, c->dnu, c->nnu, c->ncell, kmin, kmax, c->phi_inv, c->st);
     LYD_CU(c, cudaGetLastError());
     c->phi_kmin = kmin;
     c->phi_kmax = kmax;
-    c->phi_explicit = false;
-    c->phi_ready = true;
+    // a derived phi_nu replaces an uploaded one
+    cudaFree(c->phi);
+    c->phi = nullptr;
+    for (unsigned &h : c->have) h &= ~BIT_PHI;
+    c->phi_inv_ready = true;
     return check_err(c);
 }
 
@@ -776,15 +1046,16 @@ int lyd_pd_lya(lyd_ctx *c, size_t n, const double *nHII, const double *ne, const
 
 int lyd_cfl_dt(lyd_ctx *c, double ct, const double *u_r, const double *u_Z, double cfl, double *dt_out) {
     if (!c || !u_r || !u_Z || !dt_out) return LYD_ERR_ARG;
+    LYD_TRY(single_cloud(c, "lyd_cfl_dt"));
     cudaSetDevice(c->dev);
-    if (!c->geom_set) return fail(c, LYD_ERR_STATE, "geometry not set");
+    if (!all_have(c, BIT_GEOM)) return fail(c, LYD_ERR_STATE, "geometry not set");
     double *d = nullptr;
     LYD_TRY(dalloc(c, (void **)&d, c->ncell * 2 * 8));
     int r = h2d(c, d, u_r, c->ncell);
     if (r == LYD_OK) r = h2d(c, d + c->ncell, u_Z, c->ncell);
     double m = 0.0;
     if (r == LYD_OK) {
-        launch_cfl(c->r_if, c->Z_if, d, d + c->ncell, c->nr, c->nz, ct, c->small, c->st);
+        launch_cfl(c->r_if, c->Z_if, d, d + c->ncell, c->nr[0], c->nz[0], ct, c->small, c->st);
         cudaError_t e = cudaMemcpyAsync(&m, c->small, 8, cudaMemcpyDeviceToHost, c->st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
         if (e != cudaSuccess) r = fail(c, LYD_ERR_CUDA, cudaGetErrorString(e));
@@ -794,16 +1065,18 @@ int lyd_cfl_dt(lyd_ctx *c, double ct, const double *u_r, const double *u_Z, doub
     return r;
 }
 
-int lyd_edge_spectra(lyd_ctx *c, double *raw, double *norm, int32_t *ridx, int32_t *zidx) {
+int lyd_edge_spectra_cloud(lyd_ctx *c, int32_t q, double *raw, double *norm, int32_t *ridx, int32_t *zidx) {
     if (!c || !raw || !norm) return LYD_ERR_ARG;
+    LYD_TRY(bad_cloud(c, q));
     cudaSetDevice(c->dev);
     if (!c->freq_set) return fail(c, LYD_ERR_STATE, "frequency grid not set");
-    int ne = lyd_edge_count(c->nr, c->nz);
+    const int nr = c->nr[q], nz = c->nz[q];
+    int ne = lyd_edge_count(nr, nz);
     if (ne <= 0) return fail(c, LYD_ERR_ARG, "grid too small for the edge ring");
     size_t n = (size_t)ne * c->nnu;
     double *d = nullptr;
     LYD_TRY(dalloc(c, (void **)&d, 2 * n * 8));
-    launch_edge(c->prec, Jc(c, 0), c->dnu, c->nnu, c->nr, c->nz, c->jscale, d, d + n, c->st);
+    launch_edge(c->prec, at(Jc(c, 0), c->desc[q].o3, c->ssz), c->dnu, c->nnu, nr, nz, c->jscale, d, d + n, c->st);
     int r = LYD_OK;
     cudaError_t e = cudaMemcpyAsync(raw, d, n * 8, cudaMemcpyDeviceToHost, c->st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(norm, d + n, n * 8, cudaMemcpyDeviceToHost, c->st);
@@ -811,11 +1084,17 @@ int lyd_edge_spectra(lyd_ctx *c, double *raw, double *norm, int32_t *ridx, int32
     if (e != cudaSuccess) r = fail(c, LYD_ERR_CUDA, cudaGetErrorString(e));
     cudaFree(d);
     if (r != LYD_OK) return r;
-    int q = 0;
-    for (int j = 1; j <= c->nz - 2; j++, q++) { if (ridx) ridx[q] = c->nr - 2; if (zidx) zidx[q] = j; }
-    for (int i = 1; i <= c->nr - 3; i++, q++) { if (ridx) ridx[q] = i; if (zidx) zidx[q] = c->nz - 2; }
-    for (int i = 1; i <= c->nr - 3; i++, q++) { if (ridx) ridx[q] = i; if (zidx) zidx[q] = 1; }
+    int k = 0;
+    for (int j = 1; j <= nz - 2; j++, k++) { if (ridx) ridx[k] = nr - 2; if (zidx) zidx[k] = j; }
+    for (int i = 1; i <= nr - 3; i++, k++) { if (ridx) ridx[k] = i; if (zidx) zidx[k] = nz - 2; }
+    for (int i = 1; i <= nr - 3; i++, k++) { if (ridx) ridx[k] = i; if (zidx) zidx[k] = 1; }
     return check_err(c);
+}
+
+int lyd_edge_spectra(lyd_ctx *c, double *raw, double *norm, int32_t *ridx, int32_t *zidx) {
+    if (!c || !raw || !norm) return LYD_ERR_ARG;
+    LYD_TRY(single_cloud(c, "lyd_edge_spectra"));
+    return lyd_edge_spectra_cloud(c, 0, raw, norm, ridx, zidx);
 }
 
 int lyd_voigt_tables(double *out, int32_t n, double xmax) {
@@ -823,4 +1102,3 @@ int lyd_voigt_tables(double *out, int32_t n, double xmax) {
     build_voigt_lut(out, n, xmax);
     return LYD_OK;
 }
-

@@ -130,7 +130,7 @@ __device__ __forceinline__ double voigt_intH(const Lut &L, double x, double a) {
 
 // Update_Hvoigt!, src/ConstantsAndFunctions.jl:319-357 (one thread per cell and bin)
 template <typename S>
-__global__ void k_hvoigt(S *Hv, const double *T, const double *nu, const double *nuC, int nnu, int ncell, Lut L) {
+__global__ void k_hvoigt(S *Hv, const double *T, const double *nu, const double *nuC, int nnu, size_t ncell, Lut L) {
     size_t n = (size_t)nnu * ncell;
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
         int k = (int)(q % nnu);
@@ -147,7 +147,7 @@ __global__ void k_hvoigt(S *Hv, const double *T, const double *nu, const double 
     }
 }
 
-void launch_hvoigt(int prec, void *Hv, const double *T, const double *nu, const double *nuC, int nnu, int ncell,
+void launch_hvoigt(int prec, void *Hv, const double *T, const double *nu, const double *nuC, int nnu, size_t ncell,
                    const double *lut, int lut_n, double lut_xmax, cudaStream_t st) {
     Lut L;
     L.y = lut; L.n = lut_n; L.xmax = lut_xmax; L.xmin = -lut_xmax;
@@ -159,16 +159,16 @@ void launch_hvoigt(int prec, void *Hv, const double *T, const double *nu, const 
 
 // Update_phi_nu!, src/ConstantsAndFunctions.jl:362-393: per-cell 1 / sum_{kmin..kmax} dnu Hv
 template <typename S>
-__global__ void k_phi_inv(const S *Hv, const double *dnu, int nnu, int ncell, int kmin, int kmax, double *out) {
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+__global__ void k_phi_inv(const S *Hv, const double *dnu, int nnu, size_t ncell, int kmin, int kmax, double *out) {
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < ncell; c += (size_t)gridDim.x * blockDim.x) {
         double s = 0.0;
         for (int k = kmin; k <= kmax; k++) s += dnu[k] * double(Hv[(size_t)c * nnu + k]);
         out[c] = 1.0 / s;
     }
 }
-void launch_phi_inv(int prec, const void *Hv, const double *dnu, int nnu, int ncell, int kmin, int kmax,
+void launch_phi_inv(int prec, const void *Hv, const double *dnu, int nnu, size_t ncell, int kmin, int kmax,
                     double *phi_inv, cudaStream_t st) {
-    int g = grid_for((size_t)ncell);
+    int g = grid_for(ncell);
     if (prec == 0) k_phi_inv<double><<<g, 256, 0, st>>>(static_cast<const double *>(Hv), dnu, nnu, ncell, kmin, kmax, phi_inv);
     else k_phi_inv<float><<<g, 256, 0, st>>>(static_cast<const float *>(Hv), dnu, nnu, ncell, kmin, kmax, phi_inv);
 }

@@ -1,11 +1,31 @@
 // lyd_internal.h -- device-side argument blocks and launch wrappers of the Lyman-alpha
-// step kernels (shared by lyd_kernels.cu and lyd_api.cu).
+// step kernels (shared by lyd_kernels.cu, lyd_aux.cu and lyd_api.cu).
+//
+// A context holds one or more independent clouds ("a batch"). Every field of every cloud
+// lives in one concatenated device array per field; a CloudDesc gives each cloud's offsets,
+// grid size, boundary conditions and time step. The step kernels walk work lists:
+// advection tiles (cloud, i0, j0, k0) and frequency-kernel items (cloud, first cell, end
+// cell). A single cloud is a batch of one.
 #pragma once
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
 
 namespace lyd {
+
+struct CloudDesc {
+    long long o3;        // offset of the (k, i, j) fields, in cell-bins
+    long long oc;        // offset of the per-cell fields
+    long long orf;       // offset of the r-face fields ((n_r+1) n_z: A_r, u*_r)
+    long long ozf;       // offset of the Z-face fields (n_r (n_z+1): A_Z, u*_Z)
+    int ocol, orow;      // per-column (n_r: <1/r>, rCoM) and per-row (n_z: ZCoM) fields
+    int orint, ozint;    // PLM intervals per face ((n_r+1)*5, (n_z+1)*5)
+    int orif, ozif;      // interface coordinates (n_r+1, n_z+1)
+    int nr, nz;
+    int bc_r_right, bc_z_bot, bc_z_top;
+    int pb0, npb;        // this cloud's blocks in the frequency-kernel work list / partials
+    double ctdt, dt, c_tilde, z_center;
+};
 
 // Columns of the per-block reduction partials written by the step kernels:
 // [0, nnu)        E_bin(k)  = sum dnu_k max(J - 10 Jeps, 0) dV          (FindActiveBins)
@@ -18,7 +38,7 @@ constexpr int kExtraCols = 6;
 enum { PART_ACTIVE = 1, PART_DIAG = 2 };
 
 // Advection: AdvectJandH_Cylindrical! (src/AdvectJandH.jl:526-1390), reads set `in`,
-// writes set `out`. Bins outside the active window are copied through.
+// writes set `out`. Bins outside each cloud's active window are copied through.
 template <typename S>
 struct AdvArgs {
     const S *J, *Hr, *HZ;
@@ -27,14 +47,15 @@ struct AdvArgs {
     const S *Hv;
     const double *alpha, *alpha_cF;
     const double *A_r, *A_Z, *inv_dV, *inv_r_cell;
-    const double *rint, *zint;   // PLM intervals per face, [(n+1)][5]
+    const double *rint, *zint;   // PLM intervals per face, [(n+1)][5] per cloud
     const double *u_r_star, *u_Z_star;
     const double *dur_dr, *dur_dZ, *duZ_dr, *duZ_dZ, *ur_over_r;
-    const int *kwin;             // device {kmin, kmax}
-    int nnu, nr, nz;
-    double ctdt;
+    const int *kwin;             // device {kmin, kmax} per cloud
+    const CloudDesc *cl;
+    const int4 *tiles;           // (cloud, i0, j0, k0)
+    int rows;                    // rows per tile
+    int nnu;
     double jeps, heps2;          // closure floors in storage units
-    int bc_r_right, bc_z_bot, bc_z_top;
 };
 
 // Emission/absorption + frequency step + flux correction (+ partial reductions).
@@ -56,49 +77,55 @@ struct FreqArgs {
     double *Fkp, *Fk, *Fkm;      // stored frequency factors (nullptr: not kept)
     const double *nu, *nuC, *dnu, *inv_dnu, *inv_nuC;
     const double *dV, *A_r, *A_Z, *rCoM, *ZCoM;
-    double c_tilde, dt, ctdt, z_center;
+    const CloudDesc *cl;
+    const int4 *items;           // (cloud, first cell, end cell) per block
     double alpha_floor;
     double jeps, heps2, j_scale;
     int do_emission, do_freq, update_ff, recoil;
-    int bc_z_bot;
     int parts;                   // PART_* bits
     double *partials;            // [ncols][nblocks]
     int *err;                    // device error bits
-    int nnu, nr, nz;
+    int nnu;
+    int solver;                  // SOLVER_*
 };
 
-// Reduction of the partials into kmin/kmax and the step diagnostics.
+enum { SOLVER_PCR = 0, SOLVER_THOMAS = 1 };
+
+// Reduction of the partials into each cloud's kmin/kmax and step diagnostics (one CTA per
+// cloud).
 struct RedArgs {
     const double *partials;
-    int nblocks, nnu;
+    int nblocks;                 // total frequency-kernel blocks (partial stride)
+    int nnu, nclouds;
     int parts;
     int kcore_min, kcore_max;
-    double dt, c_tilde, j_scale;
-    int bc_z_bot;
-    int *kwin;                   // out {kmin, kmax}
-    double *diag;                // out: per-step record base (7 doubles per step), or nullptr
-    int *step_counter;           // index of the record to write (incremented)
-    int hist_capacity;
-    double *last;                // out: the latest record (7 doubles)
-    int *err;
+    double j_scale;
+    const CloudDesc *cl;
+    int *kwin;                   // out {kmin, kmax} per cloud
+    double *diag;                // out: [step][cloud][7], or nullptr
+    int *step_counter;           // record index (incremented once per launch)
+    int *done;                   // completion counter of the CTAs of one launch
+    int hist_capacity;           // steps
+    double *last;                // out: latest record per cloud [cloud][7]
 };
 
 // error bits
 enum { ERRB_NONFINITE = 1, ERRB_SOLVE = 2 };
 
-void launch_find_active(int prec, const void *J, int nnu, int nr, int nz, const double *dnu, const double *dV,
-                        double jeps, double *partials, int nblocks, cudaStream_t st);
-void launch_advect(int prec, int flux, const void *args, int nnu, int nr, int nz, cudaStream_t st);
-void launch_freq(int prec, const void *args, int nnu, int ncell, int nblocks, cudaStream_t st);
+int bins_per_lane(int nnu);
+void launch_find_active(int prec, const void *J, int nnu, const double *dnu, const double *dV, const CloudDesc *cl,
+                        const int4 *items, int nitems, double jeps, double *partials, cudaStream_t st);
+void launch_advect(int prec, int flux, const void *args, int ntiles, cudaStream_t st);
+void launch_freq(int prec, const void *args, int nnu, int nitems, cudaStream_t st);
 void launch_reduce(const RedArgs &a, cudaStream_t st);
 int freq_blocks(int ncell, int dev);
 
 // auxiliary kernels (lyd_aux.cu)
 void launch_convert_in(int prec, const double *src, void *dst, size_t n, double scale, cudaStream_t st);
 void launch_convert_out(int prec, const void *src, double *dst, size_t n, double scale, cudaStream_t st);
-void launch_hvoigt(int prec, void *Hv, const double *T, const double *nu, const double *nuC, int nnu, int ncell,
+void launch_hvoigt(int prec, void *Hv, const double *T, const double *nu, const double *nuC, int nnu, size_t ncell,
                    const double *lut, int lut_n, double lut_xmax, cudaStream_t st);
-void launch_phi_inv(int prec, const void *Hv, const double *dnu, int nnu, int ncell, int kmin, int kmax,
+void launch_phi_inv(int prec, const void *Hv, const double *dnu, int nnu, size_t ncell, int kmin, int kmax,
                     double *phi_inv, cudaStream_t st);
 void launch_pd(size_t n, const double *nHII, const double *ne, const double *nHI, const double *nHeI,
                const double *nH2, const double *T, double z, double *out, cudaStream_t st);

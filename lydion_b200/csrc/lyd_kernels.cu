@@ -1,20 +1,20 @@
 // lyd_kernels.cu -- the hot kernels of the Lyman-alpha M1 step on sm_100a.
 //
-//  k_advect   AdvectJandH_Cylindrical! (src/AdvectJandH.jl:526-1390) as ONE kernel: a CTA
-//             owns an 8x4 (r x Z) tile of cells and a 32-bin slice of frequencies (one bin
-//             per lane, k innermost so every warp load is a contiguous 256 B / 128 B run).
-//             Face fluxes of the tile are computed once into shared memory, then each cell
-//             is updated from them: the six face-flux arrays and the two K_phiphi arrays
-//             of the reference never touch HBM. Ghost cells of the four boundaries are
-//             produced on the fly from the boundary conditions.
-//  k_freq     LyaEmissionAbsorptionUpdate! + UpdateFreqFactors! + the per-cell tridiagonal
-//             solve + the flux correction of FrequencyUpdateJLya_AllCells! fused per cell:
-//             one warp owns one cell's whole spectrum (M contiguous bins per lane), the
-//             k +- 1 couplings travel by warp shuffles, and the tridiagonal system is solved
-//             in FP64 by parallel cyclic reduction across the warp. The epilogue
-//             accumulates the next step's FindActiveBins energies and the step diagnostics
-//             into per-CTA partials (fixed order, so results are run-to-run deterministic).
-//  k_reduce   sums the partials (one warp per column) and derives kmin/kmax, M_F, L, f_esc.
+//  k_advect   AdvectJandH_Cylindrical! (src/AdvectJandH.jl:526-1390) as ONE kernel. A CTA owns a
+//             tile of 8 columns (r) x `rows` rows (Z) x 32 bins (one bin per lane, k innermost,
+//             so every warp load is a contiguous 256 B / 128 B run) of one cloud and marches up
+//             the tile row by row. Face fluxes never touch HBM: the six face-flux arrays and the
+//             two K_phiphi arrays of the reference are replaced by shared memory and registers.
+//             Ghost cells of the four boundaries are produced on the fly from the boundary
+//             conditions.
+//  k_freq     LyaEmissionAbsorptionUpdate! + UpdateFreqFactors! + the per-cell tridiagonal solve
+//             + the flux correction of FrequencyUpdateJLya_AllCells!, fused per cell: one warp
+//             owns one cell's whole spectrum (M contiguous bins per lane), the k +- 1 couplings
+//             travel by warp shuffles, and the tridiagonal system is solved in FP64, by parallel
+//             cyclic reduction across the warp or by a lane-serial elimination. The epilogue
+//             accumulates the next step's FindActiveBins energies and the step diagnostics into
+//             per-CTA partials (fixed order, so results are run-to-run deterministic).
+//  k_reduce   one CTA per cloud sums that cloud's partials and derives kmin/kmax, M_F, L, f_esc.
 #include <cuda_runtime.h>
 
 #include "lyd_internal.h"
@@ -24,9 +24,24 @@ namespace lyd {
 
 constexpr int FREQ_THREADS = 256;
 
+// Per-CTA view of one cloud of a batch.
+struct View {
+    long long o3, oc, orf, ozf;
+    int ocol, orow, orint, ozint;
+    int nr, nz, bcr, bzb, bzt;
+    double ctdt;
+};
+
+__device__ __forceinline__ void load_view(const CloudDesc &d, View &v) {
+    v.o3 = d.o3; v.oc = d.oc; v.orf = d.orf; v.ozf = d.ozf;
+    v.ocol = d.ocol; v.orow = d.orow; v.orint = d.orint; v.ozint = d.ozint;
+    v.nr = d.nr; v.nz = d.nz; v.bcr = d.bc_r_right; v.bzb = d.bc_z_bot; v.bzt = d.bc_z_top;
+    v.ctdt = d.ctdt;
+}
+
 template <typename S, typename R>
-__device__ __forceinline__ Cell<R> ld_cell(const AdvArgs<S> &a, int i, int j, int k) {
-    size_t x = (size_t)k + (size_t)a.nnu * ((size_t)i + (size_t)a.nr * (size_t)j);
+__device__ __forceinline__ Cell<R> ld_cell(const AdvArgs<S> &a, const View &v, int i, int j, int k) {
+    long long x = v.o3 + (long long)k + (long long)a.nnu * ((long long)i + (long long)v.nr * j);
     Cell<R> c;
     c.J = R(__ldg(a.J + x));
     c.Hr = R(__ldg(a.Hr + x));
@@ -37,97 +52,96 @@ __device__ __forceinline__ Cell<R> ld_cell(const AdvArgs<S> &a, int i, int j, in
 // Radial stencil cell with the ghost cells of src/AdvectJandH.jl:662-673 (axis, always
 // reflecting) and 853-871 (outer boundary, reflecting or outflow).
 template <typename S, typename R>
-__device__ __forceinline__ Cell<R> r_cell(const AdvArgs<S> &a, int idx, int j, int k) {
+__device__ __forceinline__ Cell<R> r_cell(const AdvArgs<S> &a, const View &v, int idx, int j, int k) {
     if (idx < 0) {
-        Cell<R> c = ld_cell<S, R>(a, -1 - idx, j, k);
+        Cell<R> c = ld_cell<S, R>(a, v, -1 - idx, j, k);
         c.Hr = -c.Hr;
         return c;
     }
-    if (idx >= a.nr) {
-        if (a.bc_r_right == 0) {
-            Cell<R> c = ld_cell<S, R>(a, 2 * a.nr - 1 - idx, j, k);
+    if (idx >= v.nr) {
+        if (v.bcr == 0) {
+            Cell<R> c = ld_cell<S, R>(a, v, 2 * v.nr - 1 - idx, j, k);
             c.Hr = -c.Hr;
             return c;
         }
-        Cell<R> c = ld_cell<S, R>(a, a.nr - 1, j, k);
+        Cell<R> c = ld_cell<S, R>(a, v, v.nr - 1, j, k);
         c.Hr = c.Hr > R(0) ? c.Hr : R(0);
         return c;
     }
-    return ld_cell<S, R>(a, idx, j, k);
+    return ld_cell<S, R>(a, v, idx, j, k);
 }
 
 // Vertical stencil cell with the ghost cells of src/AdvectJandH.jl:1000-1018 (bottom) and
 // 1185-1203 (top).
 template <typename S, typename R>
-__device__ __forceinline__ Cell<R> z_cell(const AdvArgs<S> &a, int i, int idx, int k) {
+__device__ __forceinline__ Cell<R> z_cell(const AdvArgs<S> &a, const View &v, int i, int idx, int k) {
     if (idx < 0) {
-        if (a.bc_z_bot == 0) {
-            Cell<R> c = ld_cell<S, R>(a, i, -1 - idx, k);
+        if (v.bzb == 0) {
+            Cell<R> c = ld_cell<S, R>(a, v, i, -1 - idx, k);
             c.HZ = -c.HZ;
             return c;
         }
-        Cell<R> c = ld_cell<S, R>(a, i, 0, k);
+        Cell<R> c = ld_cell<S, R>(a, v, i, 0, k);
         c.HZ = c.HZ < R(0) ? c.HZ : R(0);
         return c;
     }
-    if (idx >= a.nz) {
-        if (a.bc_z_top == 0) {
-            Cell<R> c = ld_cell<S, R>(a, i, 2 * a.nz - 1 - idx, k);
+    if (idx >= v.nz) {
+        if (v.bzt == 0) {
+            Cell<R> c = ld_cell<S, R>(a, v, i, 2 * v.nz - 1 - idx, k);
             c.HZ = -c.HZ;
             return c;
         }
-        Cell<R> c = ld_cell<S, R>(a, i, a.nz - 1, k);
+        Cell<R> c = ld_cell<S, R>(a, v, i, v.nz - 1, k);
         c.HZ = c.HZ > R(0) ? c.HZ : R(0);
         return c;
     }
-    return ld_cell<S, R>(a, i, idx, k);
+    return ld_cell<S, R>(a, v, i, idx, k);
 }
 
 // alpha_F of an in-grid cell: explicit array, or alpha*H_voigt (+ alpha_cF) as set up by
 // src/StaticCloudTest.jl:283-285 and PhotoThermoChemistry.jl:2151.
 template <typename S, typename R>
-__device__ __forceinline__ R alpha_F(const AdvArgs<S> &a, int i, int j, int k) {
-    size_t c = (size_t)i + (size_t)a.nr * (size_t)j;
-    size_t x = (size_t)k + (size_t)a.nnu * c;
+__device__ __forceinline__ R alpha_F(const AdvArgs<S> &a, const View &v, int i, int j, int k) {
+    long long c = v.oc + (long long)i + (long long)v.nr * j;
+    long long x = v.o3 + (long long)k + (long long)a.nnu * ((long long)i + (long long)v.nr * j);
     if (a.aF) return R(__ldg(a.aF + x));
-    R v = R(__ldg(a.alpha + c)) * R(__ldg(a.Hv + x));
-    if (a.alpha_cF) v = v + R(__ldg(a.alpha_cF + c));
-    return v;
+    R val = R(__ldg(a.alpha + c)) * R(__ldg(a.Hv + x));
+    if (a.alpha_cF) val = val + R(__ldg(a.alpha_cF + c));
+    return val;
 }
 
-// ---- k_advect: one CTA = 8 columns (r) x ROWS rows (Z) x 32 bins, marching up in Z ----------
+// ---- k_advect: one CTA = 8 columns (r) x `rows` rows (Z) x 32 bins, marching up in Z --------
 //
-// A ring of four rows holds, for the 8 own columns and the 2 + 2 halo columns of each row,
-// the cell values every face needs: J, the reduced fluxes H/max(J, Jeps) and alpha_F (so the
+// A ring of four rows holds, for the 8 own columns and the 2 + 2 halo columns of each row, the
+// cell values every face needs: J, the reduced fluxes H/max(J, Jeps) and alpha_F (so the
 // reciprocal of J is taken once per cell, not once per face), plus the raw H of the own
-// columns for the cell update. Warp w (0..7) owns column i0+w; warp 8 stages the halo
-// columns and computes the tile's rightmost r face. Per row: stage row j+2 -> sync -> every
-// warp computes the r face on its left (warp 8: the right edge) into shared memory and its
-// Z face j+1/2 into registers -> sync -> the cell update of row j uses the two r faces from
-// shared memory and the Z faces j-1/2 (carried from the previous row) and j+1/2.
+// columns for the cell update. Warp w (0..7) owns column i0+w; warp 8 stages the halo columns
+// and computes the tile's rightmost r face. Per row: stage row j+2 -> sync -> every warp
+// computes the r face on its left (warp 8: the right edge) into shared memory and its Z face
+// j+1/2 into registers -> sync -> the cell update of row j uses the two r faces from shared
+// memory and the Z faces j-1/2 (carried from the previous row) and j+1/2.
 constexpr int MT = 8;                  // own columns per CTA
 constexpr int MWARPS = MT + 1;
 constexpr int MTHREADS = 32 * MWARPS;
 constexpr int MCOL = MT + 4;           // staged columns i0-2 .. i0+MT+1
 constexpr int RING = 4;
-constexpr int MROWS = 16;              // rows per CTA
 
 template <typename S, typename R>
-__device__ __forceinline__ Cell<R> raw_cell(const AdvArgs<S> &a, int col, int row, int k) {
-    if (col < 0 || col >= a.nr) return r_cell<S, R>(a, col, row, k);
-    if (row < 0 || row >= a.nz) return z_cell<S, R>(a, col, row, k);
-    return ld_cell<S, R>(a, col, row, k);
+__device__ __forceinline__ Cell<R> raw_cell(const AdvArgs<S> &a, const View &v, int col, int row, int k) {
+    if (col < 0 || col >= v.nr) return r_cell<S, R>(a, v, col, row, k);
+    if (row < 0 || row >= v.nz) return z_cell<S, R>(a, v, col, row, k);
+    return ld_cell<S, R>(a, v, col, row, k);
 }
 
 // Stage cell (col, row) into ring slot `slot`, staged column lc (= col - i0 + 2).
 template <typename S, typename R>
-__device__ __forceinline__ void stage_cell(const AdvArgs<S> &a, R *A, R *Hh, int slot, int lc, int col, int row,
-                                           int k, int lane, R jeps) {
-    Cell<R> c = raw_cell<S, R>(a, col, row, k);
+__device__ __forceinline__ void stage_cell(const AdvArgs<S> &a, const View &v, R *A, R *Hh, int slot, int lc,
+                                           int col, int row, int k, int lane, R jeps) {
+    Cell<R> c = raw_cell<S, R>(a, v, col, row, k);
     CellF<R> f = cell_f<R>(c.J, c.Hr, c.HZ, jeps);
-    int cc = col < 0 ? 0 : (col >= a.nr ? a.nr - 1 : col);
-    int rr = row < 0 ? 0 : (row >= a.nz ? a.nz - 1 : row);
-    R aF = alpha_F<S, R>(a, cc, rr, k);
+    int cc = col < 0 ? 0 : (col >= v.nr ? v.nr - 1 : col);
+    int rr = row < 0 ? 0 : (row >= v.nz ? v.nz - 1 : row);
+    R aF = alpha_F<S, R>(a, v, cc, rr, k);
     R *p = A + ((slot * MCOL + lc) * 4) * 32 + lane;
     p[0] = f.J; p[32] = f.fr; p[64] = f.fZ; p[96] = aF;
     if (lc >= 2 && lc < 2 + MT) {
@@ -148,8 +162,8 @@ __device__ __forceinline__ CellF<R> staged(const R *A, int slot, int lc, int lan
 // r face f (between cells f-1 and f) of row j held in ring slot `slot`; wl = f - i0 is the
 // staged column of the stencil's first cell (src/AdvectJandH.jl:641-968).
 template <typename S, typename R, int FLUX>
-__device__ __forceinline__ void face_r_staged(const AdvArgs<S> &a, const R *A, int slot, int wl, int f, int j,
-                                              int lane, R jeps, R *F, R &kL, R &kR) {
+__device__ __forceinline__ void face_r_staged(const AdvArgs<S> &a, const View &v, const R *A, int slot, int wl,
+                                              int f, int j, int lane, R jeps, R *F, R &kL, R &kR) {
     R d0, aFi, aFp, d3;
     CellF<R> cm1 = staged<R>(A, slot, wl, lane, d0);
     CellF<R> ci = staged<R>(A, slot, wl + 1, lane, aFi);
@@ -157,7 +171,7 @@ __device__ __forceinline__ void face_r_staged(const AdvArgs<S> &a, const R *A, i
     CellF<R> cp2 = staged<R>(A, slot, wl + 3, lane, d3);
     R iv[5];
 #pragma unroll
-    for (int t = 0; t < 5; t++) iv[t] = R(__ldg(a.rint + 5 * f + t));
+    for (int t = 0; t < 5; t++) iv[t] = R(__ldg(a.rint + v.orint + 5 * f + t));
     Recon<R> q = reconstruct_f<R>(cm1, ci, cp1, cp2, iv, aFi, aFp, jeps);
     R DrrL, DZZL, DrZL, DrrR, DZZR, DrZR;
     D_from_f_n<R>(q.f_L, q.nr_L, q.nZ_L, DrrL, DZZL, DrZL);
@@ -165,7 +179,7 @@ __device__ __forceinline__ void face_r_staged(const AdvArgs<S> &a, const R *A, i
     R FJ, FHr, FHZ;
     m1_flux<R, FLUX, false>(q.Hr_L, q.Hr_R, DrrL * q.J_L, DrrR * q.J_R, DrZL * q.J_L, DrZR * q.J_R, q, ci.J, cp1.J,
                             FJ, FHr, FHZ);
-    R uc = R(__ldg(a.u_r_star + f + (size_t)(a.nr + 1) * j) * kInvC);
+    R uc = R(__ldg(a.u_r_star + v.orf + f + (long long)(v.nr + 1) * j) * kInvC);
     F[0] = FJ + adv_flux(uc, q.J_L, q.J_R);
     F[1] = FHr + adv_flux(uc, q.Hr_L, q.Hr_R);
     F[2] = FHZ + adv_flux(uc, q.HZ_L, q.HZ_R);
@@ -175,8 +189,8 @@ __device__ __forceinline__ void face_r_staged(const AdvArgs<S> &a, const R *A, i
 
 // Z face f (between rows f-1 and f) of column i, staged column lc (src/AdvectJandH.jl:978-1289).
 template <typename S, typename R, int FLUX>
-__device__ __forceinline__ void face_z_staged(const AdvArgs<S> &a, const R *A, int lc, int i, int f, int lane,
-                                              R jeps, R *F) {
+__device__ __forceinline__ void face_z_staged(const AdvArgs<S> &a, const View &v, const R *A, int lc, int i, int f,
+                                              int lane, R jeps, R *F) {
     R d0, aFi, aFp, d3;
     CellF<R> cm1 = staged<R>(A, (f + 2) & (RING - 1), lc, lane, d0);     // row f-2
     CellF<R> ci = staged<R>(A, (f + 3) & (RING - 1), lc, lane, aFi);     // row f-1
@@ -184,7 +198,7 @@ __device__ __forceinline__ void face_z_staged(const AdvArgs<S> &a, const R *A, i
     CellF<R> cp2 = staged<R>(A, (f + 1) & (RING - 1), lc, lane, d3);     // row f+1
     R iv[5];
 #pragma unroll
-    for (int t = 0; t < 5; t++) iv[t] = R(__ldg(a.zint + 5 * f + t));
+    for (int t = 0; t < 5; t++) iv[t] = R(__ldg(a.zint + v.ozint + 5 * f + t));
     Recon<R> q = reconstruct_f<R>(cm1, ci, cp1, cp2, iv, aFi, aFp, jeps);
     R DrrL, DZZL, DrZL, DrrR, DZZR, DrZR;
     D_from_f_n<R>(q.f_L, q.nr_L, q.nZ_L, DrrL, DZZL, DrZL);
@@ -192,7 +206,7 @@ __device__ __forceinline__ void face_z_staged(const AdvArgs<S> &a, const R *A, i
     R FJ, FHr, FHZ;
     m1_flux<R, FLUX, true>(q.HZ_L, q.HZ_R, DrZL * q.J_L, DrZR * q.J_R, DZZL * q.J_L, DZZR * q.J_R, q, ci.J, cp1.J,
                            FJ, FHr, FHZ);
-    R uc = R(__ldg(a.u_Z_star + i + (size_t)a.nr * f) * kInvC);
+    R uc = R(__ldg(a.u_Z_star + v.ozf + i + (long long)v.nr * f) * kInvC);
     F[0] = FJ + adv_flux(uc, q.J_L, q.J_R);
     F[1] = FHr + adv_flux(uc, q.Hr_L, q.Hr_R);
     F[2] = FHZ + adv_flux(uc, q.HZ_L, q.HZ_R);
@@ -205,10 +219,13 @@ __global__ void __launch_bounds__(MTHREADS, 2) k_advect(AdvArgs<S> a) {
     R *Hh = A + RING * MCOL * 4 * 32;                     // [RING][MT][2][32]
     R *Fr = Hh + RING * MT * 2 * 32;                      // [MT+1][5][32]
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int i0 = blockIdx.x * MT, j0 = blockIdx.y * MROWS, kb = blockIdx.z * 32;
-    const int j1 = (j0 + MROWS < a.nz) ? j0 + MROWS : a.nz;
+    const int4 t = a.tiles[blockIdx.x];
+    View v;
+    load_view(a.cl[t.x], v);
+    const int i0 = t.y, j0 = t.z, kb = t.w;
+    const int j1 = (j0 + a.rows < v.nz) ? j0 + a.rows : v.nz;
     const int k = kb + lane;
-    const int kmin = a.kwin[0], kmax = a.kwin[1];
+    const int kmin = a.kwin[2 * t.x], kmax = a.kwin[2 * t.x + 1];
     const bool kact = (k >= kmin) && (k <= kmax) && (k < a.nnu);
     const bool chunk_act = (kb <= kmax) && (kb + 31 >= kmin);
     const R jeps = R(a.jeps);
@@ -216,9 +233,9 @@ __global__ void __launch_bounds__(MTHREADS, 2) k_advect(AdvArgs<S> a) {
     const bool own = (w < MT);
 
     if (!chunk_act) {
-        if (own && col < a.nr && k < a.nnu) {
+        if (own && col < v.nr && k < a.nnu) {
             for (int j = j0; j < j1; j++) {
-                size_t x = (size_t)k + (size_t)a.nnu * ((size_t)col + (size_t)a.nr * j);
+                long long x = v.o3 + (long long)k + (long long)a.nnu * ((long long)col + (long long)v.nr * j);
                 a.Jo[x] = a.J[x]; a.Hro[x] = a.Hr[x]; a.HZo[x] = a.HZ[x];
             }
         }
@@ -226,33 +243,33 @@ __global__ void __launch_bounds__(MTHREADS, 2) k_advect(AdvArgs<S> a) {
     }
 
     // prologue: own columns, rows j0-2 .. j0+1
-    if (own && kact && col <= a.nr + 1) {
+    if (own && kact && col <= v.nr + 1) {
         for (int r = j0 - 2; r <= j0 + 1; r++) {
-            bool gcol = col >= a.nr, grow = (r < 0 || r >= a.nz);
-            if (r < -2 || r > a.nz + 1 || (gcol && grow)) continue;
-            stage_cell<S, R>(a, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps);
+            bool gcol = col >= v.nr, grow = (r < 0 || r >= v.nz);
+            if (r < -2 || r > v.nz + 1 || (gcol && grow)) continue;
+            stage_cell<S, R>(a, v, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps);
         }
     }
     __syncthreads();
     R zL[3] = {R(0), R(0), R(0)};
-    if (own && kact && col < a.nr) face_z_staged<S, R, FLUX>(a, A, w + 2, col, j0, lane, jeps, zL);
+    if (own && kact && col < v.nr) face_z_staged<S, R, FLUX>(a, v, A, w + 2, col, j0, lane, jeps, zL);
 
-    const double ctdt = a.ctdt;
+    const double ctdt = v.ctdt;
     const double ctdt_c = ctdt * kInvC;
     for (int j = j0; j < j1; j++) {
         // (A) stage row j+2 of the own column; warp 8 stages the halo columns of row j
         if (kact) {
             if (own) {
                 int r = j + 2;
-                bool gcol = col >= a.nr, grow = r >= a.nz;
-                if (col <= a.nr + 1 && r <= a.nz + 1 && !(gcol && grow))
-                    stage_cell<S, R>(a, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps);
+                bool gcol = col >= v.nr, grow = r >= v.nz;
+                if (col <= v.nr + 1 && r <= v.nz + 1 && !(gcol && grow))
+                    stage_cell<S, R>(a, v, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps);
             } else {
                 const int hl[4] = {0, 1, MT + 2, MT + 3};
 #pragma unroll
-                for (int t = 0; t < 4; t++) {
-                    int c2 = i0 - 2 + hl[t];
-                    if (c2 <= a.nr + 1) stage_cell<S, R>(a, A, Hh, j & (RING - 1), hl[t], c2, j, k, lane, jeps);
+                for (int q = 0; q < 4; q++) {
+                    int c2 = i0 - 2 + hl[q];
+                    if (c2 <= v.nr + 1) stage_cell<S, R>(a, v, A, Hh, j & (RING - 1), hl[q], c2, j, k, lane, jeps);
                 }
             }
         }
@@ -260,19 +277,20 @@ __global__ void __launch_bounds__(MTHREADS, 2) k_advect(AdvArgs<S> a) {
         // (B) the r face left of the own column (warp 8: the tile's right face), the Z face j+1/2
         const int f = i0 + w;
         R zR[3] = {R(0), R(0), R(0)};
-        if (kact && f <= a.nr) {
+        if (kact && f <= v.nr) {
             R F[3], kL, kR;
-            face_r_staged<S, R, FLUX>(a, A, j & (RING - 1), w, f, j, lane, jeps, F, kL, kR);
+            face_r_staged<S, R, FLUX>(a, v, A, j & (RING - 1), w, f, j, lane, jeps, F, kL, kR);
             R *p = Fr + (w * 5) * 32 + lane;
             p[0] = F[0]; p[32] = F[1]; p[64] = F[2]; p[96] = kL; p[128] = kR;
         }
-        if (own && kact && col < a.nr) face_z_staged<S, R, FLUX>(a, A, w + 2, col, j + 1, lane, jeps, zR);
+        if (own && kact && col < v.nr) face_z_staged<S, R, FLUX>(a, v, A, w + 2, col, j + 1, lane, jeps, zR);
         __syncthreads();
         // (C) cell update, src/AdvectJandH.jl:1302-1382
-        if (own && col < a.nr && k < a.nnu) {
+        if (own && col < v.nr && k < a.nnu) {
             const int i = col;
-            size_t c = (size_t)i + (size_t)a.nr * (size_t)j;
-            size_t x = (size_t)k + (size_t)a.nnu * c;
+            long long cl = (long long)i + (long long)v.nr * j;
+            long long c = v.oc + cl;
+            long long x = v.o3 + (long long)k + (long long)a.nnu * cl;
             if (!kact) {
                 a.Jo[x] = a.J[x]; a.Hro[x] = a.Hr[x]; a.HZo[x] = a.HZ[x];
             } else {
@@ -283,8 +301,9 @@ __global__ void __launch_bounds__(MTHREADS, 2) k_advect(AdvArgs<S> a) {
                 D_edd<R>(sHr, sHZ, sJ, jeps, R(a.heps2), Drr, DZZ, DrZ);
                 const R *FL = Fr + (w * 5) * 32 + lane;
                 const R *FR = FL + 5 * 32;
-                double ArL = __ldg(a.A_r + i + (size_t)(a.nr + 1) * j), ArR = __ldg(a.A_r + i + 1 + (size_t)(a.nr + 1) * j);
-                double AZL = __ldg(a.A_Z + c), AZR = __ldg(a.A_Z + c + a.nr);
+                double ArL = __ldg(a.A_r + v.orf + i + (long long)(v.nr + 1) * j);
+                double ArR = __ldg(a.A_r + v.orf + i + 1 + (long long)(v.nr + 1) * j);
+                double AZL = __ldg(a.A_Z + v.ozf + cl), AZR = __ldg(a.A_Z + v.ozf + cl + v.nr);
                 double fac = ctdt * __ldg(a.inv_dV + c);
                 R Jn, Hrn, HZn;
                 if (sizeof(R) == 8) {
@@ -304,9 +323,9 @@ __global__ void __launch_bounds__(MTHREADS, 2) k_advect(AdvArgs<S> a) {
                 R DdU = d_colon_grad_u<R>(Drr, DrZ, DZZ, ga, gb, gc, gd, ge);
                 R Kav = R(0.5) * (FL[128] + FR[96]);
                 if (sizeof(R) == 8)
-                    Hrn += R(ctdt) * Kav * R(__ldg(a.inv_r_cell + i));
+                    Hrn += R(ctdt) * Kav * R(__ldg(a.inv_r_cell + v.ocol + i));
                 else
-                    Hrn += R(ctdt * __ldg(a.inv_r_cell + i)) * Kav;
+                    Hrn += R(ctdt * __ldg(a.inv_r_cell + v.ocol + i)) * Kav;
                 R cc = R(ctdt_c);
                 R dHr = -cc * (sHr * ga + sHZ * gb);
                 R dHZ = -cc * (sHr * gc + sHZ * gd);
@@ -349,7 +368,6 @@ __device__ __forceinline__ void nbr(const double (&v)[M], double (&out)[M], int 
                 out[m] = v[mm];
             } else {
                 int src = mm < 0 ? mm + M : mm - M;
-                // src is a compile-time index after unrolling of m and s
                 double w = 0.0;
 #pragma unroll
                 for (int q = 0; q < M; q++)
@@ -405,6 +423,38 @@ __device__ __forceinline__ void pcr_solve(Row<M> &R_, int lane) {
     for (int m = 0; m < M; m++) R_.d[m] = R_.d[m] / R_.b[m];
 }
 
+// Lane-serial elimination of the same system: the warp writes its rows to shared memory and
+// lane 0 runs the forward elimination and back substitution of dgtsv's no-interchange branch
+// (the Thomas algorithm), then the rows are read back. `sm` holds 4*32*M doubles per warp.
+template <int M>
+__device__ __forceinline__ void thomas_solve(Row<M> &R_, int lane, double *sm) {
+    constexpr int N = 32 * M;
+    double *a = sm, *b = sm + N, *c = sm + 2 * N, *d = sm + 3 * N;
+#pragma unroll
+    for (int m = 0; m < M; m++) {
+        int r = lane * M + m;
+        a[r] = R_.a[m]; b[r] = R_.b[m]; c[r] = R_.c[m]; d[r] = R_.d[m];
+    }
+    __syncwarp();
+    if (lane == 0) {
+        for (int r = 1; r < N; r++) {
+            double fact = a[r] / b[r - 1];
+            b[r] = b[r] - fact * c[r - 1];
+            d[r] = d[r] - fact * d[r - 1];
+        }
+        d[N - 1] = d[N - 1] / b[N - 1];
+        for (int r = N - 2; r >= 0; r--) d[r] = (d[r] - c[r] * d[r + 1]) / b[r];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int m = 0; m < M; m++) {
+        int r = lane * M + m;
+        R_.d[m] = d[r];
+        R_.b[m] = b[r];
+    }
+    __syncwarp();
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -414,14 +464,20 @@ __device__ __forceinline__ double warp_sum(double v) {
 // Per-k constants of UpdateFreqFactors! staged in shared memory once per CTA.
 enum { KC_NCK, KC_NCKP, KC_NCKM, KC_DNKP, KC_DNK, KC_DNKM, KC_IDNU, KC_ICK, KC_ICKP, KC_ICKM, KC_DNU, KC_N };
 
+template <int M>
+__host__ __device__ constexpr int freq_smem_doubles(int nwarps) {
+    return KC_N * 32 * M + nwarps * (32 * M + 8) + nwarps * 4 * 32 * M;
+}
+
 template <typename S, typename R, int M>
 __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
     extern __shared__ __align__(16) double fsm[];
     constexpr int NP = 32 * M;
+    const int nw = blockDim.x >> 5;
     double *kc = fsm;                              // [KC_N][NP]
     double *red = fsm + KC_N * NP;                 // [nwarps][NP + 8]
+    double *tsm = red + nw * (NP + 8);             // [nwarps][4][NP] (lane-serial solver)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nw = blockDim.x >> 5;
     const int nnu = a.nnu;
     for (int t = threadIdx.x; t < NP; t += blockDim.x) {
         bool in = (t >= 1 && t <= nnu - 2);
@@ -439,37 +495,42 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
     }
     __syncthreads();
 
-    const int ncell = a.nr * a.nz;
+    const int4 it = a.items[blockIdx.x];
+    const CloudDesc &cd = a.cl[it.x];
+    const long long o3 = cd.o3, oc = cd.oc;
+    const int nr = cd.nr, nz = cd.nz, bzb = cd.bc_z_bot;
+    const double c_tilde = cd.c_tilde, dt = cd.dt, ctdt = cd.ctdt, z_center = cd.z_center;
     const double jeps = a.jeps;
-    const double dw = 1.0 / a.ctdt;
+    const double dw = 1.0 / ctdt;
     double acc_e[M];
 #pragma unroll
     for (int m = 0; m < M; m++) acc_e[m] = 0.0;
     double acc_tot = 0.0, acc_mf = 0.0, acc_net = 0.0, acc_out = 0.0, acc_L = 0.0, acc_esc = 0.0;
     int bad = 0;
 
-    for (int c = blockIdx.x * nw + warp; c < ncell; c += gridDim.x * nw) {
-        const int i = c % a.nr, j = c / a.nr;
-        const size_t base = (size_t)c * nnu;
+    for (int cl = it.y + warp; cl < it.z; cl += nw) {
+        const int i = cl % nr, j = cl / nr;
+        const long long c = oc + cl;
+        const long long base = o3 + (long long)cl * nnu;
         R J[M], Hr[M], HZ[M], Hv[M];
         double Jo[M];
 #pragma unroll
         for (int m = 0; m < M; m++) {
             int k = lane * M + m;
-            bool v = k < nnu;
-            J[m] = v ? R(a.Jin[base + k]) : R(0);
-            Hr[m] = v ? R(a.Hrin[base + k]) : R(0);
-            HZ[m] = v ? R(a.HZin[base + k]) : R(0);
-            Hv[m] = v ? R(__ldg(a.Hv + base + k)) : R(0);
-            Jo[m] = v ? double(a.Jold[base + k]) : 0.0;
+            bool vld = k < nnu;
+            J[m] = vld ? R(a.Jin[base + k]) : R(0);
+            Hr[m] = vld ? R(a.Hrin[base + k]) : R(0);
+            HZ[m] = vld ? R(a.HZin[base + k]) : R(0);
+            Hv[m] = vld ? R(__ldg(a.Hv + base + k)) : R(0);
+            Jo[m] = vld ? double(a.Jold[base + k]) : 0.0;
         }
         double dr_sum = 0.0, dz_sum = 0.0;
         // ---- LyaEmissionAbsorptionUpdate! (src/ConstantsAndFunctions.jl:526-567) ----
         if (a.do_emission) {
             const R al = R(__ldg(a.alpha + c)), acv = R(__ldg(a.alpha_c + c));
             const R al_pd = al * R(__ldg(a.pd + c));
-            const R js_ct = R(__ldg(a.js + c) * a.c_tilde / a.j_scale);
-            const R ct = R(a.c_tilde), dtr = R(a.dt);
+            const R js_ct = R(__ldg(a.js + c) * c_tilde / a.j_scale);
+            const R ct = R(c_tilde), dtr = R(dt);
             const R pinv = a.phi ? R(0) : R(__ldg(a.phi_inv + c));
             const R acF = a.alpha_cF ? R(__ldg(a.alpha_cF + c)) : R(0);
 #pragma unroll
@@ -496,7 +557,7 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
             dr_sum = warp_sum(dr_sum);
             dz_sum = warp_sum(dz_sum);
             if (lane == 0 && a.dru_r) {
-                const double k4 = kFourPiOverC * (1.0 / a.c_tilde) * a.j_scale;
+                const double k4 = kFourPiOverC * (1.0 / c_tilde) * a.j_scale;
                 a.dru_r[c] += k4 * dr_sum;
                 a.dru_Z[c] += k4 * dz_sum;
             }
@@ -591,7 +652,10 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
                 sys.c[m] = (in && k <= nnu - 3) ? Fp[m] : 0.0;
                 sys.d[m] = in ? -dw * Jo[m] : 0.0;
             }
-            pcr_solve<M>(sys, lane);
+            if (a.solver == SOLVER_THOMAS)
+                thomas_solve<M>(sys, lane, tsm + warp * 4 * NP);
+            else
+                pcr_solve<M>(sys, lane);
             // flux correction, src/UpdateLyaJandH.jl:341-377
 #pragma unroll
             for (int m = 0; m < M; m++) {
@@ -642,11 +706,11 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
         if (a.parts & PART_DIAG) {
             // escaping flux through the outer r face, the top face and (outflow) the bottom face
             double esc = 0.0;
-            const bool rb = (i == a.nr - 1), zt = (j == a.nz - 1), zb = (j == 0 && a.bc_z_bot == 1);
+            const bool rb = (i == nr - 1), zt = (j == nz - 1), zb = (j == 0 && bzb == 1);
             if (rb || zt || zb) {
-                const double Arr = rb ? __ldg(a.A_r + a.nr + (size_t)(a.nr + 1) * j) * kFourPi : 0.0;
-                const double AZt = zt ? __ldg(a.A_Z + i + (size_t)a.nr * a.nz) * kFourPi : 0.0;
-                const double AZb = zb ? __ldg(a.A_Z + i) * kFourPi : 0.0;
+                const double Arr = rb ? __ldg(a.A_r + cd.orf + nr + (long long)(nr + 1) * j) * kFourPi : 0.0;
+                const double AZt = zt ? __ldg(a.A_Z + cd.ozf + i + (long long)nr * nz) * kFourPi : 0.0;
+                const double AZb = zb ? __ldg(a.A_Z + cd.ozf + i) * kFourPi : 0.0;
 #pragma unroll
                 for (int m = 0; m < M; m++) {
                     int k = lane * M + m;
@@ -661,13 +725,13 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
             acc_esc += esc;
             if (lane == 0) {
                 const double dV = __ldg(a.dV + c);
-                const double k4 = kFourPiOverC * (1.0 / a.c_tilde) * a.j_scale;
-                const double inv_dt = 1.0 / a.dt;
+                const double k4 = kFourPiOverC * (1.0 / c_tilde) * a.j_scale;
+                const double inv_dt = 1.0 / dt;
                 double fr = (k4 * dr_sum) * inv_dt, fz = (k4 * dz_sum) * inv_dt;
                 if (a.f_r) { a.f_r[c] = fr; a.f_Z[c] = fz; }
                 acc_mf += dV * sqrt(fr * fr + fz * fz);
                 acc_L += kFourPi * dV * __ldg(a.js + c);
-                double drr = __ldg(a.rCoM + i), dzz = __ldg(a.ZCoM + j) - a.z_center;
+                double drr = __ldg(a.rCoM + cd.ocol + i), dzz = __ldg(a.ZCoM + cd.orow + j) - z_center;
                 double dist = sqrt(drr * drr + dzz * dzz);
                 double frad = 0.0;
                 if (dist > 0.0) {
@@ -700,29 +764,33 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
     for (int col = threadIdx.x; col < ncols; col += blockDim.x) {
         int src = col < nnu ? col : NP + (col - nnu);
         double s = 0.0;
-        for (int w = 0; w < nw; w++) s += red[w * stride + src];
+        for (int w2 = 0; w2 < nw; w2++) s += red[w2 * stride + src];
         a.partials[(size_t)col * gridDim.x + blockIdx.x] = s;
     }
 }
 
-// FindActiveBins partials of the current J (src/UpdateLyaJandH.jl:47-97): one warp per cell.
+// FindActiveBins partials of the current J (src/UpdateLyaJandH.jl:47-97): one warp per cell,
+// the same work items (and so the same summation order) as k_freq.
 template <typename S, int M>
-__global__ void __launch_bounds__(FREQ_THREADS) k_find_active(const S *J, int nnu, int ncell, const double *dnu,
-                                                              const double *dV, double jeps, double *partials) {
+__global__ void __launch_bounds__(FREQ_THREADS) k_find_active(const S *J, int nnu, const double *dnu,
+                                                              const double *dV, const CloudDesc *cl, const int4 *items,
+                                                              double jeps, double *partials) {
     extern __shared__ __align__(16) double fsm[];
     constexpr int NP = 32 * M;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int4 it = items[blockIdx.x];
+    const long long o3 = cl[it.x].o3, oc = cl[it.x].oc;
     double acc_e[M];
 #pragma unroll
     for (int m = 0; m < M; m++) acc_e[m] = 0.0;
     double acc_tot = 0.0;
-    for (int c = blockIdx.x * nw + warp; c < ncell; c += gridDim.x * nw) {
-        const double v = __ldg(dV + c);
+    for (int c = it.y + warp; c < it.z; c += nw) {
+        const double v = __ldg(dV + oc + c);
 #pragma unroll
         for (int m = 0; m < M; m++) {
             int k = lane * M + m;
             if (k >= nnu) continue;
-            double Jv = double(__ldg(J + (size_t)c * nnu + k));
+            double Jv = double(__ldg(J + o3 + (long long)c * nnu + k));
             double dn = __ldg(dnu + k);
             double e1 = Jv - 10.0 * jeps, e0 = Jv - jeps;
             acc_e[m] += dn * (e1 > 0.0 ? e1 : 0.0) * v;
@@ -743,23 +811,27 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_find_active(const S *J, int nn
     }
 }
 
-// Column sums of the partials (one warp per column, fixed order), then FindActiveBins'
-// decision and the diagnostics of Update_f_Lya_MF_L_Lya! / Compute_f_esc_Lya_Cylindrical.
+// One CTA per cloud: column sums of the cloud's partials (one warp per column, fixed order),
+// then FindActiveBins' decision and the diagnostics of Update_f_Lya_MF_L_Lya! /
+// Compute_f_esc_Lya_Cylindrical. The last CTA to finish advances the record index.
 __global__ void __launch_bounds__(1024) k_reduce(RedArgs a) {
     __shared__ double col[256 + kExtraCols];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int cloud = blockIdx.x;
+    const CloudDesc &cd = a.cl[cloud];
     const int ncols = a.nnu + kExtraCols;
     for (int cc = warp; cc < ncols; cc += nw) {
         bool need = (cc < a.nnu + 1) ? (a.parts & PART_ACTIVE) : (a.parts & PART_DIAG);
         double s = 0.0;
         if (need)
-            for (int b = lane; b < a.nblocks; b += 32) s += a.partials[(size_t)cc * a.nblocks + b];
+            for (int b = lane; b < cd.npb; b += 32) s += a.partials[(size_t)cc * a.nblocks + cd.pb0 + b];
         s = warp_sum(s);
         if (lane == 0) col[cc] = s;
     }
     __syncthreads();
     if (threadIdx.x != 0) return;
-    int used_kmin = a.kwin[0], used_kmax = a.kwin[1];
+    int *kw = a.kwin + 2 * cloud;
+    int used_kmin = kw[0], used_kmax = kw[1];
     if (a.parts & PART_ACTIVE) {
         double Etot = col[a.nnu];
         int kmin = a.nnu - 1, kmax = 0;
@@ -771,8 +843,8 @@ __global__ void __launch_bounds__(1024) k_reduce(RedArgs a) {
         }
         kmax = kmax > a.kcore_max ? kmax : a.kcore_max;
         kmin = kmin < a.kcore_min ? kmin : a.kcore_min;
-        a.kwin[0] = kmin;
-        a.kwin[1] = kmax;
+        kw[0] = kmin;
+        kw[1] = kmax;
     }
     if (a.parts & PART_DIAG) {
         double MF = col[a.nnu + 1], net = col[a.nnu + 2], outw = col[a.nnu + 3];
@@ -783,17 +855,22 @@ __global__ void __launch_bounds__(1024) k_reduce(RedArgs a) {
         } else {
             MF = 0.0; net = 0.0; outw = 0.0;
         }
-        double Ltot = (a.bc_z_bot == 0) ? 2.0 * L : L;
-        double Lsim = (a.bc_z_bot == 0) ? 0.5 * Ltot : Ltot;
+        double Ltot = (cd.bc_z_bot == 0) ? 2.0 * L : L;
+        double Lsim = (cd.bc_z_bot == 0) ? 0.5 * Ltot : Ltot;
         double fesc = (Ltot > 0.0 && Lsim > 0.0) ? col[a.nnu + 5] / Lsim : 0.0;
         double rec[7] = {MF, net, outw, Ltot, fesc, (double)used_kmin, (double)used_kmax};
         if (a.last)
-            for (int q = 0; q < 7; q++) a.last[q] = rec[q];
+            for (int q = 0; q < 7; q++) a.last[(size_t)cloud * 7 + q] = rec[q];
         if (a.diag && a.step_counter) {
             int idx = *a.step_counter;
             if (idx < a.hist_capacity)
-                for (int q = 0; q < 7; q++) a.diag[(size_t)idx * 7 + q] = rec[q];
-            *a.step_counter = idx + 1;
+                for (int q = 0; q < 7; q++) a.diag[((size_t)idx * a.nclouds + cloud) * 7 + q] = rec[q];
+            __threadfence();
+            int done = atomicAdd(a.done, 1);
+            if (done == a.nclouds - 1) {
+                *a.step_counter = idx + 1;
+                *a.done = 0;
+            }
         }
     }
 }
@@ -805,28 +882,28 @@ static size_t adv_smem_bytes(int prec) {
 }
 
 template <typename S, typename R, int FLUX>
-static void adv_launch(const void *args, int nnu, int nr, int nz, cudaStream_t st, int prec) {
+static void adv_launch(const void *args, int ntiles, cudaStream_t st, int prec) {
     static bool attr = false;
     size_t sm = adv_smem_bytes(prec);
     if (!attr) {
         cudaFuncSetAttribute(k_advect<S, R, FLUX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         attr = true;
     }
-    dim3 grid((nr + MT - 1) / MT, (nz + MROWS - 1) / MROWS, (nnu + 31) / 32);
-    k_advect<S, R, FLUX><<<grid, MTHREADS, sm, st>>>(*static_cast<const AdvArgs<S> *>(args));
+    k_advect<S, R, FLUX><<<ntiles, MTHREADS, sm, st>>>(*static_cast<const AdvArgs<S> *>(args));
 }
 
-void launch_advect(int prec, int flux, const void *args, int nnu, int nr, int nz, cudaStream_t st) {
+void launch_advect(int prec, int flux, const void *args, int ntiles, cudaStream_t st) {
+    if (ntiles <= 0) return;
     if (prec == 0) {
-        if (flux == 0) adv_launch<double, double, 0>(args, nnu, nr, nz, st, prec);
-        else adv_launch<double, double, 1>(args, nnu, nr, nz, st, prec);
+        if (flux == 0) adv_launch<double, double, 0>(args, ntiles, st, prec);
+        else adv_launch<double, double, 1>(args, ntiles, st, prec);
     } else {
-        if (flux == 0) adv_launch<float, float, 0>(args, nnu, nr, nz, st, prec);
-        else adv_launch<float, float, 1>(args, nnu, nr, nz, st, prec);
+        if (flux == 0) adv_launch<float, float, 0>(args, ntiles, st, prec);
+        else adv_launch<float, float, 1>(args, ntiles, st, prec);
     }
 }
 
-static int bins_per_lane(int nnu) { return nnu <= 32 ? 1 : nnu <= 64 ? 2 : nnu <= 128 ? 4 : 8; }
+int bins_per_lane(int nnu) { return nnu <= 32 ? 1 : nnu <= 64 ? 2 : nnu <= 128 ? 4 : 8; }
 
 int freq_blocks(int ncell, int dev) {
     int sms = 148;
@@ -837,48 +914,49 @@ int freq_blocks(int ncell, int dev) {
 }
 
 template <typename S, typename R, int M>
-static void freq_launch(const void *args, int nblocks, cudaStream_t st) {
-    size_t sm = sizeof(double) * (KC_N * 32 * M + (FREQ_THREADS / 32) * (32 * M + 8));
+static void freq_launch(const void *args, int nitems, cudaStream_t st) {
+    size_t sm = sizeof(double) * freq_smem_doubles<M>(FREQ_THREADS / 32);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_freq<S, R, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         attr = true;
     }
-    k_freq<S, R, M><<<nblocks, FREQ_THREADS, sm, st>>>(*static_cast<const FreqArgs<S> *>(args));
+    k_freq<S, R, M><<<nitems, FREQ_THREADS, sm, st>>>(*static_cast<const FreqArgs<S> *>(args));
 }
 
-void launch_freq(int prec, const void *args, int nnu, int ncell, int nblocks, cudaStream_t st) {
-    (void)ncell;
+void launch_freq(int prec, const void *args, int nnu, int nitems, cudaStream_t st) {
+    if (nitems <= 0) return;
     int M = bins_per_lane(nnu);
     if (prec == 0) {
         switch (M) {
-        case 1: freq_launch<double, double, 1>(args, nblocks, st); break;
-        case 2: freq_launch<double, double, 2>(args, nblocks, st); break;
-        case 4: freq_launch<double, double, 4>(args, nblocks, st); break;
-        default: freq_launch<double, double, 8>(args, nblocks, st); break;
+        case 1: freq_launch<double, double, 1>(args, nitems, st); break;
+        case 2: freq_launch<double, double, 2>(args, nitems, st); break;
+        case 4: freq_launch<double, double, 4>(args, nitems, st); break;
+        default: freq_launch<double, double, 8>(args, nitems, st); break;
         }
     } else {
         switch (M) {
-        case 1: freq_launch<float, float, 1>(args, nblocks, st); break;
-        case 2: freq_launch<float, float, 2>(args, nblocks, st); break;
-        case 4: freq_launch<float, float, 4>(args, nblocks, st); break;
-        default: freq_launch<float, float, 8>(args, nblocks, st); break;
+        case 1: freq_launch<float, float, 1>(args, nitems, st); break;
+        case 2: freq_launch<float, float, 2>(args, nitems, st); break;
+        case 4: freq_launch<float, float, 4>(args, nitems, st); break;
+        default: freq_launch<float, float, 8>(args, nitems, st); break;
         }
     }
 }
 
 template <typename S, int M>
-static void active_launch(const S *J, int nnu, int ncell, const double *dnu, const double *dV, double jeps,
-                          double *partials, int nblocks, cudaStream_t st) {
+static void active_launch(const S *J, int nnu, const double *dnu, const double *dV, const CloudDesc *cl,
+                          const int4 *items, int nitems, double jeps, double *partials, cudaStream_t st) {
     size_t sm = sizeof(double) * (FREQ_THREADS / 32) * (32 * M + 8);
-    k_find_active<S, M><<<nblocks, FREQ_THREADS, sm, st>>>(J, nnu, ncell, dnu, dV, jeps, partials);
+    k_find_active<S, M><<<nitems, FREQ_THREADS, sm, st>>>(J, nnu, dnu, dV, cl, items, jeps, partials);
 }
 
-void launch_find_active(int prec, const void *J, int nnu, int nr, int nz, const double *dnu, const double *dV,
-                        double jeps, double *partials, int nblocks, cudaStream_t st) {
-    int ncell = nr * nz;
+void launch_find_active(int prec, const void *J, int nnu, const double *dnu, const double *dV, const CloudDesc *cl,
+                        const int4 *items, int nitems, double jeps, double *partials, cudaStream_t st) {
+    if (nitems <= 0) return;
     int M = bins_per_lane(nnu);
-#define LYD_ACT(T, MM) active_launch<T, MM>(static_cast<const T *>(J), nnu, ncell, dnu, dV, jeps, partials, nblocks, st)
+#define LYD_ACT(T, MM) \
+    active_launch<T, MM>(static_cast<const T *>(J), nnu, dnu, dV, cl, items, nitems, jeps, partials, st)
     if (prec == 0) {
         switch (M) { case 1: LYD_ACT(double, 1); break; case 2: LYD_ACT(double, 2); break;
                      case 4: LYD_ACT(double, 4); break; default: LYD_ACT(double, 8); break; }
@@ -889,6 +967,8 @@ void launch_find_active(int prec, const void *J, int nnu, int nr, int nz, const 
 #undef LYD_ACT
 }
 
-void launch_reduce(const RedArgs &a, cudaStream_t st) { k_reduce<<<1, 1024, 0, st>>>(a); }
+void launch_reduce(const RedArgs &a, cudaStream_t st) {
+    if (a.nclouds > 0) k_reduce<<<a.nclouds, 1024, 0, st>>>(a);
+}
 
 }  // namespace lyd

@@ -150,6 +150,16 @@ class M1Context:
         self._ck(lib().lyd_get_timing(self._h, _dp(ms)))
         return ms
 
+    def set_tuning(self, rows_per_tile=16, cells_per_block=0, solver=_lib.SOLVER_PCR):
+        t = _lib.Tuning(int(rows_per_tile), int(cells_per_block), int(solver), 0)
+        self._ck(lib().lyd_set_tuning(self._h, C.byref(t)))
+
+    def tuning(self):
+        """(rows_per_tile, cells_per_block, solver); cells_per_block < 0 when chosen automatically."""
+        t = _lib.Tuning()
+        self._ck(lib().lyd_get_tuning(self._h, C.byref(t)))
+        return t.rows_per_tile, t.cells_per_block, t.solver
+
     # -- set-up helpers --------------------------------------------------------------------
     def update_hvoigt(self):
         self._ck(lib().lyd_update_hvoigt(self._h))
@@ -175,6 +185,117 @@ class M1Context:
         ri = (C.c_int32 * n)(); zi = (C.c_int32 * n)()
         self._ck(lib().lyd_edge_spectra(self._h, _dp(raw), _dp(norm), ri, zi))
         return raw, norm, np.array(ri[:]), np.array(zi[:])
+
+
+class M1Batch(M1Context):
+    """Many independent clouds of uneven (n_r, n_z) on one GPU, sharing a frequency grid and a
+    configuration (lyd_batch_create). Every step kernel covers all clouds in one launch."""
+
+    def __init__(self, sizes, n_nu, kcore_min, kcore_max, alpha_floor, recoil=True, flux_method=0,
+                 precision=PREC_FP64, keep_freq_factors=False, j_scale=0.0, device=0):
+        self.sizes = [(int(a), int(b)) for a, b in sizes]
+        self.n_clouds = len(self.sizes)
+        self.n_nu = int(n_nu)
+        self.n_r = self.n_z = None
+        self.precision = precision
+        nr = (C.c_int32 * self.n_clouds)(*[a for a, _ in self.sizes])
+        nz = (C.c_int32 * self.n_clouds)(*[b for _, b in self.sizes])
+        cfg = _lib.Config(int(flux_method), int(bool(recoil)), int(precision), int(kcore_min), int(kcore_max),
+                          int(bool(keep_freq_factors)), float(alpha_floor), float(j_scale), int(device))
+        h = C.c_void_p()
+        check(lib().lyd_batch_create(C.byref(h), self.n_clouds, nr, nz, self.n_nu, C.byref(cfg)))
+        self._h = h
+        self._keep = []
+
+    @property
+    def cell_bins(self):
+        n = C.c_int64()
+        self._ck(lib().lyd_batch_info(self._h, None, C.byref(n)))
+        return int(n.value)
+
+    def set_geometry(self, g, cloud=0):
+        keep = [_c64(a) for a in (g.r, g.Z, g.rCoM, g.ZCoM, g.dV, g.inv_dV, g.A_r, g.A_Z, g.inv_r_cell,
+                                  g.dr_L, g.dr_R, g.inv_dr_i_im1, g.inv_dr_ip1_i, g.inv_dr_ip2_ip1,
+                                  g.dZ_L, g.dZ_R, g.inv_dZ_j_jm1, g.inv_dZ_jp1_j, g.inv_dZ_jp2_jp1)]
+        p = [_dp(a) for a in keep]
+        s = _lib.Geometry(*p[:14], (C.c_double * 10)(*g.dr_b), *p[14:], (C.c_double * 10)(*g.dZ_b))
+        self._ck(lib().lyd_set_geometry_cloud(self._h, int(cloud), C.byref(s)))
+
+    def upload_cloud(self, cloud, name, arr):
+        a = _c64(arr)
+        self._ck(lib().lyd_upload_cloud(self._h, int(cloud), F[name], _dp(a), a.size))
+
+    def download_cloud(self, cloud, name):
+        nr, nz = self.sizes[cloud]
+        if F[name] < 16:
+            shape = (nz, nr, self.n_nu)
+        elif name == "u_r_star":
+            shape = (nz, nr + 1)
+        elif name == "u_Z_star":
+            shape = (nz + 1, nr)
+        else:
+            shape = (nz, nr)
+        out = np.empty(shape, dtype=np.float64)
+        self._ck(lib().lyd_download_cloud(self._h, int(cloud), F[name], _dp(out), out.size))
+        return out
+
+    def download(self, name, shape=None):
+        raise TypeError("a batch downloads per cloud: use download_cloud(cloud, name)")
+
+    def find_active_bins(self):
+        a = (C.c_int32 * self.n_clouds)()
+        b = (C.c_int32 * self.n_clouds)()
+        self._ck(lib().lyd_find_active_bins(self._h, a, b))
+        return np.array(a[:]), np.array(b[:])
+
+    def batch_steps(self, n_steps, params, history=True):
+        """params: one (c_tilde, dt, z_center, bc_r_right, bc_z_bot, bc_z_top) per cloud.
+        Returns the (n_steps, n_clouds, 7) records when history is set."""
+        arr = (_lib.CloudParams * self.n_clouds)()
+        for q, (ct, dt, zc, br, bb, bt) in enumerate(params):
+            arr[q] = _lib.CloudParams(float(ct), float(dt), float(zc), int(br), int(bb), int(bt), 0)
+        if history:
+            hist = (_lib.Diag * max(1, n_steps * self.n_clouds))()
+            self._ck(lib().lyd_batch_steps(self._h, arr, int(n_steps), hist))
+            out = np.array([[d.M_F, d.M_F_radial_net, d.M_F_radial_out, d.L_tot, d.f_esc, d.kmin, d.kmax]
+                            for d in hist[:n_steps * self.n_clouds]])
+            return out.reshape(n_steps, self.n_clouds, 7)
+        self._ck(lib().lyd_batch_steps(self._h, arr, int(n_steps), None))
+        return None
+
+    def edge_spectra(self, cloud=0):
+        nr, nz = self.sizes[cloud]
+        n = lib().lyd_edge_count(nr, nz)
+        raw = np.empty((n, self.n_nu)); norm = np.empty_like(raw)
+        ri = (C.c_int32 * n)(); zi = (C.c_int32 * n)()
+        self._ck(lib().lyd_edge_spectra_cloud(self._h, int(cloud), _dp(raw), _dp(norm), ri, zi))
+        return raw, norm, np.array(ri[:]), np.array(zi[:])
+
+
+def batch_for_clouds(clouds, precision=PREC_FP64, device=0, keep_freq_factors=False, j_scale=0.0):
+    """Create a batch context holding every workloads.StaticCloud of `clouds` (one shared
+    frequency grid, configuration taken from the first cloud) and upload their inputs; H_voigt
+    and phi_nu are computed on the device."""
+    c0 = clouds[0]
+    fq = c0.freq
+    b = M1Batch([(c.nr, c.nz) for c in clouds], c0.n_nu, fq.kcore_min, fq.kcore_max, c0.alpha_floor,
+                recoil=c0.recoil, flux_method=c0.flux_method, precision=precision,
+                keep_freq_factors=keep_freq_factors, j_scale=j_scale, device=device)
+    b.set_freq_grid(fq)
+    for q, c in enumerate(clouds):
+        if c.freq is not fq and not np.array_equal(c.freq.nu, fq.nu):
+            raise ValueError("the clouds of a batch share one frequency grid")
+        b.set_geometry(c.geom, q)
+        for name in ("alpha", "alpha_c", "pd", "js", "T", "dur_dr", "dur_dZ", "duZ_dr", "duZ_dZ", "ur_over_r",
+                     "u_r_star", "u_Z_star", "alpha_cF"):
+            b.upload_cloud(q, name, getattr(c, name))
+    b.update_hvoigt()
+    b.update_phi_nu(fq.kcore_min, fq.kcore_max)
+    return b
+
+
+def cloud_params(clouds):
+    return [(c.c_tilde, c.dt, c.z_center, c.bc_r_right, c.bc_z_bot, c.bc_z_top) for c in clouds]
 
 
 def voigt_tables(n=200001, xmax=1000.0):

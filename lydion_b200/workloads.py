@@ -158,6 +158,37 @@ def config_c2(scale=1):
                         rs=0.5, umax_kms=200.0, name="c2_dusty_outflow_256x256x64")
 
 
+C3_SIDES = (32, 48, 64, 96, 128, 192, 256)
+
+
+def batch_clouds(n_clouds=512, n_nu=48, sides=C3_SIDES, seed=20261203, tau0_range=(1e4, 1e8),
+                 T_range=(1e2, 1e4), tau_abs_range=(0.0, 2.0), vmax_range=(0.0, 100.0), rs=0.5, x_max=600.0):
+    """The ragged batch of independent static clouds: per cloud, drawn from
+    numpy.random.default_rng(seed) in this order, the radial side and the vertical side
+    (independently, uniform over `sides`), log-uniform tau0, log-uniform T, uniform tau_abs,
+    uniform v_max. Every cloud has a uniform source of radius rs*R_cl, a reflecting bottom
+    boundary and its own CFL time step; all share one symmetric frequency grid of n_nu bins
+    reaching |x| = x_max Doppler widths at 1e4 K (a context holds one frequency grid)."""
+    rng = np.random.default_rng(seed)
+    fq = symmetric_frequency_grid(n_nu, x_max=x_max, T_ref=1e4)
+    out = []
+    for q in range(n_clouds):
+        nr = int(rng.choice(sides))
+        nz = int(rng.choice(sides))
+        tau0 = float(np.exp(rng.uniform(np.log(tau0_range[0]), np.log(tau0_range[1]))))
+        T0 = float(np.exp(rng.uniform(np.log(T_range[0]), np.log(T_range[1]))))
+        tau_abs = float(rng.uniform(*tau_abs_range))
+        vmax = float(rng.uniform(*vmax_range))
+        out.append(static_cloud(nr, nz, n_nu, tau0=tau0, T0=T0, tau_abs=tau_abs, rs=rs, umax_kms=vmax, freq=fq,
+                                name=f"batch{q}"))
+    return out
+
+
+def config_c3(n_clouds=512, seed=20261203):
+    """512 ragged static clouds x 48 bins, sides from {32, ..., 256} drawn independently in r and Z."""
+    return batch_clouds(n_clouds=n_clouds, seed=seed)
+
+
 def small_cloud(nr=12, nz=10, n_nu=16, **kw):
     """A cheap cloud for parity tests (the oracle finishes it in milliseconds)."""
     kw.setdefault("tau0", 1e5)
