@@ -1,0 +1,146 @@
+"""Launch-shape autotuner for the Lyman-alpha step.
+
+Three knobs of a context are tuned (lyd_set_tuning):
+  rows_per_tile    rows of the advection tile each CTA marches through (4..64);
+  cells_per_block  cells per frequency-kernel block (8..1024, or 0 = automatic);
+  solver           frequency tridiagonal solver: 0 = parallel cyclic reduction across the warp,
+                   1 = lane-serial elimination.
+The advection kernel depends only on rows_per_tile, the frequency kernel and the reductions
+only on the other two, so the search is two short sweeps: rows first (advection time), then
+cells x solver (frequency + reduction time). Every candidate is timed on the device with the
+library's per-kernel CUDA events (lyd_set_timing) over a few real steps of the caller's
+workload, after one untimed step that applies the new shape.
+
+Tuning advances the context's state by the steps it runs: tune a scratch context built from
+the same workload when the state must stay untouched. Results are cached as JSON, keyed by
+the GPU name and the workload's shape, in $LYDION_TUNE_CACHE or
+~/.cache/lydion_b200/tuning.json.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+
+ROWS = (4, 8, 16, 32)
+CELLS = (0, 16, 32, 64, 128, 256, 512)
+SOLVERS = (0, 1)
+
+
+def cache_path():
+    p = os.environ.get("LYDION_TUNE_CACHE")
+    if p:
+        return p
+    return os.path.join(os.path.expanduser("~"), ".cache", "lydion_b200", "tuning.json")
+
+
+def device_name(device=0):
+    try:
+        import torch
+        return torch.cuda.get_device_name(device)
+    except Exception:
+        return "cuda"
+
+
+def workload_key(ctx, device=0):
+    """GPU name + bins + precision + cloud sizes (hashed for batches)."""
+    sizes = getattr(ctx, "sizes", None) or [(ctx.n_r, ctx.n_z)]
+    h = hashlib.sha1(np.asarray(sorted(sizes), dtype=np.int64).tobytes()).hexdigest()[:12]
+    return f"{device_name(device)}|nnu={ctx.n_nu}|prec={ctx.precision}|clouds={len(sizes)}|sizes={h}"
+
+
+def _load(path):
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _save(path, data):
+    os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
+    tmp = path + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(data, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
+def _measure(ctx, run, tuning, steps):
+    ctx.set_tuning(*tuning)
+    run(1)
+    ctx.synchronize()
+    ctx.set_timing(True)
+    try:
+        run(steps)
+        ctx.synchronize()
+        ms = np.asarray(ctx.timing(), dtype=np.float64) / steps
+    finally:
+        ctx.set_timing(False)
+    return ms
+
+
+def search(ctx, run, steps=10, rows=ROWS, cells=CELLS, solvers=SOLVERS):
+    """Time every candidate; return (best tuning tuple, table of (tuning, ms[3]))."""
+    table = []
+    base_cells, base_solver = 0, 0
+    best_rows, best_adv = None, np.inf
+    for r in rows:
+        ms = _measure(ctx, run, (r, base_cells, base_solver), steps)
+        table.append(((r, base_cells, base_solver), ms.tolist()))
+        if ms[0] < best_adv:
+            best_rows, best_adv = r, ms[0]
+    best, best_f = None, np.inf
+    for s in solvers:
+        for cb in cells:
+            t = (best_rows, cb, s)
+            ms = _measure(ctx, run, t, steps)
+            table.append((t, ms.tolist()))
+            if ms[1] + ms[2] < best_f:
+                best, best_f = t, ms[1] + ms[2]
+    return best, table
+
+
+def autotune(ctx, run, steps=10, device=0, cache=None, force=False, **grid):
+    """Tune `ctx` for the workload `run(n)` (which runs n steps on ctx), apply the best shape,
+    and return it. A cached entry for the same GPU and workload shape is applied without
+    timing unless `force`."""
+    path = cache or cache_path()
+    key = workload_key(ctx, device)
+    data = _load(path)
+    if not force and key in data:
+        t = tuple(data[key]["tuning"])
+        ctx.set_tuning(*t)
+        return t
+    best, table = search(ctx, run, steps=steps, **grid)
+    ctx.set_tuning(*best)
+    data[key] = {"tuning": list(best), "table": [[list(t), ms] for t, ms in table], "steps": steps}
+    _save(path, data)
+    return best
+
+
+def main():
+    import argparse
+    ap = argparse.ArgumentParser(description="tune the launch shapes of a workload and cache them")
+    ap.add_argument("--workload", choices=["c2", "c3"], default="c2")
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--force", action="store_true")
+    args = ap.parse_args()
+    from . import workloads as W
+    from .m1 import batch_for_clouds, cloud_params, context_for_cloud
+    if args.workload == "c2":
+        cl = W.config_c2()
+        ctx = context_for_cloud(cl)
+        p = (cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+        run = lambda n: ctx.static_steps(n, *p, history=False)
+    else:
+        clouds = W.config_c3()
+        ctx = batch_for_clouds(clouds)
+        pp = cloud_params(clouds)
+        run = lambda n: ctx.batch_steps(n, pp, history=False)
+    t = autotune(ctx, run, steps=args.steps, force=args.force)
+    print(json.dumps({"workload": args.workload, "tuning": list(t), "cache": cache_path()}))
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,67 @@
+"""The autotuner's search and cache logic, on a fake context whose per-kernel times are a known
+function of the launch shape (no GPU)."""
+import json
+
+from lydion_b200 import autotune as A
+
+
+class FakeCtx:
+    n_nu, n_r, n_z, precision = 64, 256, 256, 0
+
+    def __init__(self):
+        self.t = (16, 0, 0)
+        self.timing_on = False
+        self.steps = 0
+        self.applied = []
+
+    def set_tuning(self, r, c, s):
+        self.t = (r, c, s)
+        self.applied.append(self.t)
+
+    def synchronize(self):
+        pass
+
+    def set_timing(self, on):
+        self.timing_on = on
+
+    def timing(self):
+        r, c, s = self.t
+        adv = 1.0 + abs(r - 8) * 0.1
+        freq = 2.0 + (0.5 if s == 1 else 0.0) + abs((c or 96) - 64) * 0.01
+        return [adv * self.steps, freq * self.steps, 0.1 * self.steps]
+
+    def run(self, n):
+        self.steps = n
+
+
+def test_search_picks_the_fastest_shape():
+    ctx = FakeCtx()
+    best, table = A.search(ctx, ctx.run, steps=5)
+    assert best == (8, 64, 0)
+    assert len(table) == len(A.ROWS) + len(A.CELLS) * len(A.SOLVERS)
+    assert not ctx.timing_on
+
+
+def test_cache_round_trip(tmp_path, monkeypatch):
+    monkeypatch.setattr(A, "device_name", lambda device=0: "fake-gpu")
+    path = str(tmp_path / "tune.json")
+    ctx = FakeCtx()
+    assert A.autotune(ctx, ctx.run, steps=3, cache=path) == (8, 64, 0)
+    data = json.load(open(path))
+    key = A.workload_key(ctx)
+    assert key.startswith("fake-gpu|nnu=64|prec=0|clouds=1|")
+    assert data[key]["tuning"] == [8, 64, 0]
+    # a second call applies the cached shape without timing anything
+    ctx2 = FakeCtx()
+    assert A.autotune(ctx2, ctx2.run, steps=3, cache=path) == (8, 64, 0)
+    assert ctx2.applied == [(8, 64, 0)]
+
+
+def test_batch_key_depends_on_sizes(monkeypatch):
+    monkeypatch.setattr(A, "device_name", lambda device=0: "g")
+    a, b = FakeCtx(), FakeCtx()
+    a.sizes = [(32, 48), (64, 64)]
+    b.sizes = [(32, 48), (64, 96)]
+    assert A.workload_key(a) != A.workload_key(b)
+    b.sizes = [(64, 64), (32, 48)]
+    assert A.workload_key(a) == A.workload_key(b)

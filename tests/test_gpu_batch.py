@@ -144,3 +144,18 @@ def test_batch_rejects_single_cloud_calls():
         b.set_tuning(2, 0, 0)
     with pytest.raises(LydionError):
         b.set_tuning(16, 0, 7)
+
+
+def test_autotune_applies_a_valid_shape(tmp_path):
+    from lydion_b200 import autotune as A
+    from lydion_b200.m1 import batch_for_clouds, cloud_params
+    clouds = _clouds()
+    b = batch_for_clouds(clouds)
+    pp = cloud_params(clouds)
+    t = A.autotune(b, lambda n: b.batch_steps(n, pp, history=False), steps=2, cache=str(tmp_path / "t.json"),
+                   rows=(4, 16), cells=(0, 32), solvers=(0, 1))
+    got = b.tuning()
+    assert got[0] == t[0] and got[2] == t[2]
+    assert t[1] == 0 and got[1] < 0 or got[1] == t[1]
+    h = b.batch_steps(2, pp)
+    assert np.isfinite(h).all()
