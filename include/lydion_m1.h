@@ -44,8 +44,12 @@ extern "C" {
 #define LYD_FLUX_HLL 1
 /* precision of the step */
 #define LYD_PREC_FP64   0   /* everything in FP64 (the reference's arithmetic)             */
-#define LYD_PREC_MIXED  1   /* FP32 storage and bulk arithmetic; FP64 tridiagonal solve,
-                               FP64 reductions                                              */
+#define LYD_PREC_MIXED  1   /* FP64 state storage; the advection's reconstruction, closure,
+                               fluxes and limiters in FP32 with the cell update accumulated
+                               in FP64; the frequency step (factors, tridiagonal solve) and
+                               all reductions in FP64                                        */
+#define LYD_PREC_FP32   2   /* FP32 storage and bulk arithmetic; FP64 tridiagonal solve and
+                               reductions (fastest, least accurate: weak bins lose digits)  */
 
 typedef struct lyd_ctx lyd_ctx;
 
@@ -65,8 +69,8 @@ typedef struct lyd_config {
     int32_t keep_freq_factors;  /* keep F+/F/F- on the device so that a later frequency
                                    update may pass update_freq_factors = 0                 */
     double alpha_floor;         /* LyaArrays.alpha_Lya_floor                               */
-    double j_scale;             /* LYD_PREC_MIXED: J and H are stored as value / j_scale;
-                                   0 selects 1e-12                                         */
+    double j_scale;             /* LYD_PREC_MIXED / _FP32: J and H are held as value / j_scale
+                                   (inside the FP32 range); 0 selects 1e-12                */
     int32_t device;             /* CUDA device ordinal                                     */
     int32_t reserved[7];
 } lyd_config;
@@ -208,11 +212,13 @@ typedef struct lyd_cloud_params {
 int  lyd_batch_steps(lyd_ctx *ctx, const lyd_cloud_params *params, int32_t n_steps, lyd_diag *hist);
 
 /* Launch-shape knobs chosen by the autotuner (lydion_b200/autotune.py): rows of the
- * advection tile (4..64), cells per frequency-kernel block (8..1024, or 0 for automatic), and
- * the frequency solver (0: parallel cyclic reduction across the warp; 1: lane-serial
- * elimination). */
+ * advection tile (4..64), cells per frequency-kernel block (8..1024, or 0 for automatic), the
+ * frequency solver (0: parallel cyclic reduction across the warp; 1: lane-serial
+ * elimination), and the advection kernel's resident CTAs per SM (2..4, or 0 for the
+ * default; FP64 arithmetic always uses 2). lyd_get_tuning reports an automatic cell count
+ * as its negative. */
 typedef struct lyd_tuning {
-    int32_t rows_per_tile, cells_per_block, solver, reserved;
+    int32_t rows_per_tile, cells_per_block, solver, adv_ctas_per_sm;
 } lyd_tuning;
 int  lyd_set_tuning(lyd_ctx *ctx, const lyd_tuning *t);
 int  lyd_get_tuning(lyd_ctx *ctx, lyd_tuning *t);

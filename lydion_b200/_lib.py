@@ -12,7 +12,7 @@ LYD_OK = 0
 LYD_ERR_ARG, LYD_ERR_CUDA, LYD_ERR_NONFINITE, LYD_ERR_SOLVE, LYD_ERR_STATE, LYD_ERR_NOMEM = -1, -2, -3, -4, -5, -6
 BC_REFLECT, BC_OUTFLOW = 0, 1
 FLUX_GLF, FLUX_HLL = 0, 1
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_FP32 = 0, 1, 2
 
 F = dict(J=0, J_old=1, H_r=2, H_Z=3, H_r_old=4, H_Z_old=5, Hvoigt=6, phi_nu=7, alpha_F=8,
          alpha=16, alpha_c=17, alpha_cF=18, pd=19, js=20, T=21, dur_dr=22, dur_dZ=23, duZ_dr=24, duZ_dZ=25,
@@ -66,7 +66,7 @@ class CloudParams(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("rows_per_tile", C.c_int32), ("cells_per_block", C.c_int32), ("solver", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("adv_ctas_per_sm", C.c_int32)]
 
 
 SOLVER_PCR, SOLVER_THOMAS = 0, 1

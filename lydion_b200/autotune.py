@@ -1,13 +1,14 @@
 """Launch-shape autotuner for the Lyman-alpha step.
 
-Three knobs of a context are tuned (lyd_set_tuning):
+Four knobs of a context are tuned (lyd_set_tuning):
   rows_per_tile    rows of the advection tile each CTA marches through (4..64);
+  adv_ctas_per_sm  resident advection CTAs per SM (2..4; FP32-arithmetic variants only);
   cells_per_block  cells per frequency-kernel block (8..1024, or 0 = automatic);
   solver           frequency tridiagonal solver: 0 = parallel cyclic reduction across the warp,
                    1 = lane-serial elimination.
-The advection kernel depends only on rows_per_tile, the frequency kernel and the reductions
-only on the other two, so the search is two short sweeps: rows first (advection time), then
-cells x solver (frequency + reduction time). Every candidate is timed on the device with the
+The advection kernel depends only on rows_per_tile and adv_ctas_per_sm, the frequency kernel
+and the reductions only on the other two, so the search is two short sweeps: rows x CTAs
+first (advection time), then cells x solver (frequency + reduction time). Every candidate is timed on the device with the
 library's per-kernel CUDA events (lyd_set_timing) over a few real steps of the caller's
 workload, after one untimed step that applies the new shape.
 
@@ -23,6 +24,7 @@ import os
 import numpy as np
 
 ROWS = (4, 8, 16, 32)
+CTAS = (2, 3, 4)
 CELLS = (0, 16, 32, 64, 128, 256, 512)
 SOLVERS = (0, 1)
 
@@ -79,20 +81,23 @@ def _measure(ctx, run, tuning, steps):
     return ms
 
 
-def search(ctx, run, steps=10, rows=ROWS, cells=CELLS, solvers=SOLVERS):
+def search(ctx, run, steps=10, rows=ROWS, cells=CELLS, solvers=SOLVERS, ctas=CTAS):
     """Time every candidate; return (best tuning tuple, table of (tuning, ms[3]))."""
     table = []
-    base_cells, base_solver = 0, 0
+    if getattr(ctx, "precision", 0) == 0:
+        ctas = (0,)                      # FP64 arithmetic has one occupancy variant
     best_rows, best_adv = None, np.inf
     for r in rows:
-        ms = _measure(ctx, run, (r, base_cells, base_solver), steps)
-        table.append(((r, base_cells, base_solver), ms.tolist()))
-        if ms[0] < best_adv:
-            best_rows, best_adv = r, ms[0]
+        for o in ctas:
+            t = (r, 0, 0, o)
+            ms = _measure(ctx, run, t, steps)
+            table.append((t, ms.tolist()))
+            if ms[0] < best_adv:
+                best_rows, best_adv = (r, o), ms[0]
     best, best_f = None, np.inf
     for s in solvers:
         for cb in cells:
-            t = (best_rows, cb, s)
+            t = (best_rows[0], cb, s, best_rows[1])
             ms = _measure(ctx, run, t, steps)
             table.append((t, ms.tolist()))
             if ms[1] + ms[2] < best_f:

@@ -52,7 +52,8 @@ struct lyd_ctx {
     std::vector<unsigned> have;        // per-cloud provided bits
     size_t ncell = 0, n3 = 0, nrf = 0, nzf = 0, ncol = 0, nrow = 0, nrint = 0, nzint = 0, nrif = 0, nzif = 0;
     lyd_config cfg{};
-    int prec = 0;
+    int prec = 0;                      // kernel variant (LYD_PREC_*)
+    int sprec = 0;                     // storage of the state arrays: 0 double, 1 float
     size_t ssz = 8;
     double jscale = 1.0, jeps_s = kJeps, heps2_s = kHeps * kHeps;
     void *set[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
@@ -242,7 +243,8 @@ int lyd_batch_create(lyd_ctx **out, int32_t ncl, const int32_t *n_r, const int32
         if (n_r[q] < 3 || n_z[q] < 3) return LYD_ERR_ARG;
         if ((long long)n_r[q] * n_z[q] * n_nu >= (1LL << 31)) return LYD_ERR_ARG;   // per-cloud int indices
     }
-    if (cfg->precision != LYD_PREC_FP64 && cfg->precision != LYD_PREC_MIXED) return LYD_ERR_ARG;
+    if (cfg->precision != LYD_PREC_FP64 && cfg->precision != LYD_PREC_MIXED && cfg->precision != LYD_PREC_FP32)
+        return LYD_ERR_ARG;
     if (cfg->flux_method != LYD_FLUX_GLF && cfg->flux_method != LYD_FLUX_HLL) return LYD_ERR_ARG;
     if (cfg->kcore_min < 0 || cfg->kcore_max >= n_nu || cfg->kcore_min > cfg->kcore_max) return LYD_ERR_ARG;
     lyd_ctx *c = new lyd_ctx();
@@ -277,8 +279,9 @@ int lyd_batch_create(lyd_ctx **out, int32_t ncl, const int32_t *n_r, const int32
     }
     if (c->nrint >= (1u << 31) || c->nzint >= (1u << 31)) { lyd_destroy(c); return LYD_ERR_ARG; }
     c->prec = cfg->precision;
-    c->ssz = c->prec == LYD_PREC_FP64 ? sizeof(double) : sizeof(float);
-    if (c->prec == LYD_PREC_MIXED) {
+    c->sprec = c->prec == LYD_PREC_FP32 ? 1 : 0;
+    c->ssz = c->sprec == 0 ? sizeof(double) : sizeof(float);
+    if (c->prec != LYD_PREC_FP64) {
         c->jscale = cfg->j_scale > 0.0 ? cfg->j_scale : 1e-12;
         c->jeps_s = 1e-30;
         c->heps2_s = 0.0;
@@ -371,10 +374,11 @@ int lyd_set_tuning(lyd_ctx *c, const lyd_tuning *t) {
     if (t->cells_per_block != 0 && (t->cells_per_block < 8 || t->cells_per_block > 1024))
         return fail(c, LYD_ERR_ARG, "cells_per_block outside 8..1024");
     if (t->solver != SOLVER_PCR && t->solver != SOLVER_THOMAS) return fail(c, LYD_ERR_ARG, "unknown solver");
+    if (t->adv_ctas_per_sm != 0 && (t->adv_ctas_per_sm < 2 || t->adv_ctas_per_sm > 4))
+        return fail(c, LYD_ERR_ARG, "adv_ctas_per_sm outside 2..4");
     cudaSetDevice(c->dev);
     LYD_CU(c, cudaStreamSynchronize(c->st));
     c->tune = *t;
-    c->tune.reserved = 0;
     return build_work(c);
 }
 
@@ -382,6 +386,7 @@ int lyd_get_tuning(lyd_ctx *c, lyd_tuning *t) {
     if (!c || !t) return LYD_ERR_ARG;
     *t = c->tune;
     if (t->cells_per_block == 0) t->cells_per_block = -cells_per_block(c);   // negative: chosen automatically
+    t->adv_ctas_per_sm = adv_ctas_per_sm(c->prec, t->adv_ctas_per_sm);
     return LYD_OK;
 }
 
@@ -469,7 +474,7 @@ static int materialize_old(lyd_ctx *c) {
 static int upload3(lyd_ctx *c, void *dst, const double *host, size_t n, double scale) {
     LYD_TRY(ensure_stage(c, n));
     LYD_CU(c, cudaMemcpyAsync(c->stage, host, n * 8, cudaMemcpyHostToDevice, c->st));
-    launch_convert_in(c->prec, c->stage, dst, n, scale, c->st);
+    launch_convert_in(c->sprec, c->stage, dst, n, scale, c->st);
     LYD_CU(c, cudaGetLastError());
     return LYD_OK;
 }
@@ -561,7 +566,7 @@ static int download_field(lyd_ctx *c, int q, int32_t field, double *host, size_t
     if (count != n) return fail(c, LYD_ERR_ARG, "wrong element count");
     if (is3) {
         LYD_TRY(ensure_stage(c, n));
-        launch_convert_out(c->prec, at(const_cast<void *>(src), d.o3, c->ssz), c->stage, n, scale, c->st);
+        launch_convert_out(c->sprec, at(const_cast<void *>(src), d.o3, c->ssz), c->stage, n, scale, c->st);
         LYD_CU(c, cudaGetLastError());
         LYD_CU(c, cudaMemcpyAsync(host, c->stage, n * 8, cudaMemcpyDeviceToHost, c->st));
     } else {
@@ -664,7 +669,7 @@ static RedArgs red_args(lyd_ctx *c, int parts) {
 
 static int run_find_active(lyd_ctx *c) {
     LYD_TRY(sync_desc(c));
-    launch_find_active(c->prec, Jc(c, 0), c->nnu, c->dnu, c->dV, c->cl, c->items, c->nitems, c->jeps_s, c->partials,
+    launch_find_active(c->sprec, Jc(c, 0), c->nnu, c->dnu, c->dV, c->cl, c->items, c->nitems, c->jeps_s, c->partials,
                        c->st);
     launch_reduce(red_args(c, PART_ACTIVE), c->st);
     LYD_CU(c, cudaGetLastError());
@@ -710,14 +715,14 @@ static int do_advect(lyd_ctx *c) {
     if (!c->active_valid) LYD_TRY(run_find_active(c));
     LYD_TRY(sync_desc(c));
     int in = c->cur, out = 1 - c->cur;
-    if (c->prec == 0) {
+    if (c->sprec == 0) {
         AdvArgs<double> a;
         fill_adv<double>(c, a, in, out);
-        launch_advect(0, c->cfg.flux_method, &a, c->ntiles, c->st);
+        launch_advect(c->prec, c->cfg.flux_method, &a, c->ntiles, c->tune.adv_ctas_per_sm, c->st);
     } else {
         AdvArgs<float> a;
         fill_adv<float>(c, a, in, out);
-        launch_advect(1, c->cfg.flux_method, &a, c->ntiles, c->st);
+        launch_advect(c->prec, c->cfg.flux_method, &a, c->ntiles, c->tune.adv_ctas_per_sm, c->st);
     }
     LYD_CU(c, cudaGetLastError());
     c->cur = out;
@@ -757,7 +762,7 @@ int lyd_emission_absorption(lyd_ctx *c, double ct, double dt) {
     LYD_TRY(need_inputs(c, true, false));
     if (!(ct > 0.0) || !(dt > 0.0)) return fail(c, LYD_ERR_ARG, "c~ and dt must be positive");
     params_all(c, ct, dt, ct * dt);
-    int r = c->prec == 0 ? freq_call<double>(c, true, false, 1, 0) : freq_call<float>(c, true, false, 1, 0);
+    int r = c->sprec == 0 ? freq_call<double>(c, true, false, 1, 0) : freq_call<float>(c, true, false, 1, 0);
     if (r != LYD_OK) return r;
     c->old_alias = true;
     c->active_valid = false;
@@ -773,7 +778,7 @@ int lyd_frequency_update(lyd_ctx *c, double ctdt, int32_t update_ff) {
         return fail(c, LYD_ERR_STATE, "update_freq_factors = 0 needs keep_freq_factors and a previous update");
     for (CloudDesc &d : c->desc) d.ctdt = ctdt;
     int uf = update_ff ? 1 : 0;
-    int r = c->prec == 0 ? freq_call<double>(c, false, true, uf, PART_ACTIVE)
+    int r = c->sprec == 0 ? freq_call<double>(c, false, true, uf, PART_ACTIVE)
                          : freq_call<float>(c, false, true, uf, PART_ACTIVE);
     if (r != LYD_OK) return r;
     launch_reduce(red_args(c, PART_ACTIVE), c->st);
@@ -841,7 +846,7 @@ int lyd_f_esc(lyd_ctx *c, double L_all, int32_t bc_z_bot, double *f) {
     cudaSetDevice(c->dev);
     if (!all_have(c, BIT_GEOM) || !c->freq_set) return fail(c, LYD_ERR_STATE, "geometry / frequency grid not set");
     if (L_all <= 0.0) { *f = 0.0; return LYD_OK; }
-    launch_fesc(c->prec, Jc(c, 1), Jc(c, 2), c->A_r, c->A_Z, c->dnu, c->nnu, c->nr[0], c->nz[0], bc_z_bot, c->jscale,
+    launch_fesc(c->sprec, Jc(c, 1), Jc(c, 2), c->A_r, c->A_Z, c->dnu, c->nnu, c->nr[0], c->nz[0], bc_z_bot, c->jscale,
                 c->small, c->st);
     LYD_CU(c, cudaGetLastError());
     double num;
@@ -866,9 +871,9 @@ static int enqueue_step(lyd_ctx *c, bool timed) {
     fa.f_r = c->cellf[CF_F_R]; fa.f_Z = c->cellf[CF_F_Z];
     RedArgs ra = red_args(c, PART_ACTIVE | PART_DIAG);
     ra.diag = c->hist; ra.step_counter = c->step_ctr; ra.done = c->step_ctr + 1; ra.hist_capacity = c->hist_cap;
-    const int prec = sizeof(S) == 8 ? 0 : 1;
+    const int prec = c->prec;
     if (timed) cudaEventRecord(c->ev[0], c->st);
-    launch_advect(prec, c->cfg.flux_method, &aa, c->ntiles, c->st);
+    launch_advect(prec, c->cfg.flux_method, &aa, c->ntiles, c->tune.adv_ctas_per_sm, c->st);
     if (timed) cudaEventRecord(c->ev[1], c->st);
     launch_freq(prec, &fa, c->nnu, c->nitems, c->st);
     if (timed) cudaEventRecord(c->ev[2], c->st);
@@ -913,7 +918,7 @@ static int run_steps(lyd_ctx *c, int n_steps, lyd_diag *hist_out) {
     if (c->timing) {
         double acc[3] = {0, 0, 0};
         for (int n = 0; n < n_steps; n++) {
-            int r = c->prec == 0 ? enqueue_step<double>(c, true) : enqueue_step<float>(c, true);
+            int r = c->sprec == 0 ? enqueue_step<double>(c, true) : enqueue_step<float>(c, true);
             if (r != LYD_OK) return r;
             LYD_CU(c, cudaEventSynchronize(c->ev[3]));
             for (int q = 0; q < 3; q++) {
@@ -928,7 +933,7 @@ static int run_steps(lyd_ctx *c, int n_steps, lyd_diag *hist_out) {
             drop_graph(c);
             cudaGraph_t g;
             LYD_CU(c, cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-            int r = c->prec == 0 ? enqueue_step<double>(c, false) : enqueue_step<float>(c, false);
+            int r = c->sprec == 0 ? enqueue_step<double>(c, false) : enqueue_step<float>(c, false);
             cudaError_t e = cudaStreamEndCapture(c->st, &g);
             if (r != LYD_OK) return r;
             if (e != cudaSuccess) return fail(c, LYD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
@@ -999,7 +1004,7 @@ int lyd_update_hvoigt(lyd_ctx *c) {
         LYD_CU(c, cudaMemcpyAsync(c->lut, h.data(), h.size() * 8, cudaMemcpyHostToDevice, c->st));
         LYD_CU(c, cudaStreamSynchronize(c->st));
     }
-    launch_hvoigt(c->prec, c->Hv, c->cellf[CF_T], c->nu, c->nuC, c->nnu, c->ncell, c->lut, kLutN, kLutXmax, c->st);
+    launch_hvoigt(c->sprec, c->Hv, c->cellf[CF_T], c->nu, c->nuC, c->nnu, c->ncell, c->lut, kLutN, kLutXmax, c->st);
     LYD_CU(c, cudaGetLastError());
     set_all(c, BIT_HV);
     c->phi_inv_ready = false;
@@ -1011,7 +1016,7 @@ int lyd_update_phi_nu(lyd_ctx *c, int32_t kmin, int32_t kmax) {
     cudaSetDevice(c->dev);
     if (kmin < 0 || kmax >= c->nnu || kmin > kmax) return fail(c, LYD_ERR_ARG, "bad bin range");
     if (!all_have(c, BIT_HV) || !c->freq_set) return fail(c, LYD_ERR_STATE, "H_voigt / frequency grid not set");
-    launch_phi_inv(c->prec, c->Hv, c->dnu, c->nnu, c->ncell, kmin, kmax, c->phi_inv, c->st);
+    launch_phi_inv(c->sprec, c->Hv, c->dnu, c->nnu, c->ncell, kmin, kmax, c->phi_inv, c->st);
     LYD_CU(c, cudaGetLastError());
     c->phi_kmin = kmin;
     c->phi_kmax = kmax;
@@ -1076,7 +1081,7 @@ int lyd_edge_spectra_cloud(lyd_ctx *c, int32_t q, double *raw, double *norm, int
     size_t n = (size_t)ne * c->nnu;
     double *d = nullptr;
     LYD_TRY(dalloc(c, (void **)&d, 2 * n * 8));
-    launch_edge(c->prec, at(Jc(c, 0), c->desc[q].o3, c->ssz), c->dnu, c->nnu, nr, nz, c->jscale, d, d + n, c->st);
+    launch_edge(c->sprec, at(Jc(c, 0), c->desc[q].o3, c->ssz), c->dnu, c->nnu, nr, nz, c->jscale, d, d + n, c->st);
     int r = LYD_OK;
     cudaError_t e = cudaMemcpyAsync(raw, d, n * 8, cudaMemcpyDeviceToHost, c->st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(norm, d + n, n * 8, cudaMemcpyDeviceToHost, c->st);

@@ -37,6 +37,11 @@ constexpr int kExtraCols = 6;
 
 enum { PART_ACTIVE = 1, PART_DIAG = 2 };
 
+// Kernel precision variants (the values of LYD_PREC_*): storage type S / arithmetic type R.
+enum { PREC_K_FP64 = 0,     // S = double, R = double
+       PREC_K_MIXED = 1,    // S = double, R = float in the advection fluxes
+       PREC_K_FP32 = 2 };   // S = float,  R = float
+
 // Advection: AdvectJandH_Cylindrical! (src/AdvectJandH.jl:526-1390), reads set `in`,
 // writes set `out`. Bins outside each cloud's active window are copied through.
 template <typename S>
@@ -113,9 +118,12 @@ struct RedArgs {
 enum { ERRB_NONFINITE = 1, ERRB_SOLVE = 2 };
 
 int bins_per_lane(int nnu);
-void launch_find_active(int prec, const void *J, int nnu, const double *dnu, const double *dV, const CloudDesc *cl,
+// `prec` of the step launches is a PREC_K_* variant; `sprec` of the others is the storage
+// type of the state arrays (0: double, 1: float).
+void launch_find_active(int sprec, const void *J, int nnu, const double *dnu, const double *dV, const CloudDesc *cl,
                         const int4 *items, int nitems, double jeps, double *partials, cudaStream_t st);
-void launch_advect(int prec, int flux, const void *args, int ntiles, cudaStream_t st);
+void launch_advect(int prec, int flux, const void *args, int ntiles, int ctas_per_sm, cudaStream_t st);
+int adv_ctas_per_sm(int prec, int want);   // the occupancy variant launch_advect uses
 void launch_freq(int prec, const void *args, int nnu, int nitems, cudaStream_t st);
 void launch_reduce(const RedArgs &a, cudaStream_t st);
 int freq_blocks(int ncell, int dev);

@@ -133,20 +133,22 @@ __device__ __forceinline__ Cell<R> raw_cell(const AdvArgs<S> &a, const View &v, 
     return ld_cell<S, R>(a, v, col, row, k);
 }
 
-// Stage cell (col, row) into ring slot `slot`, staged column lc (= col - i0 + 2).
+// Stage cell (col, row) into ring slot `slot`, staged column lc (= col - i0 + 2): the flux
+// inputs in the arithmetic type R, and for the tile's own columns the state (J, H_r, H_Z) in
+// the storage type S, which the cell update accumulates into.
 template <typename S, typename R>
-__device__ __forceinline__ void stage_cell(const AdvArgs<S> &a, const View &v, R *A, R *Hh, int slot, int lc,
+__device__ __forceinline__ void stage_cell(const AdvArgs<S> &a, const View &v, R *A, S *Hh, int slot, int lc,
                                            int col, int row, int k, int lane, R jeps) {
-    Cell<R> c = raw_cell<S, R>(a, v, col, row, k);
-    CellF<R> f = cell_f<R>(c.J, c.Hr, c.HZ, jeps);
+    Cell<S> c = raw_cell<S, S>(a, v, col, row, k);
+    CellF<R> f = cell_f<R>(R(c.J), R(c.Hr), R(c.HZ), jeps);
     int cc = col < 0 ? 0 : (col >= v.nr ? v.nr - 1 : col);
     int rr = row < 0 ? 0 : (row >= v.nz ? v.nz - 1 : row);
     R aF = alpha_F<S, R>(a, v, cc, rr, k);
     R *p = A + ((slot * MCOL + lc) * 4) * 32 + lane;
     p[0] = f.J; p[32] = f.fr; p[64] = f.fZ; p[96] = aF;
     if (lc >= 2 && lc < 2 + MT) {
-        R *q = Hh + ((slot * MT + (lc - 2)) * 2) * 32 + lane;
-        q[0] = c.Hr; q[32] = c.HZ;
+        S *q = Hh + ((slot * MT + (lc - 2)) * 3) * 32 + lane;
+        q[0] = c.J; q[32] = c.Hr; q[64] = c.HZ;
     }
 }
 
@@ -212,12 +214,12 @@ __device__ __forceinline__ void face_z_staged(const AdvArgs<S> &a, const View &v
     F[2] = FHZ + adv_flux(uc, q.HZ_L, q.HZ_R);
 }
 
-template <typename S, typename R, int FLUX>
-__global__ void __launch_bounds__(MTHREADS, 2) k_advect(AdvArgs<S> a) {
+template <typename S, typename R, int FLUX, int MINB>
+__global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
     extern __shared__ __align__(16) unsigned char adv_smem[];
-    R *A = reinterpret_cast<R *>(adv_smem);              // [RING][MCOL][4][32]
-    R *Hh = A + RING * MCOL * 4 * 32;                     // [RING][MT][2][32]
-    R *Fr = Hh + RING * MT * 2 * 32;                      // [MT+1][5][32]
+    R *A = reinterpret_cast<R *>(adv_smem);                            // [RING][MCOL][4][32]
+    S *Hh = reinterpret_cast<S *>(A + RING * MCOL * 4 * 32);            // [RING][MT][3][32]
+    R *Fr = reinterpret_cast<R *>(Hh + RING * MT * 3 * 32);             // [MT+1][5][32]
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int4 t = a.tiles[blockIdx.x];
     View v;
@@ -294,9 +296,9 @@ __global__ void __launch_bounds__(MTHREADS, 2) k_advect(AdvArgs<S> a) {
             if (!kact) {
                 a.Jo[x] = a.J[x]; a.Hro[x] = a.Hr[x]; a.HZo[x] = a.HZ[x];
             } else {
-                const R *pA = A + (((j & (RING - 1)) * MCOL + w + 2) * 4) * 32 + lane;
-                const R *pH = Hh + (((j & (RING - 1)) * MT + w) * 2) * 32 + lane;
-                R sJ = pA[0], sHr = pH[0], sHZ = pH[32];
+                const S *pH = Hh + (((j & (RING - 1)) * MT + w) * 3) * 32 + lane;
+                const S uJ = pH[0], uHr = pH[32], uHZ = pH[64];
+                const R sJ = R(uJ), sHr = R(uHr), sHZ = R(uHZ);
                 R Drr, DZZ, DrZ;
                 D_edd<R>(sHr, sHZ, sJ, jeps, R(a.heps2), Drr, DZZ, DrZ);
                 const R *FL = Fr + (w * 5) * 32 + lane;
@@ -305,37 +307,39 @@ __global__ void __launch_bounds__(MTHREADS, 2) k_advect(AdvArgs<S> a) {
                 double ArR = __ldg(a.A_r + v.orf + i + 1 + (long long)(v.nr + 1) * j);
                 double AZL = __ldg(a.A_Z + v.ozf + cl), AZR = __ldg(a.A_Z + v.ozf + cl + v.nr);
                 double fac = ctdt * __ldg(a.inv_dV + c);
-                R Jn, Hrn, HZn;
+                // increments in R, accumulated into the state in S
+                S Jn, Hrn, HZn;
+                const S ujeps = S(a.jeps);
                 if (sizeof(R) == 8) {
                     R fr_ = R(fac);
-                    Jn = sJ - fr_ * ((R(ArR) * FR[0] - R(ArL) * FL[0]) + (R(AZR) * zR[0] - R(AZL) * zL[0]));
-                    HZn = sHZ - fr_ * ((R(ArR) * FR[64] - R(ArL) * FL[64]) + (R(AZR) * zR[2] - R(AZL) * zL[2]));
-                    Hrn = sHr - fr_ * ((R(ArR) * FR[32] - R(ArL) * FL[32]) + (R(AZR) * zR[1] - R(AZL) * zL[1]));
+                    Jn = uJ - S(fr_ * ((R(ArR) * FR[0] - R(ArL) * FL[0]) + (R(AZR) * zR[0] - R(AZL) * zL[0])));
+                    HZn = uHZ - S(fr_ * ((R(ArR) * FR[64] - R(ArL) * FL[64]) + (R(AZR) * zR[2] - R(AZL) * zL[2])));
+                    Hrn = uHr - S(fr_ * ((R(ArR) * FR[32] - R(ArL) * FL[32]) + (R(AZR) * zR[1] - R(AZL) * zL[1])));
                 } else {
                     R wrL = R(fac * ArL), wrR = R(fac * ArR), wzL = R(fac * AZL), wzR = R(fac * AZR);
-                    Jn = sJ - ((wrR * FR[0] - wrL * FL[0]) + (wzR * zR[0] - wzL * zL[0]));
-                    HZn = sHZ - ((wrR * FR[64] - wrL * FL[64]) + (wzR * zR[2] - wzL * zL[2]));
-                    Hrn = sHr - ((wrR * FR[32] - wrL * FL[32]) + (wzR * zR[1] - wzL * zL[1]));
+                    Jn = uJ - S((wrR * FR[0] - wrL * FL[0]) + (wzR * zR[0] - wzL * zL[0]));
+                    HZn = uHZ - S((wrR * FR[64] - wrL * FL[64]) + (wzR * zR[2] - wzL * zL[2]));
+                    Hrn = uHr - S((wrR * FR[32] - wrL * FL[32]) + (wzR * zR[1] - wzL * zL[1]));
                 }
-                Jn = Jn > jeps ? Jn : jeps;
+                Jn = Jn > ujeps ? Jn : ujeps;
                 R ga = R(__ldg(a.dur_dr + c)), gb = R(__ldg(a.dur_dZ + c)), gc = R(__ldg(a.duZ_dr + c));
                 R gd = R(__ldg(a.duZ_dZ + c)), ge = R(__ldg(a.ur_over_r + c));
                 R DdU = d_colon_grad_u<R>(Drr, DrZ, DZZ, ga, gb, gc, gd, ge);
                 R Kav = R(0.5) * (FL[128] + FR[96]);
                 if (sizeof(R) == 8)
-                    Hrn += R(ctdt) * Kav * R(__ldg(a.inv_r_cell + v.ocol + i));
+                    Hrn += S(R(ctdt) * Kav * R(__ldg(a.inv_r_cell + v.ocol + i)));
                 else
-                    Hrn += R(ctdt * __ldg(a.inv_r_cell + v.ocol + i)) * Kav;
+                    Hrn += S(R(ctdt * __ldg(a.inv_r_cell + v.ocol + i)) * Kav);
                 R cc = R(ctdt_c);
                 R dHr = -cc * (sHr * ga + sHZ * gb);
                 R dHZ = -cc * (sHr * gc + sHZ * gd);
-                Hrn = Hrn + dHr;
-                HZn = HZn + dHZ;
-                Jn = Jn - cc * DdU * sJ;
-                Jn = Jn > jeps ? Jn : jeps;
-                R H2 = Hrn * Hrn + HZn * HZn;
+                Hrn = Hrn + S(dHr);
+                HZn = HZn + S(dHZ);
+                Jn = Jn - S(cc * DdU * sJ);
+                Jn = Jn > ujeps ? Jn : ujeps;
+                S H2 = Hrn * Hrn + HZn * HZn;
                 if (H2 > Jn * Jn) {
-                    R fsc = Jn / rsq(H2);
+                    S fsc = Jn / rsq(H2);
                     Hrn *= fsc;
                     HZn *= fsc;
                 }
@@ -466,6 +470,7 @@ enum { KC_NCK, KC_NCKP, KC_NCKM, KC_DNKP, KC_DNK, KC_DNKM, KC_IDNU, KC_ICK, KC_I
 
 template <int M>
 __host__ __device__ constexpr int freq_smem_doubles(int nwarps) {
+    // FP64 constants, per-warp reduction rows, lane-serial solver rows
     return KC_N * 32 * M + nwarps * (32 * M + 8) + nwarps * 4 * 32 * M;
 }
 
@@ -512,15 +517,16 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
         const int i = cl % nr, j = cl / nr;
         const long long c = oc + cl;
         const long long base = o3 + (long long)cl * nnu;
-        R J[M], Hr[M], HZ[M], Hv[M];
+        S J[M], Hr[M], HZ[M];
+        R Hv[M];
         double Jo[M];
 #pragma unroll
         for (int m = 0; m < M; m++) {
             int k = lane * M + m;
             bool vld = k < nnu;
-            J[m] = vld ? R(a.Jin[base + k]) : R(0);
-            Hr[m] = vld ? R(a.Hrin[base + k]) : R(0);
-            HZ[m] = vld ? R(a.HZin[base + k]) : R(0);
+            J[m] = vld ? a.Jin[base + k] : S(0);
+            Hr[m] = vld ? a.Hrin[base + k] : S(0);
+            HZ[m] = vld ? a.HZin[base + k] : S(0);
             Hv[m] = vld ? R(__ldg(a.Hv + base + k)) : R(0);
             Jo[m] = vld ? double(a.Jold[base + k]) : 0.0;
         }
@@ -541,18 +547,18 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
                               : ((k >= a.phi_kmin && k <= a.phi_kmax) ? Hv[m] * pinv : R(0));
                 R aabs = acv + al_pd * Hv[m];
                 R dJdt = js_ct * phi;
-                R Jn = (R(Jo[m]) + dJdt * dtr) / (R(1) + aabs * ct * dtr);
                 R aH = a.aF ? R(__ldg(a.aF + base + k)) : (a.alpha_cF ? al * Hv[m] + acF : al * Hv[m]);
-                R iden = R(1) / (R(1) + aH * ct * dtr);
-                R hr = Hr[m] * iden;
-                R hz = HZ[m] * iden;
                 double dn = kc[KC_DNU * NP + k];
+                R Jn = (R(Jo[m]) + dJdt * dtr) / (R(1) + aabs * ct * dtr);
+                R iden = R(1) / (R(1) + aH * ct * dtr);
+                R hr = R(Hr[m]) * iden;
+                R hz = R(HZ[m]) * iden;
                 dr_sum += dn * (double(Hr[m]) - double(hr));
                 dz_sum += dn * (double(HZ[m]) - double(hz));
-                Hr[m] = hr;
-                HZ[m] = hz;
-                J[m] = Jn;
-                Jo[m] = double(Jn);
+                Hr[m] = S(hr);
+                HZ[m] = S(hz);
+                J[m] = S(Jn);
+                Jo[m] = double(J[m]);
             }
             dr_sum = warp_sum(dr_sum);
             dz_sum = warp_sum(dz_sum);
@@ -577,6 +583,9 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
                 const R gd = R(__ldg(a.duZ_dZ + c)), ge = R(__ldg(a.ur_over_r + c));
                 // K_k = pref H_voigt[k] and 1/K_k once per bin; the k+-1 neighbours come by
                 // shuffle (the same products the reference forms at k-1 and k+1)
+                // The frequency factors stay FP64 in every precision variant: with F/dw up to
+                // ~1e9 at tau0 = 1e8, an FP32 rounding of F0 against Fm + Fp acts as a spurious
+                // source or sink tens of times larger than the step's own change.
                 double Kb[M], iK[M];
 #pragma unroll
                 for (int m = 0; m < M; m++) {
@@ -593,7 +602,7 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
                     Fp[m] = 0.0; F0[m] = 0.0; Fm[m] = 0.0;
                     if (k < 1 || k > nnu - 2) continue;
                     R Drr, DZZ, DrZ;
-                    D_edd<R>(Hr[m], HZ[m], J[m], R(jeps), R(a.heps2), Drr, DZZ, DrZ);
+                    D_edd<R>(R(Hr[m]), R(HZ[m]), R(J[m]), R(jeps), R(a.heps2), Drr, DZZ, DrZ);
                     double vel = double(d_colon_grad_u<R>(Drr, DrZ, DZZ, ga, gb, gc, gd, ge)) * kInvC;
                     double Kk = Kb[m];
                     double Kkm = (m > 0) ? Kb[m - 1] : K_up;
@@ -673,9 +682,9 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
                     hr *= fsc;
                     hz *= fsc;
                 }
-                J[m] = R(Jf);
-                Hr[m] = R(hr);
-                HZ[m] = R(hz);
+                J[m] = S(Jf);
+                Hr[m] = S(hr);
+                HZ[m] = S(hz);
             }
         }
         // ---- store ----
@@ -876,30 +885,46 @@ __global__ void __launch_bounds__(1024) k_reduce(RedArgs a) {
 }
 
 // ---- launch wrappers ----------------------------------------------------------------------
-static size_t adv_smem_bytes(int prec) {
-    size_t per = (prec == 0) ? sizeof(double) : sizeof(float);
-    return per * 32 * (RING * MCOL * 4 + RING * MT * 2 + (MT + 1) * 5);
+template <typename S, typename R>
+static size_t adv_smem_bytes() {
+    return sizeof(R) * 32 * (RING * MCOL * 4 + (MT + 1) * 5) + sizeof(S) * 32 * RING * MT * 3;
+}
+
+template <typename S, typename R, int FLUX, int MINB>
+static void adv_launch(const void *args, int ntiles, cudaStream_t st) {
+    static bool attr = false;
+    size_t sm = adv_smem_bytes<S, R>();
+    if (!attr) {
+        cudaFuncSetAttribute(k_advect<S, R, FLUX, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        attr = true;
+    }
+    k_advect<S, R, FLUX, MINB><<<ntiles, MTHREADS, sm, st>>>(*static_cast<const AdvArgs<S> *>(args));
 }
 
 template <typename S, typename R, int FLUX>
-static void adv_launch(const void *args, int ntiles, cudaStream_t st, int prec) {
-    static bool attr = false;
-    size_t sm = adv_smem_bytes(prec);
-    if (!attr) {
-        cudaFuncSetAttribute(k_advect<S, R, FLUX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        attr = true;
-    }
-    k_advect<S, R, FLUX><<<ntiles, MTHREADS, sm, st>>>(*static_cast<const AdvArgs<S> *>(args));
+static void adv_occ(const void *args, int ntiles, cudaStream_t st, int ctas) {
+    if (ctas >= 4) adv_launch<S, R, FLUX, 4>(args, ntiles, st);
+    else if (ctas == 2) adv_launch<S, R, FLUX, 2>(args, ntiles, st);
+    else adv_launch<S, R, FLUX, 3>(args, ntiles, st);
 }
 
-void launch_advect(int prec, int flux, const void *args, int ntiles, cudaStream_t st) {
+int adv_ctas_per_sm(int prec, int want) {
+    if (prec == PREC_K_FP64) return 2;            // FP64: ~100 registers and 85 KB of shared memory per CTA
+    return (want >= 2 && want <= 4) ? want : 4;
+}
+
+void launch_advect(int prec, int flux, const void *args, int ntiles, int ctas, cudaStream_t st) {
     if (ntiles <= 0) return;
-    if (prec == 0) {
-        if (flux == 0) adv_launch<double, double, 0>(args, ntiles, st, prec);
-        else adv_launch<double, double, 1>(args, ntiles, st, prec);
+    ctas = adv_ctas_per_sm(prec, ctas);
+    if (prec == PREC_K_FP64) {
+        if (flux == 0) adv_launch<double, double, 0, 2>(args, ntiles, st);
+        else adv_launch<double, double, 1, 2>(args, ntiles, st);
+    } else if (prec == PREC_K_MIXED) {
+        if (flux == 0) adv_occ<double, float, 0>(args, ntiles, st, ctas);
+        else adv_occ<double, float, 1>(args, ntiles, st, ctas);
     } else {
-        if (flux == 0) adv_launch<float, float, 0>(args, ntiles, st, prec);
-        else adv_launch<float, float, 1>(args, ntiles, st, prec);
+        if (flux == 0) adv_occ<float, float, 0>(args, ntiles, st, ctas);
+        else adv_occ<float, float, 1>(args, ntiles, st, ctas);
     }
 }
 
@@ -927,21 +952,21 @@ static void freq_launch(const void *args, int nitems, cudaStream_t st) {
 void launch_freq(int prec, const void *args, int nnu, int nitems, cudaStream_t st) {
     if (nitems <= 0) return;
     int M = bins_per_lane(nnu);
-    if (prec == 0) {
-        switch (M) {
-        case 1: freq_launch<double, double, 1>(args, nitems, st); break;
-        case 2: freq_launch<double, double, 2>(args, nitems, st); break;
-        case 4: freq_launch<double, double, 4>(args, nitems, st); break;
-        default: freq_launch<double, double, 8>(args, nitems, st); break;
-        }
-    } else {
-        switch (M) {
-        case 1: freq_launch<float, float, 1>(args, nitems, st); break;
-        case 2: freq_launch<float, float, 2>(args, nitems, st); break;
-        case 4: freq_launch<float, float, 4>(args, nitems, st); break;
-        default: freq_launch<float, float, 8>(args, nitems, st); break;
-        }
+#define LYD_FQ(S_, R_)                                             \
+    switch (M) {                                                   \
+    case 1: freq_launch<S_, R_, 1>(args, nitems, st); break;       \
+    case 2: freq_launch<S_, R_, 2>(args, nitems, st); break;       \
+    case 4: freq_launch<S_, R_, 4>(args, nitems, st); break;       \
+    default: freq_launch<S_, R_, 8>(args, nitems, st); break;      \
     }
+    // the mixed variant keeps the whole frequency step in FP64 (its state, factors and solve
+    // need it; its closure and emission are a small part of the kernel's time)
+    if (prec == PREC_K_FP32) {
+        LYD_FQ(float, float)
+    } else {
+        LYD_FQ(double, double)
+    }
+#undef LYD_FQ
 }
 
 template <typename S, int M>
@@ -951,13 +976,13 @@ static void active_launch(const S *J, int nnu, const double *dnu, const double *
     k_find_active<S, M><<<nitems, FREQ_THREADS, sm, st>>>(J, nnu, dnu, dV, cl, items, jeps, partials);
 }
 
-void launch_find_active(int prec, const void *J, int nnu, const double *dnu, const double *dV, const CloudDesc *cl,
+void launch_find_active(int sprec, const void *J, int nnu, const double *dnu, const double *dV, const CloudDesc *cl,
                         const int4 *items, int nitems, double jeps, double *partials, cudaStream_t st) {
     if (nitems <= 0) return;
     int M = bins_per_lane(nnu);
 #define LYD_ACT(T, MM) \
     active_launch<T, MM>(static_cast<const T *>(J), nnu, dnu, dV, cl, items, nitems, jeps, partials, st)
-    if (prec == 0) {
+    if (sprec == 0) {
         switch (M) { case 1: LYD_ACT(double, 1); break; case 2: LYD_ACT(double, 2); break;
                      case 4: LYD_ACT(double, 4); break; default: LYD_ACT(double, 8); break; }
     } else {

@@ -295,24 +295,6 @@ __device__ __forceinline__ void omphi_LR(double P, double &oL, double &xL, doubl
     oR = ie;
     xR = (1.0 - ie) * iP;
 }
-// FP32 variants for the mixed step (same branches, float arithmetic)
-__device__ __forceinline__ void omphi_L(float P, float &omp, float &chi) {
-    const float Pm = 40.0f;
-    if (P >= Pm) { omp = expf(-Pm); chi = (1.0f - omp) / Pm; return; }
-    if (P <= -Pm) { omp = expf(Pm); chi = (1.0f - omp) / (-Pm); return; }
-    if (fabsf(P) < 1e-3f) { omp = 1.0f - P + 0.5f * (P * P); chi = 1.0f - 0.5f * P; return; }
-    omp = expf(-P);
-    chi = (1.0f - omp) / P;
-}
-__device__ __forceinline__ void omphi_R(float P, float &omp, float &chi) {
-    const float Pm = 40.0f;
-    if (P >= Pm) { omp = expf(Pm); chi = (1.0f - omp) / Pm; return; }
-    if (P <= -Pm) { omp = expf(-Pm); chi = (1.0f - omp) / (-Pm); return; }
-    if (fabsf(P) < 1e-3f) { omp = 1.0f + P + 0.5f * (P * P); chi = -1.0f - 0.5f * P; return; }
-    omp = expf(P);
-    chi = (1.0f - omp) / P;
-}
-
 // Thermal velocity, Doppler width, Voigt parameter (src/ConstantsAndFunctions.jl:282-314)
 __host__ __device__ __forceinline__ double compute_b(double T) { return sqrt(2.0 * kKBoltz / kMH) * sqrt(T); }
 __host__ __device__ __forceinline__ double compute_dnuD(double T) { return compute_b(T) * (kNuLya / kC); }

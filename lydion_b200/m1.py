@@ -150,15 +150,16 @@ class M1Context:
         self._ck(lib().lyd_get_timing(self._h, _dp(ms)))
         return ms
 
-    def set_tuning(self, rows_per_tile=16, cells_per_block=0, solver=_lib.SOLVER_PCR):
-        t = _lib.Tuning(int(rows_per_tile), int(cells_per_block), int(solver), 0)
+    def set_tuning(self, rows_per_tile=16, cells_per_block=0, solver=_lib.SOLVER_PCR, adv_ctas_per_sm=0):
+        t = _lib.Tuning(int(rows_per_tile), int(cells_per_block), int(solver), int(adv_ctas_per_sm))
         self._ck(lib().lyd_set_tuning(self._h, C.byref(t)))
 
     def tuning(self):
-        """(rows_per_tile, cells_per_block, solver); cells_per_block < 0 when chosen automatically."""
+        """(rows_per_tile, cells_per_block, solver, adv_ctas_per_sm); cells_per_block < 0 when
+        chosen automatically."""
         t = _lib.Tuning()
         self._ck(lib().lyd_get_tuning(self._h, C.byref(t)))
-        return t.rows_per_tile, t.cells_per_block, t.solver
+        return t.rows_per_tile, t.cells_per_block, t.solver, t.adv_ctas_per_sm
 
     # -- set-up helpers --------------------------------------------------------------------
     def update_hvoigt(self):
