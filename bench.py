@@ -2,6 +2,10 @@
 dusty outflowing cloud (tau0 = 1e8, tau_abs = 1, uniform source r_s = 0.5 R_cl, Hubble
 outflow v_max = 200 km/s), one static-cloud driver iteration per step.
 
+The headline value is the mixed-precision form (FP64 state, FP32 advection arithmetic); the
+same line carries the plain-FP64 form, their ratio, and the ragged batch of 512 clouds
+(48 bins, sides 32..256) in both forms.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 One unit of work is one (cell, frequency bin) advanced through one full step: advection of
@@ -157,6 +161,109 @@ def run_reference(args):
     return 0
 
 
+def _timed(ctx, run, n, stream_of):
+    import torch
+    stream = stream_of(ctx)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    run(n)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def measure_form(cloud, prec, args, barrier, stream_of, local, world, clk=None):
+    """One precision form of the C2 step: launch shapes tuned (autotune, cached), W warm-up
+    steps, K timed steps between barriers, then per-kernel device times over a separate pass."""
+    from lydion_b200 import autotune, sharding
+    from lydion_b200.m1 import context_for_cloud
+    ctx = context_for_cloud(cloud, precision=prec, device=local)
+    p = (cloud.c_tilde, cloud.dt, cloud.z_center, cloud.bc_r_right, cloud.bc_z_bot, cloud.bc_z_top)
+    run = lambda n: ctx.static_steps(n, *p, history=False)
+    tuning = autotune.autotune(ctx, run, steps=5, device=local,
+                               cache=os.path.join(tempfile.gettempdir(), "lydion_bench_tuning.json"))
+    run(args.warmup)
+    barrier(ctx)
+    if clk is not None:
+        clk.__enter__()
+    barrier(ctx)
+    ms = _timed(ctx, run, args.steps, stream_of)
+    barrier(ctx)
+    clocks = None
+    if clk is not None:
+        clk.__exit__()
+        clocks = clk.summary()
+    ms_max = sharding.max_over_ranks(ms, device="cuda")
+    value = sharding.weak_scaling_throughput(args.steps * cloud.cell_bins, world, ms_max)
+    ctx.set_timing(True)
+    kt = min(args.steps, 200)
+    run(kt)
+    ctx.synchronize()
+    kms = ctx.timing() / kt
+    ctx.set_timing(False)
+    return ctx, {"value": value, "ms_per_step": ms_max / args.steps, "kernel_ms": kms, "tuning": list(tuning),
+                 "clocks": clocks}
+
+
+def e2e_form(ctx, cloud, args, barrier, stream_of, world):
+    """End to end through the public API with host buffers: per step, J / H_r / H_Z up from
+    pinned host memory, one step with its diagnostics record, J / H_r / H_Z back."""
+    import torch
+    from lydion_b200 import sharding
+    p = (cloud.c_tilde, cloud.dt, cloud.z_center, cloud.bc_r_right, cloud.bc_z_bot, cloud.bc_z_top)
+    n = max(3, min(20, args.steps // 50))
+    pinned = [torch.empty((cloud.nz, cloud.nr, cloud.n_nu), dtype=torch.float64, pin_memory=True).numpy()
+              for _ in range(3)]
+    names = ("J", "H_r", "H_Z")
+    for a, name in zip(pinned, names):
+        a[...] = ctx.download(name)
+    barrier(ctx)
+
+    def run(k):
+        for _ in range(k):
+            for a, name in zip(pinned, names):
+                ctx.upload(name, a)
+            ctx.static_steps(1, *p, history=True)
+            for a, name in zip(pinned, names):
+                a[...] = ctx.download(name)
+
+    ms = sharding.max_over_ranks(_timed(ctx, run, n, stream_of), device="cuda")
+    nbytes = 3 * cloud.cell_bins * 8
+    return {"value": sharding.weak_scaling_throughput(n * cloud.cell_bins, world, ms), "unit": UNIT,
+            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes + 7 * 8, "steps": n}
+
+
+def batch_form(args, barrier, stream_of, local, world):
+    """The ragged batch (512 static clouds x 48 bins, sides 32..256, per-cloud CFL step) in both
+    forms: a few graph-replayed steps of the whole batch each."""
+    from lydion_b200 import autotune, sharding
+    from lydion_b200 import workloads as W
+    from lydion_b200._lib import PREC_FP64, PREC_MIXED
+    from lydion_b200.m1 import batch_for_clouds, cloud_params
+    clouds = W.config_c3()
+    mine = clouds if world == 1 else [clouds[q] for q in sharding.partition_clouds(
+        [c.cell_bins for c in clouds], world)[int(os.environ.get("RANK", 0))]]
+    pp = cloud_params(mine)
+    out = {"workload": "c3_ragged_batch_512_clouds_x48", "clouds": len(clouds),
+           "cell_bins": int(sum(c.cell_bins for c in clouds))}
+    steps = max(3, min(20, args.steps // 150))
+    for name, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
+        b = batch_for_clouds(mine, precision=prec, device=local)
+        run = lambda n: b.batch_steps(n, pp, history=False)
+        tuning = autotune.autotune(b, run, steps=2, device=local, rows=(8, 16), cells=(0, 256), solvers=(0,),
+                                   cache=os.path.join(tempfile.gettempdir(), "lydion_bench_tuning.json"))
+        run(3)
+        barrier(b)
+        ms = sharding.max_over_ranks(_timed(b, run, steps, stream_of), device="cuda")
+        # every rank advances its share of the 512 clouds: the whole batch's cell-bins over the
+        # slowest rank's time
+        out[name] = {"value": steps * out["cell_bins"] / (ms * 1e-3), "ms_per_step": ms / steps, "steps": steps,
+                     "tuning": list(tuning)}
+        b.close()
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
+
+
 def run_gpu(args):
     import torch
     rank, world, local = rank_info()
@@ -166,97 +273,59 @@ def run_gpu(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    from lydion_b200 import sharding
     from lydion_b200 import workloads as W
-    from lydion_b200.m1 import context_for_cloud
-    from lydion_b200._lib import PREC_FP64
+    from lydion_b200._lib import PREC_FP64, PREC_MIXED
     cloud = W.config_c2()
-    prec = PREC_FP64
-    ctx = context_for_cloud(cloud, precision=prec, device=local)
-    p = (cloud.c_tilde, cloud.dt, cloud.z_center, cloud.bc_r_right, cloud.bc_z_bot, cloud.bc_z_top)
-    stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
 
-    def barrier():
+    def barrier(ctx):
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
         ctx.synchronize()
 
-    # warm-up (also instantiates the step graph)
-    ctx.static_steps(args.warmup, *p, history=False)
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        barrier()
-        e0.record(stream)
-        ctx.static_steps(args.steps, *p, history=False)
-        e1.record(stream)
-        e1.synchronize()
-        barrier()
-    ms = e0.elapsed_time(e1)
-    clocks = clk.summary()
-    ms_max = sharding.max_over_ranks(ms, device="cuda")
-    value = sharding.weak_scaling_throughput(args.steps * cloud.cell_bins, world, ms_max)
+    stream_of = lambda ctx: torch.cuda.ExternalStream(ctx.stream(), device=local)
+    ctx64, f64 = measure_form(cloud, PREC_FP64, args, barrier, stream_of, local, world)
+    ctx64.close()
+    ctxm, mix = measure_form(cloud, PREC_MIXED, args, barrier, stream_of, local, world, clk=ClockSampler(local))
+    e2e = e2e_form(ctxm, cloud, args, barrier, stream_of, world)
+    ctxm.close()
+    batch = None if args.no_batch else batch_form(args, barrier, stream_of, local, world)
 
-    # per-kernel device time over a separate pass (events around every launch)
-    ctx.set_timing(True)
-    kt_steps = min(args.steps, 200)
-    ctx.static_steps(kt_steps, *p, history=False)
-    ctx.synchronize()
-    kms = ctx.timing() / kt_steps
-    ctx.set_timing(False)
+    # roofline of the dominant kernel of the headline (mixed) form
     names = ["advect", "freq", "reduce"]
+    kms = mix["kernel_ms"]
     dom = int(np.argmax(kms[:2]))
-    s = 8 if prec == PREC_FP64 else 4
-    ab = algorithmic_bytes(cloud.n_nu, s)[names[dom]] * cloud.cell_bins
+    ab = algorithmic_bytes(cloud.n_nu, 8)[names[dom]] * cloud.cell_bins
     peaks, src = measured_peaks()
     achieved = ab / (kms[dom] * 1e-3) / 1e9
-    traffic = profile_traffic("k_" + names[dom], "fp64" if prec == PREC_FP64 else "mixed")
-
-    # end to end through the public API with host buffers: per step, J/H_r/H_Z up from pinned
-    # host memory, one step, J/H_r/H_Z and the diagnostics back
-    e2e_steps = max(3, min(20, args.steps // 50))
-    pinned = [torch.empty((cloud.nz, cloud.nr, cloud.n_nu), dtype=torch.float64, pin_memory=True).numpy()
-              for _ in range(3)]
-    for a, name in zip(pinned, ("J", "H_r", "H_Z")):
-        a[...] = ctx.download(name)
-    barrier()
-    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for _ in range(e2e_steps):
-        for a, name in zip(pinned, ("J", "H_r", "H_Z")):
-            ctx.upload(name, a)
-        ctx.static_steps(1, *p, history=True)
-        for a, name in zip(pinned, ("J", "H_r", "H_Z")):
-            a[...] = ctx.download(name)
-    f1.record(stream)
-    f1.synchronize()
-    e2e_ms = sharding.max_over_ranks(f0.elapsed_time(f1), device="cuda")
-    e2e_value = sharding.weak_scaling_throughput(e2e_steps * cloud.cell_bins, world, e2e_ms)
-    nbytes = 3 * cloud.cell_bins * 8
-
+    variant = {"advect": "mixed", "freq": "fp64"}[names[dom]]   # the mixed form runs the FP64 frequency kernel
+    traffic = profile_traffic("k_" + names[dom], variant)
     cpu = cpu_baseline(cloud) if (rank == 0 and world == 1 and not args.no_cpu) else None
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        line = {"metric": METRIC, "value": mix["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": mix["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64 state, f32 advection arithmetic",
                 "data": "synthetic (seeded static cloud set-up, no dataset)",
                 "config": {"workload": WORKLOAD, "cells": [cloud.nr, cloud.nz], "bins": cloud.n_nu, "tau0": 1e8,
-                           "tau_abs": 1.0, "source_radius": 0.5, "v_max_kms": 200.0, "precision": "fp64",
+                           "tau_abs": 1.0, "source_radius": 0.5, "v_max_kms": 200.0, "precision": "mixed",
                            "parallelism": f"{world} independent clouds (one per GPU)" if world > 1 else "single GPU",
-                           "l2": "inputs larger than L2: 7 FP64 fields x 33.5 MB resident, 56 B/cell-bin streamed per kernel"},
+                           "l2": "inputs larger than L2: 7 FP64 fields x 33.5 MB resident, 56 B/cell-bin streamed per kernel",
+                           "tuning": mix["tuning"]},
+                "fp64": {"value": f64["value"], "ms_per_step": f64["ms_per_step"], "tuning": f64["tuning"],
+                         "kernel_ms_per_step": {n: float(v) for n, v in zip(names, f64["kernel_ms"])}},
+                "mixed_over_fp64": mix["value"] / f64["value"],
+                "adjoint_over_forward": None,
+                "batch": batch,
                 "roofline": {"bound": "hbm", "kernel": "k_" + names[dom], "achieved": achieved,
                              "peak": peaks["hbm_gbs"], "peak_source": src, "unit": "GB/s",
                              "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                              "algorithmic_bytes_per_launch": ab, "ms_per_launch": float(kms[dom]),
                              "kernel_ms_per_step": {n: float(v) for n, v in zip(names, kms)}},
                 "cpu_baseline": cpu,
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes,
-                        "d2h_bytes_per_step": nbytes + 7 * 8, "steps": e2e_steps},
+                "e2e": e2e,
                 "gpu_launches": 3 * args.steps,
-                "clocks": clocks}
+                "clocks": mix["clocks"]}
         print(json.dumps(line), flush=True)
-    ctx.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -270,6 +339,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="lydion", choices=["lydion", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--no-batch", action="store_true", help="skip the ragged-batch measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
