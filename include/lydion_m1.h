@@ -223,6 +223,41 @@ typedef struct lyd_tuning {
 int  lyd_set_tuning(lyd_ctx *ctx, const lyd_tuning *t);
 int  lyd_get_tuning(lyd_ctx *ctx, lyd_tuning *t);
 
+/* ---- adjoint ------------------------------------------------------------------------------ */
+/* Gradients of  objective = w_MF * M_F(last step) + sum_k w_spec[k] * S_k(final J)  over
+ * n_steps static-driver steps from the current state, S being the edge-ring mean spectrum of
+ * lyd_edge_spectra. A forward sweep stores the state every checkpoint_every steps (0: 100);
+ * the reverse sweep recomputes each segment from its checkpoint and runs hand-written adjoint
+ * kernels of the step (advection, emission/absorption, frequency factors, transposed
+ * tridiagonal solve, flux correction). The active window of every step is the forward's.
+ * Non-smooth points (MinMod, floors, clamps, limiters) take the derivative of the branch the
+ * forward took. Needs a single-cloud FP64 context, the GLF flux and alpha_F derived from
+ * alpha and H_voigt. The context ends in the final state of the forward sweep.
+ * grad_T includes the H_voigt(T) chain when H_voigt was computed by lyd_update_hvoigt (not
+ * uploaded), and the T of the frequency factors (Doppler width, recoil); gradients with
+ * respect to n_H and a dust opacity follow from grad_alpha and grad_alpha_c by the caller's
+ * parametrisation (alpha = x_HI n_H sigma0(T)). No counterpart exists in the reference. */
+typedef struct lyd_adjoint_cfg {
+    lyd_step_params step;        /* c_tilde, dt, z_center, boundaries, n_steps */
+    int32_t checkpoint_every;
+    int32_t reserved;
+    double w_MF;
+    const double *w_spec;        /* n_nu weights, or NULL */
+} lyd_adjoint_cfg;
+
+typedef struct lyd_adjoint_out { /* host arrays; any may be NULL */
+    double *objective, *M_F;     /* 1 each */
+    double *spectrum;            /* n_nu */
+    double *grad_alpha, *grad_alpha_c, *grad_T;                /* n_r*n_z each */
+    double *grad_Hv;             /* n_nu*n_r*n_z: H_voigt as an independent input */
+    double *grad_u_r_star;       /* (n_r+1)*n_z */
+    double *grad_u_Z_star;       /* n_r*(n_z+1) */
+    double *grad_du[5];          /* dur_dr, dur_dZ, duZ_dr, duZ_dZ, ur_over_r: n_r*n_z each */
+    double *grad_J0, *grad_H_r0, *grad_H_Z0;                   /* initial state, n_nu*n_r*n_z each */
+} lyd_adjoint_out;
+
+int  lyd_adjoint_run(lyd_ctx *ctx, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out);
+
 /* ---- set-up and output helpers --------------------------------------------------------- */
 /* Update_Hvoigt! from the uploaded temperature, src/ConstantsAndFunctions.jl:319-357, using
  * the Voigt look-up tables of src/FastInterpolations.jl:175-275 built on the device. */

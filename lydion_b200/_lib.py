@@ -71,6 +71,17 @@ class Tuning(C.Structure):
 
 SOLVER_PCR, SOLVER_THOMAS = 0, 1
 
+
+class AdjointCfg(C.Structure):
+    _fields_ = [("step", StepParams), ("checkpoint_every", C.c_int32), ("reserved", C.c_int32), ("w_MF", C.c_double),
+                ("w_spec", P)]
+
+
+class AdjointOut(C.Structure):
+    _fields_ = [("objective", P), ("M_F", P), ("spectrum", P), ("grad_alpha", P), ("grad_alpha_c", P), ("grad_T", P),
+                ("grad_Hv", P), ("grad_u_r_star", P), ("grad_u_Z_star", P), ("grad_du", P * 5), ("grad_J0", P),
+                ("grad_H_r0", P), ("grad_H_Z0", P)]
+
 # name -> (restype, argtypes); this list is the ABI surface checked by the CPU tests
 I32, D, SZ, VP = C.c_int32, C.c_double, C.c_size_t, C.c_void_p
 SIGNATURES = {
@@ -104,6 +115,7 @@ SIGNATURES = {
     "lyd_batch_steps": (C.c_int, [VP, C.POINTER(CloudParams), I32, C.POINTER(Diag)]),
     "lyd_set_tuning": (C.c_int, [VP, C.POINTER(Tuning)]),
     "lyd_get_tuning": (C.c_int, [VP, C.POINTER(Tuning)]),
+    "lyd_adjoint_run": (C.c_int, [VP, C.POINTER(AdjointCfg), C.POINTER(AdjointOut)]),
     "lyd_update_hvoigt": (C.c_int, [VP]),
     "lyd_update_phi_nu": (C.c_int, [VP, I32, I32]),
     "lyd_pd_lya": (C.c_int, [VP, SZ, P, P, P, P, P, P, D, P]),

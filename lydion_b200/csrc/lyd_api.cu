@@ -23,6 +23,7 @@
 #include <string>
 #include <vector>
 
+#include "lyd_adjoint.h"
 #include "lyd_internal.h"
 #include "lyd_physics.cuh"
 #include "lydion_m1.h"
@@ -60,6 +61,7 @@ struct lyd_ctx {
     int cur = 0;
     bool old_alias = true;
     void *Hv = nullptr;
+    bool hv_from_T = false;            // H_voigt last computed on the device from T
     void *phi = nullptr;
     double *phi_inv = nullptr;
     int phi_kmin = 0, phi_kmax = -1;
@@ -504,6 +506,7 @@ static int upload_field(lyd_ctx *c, int q, int32_t field, const double *host, si
         if (count != n3) return fail(c, LYD_ERR_ARG, "wrong element count for H_voigt");
         LYD_TRY(upload3(c, at(c->Hv, d.o3, c->ssz), host, n3, 1.0));
         mark(BIT_HV);
+        c->hv_from_T = false;
         c->phi_inv_ready = false;
     } else if (field == LYD_F_PHI_NU || field == LYD_F_ALPHA_F) {
         if (count != n3) return fail(c, LYD_ERR_ARG, "wrong element count");
@@ -1007,6 +1010,7 @@ int lyd_update_hvoigt(lyd_ctx *c) {
     launch_hvoigt(c->sprec, c->Hv, c->cellf[CF_T], c->nu, c->nuC, c->nnu, c->ncell, c->lut, kLutN, kLutXmax, c->st);
     LYD_CU(c, cudaGetLastError());
     set_all(c, BIT_HV);
+    c->hv_from_T = true;
     c->phi_inv_ready = false;
     return check_err(c);
 }
@@ -1106,4 +1110,214 @@ int lyd_voigt_tables(double *out, int32_t n, double xmax) {
     if (!out || n < 2 || !(xmax > 0.0)) return LYD_ERR_ARG;
     build_voigt_lut(out, n, xmax);
     return LYD_OK;
+}
+
+// ---- adjoint of the static-driver loop ---------------------------------------------------------
+//
+// Two-level checkpointing: the forward sweep stores the state at the start of every segment of
+// `checkpoint_every` steps (and each step's active window); the reverse sweep walks the
+// segments backwards, recomputes a segment's states from its checkpoint, then runs the
+// adjoint steps of that segment from its last step to its first.
+namespace {
+struct DevBuf {
+    std::vector<void *> ptrs;
+    ~DevBuf() {
+        for (void *p : ptrs) cudaFree(p);
+    }
+};
+}  // namespace
+
+int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out) {
+    if (!c || !cfg || !out) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    const lyd_step_params *p = &cfg->step;
+    if (c->ncl != 1) return fail(c, LYD_ERR_STATE, "the adjoint runs on a single-cloud context");
+    if (c->prec != LYD_PREC_FP64) return fail(c, LYD_ERR_STATE, "the adjoint runs in LYD_PREC_FP64");
+    if (c->cfg.flux_method != LYD_FLUX_GLF) return fail(c, LYD_ERR_STATE, "the adjoint supports the GLF flux");
+    if (c->aF) return fail(c, LYD_ERR_STATE, "the adjoint needs alpha_F derived from alpha and H_voigt");
+    LYD_TRY(check_bcs(c, LYD_BC_REFLECT, p->bc_r_right, p->bc_z_bot, p->bc_z_top));
+    if (!(p->c_tilde > 0.0) || !(p->dt > 0.0) || p->n_steps < 1) return fail(c, LYD_ERR_ARG, "bad step parameters");
+    LYD_TRY(need_inputs(c, true, true));
+    const int N = p->n_steps;
+    const int K = cfg->checkpoint_every > 0 ? (cfg->checkpoint_every < N ? cfg->checkpoint_every : N) : (N < 100 ? N : 100);
+    const int nseg = (N + K - 1) / K;
+    const size_t n3 = c->n3, nc = c->ncell, S = 3 * n3;
+    const int nr = c->nr[0], nz = c->nz[0], nnu = c->nnu;
+    params_all(c, p->c_tilde, p->dt, p->c_tilde * p->dt);
+    for (CloudDesc &d : c->desc) d.z_center = p->z_center;
+    bcs_all(c, p->bc_r_right, p->bc_z_bot, p->bc_z_top);
+    LYD_TRY(sync_desc(c));
+    if (N > c->hist_cap) {
+        LYD_CU(c, cudaStreamSynchronize(c->st));
+        cudaFree(c->hist);
+        c->hist = nullptr;
+        c->hist_cap = 0;
+        LYD_TRY(dalloc(c, (void **)&c->hist, (size_t)N * 7 * 8));
+        c->hist_cap = N;
+        drop_graph(c);
+    }
+    DevBuf mem;
+    auto A = [&](size_t bytes) -> double * {
+        void *q = nullptr;
+        if (dalloc(c, &q, bytes) != LYD_OK) return nullptr;
+        mem.ptrs.push_back(q);
+        return static_cast<double *>(q);
+    };
+    double *ck = A((size_t)nseg * S * 8), *seg = A((size_t)K * S * 8), *xA = A(S * 8), *tape = A(4 * n3 * 8);
+    double *lam = A(S * 8), *lamA = A(S * 8), *lamN = A(S * 8), *pre = A(S * 8), *gaF = A(n3 * 8), *gHv = A(n3 * 8);
+    double *g_alpha = A(nc * 8), *g_alpha_c = A(nc * 8), *g_T = A(nc * 8), *g_u = A(5 * nc * 8);
+    double *g_ur = A(c->nrf * 8), *g_uZ = A(c->nzf * 8), *fin = A(S * 8), *wsp = A(nnu * 8), *edge = A(2 * (size_t)nnu * (nr + nz + 2 * nr) * 8);
+    int *win = reinterpret_cast<int *>(A((size_t)N * 2 * sizeof(int) + 16));
+    int *finwin = reinterpret_cast<int *>(A(16));
+    if (!ck || !seg || !xA || !tape || !lam || !lamA || !lamN || !pre || !gaF || !gHv || !g_alpha || !g_alpha_c ||
+        !g_T || !g_u || !g_ur || !g_uZ || !fin || !wsp || !edge || !win || !finwin)
+        return fail(c, LYD_ERR_NOMEM, "adjoint workspace: " + c->msg);
+    auto copy_state = [&](double *dst, int set) -> int {
+        for (int q = 0; q < 3; q++)
+            LYD_CU(c, cudaMemcpyAsync(dst + q * n3, c->set[set][q], n3 * 8, cudaMemcpyDeviceToDevice, c->st));
+        return LYD_OK;
+    };
+    auto load_state = [&](const double *src, int set) -> int {
+        for (int q = 0; q < 3; q++)
+            LYD_CU(c, cudaMemcpyAsync(c->set[set][q], src + q * n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
+        return LYD_OK;
+    };
+    // ---- forward sweep ----
+    LYD_CU(c, cudaMemsetAsync(c->step_ctr, 0, 2 * sizeof(int), c->st));
+    LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_R], 0, nc * 8, c->st));
+    LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_Z], 0, nc * 8, c->st));
+    if (!c->active_valid) LYD_TRY(run_find_active(c));
+    for (int n = 0; n < N; n++) {
+        if (n % K == 0) LYD_TRY(copy_state(ck + (size_t)(n / K) * S, c->cur));
+        LYD_CU(c, cudaMemcpyAsync(win + 2 * n, c->kwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+        LYD_TRY(enqueue_step<double>(c, false));
+    }
+    LYD_TRY(copy_state(fin, c->cur));
+    LYD_CU(c, cudaMemcpyAsync(finwin, c->kwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+    std::vector<int> hwin((size_t)2 * N);
+    std::vector<double> rec(7);
+    LYD_CU(c, cudaMemcpyAsync(hwin.data(), win, hwin.size() * sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    LYD_CU(c, cudaMemcpyAsync(rec.data(), c->hist + (size_t)(N - 1) * 7, 7 * 8, cudaMemcpyDeviceToHost, c->st));
+    LYD_TRY(check_err(c));
+    // objective: w_MF M_F(last step) + sum_k w_k S_k, S = edge-ring mean of the final J
+    const int ne = lyd_edge_count(nr, nz);
+    std::vector<double> spec(nnu, 0.0);
+    if (ne > 0) {
+        std::vector<double> raw((size_t)ne * nnu);
+        launch_edge(c->sprec, Jc(c, 0), c->dnu, nnu, nr, nz, c->jscale, edge, edge + (size_t)ne * nnu, c->st);
+        LYD_CU(c, cudaMemcpyAsync(raw.data(), edge, raw.size() * 8, cudaMemcpyDeviceToHost, c->st));
+        LYD_CU(c, cudaStreamSynchronize(c->st));
+        for (int e = 0; e < ne; e++)
+            for (int k = 0; k < nnu; k++) spec[k] += raw[(size_t)e * nnu + k] / ne;
+    }
+    double obj = cfg->w_MF * rec[0];
+    if (cfg->w_spec)
+        for (int k = 0; k < nnu; k++) obj += cfg->w_spec[k] * spec[k];
+    if (out->objective) *out->objective = obj;
+    if (out->M_F) *out->M_F = rec[0];
+    if (out->spectrum)
+        for (int k = 0; k < nnu; k++) out->spectrum[k] = spec[k];
+    // L of the normalisation: the record holds L_tot (x2 with a reflecting bottom)
+    const double Lsim = (p->bc_z_bot == LYD_BC_REFLECT) ? 0.5 * rec[3] : rec[3];
+    const double mf_w = (Lsim > 0.0) ? cfg->w_MF * kC / Lsim : 0.0;
+    // ---- reverse sweep ----
+    if (cfg->w_spec && ne > 0) {
+        LYD_CU(c, cudaMemcpyAsync(wsp, cfg->w_spec, nnu * 8, cudaMemcpyHostToDevice, c->st));
+        launch_seed_spectrum(lam, wsp, nnu, nr, nz, c->st);
+    }
+    const int B = 1 - c->cur;
+    for (int g = nseg - 1; g >= 0; g--) {
+        const int n0 = g * K, n1 = (n0 + K < N) ? n0 + K : N;
+        LYD_TRY(load_state(ck + (size_t)g * S, c->cur));
+        for (int n = n0; n < n1; n++) {
+            LYD_TRY(copy_state(seg + (size_t)(n - n0) * S, c->cur));
+            if (n + 1 < n1) {
+                LYD_CU(c, cudaMemcpyAsync(c->kwin, win + 2 * n, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+                LYD_CU(c, cudaMemsetAsync(c->step_ctr, 0, 2 * sizeof(int), c->st));
+                LYD_TRY(enqueue_step<double>(c, false));
+            }
+        }
+        for (int n = n1 - 1; n >= n0; n--) {
+            const double *sn = seg + (size_t)(n - n0) * S;
+            // x_A = advection of s_n in the step's window, with its tape
+            AdvArgs<double> aa;
+            fill_adv<double>(c, aa, c->cur, B);
+            aa.J = sn; aa.Hr = sn + n3; aa.HZ = sn + 2 * n3;
+            aa.Jo = xA; aa.Hro = xA + n3; aa.HZo = xA + 2 * n3;
+            aa.kwin = win + 2 * n;
+            aa.tape = tape;
+            aa.tape_stride = (long long)n3;
+            launch_advect(LYD_PREC_FP64, c->cfg.flux_method, &aa, c->ntiles, 2, c->st);
+            // frequency step adjoint: lambda_{n+1} -> lambda of x_A
+            FreqAdjArgs fa;
+            memset(&fa, 0, sizeof(fa));
+            fa.J = xA; fa.Hr = xA + n3; fa.HZ = xA + 2 * n3;
+            fa.Hv = (const double *)c->Hv;
+            fa.phi = c->phi ? (const double *)c->phi : nullptr;
+            fa.phi_inv = c->phi_inv; fa.phi_kmin = c->phi_kmin; fa.phi_kmax = c->phi_kmax;
+            fa.alpha = c->cellf[CF_ALPHA]; fa.alpha_c = c->cellf[CF_ALPHA_C];
+            fa.alpha_cF = any_have(c, 1u << CF_ALPHA_CF) ? c->cellf[CF_ALPHA_CF] : nullptr;
+            fa.pd = c->cellf[CF_PD]; fa.js = c->cellf[CF_JS]; fa.T = c->cellf[CF_T];
+            fa.dur_dr = c->cellf[CF_DUR_DR]; fa.dur_dZ = c->cellf[CF_DUR_DZ]; fa.duZ_dr = c->cellf[CF_DUZ_DR];
+            fa.duZ_dZ = c->cellf[CF_DUZ_DZ]; fa.ur_over_r = c->cellf[CF_UR_OVER_R];
+            fa.nu = c->nu; fa.nuC = c->nuC; fa.dnu = c->dnu; fa.inv_dnu = c->inv_dnu; fa.inv_nuC = c->inv_nuC;
+            fa.dV = c->dV; fa.cl = c->cl; fa.items = c->items;
+            fa.alpha_floor = c->cfg.alpha_floor; fa.jeps = c->jeps_s; fa.heps2 = c->heps2_s; fa.j_scale = c->jscale;
+            fa.recoil = c->cfg.recoil; fa.nnu = nnu; fa.ncell = (long long)nc;
+            fa.gJ = lam; fa.gHr = lam + n3; fa.gHZ = lam + 2 * n3;
+            fa.oJ = lamA; fa.oHr = lamA + n3; fa.oHZ = lamA + 2 * n3;
+            fa.g_alpha = g_alpha; fa.g_alpha_c = g_alpha_c; fa.g_T = g_T; fa.g_u = g_u; fa.g_Hv = gHv;
+            fa.mf_seed = (n == N - 1) && mf_w != 0.0;
+            fa.mf_w = mf_w;
+            launch_freq_adj(fa, c->nitems, c->st);
+            // advection adjoint: lambda of x_A -> lambda_n
+            AdjAdvArgs ad;
+            memset(&ad, 0, sizeof(ad));
+            ad.J = sn; ad.Hr = sn + n3; ad.HZ = sn + 2 * n3;
+            ad.tape = tape; ad.n3 = (long long)n3;
+            ad.gJ = lamA; ad.gHr = lamA + n3; ad.gHZ = lamA + 2 * n3;
+            ad.lJ = lamN; ad.lHr = lamN + n3; ad.lHZ = lamN + 2 * n3;
+            ad.pJ = pre; ad.pHr = pre + n3; ad.pHZ = pre + 2 * n3;
+            ad.Hv = (const double *)c->Hv; ad.alpha = c->cellf[CF_ALPHA]; ad.alpha_cF = fa.alpha_cF;
+            ad.A_r = c->A_r; ad.A_Z = c->A_Z; ad.inv_dV = c->inv_dV; ad.inv_r_cell = c->inv_r_cell;
+            ad.rint = c->rint; ad.zint = c->zint; ad.u_r_star = c->u_r_star; ad.u_Z_star = c->u_Z_star;
+            ad.dur_dr = fa.dur_dr; ad.dur_dZ = fa.dur_dZ; ad.duZ_dr = fa.duZ_dr; ad.duZ_dZ = fa.duZ_dZ;
+            ad.ur_over_r = fa.ur_over_r;
+            ad.g_aF = gaF; ad.g_u = g_u; ad.g_ur = g_ur; ad.g_uZ = g_uZ;
+            ad.nnu = nnu; ad.nr = nr; ad.nz = nz; ad.kmin = hwin[2 * n]; ad.kmax = hwin[2 * n + 1];
+            ad.bc_r_right = p->bc_r_right; ad.bc_z_bot = p->bc_z_bot; ad.bc_z_top = p->bc_z_top;
+            ad.ctdt = p->c_tilde * p->dt; ad.jeps = c->jeps_s; ad.heps2 = c->heps2_s;
+            launch_adv_adj(ad, c->st);
+            LYD_CU(c, cudaGetLastError());
+            double *t = lam;
+            lam = lamN;
+            lamN = t;
+        }
+    }
+    // alpha_F = alpha H_voigt ; H_voigt(T) when it was computed on the device
+    launch_af_params(gaF, c->cellf[CF_ALPHA], (const double *)c->Hv, nnu, (long long)nc, g_alpha, gHv, c->st);
+    if (c->hv_from_T && c->lut)
+        launch_hvoigt_adj(gHv, c->cellf[CF_T], c->nu, c->nuC, nnu, (long long)nc, c->lut, kLutN, kLutXmax, g_T, c->st);
+    LYD_CU(c, cudaGetLastError());
+    auto down = [&](double *host, const double *dev, size_t n) -> int {
+        if (host) LYD_CU(c, cudaMemcpyAsync(host, dev, n * 8, cudaMemcpyDeviceToHost, c->st));
+        return LYD_OK;
+    };
+    LYD_TRY(down(out->grad_alpha, g_alpha, nc));
+    LYD_TRY(down(out->grad_alpha_c, g_alpha_c, nc));
+    LYD_TRY(down(out->grad_T, g_T, nc));
+    LYD_TRY(down(out->grad_Hv, gHv, n3));
+    LYD_TRY(down(out->grad_u_r_star, g_ur, c->nrf));
+    LYD_TRY(down(out->grad_u_Z_star, g_uZ, c->nzf));
+    for (int q = 0; q < 5; q++) LYD_TRY(down(out->grad_du[q], g_u + (size_t)q * nc, nc));
+    // lambda of the initial state, back in the caller's units (the state is held as value / j_scale)
+    LYD_TRY(down(out->grad_J0, lam, n3));
+    LYD_TRY(down(out->grad_H_r0, lam + n3, n3));
+    LYD_TRY(down(out->grad_H_Z0, lam + 2 * n3, n3));
+    // the context ends in the forward sweep's final state
+    LYD_TRY(load_state(fin, c->cur));
+    LYD_CU(c, cudaMemcpyAsync(c->kwin, finwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+    c->old_alias = true;
+    c->active_valid = true;
+    return check_err(c);
 }

@@ -61,6 +61,9 @@ struct AdvArgs {
     int rows;                    // rows per tile
     int nnu;
     double jeps, heps2;          // closure floors in storage units
+    double *tape;                // adjoint recomputation: the cell update's values before its
+                                 // floors and limiter, 4 fields of tape_stride (or nullptr)
+    long long tape_stride;
 };
 
 // Emission/absorption + frequency step + flux correction (+ partial reductions).

@@ -321,6 +321,7 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
                     HZn = uHZ - S((wrR * FR[64] - wrL * FL[64]) + (wzR * zR[2] - wzL * zL[2]));
                     Hrn = uHr - S((wrR * FR[32] - wrL * FL[32]) + (wzR * zR[1] - wzL * zL[1]));
                 }
+                const S Jn0 = Jn;
                 Jn = Jn > ujeps ? Jn : ujeps;
                 R ga = R(__ldg(a.dur_dr + c)), gb = R(__ldg(a.dur_dZ + c)), gc = R(__ldg(a.duZ_dr + c));
                 R gd = R(__ldg(a.duZ_dZ + c)), ge = R(__ldg(a.ur_over_r + c));
@@ -336,6 +337,13 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
                 Hrn = Hrn + S(dHr);
                 HZn = HZn + S(dHZ);
                 Jn = Jn - S(cc * DdU * sJ);
+                if (a.tape) {
+                    // the values before the floors and the causality limiter, for the adjoint
+                    a.tape[x] = double(Jn0);
+                    a.tape[x + a.tape_stride] = double(Jn);
+                    a.tape[x + 2 * a.tape_stride] = double(Hrn);
+                    a.tape[x + 3 * a.tape_stride] = double(HZn);
+                }
                 Jn = Jn > ujeps ? Jn : ujeps;
                 S H2 = Hrn * Hrn + HZn * HZn;
                 if (H2 > Jn * Jn) {

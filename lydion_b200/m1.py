@@ -161,6 +161,40 @@ class M1Context:
         self._ck(lib().lyd_get_tuning(self._h, C.byref(t)))
         return t.rows_per_tile, t.cells_per_block, t.solver, t.adv_ctas_per_sm
 
+    # -- adjoint ---------------------------------------------------------------------------
+    def adjoint(self, n_steps, c_tilde, dt, z_center, bc_r_right=BC_OUTFLOW, bc_z_bot=BC_REFLECT,
+                bc_z_top=BC_OUTFLOW, w_MF=1.0, w_spec=None, checkpoint_every=0, want=None):
+        """Gradients of  w_MF * M_F(last step) + sum_k w_spec[k] * S_k(final J)  over n_steps
+        static-driver steps from the current state (lyd_adjoint_run); the context ends in
+        the final state. Returns a dict: objective, M_F, spectrum and the gradients
+        grad_alpha, grad_alpha_c, grad_T, grad_Hv, grad_u_r_star, grad_u_Z_star,
+        grad_dur_dr, grad_dur_dZ, grad_duZ_dr, grad_duZ_dZ, grad_ur_over_r, grad_J0,
+        grad_H_r0, grad_H_Z0 (numpy arrays in the reference's memory order)."""
+        nr, nz, nnu = self.n_r, self.n_z, self.n_nu
+        p = _lib.StepParams(float(c_tilde), float(dt), float(z_center), bc_r_right, bc_z_bot, bc_z_top, int(n_steps))
+        ws = None if w_spec is None else _c64(w_spec)
+        cfg = _lib.AdjointCfg(p, int(checkpoint_every), 0, float(w_MF), _dp(ws) if ws is not None else None)
+        shapes = {"objective": (1,), "M_F": (1,), "spectrum": (nnu,), "grad_alpha": (nz, nr),
+                  "grad_alpha_c": (nz, nr), "grad_T": (nz, nr), "grad_Hv": (nz, nr, nnu),
+                  "grad_u_r_star": (nz, nr + 1), "grad_u_Z_star": (nz + 1, nr),
+                  "grad_J0": (nz, nr, nnu), "grad_H_r0": (nz, nr, nnu), "grad_H_Z0": (nz, nr, nnu)}
+        du = ("grad_dur_dr", "grad_dur_dZ", "grad_duZ_dr", "grad_duZ_dZ", "grad_ur_over_r")
+        res = {k: np.zeros(v) for k, v in shapes.items() if want is None or k in want or k in ("objective", "M_F", "spectrum")}
+        for k in du:
+            if want is None or k in want:
+                res[k] = np.zeros((nz, nr))
+        o = _lib.AdjointOut()
+        for name in shapes:
+            if name in res:
+                setattr(o, name, _dp(res[name]))
+        for q, k in enumerate(du):
+            if k in res:
+                o.grad_du[q] = _dp(res[k])
+        self._ck(lib().lyd_adjoint_run(self._h, C.byref(cfg), C.byref(o)))
+        res["objective"] = float(res["objective"][0])
+        res["M_F"] = float(res["M_F"][0])
+        return res
+
     # -- set-up helpers --------------------------------------------------------------------
     def update_hvoigt(self):
         self._ck(lib().lyd_update_hvoigt(self._h))

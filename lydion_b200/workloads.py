@@ -56,6 +56,8 @@ class StaticCloud:
     alpha_floor: float
     tau0: float
     L_source: float
+    n_H: np.ndarray = None       # hydrogen density behind alpha (x_HI = 1), when the cloud is built from one
+    kappa_d: float = 0.0         # gray dust opacity per gram of dust behind alpha_c = kappa_d * 0.01 n_H m_H
 
     @property
     def n_nu(self):
@@ -187,6 +189,51 @@ def batch_clouds(n_clouds=512, n_nu=48, sides=C3_SIDES, seed=20261203, tau0_rang
 def config_c3(n_clouds=512, seed=20261203):
     """512 ragged static clouds x 48 bins, sides from {32, ..., 256} drawn independently in r and Z."""
     return batch_clouds(n_clouds=n_clouds, seed=seed)
+
+
+def gaussian_random_field(nr, nz, slope=-11.0 / 3.0, seed=20261207):
+    """Unit-variance Gaussian random field on an (n_z, n_r) grid with isotropic 2-D power
+    spectrum P(k) ~ k^slope, made by filtering seeded white noise in Fourier space."""
+    rng = np.random.default_rng(seed)
+    white = rng.standard_normal((nz, nr))
+    kz = np.fft.fftfreq(nz)[:, None]
+    kr = np.fft.rfftfreq(nr)[None, :]
+    k = np.hypot(kz, kr)
+    amp = np.zeros_like(k)
+    amp[k > 0] = k[k > 0] ** (0.5 * slope)
+    g = np.fft.irfft2(np.fft.rfft2(white) * amp, s=(nz, nr))
+    g -= g.mean()
+    return g / g.std()
+
+
+def turbulent_cloud(nr=128, nz=128, n_nu=48, n_mean=100.0, sigma_ln=1.0, T0=1e4, vmax_kms=50.0,
+                    dust_to_gas=0.01, tau_abs_mean=1.0, rs=0.5, seed=20261207, x_max=600.0, name="turbulent"):
+    """A static cloud with a lognormal turbulent density n_H = n_mean exp(sigma g - sigma^2/2)
+    (g a unit-variance Gaussian random field with P(k) ~ k^-11/3) inside R_cl, x_HI = 1 so
+    alpha = n_H sigma0(T), gray dust alpha_c = kappa_d dust_to_gas n_H m_H with kappa_d fixed so
+    that the mean density gives a dust optical depth tau_abs_mean across R_cl, a Hubble-like
+    radial outflow of v_max, and the uniform source of radius rs R_cl. The reference builds no
+    such field (its turbulence module perturbs velocities only); this generator is the
+    project's own."""
+    base = static_cloud(nr, nz, n_nu, tau0=1.0, T0=T0, rs=rs, umax_kms=vmax_kms, x_max=x_max, name=name)
+    g = gaussian_random_field(nr, nz, seed=seed)
+    nH = n_mean * np.exp(sigma_ln * g - 0.5 * sigma_ln ** 2)
+    inside = base.alpha > 0.0
+    kappa = tau_abs_mean / (dust_to_gas * n_mean * K.mH * K.pc)
+    sigma0 = K.compute_sigma0(T0)
+    base.alpha = np.where(inside, nH * sigma0, 0.0)
+    base.alpha_c = np.where(inside, kappa * dust_to_gas * nH * K.mH, 0.0)
+    base.n_H = np.where(inside, nH, 0.0)
+    base.kappa_d = kappa
+    base.tau0 = float(n_mean * sigma0 * K.pc)
+    return base
+
+
+def config_c4(scale=1):
+    """The adjoint configuration: 128 x 128 cells x 48 bins, lognormal turbulent n_H (sigma_ln = 1,
+    mean 100 cm^-3), T = 1e4 K, gray dust at 0.01 n_H, radial outflow v_max = 50 km/s."""
+    n = 128 // scale
+    return turbulent_cloud(nr=n, nz=n, n_nu=48 if scale == 1 else max(8, 48 // scale), name="c4_turbulent_128x128x48")
 
 
 def small_cloud(nr=12, nz=10, n_nu=16, **kw):

@@ -1,0 +1,158 @@
+"""The adjoint of the static-driver loop (lyd_adjoint_run) against central finite differences of
+the forward step, on a small seeded cloud.
+
+Objective: w_MF * M_F(last step) + sum_k w_k S_k(final J), S the edge-ring mean spectrum.
+Finite differences use h = 1e-4 relative (the perturbation of one input entry), as in the
+adjoint configuration this library is specified on. The FP64 step's own rounding (the stiff
+frequency solve, ~1e-13 relative) bounds how well a central difference can resolve the
+smallest gradients, so each check states its tolerance beside the quantity."""
+import numpy as np
+import pytest
+
+from helpers import random_state
+from lydion_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+H = 1e-4
+SS = 1e12     # scales the spectrum term so that both terms of the objective are O(1)
+
+
+def _cloud():
+    return W.small_cloud(nr=10, nz=9, n_nu=16)
+
+
+class Problem:
+    def __init__(self, n_steps):
+        self.cl = _cloud()
+        self.n = n_steps
+        self.w = np.random.default_rng(1).uniform(0.5, 1.5, self.cl.n_nu)
+        self.state = random_state(self.cl, 5)
+        c = self.cl
+        self.p = (c.c_tilde, c.dt, c.z_center, c.bc_r_right, c.bc_z_bot, c.bc_z_top)
+
+    def ctx(self, mod=None, state=None):
+        from lydion_b200.m1 import context_for_cloud
+        c = _cloud()
+        if mod:
+            mod(c)
+        ctx = context_for_cloud(c)
+        for name, a in zip(("J", "H_r", "H_Z"), state or self.state):
+            ctx.upload(name, a)
+            ctx.upload(name + "_old", a)
+        return ctx
+
+    def objective(self, mod=None, state=None):
+        ctx = self.ctx(mod, state)
+        h = ctx.static_steps(self.n, *self.p)
+        v = h[-1, 0] + SS * float(np.dot(self.w, ctx.edge_spectra()[0].mean(0)))
+        ctx.close()
+        return v
+
+    def adjoint(self, every=2):
+        ctx = self.ctx()
+        g = ctx.adjoint(self.n, *self.p, w_MF=1.0, w_spec=SS * self.w, checkpoint_every=every)
+        return ctx, g
+
+    def fd_field(self, field, idx):
+        v0 = getattr(self.cl, field)[idx]
+
+        def mk(s):
+            def m(c):
+                getattr(c, field)[idx] = v0 * (1 + s)
+            return m
+        return (self.objective(mk(H)) - self.objective(mk(-H))) / (2 * H), v0
+
+    def fd_state(self, q, idx):
+        base = self.state
+        x0 = base[q][idx]
+
+        def st(s):
+            out = [a.copy() for a in base]
+            out[q][idx] = x0 * (1 + s)
+            return out
+        return (self.objective(state=st(H)) - self.objective(state=st(-H))) / (2 * H), x0
+
+
+@pytest.fixture(scope="module")
+def prob():
+    P = Problem(6)
+    P.ctx_g = P.adjoint()
+    return P
+
+
+def test_objective_and_final_state(prob):
+    ctx, g = prob.ctx_g
+    assert abs(g["objective"] - prob.objective()) <= 1e-12 * abs(g["objective"])
+    # the context ends in the forward sweep's final state
+    ref = prob.ctx()
+    ref.static_steps(prob.n, *prob.p, history=False)
+    for f in ("J", "H_r", "H_Z"):
+        np.testing.assert_array_equal(ctx.download(f), ref.download(f))
+
+
+CELLS = [(2, 3), (4, 1), (0, 0), (6, 5)]
+
+
+@pytest.mark.parametrize("field,tol", [("alpha", 1e-5), ("alpha_c", 1e-5), ("T", 1e-5)])
+def test_opacity_and_temperature_gradients(prob, field, tol):
+    _, g = prob.ctx_g
+    for idx in CELLS:
+        d, v0 = prob.fd_field(field, idx)
+        adj = g["grad_" + field][idx] * v0
+        assert abs(adj - d) <= tol * abs(d), (field, idx, adj, d)
+
+
+@pytest.mark.parametrize("field", ["dur_dr", "duZ_dZ", "ur_over_r"])
+def test_velocity_gradient_gradients(prob, field):
+    # these gradients are ~1e-6 of the objective: central differences resolve them to ~1e-4
+    _, g = prob.ctx_g
+    for idx in CELLS[:2]:
+        d, v0 = prob.fd_field(field, idx)
+        adj = g["grad_" + field][idx] * v0
+        assert abs(adj - d) <= 3e-4 * abs(d), (field, idx, adj, d)
+
+
+def test_face_velocity_gradients(prob):
+    _, g = prob.ctx_g
+    for (j, i) in CELLS[:3]:
+        for field, idx in (("u_r_star", (j, i + 1)), ("u_Z_star", (j + 1, i))):
+            d, v0 = prob.fd_field(field, idx)
+            if v0 == 0.0:
+                continue
+            adj = g["grad_" + field][idx] * v0
+            assert abs(adj - d) <= 1e-4 * abs(d), (field, idx, adj, d)
+
+
+def test_initial_state_gradients(prob):
+    _, g = prob.ctx_g
+    for idx in [(2, 3, 7), (4, 1, 8), (6, 7, 5), (0, 0, 9)]:
+        for q, name in enumerate(("grad_J0", "grad_H_r0", "grad_H_Z0")):
+            d, x0 = prob.fd_state(q, idx)
+            adj = g[name][idx] * x0
+            if abs(d) < 1e-6:            # below what the difference resolves
+                assert abs(adj) < 1e-6
+                continue
+            assert abs(adj - d) <= 1e-5 * abs(d), (name, idx, adj, d)
+
+
+def test_checkpoint_spacing_does_not_change_gradients(prob):
+    # the face adjoints scatter with FP64 atomics: equal to rounding, not bitwise
+    _, g = prob.ctx_g
+    for every in (1, 4, prob.n):
+        _, g2 = prob.adjoint(every)
+        for k in ("grad_alpha", "grad_T", "grad_J0", "grad_u_r_star"):
+            np.testing.assert_allclose(g2[k], g[k], rtol=1e-10, atol=1e-11 * np.abs(g[k]).max())
+
+
+def test_adjoint_rejects_unsupported_forms():
+    from lydion_b200._lib import PREC_MIXED, LydionError
+    from lydion_b200.m1 import context_for_cloud
+    c = _cloud()
+    ctx = context_for_cloud(c, precision=PREC_MIXED)
+    with pytest.raises(LydionError):
+        ctx.adjoint(2, c.c_tilde, c.dt, c.z_center)
+    c2 = W.small_cloud(nr=10, nz=9, n_nu=16, flux_method=W.FLUX_HLL)
+    ctx2 = context_for_cloud(c2)
+    with pytest.raises(LydionError):
+        ctx2.adjoint(2, c2.c_tilde, c2.dt, c2.z_center)
