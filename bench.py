@@ -3,8 +3,8 @@ dusty outflowing cloud (tau0 = 1e8, tau_abs = 1, uniform source r_s = 0.5 R_cl, 
 outflow v_max = 200 km/s), one static-cloud driver iteration per step.
 
 The headline value is the mixed-precision form (FP64 state, FP32 advection arithmetic); the
-same line carries the plain-FP64 form, their ratio, and the ragged batch of 512 clouds
-(48 bins, sides 32..256) in both forms.
+same line carries the plain-FP64 form, their ratio, the ragged batch of 512 clouds (48 bins,
+sides 32..256) in both forms, and the adjoint/forward cost on the 128x128x48 turbulent cloud.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -264,6 +264,40 @@ def batch_form(args, barrier, stream_of, local, world):
     return out
 
 
+def adjoint_form(args, stream_of, local):
+    """Adjoint over forward cost on the turbulent cloud (128 x 128 x 48, lognormal n_H, dust,
+    v_max = 50 km/s): N forward steps from the graph-replayed step against lyd_adjoint_run of
+    the same N steps (its forward sweep, segment recomputation and reverse sweep), with the
+    state stored every 100 steps and, for comparison, every step."""
+    from lydion_b200 import adjoint as A
+    from lydion_b200 import workloads as W
+    from lydion_b200.m1 import context_for_cloud
+    cl = W.config_c4()
+    n = max(100, min(2000, args.steps))
+    p = (cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+    ctx = context_for_cloud(cl, device=local)
+    run = lambda k: ctx.static_steps(k, *p, history=False)
+    run(args.warmup)
+    ctx.synchronize()
+    fwd = _timed(ctx, run, n, stream_of)
+    w64 = np.full(64, 1.0 / 64)
+    w_MF, w_bins = A.objective_weights(cl.freq, 1.0, w64)
+    out = {"workload": "c4_turbulent_128x128x48", "steps": n, "forward_ms": fwd}
+    for every in (100, 1):
+        adj = _timed(ctx, lambda k: ctx.adjoint(k, *p, w_MF=w_MF, w_spec=1e12 * w_bins, checkpoint_every=every,
+                                                want=("grad_alpha",)), n, stream_of)
+        out[f"adjoint_ms_every_{every}"] = adj
+        out[f"ratio_every_{every}"] = adj / fwd
+    ctx.set_timing(True)
+    ctx.adjoint(n, *p, w_MF=w_MF, w_spec=1e12 * w_bins, checkpoint_every=100, want=("grad_alpha",))
+    ctx.set_timing(False)
+    ph = ctx.adjoint_timing()
+    out["phase_ms_every_100"] = {k: float(v) for k, v in zip(
+        ("forward_sweep", "recompute", "advect_with_tape", "frequency_adjoint", "advection_adjoint"), ph)}
+    ctx.close()
+    return out
+
+
 def run_gpu(args):
     import torch
     rank, world, local = rank_info()
@@ -290,6 +324,7 @@ def run_gpu(args):
     e2e = e2e_form(ctxm, cloud, args, barrier, stream_of, world)
     ctxm.close()
     batch = None if args.no_batch else batch_form(args, barrier, stream_of, local, world)
+    adj = None if (args.no_adjoint or world > 1) else adjoint_form(args, stream_of, local)
 
     # roofline of the dominant kernel of the headline (mixed) form
     names = ["advect", "freq", "reduce"]
@@ -314,7 +349,8 @@ def run_gpu(args):
                 "fp64": {"value": f64["value"], "ms_per_step": f64["ms_per_step"], "tuning": f64["tuning"],
                          "kernel_ms_per_step": {n: float(v) for n, v in zip(names, f64["kernel_ms"])}},
                 "mixed_over_fp64": mix["value"] / f64["value"],
-                "adjoint_over_forward": None,
+                "adjoint_over_forward": adj["ratio_every_100"] if adj else None,
+                "adjoint": adj,
                 "batch": batch,
                 "roofline": {"bound": "hbm", "kernel": "k_" + names[dom], "achieved": achieved,
                              "peak": peaks["hbm_gbs"], "peak_source": src, "unit": "GB/s",
@@ -340,6 +376,7 @@ def main():
     ap.add_argument("--impl", default="lydion", choices=["lydion", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-batch", action="store_true", help="skip the ragged-batch measurement")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -257,6 +257,10 @@ typedef struct lyd_adjoint_out { /* host arrays; any may be NULL */
 } lyd_adjoint_out;
 
 int  lyd_adjoint_run(lyd_ctx *ctx, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out);
+/* Device time of the phases of the last lyd_adjoint_run made with timing enabled (ms):
+ * forward sweep, segment recomputation, advection re-run with its tape, frequency-step
+ * adjoint, advection adjoint. */
+int  lyd_get_adjoint_timing(lyd_ctx *ctx, double ms[5]);
 
 /* ---- set-up and output helpers --------------------------------------------------------- */
 /* Update_Hvoigt! from the uploaded temperature, src/ConstantsAndFunctions.jl:319-357, using

@@ -116,6 +116,7 @@ SIGNATURES = {
     "lyd_set_tuning": (C.c_int, [VP, C.POINTER(Tuning)]),
     "lyd_get_tuning": (C.c_int, [VP, C.POINTER(Tuning)]),
     "lyd_adjoint_run": (C.c_int, [VP, C.POINTER(AdjointCfg), C.POINTER(AdjointOut)]),
+    "lyd_get_adjoint_timing": (C.c_int, [VP, P]),
     "lyd_update_hvoigt": (C.c_int, [VP]),
     "lyd_update_phi_nu": (C.c_int, [VP, I32, I32]),
     "lyd_pd_lya": (C.c_int, [VP, SZ, P, P, P, P, P, P, D, P]),

@@ -96,6 +96,7 @@ struct lyd_ctx {
     bool timing = false;
     cudaEvent_t ev[8] = {};
     double ms[3] = {0, 0, 0};
+    double adj_ms[5] = {0, 0, 0, 0, 0};
     std::string msg;
 };
 
@@ -1182,7 +1183,19 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
             LYD_CU(c, cudaMemcpyAsync(c->set[set][q], src + q * n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
         return LYD_OK;
     };
+    // phase timing (lyd_set_timing): events around the forward sweep and every reverse phase
+    const bool tm = c->timing;
+    double acc[5] = {0, 0, 0, 0, 0};
+    auto tick = [&](int e) { if (tm) cudaEventRecord(c->ev[e], c->st); };
+    auto tock = [&](int e0, int e1, int slot) {
+        if (!tm) return;
+        cudaEventSynchronize(c->ev[e1]);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev[e0], c->ev[e1]);
+        acc[slot] += ms;
+    };
     // ---- forward sweep ----
+    tick(0);
     LYD_CU(c, cudaMemsetAsync(c->step_ctr, 0, 2 * sizeof(int), c->st));
     LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_R], 0, nc * 8, c->st));
     LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_Z], 0, nc * 8, c->st));
@@ -1194,6 +1207,8 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     }
     LYD_TRY(copy_state(fin, c->cur));
     LYD_CU(c, cudaMemcpyAsync(finwin, c->kwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+    tick(1);
+    tock(0, 1, 0);
     std::vector<int> hwin((size_t)2 * N);
     std::vector<double> rec(7);
     LYD_CU(c, cudaMemcpyAsync(hwin.data(), win, hwin.size() * sizeof(int), cudaMemcpyDeviceToHost, c->st));
@@ -1228,6 +1243,7 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     const int B = 1 - c->cur;
     for (int g = nseg - 1; g >= 0; g--) {
         const int n0 = g * K, n1 = (n0 + K < N) ? n0 + K : N;
+        tick(0);
         LYD_TRY(load_state(ck + (size_t)g * S, c->cur));
         for (int n = n0; n < n1; n++) {
             LYD_TRY(copy_state(seg + (size_t)(n - n0) * S, c->cur));
@@ -1237,8 +1253,11 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
                 LYD_TRY(enqueue_step<double>(c, false));
             }
         }
+        tick(1);
+        tock(0, 1, 1);
         for (int n = n1 - 1; n >= n0; n--) {
             const double *sn = seg + (size_t)(n - n0) * S;
+            tick(2);
             // x_A = advection of s_n in the step's window, with its tape
             AdvArgs<double> aa;
             fill_adv<double>(c, aa, c->cur, B);
@@ -1248,6 +1267,7 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
             aa.tape = tape;
             aa.tape_stride = (long long)n3;
             launch_advect(LYD_PREC_FP64, c->cfg.flux_method, &aa, c->ntiles, 2, c->st);
+            tick(3);
             // frequency step adjoint: lambda_{n+1} -> lambda of x_A
             FreqAdjArgs fa;
             memset(&fa, 0, sizeof(fa));
@@ -1270,6 +1290,7 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
             fa.mf_seed = (n == N - 1) && mf_w != 0.0;
             fa.mf_w = mf_w;
             launch_freq_adj(fa, c->nitems, c->st);
+            tick(4);
             // advection adjoint: lambda of x_A -> lambda_n
             AdjAdvArgs ad;
             memset(&ad, 0, sizeof(ad));
@@ -1288,6 +1309,10 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
             ad.bc_r_right = p->bc_r_right; ad.bc_z_bot = p->bc_z_bot; ad.bc_z_top = p->bc_z_top;
             ad.ctdt = p->c_tilde * p->dt; ad.jeps = c->jeps_s; ad.heps2 = c->heps2_s;
             launch_adv_adj(ad, c->st);
+            tick(5);
+            tock(2, 3, 2);
+            tock(3, 4, 3);
+            tock(4, 5, 4);
             LYD_CU(c, cudaGetLastError());
             double *t = lam;
             lam = lamN;
@@ -1314,10 +1339,18 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     LYD_TRY(down(out->grad_J0, lam, n3));
     LYD_TRY(down(out->grad_H_r0, lam + n3, n3));
     LYD_TRY(down(out->grad_H_Z0, lam + 2 * n3, n3));
+    if (tm)
+        for (int q = 0; q < 5; q++) c->adj_ms[q] = acc[q];
     // the context ends in the forward sweep's final state
     LYD_TRY(load_state(fin, c->cur));
     LYD_CU(c, cudaMemcpyAsync(c->kwin, finwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
     c->old_alias = true;
     c->active_valid = true;
     return check_err(c);
+}
+
+int lyd_get_adjoint_timing(lyd_ctx *c, double ms[5]) {
+    if (!c || !ms) return LYD_ERR_ARG;
+    for (int q = 0; q < 5; q++) ms[q] = c->adj_ms[q];
+    return LYD_OK;
 }

@@ -195,6 +195,13 @@ class M1Context:
         res["M_F"] = float(res["M_F"][0])
         return res
 
+    def adjoint_timing(self):
+        """ms of the last timed adjoint: forward sweep, recomputation, advection re-run,
+        frequency-step adjoint, advection adjoint."""
+        ms = np.zeros(5)
+        self._ck(lib().lyd_get_adjoint_timing(self._h, _dp(ms)))
+        return ms
+
     # -- set-up helpers --------------------------------------------------------------------
     def update_hvoigt(self):
         self._ck(lib().lyd_update_hvoigt(self._h))
