@@ -165,6 +165,11 @@ int  lyd_update_J_and_H(lyd_ctx *ctx, double dt, double c_tilde, int32_t update_
 /* Update_f_Lya_MF_L_Lya!, src/ConstantsAndFunctions.jl:588-674: fills f_r, f_Z on the
  * device and returns {M_F, M_F_radial_net, M_F_radial_out, L_tot} in out[4]. */
 int  lyd_force_multiplier(lyd_ctx *ctx, double dt, double z_center, int32_t bc_z_bot, double out[4]);
+/* The gravity method of Update_f_Lya_MF_L_Lya!, src/ConstantsAndFunctions.jl:691-804:
+ * f_grav_r, f_grav_Z are host arrays (n_r*n_z) of the gravitational force; out[5] =
+ * {M_F, M_F_antigravity, M_F_radial_net, M_F_radial_out, L_tot}. */
+int  lyd_force_multiplier_gravity(lyd_ctx *ctx, double dt, const double *f_grav_r, const double *f_grav_Z,
+                                  double z_center, int32_t bc_z_bot, double out[5]);
 /* Compute_f_esc_Lya_Cylindrical, src/ConstantsAndFunctions.jl:969-993 */
 int  lyd_f_esc(lyd_ctx *ctx, double L_allspace, int32_t bc_z_bot, double *f_esc);
 /* Reset_Delta_rho_u!, src/ConstantsAndFunctions.jl:809-816 */

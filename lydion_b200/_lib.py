@@ -101,6 +101,7 @@ SIGNATURES = {
     "lyd_frequency_update": (C.c_int, [VP, D, I32]),
     "lyd_update_J_and_H": (C.c_int, [VP, D, D, I32, I32, I32, I32, I32]),
     "lyd_force_multiplier": (C.c_int, [VP, D, D, I32, P]),
+    "lyd_force_multiplier_gravity": (C.c_int, [VP, D, P, P, D, I32, P]),
     "lyd_f_esc": (C.c_int, [VP, D, I32, P]),
     "lyd_reset_dru": (C.c_int, [VP]),
     "lyd_static_steps": (C.c_int, [VP, C.POINTER(StepParams), C.POINTER(Diag)]),

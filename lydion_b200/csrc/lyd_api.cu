@@ -815,33 +815,60 @@ static int single_cloud(lyd_ctx *c, const char *what) {
     return LYD_OK;
 }
 
-int lyd_force_multiplier(lyd_ctx *c, double dt, double zc, int32_t bc_z_bot, double out[4]) {
-    if (!c || !out) return LYD_ERR_ARG;
+// Update_f_Lya_MF_L_Lya!, src/ConstantsAndFunctions.jl:588-674, and (g_r != nullptr, host
+// arrays) its gravity variant, :691-804.
+static int force_multiplier(lyd_ctx *c, double dt, double zc, int32_t bc_z_bot, const double *g_r,
+                            const double *g_Z, double *out) {
     LYD_TRY(single_cloud(c, "lyd_force_multiplier"));
     cudaSetDevice(c->dev);
     if (!all_have(c, BIT_GEOM)) return fail(c, LYD_ERR_STATE, "geometry not set");
     if (!(dt > 0.0)) return fail(c, LYD_ERR_ARG, "dt must be positive");
     const int nr = c->nr[0], nz = c->nz[0];
     const int nb = std::min(c->nitems, 4 * c->sms);
+    double *dg = nullptr;
+    if (g_r) {
+        LYD_TRY(dalloc(c, (void **)&dg, 2 * c->ncell * 8));
+        int r = h2d(c, dg, g_r, c->ncell);
+        if (r == LYD_OK) r = h2d(c, dg + c->ncell, g_Z, c->ncell);
+        if (r != LYD_OK) { cudaFree(dg); return r; }
+    }
     launch_mf(c->cellf[CF_DRU_R], c->cellf[CF_DRU_Z], c->cellf[CF_F_R], c->cellf[CF_F_Z], c->cellf[CF_JS], c->dV,
-              c->rCoM, c->ZCoM, nr, nz, dt, zc, c->partials, nb, c->st);
-    launch_column_sums(c->partials, 4, nb, c->small, c->st);
-    LYD_CU(c, cudaGetLastError());
-    double h[4];
-    LYD_CU(c, cudaMemcpyAsync(h, c->small, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+              c->rCoM, c->ZCoM, nr, nz, dt, zc, dg, dg ? dg + c->ncell : nullptr, c->partials, nb, c->st);
+    launch_column_sums(c->partials, 5, nb, c->small, c->st);
+    double h[5];
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, c->small, sizeof(h), cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    cudaFree(dg);
+    if (e != cudaSuccess) return fail(c, LYD_ERR_CUDA, cudaGetErrorString(e));
     LYD_TRY(check_err(c));
     set_all(c, (1u << CF_F_R) | (1u << CF_F_Z));
-    // normalisation, src/ConstantsAndFunctions.jl:652-673
-    double MF = h[0], net = h[1], outw = h[2], L = h[3];
+    // normalisation, src/ConstantsAndFunctions.jl:652-673 / 780-795
+    double MF = h[0], net = h[1], outw = h[2], L = h[3], anti = h[4];
     if (L > 0.0) {
         double k = 1.0 / (L / kC);
-        MF *= k; net *= k; outw *= k;
+        MF *= k; net *= k; outw *= k; anti *= k;
     } else {
-        MF = net = outw = 0.0;
+        MF = net = outw = anti = 0.0;
     }
-    out[0] = MF; out[1] = net; out[2] = outw;
-    out[3] = (bc_z_bot == LYD_BC_REFLECT) ? 2.0 * L : L;
+    double Ltot = (bc_z_bot == LYD_BC_REFLECT) ? 2.0 * L : L;
+    if (g_r) {
+        out[0] = MF; out[1] = anti; out[2] = net; out[3] = outw; out[4] = Ltot;
+    } else {
+        out[0] = MF; out[1] = net; out[2] = outw; out[3] = Ltot;
+    }
     return LYD_OK;
+}
+
+int lyd_force_multiplier(lyd_ctx *c, double dt, double zc, int32_t bc_z_bot, double out[4]) {
+    if (!c || !out) return LYD_ERR_ARG;
+    return force_multiplier(c, dt, zc, bc_z_bot, nullptr, nullptr, out);
+}
+
+int lyd_force_multiplier_gravity(lyd_ctx *c, double dt, const double *g_r, const double *g_Z, double zc,
+                                 int32_t bc_z_bot, double out[5]) {
+    if (!c || !out || !g_r || !g_Z) return LYD_ERR_ARG;
+    return force_multiplier(c, dt, zc, bc_z_bot, g_r, g_Z, out);
 }
 
 int lyd_f_esc(lyd_ctx *c, double L_all, int32_t bc_z_bot, double *f) {

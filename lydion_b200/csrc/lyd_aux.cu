@@ -219,12 +219,13 @@ __device__ __forceinline__ double wsum(double v) {
 }
 
 // Update_f_Lya_MF_L_Lya!, src/ConstantsAndFunctions.jl:606-650: f = dru / dt stored, and the
-// per-CTA partial sums of dV|f|, dV f.r_out, dV max(f.r_out,0), 4 pi dV js (4 columns).
+// per-CTA partial sums of dV|f|, dV f.r_out, dV max(f.r_out,0), 4 pi dV js and, with a gravity
+// field (the variant of src/ConstantsAndFunctions.jl:691-804), dV (-f . g_hat) (5 columns).
 __global__ void k_mf(const double *dru_r, const double *dru_Z, double *f_r, double *f_Z, const double *js,
                      const double *dV, const double *rCoM, const double *ZCoM, int nr, int nz, double dt,
-                     double z_center, double *partials) {
-    __shared__ double sh[4][32];
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+                     double z_center, const double *g_r, const double *g_Z, double *partials) {
+    __shared__ double sh[5][32];
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0;
     const double inv_dt = 1.0 / dt;
     const int ncell = nr * nz;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
@@ -244,12 +245,17 @@ __global__ void k_mf(const double *dru_r, const double *dru_Z, double *f_r, doub
         }
         a1 += v * frad;
         a2 += v * (frad > 0.0 ? frad : 0.0);
+        if (g_r) {
+            double gr = g_r[c], gz = g_Z[c];
+            double gm = sqrt(gr * gr + gz * gz);
+            a4 += v * (gm > 0.0 ? -(fr * gr + fz * gz) / gm : 0.0);
+        }
     }
     int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    a0 = wsum(a0); a1 = wsum(a1); a2 = wsum(a2); a3 = wsum(a3);
-    if (lane == 0) { sh[0][w] = a0; sh[1][w] = a1; sh[2][w] = a2; sh[3][w] = a3; }
+    a0 = wsum(a0); a1 = wsum(a1); a2 = wsum(a2); a3 = wsum(a3); a4 = wsum(a4);
+    if (lane == 0) { sh[0][w] = a0; sh[1][w] = a1; sh[2][w] = a2; sh[3][w] = a3; sh[4][w] = a4; }
     __syncthreads();
-    if (threadIdx.x < 4) {
+    if (threadIdx.x < 5) {
         double s = 0.0;
         for (int q = 0; q < (int)(blockDim.x >> 5); q++) s += sh[threadIdx.x][q];
         partials[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = s;
@@ -257,8 +263,10 @@ __global__ void k_mf(const double *dru_r, const double *dru_Z, double *f_r, doub
 }
 void launch_mf(const double *dru_r, const double *dru_Z, double *f_r, double *f_Z, const double *js,
                const double *dV, const double *rCoM, const double *ZCoM, int nr, int nz, double dt,
-               double z_center, double *partials, int nblocks, cudaStream_t st) {
-    k_mf<<<nblocks, 256, 0, st>>>(dru_r, dru_Z, f_r, f_Z, js, dV, rCoM, ZCoM, nr, nz, dt, z_center, partials);
+               double z_center, const double *g_r, const double *g_Z, double *partials, int nblocks,
+               cudaStream_t st) {
+    k_mf<<<nblocks, 256, 0, st>>>(dru_r, dru_Z, f_r, f_Z, js, dV, rCoM, ZCoM, nr, nz, dt, z_center, g_r, g_Z,
+                                  partials);
 }
 
 // Compute_f_esc_Lya_Cylindrical numerator, src/ConstantsAndFunctions.jl:969-993 / 914-961:

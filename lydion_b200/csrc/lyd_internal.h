@@ -142,7 +142,8 @@ void launch_pd(size_t n, const double *nHII, const double *ne, const double *nHI
                const double *nH2, const double *T, double z, double *out, cudaStream_t st);
 void launch_mf(const double *dru_r, const double *dru_Z, double *f_r, double *f_Z, const double *js,
                const double *dV, const double *rCoM, const double *ZCoM, int nr, int nz, double dt,
-               double z_center, double *partials, int nblocks, cudaStream_t st);
+               double z_center, const double *g_r, const double *g_Z, double *partials, int nblocks,
+               cudaStream_t st);   // g_r/g_Z: gravity field for M_F_antigravity, or nullptr
 void launch_fesc(int prec, const void *Hr, const void *HZ, const double *A_r, const double *A_Z,
                  const double *dnu, int nnu, int nr, int nz, int bc_z_bot, double j_scale,
                  double *out, cudaStream_t st);

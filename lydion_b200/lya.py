@@ -9,6 +9,7 @@ place, as the Julia functions mutate theirs.
     FrequencyUpdateJLyα_AllCells!    -> frequency_update_J_lya_all_cells   (src/UpdateLyaJandH.jl:231)
     UpdateLyαJandH!                  -> update_lya_J_and_H                 (src/UpdateLyaJandH.jl:409)
     Update_f_Lyα_MF_L_Lyα!           -> update_f_lya_MF_L_lya              (src/ConstantsAndFunctions.jl:588)
+      (gravity method)               -> update_f_lya_MF_L_lya_gravity      (src/ConstantsAndFunctions.jl:691)
     Compute_f_esc_Lyα_Cylindrical    -> compute_f_esc_lya_cylindrical      (src/ConstantsAndFunctions.jl:969)
     FindActiveBins                   -> find_active_bins                   (src/UpdateLyaJandH.jl:47)
     pd_Lyα                           -> pd_lya                             (src/LymanAlphaDestruction.jl:43)
@@ -208,6 +209,19 @@ def update_f_lya_MF_L_lya(f_r, f_Z, dru_r, dru_Z, js, dV, rCoM, ZCoM, dt, z_cent
     for name, a in (("dru_r", dru_r), ("dru_Z", dru_Z), ("js", js)):
         ctx.upload(name, a)
     out = ctx.force_multiplier(dt, z_center, _bc(BC_Z_bot))
+    f_r[...] = ctx.download("f_r")
+    f_Z[...] = ctx.download("f_Z")
+    return tuple(float(v) for v in out)
+
+
+def update_f_lya_MF_L_lya_gravity(f_r, f_Z, dru_r, dru_Z, js, dV, rCoM, ZCoM, dt, f_grav_r, f_grav_Z, z_center,
+                                  BC_Z_bot="Reflect", *, lya, geom):
+    """The gravity method of Update_f_Lya_MF_L_Lya! (src/ConstantsAndFunctions.jl:691-804) ->
+    (M_F, M_F_antigravity, M_F_radial_net, M_F_radial_out, L_tot); fills f_r, f_Z."""
+    ctx = _cache.get(lya, geom)
+    for name, a in (("dru_r", dru_r), ("dru_Z", dru_Z), ("js", js)):
+        ctx.upload(name, a)
+    out = ctx.force_multiplier(dt, z_center, _bc(BC_Z_bot), f_grav=(f_grav_r, f_grav_Z))
     f_r[...] = ctx.download("f_r")
     f_Z[...] = ctx.download("f_Z")
     return tuple(float(v) for v in out)

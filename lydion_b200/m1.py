@@ -118,9 +118,17 @@ class M1Context:
         self._ck(lib().lyd_update_J_and_H(self._h, float(dt), float(c_tilde), int(bool(update_freq_factors)),
                                           bc_r_left, bc_r_right, bc_z_bot, bc_z_top))
 
-    def force_multiplier(self, dt, z_center, bc_z_bot=BC_REFLECT):
-        out = np.zeros(4)
-        self._ck(lib().lyd_force_multiplier(self._h, float(dt), float(z_center), bc_z_bot, _dp(out)))
+    def force_multiplier(self, dt, z_center, bc_z_bot=BC_REFLECT, f_grav=None):
+        """{M_F, net, out, L_tot}; with f_grav = (f_grav_r, f_grav_Z) the gravity method's
+        {M_F, M_F_antigravity, net, out, L_tot}."""
+        if f_grav is None:
+            out = np.zeros(4)
+            self._ck(lib().lyd_force_multiplier(self._h, float(dt), float(z_center), bc_z_bot, _dp(out)))
+            return out
+        gr, gz = _c64(f_grav[0]), _c64(f_grav[1])
+        out = np.zeros(5)
+        self._ck(lib().lyd_force_multiplier_gravity(self._h, float(dt), _dp(gr), _dp(gz), float(z_center), bc_z_bot,
+                                                    _dp(out)))
         return out
 
     def f_esc(self, L_allspace, bc_z_bot=BC_REFLECT):

@@ -834,6 +834,27 @@ void orc_update_f_mf(orc_lya *s, const orc_geom *g, double dt, double z_center, 
     out[3] = (bc_z_bot == ORC_BC_REFLECT) ? 2.0 * L : L;
 }
 
+/* Update_f_Lya_MF_L_Lya! with gravity, src/ConstantsAndFunctions.jl:691-804: the same f and
+ * M_F family plus M_F_antigravity = sum dV (-f . g_hat) / (L/c) (zero where g = 0).
+ * out = {M_F, M_F_antigravity, M_F_radial_net, M_F_radial_out, L_tot}. */
+void orc_update_f_mf_gravity(orc_lya *s, const orc_geom *g, double dt, const double *fg_r, const double *fg_Z,
+                             double z_center, int bc_z_bot, double out[5]) {
+    double base[4];
+    orc_update_f_mf(s, g, dt, z_center, bc_z_bot, base);
+    const int nr = s->nr, nz = s->nz;
+    double L = 0.0, anti = 0.0;
+    for (int j = 0; j < nz; j++)
+        for (int i = 0; i < nr; i++) {
+            int c = i + nr * j;
+            L += FOUR_PI * g->dV[c] * s->js[c];
+            double gm = sqrt(fg_r[c] * fg_r[c] + fg_Z[c] * fg_Z[c]);
+            double fa = gm > 0.0 ? -(s->f_r[c] * fg_r[c] + s->f_Z[c] * fg_Z[c]) / gm : 0.0;
+            anti += g->dV[c] * fa;
+        }
+    anti = L > 0.0 ? anti * (1.0 / (L / C_LIGHT)) : 0.0;
+    out[0] = base[0]; out[1] = anti; out[2] = base[1]; out[3] = base[2]; out[4] = base[3];
+}
+
 /* Compute_f_esc_Lya_Cylindrical + Compute_f_esc_Cylindrical:
  * src/ConstantsAndFunctions.jl:969-993, 914-961 */
 double orc_f_esc_lya(const orc_lya *s, const orc_geom *g, double L_all, int bc_z_bot) {

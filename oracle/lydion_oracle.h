@@ -124,6 +124,8 @@ int    orc_frequency_update_all_cells(orc_lya *s, const orc_vel *v, double ctdt,
 /* Update_f_Lya_MF_L_Lya!: out = {M_F, M_F_radial_net, M_F_radial_out, L_tot} */
 void   orc_update_f_mf(orc_lya *s, const orc_geom *g, double dt, double z_center,
                        int bc_z_bot, double out[4]);
+void   orc_update_f_mf_gravity(orc_lya *s, const orc_geom *g, double dt, const double *fg_r, const double *fg_Z,
+                               double z_center, int bc_z_bot, double out[5]);
 double orc_f_esc_lya(const orc_lya *s, const orc_geom *g, double L_allspace, int bc_z_bot);
 void   orc_reset_dru(orc_lya *s);
 double orc_cfl_dt(const orc_geom *g, double c_tilde, const double *u_r, const double *u_Z,

@@ -88,6 +88,7 @@ def _declare(L):
         "orc_update_freq_factors": (None, [C.c_void_p, C.c_void_p]),
         "orc_frequency_update_all_cells": (I, [C.c_void_p, C.c_void_p, D, I, C.POINTER(C.c_long)]),
         "orc_update_f_mf": (None, [C.c_void_p, C.c_void_p, D, D, I, P]),
+        "orc_update_f_mf_gravity": (None, [C.c_void_p, C.c_void_p, D, P, P, D, I, P]),
         "orc_f_esc_lya": (D, [C.c_void_p, C.c_void_p, D, I]),
         "orc_reset_dru": (None, [C.c_void_p]),
         "orc_cfl_dt": (D, [C.c_void_p, D, P, P, D]),
@@ -241,6 +242,14 @@ class OracleState:
     def force_multiplier(self, dt):
         out = np.zeros(4)
         lib().orc_update_f_mf(C.byref(self.s), C.byref(self.g), dt, self.cloud.z_center, self.cloud.bc_z_bot, _p(out))
+        return out
+
+    def force_multiplier_gravity(self, dt, f_grav_r, f_grav_Z):
+        out = np.zeros(5)
+        gr = np.ascontiguousarray(f_grav_r, dtype=np.float64)
+        gz = np.ascontiguousarray(f_grav_Z, dtype=np.float64)
+        lib().orc_update_f_mf_gravity(C.byref(self.s), C.byref(self.g), dt, _p(gr), _p(gz), self.cloud.z_center,
+                                      self.cloud.bc_z_bot, _p(out))
         return out
 
     def f_esc(self, L_all):

@@ -169,6 +169,25 @@ def test_diagnostics_match_oracle(oracle_mod):
     np.testing.assert_allclose(ng, no, rtol=1e-13)
 
 
+def test_gravity_force_multiplier_matches_oracle(oracle_mod):
+    """The gravity method of Update_f_Lya_MF_L_Lya! (src/ConstantsAndFunctions.jl:691-804)."""
+    cl = CLOUDS["glf_outflow"]()
+    st, ctx = matched_pair(oracle_mod, cl, seed=23)
+    st.emission_absorption(cl.c_tilde, cl.dt)
+    ctx.emission_absorption(cl.c_tilde, cl.dt)
+    rng = np.random.default_rng(4)
+    gr = rng.normal(size=(cl.nz, cl.nr))
+    gz = -np.abs(rng.normal(size=(cl.nz, cl.nr)))
+    gz[0, :3] = 0.0
+    gr[0, :3] = 0.0                    # cells without gravity contribute nothing
+    mo = st.force_multiplier_gravity(cl.dt, gr, gz)
+    mg = ctx.force_multiplier(cl.dt, cl.z_center, cl.bc_z_bot, f_grav=(gr, gz))
+    np.testing.assert_allclose(mg, mo, rtol=1e-12)
+    # without gravity the plain method's values
+    m4 = ctx.force_multiplier(cl.dt, cl.z_center, cl.bc_z_bot)
+    np.testing.assert_allclose(m4, mg[[0, 2, 3, 4]], rtol=1e-14)
+
+
 def test_device_hvoigt_and_phi_match_oracle(oracle_mod):
     cl = W.small_cloud(nr=6, nz=5, n_nu=64, x_max=600.0)
     cl.T = np.linspace(30.0, 3e4, cl.nr * cl.nz).reshape(cl.nz, cl.nr)

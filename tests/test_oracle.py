@@ -188,3 +188,25 @@ def test_static_run_is_finite_and_emits(oracle_mod):
     raw, norm, ri, zi = st.edge_spectra()
     assert raw.shape[0] == (cl.nz - 2) + 2 * (cl.nr - 3)
     assert np.all(ri[: cl.nz - 2] == cl.nr - 2)
+
+
+def test_gravity_force_multiplier_antiparallel(oracle_mod):
+    """With gravity exactly opposite to the radiation force in every cell, M_F_antigravity
+    equals M_F; with no gravity it is zero (src/ConstantsAndFunctions.jl:737-750)."""
+    from lydion_b200 import workloads as W
+    cl = W.small_cloud(nr=8, nz=7, n_nu=16)
+    st = oracle_mod.OracleState(cl)
+    st.setup_profiles()
+    rng = np.random.default_rng(0)
+    st.dru_r[...] = rng.normal(size=st.dru_r.shape)
+    st.dru_Z[...] = rng.normal(size=st.dru_Z.shape)
+    out = st.force_multiplier_gravity(cl.dt, -st.dru_r, -st.dru_Z)
+    st.dru_r[...] = st.f_r * cl.dt
+    st.dru_Z[...] = st.f_Z * cl.dt
+    plain = st.force_multiplier(cl.dt)
+    assert out[1] == pytest.approx(out[0], rel=1e-13)
+    np.testing.assert_allclose(out[[0, 2, 3, 4]], plain, rtol=1e-13)
+    st.dru_r[...] = st.f_r * cl.dt
+    st.dru_Z[...] = st.f_Z * cl.dt
+    z = np.zeros_like(st.dru_r)
+    assert st.force_multiplier_gravity(cl.dt, z, z)[1] == 0.0
