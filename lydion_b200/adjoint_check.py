@@ -1,6 +1,6 @@
 """Finite-difference check of the adjoint on the turbulent-cloud workload.
 
-    python -m lydion_b200.adjoint_check [--scale S] [--steps N] [--cells C] [--every K]
+    python -m lydion_b200.adjoint_check [--scale S] [--steps N] [--cells C] [--every K] [--h H]
 
 Objective: M_F of the last step plus the 64-point emergent spectrum (the edge-ring spectrum
 linearly interpolated onto 64 points in x), each point weighted by 1 / (64 * its mean value
@@ -103,8 +103,9 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--cells", type=int, default=64)
     ap.add_argument("--every", type=int, default=100)
+    ap.add_argument("--h", type=float, default=1e-4, help="relative finite-difference step")
     a = ap.parse_args()
-    print(json.dumps(run(a.scale, a.steps, a.cells, a.every)), flush=True)
+    print(json.dumps(run(a.scale, a.steps, a.cells, a.every, a.h)), flush=True)
 
 
 if __name__ == "__main__":

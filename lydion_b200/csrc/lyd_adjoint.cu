@@ -201,8 +201,10 @@ __device__ __forceinline__ void ff_adj(const FfIn &q, double gFp, double gF0, do
     }
 }
 
+// 2 CTAs per SM (128 registers, a few hundred bytes of spills) measured 1.7x faster than the
+// unconstrained 202-register form at 1 CTA per SM.
 template <int M>
-__global__ void __launch_bounds__(ADJ_THREADS) k_freq_adj(FreqAdjArgs a) {
+__global__ void __launch_bounds__(ADJ_THREADS, 2) k_freq_adj(FreqAdjArgs a) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int nnu = a.nnu;
     const int4 it = a.items[blockIdx.x];
@@ -589,8 +591,9 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adv_adj_cell(AdjAdvArgs a) {
 
 // One face's adjoint: warp = one face x 32 bins. ZDIR false: r faces f = 0..nr of row j;
 // true: Z faces f = 0..nz of column i.
+// 2 CTAs per SM: 1.4x faster than the unconstrained 206-register form.
 template <bool ZDIR>
-__global__ void __launch_bounds__(ADJ_THREADS) k_adv_adj_face(AdjAdvArgs a) {
+__global__ void __launch_bounds__(ADJ_THREADS, 2) k_adv_adj_face(AdjAdvArgs a) {
     const int lane = threadIdx.x & 31;
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nkb = (a.nnu + 31) / 32;
