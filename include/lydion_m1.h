@@ -263,8 +263,8 @@ typedef struct lyd_adjoint_out { /* host arrays; any may be NULL */
 
 int  lyd_adjoint_run(lyd_ctx *ctx, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out);
 /* Device time of the phases of the last lyd_adjoint_run made with timing enabled (ms):
- * forward sweep, segment recomputation, advection re-run with its tape, frequency-step
- * adjoint, advection adjoint. */
+ * forward sweep, segment recomputation (which also records the advection's tapes), 0
+ * (reserved), frequency-step adjoint, advection adjoint. */
 int  lyd_get_adjoint_timing(lyd_ctx *ctx, double ms[5]);
 
 /* ---- set-up and output helpers --------------------------------------------------------- */

@@ -1191,13 +1191,16 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
         mem.ptrs.push_back(q);
         return static_cast<double *>(q);
     };
-    double *ck = A((size_t)nseg * S * 8), *seg = A((size_t)K * S * 8), *xA = A(S * 8), *tape = A(4 * n3 * 8);
+    // checkpoints; and per step of one segment: the state, the advected state x_A and the
+    // advection's tape (recorded while the segment is recomputed)
+    double *ck = A((size_t)nseg * S * 8), *seg = A((size_t)K * S * 8), *segA = A((size_t)K * S * 8);
+    double *segT = A((size_t)K * 4 * n3 * 8);
     double *lam = A(S * 8), *lamA = A(S * 8), *lamN = A(S * 8), *pre = A(S * 8), *gaF = A(n3 * 8), *gHv = A(n3 * 8);
     double *g_alpha = A(nc * 8), *g_alpha_c = A(nc * 8), *g_T = A(nc * 8), *g_u = A(5 * nc * 8);
     double *g_ur = A(c->nrf * 8), *g_uZ = A(c->nzf * 8), *fin = A(S * 8), *wsp = A(nnu * 8), *edge = A(2 * (size_t)nnu * (nr + nz + 2 * nr) * 8);
     int *win = reinterpret_cast<int *>(A((size_t)N * 2 * sizeof(int) + 16));
     int *finwin = reinterpret_cast<int *>(A(16));
-    if (!ck || !seg || !xA || !tape || !lam || !lamA || !lamN || !pre || !gaF || !gHv || !g_alpha || !g_alpha_c ||
+    if (!ck || !seg || !segA || !segT || !lam || !lamA || !lamN || !pre || !gaF || !gHv || !g_alpha || !g_alpha_c ||
         !g_T || !g_u || !g_ur || !g_uZ || !fin || !wsp || !edge || !win || !finwin)
         return fail(c, LYD_ERR_NOMEM, "adjoint workspace: " + c->msg);
     auto copy_state = [&](double *dst, int set) -> int {
@@ -1272,28 +1275,35 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
         const int n0 = g * K, n1 = (n0 + K < N) ? n0 + K : N;
         tick(0);
         LYD_TRY(load_state(ck + (size_t)g * S, c->cur));
+        // recompute the segment: advection of s_n in the step's window into x_A with its tape,
+        // then (except after the last step) emission + frequency step x_A -> s_{n+1}
         for (int n = n0; n < n1; n++) {
-            LYD_TRY(copy_state(seg + (size_t)(n - n0) * S, c->cur));
-            if (n + 1 < n1) {
-                LYD_CU(c, cudaMemcpyAsync(c->kwin, win + 2 * n, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
-                LYD_CU(c, cudaMemsetAsync(c->step_ctr, 0, 2 * sizeof(int), c->st));
-                LYD_TRY(enqueue_step<double>(c, false));
-            }
-        }
-        tick(1);
-        tock(0, 1, 1);
-        for (int n = n1 - 1; n >= n0; n--) {
-            const double *sn = seg + (size_t)(n - n0) * S;
-            tick(2);
-            // x_A = advection of s_n in the step's window, with its tape
+            double *sn = seg + (size_t)(n - n0) * S, *xA = segA + (size_t)(n - n0) * S;
+            LYD_TRY(copy_state(sn, c->cur));
             AdvArgs<double> aa;
             fill_adv<double>(c, aa, c->cur, B);
             aa.J = sn; aa.Hr = sn + n3; aa.HZ = sn + 2 * n3;
             aa.Jo = xA; aa.Hro = xA + n3; aa.HZo = xA + 2 * n3;
             aa.kwin = win + 2 * n;
-            aa.tape = tape;
+            aa.tape = segT + (size_t)(n - n0) * 4 * n3;
             aa.tape_stride = (long long)n3;
             launch_advect(LYD_PREC_FP64, c->cfg.flux_method, &aa, c->ntiles, 2, c->st);
+            if (n + 1 < n1) {
+                FreqArgs<double> fq;
+                fill_freq<double>(c, fq, xA, xA + n3, xA + 2 * n3, xA, c->set[c->cur][0], c->set[c->cur][1],
+                                  c->set[c->cur][2]);
+                fq.do_emission = 1; fq.do_freq = 1; fq.update_ff = 1;
+                fq.parts = 0;
+                launch_freq(LYD_PREC_FP64, &fq, nnu, c->nitems, c->st);
+            }
+            LYD_CU(c, cudaGetLastError());
+        }
+        tick(1);
+        tock(0, 1, 1);
+        for (int n = n1 - 1; n >= n0; n--) {
+            const double *sn = seg + (size_t)(n - n0) * S;
+            const double *xA = segA + (size_t)(n - n0) * S, *tape = segT + (size_t)(n - n0) * 4 * n3;
+            tick(2);
             tick(3);
             // frequency step adjoint: lambda_{n+1} -> lambda of x_A
             FreqAdjArgs fa;

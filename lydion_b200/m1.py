@@ -204,8 +204,8 @@ class M1Context:
         return res
 
     def adjoint_timing(self):
-        """ms of the last timed adjoint: forward sweep, recomputation, advection re-run,
-        frequency-step adjoint, advection adjoint."""
+        """ms of the last timed adjoint: forward sweep, recomputation (with the advection's
+        tapes), 0 (reserved), frequency-step adjoint, advection adjoint."""
         ms = np.zeros(5)
         self._ck(lib().lyd_get_adjoint_timing(self._h, _dp(ms)))
         return ms
