@@ -467,6 +467,52 @@ __device__ __forceinline__ void thomas_solve(Row<M> &R_, int lane, double *sm) {
     __syncwarp();
 }
 
+// Two rows per lane (rows 2l and 2l+1): one cyclic-reduction step eliminates the odd rows,
+// leaving one row per lane, which parallel cyclic reduction across the warp solves in five
+// levels; the odd rows then follow by back-substitution. Half the divisions and shuffles of
+// PCR on all 64 rows, the same arithmetic per eliminated row. Returns x in d.
+__device__ __forceinline__ void cr_pcr_solve2(Row<2> &R_, int lane) {
+    // odd row o = 2l+1 of this lane; o- = 2l-1 is the previous lane's odd row
+    const double ibo = 1.0 / R_.b[1];
+    double a_om = __shfl_up_sync(0xffffffffu, R_.a[1], 1);
+    double c_om = __shfl_up_sync(0xffffffffu, R_.c[1], 1);
+    double d_om = __shfl_up_sync(0xffffffffu, R_.d[1], 1);
+    double ib_om = __shfl_up_sync(0xffffffffu, ibo, 1);
+    if (lane == 0) { a_om = 0.0; c_om = 0.0; d_om = 0.0; ib_om = 1.0; }
+    // even row e = 2l: eliminate x_{e-1} (row o-) and x_{e+1} (row o)
+    double al = -R_.a[0] * ib_om;
+    double ga = -R_.c[0] * ibo;
+    double ea = al * a_om;
+    double eb = R_.b[0] + al * c_om + ga * R_.a[1];
+    double ec = ga * R_.c[1];
+    double ed = R_.d[0] + al * d_om + ga * R_.d[1];
+    // PCR over the 32 even rows (one per lane)
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1) {
+        double ib = 1.0 / eb;
+        double am = __shfl_up_sync(0xffffffffu, ea, s), cm = __shfl_up_sync(0xffffffffu, ec, s);
+        double dm = __shfl_up_sync(0xffffffffu, ed, s), ibm = __shfl_up_sync(0xffffffffu, ib, s);
+        double ap = __shfl_down_sync(0xffffffffu, ea, s), cp = __shfl_down_sync(0xffffffffu, ec, s);
+        double dp = __shfl_down_sync(0xffffffffu, ed, s), ibp = __shfl_down_sync(0xffffffffu, ib, s);
+        if (lane < s) { am = 0.0; cm = 0.0; dm = 0.0; ibm = 1.0; }
+        if (lane + s > 31) { ap = 0.0; cp = 0.0; dp = 0.0; ibp = 1.0; }
+        double a1 = -ea * ibm, g1 = -ec * ibp;
+        double nb = eb + a1 * cm + g1 * ap;
+        double nd = ed + a1 * dm + g1 * dp;
+        ea = a1 * am;
+        ec = g1 * cp;
+        eb = nb;
+        ed = nd;
+    }
+    const double xe = ed / eb;
+    // odd rows: x_o = (d_o - a_o x_e - c_o x_{e+2}) / b_o
+    double xe2 = __shfl_down_sync(0xffffffffu, xe, 1);
+    if (lane == 31) xe2 = 0.0;
+    R_.d[0] = xe;
+    R_.d[1] = (R_.d[1] - R_.a[1] * xe - R_.c[1] * xe2) * ibo;
+    R_.b[0] = eb;                      // the pivots, for the zero-pivot check (b[1] is b_o)
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -672,7 +718,8 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
             if (a.solver == SOLVER_THOMAS)
                 thomas_solve<M>(sys, lane, tsm + warp * 4 * NP);
             else
-                pcr_solve<M>(sys, lane);
+                if constexpr (M == 2) cr_pcr_solve2(sys, lane);
+                else pcr_solve<M>(sys, lane);
             // flux correction, src/UpdateLyaJandH.jl:341-377
 #pragma unroll
             for (int m = 0; m < M; m++) {
