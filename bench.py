@@ -180,8 +180,11 @@ def measure_form(cloud, prec, args, barrier, stream_of, local, world, clk=None):
     ctx = context_for_cloud(cloud, precision=prec, device=local)
     p = (cloud.c_tilde, cloud.dt, cloud.z_center, cloud.bc_r_right, cloud.bc_z_bot, cloud.bc_z_top)
     run = lambda n: ctx.static_steps(n, *p, history=False)
-    tuning = autotune.autotune(ctx, run, steps=5, device=local,
-                               cache=os.path.join(tempfile.gettempdir(), "lydion_bench_tuning.json"))
+    if args.no_tune:
+        tuning = ctx.tuning()
+    else:
+        tuning = autotune.autotune(ctx, run, steps=5, device=local,
+                                   cache=os.path.join(tempfile.gettempdir(), "lydion_bench_tuning.json"))
     run(args.warmup)
     barrier(ctx)
     if clk is not None:
@@ -318,8 +321,11 @@ def run_gpu(args):
         ctx.synchronize()
 
     stream_of = lambda ctx: torch.cuda.ExternalStream(ctx.stream(), device=local)
-    ctx64, f64 = measure_form(cloud, PREC_FP64, args, barrier, stream_of, local, world)
-    ctx64.close()
+    if args.only_mixed:
+        f64 = None
+    else:
+        ctx64, f64 = measure_form(cloud, PREC_FP64, args, barrier, stream_of, local, world)
+        ctx64.close()
     ctxm, mix = measure_form(cloud, PREC_MIXED, args, barrier, stream_of, local, world, clk=ClockSampler(local))
     e2e = e2e_form(ctxm, cloud, args, barrier, stream_of, world)
     ctxm.close()
@@ -346,9 +352,10 @@ def run_gpu(args):
                            "parallelism": f"{world} independent clouds (one per GPU)" if world > 1 else "single GPU",
                            "l2": "inputs larger than L2: 7 FP64 fields x 33.5 MB resident, 56 B/cell-bin streamed per kernel",
                            "tuning": mix["tuning"]},
-                "fp64": {"value": f64["value"], "ms_per_step": f64["ms_per_step"], "tuning": f64["tuning"],
-                         "kernel_ms_per_step": {n: float(v) for n, v in zip(names, f64["kernel_ms"])}},
-                "mixed_over_fp64": mix["value"] / f64["value"],
+                "fp64": None if f64 is None else {
+                    "value": f64["value"], "ms_per_step": f64["ms_per_step"], "tuning": f64["tuning"],
+                    "kernel_ms_per_step": {n: float(v) for n, v in zip(names, f64["kernel_ms"])}},
+                "mixed_over_fp64": None if f64 is None else mix["value"] / f64["value"],
                 "adjoint_over_forward": adj["ratio_every_100"] if adj else None,
                 "adjoint": adj,
                 "batch": batch,
@@ -377,6 +384,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-batch", action="store_true", help="skip the ragged-batch measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
+    ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of the autotuner")
+    ap.add_argument("--only-mixed", action="store_true", help="measure the mixed-precision form only")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

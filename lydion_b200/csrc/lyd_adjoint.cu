@@ -116,6 +116,51 @@ __device__ __forceinline__ void pcr(RowA<M> &R_, int lane) {
     for (int m = 0; m < M; m++) R_.d[m] = R_.d[m] / R_.b[m];
 }
 
+// Two rows per lane: one cyclic-reduction step over the odd rows, PCR across the warp on the
+// even rows, back-substitution of the odd rows (the same scheme as the forward frequency
+// kernel's two-bins-per-lane solve).
+__device__ __forceinline__ void cr_pcr2(RowA<2> &R_, int lane) {
+    const double ibo = 1.0 / R_.b[1];
+    double a_om = __shfl_up_sync(0xffffffffu, R_.a[1], 1);
+    double c_om = __shfl_up_sync(0xffffffffu, R_.c[1], 1);
+    double d_om = __shfl_up_sync(0xffffffffu, R_.d[1], 1);
+    double ib_om = __shfl_up_sync(0xffffffffu, ibo, 1);
+    if (lane == 0) { a_om = 0.0; c_om = 0.0; d_om = 0.0; ib_om = 1.0; }
+    double al = -R_.a[0] * ib_om, ga = -R_.c[0] * ibo;
+    double ea = al * a_om;
+    double eb = R_.b[0] + al * c_om + ga * R_.a[1];
+    double ec = ga * R_.c[1];
+    double ed = R_.d[0] + al * d_om + ga * R_.d[1];
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1) {
+        double ib = 1.0 / eb;
+        double am = __shfl_up_sync(0xffffffffu, ea, s), cm = __shfl_up_sync(0xffffffffu, ec, s);
+        double dm = __shfl_up_sync(0xffffffffu, ed, s), ibm = __shfl_up_sync(0xffffffffu, ib, s);
+        double ap = __shfl_down_sync(0xffffffffu, ea, s), cp = __shfl_down_sync(0xffffffffu, ec, s);
+        double dp = __shfl_down_sync(0xffffffffu, ed, s), ibp = __shfl_down_sync(0xffffffffu, ib, s);
+        if (lane < s) { am = 0.0; cm = 0.0; dm = 0.0; ibm = 1.0; }
+        if (lane + s > 31) { ap = 0.0; cp = 0.0; dp = 0.0; ibp = 1.0; }
+        double a1 = -ea * ibm, g1 = -ec * ibp;
+        double nb = eb + a1 * cm + g1 * ap;
+        double nd = ed + a1 * dm + g1 * dp;
+        ea = a1 * am;
+        ec = g1 * cp;
+        eb = nb;
+        ed = nd;
+    }
+    const double xe = ed / eb;
+    double xe2 = __shfl_down_sync(0xffffffffu, xe, 1);
+    if (lane == 31) xe2 = 0.0;
+    R_.d[0] = xe;
+    R_.d[1] = (R_.d[1] - R_.a[1] * xe - R_.c[1] * xe2) * ibo;
+}
+
+template <int M>
+__device__ __forceinline__ void solve(RowA<M> &R_, int lane) {
+    if constexpr (M == 2) cr_pcr2(reinterpret_cast<RowA<2> &>(R_), lane);
+    else pcr<M>(R_, lane);
+}
+
 // Frequency factors F+, F, F- of one row k (src/FreqFactors.jl:181-275) and, with g != 0,
 // their adjoint: returns the adjoints of vel, K_{k-1}, K_k, K_{k+1} and rec0.
 struct FfIn {
@@ -294,7 +339,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 2) k_freq_adj(FreqAdjArgs a) {
         double sa[M], sb[M], sc[M];
 #pragma unroll
         for (int m = 0; m < M; m++) { sa[m] = sys.a[m]; sb[m] = sys.b[m]; sc[m] = sys.c[m]; }
-        pcr<M>(sys, lane);
+        solve<M>(sys, lane);
         double x[M];
 #pragma unroll
         for (int m = 0; m < M; m++) x[m] = sys.d[m];
@@ -348,7 +393,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 2) k_freq_adj(FreqAdjArgs a) {
                 tr.c[m] = ap1[m];
                 tr.d[m] = gx[m];
             }
-            pcr<M>(tr, lane);
+            solve<M>(tr, lane);
             double xm[M], xp[M];
             nbr1<M>(x, xm, -1, lane, 0.0);
             nbr1<M>(x, xp, +1, lane, 0.0);
