@@ -219,9 +219,9 @@ int  lyd_batch_steps(lyd_ctx *ctx, const lyd_cloud_params *params, int32_t n_ste
 /* Launch-shape knobs chosen by the autotuner (lydion_b200/autotune.py): rows of the
  * advection tile (4..64), cells per frequency-kernel block (8..1024, or 0 for automatic), the
  * frequency solver (0: parallel cyclic reduction across the warp; 1: lane-serial
- * elimination), and the advection kernel's resident CTAs per SM (2..4, or 0 for the
- * default; FP64 arithmetic always uses 2). lyd_get_tuning reports an automatic cell count
- * as its negative. */
+ * elimination), and the advection kernel's resident CTAs per SM (2..4 with FP32 arithmetic,
+ * 2..3 with FP64, or 0 for the default: 4 and 3). lyd_get_tuning reports an automatic cell
+ * count as its negative. */
 typedef struct lyd_tuning {
     int32_t rows_per_tile, cells_per_block, solver, adv_ctas_per_sm;
 } lyd_tuning;

@@ -2,7 +2,7 @@
 
 Four knobs of a context are tuned (lyd_set_tuning):
   rows_per_tile    rows of the advection tile each CTA marches through (4..64);
-  adv_ctas_per_sm  resident advection CTAs per SM (2..4; FP32-arithmetic variants only);
+  adv_ctas_per_sm  resident advection CTAs per SM (2..4 with FP32 arithmetic, 2..3 with FP64);
   cells_per_block  cells per frequency-kernel block (8..1024, or 0 = automatic);
   solver           frequency tridiagonal solver: 0 = parallel cyclic reduction across the warp,
                    1 = lane-serial elimination.
@@ -85,7 +85,7 @@ def search(ctx, run, steps=10, rows=ROWS, cells=CELLS, solvers=SOLVERS, ctas=CTA
     """Time every candidate; return (best tuning tuple, table of (tuning, ms[3]))."""
     table = []
     if getattr(ctx, "precision", 0) == 0:
-        ctas = (0,)                      # FP64 arithmetic has one occupancy variant
+        ctas = tuple(o for o in ctas if o in (2, 3)) or (0,)   # FP64 arithmetic: 2 or 3 CTAs per SM
     best_rows, best_adv = None, np.inf
     for r in rows:
         for o in ctas:

@@ -113,10 +113,12 @@ __device__ __forceinline__ R alpha_F(const AdvArgs<S> &a, const View &v, int i, 
 // ---- k_advect: one CTA = 8 columns (r) x `rows` rows (Z) x 32 bins, marching up in Z --------
 //
 // A ring of four rows holds, for the 8 own columns and the 2 + 2 halo columns of each row, the
-// cell values every face needs: J, the reduced fluxes H/max(J, Jeps) and alpha_F (so the
-// reciprocal of J is taken once per cell, not once per face), plus the raw H of the own
-// columns for the cell update. Warp w (0..7) owns column i0+w; warp 8 stages the halo columns
-// and computes the tile's rightmost r face. Per row: stage row j+2 -> sync -> every warp
+// cell values every face needs: J and the reduced fluxes H/max(J, Jeps) (so the reciprocal of
+// J is taken once per cell, not once per face), plus the state of the own columns for the
+// cell update. With FP32 arithmetic the ring also holds alpha_F; with FP64 arithmetic alpha_F of
+// the two cells beside a face is formed at the face from alpha and H_voigt (L1-resident loads)
+// instead, which keeps the FP64 tile (65 KB) within three CTAs per SM. Warp w (0..7) owns
+// column i0+w; warp 8 stages the halo columns and computes the tile's rightmost r face. Per row: stage row j+2 -> sync -> every warp
 // computes the r face on its left (warp 8: the right edge) into shared memory and its Z face
 // j+1/2 into registers -> sync -> the cell update of row j uses the two r faces from shared
 // memory and the Z faces j-1/2 (carried from the previous row) and j+1/2.
@@ -125,6 +127,8 @@ constexpr int MWARPS = MT + 1;
 constexpr int MTHREADS = 32 * MWARPS;
 constexpr int MCOL = MT + 4;           // staged columns i0-2 .. i0+MT+1
 constexpr int RING = 4;
+// staged fields per cell: J, f_r, f_Z (+ alpha_F with FP32 arithmetic)
+template <typename R> __host__ __device__ constexpr int nf() { return sizeof(R) == 4 ? 4 : 3; }
 
 template <typename S, typename R>
 __device__ __forceinline__ Cell<R> raw_cell(const AdvArgs<S> &a, const View &v, int col, int row, int k) {
@@ -140,24 +144,33 @@ template <typename S, typename R>
 __device__ __forceinline__ void stage_cell(const AdvArgs<S> &a, const View &v, R *A, S *Hh, int slot, int lc,
                                            int col, int row, int k, int lane, R jeps) {
     Cell<S> c = raw_cell<S, S>(a, v, col, row, k);
+    // the alpha_F loads are issued together with the state's (one load latency per cell)
+    R aF = R(0);
+    if (nf<R>() == 4) {
+        int cc = col < 0 ? 0 : (col >= v.nr ? v.nr - 1 : col);
+        int rr = row < 0 ? 0 : (row >= v.nz ? v.nz - 1 : row);
+        aF = alpha_F<S, R>(a, v, cc, rr, k);
+    }
     CellF<R> f = cell_f<R>(R(c.J), R(c.Hr), R(c.HZ), jeps);
-    int cc = col < 0 ? 0 : (col >= v.nr ? v.nr - 1 : col);
-    int rr = row < 0 ? 0 : (row >= v.nz ? v.nz - 1 : row);
-    R aF = alpha_F<S, R>(a, v, cc, rr, k);
-    R *p = A + ((slot * MCOL + lc) * 4) * 32 + lane;
-    p[0] = f.J; p[32] = f.fr; p[64] = f.fZ; p[96] = aF;
+    R *p = A + ((slot * MCOL + lc) * nf<R>()) * 32 + lane;
+    p[0] = f.J; p[32] = f.fr; p[64] = f.fZ;
+    if (nf<R>() == 4) p[96] = aF;
     if (lc >= 2 && lc < 2 + MT) {
-        S *q = Hh + ((slot * MT + (lc - 2)) * 3) * 32 + lane;
-        q[0] = c.J; q[32] = c.Hr; q[64] = c.HZ;
+        // the state in S; with S == R the ring's J is the state's J
+        constexpr int HF = sizeof(S) == sizeof(R) ? 2 : 3;
+        S *q = Hh + ((slot * MT + (lc - 2)) * HF) * 32 + lane;
+        q[0] = c.Hr; q[32] = c.HZ;
+        if (HF == 3) q[64] = c.J;
     }
 }
 
+// A staged cell; with FP32 arithmetic also its alpha_F from the ring.
 template <typename R>
 __device__ __forceinline__ CellF<R> staged(const R *A, int slot, int lc, int lane, R &aF) {
-    const R *p = A + ((slot * MCOL + lc) * 4) * 32 + lane;
+    const R *p = A + ((slot * MCOL + lc) * nf<R>()) * 32 + lane;
     CellF<R> c;
     c.J = p[0]; c.fr = p[32]; c.fZ = p[64];
-    aF = p[96];
+    if (nf<R>() == 4) aF = p[96];
     return c;
 }
 
@@ -165,12 +178,16 @@ __device__ __forceinline__ CellF<R> staged(const R *A, int slot, int lc, int lan
 // staged column of the stencil's first cell (src/AdvectJandH.jl:641-968).
 template <typename S, typename R, int FLUX>
 __device__ __forceinline__ void face_r_staged(const AdvArgs<S> &a, const View &v, const R *A, int slot, int wl,
-                                              int f, int j, int lane, R jeps, R *F, R &kL, R &kR) {
+                                              int f, int j, int k, int lane, R jeps, R *F, R &kL, R &kR) {
     R d0, aFi, aFp, d3;
     CellF<R> cm1 = staged<R>(A, slot, wl, lane, d0);
     CellF<R> ci = staged<R>(A, slot, wl + 1, lane, aFi);
     CellF<R> cp1 = staged<R>(A, slot, wl + 2, lane, aFp);
     CellF<R> cp2 = staged<R>(A, slot, wl + 3, lane, d3);
+    if (nf<R>() == 3) {   // FP64 arithmetic: alpha_F formed here from alpha and H_voigt
+        aFi = alpha_F<S, R>(a, v, f - 1 < 0 ? 0 : (f - 1 >= v.nr ? v.nr - 1 : f - 1), j, k);
+        aFp = alpha_F<S, R>(a, v, f >= v.nr ? v.nr - 1 : f, j, k);
+    }
     R iv[5];
 #pragma unroll
     for (int t = 0; t < 5; t++) iv[t] = R(__ldg(a.rint + v.orint + 5 * f + t));
@@ -192,12 +209,16 @@ __device__ __forceinline__ void face_r_staged(const AdvArgs<S> &a, const View &v
 // Z face f (between rows f-1 and f) of column i, staged column lc (src/AdvectJandH.jl:978-1289).
 template <typename S, typename R, int FLUX>
 __device__ __forceinline__ void face_z_staged(const AdvArgs<S> &a, const View &v, const R *A, int lc, int i, int f,
-                                              int lane, R jeps, R *F) {
+                                              int k, int lane, R jeps, R *F) {
     R d0, aFi, aFp, d3;
     CellF<R> cm1 = staged<R>(A, (f + 2) & (RING - 1), lc, lane, d0);     // row f-2
     CellF<R> ci = staged<R>(A, (f + 3) & (RING - 1), lc, lane, aFi);     // row f-1
     CellF<R> cp1 = staged<R>(A, f & (RING - 1), lc, lane, aFp);          // row f
     CellF<R> cp2 = staged<R>(A, (f + 1) & (RING - 1), lc, lane, d3);     // row f+1
+    if (nf<R>() == 3) {
+        aFi = alpha_F<S, R>(a, v, i, f - 1 < 0 ? 0 : (f - 1 >= v.nz ? v.nz - 1 : f - 1), k);
+        aFp = alpha_F<S, R>(a, v, i, f >= v.nz ? v.nz - 1 : f, k);
+    }
     R iv[5];
 #pragma unroll
     for (int t = 0; t < 5; t++) iv[t] = R(__ldg(a.zint + v.ozint + 5 * f + t));
@@ -217,9 +238,11 @@ __device__ __forceinline__ void face_z_staged(const AdvArgs<S> &a, const View &v
 template <typename S, typename R, int FLUX, int MINB>
 __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
     extern __shared__ __align__(16) unsigned char adv_smem[];
-    R *A = reinterpret_cast<R *>(adv_smem);                            // [RING][MCOL][4][32]
-    S *Hh = reinterpret_cast<S *>(A + RING * MCOL * 4 * 32);            // [RING][MT][3][32]
-    R *Fr = reinterpret_cast<R *>(Hh + RING * MT * 3 * 32);             // [MT+1][5][32]
+    constexpr int HF = sizeof(S) == sizeof(R) ? 2 : 3;
+    constexpr int NF = nf<R>();
+    R *A = reinterpret_cast<R *>(adv_smem);                            // [RING][MCOL][NF][32]
+    S *Hh = reinterpret_cast<S *>(A + RING * MCOL * NF * 32);           // [RING][MT][HF][32]
+    R *Fr = reinterpret_cast<R *>(Hh + RING * MT * HF * 32);            // [MT+1][5][32]
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int4 t = a.tiles[blockIdx.x];
     View v;
@@ -254,7 +277,7 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
     }
     __syncthreads();
     R zL[3] = {R(0), R(0), R(0)};
-    if (own && kact && col < v.nr) face_z_staged<S, R, FLUX>(a, v, A, w + 2, col, j0, lane, jeps, zL);
+    if (own && kact && col < v.nr) face_z_staged<S, R, FLUX>(a, v, A, w + 2, col, j0, k, lane, jeps, zL);
 
     const double ctdt = v.ctdt;
     const double ctdt_c = ctdt * kInvC;
@@ -281,11 +304,11 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
         R zR[3] = {R(0), R(0), R(0)};
         if (kact && f <= v.nr) {
             R F[3], kL, kR;
-            face_r_staged<S, R, FLUX>(a, v, A, j & (RING - 1), w, f, j, lane, jeps, F, kL, kR);
+            face_r_staged<S, R, FLUX>(a, v, A, j & (RING - 1), w, f, j, k, lane, jeps, F, kL, kR);
             R *p = Fr + (w * 5) * 32 + lane;
             p[0] = F[0]; p[32] = F[1]; p[64] = F[2]; p[96] = kL; p[128] = kR;
         }
-        if (own && kact && col < v.nr) face_z_staged<S, R, FLUX>(a, v, A, w + 2, col, j + 1, lane, jeps, zR);
+        if (own && kact && col < v.nr) face_z_staged<S, R, FLUX>(a, v, A, w + 2, col, j + 1, k, lane, jeps, zR);
         __syncthreads();
         // (C) cell update, src/AdvectJandH.jl:1302-1382
         if (own && col < v.nr && k < a.nnu) {
@@ -296,8 +319,9 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
             if (!kact) {
                 a.Jo[x] = a.J[x]; a.Hro[x] = a.Hr[x]; a.HZo[x] = a.HZ[x];
             } else {
-                const S *pH = Hh + (((j & (RING - 1)) * MT + w) * 3) * 32 + lane;
-                const S uJ = pH[0], uHr = pH[32], uHZ = pH[64];
+                const S *pH = Hh + (((j & (RING - 1)) * MT + w) * HF) * 32 + lane;
+                const S uHr = pH[0], uHZ = pH[32];
+                const S uJ = HF == 3 ? pH[64] : S(A[(((j & (RING - 1)) * MCOL + w + 2) * NF) * 32 + lane]);
                 const R sJ = R(uJ), sHr = R(uHr), sHZ = R(uHZ);
                 R Drr, DZZ, DrZ;
                 D_edd<R>(sHr, sHZ, sJ, jeps, R(a.heps2), Drr, DZZ, DrZ);
@@ -942,7 +966,8 @@ __global__ void __launch_bounds__(1024) k_reduce(RedArgs a) {
 // ---- launch wrappers ----------------------------------------------------------------------
 template <typename S, typename R>
 static size_t adv_smem_bytes() {
-    return sizeof(R) * 32 * (RING * MCOL * 4 + (MT + 1) * 5) + sizeof(S) * 32 * RING * MT * 3;
+    constexpr int HF = sizeof(S) == sizeof(R) ? 2 : 3;
+    return sizeof(R) * 32 * (RING * MCOL * nf<R>() + (MT + 1) * 5) + sizeof(S) * 32 * RING * MT * HF;
 }
 
 template <typename S, typename R, int FLUX, int MINB>
@@ -964,7 +989,7 @@ static void adv_occ(const void *args, int ntiles, cudaStream_t st, int ctas) {
 }
 
 int adv_ctas_per_sm(int prec, int want) {
-    if (prec == PREC_K_FP64) return 2;            // FP64: ~100 registers and 85 KB of shared memory per CTA
+    if (prec == PREC_K_FP64) return (want == 2) ? 2 : 3;   // FP64: 65 KB of shared memory, 72 registers
     return (want >= 2 && want <= 4) ? want : 4;
 }
 
@@ -972,8 +997,13 @@ void launch_advect(int prec, int flux, const void *args, int ntiles, int ctas, c
     if (ntiles <= 0) return;
     ctas = adv_ctas_per_sm(prec, ctas);
     if (prec == PREC_K_FP64) {
-        if (flux == 0) adv_launch<double, double, 0, 2>(args, ntiles, st);
-        else adv_launch<double, double, 1, 2>(args, ntiles, st);
+        if (ctas == 3) {
+            if (flux == 0) adv_launch<double, double, 0, 3>(args, ntiles, st);
+            else adv_launch<double, double, 1, 3>(args, ntiles, st);
+        } else {
+            if (flux == 0) adv_launch<double, double, 0, 2>(args, ntiles, st);
+            else adv_launch<double, double, 1, 2>(args, ntiles, st);
+        }
     } else if (prec == PREC_K_MIXED) {
         if (flux == 0) adv_occ<double, float, 0>(args, ntiles, st, ctas);
         else adv_occ<double, float, 1>(args, ntiles, st, ctas);
