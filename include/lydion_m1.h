@@ -152,6 +152,12 @@ int  lyd_find_active_bins(lyd_ctx *ctx, int32_t *kmin, int32_t *kmax);
  * UpdateJold = true + H_old = H); bc_r_left must be LYD_BC_REFLECT (cylindrical axis). */
 int  lyd_advect(lyd_ctx *ctx, double ctdt, int32_t bc_r_left, int32_t bc_r_right,
                 int32_t bc_z_bot, int32_t bc_z_top);
+/* AdvectJandH!, src/AdvectJandH.jl:2227-2464, with the caller's bin range [kmin, kmax]
+ * (0-based) and J_old rule: update_jold != 0 sets J_old = J after the step, otherwise J_old
+ * keeps its value; H_old is left alone. This is the form the stellar/IR bands use
+ * (PhotoThermoChemistry.jl:3854-3868: all bands, UpdateJold = false, explicit alpha_F). */
+int  lyd_advect_jh(lyd_ctx *ctx, double ctdt, int32_t kmin, int32_t kmax, int32_t update_jold,
+                   int32_t bc_r_left, int32_t bc_r_right, int32_t bc_z_bot, int32_t bc_z_top);
 /* LyaEmissionAbsorptionUpdate!, src/ConstantsAndFunctions.jl:483-573 (reads the uploaded
  * alpha, alpha_c, pd, js, H_voigt, phi_nu, alpha_F; accumulates into Delta rho u). */
 int  lyd_emission_absorption(lyd_ctx *ctx, double c_tilde, double dt);

@@ -97,6 +97,7 @@ SIGNATURES = {
     "lyd_get_stream": (C.c_int, [VP, C.POINTER(VP)]),
     "lyd_find_active_bins": (C.c_int, [VP, C.POINTER(I32), C.POINTER(I32)]),
     "lyd_advect": (C.c_int, [VP, D, I32, I32, I32, I32]),
+    "lyd_advect_jh": (C.c_int, [VP, D, I32, I32, I32, I32, I32, I32, I32]),
     "lyd_emission_absorption": (C.c_int, [VP, D, D]),
     "lyd_frequency_update": (C.c_int, [VP, D, I32]),
     "lyd_update_J_and_H": (C.c_int, [VP, D, D, I32, I32, I32, I32, I32]),

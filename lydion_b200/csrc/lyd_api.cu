@@ -746,6 +746,59 @@ int lyd_advect(lyd_ctx *c, double ctdt, int32_t bl, int32_t br, int32_t bb, int3
     return do_advect(c);
 }
 
+// AdvectJandH! with its own bin range and J_old rule (src/AdvectJandH.jl:2227-2464): the
+// stellar/IR bands and any caller that does not want FindActiveBins. J_old becomes the new J
+// when update_jold is set and is otherwise left as it was; H_old is never touched.
+int lyd_advect_jh(lyd_ctx *c, double ctdt, int32_t kmin, int32_t kmax, int32_t update_jold, int32_t bl, int32_t br,
+                  int32_t bb, int32_t bt) {
+    if (!c) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    LYD_TRY(check_bcs(c, bl, br, bb, bt));
+    LYD_TRY(need_inputs(c, false, false));
+    if (!(ctdt > 0.0)) return fail(c, LYD_ERR_ARG, "c~ dt must be positive");
+    if (kmin < 0 || kmax >= c->nnu || kmin > kmax) return fail(c, LYD_ERR_ARG, "bad bin range");
+    for (CloudDesc &d : c->desc) d.ctdt = ctdt;
+    bcs_all(c, br, bb, bt);
+    LYD_TRY(sync_desc(c));
+    const bool alias = c->old_alias;
+    const size_t bytes = c->n3 * c->ssz;
+    void *saved = nullptr;
+    if (!alias) {
+        // the old set is about to receive the advected state: keep J_old and H_old
+        LYD_TRY(dalloc(c, &saved, 3 * bytes));
+        for (int q = 0; q < 3; q++)
+            LYD_CU(c, cudaMemcpyAsync(at(saved, q * c->n3, c->ssz), c->set[1 - c->cur][q], bytes,
+                                      cudaMemcpyDeviceToDevice, c->st));
+    }
+    std::vector<int> w((size_t)2 * c->ncl);
+    for (int q = 0; q < c->ncl; q++) { w[2 * q] = kmin; w[2 * q + 1] = kmax; }
+    LYD_CU(c, cudaMemcpyAsync(c->kwin, w.data(), w.size() * sizeof(int), cudaMemcpyHostToDevice, c->st));
+    const int in = c->cur, out = 1 - c->cur;
+    if (c->sprec == 0) {
+        AdvArgs<double> a;
+        fill_adv<double>(c, a, in, out);
+        launch_advect(c->prec, c->cfg.flux_method, &a, c->ntiles, c->tune.adv_ctas_per_sm, c->st);
+    } else {
+        AdvArgs<float> a;
+        fill_adv<float>(c, a, in, out);
+        launch_advect(c->prec, c->cfg.flux_method, &a, c->ntiles, c->tune.adv_ctas_per_sm, c->st);
+    }
+    cudaError_t e = cudaGetLastError();
+    c->cur = out;
+    // the set `in` now holds the state before the advection: make it J_old / H_old
+    if (e == cudaSuccess && saved)
+        for (int q = 0; q < 3 && e == cudaSuccess; q++)
+            e = cudaMemcpyAsync(c->set[in][q], at(saved, q * c->n3, c->ssz), bytes, cudaMemcpyDeviceToDevice, c->st);
+    if (e == cudaSuccess && update_jold)
+        e = cudaMemcpyAsync(c->set[in][0], c->set[out][0], bytes, cudaMemcpyDeviceToDevice, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    cudaFree(saved);
+    if (e != cudaSuccess) return fail(c, LYD_ERR_CUDA, cudaGetErrorString(e));
+    c->old_alias = false;
+    c->active_valid = false;
+    return LYD_OK;
+}
+
 template <typename S>
 static int freq_call(lyd_ctx *c, bool emission, bool freq, int update_ff, int parts) {
     LYD_TRY(sync_desc(c));

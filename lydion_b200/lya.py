@@ -5,6 +5,7 @@ the CUDA kernels through the C ABI and writes the results back into the caller's
 place, as the Julia functions mutate theirs.
 
     advect_lya!                      -> advect_lya                        (src/UpdateLyaJandH.jl:107)
+    AdvectJandH!                     -> advect_J_and_H                    (src/AdvectJandH.jl:2227)
     LyαEmissionAbsorptionUpdate!     -> lya_emission_absorption_update     (src/ConstantsAndFunctions.jl:483)
     FrequencyUpdateJLyα_AllCells!    -> frequency_update_J_lya_all_cells   (src/UpdateLyaJandH.jl:231)
     UpdateLyαJandH!                  -> update_lya_J_and_H                 (src/UpdateLyaJandH.jl:409)
@@ -157,6 +158,54 @@ def advect_lya(ctdt, lya, geom, u_r_star, u_Z_star, dur_dr, dur_dZ, duZ_dr, duZ_
     _push_velocity(ctx, u_r_star, u_Z_star, dur_dr, dur_dZ, duZ_dr, duZ_dZ, ur_over_r)
     ctx.advect(ctdt, _bc(BC_r_right), _bc(BC_Z_bot), _bc(BC_Z_top), bc_r_left=_bc(BC_r_left))
     _pull_state(ctx, lya)
+
+
+class _BandCache:
+    """One device context per (bands, grid shape, flux method, geometry) for AdvectJandH!."""
+
+    def __init__(self):
+        self.key = None
+        self.ctx = None
+
+    def get(self, n, nr, nz, flux, geom):
+        key = (n, nr, nz, flux, id(geom))
+        if key != self.key:
+            if self.ctx is not None:
+                self.ctx.close()
+            from .grid import FreqGrid, alpha_floor
+            self.ctx = M1Context(n, nr, nz, 0, 0, alpha_floor(geom), recoil=False, flux_method=flux)
+            self.ctx.set_geometry(geom)
+            # the bands' frequencies are not read by the advection; any increasing grid will do
+            nu = np.arange(n + 1, dtype=np.float64) + 1.0
+            nuC = 0.5 * (nu[1:] + nu[:-1])
+            dnu = np.diff(nu)
+            self.ctx.set_freq_grid(FreqGrid(nu, nuC, dnu, 1.0 / dnu, 1.0 / nuC, 0, 0))
+            self.key = key
+        return self.ctx
+
+
+_band_cache = _BandCache()
+
+
+def advect_J_and_H(ctdt, alpha_F, J, J_old, H_r, H_Z, geom, u_r_star, u_Z_star, dur_dr, dur_dZ, duZ_dr, duZ_dZ,
+                   ur_over_r, UpdateJold=True, BC_r_left="Reflect", BC_r_right="Outflow", BC_Z_bot="Reflect",
+                   BC_Z_top="Outflow", kmin=0, kmax=None, FluxSolver="HLL"):
+    """AdvectJandH! (src/AdvectJandH.jl:2227-2464) for any set of bands: advects bins
+    kmin..kmax (0-based, default all) of J, H_r, H_Z with the flux opacities alpha_F; J_old
+    becomes J when UpdateJold, and is left alone otherwise (the stellar/IR call of
+    PhotoThermoChemistry.jl:3854-3868 passes UpdateJold = false). Mutates J, H_r, H_Z (and
+    J_old)."""
+    nz, nr, n = J.shape
+    flux = FLUX_HLL if str(FluxSolver).strip(":").upper() == "HLL" else FLUX_GLF
+    ctx = _band_cache.get(n, nr, nz, flux, geom)
+    for name, a in (("J", J), ("H_r", H_r), ("H_Z", H_Z), ("J_old", J_old), ("alpha_F", alpha_F)):
+        ctx.upload(name, a)
+    _push_velocity(ctx, u_r_star, u_Z_star, dur_dr, dur_dZ, duZ_dr, duZ_dZ, ur_over_r)
+    kmax = n - 1 if kmax is None else kmax
+    ctx.advect_jh(ctdt, kmin, kmax, UpdateJold, _bc(BC_r_right), _bc(BC_Z_bot), _bc(BC_Z_top),
+                  bc_r_left=_bc(BC_r_left))
+    for name, a in (("J", J), ("H_r", H_r), ("H_Z", H_Z), ("J_old", J_old)):
+        a[...] = ctx.download(name)
 
 
 def lya_emission_absorption_update(J, J_old, H_r, H_Z, H_r_old, H_Z_old, js, phi_nu, Hvoigt, alpha, alpha_c,

@@ -107,6 +107,12 @@ class M1Context:
     def advect(self, ctdt, bc_r_right=BC_OUTFLOW, bc_z_bot=BC_REFLECT, bc_z_top=BC_OUTFLOW, bc_r_left=BC_REFLECT):
         self._ck(lib().lyd_advect(self._h, float(ctdt), bc_r_left, bc_r_right, bc_z_bot, bc_z_top))
 
+    def advect_jh(self, ctdt, kmin, kmax, update_jold, bc_r_right=BC_OUTFLOW, bc_z_bot=BC_REFLECT,
+                  bc_z_top=BC_OUTFLOW, bc_r_left=BC_REFLECT):
+        """AdvectJandH! over bins kmin..kmax (0-based) with the J_old rule of update_jold."""
+        self._ck(lib().lyd_advect_jh(self._h, float(ctdt), int(kmin), int(kmax), int(bool(update_jold)), bc_r_left,
+                                     bc_r_right, bc_z_bot, bc_z_top))
+
     def emission_absorption(self, c_tilde, dt):
         self._ck(lib().lyd_emission_absorption(self._h, float(c_tilde), float(dt)))
 

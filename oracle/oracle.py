@@ -230,6 +230,11 @@ class OracleState:
                              c.bc_z_top, C.byref(a), C.byref(b))
         return a.value, b.value
 
+    def advect_jh(self, ctdt, kmin, kmax, update_jold):
+        c = self.cloud
+        lib().orc_advect_jh(C.byref(self.s), C.byref(self.g), C.byref(self.v), ctdt, int(update_jold), c.bc_r_right,
+                            c.bc_z_bot, c.bc_z_top, int(kmin), int(kmax))
+
     def emission_absorption(self, c_tilde, dt):
         lib().orc_emission_absorption(C.byref(self.s), c_tilde, dt)
 

@@ -169,6 +169,46 @@ def test_diagnostics_match_oracle(oracle_mod):
     np.testing.assert_allclose(ng, no, rtol=1e-13)
 
 
+def _band_cloud(n_bands=7):
+    """A cloud whose 'frequency grid' is n_bands stellar/IR bands (the advection does not read
+    the frequencies)."""
+    from lydion_b200.grid import FreqGrid
+    nu = np.arange(n_bands + 1, dtype=np.float64) + 1.0
+    nuC = 0.5 * (nu[1:] + nu[:-1])
+    dnu = np.diff(nu)
+    fq = FreqGrid(nu, nuC, dnu, 1.0 / dnu, 1.0 / nuC, 0, 0)
+    return W.static_cloud(11, 9, n_bands, tau0=1e4, tau_abs=0.5, rs=0.5, umax_kms=100.0, freq=fq,
+                          flux_method=W.FLUX_HLL, name="bands")
+
+
+@pytest.mark.parametrize("kmin,kmax,update_jold", [(0, 6, 0), (2, 4, 1), (0, 6, 1)])
+def test_advect_jh_bands_match_oracle(oracle_mod, kmin, kmax, update_jold):
+    """AdvectJandH! for 7 stellar/IR bands with HLL, explicit alpha_F, the caller's bin range and
+    J_old rule (src/AdvectJandH.jl:2227-2464; PhotoThermoChemistry.jl:3854-3868)."""
+    from lydion_b200 import lya
+    cl = _band_cloud(7)
+    st = oracle_mod.OracleState(cl)
+    rng = np.random.default_rng(31)
+    J, Hr, HZ = random_state(cl, 8)
+    Jold = J * rng.uniform(0.5, 1.5, J.shape)
+    aF = rng.uniform(1e-19, 1e-17, J.shape)
+    for name, a in (("J", J), ("H_r", Hr), ("H_Z", HZ), ("J_old", Jold), ("alpha_F", aF)):
+        getattr(st, name)[...] = a
+    ctdt = cl.c_tilde * cl.dt
+    st.advect_jh(ctdt, kmin, kmax, update_jold)
+    Jg, Hrg, HZg, Jog = J.copy(), Hr.copy(), HZ.copy(), Jold.copy()
+    lya.advect_J_and_H(ctdt, aF, Jg, Jog, Hrg, HZg, cl.geom, cl.u_r_star, cl.u_Z_star, cl.dur_dr, cl.dur_dZ,
+                       cl.duZ_dr, cl.duZ_dZ, cl.ur_over_r, UpdateJold=bool(update_jold), BC_r_right="Outflow",
+                       BC_Z_bot="Reflect", BC_Z_top="Outflow", kmin=kmin, kmax=kmax, FluxSolver="HLL")
+    for got, ref in ((Jg, st.J), (Hrg, st.H_r), (HZg, st.H_Z)):
+        assert norm_err(got, ref) < 1e-12
+    np.testing.assert_array_equal(Jg[:, :, :kmin], J[:, :, :kmin])     # bins outside the range pass through
+    if update_jold:
+        np.testing.assert_array_equal(Jog, Jg)
+    else:
+        np.testing.assert_array_equal(Jog, Jold)
+
+
 def test_gravity_force_multiplier_matches_oracle(oracle_mod):
     """The gravity method of Update_f_Lya_MF_L_Lya! (src/ConstantsAndFunctions.jl:691-804)."""
     cl = CLOUDS["glf_outflow"]()
