@@ -97,6 +97,8 @@ struct lyd_ctx {
     cudaEvent_t ev[8] = {};
     double ms[3] = {0, 0, 0};
     double adj_ms[5] = {0, 0, 0, 0, 0};
+    void *adj_ws = nullptr;            // adjoint workspace, kept between calls (grow only)
+    size_t adj_ws_bytes = 0;
     std::string msg;
 };
 
@@ -342,7 +344,7 @@ int lyd_destroy(lyd_ctx *c) {
     void *ps[] = {c->Hv, c->phi, c->phi_inv, c->aF, c->Ff[0], c->Ff[1], c->Ff[2], c->u_r_star, c->u_Z_star, c->dV,
                   c->inv_dV, c->A_r, c->A_Z, c->inv_r_cell, c->rCoM, c->ZCoM, c->rint, c->zint, c->r_if, c->Z_if,
                   c->nu, c->nuC, c->dnu, c->inv_dnu, c->inv_nuC, c->partials, c->kwin, c->hist, c->step_ctr,
-                  c->last, c->err, c->lut, c->stage, c->small, c->cl, c->tiles, c->items};
+                  c->last, c->err, c->lut, c->stage, c->small, c->cl, c->tiles, c->items, c->adj_ws};
     for (void *p : ps) cudaFree(p);
     for (int q = 0; q < CF_N; q++) cudaFree(c->cellf[q]);
     for (int q = 0; q < 8; q++)
@@ -1199,14 +1201,6 @@ int lyd_voigt_tables(double *out, int32_t n, double xmax) {
 // `checkpoint_every` steps (and each step's active window); the reverse sweep walks the
 // segments backwards, recomputes a segment's states from its checkpoint, then runs the
 // adjoint steps of that segment from its last step to its first.
-namespace {
-struct DevBuf {
-    std::vector<void *> ptrs;
-    ~DevBuf() {
-        for (void *p : ptrs) cudaFree(p);
-    }
-};
-}  // namespace
 
 int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out) {
     if (!c || !cfg || !out) return LYD_ERR_ARG;
@@ -1237,25 +1231,41 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
         c->hist_cap = N;
         drop_graph(c);
     }
-    DevBuf mem;
-    auto A = [&](size_t bytes) -> double * {
-        void *q = nullptr;
-        if (dalloc(c, &q, bytes) != LYD_OK) return nullptr;
-        mem.ptrs.push_back(q);
-        return static_cast<double *>(q);
-    };
-    // checkpoints; and per step of one segment: the state, the advected state x_A and the
-    // advection's tape (recorded while the segment is recomputed)
-    double *ck = A((size_t)nseg * S * 8), *seg = A((size_t)K * S * 8), *segA = A((size_t)K * S * 8);
-    double *segT = A((size_t)K * 4 * n3 * 8);
-    double *lam = A(S * 8), *lamA = A(S * 8), *lamN = A(S * 8), *pre = A(S * 8), *gaF = A(n3 * 8), *gHv = A(n3 * 8);
-    double *g_alpha = A(nc * 8), *g_alpha_c = A(nc * 8), *g_T = A(nc * 8), *g_u = A(5 * nc * 8);
-    double *g_ur = A(c->nrf * 8), *g_uZ = A(c->nzf * 8), *fin = A(S * 8), *wsp = A(nnu * 8), *edge = A(2 * (size_t)nnu * (nr + nz + 2 * nr) * 8);
-    int *win = reinterpret_cast<int *>(A((size_t)N * 2 * sizeof(int) + 16));
-    int *finwin = reinterpret_cast<int *>(A(16));
-    if (!ck || !seg || !segA || !segT || !lam || !lamA || !lamN || !pre || !gaF || !gHv || !g_alpha || !g_alpha_c ||
-        !g_T || !g_u || !g_ur || !g_uZ || !fin || !wsp || !edge || !win || !finwin)
-        return fail(c, LYD_ERR_NOMEM, "adjoint workspace: " + c->msg);
+    // One workspace, kept in the context between calls. It holds: the checkpoints; per step of
+    // one segment the state, the advected state x_A and the advection's tape (recorded while
+    // the segment is recomputed); the adjoints; and the gradient accumulators (zeroed here).
+    const size_t sizes[] = {(size_t)nseg * S * 8, (size_t)K * S * 8, (size_t)K * S * 8, (size_t)K * 4 * n3 * 8,
+                            S * 8, S * 8, S * 8, S * 8, n3 * 8, n3 * 8, nc * 8, nc * 8, nc * 8, 5 * nc * 8,
+                            c->nrf * 8, c->nzf * 8, S * 8, (size_t)nnu * 8, 2 * (size_t)nnu * (nr + nz + 2 * nr) * 8,
+                            (size_t)N * 2 * sizeof(int) + 16, 16};
+    constexpr int NB = sizeof(sizes) / sizeof(sizes[0]);
+    size_t offs[NB], total = 0;
+    for (int q = 0; q < NB; q++) {
+        offs[q] = total;
+        total += (sizes[q] + 255) / 256 * 256;
+    }
+    if (total > c->adj_ws_bytes) {
+        LYD_CU(c, cudaStreamSynchronize(c->st));
+        cudaFree(c->adj_ws);
+        c->adj_ws = nullptr;
+        c->adj_ws_bytes = 0;
+        if (cudaMalloc(&c->adj_ws, total) != cudaSuccess) {
+            cudaGetLastError();
+            c->adj_ws = nullptr;
+            return fail(c, LYD_ERR_NOMEM, "adjoint workspace: out of device memory (lower checkpoint_every)");
+        }
+        c->adj_ws_bytes = total;
+    }
+    auto W_ = [&](int q) { return reinterpret_cast<double *>(static_cast<char *>(c->adj_ws) + offs[q]); };
+    double *ck = W_(0), *seg = W_(1), *segA = W_(2), *segT = W_(3);
+    double *lam = W_(4), *lamA = W_(5), *lamN = W_(6), *pre = W_(7), *gaF = W_(8), *gHv = W_(9);
+    double *g_alpha = W_(10), *g_alpha_c = W_(11), *g_T = W_(12), *g_u = W_(13);
+    double *g_ur = W_(14), *g_uZ = W_(15), *fin = W_(16), *wsp = W_(17), *edge = W_(18);
+    int *win = reinterpret_cast<int *>(W_(19));
+    int *finwin = reinterpret_cast<int *>(W_(20));
+    // lambda and the accumulators start at zero (buffers 4 and 8..15 are contiguous in order)
+    LYD_CU(c, cudaMemsetAsync(lam, 0, S * 8, c->st));
+    LYD_CU(c, cudaMemsetAsync(gaF, 0, offs[16] - offs[8], c->st));
     auto copy_state = [&](double *dst, int set) -> int {
         for (int q = 0; q < 3; q++)
             LYD_CU(c, cudaMemcpyAsync(dst + q * n3, c->set[set][q], n3 * 8, cudaMemcpyDeviceToDevice, c->st));
