@@ -4,7 +4,8 @@ outflow v_max = 200 km/s), one static-cloud driver iteration per step.
 
 The headline value is the mixed-precision form (FP64 state, FP32 advection arithmetic); the
 same line carries the plain-FP64 form, their ratio, the ragged batch of 512 clouds (48 bins,
-sides 32..256) in both forms, and the adjoint/forward cost on the 128x128x48 turbulent cloud.
+sides 32..256) in both forms, the adjoint/forward cost on the 128x128x48 turbulent cloud, and
+the 1024x1024x128 field in both forms.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -267,6 +268,39 @@ def batch_form(args, barrier, stream_of, local, world):
     return out
 
 
+def c5_form(args, stream_of, local):
+    """The largest single field (1024 x 1024 cells x 128 bins of a synthetic RHD snapshot: lognormal
+    n_H, photoionised bubble, shell outflow, dust): both forms, a few graph-replayed steps each,
+    with the per-kernel times and each kernel's algorithmic HBM rate (the working set, 7 x 1.07 GB,
+    is far above L2)."""
+    from lydion_b200 import workloads as W
+    from lydion_b200._lib import PREC_FP64, PREC_MIXED
+    from lydion_b200.m1 import context_for_cloud
+    cl = W.config_c5()
+    p = (cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+    steps = max(3, min(10, args.steps // 300))
+    out = {"workload": "c5_rhd_snapshot_1024x1024x128", "cell_bins": int(cl.cell_bins), "steps": steps}
+    ab = algorithmic_bytes(cl.n_nu, 8)
+    for name, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
+        ctx = context_for_cloud(cl, precision=prec, device=local)
+        run = lambda k: ctx.static_steps(k, *p, history=False)
+        run(2)
+        ctx.synchronize()
+        ms = _timed(ctx, run, steps, stream_of)
+        ctx.set_timing(True)
+        run(steps)
+        ctx.synchronize()
+        kms = ctx.timing() / steps
+        ctx.set_timing(False)
+        out[name] = {"value": steps * cl.cell_bins / (ms * 1e-3), "ms_per_step": ms / steps,
+                     "kernel_ms_per_step": {"advect": float(kms[0]), "freq": float(kms[1]), "reduce": float(kms[2])},
+                     "hbm_gbs": {"advect": ab["advect"] * cl.cell_bins / (kms[0] * 1e-3) / 1e9,
+                                 "freq": ab["freq"] * cl.cell_bins / (kms[1] * 1e-3) / 1e9}}
+        ctx.close()
+    out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
+
+
 def adjoint_form(args, stream_of, local):
     """Adjoint over forward cost on the turbulent cloud (128 x 128 x 48, lognormal n_H, dust,
     v_max = 50 km/s): N forward steps from the graph-replayed step against lyd_adjoint_run of
@@ -331,6 +365,7 @@ def run_gpu(args):
     ctxm.close()
     batch = None if args.no_batch else batch_form(args, barrier, stream_of, local, world)
     adj = None if (args.no_adjoint or world > 1) else adjoint_form(args, stream_of, local)
+    c5 = None if (args.no_c5 or world > 1) else c5_form(args, stream_of, local)
 
     # roofline of the dominant kernel of the headline (mixed) form
     names = ["advect", "freq", "reduce"]
@@ -358,6 +393,7 @@ def run_gpu(args):
                 "mixed_over_fp64": None if f64 is None else mix["value"] / f64["value"],
                 "adjoint_over_forward": adj["ratio_every_100"] if adj else None,
                 "adjoint": adj,
+                "largest_field": c5,
                 "batch": batch,
                 "roofline": {"bound": "hbm", "kernel": "k_" + names[dom], "achieved": achieved,
                              "peak": peaks["hbm_gbs"], "peak_source": src, "unit": "GB/s",
@@ -385,6 +421,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the ragged-batch measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of the autotuner")
+    ap.add_argument("--no-c5", action="store_true", help="skip the 1024x1024x128 field")
     ap.add_argument("--only-mixed", action="store_true", help="measure the mixed-precision form only")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -537,6 +537,65 @@ __device__ __forceinline__ void cr_pcr_solve2(Row<2> &R_, int lane) {
     R_.b[0] = eb;                      // the pivots, for the zero-pivot check (b[1] is b_o)
 }
 
+// PCR over one row per lane (lane l holds row l of a 32-row system coupled to lanes l +- s);
+// returns the reduced diagonal and right-hand side, x = ed / eb.
+__device__ __forceinline__ void pcr_lanes(double &ea, double &eb, double &ec, double &ed, int lane) {
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1) {
+        double ib = 1.0 / eb;
+        double am = __shfl_up_sync(0xffffffffu, ea, s), cm = __shfl_up_sync(0xffffffffu, ec, s);
+        double dm = __shfl_up_sync(0xffffffffu, ed, s), ibm = __shfl_up_sync(0xffffffffu, ib, s);
+        double ap = __shfl_down_sync(0xffffffffu, ea, s), cp = __shfl_down_sync(0xffffffffu, ec, s);
+        double dp = __shfl_down_sync(0xffffffffu, ed, s), ibp = __shfl_down_sync(0xffffffffu, ib, s);
+        if (lane < s) { am = 0.0; cm = 0.0; dm = 0.0; ibm = 1.0; }
+        if (lane + s > 31) { ap = 0.0; cp = 0.0; dp = 0.0; ibp = 1.0; }
+        double a1 = -ea * ibm, g1 = -ec * ibp;
+        double nb = eb + a1 * cm + g1 * ap;
+        double nd = ed + a1 * dm + g1 * dp;
+        ea = a1 * am;
+        ec = g1 * cp;
+        eb = nb;
+        ed = nd;
+    }
+}
+
+// Four rows per lane (rows 4l .. 4l+3): two cyclic-reduction steps (the odd rows, then rows
+// 4l+2) leave row 4l, solved by PCR across the warp; rows 4l+2, then the odd rows follow by
+// back-substitution. Returns x in d; b holds the pivots for the zero-pivot check.
+__device__ __forceinline__ void cr_pcr_solve4(Row<4> &R_, int lane) {
+    const double ib1 = 1.0 / R_.b[1], ib3 = 1.0 / R_.b[3];
+    double a3p = __shfl_up_sync(0xffffffffu, R_.a[3], 1), c3p = __shfl_up_sync(0xffffffffu, R_.c[3], 1);
+    double d3p = __shfl_up_sync(0xffffffffu, R_.d[3], 1), ib3p = __shfl_up_sync(0xffffffffu, ib3, 1);
+    if (lane == 0) { a3p = 0.0; c3p = 0.0; d3p = 0.0; ib3p = 1.0; }
+    // level 1: rows 4l (eliminate 4l-1, 4l+1) and 4l+2 (eliminate 4l+1, 4l+3)
+    double al = -R_.a[0] * ib3p, ga = -R_.c[0] * ib1;
+    double a0 = al * a3p, b0 = R_.b[0] + al * c3p + ga * R_.a[1], c0 = ga * R_.c[1];
+    double d0 = R_.d[0] + al * d3p + ga * R_.d[1];
+    al = -R_.a[2] * ib1;
+    ga = -R_.c[2] * ib3;
+    double a2 = al * R_.a[1], b2 = R_.b[2] + al * R_.c[1] + ga * R_.a[3], c2 = ga * R_.c[3];
+    double d2 = R_.d[2] + al * R_.d[1] + ga * R_.d[3];
+    // level 2: row 4l eliminates 4l-2 (previous lane's row 2) and 4l+2
+    const double ib2 = 1.0 / b2;
+    double a2p = __shfl_up_sync(0xffffffffu, a2, 1), c2p = __shfl_up_sync(0xffffffffu, c2, 1);
+    double d2p = __shfl_up_sync(0xffffffffu, d2, 1), ib2p = __shfl_up_sync(0xffffffffu, ib2, 1);
+    if (lane == 0) { a2p = 0.0; c2p = 0.0; d2p = 0.0; ib2p = 1.0; }
+    al = -a0 * ib2p;
+    ga = -c0 * ib2;
+    double ea = al * a2p, eb = b0 + al * c2p + ga * a2, ec = ga * c2, ed = d0 + al * d2p + ga * d2;
+    pcr_lanes(ea, eb, ec, ed, lane);
+    const double x0 = ed / eb;
+    double x4 = __shfl_down_sync(0xffffffffu, x0, 1);
+    if (lane == 31) x4 = 0.0;
+    const double x2 = (d2 - a2 * x0 - c2 * x4) * ib2;
+    R_.d[1] = (R_.d[1] - R_.a[1] * x0 - R_.c[1] * x2) * ib1;
+    R_.d[3] = (R_.d[3] - R_.a[3] * x2 - R_.c[3] * x4) * ib3;
+    R_.d[0] = x0;
+    R_.d[2] = x2;
+    R_.b[0] = eb;
+    R_.b[2] = b2;
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -552,8 +611,10 @@ __host__ __device__ constexpr int freq_smem_doubles(int nwarps) {
     return KC_N * 32 * M + nwarps * (32 * M + 8) + nwarps * 4 * 32 * M;
 }
 
+// Four bins per lane: 2 CTAs per SM (128 registers, ~230 B of spills) measured 1.4x faster than
+// 1 CTA at 172 registers.
 template <typename S, typename R, int M>
-__global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
+__global__ void __launch_bounds__(FREQ_THREADS, M == 4 ? 2 : 1) k_freq(FreqArgs<S> a) {
     extern __shared__ __align__(16) double fsm[];
     constexpr int NP = 32 * M;
     const int nw = blockDim.x >> 5;
@@ -743,6 +804,7 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_freq(FreqArgs<S> a) {
                 thomas_solve<M>(sys, lane, tsm + warp * 4 * NP);
             else
                 if constexpr (M == 2) cr_pcr_solve2(sys, lane);
+                else if constexpr (M == 4) cr_pcr_solve4(sys, lane);
                 else pcr_solve<M>(sys, lane);
             // flux correction, src/UpdateLyaJandH.jl:341-377
 #pragma unroll

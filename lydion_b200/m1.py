@@ -377,6 +377,11 @@ def context_for_cloud(cloud, precision=PREC_FP64, device=0, keep_freq_factors=Fa
     for name in ("alpha", "alpha_c", "pd", "js", "T", "dur_dr", "dur_dZ", "duZ_dr", "duZ_dZ", "ur_over_r",
                  "u_r_star", "u_Z_star"):
         ctx.upload(name, getattr(cloud, name))
+    if getattr(cloud, "species", None):
+        # destruction probability from the cell's species densities, on the device (pd_Lya)
+        sp = cloud.species
+        cloud.pd = ctx.pd_lya(sp["nHII"], sp["ne"], sp["nHI"], sp["nHeI"], sp["nH2"], cloud.T)
+        ctx.upload("pd", cloud.pd)
     if np.any(cloud.alpha_cF):
         ctx.upload("alpha_cF", cloud.alpha_cF)
     if hvoigt is None:

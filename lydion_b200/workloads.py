@@ -58,6 +58,7 @@ class StaticCloud:
     L_source: float
     n_H: np.ndarray = None       # hydrogen density behind alpha (x_HI = 1), when the cloud is built from one
     kappa_d: float = 0.0         # gray dust opacity per gram of dust behind alpha_c = kappa_d * 0.01 n_H m_H
+    species: dict = None         # n_HII, n_e, n_HI, n_HeI, n_H2 per cell: pd is then computed on the device
 
     @property
     def n_nu(self):
@@ -234,6 +235,74 @@ def config_c4(scale=1):
     mean 100 cm^-3), T = 1e4 K, gray dust at 0.01 n_H, radial outflow v_max = 50 km/s."""
     n = 128 // scale
     return turbulent_cloud(nr=n, nz=n, n_nu=48 if scale == 1 else max(8, 48 // scale), name="c4_turbulent_128x128x48")
+
+
+def radial_flow(r, Z, Zc, v_of_R, dv_of_R):
+    """u = v(R) R_hat about (0, Zc) and its gradient in (r, Z): u_i = v x_i / R gives
+    du_i/dx_j = (v/R) delta_ij + (v' - v/R) x_i x_j / R^2, and u_r / r = v / R."""
+    dz = Z - Zc
+    R = np.hypot(r, dz)
+    Rs = np.where(R > 0, R, 1.0)
+    v = v_of_R(R)
+    dv = dv_of_R(R)
+    q = np.where(R > 0, v / Rs, dv)                 # v/R -> v'(0) at the centre
+    s = np.where(R > 0, (dv - q) / (Rs * Rs), 0.0)
+    return dict(u_r=q * r, u_Z=q * dz, dur_dr=q + s * r * r, dur_dZ=s * r * dz, duZ_dr=s * r * dz,
+                duZ_dZ=q + s * dz * dz, ur_over_r=q)
+
+
+def rhd_snapshot_cloud(n=1024, n_nu=128, sigma_ln=1.5, n_mean=100.0, bubble=0.2, x_HI_bubble=1e-4, T_in=1e4,
+                       T_out=100.0, v_shell_kms=30.0, shell_width=0.05, dust_to_gas=0.01, tau_abs_mean=1.0,
+                       seed=20261208, x_max=600.0, name="rhd_snapshot"):
+    """One synthetic RHD snapshot on an n x n (r, Z) grid, frequency bins to |x| = x_max at 1e4 K:
+    a lognormal turbulent n_H (sigma_ln) with P(k) ~ k^-11/3; a photoionised bubble of radius
+    `bubble` R_cl (x_HI = 1e-4, T = 1e4 K, n_HII = n_e = (1 - x_HI) n_H, p_d from pd_Lya) with a
+    uniform Lyman-alpha source inside it; neutral gas at T_out outside; a radial shell velocity
+    v(R) = v_shell exp(-(R - R_b)^2 / (2 w^2)) about the bubble edge (w = shell_width R_cl);
+    gray dust at dust_to_gas n_H (kappa_d as in turbulent_cloud). The reference has no such
+    snapshot generator; this one is the project's own."""
+    base = static_cloud(n, n, n_nu, tau0=1.0, T0=1e4, rs=bubble, umax_kms=0.0, x_max=x_max, name=name)
+    g = base.geom
+    rC, ZC = np.meshgrid(g.rCoM, g.ZCoM)
+    Zc, Rcl = base.z_center, K.pc
+    R = np.hypot(rC, ZC - Zc)
+    inside = R < Rcl
+    nH = n_mean * np.exp(sigma_ln * gaussian_random_field(n, n, seed=seed) - 0.5 * sigma_ln ** 2)
+    nH = np.where(inside, nH, 0.0)
+    ion = R < bubble * Rcl
+    x_HI = np.where(ion, x_HI_bubble, 1.0)
+    T = np.where(ion, T_in, T_out)
+    nHI = x_HI * nH
+    nHII = (1.0 - x_HI) * nH
+    sigma0 = K.sigma0_prefact / (K.b_prefact * np.sqrt(T))
+    kappa = tau_abs_mean / (dust_to_gas * n_mean * K.mH * K.pc)
+    base.T = T
+    base.alpha = nHI * sigma0
+    base.alpha_c = kappa * dust_to_gas * nH * K.mH
+    base.n_H = nH
+    base.kappa_d = kappa
+    base.species = dict(nHII=nHII, ne=nHII.copy(), nHI=nHI, nHeI=np.zeros_like(nH), nH2=np.zeros_like(nH))
+    Rb, w, vs = bubble * Rcl, shell_width * Rcl, v_shell_kms * K.kms
+    v_of = lambda x: vs * np.exp(-0.5 * ((x - Rb) / w) ** 2)
+    dv_of = lambda x: -vs * (x - Rb) / (w * w) * np.exp(-0.5 * ((x - Rb) / w) ** 2)
+    fl = radial_flow(rC, ZC, Zc, v_of, dv_of)
+    for k in ("dur_dr", "dur_dZ", "duZ_dr", "duZ_dZ", "ur_over_r"):
+        setattr(base, k, fl[k])
+    base.u_r, base.u_Z = fl["u_r"], fl["u_Z"]
+    rf, Zrow = np.meshgrid(g.r, g.ZCoM)
+    base.u_r_star = np.ascontiguousarray(radial_flow(rf, Zrow, Zc, v_of, dv_of)["u_r"])
+    rcol, Zf = np.meshgrid(g.rCoM, g.Z)
+    base.u_Z_star = np.ascontiguousarray(radial_flow(rcol, Zf, Zc, v_of, dv_of)["u_Z"])
+    base.dt = cfl_dt(g, base.c_tilde, base.u_r, base.u_Z, 0.4)
+    base.tau0 = float(n_mean * K.compute_sigma0(T_out) * K.pc)
+    return base
+
+
+def config_c5(scale=1):
+    """The largest field: 1024 x 1024 cells x 128 bins of one synthetic RHD snapshot."""
+    n = 1024 // scale
+    return rhd_snapshot_cloud(n=n, n_nu=128 if scale == 1 else max(16, 128 // scale),
+                              name="c5_rhd_snapshot_1024x1024x128")
 
 
 def small_cloud(nr=12, nz=10, n_nu=16, **kw):
