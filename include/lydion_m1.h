@@ -242,7 +242,7 @@ int  lyd_get_tuning(lyd_ctx *ctx, lyd_tuning *t);
  * kernels of the step (advection, emission/absorption, frequency factors, transposed
  * tridiagonal solve, flux correction). The active window of every step is the forward's.
  * Non-smooth points (MinMod, floors, clamps, limiters) take the derivative of the branch the
- * forward took. Needs a single-cloud FP64 context, the GLF flux and alpha_F derived from
+ * forward took. Needs a single-cloud FP64 context (GLF or HLL flux) and alpha_F derived from
  * alpha and H_voigt. The context ends in the final state of the forward sweep.
  * grad_T includes the H_voigt(T) chain when H_voigt was computed by lyd_update_hvoigt (not
  * uploaded), and the T of the frequency factors (Doppler width, recoil); gradients with

@@ -1,4 +1,4 @@
-// lyd_adjoint.cu -- reverse-mode kernels of the Lyman-alpha step (FP64, GLF flux, one cloud).
+// lyd_adjoint.cu -- reverse-mode kernels of the Lyman-alpha step (FP64, GLF or HLL flux, one cloud).
 //
 // One static-driver step maps the state s_n = (J, H_r, H_Z) to s_{n+1} through
 //   A  AdvectLya!               s_n -> x_A        (active window of the step)
@@ -13,7 +13,7 @@
 //   k_adv_adj_cell  one warp per (cell, 32 bins): the cell update's local terms and the
 //                   adjoints of its face-flux sums
 //   k_adv_adj_face  one warp per (face, 32 bins): the adjoint of one face's reconstruction,
-//                   closure and GLF + upwind flux, scattered onto its four stencil cells
+//                   closure and GLF/HLL + upwind flux, scattered onto its four stencil cells
 // Scatters use FP64 atomics, so gradients agree run to run to rounding (~1e-15), not bitwise.
 #include <cuda_runtime.h>
 
@@ -637,7 +637,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adv_adj_cell(AdjAdvArgs a) {
 // One face's adjoint: warp = one face x 32 bins. ZDIR false: r faces f = 0..nr of row j;
 // true: Z faces f = 0..nz of column i.
 // 2 CTAs per SM: 1.4x faster than the unconstrained 206-register form.
-template <bool ZDIR>
+template <bool ZDIR, int FLUX>
 __global__ void __launch_bounds__(ADJ_THREADS, 2) k_adv_adj_face(AdjAdvArgs a) {
     const int lane = threadIdx.x & 31;
     const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -692,7 +692,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 2) k_adv_adj_face(AdjAdvArgs a) {
         double aFp = ZDIR ? alpha_F_at(a, line, pp, k) : alpha_F_at(a, pp, line, k);
         double uc = (ZDIR ? a.u_Z_star[fi] : a.u_r_star[fi]) * kInvC;
         double gaFi = 0.0, gaFp = 0.0;
-        adj_face_glf<ZDIR>(cs, iv, aFi, aFp, uc, a.jeps, !ZDIR && f == 0, gF, gkL, gkR, gc, gaFi, gaFp, guc);
+        adj_face<ZDIR, FLUX>(cs, iv, aFi, aFp, uc, a.jeps, !ZDIR && f == 0, gF, gkL, gkR, gc, gaFi, gaFp, guc);
 #pragma unroll
         for (int s = 0; s < 4; s++) {
             double gJ = 0.0, gHr = 0.0, gHZ = 0.0;
@@ -853,8 +853,14 @@ void launch_adv_adj(const AdjAdvArgs &a, cudaStream_t st) {
     const long long nkb = (a.nnu + 31) / 32;
     const long long ncell = (long long)a.nr * a.nz;
     k_adv_adj_cell<<<warps_grid(ncell * nkb), ADJ_THREADS, 0, st>>>(a);
-    k_adv_adj_face<false><<<warps_grid((long long)(a.nr + 1) * a.nz * nkb), ADJ_THREADS, 0, st>>>(a);
-    k_adv_adj_face<true><<<warps_grid((long long)a.nr * (a.nz + 1) * nkb), ADJ_THREADS, 0, st>>>(a);
+    const int gr = warps_grid((long long)(a.nr + 1) * a.nz * nkb), gz = warps_grid((long long)a.nr * (a.nz + 1) * nkb);
+    if (a.flux == 0) {
+        k_adv_adj_face<false, 0><<<gr, ADJ_THREADS, 0, st>>>(a);
+        k_adv_adj_face<true, 0><<<gz, ADJ_THREADS, 0, st>>>(a);
+    } else {
+        k_adv_adj_face<false, 1><<<gr, ADJ_THREADS, 0, st>>>(a);
+        k_adv_adj_face<true, 1><<<gz, ADJ_THREADS, 0, st>>>(a);
+    }
 }
 
 void launch_seed_spectrum(double *gJ, const double *w, int nnu, int nr, int nz, cudaStream_t st) {

@@ -215,12 +215,47 @@ __device__ __forceinline__ void adj_recon(const ReconT &t, const CellF<double> c
     gc[2].fZ += gdfZc * iv[3]; gc[1].fZ -= gdfZc * iv[3];
 }
 
-// Forward of one face (GLF flux + upwind advection flux + the K_phiphi face values), with its
-// adjoint. Direction ZDIR: false = r face (F_J = H_r, F_Hr = D_rr J, F_HZ = D_rZ J),
+// HLL_Eigenvalues (src/M1Closure.jl:273-296) recomputed, with the adjoints gl1, gl3 of the
+// clamped outputs taken back to f and mu (+=). The clamps pass a derivative on the branch the
+// forward took; sqrt(max(g, 0)) passes none where g <= 0.
+__device__ __forceinline__ void adj_hll_eigen(double f0, double mu0, double gl1, double gl3, double &gf,
+                                              double &gmu) {
+    const bool fin = !(f0 < kFmin) && !(f0 > kFmax);
+    const bool muin = !(mu0 < -1.0) && !(mu0 > 1.0);
+    double f = f0 < kFmin ? kFmin : (f0 > kFmax ? kFmax : f0);
+    double mu = mu0 < -1.0 ? -1.0 : (mu0 > 1.0 ? 1.0 : mu0);
+    double f2 = f * f, mu2 = mu * mu, muf = mu * f;
+    double t = 4.0 - 3.0 * f2;
+    const bool tpos = t > 0.0;
+    double sq = sqrt(tpos ? t : 0.0);
+    double inv_sq = 1.0 / sq;
+    double g = (2.0 / 3.0) * (4.0 - 3.0 * f2 - sq) + 2.0 * mu2 * (2.0 - f2 - sq);
+    const bool gpos = g > 0.0;
+    double fac = sqrt(gpos ? g : 0.0);
+    double x1 = (muf - fac) * inv_sq, x3 = (muf + fac) * inv_sq;
+    double gx1 = (x1 < -1.0 || x1 > 1.0) ? 0.0 : gl1;
+    double gx3 = (x3 < -1.0 || x3 > 1.0) ? 0.0 : gl3;
+    double gmuf = (gx1 + gx3) * inv_sq;
+    double gfac = (gx3 - gx1) * inv_sq;
+    double ginv = gx1 * (muf - fac) + gx3 * (muf + fac);
+    double gsq = -ginv * inv_sq * inv_sq;
+    double gg = gpos && fac > 0.0 ? 0.5 * gfac / fac : 0.0;
+    double gf2 = gg * (-2.0 - 2.0 * mu2);
+    gsq += gg * (-2.0 / 3.0 - 2.0 * mu2);
+    double gmu2 = gg * 2.0 * (2.0 - f2 - sq);
+    if (tpos) gf2 += -3.0 * (0.5 * gsq / sq);
+    double gfl = gmuf * mu + 2.0 * f * gf2;
+    double gml = gmuf * f + 2.0 * mu * gmu2;
+    if (fin) gf += gfl;
+    if (muin) gmu += gml;
+}
+
+// Forward of one face (GLF or HLL flux + upwind advection flux + the K_phiphi face values),
+// with its adjoint. Direction ZDIR: false = r face (F_J = H_r, F_Hr = D_rr J, F_HZ = D_rZ J),
 // true = Z face (F_J = H_Z, F_Hr = D_rZ J, F_HZ = D_ZZ J). `axis` marks the r = 0 face, whose
-// right K_phiphi uses Compute_K_phiphi_InnerAxis.
-template <bool ZDIR>
-__device__ __forceinline__ void adj_face_glf(const CellF<double> cs[4], const double iv[5], double aFi, double aFp,
+// right K_phiphi uses Compute_K_phiphi_InnerAxis. FLUX: 0 = GLF, 1 = HLL.
+template <bool ZDIR, int FLUX>
+__device__ __forceinline__ void adj_face(const CellF<double> cs[4], const double iv[5], double aFi, double aFp,
                                              double uc, double jeps, bool axis, const double gF[3], double gkL,
                                              double gkR, CellF<double> gc[4], double &gaFi, double &gaFp,
                                              double &guc) {
@@ -242,7 +277,7 @@ __device__ __forceinline__ void adj_face_glf(const CellF<double> cs[4], const do
         else { g.J_L += uc * gF[0]; g.Hr_L += uc * gF[1]; g.HZ_L += uc * gF[2]; }
     }
     // GLF flux with the diffusion-limit blend, src/AdvectJandH.jl:81-118
-    {
+    if (FLUX == 0) {
         const double FJ_L = ZDIR ? q.HZ_L : q.Hr_L, FJ_R = ZDIR ? q.HZ_R : q.Hr_R;
         const double DaL = ZDIR ? DrZL : DrrL, DaR = ZDIR ? DrZR : DrrR;   // F_Hr = Da J
         const double DbL = ZDIR ? DZZL : DrZL, DbR = ZDIR ? DZZR : DrZR;   // F_HZ = Db J
@@ -263,7 +298,6 @@ __device__ __forceinline__ void adj_face_glf(const CellF<double> cs[4], const do
         g.J_R -= 0.5 * gFJg;
         g.J_L += 0.5 * gFJg;
         // F_Hr = 0.5 (Da_L J_L + Da_R J_R) - he (Hr_R - Hr_L)
-        gDrrL += 0.0;
         double gDaL = 0.5 * gF[1] * q.J_L, gDaR = 0.5 * gF[1] * q.J_R;
         double gDbL = 0.5 * gF[2] * q.J_L, gDbR = 0.5 * gF[2] * q.J_R;
         g.J_L += 0.5 * (gF[1] * DaL + gF[2] * DbL);
@@ -278,6 +312,84 @@ __device__ __forceinline__ void adj_face_glf(const CellF<double> cs[4], const do
             gDrrL += gDaL; gDrrR += gDaR; gDrZL += gDbL; gDrZR += gDbR;
         }
         // diffusion term
+        double gd = -(1.0 / 3.0) / te * gFJd;
+        gc[2].J += gd;
+        gc[1].J -= gd;
+        double gte = gFJd * (1.0 / 3.0) * (Jp - Ji) / (te * te);
+        double gtau = tpos ? gte : 0.0;
+        gtau += geps * (tau * tau - 2.0 * tau * num) / (den * den);
+        g.tau_L += gtau;
+        g.tau_R += gtau;
+    } else {
+        // HLL flux with the diffusion-limit blend, src/AdvectJandH.jl:155-204; wave speeds
+        // from M1WaveSpeeds_r/Z, src/M1Closure.jl:301-326
+        const double FJ_L = ZDIR ? q.HZ_L : q.Hr_L, FJ_R = ZDIR ? q.HZ_R : q.Hr_R;
+        const double DaL = ZDIR ? DrZL : DrrL, DaR = ZDIR ? DrZR : DrrR;   // F_Hr = Da J
+        const double DbL = ZDIR ? DZZL : DrZL, DbR = ZDIR ? DZZR : DrZR;   // F_HZ = Db J
+        const double FHr_L = DaL * q.J_L, FHr_R = DaR * q.J_R, FHZ_L = DbL * q.J_L, FHZ_R = DbR * q.J_R;
+        double tau = q.tau_L + q.tau_R;
+        double num = 0.2 + tau;
+        double den = num + tau * tau;
+        double eps = num / den;
+        double ome = 1.0 - eps;
+        const bool tpos = tau > Num<double>::tiny();
+        double te = tpos ? tau : Num<double>::tiny();
+        double Ji = cs[1].J, Jp = cs[2].J;
+        double FJd = -(1.0 / 3.0) * (Jp - Ji) / te;
+        const double muL = ZDIR ? q.nZ_L : q.nr_L, muR = ZDIR ? q.nZ_R : q.nr_R;
+        double l1L, l3L, l1R, l3R;
+        hll_eigen<double>(q.f_L, muL, l1L, l3L);
+        hll_eigen<double>(q.f_R, muR, l1R, l3R);
+        double m3 = fmax(l3L, l3R), m1 = fmin(l1L, l1R);
+        double SR = fmax(m3, 0.0), SL = fmin(m1, 0.0);
+        double dS = SR - SL;
+        const bool dpos = dS > Num<double>::tiny();
+        double inv = 1.0 / (dpos ? dS : Num<double>::tiny());
+        double SRSL = SR * SL;
+        double dJ = q.J_R - q.J_L, dHr = q.Hr_R - q.Hr_L, dHZ = q.HZ_R - q.HZ_L;
+        double nJ = SR * FJ_L - SL * FJ_R + SRSL * dJ;
+        double nHr = SR * FHr_L - SL * FHr_R + SRSL * dHr;
+        double nHZ = SR * FHZ_L - SL * FHZ_R + SRSL * dHZ;
+        double hom = 0.5 * ome;
+        double geps = gF[0] * (nJ * inv - FJd) + gF[1] * (nHr * inv - 0.5 * (FHr_L + FHr_R)) +
+                      gF[2] * (nHZ * inv - 0.5 * (FHZ_L + FHZ_R));
+        double gJh = gF[0] * eps, gHrh = gF[1] * eps, gHZh = gF[2] * eps, gFJd = gF[0] * ome;
+        // physical fluxes
+        double gFJ_L = gJh * SR * inv, gFJ_R = -gJh * SL * inv;
+        double gFHr_L = gHrh * SR * inv + gF[1] * hom, gFHr_R = -gHrh * SL * inv + gF[1] * hom;
+        double gFHZ_L = gHZh * SR * inv + gF[2] * hom, gFHZ_R = -gHZh * SL * inv + gF[2] * hom;
+        // jumps of the states
+        double cJ = gJh * SRSL * inv, cHr = gHrh * SRSL * inv, cHZ = gHZh * SRSL * inv;
+        g.J_R += cJ; g.J_L -= cJ;
+        g.Hr_R += cHr; g.Hr_L -= cHr;
+        g.HZ_R += cHZ; g.HZ_L -= cHZ;
+        // wave speeds
+        double gSR = (gJh * (FJ_L + SL * dJ) + gHrh * (FHr_L + SL * dHr) + gHZh * (FHZ_L + SL * dHZ)) * inv;
+        double gSL = (gJh * (SR * dJ - FJ_R) + gHrh * (SR * dHr - FHr_R) + gHZh * (SR * dHZ - FHZ_R)) * inv;
+        if (dpos) {
+            double gdS = -(gJh * nJ + gHrh * nHr + gHZh * nHZ) * inv * inv;
+            gSR += gdS;
+            gSL -= gdS;
+        }
+        double gl1L = 0.0, gl3L = 0.0, gl1R = 0.0, gl3R = 0.0;
+        if (m3 > 0.0) { if (l3L >= l3R) gl3L = gSR; else gl3R = gSR; }
+        if (m1 < 0.0) { if (l1L <= l1R) gl1L = gSL; else gl1R = gSL; }
+        double gmuL = 0.0, gmuR = 0.0;
+        adj_hll_eigen(q.f_L, muL, gl1L, gl3L, g.f_L, gmuL);
+        adj_hll_eigen(q.f_R, muR, gl1R, gl3R, g.f_R, gmuR);
+        g.J_L += gFHr_L * DaL + gFHZ_L * DbL;
+        g.J_R += gFHr_R * DaR + gFHZ_R * DbR;
+        double gDaL = gFHr_L * q.J_L, gDaR = gFHr_R * q.J_R, gDbL = gFHZ_L * q.J_L, gDbR = gFHZ_R * q.J_R;
+        if (ZDIR) {
+            g.nZ_L += gmuL; g.nZ_R += gmuR;
+            g.HZ_L += gFJ_L; g.HZ_R += gFJ_R;
+            gDrZL += gDaL; gDrZR += gDaR; gDZZL += gDbL; gDZZR += gDbR;
+        } else {
+            g.nr_L += gmuL; g.nr_R += gmuR;
+            g.Hr_L += gFJ_L; g.Hr_R += gFJ_R;
+            gDrrL += gDaL; gDrrR += gDaR; gDrZL += gDbL; gDrZR += gDbR;
+        }
+        // diffusion term and the blend weight, as in the GLF branch
         double gd = -(1.0 / 3.0) / te * gFJd;
         gc[2].J += gd;
         gc[1].J -= gd;

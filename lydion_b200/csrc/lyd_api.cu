@@ -1208,7 +1208,6 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     const lyd_step_params *p = &cfg->step;
     if (c->ncl != 1) return fail(c, LYD_ERR_STATE, "the adjoint runs on a single-cloud context");
     if (c->prec != LYD_PREC_FP64) return fail(c, LYD_ERR_STATE, "the adjoint runs in LYD_PREC_FP64");
-    if (c->cfg.flux_method != LYD_FLUX_GLF) return fail(c, LYD_ERR_STATE, "the adjoint supports the GLF flux");
     if (c->aF) return fail(c, LYD_ERR_STATE, "the adjoint needs alpha_F derived from alpha and H_voigt");
     LYD_TRY(check_bcs(c, LYD_BC_REFLECT, p->bc_r_right, p->bc_z_bot, p->bc_z_top));
     if (!(p->c_tilde > 0.0) || !(p->dt > 0.0) || p->n_steps < 1) return fail(c, LYD_ERR_ARG, "bad step parameters");
@@ -1408,6 +1407,7 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
             ad.nnu = nnu; ad.nr = nr; ad.nz = nz; ad.kmin = hwin[2 * n]; ad.kmax = hwin[2 * n + 1];
             ad.bc_r_right = p->bc_r_right; ad.bc_z_bot = p->bc_z_bot; ad.bc_z_top = p->bc_z_top;
             ad.ctdt = p->c_tilde * p->dt; ad.jeps = c->jeps_s; ad.heps2 = c->heps2_s;
+            ad.flux = c->cfg.flux_method == LYD_FLUX_HLL ? 1 : 0;
             launch_adv_adj(ad, c->st);
             tick(5);
             tock(2, 3, 2);

@@ -611,10 +611,11 @@ __host__ __device__ constexpr int freq_smem_doubles(int nwarps) {
     return KC_N * 32 * M + nwarps * (32 * M + 8) + nwarps * 4 * 32 * M;
 }
 
-// Four bins per lane: 2 CTAs per SM (128 registers, ~230 B of spills) measured 1.4x faster than
-// 1 CTA at 172 registers.
+// Up to four bins per lane the kernel is held to 2 CTAs per SM (128 registers). Four bins:
+// ~230 B of spills, measured 1.4x faster than 1 CTA at 172 registers. Two bins: 1.8x faster
+// than the 164 registers ptxas picks when only the block size bounds it.
 template <typename S, typename R, int M>
-__global__ void __launch_bounds__(FREQ_THREADS, M == 4 ? 2 : 1) k_freq(FreqArgs<S> a) {
+__global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<S> a) {
     extern __shared__ __align__(16) double fsm[];
     constexpr int NP = 32 * M;
     const int nw = blockDim.x >> 5;
