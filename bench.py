@@ -229,7 +229,7 @@ def e2e_form(ctx, cloud, args, barrier, stream_of, world):
                 ctx.upload(name, a)
             ctx.static_steps(1, *p, history=True)
             for a, name in zip(pinned, names):
-                a[...] = ctx.download(name)
+                ctx.download(name, out=a)
 
     ms = sharding.max_over_ranks(_timed(ctx, run, n, stream_of), device="cuda")
     nbytes = 3 * cloud.cell_bins * 8

@@ -433,7 +433,7 @@ __device__ __forceinline__ void pcr_solve(Row<M> &R_, int lane) {
     for (int s = 1; s < 32 * M; s <<= 1) {
         double ib[M];
 #pragma unroll
-        for (int m = 0; m < M; m++) ib[m] = 1.0 / R_.b[m];
+        for (int m = 0; m < M; m++) ib[m] = rcp<double>(R_.b[m]);
         double am[M], cm[M], dm[M], ibm[M], ap[M], cp[M], dp[M], ibp[M];
         nbr<M>(R_.a, am, s, -1, lane, 0.0);
         nbr<M>(R_.c, cm, s, -1, lane, 0.0);
@@ -456,7 +456,7 @@ __device__ __forceinline__ void pcr_solve(Row<M> &R_, int lane) {
         }
     }
 #pragma unroll
-    for (int m = 0; m < M; m++) R_.d[m] = R_.d[m] / R_.b[m];
+    for (int m = 0; m < M; m++) R_.d[m] = R_.d[m] * rcp<double>(R_.b[m]);
 }
 
 // Lane-serial elimination of the same system: the warp writes its rows to shared memory and
@@ -497,7 +497,7 @@ __device__ __forceinline__ void thomas_solve(Row<M> &R_, int lane, double *sm) {
 // PCR on all 64 rows, the same arithmetic per eliminated row. Returns x in d.
 __device__ __forceinline__ void cr_pcr_solve2(Row<2> &R_, int lane) {
     // odd row o = 2l+1 of this lane; o- = 2l-1 is the previous lane's odd row
-    const double ibo = 1.0 / R_.b[1];
+    const double ibo = rcp<double>(R_.b[1]);
     double a_om = __shfl_up_sync(0xffffffffu, R_.a[1], 1);
     double c_om = __shfl_up_sync(0xffffffffu, R_.c[1], 1);
     double d_om = __shfl_up_sync(0xffffffffu, R_.d[1], 1);
@@ -513,7 +513,7 @@ __device__ __forceinline__ void cr_pcr_solve2(Row<2> &R_, int lane) {
     // PCR over the 32 even rows (one per lane)
 #pragma unroll
     for (int s = 1; s < 32; s <<= 1) {
-        double ib = 1.0 / eb;
+        double ib = rcp<double>(eb);
         double am = __shfl_up_sync(0xffffffffu, ea, s), cm = __shfl_up_sync(0xffffffffu, ec, s);
         double dm = __shfl_up_sync(0xffffffffu, ed, s), ibm = __shfl_up_sync(0xffffffffu, ib, s);
         double ap = __shfl_down_sync(0xffffffffu, ea, s), cp = __shfl_down_sync(0xffffffffu, ec, s);
@@ -528,7 +528,7 @@ __device__ __forceinline__ void cr_pcr_solve2(Row<2> &R_, int lane) {
         eb = nb;
         ed = nd;
     }
-    const double xe = ed / eb;
+    const double xe = ed * rcp<double>(eb);
     // odd rows: x_o = (d_o - a_o x_e - c_o x_{e+2}) / b_o
     double xe2 = __shfl_down_sync(0xffffffffu, xe, 1);
     if (lane == 31) xe2 = 0.0;
@@ -542,7 +542,7 @@ __device__ __forceinline__ void cr_pcr_solve2(Row<2> &R_, int lane) {
 __device__ __forceinline__ void pcr_lanes(double &ea, double &eb, double &ec, double &ed, int lane) {
 #pragma unroll
     for (int s = 1; s < 32; s <<= 1) {
-        double ib = 1.0 / eb;
+        double ib = rcp<double>(eb);
         double am = __shfl_up_sync(0xffffffffu, ea, s), cm = __shfl_up_sync(0xffffffffu, ec, s);
         double dm = __shfl_up_sync(0xffffffffu, ed, s), ibm = __shfl_up_sync(0xffffffffu, ib, s);
         double ap = __shfl_down_sync(0xffffffffu, ea, s), cp = __shfl_down_sync(0xffffffffu, ec, s);
@@ -563,7 +563,7 @@ __device__ __forceinline__ void pcr_lanes(double &ea, double &eb, double &ec, do
 // 4l+2) leave row 4l, solved by PCR across the warp; rows 4l+2, then the odd rows follow by
 // back-substitution. Returns x in d; b holds the pivots for the zero-pivot check.
 __device__ __forceinline__ void cr_pcr_solve4(Row<4> &R_, int lane) {
-    const double ib1 = 1.0 / R_.b[1], ib3 = 1.0 / R_.b[3];
+    const double ib1 = rcp<double>(R_.b[1]), ib3 = rcp<double>(R_.b[3]);
     double a3p = __shfl_up_sync(0xffffffffu, R_.a[3], 1), c3p = __shfl_up_sync(0xffffffffu, R_.c[3], 1);
     double d3p = __shfl_up_sync(0xffffffffu, R_.d[3], 1), ib3p = __shfl_up_sync(0xffffffffu, ib3, 1);
     if (lane == 0) { a3p = 0.0; c3p = 0.0; d3p = 0.0; ib3p = 1.0; }
@@ -576,7 +576,7 @@ __device__ __forceinline__ void cr_pcr_solve4(Row<4> &R_, int lane) {
     double a2 = al * R_.a[1], b2 = R_.b[2] + al * R_.c[1] + ga * R_.a[3], c2 = ga * R_.c[3];
     double d2 = R_.d[2] + al * R_.d[1] + ga * R_.d[3];
     // level 2: row 4l eliminates 4l-2 (previous lane's row 2) and 4l+2
-    const double ib2 = 1.0 / b2;
+    const double ib2 = rcp<double>(b2);
     double a2p = __shfl_up_sync(0xffffffffu, a2, 1), c2p = __shfl_up_sync(0xffffffffu, c2, 1);
     double d2p = __shfl_up_sync(0xffffffffu, d2, 1), ib2p = __shfl_up_sync(0xffffffffu, ib2, 1);
     if (lane == 0) { a2p = 0.0; c2p = 0.0; d2p = 0.0; ib2p = 1.0; }
@@ -584,7 +584,7 @@ __device__ __forceinline__ void cr_pcr_solve4(Row<4> &R_, int lane) {
     ga = -c0 * ib2;
     double ea = al * a2p, eb = b0 + al * c2p + ga * a2, ec = ga * c2, ed = d0 + al * d2p + ga * d2;
     pcr_lanes(ea, eb, ec, ed, lane);
-    const double x0 = ed / eb;
+    const double x0 = ed * rcp<double>(eb);
     double x4 = __shfl_down_sync(0xffffffffu, x0, 1);
     if (lane == 31) x4 = 0.0;
     const double x2 = (d2 - a2 * x0 - c2 * x4) * ib2;
@@ -605,10 +605,51 @@ __device__ __forceinline__ double warp_sum(double v) {
 // Per-k constants of UpdateFreqFactors! staged in shared memory once per CTA.
 enum { KC_NCK, KC_NCKP, KC_NCKM, KC_DNKP, KC_DNK, KC_DNKM, KC_IDNU, KC_ICK, KC_ICKP, KC_ICKM, KC_DNU, KC_N };
 
+// Per-cell inputs staged in shared memory, 32 cells at a time per warp.
+enum { CS_ALPHA, CS_ALPHA_C, CS_PD, CS_JS, CS_PHI_INV, CS_ALPHA_CF, CS_T, CS_DUR_DR, CS_DUR_DZ, CS_DUZ_DR,
+       CS_DUZ_DZ, CS_UR_OVER_R, CS_DV, CS_DRU_R, CS_DRU_Z, CS_N };
+
+// The next cell's bin rows (J, H_r, H_Z, H_voigt, J_old) are prefetched into a per-warp double
+// buffer while the current cell computes, up to two bins per lane (four or more would leave
+// shared memory for one CTA per SM).
+template <int M> __host__ __device__ constexpr bool freq_prefetch() { return M <= 2; }
+
+// Shared memory of the frequency kernel, in doubles: FP64 per-k constants, per-warp reduction
+// rows, per-warp staged cell inputs, the per-warp prefetch buffers, and the lane-serial
+// solver rows when that solver runs.
 template <int M>
-__host__ __device__ constexpr int freq_smem_doubles(int nwarps) {
-    // FP64 constants, per-warp reduction rows, lane-serial solver rows
-    return KC_N * 32 * M + nwarps * (32 * M + 8) + nwarps * 4 * 32 * M;
+__host__ __device__ constexpr int freq_smem_off_cs(int nwarps) { return KC_N * 32 * M + nwarps * (32 * M + 8); }
+template <int M>
+__host__ __device__ constexpr int freq_smem_off_pf(int nwarps) { return freq_smem_off_cs<M>(nwarps) + nwarps * CS_N * 32; }
+template <int M>
+__host__ __device__ constexpr int freq_smem_off_tsm(int nwarps) {
+    return freq_smem_off_pf<M>(nwarps) + (freq_prefetch<M>() ? nwarps * 2 * 5 * 32 * M : 0);
+}
+template <int M>
+__host__ __device__ constexpr int freq_smem_doubles(int nwarps, bool thomas) {
+    return freq_smem_off_tsm<M>(nwarps) + (thomas ? nwarps * 4 * 32 * M : 0);
+}
+
+// Asynchronous global -> shared copy of one 4- or 8-byte element (cp.async, L1-allocating).
+template <typename T>
+__device__ __forceinline__ void cp_async_el(T *dst, const T *src) {
+    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "element size");
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// The cells [wbeg, wend) of a work item that warp `warp` of `nw` handles: one contiguous run
+// per warp (k_freq and k_find_active sum their partials in this order).
+__device__ __forceinline__ void warp_cell_run(int4 it, int warp, int nw, int &wbeg, int &wend) {
+    const int per = (it.z - it.y + nw - 1) / nw;
+    wbeg = it.y + warp * per;
+    wend = min(it.z, wbeg + per);
 }
 
 // Up to four bins per lane the kernel is held to 2 CTAs per SM (128 registers). Four bins:
@@ -619,9 +660,10 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
     extern __shared__ __align__(16) double fsm[];
     constexpr int NP = 32 * M;
     const int nw = blockDim.x >> 5;
+    constexpr bool PF = freq_prefetch<M>();
     double *kc = fsm;                              // [KC_N][NP]
     double *red = fsm + KC_N * NP;                 // [nwarps][NP + 8]
-    double *tsm = red + nw * (NP + 8);             // [nwarps][4][NP] (lane-serial solver)
+    double *tsm = fsm + freq_smem_off_tsm<M>(nw);  // [nwarps][4][NP] (lane-serial solver)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nnu = a.nnu;
     for (int t = threadIdx.x; t < NP; t += blockDim.x) {
@@ -653,32 +695,103 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
     double acc_tot = 0.0, acc_mf = 0.0, acc_net = 0.0, acc_out = 0.0, acc_L = 0.0, acc_esc = 0.0;
     int bad = 0;
 
-    for (int cl = it.y + warp; cl < it.z; cl += nw) {
+    int wbeg, wend;
+    warp_cell_run(it, warp, nw, wbeg, wend);
+    double *cs = fsm + freq_smem_off_cs<M>(nw) + warp * CS_N * 32;      // [CS_N][32]
+    S *pf = reinterpret_cast<S *>(fsm + freq_smem_off_pf<M>(nw)) + warp * 2 * 5 * NP;  // [2][5][NP]
+    const bool jo_alias = a.Jold == a.Jin;
+    const bool need_ff = a.do_freq && a.update_ff, need_js = a.do_emission || (a.parts & PART_DIAG);
+    // copies of cell cl's bin rows into prefetch buffer b (element k of lane l, bin m at m*32+l)
+    auto issue = [&](int cl, int b) {
+        const long long base = o3 + (long long)cl * nnu;
+        S *d = pf + b * 5 * NP;
+#pragma unroll
+        for (int m = 0; m < M; m++) {
+            const int k = lane * M + m, q = m * 32 + lane;
+            if (k < nnu) {
+                cp_async_el(d + q, a.Jin + base + k);
+                cp_async_el(d + NP + q, a.Hrin + base + k);
+                cp_async_el(d + 2 * NP + q, a.HZin + base + k);
+                cp_async_el(d + 3 * NP + q, a.Hv + base + k);
+                if (!jo_alias) cp_async_el(d + 4 * NP + q, a.Jold + base + k);
+            }
+        }
+    };
+    if constexpr (PF) {
+        if (wbeg < wend) issue(wbeg, 0);
+        cp_async_commit();
+    }
+    int g0 = wbeg;
+    for (int cl = wbeg; cl < wend; cl++) {
         const int i = cl % nr, j = cl / nr;
         const long long c = oc + cl;
         const long long base = o3 + (long long)cl * nnu;
+        if (((cl - wbeg) & 31) == 0) {
+            // stage the per-cell inputs of the next 32 cells of the run (one coalesced load per
+            // field instead of a dependent load per cell)
+            g0 = cl;
+            __syncwarp();
+            const bool v = cl + lane < wend;
+            const long long cc = c + lane;
+            auto ld = [&](const double *p, bool need) { return (v && need && p) ? __ldg(p + cc) : 0.0; };
+            cs[CS_ALPHA * 32 + lane] = ld(a.alpha, a.do_emission || need_ff);
+            cs[CS_ALPHA_C * 32 + lane] = ld(a.alpha_c, a.do_emission);
+            cs[CS_PD * 32 + lane] = ld(a.pd, a.do_emission);
+            cs[CS_JS * 32 + lane] = ld(a.js, need_js);
+            cs[CS_PHI_INV * 32 + lane] = ld(a.phi_inv, a.do_emission && !a.phi);
+            cs[CS_ALPHA_CF * 32 + lane] = ld(a.alpha_cF, a.do_emission);
+            cs[CS_T * 32 + lane] = ld(a.T, need_ff);
+            cs[CS_DUR_DR * 32 + lane] = ld(a.dur_dr, need_ff);
+            cs[CS_DUR_DZ * 32 + lane] = ld(a.dur_dZ, need_ff);
+            cs[CS_DUZ_DR * 32 + lane] = ld(a.duZ_dr, need_ff);
+            cs[CS_DUZ_DZ * 32 + lane] = ld(a.duZ_dZ, need_ff);
+            cs[CS_UR_OVER_R * 32 + lane] = ld(a.ur_over_r, need_ff);
+            cs[CS_DV * 32 + lane] = ld(a.dV, a.parts != 0);
+            cs[CS_DRU_R * 32 + lane] = ld(a.dru_r, a.do_emission);
+            cs[CS_DRU_Z * 32 + lane] = ld(a.dru_Z, a.do_emission);
+            __syncwarp();
+        }
+        const double *cv = cs + (cl - g0);        // cv[f * 32]: field f of this cell
         S J[M], Hr[M], HZ[M];
         R Hv[M];
         double Jo[M];
+        if constexpr (PF) {
+            const int b = (cl - wbeg) & 1;
+            if (cl + 1 < wend) issue(cl + 1, b ^ 1);
+            cp_async_commit();
+            cp_async_wait<1>();                   // this cell's copies (each lane reads its own)
+            const S *d = pf + b * 5 * NP;
 #pragma unroll
-        for (int m = 0; m < M; m++) {
-            int k = lane * M + m;
-            bool vld = k < nnu;
-            J[m] = vld ? a.Jin[base + k] : S(0);
-            Hr[m] = vld ? a.Hrin[base + k] : S(0);
-            HZ[m] = vld ? a.HZin[base + k] : S(0);
-            Hv[m] = vld ? R(__ldg(a.Hv + base + k)) : R(0);
-            Jo[m] = vld ? double(a.Jold[base + k]) : 0.0;
+            for (int m = 0; m < M; m++) {
+                const int k = lane * M + m, q = m * 32 + lane;
+                const bool vld = k < nnu;
+                J[m] = vld ? d[q] : S(0);
+                Hr[m] = vld ? d[NP + q] : S(0);
+                HZ[m] = vld ? d[2 * NP + q] : S(0);
+                Hv[m] = vld ? R(d[3 * NP + q]) : R(0);
+                Jo[m] = vld ? double(jo_alias ? d[q] : d[4 * NP + q]) : 0.0;
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < M; m++) {
+                int k = lane * M + m;
+                bool vld = k < nnu;
+                J[m] = vld ? a.Jin[base + k] : S(0);
+                Hr[m] = vld ? a.Hrin[base + k] : S(0);
+                HZ[m] = vld ? a.HZin[base + k] : S(0);
+                Hv[m] = vld ? R(__ldg(a.Hv + base + k)) : R(0);
+                Jo[m] = vld ? double(a.Jold[base + k]) : 0.0;
+            }
         }
         double dr_sum = 0.0, dz_sum = 0.0;
         // ---- LyaEmissionAbsorptionUpdate! (src/ConstantsAndFunctions.jl:526-567) ----
         if (a.do_emission) {
-            const R al = R(__ldg(a.alpha + c)), acv = R(__ldg(a.alpha_c + c));
-            const R al_pd = al * R(__ldg(a.pd + c));
-            const R js_ct = R(__ldg(a.js + c) * c_tilde / a.j_scale);
+            const R al = R(cv[CS_ALPHA * 32]), acv = R(cv[CS_ALPHA_C * 32]);
+            const R al_pd = al * R(cv[CS_PD * 32]);
+            const R js_ct = R(cv[CS_JS * 32] * c_tilde / a.j_scale);
             const R ct = R(c_tilde), dtr = R(dt);
-            const R pinv = a.phi ? R(0) : R(__ldg(a.phi_inv + c));
-            const R acF = a.alpha_cF ? R(__ldg(a.alpha_cF + c)) : R(0);
+            const R pinv = a.phi ? R(0) : R(cv[CS_PHI_INV * 32]);
+            const R acF = a.alpha_cF ? R(cv[CS_ALPHA_CF * 32]) : R(0);
 #pragma unroll
             for (int m = 0; m < M; m++) {
                 int k = lane * M + m;
@@ -689,8 +802,8 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
                 R dJdt = js_ct * phi;
                 R aH = a.aF ? R(__ldg(a.aF + base + k)) : (a.alpha_cF ? al * Hv[m] + acF : al * Hv[m]);
                 double dn = kc[KC_DNU * NP + k];
-                R Jn = (R(Jo[m]) + dJdt * dtr) / (R(1) + aabs * ct * dtr);
-                R iden = R(1) / (R(1) + aH * ct * dtr);
+                R Jn = (R(Jo[m]) + dJdt * dtr) * rcp<R>(R(1) + aabs * ct * dtr);
+                R iden = rcp<R>(R(1) + aH * ct * dtr);
                 R hr = R(Hr[m]) * iden;
                 R hz = R(HZ[m]) * iden;
                 dr_sum += dn * (double(Hr[m]) - double(hr));
@@ -704,8 +817,8 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
             dz_sum = warp_sum(dz_sum);
             if (lane == 0 && a.dru_r) {
                 const double k4 = kFourPiOverC * (1.0 / c_tilde) * a.j_scale;
-                a.dru_r[c] += k4 * dr_sum;
-                a.dru_Z[c] += k4 * dz_sum;
+                a.dru_r[c] = cv[CS_DRU_R * 32] + k4 * dr_sum;
+                a.dru_Z[c] = cv[CS_DRU_Z * 32] + k4 * dz_sum;
             }
         }
         // ---- FrequencyUpdateJLya_AllCells! (src/UpdateLyaJandH.jl:231-391) ----
@@ -714,13 +827,13 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
             double Fp[M], F0[M], Fm[M];
             if (a.update_ff) {
                 // UpdateFreqFactors!, src/FreqFactors.jl:181-275
-                const double T = __ldg(a.T + c);
+                const double T = cv[CS_T * 32];
                 const double dnuD = compute_dnuD(T);
-                const double alv = __ldg(a.alpha + c);
+                const double alv = cv[CS_ALPHA * 32];
                 const double pref = 0.5 * (alv > a.alpha_floor ? alv : a.alpha_floor) * (dnuD * dnuD);
                 const double rec0 = kHOverKB / T;
-                const R ga = R(__ldg(a.dur_dr + c)), gb = R(__ldg(a.dur_dZ + c)), gc = R(__ldg(a.duZ_dr + c));
-                const R gd = R(__ldg(a.duZ_dZ + c)), ge = R(__ldg(a.ur_over_r + c));
+                const R ga = R(cv[CS_DUR_DR * 32]), gb = R(cv[CS_DUR_DZ * 32]), gc = R(cv[CS_DUZ_DR * 32]);
+                const R gd = R(cv[CS_DUZ_DZ * 32]), ge = R(cv[CS_UR_OVER_R * 32]);
                 // K_k = pref H_voigt[k] and 1/K_k once per bin; the k+-1 neighbours come by
                 // shuffle (the same products the reference forms at k-1 and k+1)
                 // The frequency factors stay FP64 in every precision variant: with F/dw up to
@@ -730,7 +843,7 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
 #pragma unroll
                 for (int m = 0; m < M; m++) {
                     Kb[m] = pref * double(Hv[m]);
-                    iK[m] = 1.0 / Kb[m];
+                    iK[m] = rcp<double>(Kb[m]);
                 }
                 double K_up = __shfl_up_sync(0xffffffffu, Kb[M - 1], 1);
                 double K_dn = __shfl_down_sync(0xffffffffu, Kb[0], 1);
@@ -767,8 +880,8 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
                     omphi_LR(Pk, oLk, xLk, oRk, xRk);
                     omphi_L(Pkm, oLkm, xLkm);
                     double idn = kc[KC_IDNU * NP + k];
-                    double dkp = idn * (1.0 / (xLk * rk - xRkp * rkp));
-                    double dkm = idn * (1.0 / (xLkm * rkm - xRk * rk));
+                    double dkp = idn * rcp<double>(xLk * rk - xRkp * rkp);
+                    double dkm = idn * rcp<double>(xLkm * rkm - xRk * rk);
                     Fp[m] = oRkp * dkp;
                     Fm[m] = oLkm * dkm;
                     F0[m] = oLk * dkp + oRk * dkm;
@@ -816,7 +929,7 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
                 double Jn = in ? sys.d[m] : double(J[m]);
                 if (!(sys.b[m] != 0.0)) bad |= ERRB_SOLVE;
                 double Jf = Jn > jeps ? Jn : jeps;
-                double ratio = Jf * (1.0 / (Jo[m] > jeps ? Jo[m] : jeps));
+                double ratio = Jf * rcp<double>(Jo[m] > jeps ? Jo[m] : jeps);
                 double hr = double(Hr[m]) * ratio, hz = double(HZ[m]) * ratio;
                 double H2 = hr * hr + hz * hz;
                 if (H2 > Jf * Jf) {
@@ -842,7 +955,7 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
         }
         // ---- epilogue partials ----
         if (a.parts & PART_ACTIVE) {
-            const double dV = __ldg(a.dV + c);
+            const double dV = cv[CS_DV * 32];
 #pragma unroll
             for (int m = 0; m < M; m++) {
                 int k = lane * M + m;
@@ -875,13 +988,13 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
             }
             acc_esc += esc;
             if (lane == 0) {
-                const double dV = __ldg(a.dV + c);
+                const double dV = cv[CS_DV * 32];
                 const double k4 = kFourPiOverC * (1.0 / c_tilde) * a.j_scale;
                 const double inv_dt = 1.0 / dt;
                 double fr = (k4 * dr_sum) * inv_dt, fz = (k4 * dz_sum) * inv_dt;
                 if (a.f_r) { a.f_r[c] = fr; a.f_Z[c] = fz; }
                 acc_mf += dV * sqrt(fr * fr + fz * fz);
-                acc_L += kFourPi * dV * __ldg(a.js + c);
+                acc_L += kFourPi * dV * cv[CS_JS * 32];
                 double drr = __ldg(a.rCoM + cd.ocol + i), dzz = __ldg(a.ZCoM + cd.orow + j) - z_center;
                 double dist = sqrt(drr * drr + dzz * dzz);
                 double frad = 0.0;
@@ -894,6 +1007,7 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
             }
         }
     }
+    if constexpr (PF) cp_async_wait<0>();
     if (bad) atomicOr(a.err, bad);
     if (!a.parts) return;
     // ---- CTA reduction of the partials, fixed order ----
@@ -935,7 +1049,9 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_find_active(const S *J, int nn
 #pragma unroll
     for (int m = 0; m < M; m++) acc_e[m] = 0.0;
     double acc_tot = 0.0;
-    for (int c = it.y + warp; c < it.z; c += nw) {
+    int wbeg, wend;
+    warp_cell_run(it, warp, nw, wbeg, wend);
+    for (int c = wbeg; c < wend; c++) {
         const double v = __ldg(dV + oc + c);
 #pragma unroll
         for (int m = 0; m < M; m++) {
@@ -1088,13 +1204,15 @@ int freq_blocks(int ncell, int dev) {
 
 template <typename S, typename R, int M>
 static void freq_launch(const void *args, int nitems, cudaStream_t st) {
-    size_t sm = sizeof(double) * freq_smem_doubles<M>(FREQ_THREADS / 32);
+    const FreqArgs<S> &fa = *static_cast<const FreqArgs<S> *>(args);
+    const size_t sm = sizeof(double) * freq_smem_doubles<M>(FREQ_THREADS / 32, fa.solver == SOLVER_THOMAS);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_freq<S, R, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        const size_t smax = sizeof(double) * freq_smem_doubles<M>(FREQ_THREADS / 32, true);
+        cudaFuncSetAttribute(k_freq<S, R, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
         attr = true;
     }
-    k_freq<S, R, M><<<nitems, FREQ_THREADS, sm, st>>>(*static_cast<const FreqArgs<S> *>(args));
+    k_freq<S, R, M><<<nitems, FREQ_THREADS, sm, st>>>(fa);
 }
 
 void launch_freq(int prec, const void *args, int nnu, int nitems, cudaStream_t st) {

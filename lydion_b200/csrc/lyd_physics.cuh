@@ -56,6 +56,22 @@ template <> struct Num<float> {
 __device__ __forceinline__ double rsq(double x) { return sqrt(x); }
 __device__ __forceinline__ float rsq(float x) { return sqrtf(x); }
 
+// Reciprocal 1 / y. FP64: the hardware's approximate reciprocal (PTX rcp.approx.ftz.f64)
+// refined by two Newton-Raphson steps for 1/y, x <- x + x (1 - y x), each written as two
+// fused multiply-adds; every step squares the relative error (Markstein, IBM J. Res. Dev. 34
+// (1990) 111-119). No special-case branches: the callers divide by positive normal numbers
+// whose reciprocals are normal. FP32: the IEEE division.
+template <typename R> __device__ __forceinline__ R rcp(R y);
+template <> __device__ __forceinline__ double rcp<double>(double y) {
+    double x;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(x) : "d"(y));
+    double e = fma(-y, x, 1.0);
+    x = fma(x, e, x);
+    e = fma(-y, x, 1.0);
+    return fma(x, e, x);
+}
+template <> __device__ __forceinline__ float rcp<float>(float y) { return 1.0f / y; }
+
 // MinMod, src/ConstantsAndFunctions.jl:1571-1582
 template <typename R>
 __device__ __forceinline__ R minmod(R a, R b) {
@@ -66,7 +82,7 @@ __device__ __forceinline__ R minmod(R a, R b) {
 template <typename R>
 __device__ __forceinline__ R chi_L84(R f) {
     R f2 = f * f;
-    return (R(3) + R(4) * f2) / (R(5) + R(2) * rsq(R(4) - R(3) * f2));
+    return (R(3) + R(4) * f2) * rcp<R>(R(5) + R(2) * rsq(R(4) - R(3) * f2));
 }
 
 // Compute_D_Edd_from_f_n, src/M1Closure.jl:91-119
@@ -96,10 +112,10 @@ __device__ __forceinline__ void D_edd(R Hr, R HZ, R J, R jeps, R heps2, R &Drr, 
         return;
     }
     R Hmag = rsq(H2);
-    R f = Hmag / J;
+    R f = Hmag * rcp<R>(J);
     f = f < Num<R>::fmin() ? Num<R>::fmin() : (f > Num<R>::fmax() ? Num<R>::fmax() : f);
     R chi = chi_L84(f);
-    R inv_H = R(1) / Hmag;
+    R inv_H = rcp<R>(Hmag);
     R a = (R(1) - chi) * R(0.5);
     R b = (R(3) * chi - R(1)) * R(0.5);
     R nr = Hr * inv_H, nZ = HZ * inv_H;
@@ -117,7 +133,7 @@ __device__ __forceinline__ void hll_eigen(R f, R mu, R &l1, R &l3) {
     R f2 = f * f, mu2 = mu * mu, muf = mu * f;
     R t = R(4) - R(3) * f2;
     R sq = rsq(t > R(0) ? t : R(0));
-    R inv_sq = R(1) / sq;
+    R inv_sq = rcp<R>(sq);
     R g = R(2) / R(3) * (R(4) - R(3) * f2 - sq) + R(2) * mu2 * (R(2) - f2 - sq);
     R fac = rsq(g > R(0) ? g : R(0));
     R x1 = (muf - fac) * inv_sq, x3 = (muf + fac) * inv_sq;
@@ -140,7 +156,7 @@ template <typename R> struct CellF { R J, fr, fZ; };
 
 template <typename R>
 __device__ __forceinline__ CellF<R> cell_f(R J, R Hr, R HZ, R jeps) {
-    R iJ = R(1) / (J > jeps ? J : jeps);
+    R iJ = rcp<R>(J > jeps ? J : jeps);
     CellF<R> c;
     c.J = J; c.fr = Hr * iJ; c.fZ = HZ * iJ;
     return c;
@@ -173,15 +189,15 @@ __device__ __forceinline__ Recon<R> reconstruct_f(const CellF<R> &cm1, const Cel
     R fZL = ci.fZ + dfZL * dL, fZR = cp1.fZ - dfZR * dR;
 
     R fL = rsq(frL * frL + fZL * fZL);
-    if (fL > R(1)) { R inv = R(1) / fL; frL *= inv; fZL *= inv; fL = R(1); }
+    if (fL > R(1)) { R inv = rcp<R>(fL); frL *= inv; fZL *= inv; fL = R(1); }
     R fR = rsq(frR * frR + fZR * fZR);
-    if (fR > R(1)) { R inv = R(1) / fR; frR *= inv; fZR *= inv; fR = R(1); }
+    if (fR > R(1)) { R inv = rcp<R>(fR); frR *= inv; fZR *= inv; fR = R(1); }
 
     o.Hr_L = frL * o.J_L; o.Hr_R = frR * o.J_R;
     o.HZ_L = fZL * o.J_L; o.HZ_R = fZR * o.J_R;
-    if (fL > R(0)) { R inv = R(1) / fL; o.nr_L = frL * inv; o.nZ_L = fZL * inv; }
+    if (fL > R(0)) { R inv = rcp<R>(fL); o.nr_L = frL * inv; o.nZ_L = fZL * inv; }
     else { o.nr_L = R(0); o.nZ_L = R(0); }
-    if (fR > R(0)) { R inv = R(1) / fR; o.nr_R = frR * inv; o.nZ_R = fZR * inv; }
+    if (fR > R(0)) { R inv = rcp<R>(fR); o.nr_R = frR * inv; o.nZ_R = fZR * inv; }
     else { o.nr_R = R(0); o.nZ_R = R(0); }
     o.f_L = fL; o.f_R = fR;
     return o;
@@ -205,10 +221,10 @@ __device__ __forceinline__ void m1_flux(R FJ_L, R FJ_R, R FHr_L, R FHr_R, R FHZ_
                                         const Recon<R> &q, R Ji, R Jip1, R &FJ, R &FHr, R &FHZ) {
     R tau = q.tau_L + q.tau_R;
     R num = R(0.2) + tau;
-    R eps = num / (num + tau * tau);
+    R eps = num * rcp<R>(num + tau * tau);
     R ome = R(1) - eps;
     R tau_eff = tau > Num<R>::tiny() ? tau : Num<R>::tiny();
-    R FJ_diff = -Num<R>::third() * (Jip1 - Ji) / tau_eff;
+    R FJ_diff = -Num<R>::third() * (Jip1 - Ji) * rcp<R>(tau_eff);
     if (FLUX == 0) {
         R FJ_glf = R(0.5) * (FJ_L + FJ_R) - R(0.5) * (q.J_R - q.J_L);
         FJ = eps * FJ_glf + ome * FJ_diff;
@@ -222,7 +238,7 @@ __device__ __forceinline__ void m1_flux(R FJ_L, R FJ_R, R FHr_L, R FHr_R, R FHZ_
         R SR = fmax(fmax(l3L, l3R), R(0));
         R SL = fmin(fmin(l1L, l1R), R(0));
         R dS = SR - SL;
-        R inv_dS = R(1) / (dS > Num<R>::tiny() ? dS : Num<R>::tiny());
+        R inv_dS = rcp<R>(dS > Num<R>::tiny() ? dS : Num<R>::tiny());
         R SRSL = SR * SL;
         R FJh = (SR * FJ_L - SL * FJ_R + SRSL * (q.J_R - q.J_L)) * inv_dS;
         R FHrh = (SR * FHr_L - SL * FHr_R + SRSL * (q.Hr_R - q.Hr_L)) * inv_dS;
@@ -242,7 +258,7 @@ __device__ __forceinline__ R adv_flux(R uc, R L, R Rv) { return uc * (uc < R(0) 
 template <typename R>
 __device__ __forceinline__ R k_phiphi_axis(R J, R HZ, R jeps) {
     J = J > jeps ? J : jeps;
-    R fZ = HZ / J;
+    R fZ = HZ * rcp<R>(J);
     fZ = fZ < R(-1) ? R(-1) : (fZ > R(1) ? R(1) : fZ);
     R f = fabs(fZ);
     R nZ = f > R(0) ? (fZ > R(0) ? R(1) : R(-1)) : R(0);
@@ -270,14 +286,14 @@ __device__ __forceinline__ void omphi_L(double P, double &omp, double &chi) {
     if (P <= -kPmax) { omp = exp(kPmax); chi = (1.0 - omp) / (-kPmax); return; }
     if (fabs(P) < kPmin) { omp = 1.0 - P + 0.5 * (P * P); chi = 1.0 - 0.5 * P; return; }
     omp = exp(-P);
-    chi = (1.0 - omp) / P;
+    chi = (1.0 - omp) * rcp<double>(P);
 }
 __device__ __forceinline__ void omphi_R(double P, double &omp, double &chi) {
     if (P >= kPmax) { omp = exp(kPmax); chi = (1.0 - omp) / kPmax; return; }
     if (P <= -kPmax) { omp = exp(-kPmax); chi = (1.0 - omp) / (-kPmax); return; }
     if (fabs(P) < kPmin) { omp = 1.0 + P + 0.5 * (P * P); chi = -1.0 - 0.5 * P; return; }
     omp = exp(P);
-    chi = (1.0 - omp) / P;
+    chi = (1.0 - omp) * rcp<double>(P);
 }
 // Both of the above at once for the same P (used for P_k, which needs phi^L and phi^R):
 // one exponential and one reciprocal of P serve the two branches.
@@ -288,8 +304,8 @@ __device__ __forceinline__ void omphi_LR(double P, double &oL, double &xL, doubl
         return;
     }
     double e = exp(-P);
-    double ie = 1.0 / e;
-    double iP = 1.0 / P;
+    double ie = rcp<double>(e);
+    double iP = rcp<double>(P);
     oL = e;
     xL = (1.0 - e) * iP;
     oR = ie;

@@ -76,7 +76,15 @@ class M1Context:
         a = _c64(arr)
         self._ck(lib().lyd_upload(self._h, F[name], _dp(a), a.size))
 
-    def download(self, name, shape=None):
+    def download(self, name, shape=None, out=None):
+        """Copy a field to the host. `out`, when given, is a C-contiguous float64 array of the
+        field's size that receives the data in place (page-locked memory makes the copy a
+        direct DMA); otherwise a new array is returned."""
+        if out is not None:
+            if out.dtype != np.float64 or not out.flags.c_contiguous:
+                raise ValueError("out must be a C-contiguous float64 array")
+            self._ck(lib().lyd_download(self._h, F[name], _dp(out), out.size))
+            return out
         if shape is None:
             if F[name] < 16:
                 shape = (self.n_z, self.n_r, self.n_nu)
