@@ -90,7 +90,7 @@ __device__ __forceinline__ void pcr(RowA<M> &R_, int lane) {
     for (int s = 1; s < 32 * M; s <<= 1) {
         double ib[M];
 #pragma unroll
-        for (int m = 0; m < M; m++) ib[m] = 1.0 / R_.b[m];
+        for (int m = 0; m < M; m++) ib[m] = rcp<double>(R_.b[m]);
         double am[M], cm[M], dm[M], ibm[M], ap[M], cp[M], dp[M], ibp[M];
         nbrs<M>(R_.a, am, s, -1, lane, 0.0);
         nbrs<M>(R_.c, cm, s, -1, lane, 0.0);
@@ -113,14 +113,14 @@ __device__ __forceinline__ void pcr(RowA<M> &R_, int lane) {
         }
     }
 #pragma unroll
-    for (int m = 0; m < M; m++) R_.d[m] = R_.d[m] / R_.b[m];
+    for (int m = 0; m < M; m++) R_.d[m] = R_.d[m] * rcp<double>(R_.b[m]);
 }
 
 // Two rows per lane: one cyclic-reduction step over the odd rows, PCR across the warp on the
 // even rows, back-substitution of the odd rows (the same scheme as the forward frequency
 // kernel's two-bins-per-lane solve).
 __device__ __forceinline__ void cr_pcr2(RowA<2> &R_, int lane) {
-    const double ibo = 1.0 / R_.b[1];
+    const double ibo = rcp<double>(R_.b[1]);
     double a_om = __shfl_up_sync(0xffffffffu, R_.a[1], 1);
     double c_om = __shfl_up_sync(0xffffffffu, R_.c[1], 1);
     double d_om = __shfl_up_sync(0xffffffffu, R_.d[1], 1);
@@ -133,7 +133,7 @@ __device__ __forceinline__ void cr_pcr2(RowA<2> &R_, int lane) {
     double ed = R_.d[0] + al * d_om + ga * R_.d[1];
 #pragma unroll
     for (int s = 1; s < 32; s <<= 1) {
-        double ib = 1.0 / eb;
+        double ib = rcp<double>(eb);
         double am = __shfl_up_sync(0xffffffffu, ea, s), cm = __shfl_up_sync(0xffffffffu, ec, s);
         double dm = __shfl_up_sync(0xffffffffu, ed, s), ibm = __shfl_up_sync(0xffffffffu, ib, s);
         double ap = __shfl_down_sync(0xffffffffu, ea, s), cp = __shfl_down_sync(0xffffffffu, ec, s);
@@ -148,7 +148,7 @@ __device__ __forceinline__ void cr_pcr2(RowA<2> &R_, int lane) {
         eb = nb;
         ed = nd;
     }
-    const double xe = ed / eb;
+    const double xe = ed * rcp<double>(eb);
     double xe2 = __shfl_down_sync(0xffffffffu, xe, 1);
     if (lane == 31) xe2 = 0.0;
     R_.d[0] = xe;
@@ -168,8 +168,49 @@ struct FfIn {
     int recoil;
 };
 
+// phi / chi of one P and their P-derivatives with one exponential and one reciprocal
+// (OneMinusphi_L/R_and_chi_L/R, src/FreqFactors.jl:54-133). L: omp = e^-P, chi = (1 - omp)/P;
+// R: omp = e^P, chi = (1 - omp)/P; the clamp and Taylor branches as the forward takes them.
+struct Omphi { double o, x, d_o, d_x; };
+template <bool LEFT>
+__device__ __forceinline__ Omphi omphi_d(double P) {
+    Omphi r;
+    const double sg = LEFT ? -1.0 : 1.0;
+    if (P >= kPmax || P <= -kPmax) {
+        const double Pc = P >= kPmax ? kPmax : -kPmax;
+        r.o = exp(sg * Pc);
+        r.x = (1.0 - r.o) / Pc;
+        r.d_o = 0.0; r.d_x = 0.0;
+        return r;
+    }
+    if (fabs(P) < kPmin) {
+        r.o = 1.0 + sg * P + 0.5 * (P * P);
+        r.x = -sg - 0.5 * P;
+        r.d_o = sg + P;
+        r.d_x = -0.5;
+        return r;
+    }
+    r.o = exp(sg * P);
+    const double iP = rcp<double>(P);
+    r.x = (1.0 - r.o) * iP;
+    r.d_o = sg * r.o;
+    r.d_x = (-r.d_o - r.x) * iP;
+    return r;
+}
+// Both sides of the same P: e^P = 1 / e^-P and one reciprocal of P serve the two.
+__device__ __forceinline__ void omphi_d_LR(double P, Omphi &L, Omphi &R_) {
+    if (P >= kPmax || P <= -kPmax || fabs(P) < kPmin) {
+        L = omphi_d<true>(P);
+        R_ = omphi_d<false>(P);
+        return;
+    }
+    const double e = exp(-P), ie = rcp<double>(e), iP = rcp<double>(P);
+    L.o = e; L.x = (1.0 - e) * iP; L.d_o = -e; L.d_x = (e - L.x) * iP;
+    R_.o = ie; R_.x = (1.0 - ie) * iP; R_.d_o = ie; R_.d_x = (-ie - R_.x) * iP;
+}
+
 __device__ __forceinline__ void ff_fwd(const FfIn &q, double &Fp, double &F0, double &Fm) {
-    double iKkm = 1.0 / q.Kkm, iKk = 1.0 / q.Kk, iKkp = 1.0 / q.Kkp;
+    double iKkm = rcp<double>(q.Kkm), iKk = rcp<double>(q.Kk), iKkp = rcp<double>(q.Kkp);
     double Ckp = q.vel * q.nCkp, Ck = q.vel * q.nCk, Ckm = q.vel * q.nCkm;
     if (q.recoil) {
         Ckp += q.Kkp * (q.rec0 - 2.0 * q.ICkp);
@@ -182,11 +223,10 @@ __device__ __forceinline__ void ff_fwd(const FfIn &q, double &Fp, double &F0, do
     double Pkm = fmin(fmax(Ckm * rkm, -kPmax), kPmax);
     double oRkp, xRkp, oLk, xLk, oRk, xRk, oLkm, xLkm;
     omphi_R(Pkp, oRkp, xRkp);
-    omphi_L(Pk, oLk, xLk);
-    omphi_R(Pk, oRk, xRk);
+    omphi_LR(Pk, oLk, xLk, oRk, xRk);
     omphi_L(Pkm, oLkm, xLkm);
-    double dkp = q.idn / (xLk * rk - xRkp * rkp);
-    double dkm = q.idn / (xLkm * rkm - xRk * rk);
+    double dkp = q.idn * rcp<double>(xLk * rk - xRkp * rkp);
+    double dkm = q.idn * rcp<double>(xLkm * rkm - xRk * rk);
     Fp = oRkp * dkp;
     Fm = oLkm * dkm;
     F0 = oLk * dkp + oRk * dkm;
@@ -194,7 +234,7 @@ __device__ __forceinline__ void ff_fwd(const FfIn &q, double &Fp, double &F0, do
 
 __device__ __forceinline__ void ff_adj(const FfIn &q, double gFp, double gF0, double gFm, double &gvel, double &gKkm,
                                        double &gKk, double &gKkp, double &grec0) {
-    double iKkm = 1.0 / q.Kkm, iKk = 1.0 / q.Kk, iKkp = 1.0 / q.Kkp;
+    double iKkm = rcp<double>(q.Kkm), iKk = rcp<double>(q.Kk), iKkp = rcp<double>(q.Kkp);
     double Ckp = q.vel * q.nCkp, Ck = q.vel * q.nCk, Ckm = q.vel * q.nCkm;
     const double ekp = q.rec0 - 2.0 * q.ICkp, ek = q.rec0 - 2.0 * q.ICk, ekm = q.rec0 - 2.0 * q.ICkm;
     if (q.recoil) {
@@ -207,26 +247,22 @@ __device__ __forceinline__ void ff_adj(const FfIn &q, double gFp, double gF0, do
     double Pkp = fmin(fmax(Pkp0, -kPmax), kPmax);
     double Pk = fmin(fmax(Pk0, -kPmax), kPmax);
     double Pkm = fmin(fmax(Pkm0, -kPmax), kPmax);
-    double oRkp, xRkp, oLk, xLk, oRk, xRk, oLkm, xLkm;
-    omphi_R(Pkp, oRkp, xRkp);
-    omphi_L(Pk, oLk, xLk);
-    omphi_R(Pk, oRk, xRk);
-    omphi_L(Pkm, oLkm, xLkm);
-    double Dp = xLk * rk - xRkp * rkp, Dm = xLkm * rkm - xRk * rk;
-    double dkp = q.idn / Dp, dkm = q.idn / Dm;
+    const Omphi Rkp = omphi_d<false>(Pkp), Lkm = omphi_d<true>(Pkm);
+    Omphi Lk, Rk;
+    omphi_d_LR(Pk, Lk, Rk);
+    double Dp = Lk.x * rk - Rkp.x * rkp, Dm = Lkm.x * rkm - Rk.x * rk;
+    const double iDp = rcp<double>(Dp), iDm = rcp<double>(Dm);
+    double dkp = q.idn * iDp, dkm = q.idn * iDm;
     // F+ = oR(Pkp) dkp ; F- = oL(Pkm) dkm ; F = oL(Pk) dkp + oR(Pk) dkm
-    double gdkp = gFp * oRkp + gF0 * oLk;
-    double gdkm = gFm * oLkm + gF0 * oRk;
+    double gdkp = gFp * Rkp.o + gF0 * Lk.o;
+    double gdkm = gFm * Lkm.o + gF0 * Rk.o;
     double goRkp = gFp * dkp, goLkm = gFm * dkm, goLk = gF0 * dkp, goRk = gF0 * dkm;
-    double gDp = -gdkp * dkp / Dp, gDm = -gdkm * dkm / Dm;
+    double gDp = -gdkp * dkp * iDp, gDm = -gdkm * dkm * iDm;
     double gxLk = gDp * rk, gxRkp = -gDp * rkp, gxLkm = gDm * rkm, gxRk = -gDm * rk;
-    double grk = gDp * xLk - gDm * xRk, grkp = -gDp * xRkp, grkm = gDm * xLkm;
-    double d_o, d_x;
-    double gPkp = 0.0, gPk = 0.0, gPkm = 0.0;
-    d_omphi_R(Pkp, d_o, d_x); gPkp += goRkp * d_o + gxRkp * d_x;
-    d_omphi_L(Pk, d_o, d_x); gPk += goLk * d_o + gxLk * d_x;
-    d_omphi_R(Pk, d_o, d_x); gPk += goRk * d_o + gxRk * d_x;
-    d_omphi_L(Pkm, d_o, d_x); gPkm += goLkm * d_o + gxLkm * d_x;
+    double grk = gDp * Lk.x - gDm * Rk.x, grkp = -gDp * Rkp.x, grkm = gDm * Lkm.x;
+    double gPkp = goRkp * Rkp.d_o + gxRkp * Rkp.d_x;
+    double gPk = goLk * Lk.d_o + gxLk * Lk.d_x + goRk * Rk.d_o + gxRk * Rk.d_x;
+    double gPkm = goLkm * Lkm.d_o + gxLkm * Lkm.d_x;
     // clamps pass nothing when active
     if (!(Pkp0 > -kPmax && Pkp0 < kPmax)) gPkp = 0.0;
     if (!(Pk0 > -kPmax && Pk0 < kPmax)) gPk = 0.0;
@@ -264,11 +300,26 @@ __global__ void __launch_bounds__(ADJ_THREADS, 2) k_freq_adj(FreqAdjArgs a) {
         for (int m = 0; m < M; m++) {
             int k = lane * M + m;
             bool v = k < nnu;
-            JA[m] = v ? a.J[base + k] : 0.0;
-            HrA[m] = v ? a.Hr[base + k] : 0.0;
-            HZA[m] = v ? a.HZ[base + k] : 0.0;
             Hv[m] = v ? a.Hv[base + k] : 1.0;
             dn[m] = v ? a.dnu[k] : 0.0;
+            if (v && k >= a.kmin && k <= a.kmax) {
+                // x_A from the advection's tape: the second J floor and the causality limiter
+                // of the cell update, as k_advect applies them
+                const double t1 = a.tape[base + k + a.tape_stride];
+                double hr = a.tape[base + k + 2 * a.tape_stride], hz = a.tape[base + k + 3 * a.tape_stride];
+                const double Jn = t1 > jeps ? t1 : jeps;
+                const double H2 = hr * hr + hz * hz;
+                if (H2 > Jn * Jn) {
+                    const double fsc = Jn / sqrt(H2);
+                    hr *= fsc;
+                    hz *= fsc;
+                }
+                JA[m] = Jn; HrA[m] = hr; HZA[m] = hz;
+            } else {
+                JA[m] = v ? a.J[base + k] : 0.0;
+                HrA[m] = v ? a.Hr[base + k] : 0.0;
+                HZA[m] = v ? a.HZ[base + k] : 0.0;
+            }
         }
         // ---- emission / absorption forward, src/ConstantsAndFunctions.jl:526-567 ----
         const double al = a.alpha[c], acv = a.alpha_c[c], pdv = a.pd[c];
@@ -285,10 +336,10 @@ __global__ void __launch_bounds__(ADJ_THREADS, 2) k_freq_adj(FreqAdjArgs a) {
                      : (a.phi ? a.phi[base + k] : ((k >= a.phi_kmin && k <= a.phi_kmax) ? Hv[m] * pinv : 0.0));
             double aabs = acv + al_pd * Hv[m];
             double dJdt = js_ct * phi[m];
-            eden[m] = 1.0 + aabs * c_tilde * dt;
-            J1[m] = (JA[m] + dJdt * dt) / eden[m];
+            eden[m] = rcp<double>(1.0 + aabs * c_tilde * dt);     // held as its reciprocal
+            J1[m] = (JA[m] + dJdt * dt) * eden[m];
             double aH = a.alpha_cF ? al * Hv[m] + acF : al * Hv[m];
-            idn[m] = 1.0 / (1.0 + aH * c_tilde * dt);
+            idn[m] = rcp<double>(1.0 + aH * c_tilde * dt);
             Hr1[m] = HrA[m] * idn[m];
             HZ1[m] = HZA[m] * idn[m];
             if (k < nnu) {
@@ -355,7 +406,8 @@ __global__ void __launch_bounds__(ADJ_THREADS, 2) k_freq_adj(FreqAdjArgs a) {
             double Jn = in ? x[m] : J1[m];
             double Jf = Jn > jeps ? Jn : jeps;
             double Jod = J1[m] > jeps ? J1[m] : jeps;
-            double ratio = Jf * (1.0 / Jod);
+            const double iJod = rcp<double>(Jod);
+            double ratio = Jf * iJod;
             double hr = Hr1[m] * ratio, hz = HZ1[m] * ratio;
             double H2 = hr * hr + hz * hz;
             double gJo = a.gJ[base + k], gHo = a.gHr[base + k], gZo = a.gHZ[base + k];
@@ -374,8 +426,8 @@ __global__ void __launch_bounds__(ADJ_THREADS, 2) k_freq_adj(FreqAdjArgs a) {
             gHr1[m] = ghr * ratio;
             gHZ1[m] = ghz * ratio;
             double gratio = ghr * Hr1[m] + ghz * HZ1[m];
-            gJf += gratio / Jod;
-            if (J1[m] > jeps) gJ1[m] += -gratio * ratio / Jod;
+            gJf += gratio * iJod;
+            if (J1[m] > jeps) gJ1[m] += -gratio * ratio * iJod;
             double gJn = Jn > jeps ? gJf : 0.0;
             if (in) gx[m] = gJn;
             else gJ1[m] += gJn;
@@ -474,16 +526,17 @@ __global__ void __launch_bounds__(ADJ_THREADS, 2) k_freq_adj(FreqAdjArgs a) {
             int k = lane * M + m;
             if (k >= nnu) continue;
             // recover H_A (the arrays were reused for the M_F adjoint)
-            double hrA = Hr1[m] / idn[m], hzA = HZ1[m] / idn[m];
+            const double hden = 1.0 + (a.alpha_cF ? al * Hv[m] + acF : al * Hv[m]) * c_tilde * dt;
+            double hrA = Hr1[m] * hden, hzA = HZ1[m] * hden;
             double gHrA = gHr1[m] * idn[m] + HrA[m];
             double gHZA = gHZ1[m] * idn[m] + HZA[m];
             double gidn = gHr1[m] * hrA + gHZ1[m] * hzA;
             double gaH = -gidn * idn[m] * idn[m] * c_tilde * dt;
             galpha += gaH * Hv[m];
             gHv[m] += gaH * al;
-            double gJA = gJ1[m] / eden[m];
-            double gdJdt = gJ1[m] / eden[m] * dt;
-            double gaabs = -gJ1[m] * J1[m] / eden[m] * c_tilde * dt;
+            double gJA = gJ1[m] * eden[m];
+            double gdJdt = gJ1[m] * eden[m] * dt;
+            double gaabs = -gJ1[m] * J1[m] * eden[m] * c_tilde * dt;
             galpha_c += gaabs;
             galpha += gaabs * pdv * Hv[m];
             gHv[m] += gaabs * al_pd;

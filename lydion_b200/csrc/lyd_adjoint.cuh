@@ -16,8 +16,9 @@ __device__ __forceinline__ double dchi_L84(double f) {
     double s = sqrt(4.0 - 3.0 * f2);
     double den = 5.0 + 2.0 * s;
     double num = 3.0 + 4.0 * f2;
-    double ds = -3.0 * f / s;
-    return (8.0 * f * den - num * 2.0 * ds) / (den * den);
+    double ds = -3.0 * f * rcp<double>(s);
+    const double iden = rcp<double>(den);
+    return (8.0 * f * den - num * 2.0 * ds) * (iden * iden);
 }
 
 __device__ __forceinline__ void adj_minmod(double a, double b, double g, double &ga, double &gb) {
@@ -49,12 +50,13 @@ __device__ __forceinline__ void adj_D_edd(double Hr, double HZ, double J, double
     const double fmin2 = kFmin * kFmin;
     if (J <= jeps || H2 <= heps2 || H2 <= fmin2 * J * J) return;
     double Hm = sqrt(H2);
-    double fr = Hm / J;
+    const double iJ = rcp<double>(J);
+    double fr = Hm * iJ;
     const bool inside = fr > kFmin && fr < kFmax;
     double f = fr < kFmin ? kFmin : (fr > kFmax ? kFmax : fr);
     double chi = chi_L84(f);
     double b = (3.0 * chi - 1.0) * 0.5;
-    double iH = 1.0 / Hm;
+    double iH = rcp<double>(Hm);
     double nr = Hr * iH, nZ = HZ * iH;
     double ga = gDrr + gDZZ;
     double gb = gDrr * nr * nr + gDZZ * nZ * nZ + gDrZ * nr * nZ;
@@ -63,8 +65,8 @@ __device__ __forceinline__ void adj_D_edd(double Hr, double HZ, double J, double
     double gchi = -0.5 * ga + 1.5 * gb;
     double gf = inside ? gchi * dchi_L84(f) : 0.0;
     // f = Hm / J ; n = H / Hm
-    double gHm = gf / J - (gnr * nr + gnZ * nZ) * iH;
-    gJ += -gf * fr / J;
+    double gHm = gf * iJ - (gnr * nr + gnZ * nZ) * iH;
+    gJ += -gf * fr * iJ;
     gHr += gnr * iH + gHm * nr;
     gHZ += gnZ * iH + gHm * nZ;
 }
@@ -125,15 +127,15 @@ __device__ __forceinline__ void recon_fwd(const CellF<double> &cm1, const CellF<
     double frL = t.frL0, fZL = t.fZL0, frR = t.frR0, fZR = t.fZR0;
     double fL = sqrt(frL * frL + fZL * fZL);
     t.fL0 = fL;
-    if (fL > 1.0) { double inv = 1.0 / fL; frL *= inv; fZL *= inv; fL = 1.0; }
+    if (fL > 1.0) { double inv = rcp<double>(fL); frL *= inv; fZL *= inv; fL = 1.0; }
     double fR = sqrt(frR * frR + fZR * fZR);
     t.fR0 = fR;
-    if (fR > 1.0) { double inv = 1.0 / fR; frR *= inv; fZR *= inv; fR = 1.0; }
+    if (fR > 1.0) { double inv = rcp<double>(fR); frR *= inv; fZR *= inv; fR = 1.0; }
     o.Hr_L = frL * o.J_L; o.Hr_R = frR * o.J_R;
     o.HZ_L = fZL * o.J_L; o.HZ_R = fZR * o.J_R;
-    if (fL > 0.0) { double inv = 1.0 / fL; o.nr_L = frL * inv; o.nZ_L = fZL * inv; }
+    if (fL > 0.0) { double inv = rcp<double>(fL); o.nr_L = frL * inv; o.nZ_L = fZL * inv; }
     else { o.nr_L = 0.0; o.nZ_L = 0.0; }
-    if (fR > 0.0) { double inv = 1.0 / fR; o.nr_R = frR * inv; o.nZ_R = fZR * inv; }
+    if (fR > 0.0) { double inv = rcp<double>(fR); o.nr_R = frR * inv; o.nZ_R = fZR * inv; }
     else { o.nr_R = 0.0; o.nZ_R = 0.0; }
     o.f_L = fL; o.f_R = fR;
 }
@@ -147,12 +149,13 @@ __device__ __forceinline__ void adj_side_f(double fr0, double fZ0, double f0, do
     // outputs: H = f_vec * J, n = f_vec / |f_vec|, f = |f_vec| (all after renormalisation)
     double fr = fr0, fZ = fZ0, f = f0;
     const bool ren = f0 > 1.0;
-    if (ren) { fr = fr0 / f0; fZ = fZ0 / f0; f = 1.0; }
+    const double if0 = f0 > 0.0 ? rcp<double>(f0) : 0.0;
+    if (ren) { fr = fr0 * if0; fZ = fZ0 * if0; f = 1.0; }
     gJ += gH_r * fr + gH_Z * fZ;
     double gfr = gH_r * J, gfZ = gH_Z * J;
     double gfm = ren ? 0.0 : gf;                  // after renormalisation |f| is the constant 1
     if (f > 0.0) {
-        double inv = 1.0 / f;
+        double inv = rcp<double>(f);
         double nr = fr * inv, nZ = fZ * inv;
         gfr += gn_r * inv;
         gfZ += gn_Z * inv;
@@ -162,14 +165,14 @@ __device__ __forceinline__ void adj_side_f(double fr0, double fZ0, double f0, do
         // v / |v| with v = (fr0, fZ0): d = (g - u (u . g)) / |v|, u = v / |v|
         double ur = fr, uZ = fZ;
         double dot = ur * gfr + uZ * gfZ;
-        gfr0 += (gfr - ur * dot) / f0;
-        gfZ0 += (gfZ - uZ * dot) / f0;
+        gfr0 += (gfr - ur * dot) * if0;
+        gfZ0 += (gfZ - uZ * dot) * if0;
     } else {
         gfr0 += gfr;
         gfZ0 += gfZ;
         if (f0 > 0.0) {
-            gfr0 += gfm * fr0 / f0;
-            gfZ0 += gfm * fZ0 / f0;
+            gfr0 += gfm * fr0 * if0;
+            gfZ0 += gfm * fZ0 * if0;
         }
     }
 }
@@ -228,7 +231,7 @@ __device__ __forceinline__ void adj_hll_eigen(double f0, double mu0, double gl1,
     double t = 4.0 - 3.0 * f2;
     const bool tpos = t > 0.0;
     double sq = sqrt(tpos ? t : 0.0);
-    double inv_sq = 1.0 / sq;
+    double inv_sq = rcp<double>(sq);
     double g = (2.0 / 3.0) * (4.0 - 3.0 * f2 - sq) + 2.0 * mu2 * (2.0 - f2 - sq);
     const bool gpos = g > 0.0;
     double fac = sqrt(gpos ? g : 0.0);
@@ -284,12 +287,14 @@ __device__ __forceinline__ void adj_face(const CellF<double> cs[4], const double
         double tau = q.tau_L + q.tau_R;
         double num = 0.2 + tau;
         double den = num + tau * tau;
-        double eps = num / den;
+        const double iden = rcp<double>(den);
+        double eps = num * iden;
         double ome = 1.0 - eps;
         const bool tpos = tau > Num<double>::tiny();
         double te = tpos ? tau : Num<double>::tiny();
+        const double ite = rcp<double>(te);
         double Ji = cs[1].J, Jp = cs[2].J;
-        double FJd = -(1.0 / 3.0) * (Jp - Ji) / te;
+        double FJd = -(1.0 / 3.0) * (Jp - Ji) * ite;
         double FJg = 0.5 * (FJ_L + FJ_R) - 0.5 * (q.J_R - q.J_L);
         double he = 0.5 * eps;
         double geps = gF[0] * (FJg - FJd) - 0.5 * (gF[1] * (q.Hr_R - q.Hr_L) + gF[2] * (q.HZ_R - q.HZ_L));
@@ -312,12 +317,12 @@ __device__ __forceinline__ void adj_face(const CellF<double> cs[4], const double
             gDrrL += gDaL; gDrrR += gDaR; gDrZL += gDbL; gDrZR += gDbR;
         }
         // diffusion term
-        double gd = -(1.0 / 3.0) / te * gFJd;
+        double gd = -(1.0 / 3.0) * ite * gFJd;
         gc[2].J += gd;
         gc[1].J -= gd;
-        double gte = gFJd * (1.0 / 3.0) * (Jp - Ji) / (te * te);
+        double gte = gFJd * (1.0 / 3.0) * (Jp - Ji) * (ite * ite);
         double gtau = tpos ? gte : 0.0;
-        gtau += geps * (tau * tau - 2.0 * tau * num) / (den * den);
+        gtau += geps * (tau * tau - 2.0 * tau * num) * (iden * iden);
         g.tau_L += gtau;
         g.tau_R += gtau;
     } else {
@@ -330,12 +335,14 @@ __device__ __forceinline__ void adj_face(const CellF<double> cs[4], const double
         double tau = q.tau_L + q.tau_R;
         double num = 0.2 + tau;
         double den = num + tau * tau;
-        double eps = num / den;
+        const double iden = rcp<double>(den);
+        double eps = num * iden;
         double ome = 1.0 - eps;
         const bool tpos = tau > Num<double>::tiny();
         double te = tpos ? tau : Num<double>::tiny();
+        const double ite = rcp<double>(te);
         double Ji = cs[1].J, Jp = cs[2].J;
-        double FJd = -(1.0 / 3.0) * (Jp - Ji) / te;
+        double FJd = -(1.0 / 3.0) * (Jp - Ji) * ite;
         const double muL = ZDIR ? q.nZ_L : q.nr_L, muR = ZDIR ? q.nZ_R : q.nr_R;
         double l1L, l3L, l1R, l3R;
         hll_eigen<double>(q.f_L, muL, l1L, l3L);
@@ -344,7 +351,7 @@ __device__ __forceinline__ void adj_face(const CellF<double> cs[4], const double
         double SR = fmax(m3, 0.0), SL = fmin(m1, 0.0);
         double dS = SR - SL;
         const bool dpos = dS > Num<double>::tiny();
-        double inv = 1.0 / (dpos ? dS : Num<double>::tiny());
+        double inv = rcp<double>(dpos ? dS : Num<double>::tiny());
         double SRSL = SR * SL;
         double dJ = q.J_R - q.J_L, dHr = q.Hr_R - q.Hr_L, dHZ = q.HZ_R - q.HZ_L;
         double nJ = SR * FJ_L - SL * FJ_R + SRSL * dJ;
@@ -390,12 +397,12 @@ __device__ __forceinline__ void adj_face(const CellF<double> cs[4], const double
             gDrrL += gDaL; gDrrR += gDaR; gDrZL += gDbL; gDrZR += gDbR;
         }
         // diffusion term and the blend weight, as in the GLF branch
-        double gd = -(1.0 / 3.0) / te * gFJd;
+        double gd = -(1.0 / 3.0) * ite * gFJd;
         gc[2].J += gd;
         gc[1].J -= gd;
-        double gte = gFJd * (1.0 / 3.0) * (Jp - Ji) / (te * te);
+        double gte = gFJd * (1.0 / 3.0) * (Jp - Ji) * (ite * ite);
         double gtau = tpos ? gte : 0.0;
-        gtau += geps * (tau * tau - 2.0 * tau * num) / (den * den);
+        gtau += geps * (tau * tau - 2.0 * tau * num) * (iden * iden);
         g.tau_L += gtau;
         g.tau_R += gtau;
     }
@@ -446,7 +453,7 @@ __device__ __forceinline__ void adj_face(const CellF<double> cs[4], const double
 __device__ __forceinline__ void adj_cell_f(double J, double Hr, double HZ, double jeps, const CellF<double> &g,
                                            double &gJ, double &gHr, double &gHZ) {
     const bool jf = J > jeps;
-    double iJ = 1.0 / (jf ? J : jeps);
+    double iJ = rcp<double>(jf ? J : jeps);
     gHr += g.fr * iJ;
     gHZ += g.fZ * iJ;
     gJ += g.J;
@@ -458,17 +465,19 @@ __device__ __forceinline__ void d_omphi_L(double P, double &domp, double &dchi) 
     if (P >= kPmax || P <= -kPmax) { domp = 0.0; dchi = 0.0; return; }
     if (fabs(P) < kPmin) { domp = -1.0 + P; dchi = -0.5; return; }
     double omp = exp(-P);
-    double chi = (1.0 - omp) / P;
+    const double iP = rcp<double>(P);
+    double chi = (1.0 - omp) * iP;
     domp = -omp;
-    dchi = (omp - chi) / P;
+    dchi = (omp - chi) * iP;
 }
 __device__ __forceinline__ void d_omphi_R(double P, double &domp, double &dchi) {
     if (P >= kPmax || P <= -kPmax) { domp = 0.0; dchi = 0.0; return; }
     if (fabs(P) < kPmin) { domp = 1.0 + P; dchi = -0.5; return; }
     double omp = exp(P);
-    double chi = (1.0 - omp) / P;
+    const double iP = rcp<double>(P);
+    double chi = (1.0 - omp) * iP;
     domp = omp;
-    dchi = (-omp - chi) / P;
+    dchi = (-omp - chi) * iP;
 }
 
 }  // namespace lyd

@@ -7,10 +7,15 @@
 
 namespace lyd {
 
-// Frequency step adjoint: forward inputs (the advected state x_A and the per-cell fields),
-// the adjoint of the step's output, and the outputs (adjoint of x_A, accumulated gradients).
+// Frequency step adjoint: forward inputs (the step's input state s_n, the advection tape and
+// the step's active window, from which the advected state x_A is rebuilt, and the per-cell
+// fields), the adjoint of the step's output, and the outputs (adjoint of x_A, accumulated
+// gradients).
 struct FreqAdjArgs {
-    const double *J, *Hr, *HZ;          // x_A
+    const double *J, *Hr, *HZ;          // s_n (x_A outside the step's window)
+    const double *tape;                 // [4][tape_stride] of the step's advection
+    long long tape_stride;
+    int kmin, kmax;                     // the step's active window
     const double *Hv, *phi, *phi_inv;   // phi: explicit profile or nullptr (derived from Hv)
     int phi_kmin, phi_kmax;
     const double *alpha, *alpha_c, *alpha_cF, *pd, *js, *T;

@@ -945,10 +945,12 @@ int lyd_f_esc(lyd_ctx *c, double L_all, int32_t bc_z_bot, double *f) {
 
 // ---- fused static-cloud step -----------------------------------------------------------------
 template <typename S>
-static int enqueue_step(lyd_ctx *c, bool timed) {
+static int enqueue_step(lyd_ctx *c, bool timed, double *tape = nullptr) {
     const int A = c->cur, B = 1 - c->cur;
     AdvArgs<S> aa;
     fill_adv<S>(c, aa, A, B);
+    aa.tape = tape;                    // the adjoint's forward sweep records the advection tape
+    aa.tape_stride = (long long)c->n3;
     FreqArgs<S> fa;
     fill_freq<S>(c, fa, c->set[B][0], c->set[B][1], c->set[B][2], c->set[B][0], c->set[A][0], c->set[A][1],
                  c->set[A][2]);
@@ -1213,9 +1215,21 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     if (!(p->c_tilde > 0.0) || !(p->dt > 0.0) || p->n_steps < 1) return fail(c, LYD_ERR_ARG, "bad step parameters");
     LYD_TRY(need_inputs(c, true, true));
     const int N = p->n_steps;
-    const int K = cfg->checkpoint_every > 0 ? (cfg->checkpoint_every < N ? cfg->checkpoint_every : N) : (N < 100 ? N : 100);
-    const int nseg = (N + K - 1) / K;
     const size_t n3 = c->n3, nc = c->ncell, S = 3 * n3;
+    // checkpoint_every 1, or 0 when every step's state and advection tape fit in free device
+    // memory: the forward sweep keeps them all and the reverse sweep recomputes nothing.
+    // Otherwise a checkpoint every K steps (0: 100) and one recomputation of each segment.
+    bool store_all = cfg->checkpoint_every == 1;
+    if (cfg->checkpoint_every == 0) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) { cudaGetLastError(); fr = 0; }
+        const size_t need = (size_t)N * (S + 4 * n3) * 8 + 16 * S * 8 + ((size_t)2 << 30);
+        store_all = need <= fr + c->adj_ws_bytes;
+    }
+    const int K = store_all ? 1
+                            : (cfg->checkpoint_every > 0 ? (cfg->checkpoint_every < N ? cfg->checkpoint_every : N)
+                                                         : (N < 100 ? N : 100));
+    const int nseg = (N + K - 1) / K;
     const int nr = c->nr[0], nz = c->nz[0], nnu = c->nnu;
     params_all(c, p->c_tilde, p->dt, p->c_tilde * p->dt);
     for (CloudDesc &d : c->desc) d.z_center = p->z_center;
@@ -1230,10 +1244,13 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
         c->hist_cap = N;
         drop_graph(c);
     }
-    // One workspace, kept in the context between calls. It holds: the checkpoints; per step of
-    // one segment the state, the advected state x_A and the advection's tape (recorded while
-    // the segment is recomputed); the adjoints; and the gradient accumulators (zeroed here).
-    const size_t sizes[] = {(size_t)nseg * S * 8, (size_t)K * S * 8, (size_t)K * S * 8, (size_t)K * 4 * n3 * 8,
+    // One workspace, kept in the context between calls. It holds: the checkpoints (every
+    // step's state when all are kept); per step of one segment the state (recomputation only);
+    // the advected state of the step being recomputed; the advection tapes (of every step when
+    // all are kept, else of one segment, recorded while it is recomputed); the adjoints; and
+    // the gradient accumulators (zeroed here).
+    const size_t ntape = store_all ? (size_t)N : (size_t)K;
+    const size_t sizes[] = {(size_t)nseg * S * 8, store_all ? 0 : (size_t)K * S * 8, S * 8, ntape * 4 * n3 * 8,
                             S * 8, S * 8, S * 8, S * 8, n3 * 8, n3 * 8, nc * 8, nc * 8, nc * 8, 5 * nc * 8,
                             c->nrf * 8, c->nzf * 8, S * 8, (size_t)nnu * 8, 2 * (size_t)nnu * (nr + nz + 2 * nr) * 8,
                             (size_t)N * 2 * sizeof(int) + 16, 16};
@@ -1295,7 +1312,7 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     for (int n = 0; n < N; n++) {
         if (n % K == 0) LYD_TRY(copy_state(ck + (size_t)(n / K) * S, c->cur));
         LYD_CU(c, cudaMemcpyAsync(win + 2 * n, c->kwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
-        LYD_TRY(enqueue_step<double>(c, false));
+        LYD_TRY(enqueue_step<double>(c, false, store_all ? segT + (size_t)n * 4 * n3 : nullptr));
     }
     LYD_TRY(copy_state(fin, c->cur));
     LYD_CU(c, cudaMemcpyAsync(finwin, c->kwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
@@ -1335,12 +1352,14 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     const int B = 1 - c->cur;
     for (int g = nseg - 1; g >= 0; g--) {
         const int n0 = g * K, n1 = (n0 + K < N) ? n0 + K : N;
-        tick(0);
-        LYD_TRY(load_state(ck + (size_t)g * S, c->cur));
+        if (!store_all) {
+            tick(0);
+            LYD_TRY(load_state(ck + (size_t)g * S, c->cur));
+        }
         // recompute the segment: advection of s_n in the step's window into x_A with its tape,
         // then (except after the last step) emission + frequency step x_A -> s_{n+1}
-        for (int n = n0; n < n1; n++) {
-            double *sn = seg + (size_t)(n - n0) * S, *xA = segA + (size_t)(n - n0) * S;
+        for (int n = n0; n < n1 && !store_all; n++) {
+            double *sn = seg + (size_t)(n - n0) * S, *xA = segA;
             LYD_TRY(copy_state(sn, c->cur));
             AdvArgs<double> aa;
             fill_adv<double>(c, aa, c->cur, B);
@@ -1360,17 +1379,21 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
             }
             LYD_CU(c, cudaGetLastError());
         }
-        tick(1);
-        tock(0, 1, 1);
+        if (!store_all) {
+            tick(1);
+            tock(0, 1, 1);
+        }
         for (int n = n1 - 1; n >= n0; n--) {
-            const double *sn = seg + (size_t)(n - n0) * S;
-            const double *xA = segA + (size_t)(n - n0) * S, *tape = segT + (size_t)(n - n0) * 4 * n3;
+            const double *sn = store_all ? ck + (size_t)n * S : seg + (size_t)(n - n0) * S;
+            const double *tape = segT + (size_t)(store_all ? n : n - n0) * 4 * n3;
             tick(2);
             tick(3);
             // frequency step adjoint: lambda_{n+1} -> lambda of x_A
             FreqAdjArgs fa;
             memset(&fa, 0, sizeof(fa));
-            fa.J = xA; fa.Hr = xA + n3; fa.HZ = xA + 2 * n3;
+            fa.J = sn; fa.Hr = sn + n3; fa.HZ = sn + 2 * n3;
+            fa.tape = tape; fa.tape_stride = (long long)n3;
+            fa.kmin = hwin[2 * n]; fa.kmax = hwin[2 * n + 1];
             fa.Hv = (const double *)c->Hv;
             fa.phi = c->phi ? (const double *)c->phi : nullptr;
             fa.phi_inv = c->phi_inv; fa.phi_kmin = c->phi_kmin; fa.phi_kmax = c->phi_kmax;
