@@ -10,10 +10,11 @@
 // before the floors and the causality limiter):
 //   k_freq_adj      one warp per cell: E and F forward, then F^T (flux correction, transposed
 //                   tridiagonal solve by the same warp PCR, frequency factors) and E^T
-//   k_adv_adj_cell  one warp per (cell, 32 bins): the cell update's local terms and the
-//                   adjoints of its face-flux sums
-//   k_adv_adj_face  one warp per (face, 32 bins): the adjoint of one face's reconstruction,
-//                   closure and GLF/HLL + upwind flux, scattered onto its four stencil cells
+//   k_adv_adj_cell  one thread per cell-bin: the cell update's local terms and the adjoints
+//                   of its face-flux sums
+//   k_adv_adj_face  one thread per (face, active bin), the step's active bins packed densely
+//                   across the threads: the adjoint of one face's reconstruction, closure and
+//                   GLF/HLL + upwind flux, scattered onto its four stencil cells
 // Scatters use FP64 atomics, so gradients agree run to run to rounding (~1e-15), not bitwise.
 #include <cuda_runtime.h>
 
@@ -29,6 +30,21 @@ constexpr int ADJ_THREADS = 256;
 __device__ __forceinline__ double wsum_d(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Segmented warp sum: the lanes form runs of equal `key` (keys are contiguous runs across the
+// warp). Returns, in the first lane of each run (head), the run's sum; other lanes get partial
+// sums. Every lane of the warp must call it.
+__device__ __forceinline__ double seg_sum(double v, long long key, int lane, bool &head) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double w = __shfl_down_sync(0xffffffffu, v, o);
+        const long long kk = __shfl_down_sync(0xffffffffu, key, o);
+        if (lane + o < 32 && kk == key) v += w;
+    }
+    const long long kp = __shfl_up_sync(0xffffffffu, key, 1);
+    head = lane == 0 || kp != key;
     return v;
 }
 
@@ -616,16 +632,15 @@ __device__ __forceinline__ double alpha_F_at(const AdjAdvArgs &a, int i, int j, 
 }
 
 // Cell update adjoint (src/AdvectJandH.jl:1302-1382 reversed): warp = one cell x 32 bins.
+// One thread per cell-bin, cell-major (a warp may span two or three cells).
 __global__ void __launch_bounds__(ADJ_THREADS) k_adv_adj_cell(AdjAdvArgs a) {
     const int lane = threadIdx.x & 31;
-    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nkb = (a.nnu + 31) / 32;
+    const long long item = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long ncell = (long long)a.nr * a.nz;
-    if (gw >= ncell * nkb) return;
-    const long long c = gw / nkb;
-    const int k = (int)(gw % nkb) * 32 + lane;
-    const int i = (int)(c % a.nr);
-    const bool valid = k < a.nnu;
+    const bool valid = item < ncell * a.nnu;
+    const long long c = valid ? item / a.nnu : -1;
+    const int k = valid ? (int)(item % a.nnu) : 0;
+    const int i = valid ? (int)(c % a.nr) : 0;
     const bool act = valid && k >= a.kmin && k <= a.kmax;
     const long long x = (long long)k + (long long)a.nnu * c;
     double gu[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -679,31 +694,31 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adv_adj_cell(AdjAdvArgs a) {
         a.pJ[x] = gJn0; a.pHr[x] = gHrp; a.pHZ[x] = gHZp;
     }
     (void)i;
+    bool head = false;
 #pragma unroll
-    for (int q = 0; q < 5; q++) gu[q] = wsum_d(gu[q]);
-    if (lane == 0)
+    for (int q = 0; q < 5; q++) gu[q] = seg_sum(gu[q], c, lane, head);
+    if (valid && head)
 #pragma unroll
         for (int q = 0; q < 5; q++)
             if (gu[q] != 0.0) atomicAdd(a.g_u + (size_t)q * ncell + c, gu[q]);
 }
 
-// One face's adjoint: warp = one face x 32 bins. ZDIR false: r faces f = 0..nr of row j;
-// true: Z faces f = 0..nz of column i.
+// One face's adjoint: thread = one face x one active bin. ZDIR false: r faces f = 0..nr of
+// row j; true: Z faces f = 0..nz of column i.
 // 2 CTAs per SM: 1.4x faster than the unconstrained 206-register form.
 template <bool ZDIR, int FLUX>
 __global__ void __launch_bounds__(ADJ_THREADS, 2) k_adv_adj_face(AdjAdvArgs a) {
     const int lane = threadIdx.x & 31;
-    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nkb = (a.nnu + 31) / 32;
+    const long long item = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int nact = a.kmax - a.kmin + 1;          // the step's active bins, packed densely
     const int nr = a.nr, nz = a.nz;
     const long long nfaces = ZDIR ? (long long)nr * (nz + 1) : (long long)(nr + 1) * nz;
-    if (gw >= nfaces * nkb) return;
-    const long long fi = gw / nkb;
-    const int k = (int)(gw % nkb) * 32 + lane;
+    const bool act = nact > 0 && item < nfaces * nact;
+    const long long fi = act ? item / nact : -1;
+    const int k = act ? a.kmin + (int)(item % nact) : 0;
     // r face: fi = f + (nr+1) j ; Z face: fi = i + nr f
-    const int f = ZDIR ? (int)(fi / nr) : (int)(fi % (nr + 1));
-    const int line = ZDIR ? (int)(fi % nr) : (int)(fi / (nr + 1));
-    const bool act = k < a.nnu && k >= a.kmin && k <= a.kmax;
+    const int f = !act ? 0 : (ZDIR ? (int)(fi / nr) : (int)(fi % (nr + 1)));
+    const int line = !act ? 0 : (ZDIR ? (int)(fi % nr) : (int)(fi / (nr + 1)));
     double guc = 0.0;
     if (act) {
         const double ctdt = a.ctdt;
@@ -762,8 +777,9 @@ __global__ void __launch_bounds__(ADJ_THREADS, 2) k_adv_adj_face(AdjAdvArgs a) {
         if (gaFi != 0.0) atomicAdd(a.g_aF + xi, gaFi);
         if (gaFp != 0.0) atomicAdd(a.g_aF + xp, gaFp);
     }
-    guc = wsum_d(guc);
-    if (lane == 0 && guc != 0.0) atomicAdd((ZDIR ? a.g_uZ : a.g_ur) + fi, guc * kInvC);
+    bool head = false;
+    guc = seg_sum(guc, fi, lane, head);
+    if (act && head && guc != 0.0) atomicAdd((ZDIR ? a.g_uZ : a.g_ur) + fi, guc * kInvC);
 }
 
 // ---- seeds and parameter chains --------------------------------------------------------------
@@ -902,11 +918,14 @@ void launch_freq_adj(const FreqAdjArgs &a, int nitems, cudaStream_t st) {
 
 static int warps_grid(long long nwarps) { return (int)((nwarps * 32 + ADJ_THREADS - 1) / ADJ_THREADS); }
 
+static int threads_grid(long long n) { return (int)((n + ADJ_THREADS - 1) / ADJ_THREADS); }
+
 void launch_adv_adj(const AdjAdvArgs &a, cudaStream_t st) {
-    const long long nkb = (a.nnu + 31) / 32;
     const long long ncell = (long long)a.nr * a.nz;
-    k_adv_adj_cell<<<warps_grid(ncell * nkb), ADJ_THREADS, 0, st>>>(a);
-    const int gr = warps_grid((long long)(a.nr + 1) * a.nz * nkb), gz = warps_grid((long long)a.nr * (a.nz + 1) * nkb);
+    k_adv_adj_cell<<<threads_grid(ncell * a.nnu), ADJ_THREADS, 0, st>>>(a);
+    const long long nact = a.kmax - a.kmin + 1;
+    if (nact <= 0) return;
+    const int gr = threads_grid((long long)(a.nr + 1) * a.nz * nact), gz = threads_grid((long long)a.nr * (a.nz + 1) * nact);
     if (a.flux == 0) {
         k_adv_adj_face<false, 0><<<gr, ADJ_THREADS, 0, st>>>(a);
         k_adv_adj_face<true, 0><<<gz, ADJ_THREADS, 0, st>>>(a);

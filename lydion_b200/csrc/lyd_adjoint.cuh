@@ -10,15 +10,17 @@
 
 namespace lyd {
 
-// chi_L84(f) and its derivative, src/M1Closure.jl:28-33
-__device__ __forceinline__ double dchi_L84(double f) {
-    double f2 = f * f;
-    double s = sqrt(4.0 - 3.0 * f2);
-    double den = 5.0 + 2.0 * s;
-    double num = 3.0 + 4.0 * f2;
-    double ds = -3.0 * f * rcp<double>(s);
+// chi_L84(f) and its derivative together, src/M1Closure.jl:28-33: chi = (3 + 4f^2) / (5 + 2s),
+// s = sqrt(4 - 3f^2), chi' = (8f (5 + 2s) + 6 (3 + 4f^2) f / s) / (5 + 2s)^2; chi is formed as
+// chi_L84 forms it.
+__device__ __forceinline__ void chi_dchi_L84(double f, double &chi, double &dchi) {
+    const double f2 = f * f;
+    const double s = sqrt(4.0 - 3.0 * f2);
+    const double den = 5.0 + 2.0 * s;
+    const double num = 3.0 + 4.0 * f2;
     const double iden = rcp<double>(den);
-    return (8.0 * f * den - num * 2.0 * ds) * (iden * iden);
+    chi = num * iden;
+    dchi = (8.0 * f * den + 6.0 * num * f * rcp<double>(s)) * (iden * iden);
 }
 
 __device__ __forceinline__ void adj_minmod(double a, double b, double g, double &ga, double &gb) {
@@ -33,14 +35,15 @@ __device__ __forceinline__ void adj_D_from_f_n(double f, double nr, double nZ, d
     if (!(f > kFmin)) return;
     const bool clamped = !(f < kFmax);
     double fc = clamped ? kFmax : f;
-    double chi = chi_L84(fc);
+    double chi, dchi;
+    chi_dchi_L84(fc, chi, dchi);
     double b = (3.0 * chi - 1.0) * 0.5;
     double ga = gDrr + gDZZ;
     double gb = gDrr * nr * nr + gDZZ * nZ * nZ + gDrZ * nr * nZ;
     gnr += 2.0 * b * nr * gDrr + b * nZ * gDrZ;
     gnZ += 2.0 * b * nZ * gDZZ + b * nr * gDrZ;
     double gchi = -0.5 * ga + 1.5 * gb;
-    if (!clamped) gf += gchi * dchi_L84(fc);
+    if (!clamped) gf += gchi * dchi;
 }
 
 // Compute_D_Edd (src/M1Closure.jl:46-83): (Hr, HZ, J) -> (Drr, DZZ, DrZ)
@@ -54,7 +57,8 @@ __device__ __forceinline__ void adj_D_edd(double Hr, double HZ, double J, double
     double fr = Hm * iJ;
     const bool inside = fr > kFmin && fr < kFmax;
     double f = fr < kFmin ? kFmin : (fr > kFmax ? kFmax : fr);
-    double chi = chi_L84(f);
+    double chi, dchi;
+    chi_dchi_L84(f, chi, dchi);
     double b = (3.0 * chi - 1.0) * 0.5;
     double iH = rcp<double>(Hm);
     double nr = Hr * iH, nZ = HZ * iH;
@@ -63,7 +67,7 @@ __device__ __forceinline__ void adj_D_edd(double Hr, double HZ, double J, double
     double gnr = 2.0 * b * nr * gDrr + b * nZ * gDrZ;
     double gnZ = 2.0 * b * nZ * gDZZ + b * nr * gDrZ;
     double gchi = -0.5 * ga + 1.5 * gb;
-    double gf = inside ? gchi * dchi_L84(f) : 0.0;
+    double gf = inside ? gchi * dchi : 0.0;
     // f = Hm / J ; n = H / Hm
     double gHm = gf * iJ - (gnr * nr + gnZ * nZ) * iH;
     gJ += -gf * fr * iJ;

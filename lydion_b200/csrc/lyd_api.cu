@@ -945,15 +945,23 @@ int lyd_f_esc(lyd_ctx *c, double L_all, int32_t bc_z_bot, double *f) {
 
 // ---- fused static-cloud step -----------------------------------------------------------------
 template <typename S>
-static int enqueue_step(lyd_ctx *c, bool timed, double *tape = nullptr) {
+// One step from set[cur] back into set[cur] (x_A in the other set). The adjoint's forward sweep
+// passes `tape` to record the advection's tape, and `in` / `out` (three fields each, n3 apart)
+// to read s_n from and write s_{n+1} into its own storage instead.
+static int enqueue_step(lyd_ctx *c, bool timed, double *tape = nullptr, const S *in = nullptr, S *out = nullptr) {
     const int A = c->cur, B = 1 - c->cur;
     AdvArgs<S> aa;
     fill_adv<S>(c, aa, A, B);
-    aa.tape = tape;                    // the adjoint's forward sweep records the advection tape
+    aa.tape = tape;
     aa.tape_stride = (long long)c->n3;
+    if (in) { aa.J = in; aa.Hr = in + c->n3; aa.HZ = in + 2 * c->n3; }
     FreqArgs<S> fa;
-    fill_freq<S>(c, fa, c->set[B][0], c->set[B][1], c->set[B][2], c->set[B][0], c->set[A][0], c->set[A][1],
-                 c->set[A][2]);
+    if (out)
+        fill_freq<S>(c, fa, c->set[B][0], c->set[B][1], c->set[B][2], c->set[B][0], out, out + c->n3,
+                     out + 2 * c->n3);
+    else
+        fill_freq<S>(c, fa, c->set[B][0], c->set[B][1], c->set[B][2], c->set[B][0], c->set[A][0], c->set[A][1],
+                     c->set[A][2]);
     fa.do_emission = 1; fa.do_freq = 1; fa.update_ff = 1;
     fa.parts = PART_ACTIVE | PART_DIAG;
     fa.f_r = c->cellf[CF_F_R]; fa.f_Z = c->cellf[CF_F_Z];
@@ -1309,10 +1317,21 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_R], 0, nc * 8, c->st));
     LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_Z], 0, nc * 8, c->st));
     if (!c->active_valid) LYD_TRY(run_find_active(c));
-    for (int n = 0; n < N; n++) {
-        if (n % K == 0) LYD_TRY(copy_state(ck + (size_t)(n / K) * S, c->cur));
-        LYD_CU(c, cudaMemcpyAsync(win + 2 * n, c->kwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
-        LYD_TRY(enqueue_step<double>(c, false, store_all ? segT + (size_t)n * 4 * n3 : nullptr));
+    if (store_all) {
+        // every state lives in the checkpoint storage: step n reads slot n and writes slot n + 1
+        // (the last step writes the context's state)
+        LYD_TRY(copy_state(ck, c->cur));
+        for (int n = 0; n < N; n++) {
+            LYD_CU(c, cudaMemcpyAsync(win + 2 * n, c->kwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+            double *out = n + 1 < N ? ck + (size_t)(n + 1) * S : nullptr;
+            LYD_TRY(enqueue_step<double>(c, false, segT + (size_t)n * 4 * n3, ck + (size_t)n * S, out));
+        }
+    } else {
+        for (int n = 0; n < N; n++) {
+            if (n % K == 0) LYD_TRY(copy_state(ck + (size_t)(n / K) * S, c->cur));
+            LYD_CU(c, cudaMemcpyAsync(win + 2 * n, c->kwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+            LYD_TRY(enqueue_step<double>(c, false));
+        }
     }
     LYD_TRY(copy_state(fin, c->cur));
     LYD_CU(c, cudaMemcpyAsync(finwin, c->kwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
