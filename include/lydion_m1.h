@@ -238,8 +238,9 @@ int  lyd_get_tuning(lyd_ctx *ctx, lyd_tuning *t);
 /* Gradients of  objective = w_MF * M_F(last step) + sum_k w_spec[k] * S_k(final J)  over
  * n_steps static-driver steps from the current state, S being the edge-ring mean spectrum of
  * lyd_edge_spectra. With checkpoint_every = 1, or 0 when they fit in free device memory
- * (7 * n_nu*n_r*n_z doubles per step), the forward sweep keeps every step's state and
- * advection tape and nothing is recomputed; with checkpoint_every = K > 1 (0 otherwise: 100)
+ * (7 doubles per cell-bin per step), the forward sweep keeps every step's state and advection
+ * tape, plus its frequency factors when 10 doubles per cell-bin per step fit, and nothing is
+ * recomputed; with checkpoint_every = K > 1 (0 otherwise: 100)
  * it stores the state every K steps and the reverse sweep recomputes each segment once. The
  * reverse sweep runs hand-written adjoint kernels of the step (advection, emission/absorption,
  * frequency factors, transposed tridiagonal solve, flux correction). The active window of every step is the forward's.

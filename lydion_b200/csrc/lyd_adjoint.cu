@@ -389,13 +389,19 @@ __global__ void __launch_bounds__(ADJ_THREADS, 2) k_freq_adj(FreqAdjArgs a) {
                 double Drr, DZZ, DrZ;
                 D_edd<double>(Hr1[m], HZ1[m], J1[m], jeps, a.heps2, Drr, DZZ, DrZ);
                 vel[m] = d_colon_grad_u<double>(Drr, DrZ, DZZ, gu0, gu1, gu2, gu3, gu4) * kInvC;
-                FfIn q;
-                q.vel = vel[m]; q.Kkm = Km[m]; q.Kk = Kb[m]; q.Kkp = Kp[m];
-                q.nCkm = a.nuC[k - 1]; q.nCk = a.nuC[k]; q.nCkp = a.nuC[k + 1];
-                q.ICkm = a.inv_nuC[k - 1]; q.ICk = a.inv_nuC[k]; q.ICkp = a.inv_nuC[k + 1];
-                q.DNKM = a.nu[k] - a.nuC[k - 1]; q.DNK = a.nu[k + 1] - a.nuC[k]; q.DNKP = a.nuC[k + 1] - a.nu[k + 1];
-                q.idn = a.inv_dnu[k]; q.rec0 = rec0; q.recoil = a.recoil;
-                ff_fwd(q, Fp[m], F0[m], Fm[m]);
+                if (a.Fkp) {
+                    // the factors the forward sweep stored
+                    Fp[m] = a.Fkp[base + k]; F0[m] = a.Fk[base + k]; Fm[m] = a.Fkm[base + k];
+                } else {
+                    FfIn q;
+                    q.vel = vel[m]; q.Kkm = Km[m]; q.Kk = Kb[m]; q.Kkp = Kp[m];
+                    q.nCkm = a.nuC[k - 1]; q.nCk = a.nuC[k]; q.nCkp = a.nuC[k + 1];
+                    q.ICkm = a.inv_nuC[k - 1]; q.ICk = a.inv_nuC[k]; q.ICkp = a.inv_nuC[k + 1];
+                    q.DNKM = a.nu[k] - a.nuC[k - 1]; q.DNK = a.nu[k + 1] - a.nuC[k];
+                    q.DNKP = a.nuC[k + 1] - a.nu[k + 1];
+                    q.idn = a.inv_dnu[k]; q.rec0 = rec0; q.recoil = a.recoil;
+                    ff_fwd(q, Fp[m], F0[m], Fm[m]);
+                }
             }
             bool in = (k >= 1 && k <= nnu - 2);
             sys.a[m] = (in && k >= 2) ? Fm[m] : 0.0;

@@ -16,6 +16,7 @@ struct FreqAdjArgs {
     const double *tape;                 // [4][tape_stride] of the step's advection
     long long tape_stride;
     int kmin, kmax;                     // the step's active window
+    const double *Fkp, *Fk, *Fkm;       // the step's frequency factors, or nullptr: recomputed
     const double *Hv, *phi, *phi_inv;   // phi: explicit profile or nullptr (derived from Hv)
     int phi_kmin, phi_kmax;
     const double *alpha, *alpha_c, *alpha_cF, *pd, *js, *T;

@@ -946,9 +946,11 @@ int lyd_f_esc(lyd_ctx *c, double L_all, int32_t bc_z_bot, double *f) {
 // ---- fused static-cloud step -----------------------------------------------------------------
 template <typename S>
 // One step from set[cur] back into set[cur] (x_A in the other set). The adjoint's forward sweep
-// passes `tape` to record the advection's tape, and `in` / `out` (three fields each, n3 apart)
-// to read s_n from and write s_{n+1} into its own storage instead.
-static int enqueue_step(lyd_ctx *c, bool timed, double *tape = nullptr, const S *in = nullptr, S *out = nullptr) {
+// passes `tape` to record the advection's tape, `in` / `out` (three fields each, n3 apart) to
+// read s_n from and write s_{n+1} into its own storage instead, and `ff` to keep the frequency
+// factors F+, F, F- (n3 apart).
+static int enqueue_step(lyd_ctx *c, bool timed, double *tape = nullptr, const S *in = nullptr, S *out = nullptr,
+                        double *ff = nullptr) {
     const int A = c->cur, B = 1 - c->cur;
     AdvArgs<S> aa;
     fill_adv<S>(c, aa, A, B);
@@ -965,6 +967,7 @@ static int enqueue_step(lyd_ctx *c, bool timed, double *tape = nullptr, const S 
     fa.do_emission = 1; fa.do_freq = 1; fa.update_ff = 1;
     fa.parts = PART_ACTIVE | PART_DIAG;
     fa.f_r = c->cellf[CF_F_R]; fa.f_Z = c->cellf[CF_F_Z];
+    if (ff) { fa.Fkp = ff; fa.Fk = ff + c->n3; fa.Fkm = ff + 2 * c->n3; }
     RedArgs ra = red_args(c, PART_ACTIVE | PART_DIAG);
     ra.diag = c->hist; ra.step_counter = c->step_ctr; ra.done = c->step_ctr + 1; ra.hist_capacity = c->hist_cap;
     const int prec = c->prec;
@@ -1227,13 +1230,14 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     // checkpoint_every 1, or 0 when every step's state and advection tape fit in free device
     // memory: the forward sweep keeps them all and the reverse sweep recomputes nothing.
     // Otherwise a checkpoint every K steps (0: 100) and one recomputation of each segment.
+    // When there is room, every step's frequency factors are kept too (3 more doubles per
+    // cell-bin), and the frequency-step adjoint reads them instead of recomputing them.
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) { cudaGetLastError(); fr = 0; }
+    const size_t avail = fr + c->adj_ws_bytes, margin = 16 * S * 8 + ((size_t)2 << 30);
     bool store_all = cfg->checkpoint_every == 1;
-    if (cfg->checkpoint_every == 0) {
-        size_t fr = 0, tot = 0;
-        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) { cudaGetLastError(); fr = 0; }
-        const size_t need = (size_t)N * (S + 4 * n3) * 8 + 16 * S * 8 + ((size_t)2 << 30);
-        store_all = need <= fr + c->adj_ws_bytes;
-    }
+    if (cfg->checkpoint_every == 0) store_all = (size_t)N * (S + 4 * n3) * 8 + margin <= avail;
+    const bool keep_ff = store_all && (size_t)N * (S + 7 * n3) * 8 + margin <= avail;
     const int K = store_all ? 1
                             : (cfg->checkpoint_every > 0 ? (cfg->checkpoint_every < N ? cfg->checkpoint_every : N)
                                                          : (N < 100 ? N : 100));
@@ -1261,7 +1265,7 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     const size_t sizes[] = {(size_t)nseg * S * 8, store_all ? 0 : (size_t)K * S * 8, S * 8, ntape * 4 * n3 * 8,
                             S * 8, S * 8, S * 8, S * 8, n3 * 8, n3 * 8, nc * 8, nc * 8, nc * 8, 5 * nc * 8,
                             c->nrf * 8, c->nzf * 8, S * 8, (size_t)nnu * 8, 2 * (size_t)nnu * (nr + nz + 2 * nr) * 8,
-                            (size_t)N * 2 * sizeof(int) + 16, 16};
+                            (size_t)N * 2 * sizeof(int) + 16, 16, keep_ff ? (size_t)N * 3 * n3 * 8 : 0};
     constexpr int NB = sizeof(sizes) / sizeof(sizes[0]);
     size_t offs[NB], total = 0;
     for (int q = 0; q < NB; q++) {
@@ -1287,6 +1291,7 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     double *g_ur = W_(14), *g_uZ = W_(15), *fin = W_(16), *wsp = W_(17), *edge = W_(18);
     int *win = reinterpret_cast<int *>(W_(19));
     int *finwin = reinterpret_cast<int *>(W_(20));
+    double *ffs = keep_ff ? W_(21) : nullptr;
     // lambda and the accumulators start at zero (buffers 4 and 8..15 are contiguous in order)
     LYD_CU(c, cudaMemsetAsync(lam, 0, S * 8, c->st));
     LYD_CU(c, cudaMemsetAsync(gaF, 0, offs[16] - offs[8], c->st));
@@ -1324,7 +1329,8 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
         for (int n = 0; n < N; n++) {
             LYD_CU(c, cudaMemcpyAsync(win + 2 * n, c->kwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
             double *out = n + 1 < N ? ck + (size_t)(n + 1) * S : nullptr;
-            LYD_TRY(enqueue_step<double>(c, false, segT + (size_t)n * 4 * n3, ck + (size_t)n * S, out));
+            LYD_TRY(enqueue_step<double>(c, false, segT + (size_t)n * 4 * n3, ck + (size_t)n * S, out,
+                                         ffs ? ffs + (size_t)n * 3 * n3 : nullptr));
         }
     } else {
         for (int n = 0; n < N; n++) {
@@ -1413,6 +1419,11 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
             fa.J = sn; fa.Hr = sn + n3; fa.HZ = sn + 2 * n3;
             fa.tape = tape; fa.tape_stride = (long long)n3;
             fa.kmin = hwin[2 * n]; fa.kmax = hwin[2 * n + 1];
+            if (ffs) {
+                fa.Fkp = ffs + (size_t)n * 3 * n3;
+                fa.Fk = fa.Fkp + n3;
+                fa.Fkm = fa.Fkp + 2 * n3;
+            }
             fa.Hv = (const double *)c->Hv;
             fa.phi = c->phi ? (const double *)c->phi : nullptr;
             fa.phi_inv = c->phi_inv; fa.phi_kmin = c->phi_kmin; fa.phi_kmax = c->phi_kmax;
