@@ -51,10 +51,15 @@ def measured_peaks():
 
 def profile_traffic(kernel, precision):
     """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+    return profile_figure(kernel, precision, "dram_bytes_per_launch")
+
+
+def profile_figure(kernel, precision, key):
+    """A `key: value` figure of the committed ncu summary of `kernel`, or None."""
     path = os.path.join(ROOT, "profiles", f"{kernel}_c2_{precision}.md")
     if not os.path.exists(path):
         return None
-    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    m = re.search(key + r":\s*([0-9.eE+]+)", open(path).read())
     return float(m.group(1)) if m else None
 
 
@@ -205,8 +210,11 @@ def measure_form(cloud, prec, args, barrier, stream_of, local, world, clk=None):
     ctx.synchronize()
     kms = ctx.timing() / kt
     ctx.set_timing(False)
+    # the active window of the advection over 50 further steps (the work unit counts every bin)
+    h = ctx.static_steps(50, *p, history=True)
+    active = float(np.mean((h[:, 6] - h[:, 5] + 1) / cloud.n_nu))
     return ctx, {"value": value, "ms_per_step": ms_max / args.steps, "kernel_ms": kms, "tuning": list(tuning),
-                 "clocks": clocks}
+                 "clocks": clocks, "active_fraction": active}
 
 
 def e2e_form(ctx, cloud, args, barrier, stream_of, world):
@@ -401,7 +409,10 @@ def run_gpu(args):
                              "peak": peaks["hbm_gbs"], "peak_source": src, "unit": "GB/s",
                              "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                              "algorithmic_bytes_per_launch": ab, "ms_per_launch": float(kms[dom]),
-                             "kernel_ms_per_step": {n: float(v) for n, v in zip(names, kms)}},
+                             "kernel_ms_per_step": {n: float(v) for n, v in zip(names, kms)},
+                             "ncu_fp64_pipe_pct": profile_figure("k_" + names[dom], variant, "fp64_pipe_pct"),
+                             "ncu_fma_pipe_pct": profile_figure("k_" + names[dom], variant, "fma_pipe_pct")},
+                "active_fraction": mix["active_fraction"],
                 "cpu_baseline": cpu,
                 "e2e": e2e,
                 "gpu_launches": 3 * args.steps,
