@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define LYD_ABI_VERSION 2
+#define LYD_ABI_VERSION 3
 
 /* status codes */
 #define LYD_OK              0
@@ -109,6 +109,7 @@ enum lyd_field {
     LYD_F_ALPHA = 16, LYD_F_ALPHA_C = 17, LYD_F_ALPHA_CF = 18, LYD_F_PD = 19, LYD_F_JS = 20,
     LYD_F_T = 21, LYD_F_DUR_DR = 22, LYD_F_DUR_DZ = 23, LYD_F_DUZ_DR = 24, LYD_F_DUZ_DZ = 25,
     LYD_F_UR_OVER_R = 26, LYD_F_DRU_R = 27, LYD_F_DRU_Z = 28, LYD_F_F_R = 29, LYD_F_F_Z = 30,
+    LYD_F_E_LYA = 31,     /* e_Lya, the Lya energy density of the RHD sub-cycle (erg cm^-3) */
     /* faces */
     LYD_F_U_R_STAR = 40,  /* (n_r+1, n_z) */
     LYD_F_U_Z_STAR = 41   /* (n_r, n_z+1) */
@@ -293,6 +294,47 @@ int  lyd_cfl_dt(lyd_ctx *ctx, double c_tilde, const double *u_r, const double *u
  * n_edge = (n_z-2) + 2*(n_r-3) cells; raw and normalised are (n_edge, n_nu) row-major. */
 int  lyd_edge_count(int32_t n_r, int32_t n_z);
 int  lyd_edge_spectra(lyd_ctx *ctx, double *raw, double *norm, int32_t *r_index, int32_t *z_index);
+/* ---- RHD-side Lyman-alpha block ---------------------------------------------------------------
+ * The Lya part of the per-cell photo-thermochemistry sub-cycle of the RHD drivers, on the device
+ * for every cell of the context at once, so that an RHD code whose chemistry runs on the GPU
+ * never copies J and H to the host between transport steps. */
+typedef struct lyd_dust_lya {
+    double kappa_abs[3];   /* Lya absorption opacity per dust mass, Sil / C / PAH (cm^2 g^-1)  */
+    double kappa_F[3];     /* Lya flux (absorption + scattering) opacity per dust mass         */
+    double rho_ignore;     /* dust densities at or below this are ignored (rho_d_IGNORE)       */
+} lyd_dust_lya;
+/* PrepareLyaSubCycling!, src/PhotoChemistryAndCooling/PhotoThermoChemistry.jl:2087-2155, for
+ * every cell: T and the species number densities (cm^-3) and the three dust mass densities
+ * rho_d[3][n_r*n_z] (g cm^-3) are host arrays. Sets T; H_voigt (lyd_update_hvoigt) and phi_nu
+ * normalised over all bins (Update_Hvoigt_And_phinu_cell!, :2039-2080); alpha = nHI sigma0(T);
+ * alpha_c (dust and gas continuum absorption); alpha_cF (dust and gas continuum flux opacity,
+ * so that alpha_F = alpha H_voigt + alpha_cF); pd (pd_Lya when destruction != 0, else 0); and
+ * js = recombination (Case B if ots, else Case A) + collisional emissivity
+ * (src/LymanAlphaEmission.jl:106-175). */
+int  lyd_rhd_lya_prepare(lyd_ctx *ctx, const double *T, const double *nHI, const double *nH2, const double *nHII,
+                         const double *nHeI, const double *ne, const double *nOHx, const double *nCHx,
+                         const double *rho_d, const lyd_dust_lya *dust, double z, int32_t ots,
+                         int32_t destruction);
+/* Per-cell results of lyd_rhd_lya_absorb, host arrays of n_r*n_z (split: 8 per cell,
+ * split[q*n_r*n_z + cell] for q = gas r, gas Z, Sil r, Sil Z, C r, C Z, PAH r, PAH Z); any may be
+ * NULL. */
+typedef struct lyd_rhd_lya_out {
+    int32_t *reject;       /* 1 where the sub-step is rejected                                    */
+    double *de;            /* |e_new - e_Lya| / (e_Lya + e_floor)                                 */
+    double *e_new;         /* 4 pi / c sum_k dnu_k J_k after the sub-step (erg cm^-3)             */
+    double *dru_r, *dru_Z; /* radiation momentum of the sub-step (g cm^-2 s^-1)                   */
+    double *split;         /* its split between gas and the three dust kinds (SplitRadPressure)   */
+    double *dt_lya;        /* the absorption time 1 / (c~ (alpha_c + pd alpha)) (s)               */
+} lyd_rhd_lya_out;
+/* The Lya block of AbsorptionStep, src/PhotoChemistryAndCooling/PhotoThermoChemistry.jl:
+ * 1580-1680, for every cell over its own sub-step dt[cell] (host array, s): J = max((J_old +
+ * dt c~ js phi)/(1 + (alpha_c + pd alpha H_voigt) c~ dt), Jeps), H = H_old/(1 + alpha_F c~ dt),
+ * the momentum and its split, e_new and the rejection test (relative change of e_Lya above 0.1
+ * while dt exceeds 0.1 of the absorption time, or not finite). J and H are written for every
+ * cell. With commit != 0, accepted cells then take J_old = J, H_old = H and e_Lya = e_new
+ * (:3197-3206) and rejected cells get J = J_old, H = H_old back (RestoreLyaRejection, :980-991). */
+int  lyd_rhd_lya_absorb(lyd_ctx *ctx, const double *dt, double c_tilde, int32_t commit, lyd_rhd_lya_out *out);
+
 /* The five Voigt look-up tables the device evaluates (CreateVoigtLUTs,
  * src/FastInterpolations.jl:178-197): erf, Dawson's integral, exp(-x^2), x exp(-x^2) and
  * (1-2x^2) exp(-x^2) at x_i = -xmax + 2 xmax i/(n-1), written to out[5*n] table after table.

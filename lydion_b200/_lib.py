@@ -16,7 +16,7 @@ PREC_FP64, PREC_MIXED, PREC_FP32 = 0, 1, 2
 
 F = dict(J=0, J_old=1, H_r=2, H_Z=3, H_r_old=4, H_Z_old=5, Hvoigt=6, phi_nu=7, alpha_F=8,
          alpha=16, alpha_c=17, alpha_cF=18, pd=19, js=20, T=21, dur_dr=22, dur_dZ=23, duZ_dr=24, duZ_dZ=25,
-         ur_over_r=26, dru_r=27, dru_Z=28, f_r=29, f_Z=30, u_r_star=40, u_Z_star=41)
+         ur_over_r=26, dru_r=27, dru_Z=28, f_r=29, f_Z=30, e_Lya=31, u_r_star=40, u_Z_star=41)
 
 P = C.POINTER(C.c_double)
 
@@ -77,6 +77,15 @@ class AdjointCfg(C.Structure):
                 ("w_spec", P)]
 
 
+class DustLya(C.Structure):
+    _fields_ = [("kappa_abs", C.c_double * 3), ("kappa_F", C.c_double * 3), ("rho_ignore", C.c_double)]
+
+
+class RhdLyaOut(C.Structure):
+    _fields_ = [("reject", C.POINTER(C.c_int32)), ("de", P), ("e_new", P), ("dru_r", P), ("dru_Z", P),
+                ("split", P), ("dt_lya", P)]
+
+
 class AdjointOut(C.Structure):
     _fields_ = [("objective", P), ("M_F", P), ("spectrum", P), ("grad_alpha", P), ("grad_alpha_c", P), ("grad_T", P),
                 ("grad_Hv", P), ("grad_u_r_star", P), ("grad_u_Z_star", P), ("grad_du", P * 5), ("grad_J0", P),
@@ -122,6 +131,8 @@ SIGNATURES = {
     "lyd_update_hvoigt": (C.c_int, [VP]),
     "lyd_update_phi_nu": (C.c_int, [VP, I32, I32]),
     "lyd_pd_lya": (C.c_int, [VP, SZ, P, P, P, P, P, P, D, P]),
+    "lyd_rhd_lya_prepare": (C.c_int, [VP, P, P, P, P, P, P, P, P, P, C.POINTER(DustLya), D, I32, I32]),
+    "lyd_rhd_lya_absorb": (C.c_int, [VP, P, D, I32, C.POINTER(RhdLyaOut)]),
     "lyd_cfl_dt": (C.c_int, [VP, D, P, P, D, P]),
     "lyd_edge_count": (C.c_int, [I32, I32]),
     "lyd_edge_spectra": (C.c_int, [VP, P, P, C.POINTER(I32), C.POINTER(I32)]),

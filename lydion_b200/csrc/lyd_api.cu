@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "lyd_adjoint.h"
@@ -38,7 +39,7 @@ constexpr int kDefaultRows = 16;
 
 // per-cloud "was provided" bits: per-cell fields use their index (field - LYD_F_ALPHA)
 enum { CF_ALPHA = 0, CF_ALPHA_C, CF_ALPHA_CF, CF_PD, CF_JS, CF_T, CF_DUR_DR, CF_DUR_DZ, CF_DUZ_DR, CF_DUZ_DZ,
-       CF_UR_OVER_R, CF_DRU_R, CF_DRU_Z, CF_F_R, CF_F_Z, CF_N };
+       CF_UR_OVER_R, CF_DRU_R, CF_DRU_Z, CF_F_R, CF_F_Z, CF_E_LYA, CF_N };
 enum : unsigned { BIT_HV = 1u << 16, BIT_PHI = 1u << 17, BIT_AF = 1u << 18, BIT_GEOM = 1u << 19 };
 }  // namespace
 
@@ -70,6 +71,8 @@ struct lyd_ctx {
     double *Ff[3] = {nullptr, nullptr, nullptr};
     bool ff_valid = false;
     double *cellf[CF_N] = {};
+    double *dust_F = nullptr;      // [3][ncell] dust flux opacities of the RHD Lya block (set by
+                                   // lyd_rhd_lya_prepare)
     double *u_r_star = nullptr, *u_Z_star = nullptr;
     double *dV = nullptr, *inv_dV = nullptr, *A_r = nullptr, *A_Z = nullptr, *inv_r_cell = nullptr;
     double *rCoM = nullptr, *ZCoM = nullptr, *rint = nullptr, *zint = nullptr, *r_if = nullptr, *Z_if = nullptr;
@@ -347,6 +350,7 @@ int lyd_destroy(lyd_ctx *c) {
                   c->last, c->err, c->lut, c->stage, c->small, c->cl, c->tiles, c->items, c->adj_ws};
     for (void *p : ps) cudaFree(p);
     for (int q = 0; q < CF_N; q++) cudaFree(c->cellf[q]);
+    cudaFree(c->dust_F);
     for (int q = 0; q < 8; q++)
         if (c->ev[q]) cudaEventDestroy(c->ev[q]);
     if (c->st) cudaStreamDestroy(c->st);
@@ -517,7 +521,7 @@ static int upload_field(lyd_ctx *c, int q, int32_t field, const double *host, si
         if (!*p) LYD_TRY(dalloc(c, p, c->n3 * c->ssz));
         LYD_TRY(upload3(c, at(*p, d.o3, c->ssz), host, n3, 1.0));
         mark(field == LYD_F_PHI_NU ? BIT_PHI : BIT_AF);
-    } else if (field >= LYD_F_ALPHA && field <= LYD_F_F_Z) {
+    } else if (field >= LYD_F_ALPHA && field <= LYD_F_E_LYA) {
         if (count != nc) return fail(c, LYD_ERR_ARG, "wrong element count for a per-cell field");
         int k = field - LYD_F_ALPHA;
         LYD_TRY(h2d(c, c->cellf[k] + d.oc, host, nc));
@@ -560,7 +564,7 @@ static int download_field(lyd_ctx *c, int q, int32_t field, double *host, size_t
         src = field == LYD_F_PHI_NU ? c->phi : c->aF;
         if (!src) return fail(c, LYD_ERR_STATE, "field is derived on the device and was never uploaded");
         n = n3; is3 = true;
-    } else if (field >= LYD_F_ALPHA && field <= LYD_F_F_Z) {
+    } else if (field >= LYD_F_ALPHA && field <= LYD_F_E_LYA) {
         src = c->cellf[field - LYD_F_ALPHA] + d.oc; n = nc;
     } else if (field == LYD_F_U_R_STAR) {
         src = c->u_r_star + d.orf; n = one ? (size_t)(d.nr + 1) * d.nz : c->nrf;
@@ -1125,6 +1129,94 @@ int lyd_update_phi_nu(lyd_ctx *c, int32_t kmin, int32_t kmax) {
     c->phi = nullptr;
     for (unsigned &h : c->have) h &= ~BIT_PHI;
     c->phi_inv_ready = true;
+    return check_err(c);
+}
+
+// ---- RHD-side Lyman-alpha block ---------------------------------------------------------------
+int lyd_rhd_lya_prepare(lyd_ctx *c, const double *T, const double *nHI, const double *nH2, const double *nHII,
+                        const double *nHeI, const double *ne, const double *nOHx, const double *nCHx,
+                        const double *rho_d, const lyd_dust_lya *dust, double z, int32_t ots, int32_t destruction) {
+    if (!c) return LYD_ERR_ARG;
+    if (!T || !nHI || !nH2 || !nHII || !nHeI || !ne || !nOHx || !nCHx || !rho_d || !dust)
+        return fail(c, LYD_ERR_ARG, "null input");
+    cudaSetDevice(c->dev);
+    if (!c->freq_set) return fail(c, LYD_ERR_STATE, "frequency grid not set");
+    const size_t nc = c->ncell;
+    LYD_TRY(ensure_stage(c, 11 * nc));
+    double *d = c->stage;
+    const double *src[8] = {T, nHI, nH2, nHII, nHeI, ne, nOHx, nCHx};
+    for (int q = 0; q < 8; q++) LYD_TRY(h2d(c, d + q * nc, src[q], nc));
+    LYD_TRY(h2d(c, d + 8 * nc, rho_d, 3 * nc));
+    RhdPrepArgs a;
+    memset(&a, 0, sizeof(a));
+    a.T = d; a.nHI = d + nc; a.nH2 = d + 2 * nc; a.nHII = d + 3 * nc; a.nHeI = d + 4 * nc; a.ne = d + 5 * nc;
+    a.nOHx = d + 6 * nc; a.nCHx = d + 7 * nc; a.rho_d = d + 8 * nc;
+    for (int q = 0; q < 3; q++) { a.kabs[q] = dust->kappa_abs[q]; a.kF[q] = dust->kappa_F[q]; }
+    a.rho_ignore = dust->rho_ignore; a.z = z; a.ots = ots; a.destruction = destruction; a.ncell = nc;
+    a.alpha = c->cellf[CF_ALPHA]; a.alpha_c = c->cellf[CF_ALPHA_C]; a.alpha_cF = c->cellf[CF_ALPHA_CF];
+    a.pd = c->cellf[CF_PD]; a.js = c->cellf[CF_JS]; a.T_out = c->cellf[CF_T];
+    if (!c->dust_F) LYD_TRY(dalloc(c, (void **)&c->dust_F, 3 * nc * 8));
+    a.dust_F = c->dust_F;
+    launch_rhd_prep(a, c->st);
+    LYD_CU(c, cudaGetLastError());
+    set_all(c, (1u << CF_ALPHA) | (1u << CF_ALPHA_C) | (1u << CF_ALPHA_CF) | (1u << CF_PD) | (1u << CF_JS) |
+                   (1u << CF_T));
+    LYD_TRY(lyd_update_hvoigt(c));
+    return lyd_update_phi_nu(c, 0, c->nnu - 1);
+}
+
+int lyd_rhd_lya_absorb(lyd_ctx *c, const double *dt, double c_tilde, int32_t commit, lyd_rhd_lya_out *out) {
+    if (!c) return LYD_ERR_ARG;
+    if (!dt) return fail(c, LYD_ERR_ARG, "null dt");
+    if (!(c_tilde > 0.0)) return fail(c, LYD_ERR_ARG, "c_tilde must be positive");
+    cudaSetDevice(c->dev);
+    if (!c->dust_F || !c->phi_inv_ready || c->phi || c->phi_kmin != 0 || c->phi_kmax != c->nnu - 1)
+        return fail(c, LYD_ERR_STATE, "call lyd_rhd_lya_prepare first (it sets phi_nu over all bins)");
+    const size_t nc = c->ncell;
+    LYD_TRY(materialize_old(c));
+    LYD_TRY(ensure_stage(c, 15 * nc));
+    double *d = c->stage;                     // [0, nc): dt ; [nc, 15 nc): outputs
+    LYD_TRY(h2d(c, d, dt, nc));
+    const void *args = nullptr;
+    RhdAbsorbArgs<double> a64;
+    RhdAbsorbArgs<float> a32;
+    auto fill = [&](auto &a, auto *tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        memset(&a, 0, sizeof(a));
+        a.dt = d;
+        a.alpha = c->cellf[CF_ALPHA]; a.alpha_c = c->cellf[CF_ALPHA_C]; a.alpha_cF = c->cellf[CF_ALPHA_CF];
+        a.pd = c->cellf[CF_PD]; a.js = c->cellf[CF_JS]; a.phi_inv = c->phi_inv; a.dust_F = c->dust_F;
+        a.dnu = c->dnu;
+        a.Hv = (const S *)c->Hv;
+        a.J = (S *)Jc(c, 0); a.Hr = (S *)Jc(c, 1); a.HZ = (S *)Jc(c, 2);
+        a.Jold = (S *)Jold(c, 0); a.Hrold = (S *)Jold(c, 1); a.HZold = (S *)Jold(c, 2);
+        a.e_lya = c->cellf[CF_E_LYA];
+        a.out = d + nc;
+        a.c_tilde = c_tilde; a.jeps = c->jeps_s; a.j_scale = c->jscale;
+        a.nnu = c->nnu; a.commit = commit ? 1 : 0; a.ncell = nc;
+    };
+    if (c->sprec == 0) { fill(a64, (double *)nullptr); args = &a64; }
+    else { fill(a32, (float *)nullptr); args = &a32; }
+    launch_rhd_absorb(c->sprec, args, c->st);
+    LYD_CU(c, cudaGetLastError());
+    c->active_valid = false;
+    if (out) {
+        std::vector<double> flag;
+        const double *o = d + nc;
+        if (out->reject) {
+            flag.resize(nc);
+            LYD_CU(c, cudaMemcpyAsync(flag.data(), o, nc * 8, cudaMemcpyDeviceToHost, c->st));
+        }
+        if (out->de) LYD_CU(c, cudaMemcpyAsync(out->de, o + nc, nc * 8, cudaMemcpyDeviceToHost, c->st));
+        if (out->e_new) LYD_CU(c, cudaMemcpyAsync(out->e_new, o + 2 * nc, nc * 8, cudaMemcpyDeviceToHost, c->st));
+        if (out->dru_r) LYD_CU(c, cudaMemcpyAsync(out->dru_r, o + 3 * nc, nc * 8, cudaMemcpyDeviceToHost, c->st));
+        if (out->dru_Z) LYD_CU(c, cudaMemcpyAsync(out->dru_Z, o + 4 * nc, nc * 8, cudaMemcpyDeviceToHost, c->st));
+        if (out->split) LYD_CU(c, cudaMemcpyAsync(out->split, o + 5 * nc, 8 * nc * 8, cudaMemcpyDeviceToHost, c->st));
+        if (out->dt_lya) LYD_CU(c, cudaMemcpyAsync(out->dt_lya, o + 13 * nc, nc * 8, cudaMemcpyDeviceToHost, c->st));
+        LYD_CU(c, cudaStreamSynchronize(c->st));
+        if (out->reject)
+            for (size_t q = 0; q < nc; q++) out->reject[q] = flag[q] != 0.0 ? 1 : 0;
+    }
     return check_err(c);
 }
 

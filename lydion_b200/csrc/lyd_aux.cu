@@ -4,6 +4,7 @@
 
 #include "lyd_internal.h"
 #include "lyd_physics.cuh"
+#include "lyd_species.cuh"
 
 namespace lyd {
 
@@ -173,35 +174,6 @@ void launch_phi_inv(int prec, const void *Hv, const double *dnu, int nnu, size_t
     else k_phi_inv<float><<<g, 256, 0, st>>>(static_cast<const float *>(Hv), dnu, nnu, ncell, kmin, kmax, phi_inv);
 }
 
-// pd_Lya, src/LymanAlphaDestruction.jl:43-97
-__device__ double pd_lya_dev(double nHII, double ne, double nHI, double nHeI, double nH2, double T, double z) {
-    T = fmin(fmax(T, 1.0), 1e5);
-    double T100 = T / 100.0;
-    double lT = log10(T);
-    double lT2 = lT * lT, lT3 = lT2 * lT, lT4 = lT3 * lT;
-    double Gp2s = 3.1e-6 * (1.0 + z);
-    double Gs2p = 3.0 * Gp2s;
-    double r25 = 2.5 / T;
-    double Ce = 5e-5 * exp(-(r25 * r25)) * ne / (1.0 + pow(T100, 0.45));
-    double CHII = (6.98e-3 * (1.0 + 0.933 * lT) * exp(-pow(601.0 / T, 0.406)) / pow(T, 0.5) +
-                   pow(10.0, -7.69 + 1.21 * lT + 0.455 * lT2 - 0.199 * lT3 + 0.0182 * lT4)) * nHII;
-    double CHeI = 2.6e-9 * pow(T100, 0.315) * nHeI;
-    double CH2 = 1.7e-9 * pow(T100, 0.3) * nH2;
-    double den = 8.9 * pow(T, -0.55) + 0.078 * pow(T, 0.35);
-    double CHI = (4.1e-11 * exp(-pow(1.6 / T, 0.75) - 0.15 * T) + (1.6e-10 + 1.57e-12 * pow(T, 1.1)) / (den * den)) * nHI;
-    double Cs2p = Ce + CHII + CHeI + CH2 + CHI;
-    double Cp2s = (1.0 / 3.0) * Cs2p;
-    double Rp2s = (2.0 / 3.0) * kA2p2s + Cp2s + Gp2s;
-    double Rs2p = kA2s2p + Cs2p + Gs2p;
-    double pdHI = Rp2s / ((kALya / kA2g) * (kA2g + Rs2p) + Rp2s);
-    double pdH2 = 0.0;
-    if (nHI > 1e-20) {
-        double num = 33.0 * exp(-14540.0 / T) + 13.0 * exp(-15564.0 / T);
-        double dd = 46.0 + 1e3 * exp(-pow(1e3 / T, 1.5));
-        pdH2 = fmin(num / dd, 1.3e-3) * (nH2 / nHI);
-    }
-    return fmin(pdHI + pdH2, 1.0);
-}
 __global__ void k_pd(size_t n, const double *nHII, const double *ne, const double *nHI, const double *nHeI,
                      const double *nH2, const double *T, double z, double *out) {
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)

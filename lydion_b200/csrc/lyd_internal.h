@@ -154,4 +154,28 @@ void launch_edge(int prec, const void *J, const double *dnu, int nnu, int nr, in
                  double *raw, double *norm, cudaStream_t st);
 void build_voigt_lut(double *host, int n, double xmax);   // host: 5 tables of n entries
 
+// RHD-side Lyman-alpha block (lyd_rhd.cu)
+struct RhdPrepArgs {
+    const double *T, *nHI, *nH2, *nHII, *nHeI, *ne, *nOHx, *nCHx, *rho_d;   // rho_d: [3][ncell]
+    double kabs[3], kF[3], rho_ignore, z;
+    int ots, destruction;
+    size_t ncell;
+    double *alpha, *alpha_c, *alpha_cF, *pd, *js, *T_out, *dust_F;         // dust_F: [3][ncell]
+};
+template <typename S>
+struct RhdAbsorbArgs {
+    const double *dt;                          // per cell
+    const double *alpha, *alpha_c, *alpha_cF, *pd, *js, *phi_inv, *dust_F, *dnu;
+    const S *Hv;
+    S *J, *Hr, *HZ;                            // written
+    S *Jold, *Hrold, *HZold;                   // read; written by an accepting commit
+    double *e_lya;                             // per cell: read, and written by a commit
+    double *out;                               // [14][ncell]
+    double c_tilde, jeps, j_scale;
+    int nnu, commit;
+    size_t ncell;
+};
+void launch_rhd_prep(const RhdPrepArgs &a, cudaStream_t st);
+void launch_rhd_absorb(int sprec, const void *args, cudaStream_t st);
+
 }  // namespace lyd

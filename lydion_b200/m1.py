@@ -237,6 +237,36 @@ class M1Context:
         self._ck(lib().lyd_pd_lya(self._h, out.size, *[_dp(a) for a in arrs], float(z), _dp(out)))
         return out.reshape(np.shape(nHII))
 
+    # -- RHD-side Lyman-alpha block --------------------------------------------------------
+    def rhd_lya_prepare(self, T, nHI, nH2, nHII, nHeI, ne, nOHx, nCHx, rho_d, kappa_abs, kappa_F, rho_ignore,
+                        z=0.0, ots=True, destruction=True):
+        """PrepareLyaSubCycling! for every cell (lyd_rhd_lya_prepare): per-cell arrays of shape
+        (n_z, n_r); rho_d (3, n_z, n_r) holds the silicate, carbonaceous and PAH dust densities."""
+        arrs = [_c64(np.ravel(a)) for a in (T, nHI, nH2, nHII, nHeI, ne, nOHx, nCHx)]
+        rho = _c64(np.reshape(rho_d, (3, -1)))
+        if any(a.size != self.n_r * self.n_z for a in arrs) or rho.shape[1] != self.n_r * self.n_z:
+            raise ValueError("per-cell arrays must have n_r * n_z entries")
+        d = _lib.DustLya((C.c_double * 3)(*kappa_abs), (C.c_double * 3)(*kappa_F), float(rho_ignore))
+        self._ck(lib().lyd_rhd_lya_prepare(self._h, *[_dp(a) for a in arrs], _dp(rho), C.byref(d), float(z),
+                                           int(bool(ots)), int(bool(destruction))))
+
+    def rhd_lya_absorb(self, dt, c_tilde, commit=False):
+        """The Lyman-alpha block of AbsorptionStep for every cell over its own sub-step dt
+        (lyd_rhd_lya_absorb). Returns the per-cell results as (n_z, n_r) arrays (split: 8 of them)."""
+        shape = (self.n_z, self.n_r)
+        dts = _c64(np.broadcast_to(np.asarray(dt, dtype=np.float64), shape))
+        n = self.n_r * self.n_z
+        rej = np.zeros(n, dtype=np.int32)
+        res = {k: np.empty(n) for k in ("de", "e_new", "dru_r", "dru_Z", "dt_lya")}
+        split = np.empty(8 * n)
+        out = _lib.RhdLyaOut(rej.ctypes.data_as(C.POINTER(C.c_int32)), _dp(res["de"]), _dp(res["e_new"]),
+                             _dp(res["dru_r"]), _dp(res["dru_Z"]), _dp(split), _dp(res["dt_lya"]))
+        self._ck(lib().lyd_rhd_lya_absorb(self._h, _dp(dts), float(c_tilde), int(bool(commit)), C.byref(out)))
+        r = {k: v.reshape(shape) for k, v in res.items()}
+        r["reject"] = rej.reshape(shape).astype(bool)
+        r["split"] = split.reshape((8,) + shape)
+        return r
+
     def cfl_dt(self, c_tilde, u_r, u_Z, cfl):
         a, b = _c64(u_r), _c64(u_Z)
         out = C.c_double()

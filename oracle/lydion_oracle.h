@@ -144,6 +144,22 @@ void   orc_static_run(orc_lya *s, const orc_geom *g, const orc_vel *v, double c_
                       double dt, double z_center, int bc_r_right, int bc_z_bot, int bc_z_top,
                       int n_steps, double *diag_hist /* n_steps*7 */);
 
+/* RHD-side Lyman-alpha block (lydion_oracle_rhd.c) */
+typedef struct orc_dust_lya {
+    double kappa_abs[3], kappa_F[3];   /* Sil, C, PAH (cm^2 g^-1) */
+    double rho_ignore;                 /* dust densities at or below this are ignored */
+} orc_dust_lya;
+double orc_prob_lya_sh95(double T, double ne, int caseB);
+double orc_krec_hii(double T, int ots);
+double orc_js_rec_lya(double T, double nHII, double ne, int ots);
+double orc_js_coll_lya(double T, double nHI, double ne);
+void   orc_rhd_lya_prepare_cell(const double sp[11], const orc_dust_lya *d, double z, int ots, int destruction,
+                                double out[8]);
+int    orc_rhd_lya_absorb_cell(int nnu, const double *dnu, const double *Hv, const double *phi, const double *J_old,
+                               const double *Hr_old, const double *HZ_old, double *J, double *Hr, double *HZ,
+                               const double cell[8], double dt, double c_tilde, double e_old, double jeps,
+                               double out[13]);
+
 int    orc_num_threads(void);
 void   orc_set_num_threads(int n);
 

@@ -97,6 +97,10 @@ def _declare(L):
         "orc_static_step": (None, [C.c_void_p, C.c_void_p, C.c_void_p, D, D, D, I, I, I, P]),
         "orc_static_run": (None, [C.c_void_p, C.c_void_p, C.c_void_p, D, D, D, I, I, I, I, P]),
         "orc_num_threads": (I, []), "orc_set_num_threads": (None, [I]),
+        "orc_prob_lya_sh95": (D, [D, D, I]), "orc_krec_hii": (D, [D, I]),
+        "orc_js_rec_lya": (D, [D, D, D, I]), "orc_js_coll_lya": (D, [D, D, D]),
+        "orc_rhd_lya_prepare_cell": (None, [P, C.c_void_p, D, I, I, P]),
+        "orc_rhd_lya_absorb_cell": (I, [I, P, P, P, P, P, P, P, P, P, P, D, D, D, D, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -296,3 +300,73 @@ def vec_fn(name, *args, n=3):
     out = np.zeros(n)
     getattr(lib(), name)(*args, _p(out))
     return out
+
+
+# ---- RHD-side Lyman-alpha block (oracle/lydion_oracle_rhd.c) -------------------------------
+class DustLya(C.Structure):
+    _fields_ = [("kappa_abs", C.c_double * 3), ("kappa_F", C.c_double * 3), ("rho_ignore", C.c_double)]
+
+
+def rhd_lya_prepare(state, sp, rho_d, kappa_abs, kappa_F, rho_ignore, z=0.0, ots=True, destruction=True):
+    """PrepareLyaSubCycling! on an OracleState: sp holds the per-cell arrays T, nHI, nH2, nHII,
+    nHeI, ne, nOHx, nCHx ((n_z, n_r) each); rho_d is (3, n_z, n_r). Sets T, alpha, alpha_c, pd,
+    js, H_voigt and phi_nu (all bins) on the state; returns alpha_cF and the dust flux opacities
+    (3, n_z, n_r)."""
+    d = DustLya((C.c_double * 3)(*kappa_abs), (C.c_double * 3)(*kappa_F), float(rho_ignore))
+    nz, nr = state.T.shape
+    acF = np.zeros((nz, nr))
+    dF = np.zeros((3, nz, nr))
+    out = np.zeros(8)
+    names = ("T", "nHI", "nH2", "nHII", "nHeI", "ne", "nOHx", "nCHx")
+    for j in range(nz):
+        for i in range(nr):
+            v = np.array([float(sp[n][j, i]) for n in names] + [float(rho_d[q][j, i]) for q in range(3)])
+            lib().orc_rhd_lya_prepare_cell(_p(v), C.byref(d), float(z), int(bool(ots)), int(bool(destruction)),
+                                           _p(out))
+            state.T[j, i] = v[0]
+            state.alpha[j, i], state.alpha_c[j, i], acF[j, i] = out[0], out[1], out[2]
+            state.pd[j, i], state.js[j, i] = out[3], out[4]
+            dF[:, j, i] = out[5:8]
+    lut = state.lut or OracleLUT()
+    state.lut = lut
+    lib().orc_update_hvoigt(lut.ref, C.byref(state.s))
+    lib().orc_update_phi_nu(C.byref(state.s), 0, state.cloud.n_nu - 1)
+    return acF, dF
+
+
+def rhd_lya_absorb(state, acF, dF, dt, c_tilde, e_lya, jeps=1e-60, commit=False):
+    """The Lyman-alpha block of AbsorptionStep for every cell of an OracleState from its J_old /
+    H_old over the per-cell sub-step dt; writes J, H (and, with commit, the accepted cells' old
+    state and e_lya, or restores the rejected ones). Returns a dict of per-cell results."""
+    nz, nr = state.T.shape
+    nnu = state.cloud.n_nu
+    dnu = np.ascontiguousarray(state.cloud.freq.dnu, dtype=np.float64)
+    res = {k: np.zeros((nz, nr)) for k in ("de", "e_new", "dru_r", "dru_Z", "dt_lya")}
+    res["split"] = np.zeros((8, nz, nr))
+    res["reject"] = np.zeros((nz, nr), dtype=bool)
+    out = np.zeros(13)
+    cell = np.zeros(8)
+    dt = np.broadcast_to(np.asarray(dt, dtype=np.float64), (nz, nr))
+    for j in range(nz):
+        for i in range(nr):
+            cell[:] = [state.alpha[j, i], state.alpha_c[j, i], acF[j, i], state.pd[j, i], state.js[j, i],
+                       dF[0, j, i], dF[1, j, i], dF[2, j, i]]
+            row = lambda a: np.ascontiguousarray(a[j, i])
+            Hv, phi = row(state.Hvoigt), row(state.phi_nu)
+            Jo, Hro, HZo = row(state.J_old), row(state.H_r_old), row(state.H_Z_old)
+            J, Hr, HZ = np.zeros(nnu), np.zeros(nnu), np.zeros(nnu)
+            rej = lib().orc_rhd_lya_absorb_cell(nnu, _p(dnu), _p(Hv), _p(phi), _p(Jo), _p(Hro), _p(HZo), _p(J),
+                                                _p(Hr), _p(HZ), _p(cell), float(dt[j, i]), float(c_tilde),
+                                                float(e_lya[j, i]), float(jeps), _p(out))
+            state.J[j, i], state.H_r[j, i], state.H_Z[j, i] = J, Hr, HZ
+            res["reject"][j, i] = bool(rej)
+            res["e_new"][j, i], res["de"][j, i], res["dru_r"][j, i], res["dru_Z"][j, i] = out[0], out[1], out[2], out[3]
+            res["split"][:, j, i] = out[4:12]
+            res["dt_lya"][j, i] = out[12]
+            if commit:
+                if rej:
+                    state.J[j, i], state.H_r[j, i], state.H_Z[j, i] = Jo, Hro, HZo
+                else:
+                    state.J_old[j, i], state.H_r_old[j, i], state.H_Z_old[j, i] = J, Hr, HZ
+                    e_lya[j, i] = out[0]
+    return res

@@ -210,3 +210,26 @@ def test_gravity_force_multiplier_antiparallel(oracle_mod):
     st.dru_Z[...] = st.f_Z * cl.dt
     z = np.zeros_like(st.dru_r)
     assert st.force_multiplier_gravity(cl.dt, z, z)[1] == 0.0
+
+
+def test_rhd_lya_oracle_pins():
+    """Pinned points of the RHD-side Lyman-alpha block's oracle: the Storey & Hummer (1995)
+    table nodes (src/LymanAlphaEmission.jl:36-65), the flat extrapolation, linear interpolation
+    between nodes in log space, and the Case B recombination rate at 1e4 K (2.59e-13 cm^3 s^-1,
+    the value of the fit in src/PhotoChemistryAndCooling/GasChemistryRates.jl:176-181)."""
+    from oracle import oracle as O
+    L = O.lib()
+    assert L.orc_prob_lya_sh95(1e4, 1e2, 1) == 0.68808416
+    assert L.orc_prob_lya_sh95(1e4, 1e2, 0) == 0.40023971
+    assert L.orc_prob_lya_sh95(3e4, 1e14, 1) == 0.96391965
+    assert L.orc_prob_lya_sh95(1e6, 1e20, 1) == 0.96391965          # clamped to the grid's corner
+    assert L.orc_prob_lya_sh95(1.0, 1.0, 0) == 0.58042473
+    mid = L.orc_prob_lya_sh95(1e4, 10 ** 2.5, 1)
+    assert abs(mid - 0.5 * (0.68808416 + 0.76220739)) < 1e-15
+    assert abs(L.orc_krec_hii(1e4, 1) - 2.59e-13) < 1e-3 * 2.59e-13
+    assert L.orc_krec_hii(1e4, 0) > L.orc_krec_hii(1e4, 1)           # Case A exceeds Case B
+    E = 6.626069573e-27 * 2.466068e15 / (4 * np.pi)
+    js = L.orc_js_rec_lya(1e4, 2.0, 3.0, 1)
+    assert abs(js - L.orc_prob_lya_sh95(1e4, 3.0, 1) * L.orc_krec_hii(1e4, 1) * 2.0 * 3.0 * E) < 1e-12 * js
+    # collisional excitation is negligible in cold gas and rises steeply with T
+    assert L.orc_js_coll_lya(1e3, 1.0, 1.0) < 1e-40 < L.orc_js_coll_lya(1e4, 1.0, 1.0)
