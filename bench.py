@@ -276,6 +276,38 @@ def batch_form(args, barrier, stream_of, local, world):
     return out
 
 
+def rhd_form(args, stream_of, local):
+    """The RHD-side Lyman-alpha block on the 256 x 256 x 64 grid in FP64: lyd_rhd_lya_prepare
+    (11 per-cell host arrays up, opacities, emissivities, H_voigt and phi_nu) and
+    lyd_rhd_lya_absorb over per-cell sub-steps of a tenth of each cell's absorption time (the
+    sub-steps up, no results back, no commit), on a seeded gas and dust state."""
+    from lydion_b200 import workloads as W
+    from lydion_b200.m1 import context_for_cloud
+    cl = W.config_c2()
+    ctx = context_for_cloud(cl, device=local)
+    sp, rho_d = W.rhd_gas_state(cl, 20261203)
+    prep = lambda k: [ctx.rhd_lya_prepare(sp["T"], sp["nHI"], sp["nH2"], sp["nHII"], sp["nHeI"], sp["ne"], sp["nOHx"],
+                                          sp["nCHx"], rho_d, W.DUST_KAPPA_ABS, W.DUST_KAPPA_F, W.DUST_RHO_IGNORE,
+                                          z=0.0) for _ in range(k)]
+    prep(2)
+    n_prep = 10
+    prep_ms = _timed(ctx, prep, n_prep, stream_of) / n_prep
+    c_tilde = cl.c_tilde
+    a, ac, pd = ctx.download("alpha"), ctx.download("alpha_c"), ctx.download("pd")
+    dt = 0.1 / (c_tilde * np.maximum(ac + pd * a, 1e-300))
+    absorb = lambda k: [ctx.rhd_lya_absorb(dt, c_tilde, results=False) for _ in range(k)]
+    absorb(3)
+    n_abs = 50
+    abs_ms = _timed(ctx, absorb, n_abs, stream_of) / n_abs
+    ctx.close()
+    n3 = cl.cell_bins
+    return {"workload": "rhd_lya_block_256x256x64", "cell_bins": n3,
+            "prepare_ms": prep_ms, "absorb_ms": abs_ms,
+            "absorb_cell_bins_per_s": n3 / (abs_ms * 1e-3),
+            # J_old, H_r_old, H_Z_old, H_voigt read and J, H_r, H_Z written: 56 B per cell-bin in FP64
+            "absorb_hbm_gbs": 56.0 * n3 / (abs_ms * 1e-3) / 1e9}
+
+
 def c5_form(args, stream_of, local):
     """The largest single field (1024 x 1024 cells x 128 bins of a synthetic RHD snapshot: lognormal
     n_H, photoionised bubble, shell outflow, dust): both forms, a few graph-replayed steps each,
@@ -376,6 +408,7 @@ def run_gpu(args):
     batch = None if args.no_batch else batch_form(args, barrier, stream_of, local, world)
     adj = None if (args.no_adjoint or world > 1) else adjoint_form(args, stream_of, local)
     c5 = None if (args.no_c5 or world > 1) else c5_form(args, stream_of, local)
+    rhd = None if (args.no_rhd or world > 1) else rhd_form(args, stream_of, local)
 
     # roofline of the dominant kernel of the headline (mixed) form
     names = ["advect", "freq", "reduce"]
@@ -404,6 +437,7 @@ def run_gpu(args):
                 "adjoint_over_forward": adj["ratio_auto"] if adj else None,
                 "adjoint": adj,
                 "largest_field": c5,
+                "rhd_lya_block": rhd,
                 "batch": batch,
                 "roofline": {"bound": "hbm", "kernel": "k_" + names[dom], "achieved": achieved,
                              "peak": peaks["hbm_gbs"], "peak_source": src, "unit": "GB/s",
@@ -435,6 +469,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of the autotuner")
     ap.add_argument("--no-c5", action="store_true", help="skip the 1024x1024x128 field")
+    ap.add_argument("--no-rhd", action="store_true", help="skip the RHD-side Lyman-alpha block")
     ap.add_argument("--only-mixed", action="store_true", help="measure the mixed-precision form only")
     args = ap.parse_args()
     if args.warmup < 3:

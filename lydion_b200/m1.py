@@ -250,11 +250,15 @@ class M1Context:
         self._ck(lib().lyd_rhd_lya_prepare(self._h, *[_dp(a) for a in arrs], _dp(rho), C.byref(d), float(z),
                                            int(bool(ots)), int(bool(destruction))))
 
-    def rhd_lya_absorb(self, dt, c_tilde, commit=False):
+    def rhd_lya_absorb(self, dt, c_tilde, commit=False, results=True):
         """The Lyman-alpha block of AbsorptionStep for every cell over its own sub-step dt
-        (lyd_rhd_lya_absorb). Returns the per-cell results as (n_z, n_r) arrays (split: 8 of them)."""
+        (lyd_rhd_lya_absorb). Returns the per-cell results as (n_z, n_r) arrays (split: 8 of them),
+        or None without `results` (nothing is copied back)."""
         shape = (self.n_z, self.n_r)
         dts = _c64(np.broadcast_to(np.asarray(dt, dtype=np.float64), shape))
+        if not results:
+            self._ck(lib().lyd_rhd_lya_absorb(self._h, _dp(dts), float(c_tilde), int(bool(commit)), None))
+            return None
         n = self.n_r * self.n_z
         rej = np.zeros(n, dtype=np.int32)
         res = {k: np.empty(n) for k in ("de", "e_new", "dru_r", "dru_Z", "dt_lya")}

@@ -313,3 +313,29 @@ def small_cloud(nr=12, nz=10, n_nu=16, **kw):
     kw.setdefault("tau_abs", 0.5)
     kw.setdefault("x_max", 60.0)
     return static_cloud(nr, nz, n_nu, name="small", **kw)
+
+
+# ---- gas and dust state for the RHD-side Lyman-alpha block ----------------------------------
+DUST_KAPPA_ABS = (3.0e4, 5.0e4, 8.0e4)    # Lya absorption opacity per dust mass, Sil / C / PAH (cm^2 g^-1)
+DUST_KAPPA_F = (6.0e4, 9.0e4, 1.2e5)      # Lya flux opacity per dust mass
+DUST_RHO_IGNORE = 1.1e-13 * K.mH          # 1.1 rho_d_floor with rho_d_floor = 1e-13 m_H (src/Hydrodynamics.jl:53-54)
+
+
+def rhd_gas_state(cloud, seed):
+    """A seeded per-cell gas and dust state for lyd_rhd_lya_prepare: T log-uniform over 30 K ..
+    4e4 K (both edges of the recombination tables and their interior), n_H log-uniform over
+    0.1 .. 1e3 cm^-3, ionised fraction 1e-4 .. 1, molecular, He, OH and CH fractions, and dust
+    at 1e-4 .. 1e-2 of the gas mass in three kinds, a fifth of the silicate below the ignore
+    level. The dust opacities are this project's choice. Returns (species dict, rho_d (3, n_z, n_r))."""
+    rng = np.random.default_rng(seed)
+    shape = (cloud.nz, cloud.nr)
+    lg = lambda lo, hi: 10.0 ** rng.uniform(lo, hi, size=shape)
+    T = lg(1.5, 4.6)
+    nH = lg(-1.0, 3.0)
+    xHII = lg(-4.0, 0.0)
+    sp = {"T": T, "nHI": nH * (1.0 - xHII), "nHII": nH * xHII, "ne": nH * xHII * 1.1,
+          "nH2": nH * lg(-6.0, -1.0), "nHeI": 0.08 * nH, "nOHx": nH * lg(-9.0, -6.0), "nCHx": nH * lg(-9.0, -6.0)}
+    rho = 0.01 * nH * K.mH * lg(-2.0, 0.0)
+    rho_d = np.stack([rho, 0.5 * rho, 0.05 * rho])
+    rho_d[0][rng.uniform(size=shape) < 0.2] = 0.5 * DUST_RHO_IGNORE
+    return sp, rho_d

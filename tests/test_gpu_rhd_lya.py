@@ -12,33 +12,15 @@ from lydion_b200._lib import PREC_FP32, PREC_FP64, PREC_MIXED
 
 pytestmark = pytest.mark.gpu
 
-MH = 1.0080 * 1.660539069e-24
-KAPPA_ABS = (3.0e4, 5.0e4, 8.0e4)     # cm^2 g^-1 (Sil, C, PAH), set for the test
-KAPPA_F = (6.0e4, 9.0e4, 1.2e5)
-RHO_IGNORE = 1.1e-13 * MH             # 1.1 rho_d_floor, rho_d_floor = 1e-13 m_H (Hydrodynamics.jl:53-54)
+KAPPA_ABS, KAPPA_F, RHO_IGNORE = W.DUST_KAPPA_ABS, W.DUST_KAPPA_F, W.DUST_RHO_IGNORE
 C_TILDE = 3e8
-
-
-def gas_state(cloud, seed):
-    rng = np.random.default_rng(seed)
-    shape = (cloud.nz, cloud.nr)
-    lg = lambda lo, hi: 10.0 ** rng.uniform(lo, hi, size=shape)
-    T = lg(1.5, 4.6)                        # 30 K .. 4e4 K: both table edges and the interior
-    nH = lg(-1.0, 3.0)
-    xHII = lg(-4.0, 0.0)
-    sp = {"T": T, "nHI": nH * (1.0 - xHII), "nHII": nH * xHII, "ne": nH * xHII * 1.1,
-          "nH2": nH * lg(-6.0, -1.0), "nHeI": 0.08 * nH, "nOHx": nH * lg(-9.0, -6.0), "nCHx": nH * lg(-9.0, -6.0)}
-    rho = 0.01 * nH * MH * lg(-2.0, 0.0)
-    rho_d = np.stack([rho, 0.5 * rho, 0.05 * rho])
-    rho_d[0][rng.uniform(size=shape) < 0.2] = 0.5 * RHO_IGNORE   # some dust below the ignore level
-    return sp, rho_d
 
 
 def matched(precision, seed, oracle_hvoigt=False):
     from oracle import oracle as O
     from lydion_b200.m1 import context_for_cloud
     cl = W.small_cloud(nr=10, nz=9, n_nu=24)
-    sp, rho_d = gas_state(cl, seed)
+    sp, rho_d = W.rhd_gas_state(cl, seed)
     st = O.OracleState(cl)
     ctx = context_for_cloud(cl, precision=precision)
     acF, dF = O.rhd_lya_prepare(st, sp, rho_d, KAPPA_ABS, KAPPA_F, RHO_IGNORE, z=0.5)
