@@ -72,8 +72,21 @@ typedef struct lyd_config {
     double j_scale;             /* LYD_PREC_MIXED / _FP32: J and H are held as value / j_scale
                                    (inside the FP32 range); 0 selects 1e-12                */
     int32_t device;             /* CUDA device ordinal                                     */
-    int32_t reserved[7];
+    int32_t geometry;           /* LYD_GEOM_CYLINDRICAL (0) or LYD_GEOM_CARTESIAN (1)         */
+    int32_t bc_r_left;          /* boundary at the first r (X) interface of the static-driver
+                                   steps: always LYD_BC_REFLECT (the axis) for a cylindrical
+                                   grid; LYD_BC_REFLECT or LYD_BC_OUTFLOW for a Cartesian one  */
+    int32_t reserved[5];
 } lyd_config;
+
+/* Geometries (LyaArrays on GeometryCylindrical or GeometryCartesian). A Cartesian context runs
+ * AdvectJandH_Cartesian! (src/AdvectJandH.jl:1396-2222): r and Z stand for X and Y, the areas
+ * and volumes of lyd_set_geometry are the Cartesian ones (A_X = dY, A_Y = dX, dV = dX dY, per
+ * unit depth; src/SpatialGrid.jl:1061-1135), there is no K_phiphi source and no u_r / r term
+ * (the context ignores inv_r_cell and rejects u_r / r), and the first X interface may be an
+ * outflow boundary (ghost H_X = min(H_X, 0)). */
+#define LYD_GEOM_CYLINDRICAL 0
+#define LYD_GEOM_CARTESIAN   1
 
 /* Cylindrical geometry: the fields of GeometryCylindrical read by AdvectJandH!
  * (src/AdvectJandH.jl:2272-2319). Arrays as described at the top of this file. */
@@ -129,7 +142,7 @@ typedef struct lyd_step_params {
     double c_tilde;        /* reduced speed of light                  */
     double dt;             /* time step                               */
     double z_center;       /* cloud centre for the radial M_F         */
-    int32_t bc_r_right, bc_z_bot, bc_z_top;   /* r = 0 is always reflecting */
+    int32_t bc_r_right, bc_z_bot, bc_z_top;   /* the first r interface: lyd_config.bc_r_left */
     int32_t n_steps;
 } lyd_step_params;
 

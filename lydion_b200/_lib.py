@@ -12,6 +12,7 @@ LYD_OK = 0
 LYD_ERR_ARG, LYD_ERR_CUDA, LYD_ERR_NONFINITE, LYD_ERR_SOLVE, LYD_ERR_STATE, LYD_ERR_NOMEM = -1, -2, -3, -4, -5, -6
 BC_REFLECT, BC_OUTFLOW = 0, 1
 FLUX_GLF, FLUX_HLL = 0, 1
+GEOM_CYLINDRICAL, GEOM_CARTESIAN = 0, 1
 PREC_FP64, PREC_MIXED, PREC_FP32 = 0, 1, 2
 
 F = dict(J=0, J_old=1, H_r=2, H_Z=3, H_r_old=4, H_Z_old=5, Hvoigt=6, phi_nu=7, alpha_F=8,
@@ -35,7 +36,7 @@ class Config(C.Structure):
     _fields_ = [("flux_method", C.c_int32), ("recoil", C.c_int32), ("precision", C.c_int32),
                 ("kcore_min", C.c_int32), ("kcore_max", C.c_int32), ("keep_freq_factors", C.c_int32),
                 ("alpha_floor", C.c_double), ("j_scale", C.c_double), ("device", C.c_int32),
-                ("reserved", C.c_int32 * 7)]
+                ("geometry", C.c_int32), ("bc_r_left", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 class Geometry(C.Structure):

@@ -612,7 +612,7 @@ __device__ __forceinline__ GCell gcell(const AdjAdvArgs &a, int i, int j, int k)
     GCell g;
     g.sHr = 1.0; g.sHZ = 1.0;
     const int nr = a.nr, nz = a.nz;
-    if (i < 0) { g.i = -1 - i; g.sHr = -1.0; }
+    if (i < 0) { if (a.bc_r_left == 0) { g.i = -1 - i; g.sHr = -1.0; } else { g.i = 0; g.sHr = -2.0; } }
     else if (i >= nr) { if (a.bc_r_right == 0) { g.i = 2 * nr - 1 - i; g.sHr = -1.0; } else { g.i = nr - 1; g.sHr = 2.0; } }
     else g.i = i;
     if (j < 0) { if (a.bc_z_bot == 0) { g.j = -1 - j; g.sHZ = -1.0; } else { g.j = 0; g.sHZ = -2.0; } }
@@ -623,6 +623,7 @@ __device__ __forceinline__ GCell gcell(const AdjAdvArgs &a, int i, int j, int k)
     double hr = a.Hr[x], hz = a.HZ[x];
     // outflow ghosts keep only the outgoing sign: 2.0 marks max(H, 0), -2.0 min(H, 0)
     if (g.sHr == 2.0) { g.sHr = hr > 0.0 ? 1.0 : 0.0; }
+    else if (g.sHr == -2.0) { g.sHr = hr < 0.0 ? 1.0 : 0.0; }
     if (g.sHZ == 2.0) { g.sHZ = hz > 0.0 ? 1.0 : 0.0; }
     else if (g.sHZ == -2.0) { g.sHZ = hz < 0.0 ? 1.0 : 0.0; }
     g.Hr = g.sHr * hr;

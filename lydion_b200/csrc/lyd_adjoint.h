@@ -51,7 +51,7 @@ struct AdjAdvArgs {
     double *g_u;                        // [5][ncell] (+=)
     double *g_ur, *g_uZ;                // face velocities (+=)
     int nnu, nr, nz, kmin, kmax;
-    int bc_r_right, bc_z_bot, bc_z_top;
+    int bc_r_left, bc_r_right, bc_z_bot, bc_z_top;
     int flux;                           // 0 = GLF, 1 = HLL
     double ctdt, jeps, heps2;
 };

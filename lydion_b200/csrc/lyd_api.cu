@@ -255,6 +255,9 @@ int lyd_batch_create(lyd_ctx **out, int32_t ncl, const int32_t *n_r, const int32
         return LYD_ERR_ARG;
     if (cfg->flux_method != LYD_FLUX_GLF && cfg->flux_method != LYD_FLUX_HLL) return LYD_ERR_ARG;
     if (cfg->kcore_min < 0 || cfg->kcore_max >= n_nu || cfg->kcore_min > cfg->kcore_max) return LYD_ERR_ARG;
+    if (cfg->geometry != LYD_GEOM_CYLINDRICAL && cfg->geometry != LYD_GEOM_CARTESIAN) return LYD_ERR_ARG;
+    if (cfg->bc_r_left != LYD_BC_REFLECT && cfg->bc_r_left != LYD_BC_OUTFLOW) return LYD_ERR_ARG;
+    if (cfg->geometry == LYD_GEOM_CYLINDRICAL && cfg->bc_r_left != LYD_BC_REFLECT) return LYD_ERR_ARG;
     lyd_ctx *c = new lyd_ctx();
     c->cfg = *cfg;
     c->dev = cfg->device;
@@ -420,7 +423,10 @@ int lyd_set_geometry_cloud(lyd_ctx *c, int32_t q, const lyd_geometry *g) {
     LYD_TRY(h2d(c, c->inv_dV + d.oc, g->inv_dV, nc));
     LYD_TRY(h2d(c, c->A_r + d.orf, g->A_r, (size_t)(nr + 1) * nz));
     LYD_TRY(h2d(c, c->A_Z + d.ozf, g->A_Z, (size_t)nr * (nz + 1)));
-    LYD_TRY(h2d(c, c->inv_r_cell + d.ocol, g->inv_r_cell, nr));
+    if (c->cfg.geometry == LYD_GEOM_CARTESIAN)   // no K_phiphi source on a Cartesian grid
+        LYD_CU(c, cudaMemsetAsync(c->inv_r_cell + d.ocol, 0, (size_t)nr * 8, c->st));
+    else
+        LYD_TRY(h2d(c, c->inv_r_cell + d.ocol, g->inv_r_cell, nr));
     LYD_TRY(h2d(c, c->rCoM + d.ocol, g->rCoM, nr));
     LYD_TRY(h2d(c, c->ZCoM + d.orow, g->ZCoM, nz));
     LYD_TRY(h2d(c, c->r_if + d.orif, g->r, nr + 1));
@@ -523,6 +529,8 @@ static int upload_field(lyd_ctx *c, int q, int32_t field, const double *host, si
         mark(field == LYD_F_PHI_NU ? BIT_PHI : BIT_AF);
     } else if (field >= LYD_F_ALPHA && field <= LYD_F_E_LYA) {
         if (count != nc) return fail(c, LYD_ERR_ARG, "wrong element count for a per-cell field");
+        if (field == LYD_F_UR_OVER_R && c->cfg.geometry == LYD_GEOM_CARTESIAN)
+            return fail(c, LYD_ERR_ARG, "a Cartesian grid has no u_r / r term");
         int k = field - LYD_F_ALPHA;
         LYD_TRY(h2d(c, c->cellf[k] + d.oc, host, nc));
         mark(1u << k);
@@ -703,9 +711,10 @@ int lyd_find_active_bins(lyd_ctx *c, int32_t *kmin, int32_t *kmax) {
 }
 
 static int check_bcs(lyd_ctx *c, int l, int r, int b, int t) {
-    if (l != LYD_BC_REFLECT) return fail(c, LYD_ERR_ARG, "the r = 0 boundary of a cylindrical grid is always reflecting");
     auto ok = [](int v) { return v == LYD_BC_REFLECT || v == LYD_BC_OUTFLOW; };
-    if (!ok(r) || !ok(b) || !ok(t)) return fail(c, LYD_ERR_ARG, "unknown boundary condition");
+    if (c->cfg.geometry == LYD_GEOM_CYLINDRICAL && l != LYD_BC_REFLECT)
+        return fail(c, LYD_ERR_ARG, "the r = 0 boundary of a cylindrical grid is always reflecting");
+    if (!ok(l) || !ok(r) || !ok(b) || !ok(t)) return fail(c, LYD_ERR_ARG, "unknown boundary condition");
     return LYD_OK;
 }
 
@@ -715,9 +724,9 @@ static void params_all(lyd_ctx *c, double ct, double dt, double ctdt) {
         d.c_tilde = ct; d.dt = dt; d.ctdt = ctdt;
     }
 }
-static void bcs_all(lyd_ctx *c, int bcr, int bzb, int bzt) {
+static void bcs_all(lyd_ctx *c, int bcl, int bcr, int bzb, int bzt) {
     for (CloudDesc &d : c->desc) {
-        d.bc_r_right = bcr; d.bc_z_bot = bzb; d.bc_z_top = bzt;
+        d.bc_r_left = bcl; d.bc_r_right = bcr; d.bc_z_bot = bzb; d.bc_z_top = bzt;
     }
 }
 
@@ -748,7 +757,7 @@ int lyd_advect(lyd_ctx *c, double ctdt, int32_t bl, int32_t br, int32_t bb, int3
     LYD_TRY(need_inputs(c, false, false));
     if (!(ctdt > 0.0)) return fail(c, LYD_ERR_ARG, "c~ dt must be positive");
     for (CloudDesc &d : c->desc) d.ctdt = ctdt;
-    bcs_all(c, br, bb, bt);
+    bcs_all(c, bl, br, bb, bt);
     return do_advect(c);
 }
 
@@ -764,7 +773,7 @@ int lyd_advect_jh(lyd_ctx *c, double ctdt, int32_t kmin, int32_t kmax, int32_t u
     if (!(ctdt > 0.0)) return fail(c, LYD_ERR_ARG, "c~ dt must be positive");
     if (kmin < 0 || kmax >= c->nnu || kmin > kmax) return fail(c, LYD_ERR_ARG, "bad bin range");
     for (CloudDesc &d : c->desc) d.ctdt = ctdt;
-    bcs_all(c, br, bb, bt);
+    bcs_all(c, bl, br, bb, bt);
     LYD_TRY(sync_desc(c));
     const bool alias = c->old_alias;
     const size_t bytes = c->n3 * c->ssz;
@@ -1070,11 +1079,11 @@ static int run_steps(lyd_ctx *c, int n_steps, lyd_diag *hist_out) {
 int lyd_static_steps(lyd_ctx *c, const lyd_step_params *p, lyd_diag *hist_out) {
     if (!c || !p) return LYD_ERR_ARG;
     cudaSetDevice(c->dev);
-    LYD_TRY(check_bcs(c, LYD_BC_REFLECT, p->bc_r_right, p->bc_z_bot, p->bc_z_top));
+    LYD_TRY(check_bcs(c, c->cfg.bc_r_left, p->bc_r_right, p->bc_z_bot, p->bc_z_top));
     if (!(p->c_tilde > 0.0) || !(p->dt > 0.0) || p->n_steps < 0) return fail(c, LYD_ERR_ARG, "bad step parameters");
     params_all(c, p->c_tilde, p->dt, p->c_tilde * p->dt);
     for (CloudDesc &d : c->desc) d.z_center = p->z_center;
-    bcs_all(c, p->bc_r_right, p->bc_z_bot, p->bc_z_top);
+    bcs_all(c, c->cfg.bc_r_left, p->bc_r_right, p->bc_z_bot, p->bc_z_top);
     return run_steps(c, p->n_steps, hist_out);
 }
 
@@ -1083,12 +1092,13 @@ int lyd_batch_steps(lyd_ctx *c, const lyd_cloud_params *p, int32_t n_steps, lyd_
     cudaSetDevice(c->dev);
     if (n_steps < 0) return fail(c, LYD_ERR_ARG, "bad step count");
     for (int q = 0; q < c->ncl; q++) {
-        LYD_TRY(check_bcs(c, LYD_BC_REFLECT, p[q].bc_r_right, p[q].bc_z_bot, p[q].bc_z_top));
+        LYD_TRY(check_bcs(c, c->cfg.bc_r_left, p[q].bc_r_right, p[q].bc_z_bot, p[q].bc_z_top));
         if (!(p[q].c_tilde > 0.0) || !(p[q].dt > 0.0)) return fail(c, LYD_ERR_ARG, "bad step parameters");
     }
     for (int q = 0; q < c->ncl; q++) {
         CloudDesc &d = c->desc[q];
         d.c_tilde = p[q].c_tilde; d.dt = p[q].dt; d.ctdt = p[q].c_tilde * p[q].dt; d.z_center = p[q].z_center;
+        d.bc_r_left = c->cfg.bc_r_left;
         d.bc_r_right = p[q].bc_r_right; d.bc_z_bot = p[q].bc_z_bot; d.bc_z_top = p[q].bc_z_top;
     }
     return run_steps(c, n_steps, hist_out);
@@ -1314,7 +1324,7 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     if (c->ncl != 1) return fail(c, LYD_ERR_STATE, "the adjoint runs on a single-cloud context");
     if (c->prec != LYD_PREC_FP64) return fail(c, LYD_ERR_STATE, "the adjoint runs in LYD_PREC_FP64");
     if (c->aF) return fail(c, LYD_ERR_STATE, "the adjoint needs alpha_F derived from alpha and H_voigt");
-    LYD_TRY(check_bcs(c, LYD_BC_REFLECT, p->bc_r_right, p->bc_z_bot, p->bc_z_top));
+    LYD_TRY(check_bcs(c, c->cfg.bc_r_left, p->bc_r_right, p->bc_z_bot, p->bc_z_top));
     if (!(p->c_tilde > 0.0) || !(p->dt > 0.0) || p->n_steps < 1) return fail(c, LYD_ERR_ARG, "bad step parameters");
     LYD_TRY(need_inputs(c, true, true));
     const int N = p->n_steps;
@@ -1337,7 +1347,7 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     const int nr = c->nr[0], nz = c->nz[0], nnu = c->nnu;
     params_all(c, p->c_tilde, p->dt, p->c_tilde * p->dt);
     for (CloudDesc &d : c->desc) d.z_center = p->z_center;
-    bcs_all(c, p->bc_r_right, p->bc_z_bot, p->bc_z_top);
+    bcs_all(c, c->cfg.bc_r_left, p->bc_r_right, p->bc_z_bot, p->bc_z_top);
     LYD_TRY(sync_desc(c));
     if (N > c->hist_cap) {
         LYD_CU(c, cudaStreamSynchronize(c->st));
@@ -1550,6 +1560,7 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
             ad.ur_over_r = fa.ur_over_r;
             ad.g_aF = gaF; ad.g_u = g_u; ad.g_ur = g_ur; ad.g_uZ = g_uZ;
             ad.nnu = nnu; ad.nr = nr; ad.nz = nz; ad.kmin = hwin[2 * n]; ad.kmax = hwin[2 * n + 1];
+            ad.bc_r_left = c->cfg.bc_r_left;
             ad.bc_r_right = p->bc_r_right; ad.bc_z_bot = p->bc_z_bot; ad.bc_z_top = p->bc_z_top;
             ad.ctdt = p->c_tilde * p->dt; ad.jeps = c->jeps_s; ad.heps2 = c->heps2_s;
             ad.flux = c->cfg.flux_method == LYD_FLUX_HLL ? 1 : 0;

@@ -22,7 +22,7 @@ struct CloudDesc {
     int orint, ozint;    // PLM intervals per face ((n_r+1)*5, (n_z+1)*5)
     int orif, ozif;      // interface coordinates (n_r+1, n_z+1)
     int nr, nz;
-    int bc_r_right, bc_z_bot, bc_z_top;
+    int bc_r_left, bc_r_right, bc_z_bot, bc_z_top;
     int pb0, npb;        // this cloud's blocks in the frequency-kernel work list / partials
     double ctdt, dt, c_tilde, z_center;
 };

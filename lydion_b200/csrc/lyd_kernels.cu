@@ -28,14 +28,14 @@ constexpr int FREQ_THREADS = 256;
 struct View {
     long long o3, oc, orf, ozf;
     int ocol, orow, orint, ozint;
-    int nr, nz, bcr, bzb, bzt;
+    int nr, nz, bcl, bcr, bzb, bzt;
     double ctdt;
 };
 
 __device__ __forceinline__ void load_view(const CloudDesc &d, View &v) {
     v.o3 = d.o3; v.oc = d.oc; v.orf = d.orf; v.ozf = d.ozf;
     v.ocol = d.ocol; v.orow = d.orow; v.orint = d.orint; v.ozint = d.ozint;
-    v.nr = d.nr; v.nz = d.nz; v.bcr = d.bc_r_right; v.bzb = d.bc_z_bot; v.bzt = d.bc_z_top;
+    v.nr = d.nr; v.nz = d.nz; v.bcl = d.bc_r_left; v.bcr = d.bc_r_right; v.bzb = d.bc_z_bot; v.bzt = d.bc_z_top;
     v.ctdt = d.ctdt;
 }
 
@@ -50,12 +50,19 @@ __device__ __forceinline__ Cell<R> ld_cell(const AdvArgs<S> &a, const View &v, i
 }
 
 // Radial stencil cell with the ghost cells of src/AdvectJandH.jl:662-673 (axis, always
-// reflecting) and 853-871 (outer boundary, reflecting or outflow).
+// reflecting) and 853-871 (outer boundary, reflecting or outflow); on a Cartesian grid the
+// first X interface reflects or lets flow out (src/AdvectJandH.jl:1528-1545: both ghosts take
+// cell 1 with H_X = min(H_X, 0)).
 template <typename S, typename R>
 __device__ __forceinline__ Cell<R> r_cell(const AdvArgs<S> &a, const View &v, int idx, int j, int k) {
     if (idx < 0) {
-        Cell<R> c = ld_cell<S, R>(a, v, -1 - idx, j, k);
-        c.Hr = -c.Hr;
+        if (v.bcl == 0) {
+            Cell<R> c = ld_cell<S, R>(a, v, -1 - idx, j, k);
+            c.Hr = -c.Hr;
+            return c;
+        }
+        Cell<R> c = ld_cell<S, R>(a, v, 0, j, k);
+        c.Hr = c.Hr < R(0) ? c.Hr : R(0);
         return c;
     }
     if (idx >= v.nr) {

@@ -50,6 +50,7 @@ class CylGeometry:
     inv_dZ_jp1_j: np.ndarray
     inv_dZ_jp2_jp1: np.ndarray
     dZ_b: np.ndarray
+    cartesian: bool = False   # GeometryCartesian: r, Z stand for X, Y
 
     @property
     def nr(self):
@@ -123,6 +124,32 @@ def cylindrical_geometry(r, Z):
                        inv_r_cell=inv_r_cell, dr_L=rL, dr_R=rR, inv_dr_i_im1=ra, inv_dr_ip1_i=rb,
                        inv_dr_ip2_ip1=rc, dr_b=rbnd, dZ_L=zL, dZ_R=zR, inv_dZ_j_jm1=za,
                        inv_dZ_jp1_j=zb, inv_dZ_jp2_jp1=zc, dZ_b=zbnd)
+
+
+def cartesian_geometry(X, Y):
+    """GeometryCartesian from interface coordinates (SetupCartesianGrid, src/SpatialGrid.jl:1349-1440):
+    cell centres at the midpoints, dV = dX dY, A_X = dY and A_Y = dX per unit depth
+    (src/SpatialGrid.jl:1061-1135), the same PLM intervals as the cylindrical Z coordinate
+    (Compute_Grid_Differences!), and no <1/r>. Stored in the cylindrical field names (r = X,
+    Z = Y)."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    Y = np.ascontiguousarray(Y, dtype=np.float64)
+    nx, ny = X.size - 1, Y.size - 1
+    if nx < 3 or ny < 3:
+        raise ValueError("the M1 stencil needs N_X >= 3 and N_Y >= 3")
+    XC = 0.5 * (X[:-1] + X[1:])
+    YC = 0.5 * (Y[:-1] + Y[1:])
+    dX = X[1:] - X[:-1]
+    dY = Y[1:] - Y[:-1]
+    dV = dX[None, :] * dY[:, None]
+    A_r = np.broadcast_to(dY[:, None], (ny, nx + 1)).copy()
+    A_Z = np.broadcast_to(dX[None, :], (ny + 1, nx)).copy()
+    rL, rR, ra, rb, rc, rbnd = grid_differences(X, XC)
+    zL, zR, za, zb, zc, zbnd = grid_differences(Y, YC)
+    return CylGeometry(r=X, Z=Y, rCoM=XC, ZCoM=YC, dV=dV, inv_dV=1.0 / dV, A_r=A_r, A_Z=A_Z,
+                       inv_r_cell=np.zeros(nx), dr_L=rL, dr_R=rR, inv_dr_i_im1=ra, inv_dr_ip1_i=rb,
+                       inv_dr_ip2_ip1=rc, dr_b=rbnd, dZ_L=zL, dZ_R=zR, inv_dZ_j_jm1=za,
+                       inv_dZ_jp1_j=zb, inv_dZ_jp2_jp1=zc, dZ_b=zbnd, cartesian=True)
 
 
 def uniform_cylindrical_geometry(rmax, zmax, nr, nz):

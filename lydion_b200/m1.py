@@ -22,12 +22,14 @@ class M1Context:
     """One Lyman-alpha state on one GPU (see include/lydion_m1.h)."""
 
     def __init__(self, n_nu, n_r, n_z, kcore_min, kcore_max, alpha_floor, recoil=True, flux_method=0,
-                 precision=PREC_FP64, keep_freq_factors=False, j_scale=0.0, device=0):
+                 precision=PREC_FP64, keep_freq_factors=False, j_scale=0.0, device=0, cartesian=False,
+                 bc_r_left=BC_REFLECT):
         self.n_nu, self.n_r, self.n_z = int(n_nu), int(n_r), int(n_z)
         self.precision = precision
         dims = _lib.Dims(self.n_nu, self.n_r, self.n_z, 0)
         cfg = _lib.Config(int(flux_method), int(bool(recoil)), int(precision), int(kcore_min), int(kcore_max),
-                          int(bool(keep_freq_factors)), float(alpha_floor), float(j_scale), int(device))
+                          int(bool(keep_freq_factors)), float(alpha_floor), float(j_scale), int(device),
+                          _lib.GEOM_CARTESIAN if cartesian else _lib.GEOM_CYLINDRICAL, int(bc_r_left))
         h = C.c_void_p()
         check(lib().lyd_create(C.byref(h), C.byref(dims), C.byref(cfg)))
         self._h = h
@@ -411,13 +413,17 @@ def context_for_cloud(cloud, precision=PREC_FP64, device=0, keep_freq_factors=Fa
     phi_nu is derived on the device over the core bins (lyd_update_phi_nu) unless given;
     alpha_F is alpha*H_voigt (+ alpha_cF) unless given."""
     fq = cloud.freq
+    cart = bool(getattr(cloud.geom, "cartesian", False))
     ctx = M1Context(cloud.n_nu, cloud.nr, cloud.nz, fq.kcore_min, fq.kcore_max, cloud.alpha_floor,
                     recoil=cloud.recoil, flux_method=cloud.flux_method, precision=precision,
-                    keep_freq_factors=keep_freq_factors, j_scale=j_scale, device=device)
+                    keep_freq_factors=keep_freq_factors, j_scale=j_scale, device=device, cartesian=cart,
+                    bc_r_left=getattr(cloud, "bc_r_left", BC_REFLECT))
     ctx.set_geometry(cloud.geom)
     ctx.set_freq_grid(fq)
     for name in ("alpha", "alpha_c", "pd", "js", "T", "dur_dr", "dur_dZ", "duZ_dr", "duZ_dZ", "ur_over_r",
                  "u_r_star", "u_Z_star"):
+        if cart and name == "ur_over_r":
+            continue            # no u_r / r term on a Cartesian grid
         ctx.upload(name, getattr(cloud, name))
     if getattr(cloud, "species", None):
         # destruction probability from the cell's species densities, on the device (pd_Lya)

@@ -59,6 +59,7 @@ class StaticCloud:
     n_H: np.ndarray = None       # hydrogen density behind alpha (x_HI = 1), when the cloud is built from one
     kappa_d: float = 0.0         # gray dust opacity per gram of dust behind alpha_c = kappa_d * 0.01 n_H m_H
     species: dict = None         # n_HII, n_e, n_HI, n_HeI, n_H2 per cell: pd is then computed on the device
+    bc_r_left: int = BC_REFLECT  # first r (X) interface: the axis (cylindrical) or either rule (Cartesian)
 
     @property
     def n_nu(self):
@@ -339,3 +340,25 @@ def rhd_gas_state(cloud, seed):
     rho_d = np.stack([rho, 0.5 * rho, 0.05 * rho])
     rho_d[0][rng.uniform(size=shape) < 0.2] = 0.5 * DUST_RHO_IGNORE
     return sp, rho_d
+
+
+def cartesian_cloud(nx=12, ny=10, n_nu=16, bc_left=BC_OUTFLOW, seed=3, **kw):
+    """A small cloud on a Cartesian (X, Y) grid: the fields of small_cloud moved onto a uniform
+    Cartesian grid over the same extent, with seeded velocity gradients, no u_r / r term, and the
+    chosen boundary at the first X interface. For parity tests of the Cartesian advection."""
+    from .grid import cartesian_geometry, julia_linrange
+    cl = small_cloud(nr=nx, nz=ny, n_nu=n_nu, **kw)
+    g = cl.geom
+    geom = cartesian_geometry(julia_linrange(-g.r[-1], g.r[-1], nx + 1), julia_linrange(0.0, g.Z[-1], ny + 1))
+    rng = np.random.default_rng(seed)
+    shape = (ny, nx)
+    scale = 1e5 / K.pc
+    cl.geom = geom
+    cl.bc_r_left = bc_left
+    cl.ur_over_r = np.zeros(shape)
+    for name in ("dur_dr", "dur_dZ", "duZ_dr", "duZ_dZ"):
+        setattr(cl, name, scale * rng.normal(size=shape))
+    cl.u_r_star = 1e6 * rng.normal(size=(ny, nx + 1))
+    cl.u_Z_star = 1e6 * rng.normal(size=(ny + 1, nx))
+    cl.name = "cartesian"
+    return cl

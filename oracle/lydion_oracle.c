@@ -335,9 +335,14 @@ void orc_advect_jh(orc_lya *s, const orc_geom *g, const orc_vel *v, double ctdt,
             double Hr1 = Hr[I3(k, 0, j)], Hr2 = Hr[I3(k, 1, j)];
             double HZ1 = HZ[I3(k, 0, j)], HZ2 = HZ[I3(k, 1, j)];
             double aF1 = aF[I3(k, 0, j)];
-            /* axis ghost cells (always reflecting), src/AdvectJandH.jl:662-673 */
+            /* axis ghost cells (always reflecting), src/AdvectJandH.jl:662-673; on a Cartesian
+             * grid the first interface may let flow out instead (:1537-1545) */
             double J0 = J1, Hr0 = -Hr1, HZ0 = HZ1;
             double Jm1 = J2, Hrm1 = -Hr2, HZm1 = HZ2;
+            if (g->bc_r_left == ORC_BC_OUTFLOW) {
+                Hr0 = dmin(Hr1, 0.0);
+                Jm1 = J0; Hrm1 = Hr0; HZm1 = HZ0;
+            }
             recon q = reconstruct(J0, J1, J2, Jm1, Hr0, Hr1, Hr2, Hrm1, HZ0, HZ1, HZ2, HZm1,
                                   g->dr_b[0], g->dr_b[1], g->dr_b[2], g->dr_b[3], g->dr_b[4], aF1, aF1);
             double Fo[3], kL, kR;

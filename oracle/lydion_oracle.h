@@ -50,6 +50,10 @@ typedef struct orc_geom {
     double dr_b[10];
     const double *dZ_L, *dZ_R, *inv_dZ_j_jm1, *inv_dZ_jp1_j, *inv_dZ_jp2_jp1;
     double dZ_b[10];
+    /* boundary at the first r interface: ORC_BC_REFLECT (the axis of a cylindrical grid) or,
+     * on a Cartesian grid (inv_r_cell = 0, u_r/r = 0; src/AdvectJandH.jl:1396-2222),
+     * ORC_BC_OUTFLOW */
+    int bc_r_left;
 } orc_geom;
 
 /* The Lyman-alpha state, mirrors LyaArrays{FluxMethod} (src/Structs.jl:23-124). */

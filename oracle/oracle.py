@@ -41,7 +41,7 @@ class Geom(C.Structure):
                 ("dr_L", P), ("dr_R", P), ("inv_dr_i_im1", P), ("inv_dr_ip1_i", P), ("inv_dr_ip2_ip1", P),
                 ("dr_b", C.c_double * 10),
                 ("dZ_L", P), ("dZ_R", P), ("inv_dZ_j_jm1", P), ("inv_dZ_jp1_j", P), ("inv_dZ_jp2_jp1", P),
-                ("dZ_b", C.c_double * 10)]
+                ("dZ_b", C.c_double * 10), ("bc_r_left", C.c_int)]
 
 
 class Lya(C.Structure):
@@ -147,7 +147,7 @@ class OracleLUT:
         return C.byref(self.s)
 
 
-def geom_struct(geom):
+def geom_struct(geom, bc_r_left=0):
     keep = []
 
     def q(a):
@@ -159,7 +159,7 @@ def geom_struct(geom):
              q(geom.A_r), q(geom.A_Z), q(geom.inv_r_cell), q(geom.dr_L), q(geom.dr_R), q(geom.inv_dr_i_im1),
              q(geom.inv_dr_ip1_i), q(geom.inv_dr_ip2_ip1), (C.c_double * 10)(*geom.dr_b),
              q(geom.dZ_L), q(geom.dZ_R), q(geom.inv_dZ_j_jm1), q(geom.inv_dZ_jp1_j), q(geom.inv_dZ_jp2_jp1),
-             (C.c_double * 10)(*geom.dZ_b))
+             (C.c_double * 10)(*geom.dZ_b), int(bc_r_left))
     return g, keep
 
 
@@ -196,7 +196,7 @@ class OracleState:
                      int(cloud.recoil), int(cloud.flux_method), float(cloud.alpha_floor),
                      _p(self.F_r), _p(self.F_Z), _p(self.F_r_Hr), _p(self.F_Z_Hr), _p(self.F_r_HZ), _p(self.F_Z_HZ),
                      _p(self.K_iph), _p(self.K_imh), _p(self.Fkp), _p(self.Fk), _p(self.Fkm))
-        self.g, self._gkeep = geom_struct(cloud.geom)
+        self.g, self._gkeep = geom_struct(cloud.geom, getattr(cloud, "bc_r_left", 0))
         self._vel = [np.ascontiguousarray(a, dtype=np.float64) for a in
                      (cloud.u_r_star, cloud.u_Z_star, cloud.dur_dr, cloud.dur_dZ, cloud.duZ_dr, cloud.duZ_dZ,
                       cloud.ur_over_r)]
