@@ -348,6 +348,18 @@ typedef struct lyd_rhd_lya_out {
  * (:3197-3206) and rejected cells get J = J_old, H = H_old back (RestoreLyaRejection, :980-991). */
 int  lyd_rhd_lya_absorb(lyd_ctx *ctx, const double *dt, double c_tilde, int32_t commit, lyd_rhd_lya_out *out);
 
+/* FindRSL_LyaRT, src/PhotoChemistryAndCooling/PhotoThermoChemistry.jl:614-711: the reduced speed
+ * of light the Lya transport needs from the hydro and chemistry state, a maximum over the cells
+ * (single-cloud contexts). Host arrays of n_r*n_z: cell velocities u_r, u_Z (cm/s), pressure,
+ * density, adiabatic index, T, x_HII, x_H2, and rho_d[3][n_r*n_z]; the context supplies the cell
+ * widths (lyd_set_geometry) and pd (lyd_rhd_lya_prepare or an upload). eps_rsl is the reference's
+ * eps_RSL (4), X_over_mH the hydrogen mass fraction over m_H. The result is clamped to
+ * [c_tilde_min, c], and to [0.75, 4] times c_tilde_old. */
+int  lyd_find_rsl_lya(lyd_ctx *ctx, double c_tilde_old, double c_tilde_min, const double *u_r, const double *u_Z,
+                      const double *P, const double *rho, const double *gamma_ad, const double *T,
+                      const double *xHII, const double *xH2, const double *rho_d, const lyd_dust_lya *dust,
+                      double eps_rsl, double X_over_mH, double *c_tilde_new);
+
 /* The five Voigt look-up tables the device evaluates (CreateVoigtLUTs,
  * src/FastInterpolations.jl:178-197): erf, Dawson's integral, exp(-x^2), x exp(-x^2) and
  * (1-2x^2) exp(-x^2) at x_i = -xmax + 2 xmax i/(n-1), written to out[5*n] table after table.

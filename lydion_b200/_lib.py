@@ -134,6 +134,7 @@ SIGNATURES = {
     "lyd_pd_lya": (C.c_int, [VP, SZ, P, P, P, P, P, P, D, P]),
     "lyd_rhd_lya_prepare": (C.c_int, [VP, P, P, P, P, P, P, P, P, P, C.POINTER(DustLya), D, I32, I32]),
     "lyd_rhd_lya_absorb": (C.c_int, [VP, P, D, I32, C.POINTER(RhdLyaOut)]),
+    "lyd_find_rsl_lya": (C.c_int, [VP, D, D, P, P, P, P, P, P, P, P, P, C.POINTER(DustLya), D, D, P]),
     "lyd_cfl_dt": (C.c_int, [VP, D, P, P, D, P]),
     "lyd_edge_count": (C.c_int, [I32, I32]),
     "lyd_edge_spectra": (C.c_int, [VP, P, P, C.POINTER(I32), C.POINTER(I32)]),

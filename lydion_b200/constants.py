@@ -20,6 +20,12 @@ h = 6.626069573e-27
 kB = 1.380648813e-16
 mu = 1.660539069e-24
 mH = 1.0080 * mu
+mD = 2.014 * mu
+# pristine-gas mass fractions, src/ConstantsAndFunctions.jl:124-127
+Y_He = 0.247
+D_H_ratio = 2.53e-5
+X_D = D_H_ratio * (1 - Y_He) * mD / mH
+X_H = 1 - Y_He - X_D
 me = 9.109382917e-28
 e = 4.80320451e-10
 nu_lya = 2.466068e15

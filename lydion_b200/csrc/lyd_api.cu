@@ -1230,6 +1230,45 @@ int lyd_rhd_lya_absorb(lyd_ctx *c, const double *dt, double c_tilde, int32_t com
     return check_err(c);
 }
 
+int lyd_find_rsl_lya(lyd_ctx *c, double ct_old, double ct_min, const double *u_r, const double *u_Z, const double *P,
+                     const double *rho, const double *gamma_ad, const double *T, const double *xHII,
+                     const double *xH2, const double *rho_d, const lyd_dust_lya *dust, double eps_rsl,
+                     double X_over_mH, double *ct_new) {
+    if (!c) return LYD_ERR_ARG;
+    if (!u_r || !u_Z || !P || !rho || !gamma_ad || !T || !xHII || !xH2 || !rho_d || !dust || !ct_new)
+        return fail(c, LYD_ERR_ARG, "null argument");
+    LYD_TRY(single_cloud(c, "lyd_find_rsl_lya"));
+    cudaSetDevice(c->dev);
+    if (!all_have(c, BIT_GEOM)) return fail(c, LYD_ERR_STATE, "geometry not set");
+    if (!all_have(c, 1u << CF_PD)) return fail(c, LYD_ERR_STATE, "pd not set (lyd_rhd_lya_prepare or an upload)");
+    const size_t nc = c->ncell;
+    LYD_TRY(ensure_stage(c, 11 * nc + 1));
+    double *d = c->stage;
+    const double *src[8] = {u_r, u_Z, P, rho, gamma_ad, T, xHII, xH2};
+    for (int q = 0; q < 8; q++) LYD_TRY(h2d(c, d + q * nc, src[q], nc));
+    LYD_TRY(h2d(c, d + 8 * nc, rho_d, 3 * nc));
+    RslArgs a;
+    memset(&a, 0, sizeof(a));
+    a.r_if = c->r_if; a.Z_if = c->Z_if;
+    a.u_r = d; a.u_Z = d + nc; a.P = d + 2 * nc; a.rho = d + 3 * nc; a.gamma = d + 4 * nc; a.T = d + 5 * nc;
+    a.xHII = d + 6 * nc; a.xH2 = d + 7 * nc; a.rho_d = d + 8 * nc; a.pd = c->cellf[CF_PD];
+    for (int q = 0; q < 3; q++) a.kabs[q] = dust->kappa_abs[q];
+    a.eps_rsl = eps_rsl; a.X_over_mH = X_over_mH; a.nr = c->nr[0]; a.ncell = nc;
+    a.out = reinterpret_cast<unsigned long long *>(d + 11 * nc);
+    launch_rsl(a, c->st);
+    LYD_CU(c, cudaGetLastError());
+    double m = 0.0;
+    LYD_CU(c, cudaMemcpyAsync(&m, a.out, 8, cudaMemcpyDeviceToHost, c->st));
+    LYD_CU(c, cudaStreamSynchronize(c->st));
+    // clamps and the limits on the change from the previous value (:697-711)
+    double v = m < ct_min ? ct_min : m;
+    v = v < kC ? v : kC;
+    if (v < ct_old) v = v > 0.75 * ct_old ? v : 0.75 * ct_old;
+    if (v > ct_old) v = v < 4.0 * ct_old ? v : 4.0 * ct_old;
+    *ct_new = v;
+    return check_err(c);
+}
+
 int lyd_pd_lya(lyd_ctx *c, size_t n, const double *nHII, const double *ne, const double *nHI, const double *nHeI,
                const double *nH2, const double *T, double z, double *out) {
     if (!c || !out || !nHII || !ne || !nHI || !nHeI || !nH2 || !T) return LYD_ERR_ARG;

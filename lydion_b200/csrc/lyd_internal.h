@@ -175,7 +175,16 @@ struct RhdAbsorbArgs {
     int nnu, commit;
     size_t ncell;
 };
+struct RslArgs {
+    const double *r_if, *Z_if;                 // interface coordinates
+    const double *u_r, *u_Z, *P, *rho, *gamma, *T, *xHII, *xH2, *rho_d, *pd;   // rho_d: [3][ncell]
+    double kabs[3], eps_rsl, X_over_mH;
+    int nr;
+    size_t ncell;
+    unsigned long long *out;                   // bits of the maximum (non-negative double)
+};
 void launch_rhd_prep(const RhdPrepArgs &a, cudaStream_t st);
+void launch_rsl(const RslArgs &a, cudaStream_t st);
 void launch_rhd_absorb(int sprec, const void *args, cudaStream_t st);
 
 }  // namespace lyd

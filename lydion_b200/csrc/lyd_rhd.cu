@@ -138,6 +138,47 @@ __global__ void k_rhd_absorb(RhdAbsorbArgs<S> a) {
     }
 }
 
+// FindRSL_LyaRT, src/PhotoChemistryAndCooling/PhotoThermoChemistry.jl:614-711: per cell the
+// speed eps_RSL max(1, (a tau)^(1/3) f_abs) max(|u|, c_s) that keeps the Lya transport accurate,
+// with tau = alpha max(dr, dZ) and f_abs = 1 / (1 + (a tau)^(1/3) tau_c + 0.6 pd tau); the
+// maximum over the cells goes to *out (non-negative doubles order like their bit patterns).
+__global__ void k_rsl(RslArgs a) {
+    double m = 0.0;
+    for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < a.ncell; c += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % a.nr), j = (int)(c / a.nr);
+        const double dr = a.r_if[i + 1] - a.r_if[i], dz = a.Z_if[j + 1] - a.Z_if[j];
+        const double rho = a.rho[c], T = a.T[c];
+        const double cs = sqrt(a.gamma[c] * a.P[c] / rho);
+        double xHI = 1.0 - a.xHII[c] - 2.0 * a.xH2[c];
+        xHI = xHI > 0.0 ? xHI : 0.0;
+        const double nHI = xHI * a.X_over_mH * rho;
+        const double alpha = nHI * compute_sigma0(T);
+        const double dX = dr > dz ? dr : dz;
+        const double tau = alpha * dX;
+        const double tauc = (a.kabs[0] * a.rho_d[c] + a.kabs[1] * a.rho_d[a.ncell + c] +
+                             a.kabs[2] * a.rho_d[2 * a.ncell + c]) * dX;
+        const double at = compute_a(T) * tau;
+        const double at13 = pow(at, 1.0 / 3.0);
+        const double fabs_ = 1.0 / (1.0 + at13 * tauc + 0.6 * a.pd[c] * tau);
+        const double u = hypot(a.u_r[c], a.u_Z[c]);
+        const double f = at13 * fabs_;
+        const double v = a.eps_rsl * (f > 1.0 ? f : 1.0) * (u > cs ? u : cs);
+        m = v > m ? v : m;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double w = __shfl_xor_sync(0xffffffffu, m, o);
+        m = w > m ? w : m;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMax(a.out, (unsigned long long)__double_as_longlong(m));
+}
+
+void launch_rsl(const RslArgs &a, cudaStream_t st) {
+    cudaMemsetAsync(a.out, 0, 8, st);
+    const size_t g = (a.ncell + 255) / 256;
+    k_rsl<<<(int)(g < 1184 ? (g > 0 ? g : 1) : 1184), 256, 0, st>>>(a);
+}
+
 void launch_rhd_absorb(int sprec, const void *args, cudaStream_t st) {
     const int blocks = 148 * 8;
     if (sprec == 0) k_rhd_absorb<double><<<blocks, 256, 0, st>>>(*static_cast<const RhdAbsorbArgs<double> *>(args));

@@ -273,6 +273,20 @@ class M1Context:
         r["split"] = split.reshape((8,) + shape)
         return r
 
+    def find_rsl_lya(self, c_tilde_old, c_tilde_min, u_r, u_Z, P, rho, gamma_ad, T, xHII, xH2, rho_d, kappa_abs,
+                     eps_rsl=4.0, X_over_mH=None):
+        """FindRSL_LyaRT (lyd_find_rsl_lya): the reduced speed of light the Lya transport needs."""
+        from . import constants as K
+        if X_over_mH is None:
+            X_over_mH = K.X_H / K.mH
+        arrs = [_c64(np.ravel(a)) for a in (u_r, u_Z, P, rho, gamma_ad, T, xHII, xH2)]
+        rho = _c64(np.reshape(rho_d, (3, -1)))
+        d = _lib.DustLya((C.c_double * 3)(*kappa_abs), (C.c_double * 3)(0.0, 0.0, 0.0), 0.0)
+        out = C.c_double()
+        self._ck(lib().lyd_find_rsl_lya(self._h, float(c_tilde_old), float(c_tilde_min), *[_dp(a) for a in arrs],
+                                        _dp(rho), C.byref(d), float(eps_rsl), float(X_over_mH), C.byref(out)))
+        return out.value
+
     def cfl_dt(self, c_tilde, u_r, u_Z, cfl):
         a, b = _c64(u_r), _c64(u_Z)
         out = C.c_double()

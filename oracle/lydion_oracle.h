@@ -164,6 +164,12 @@ int    orc_rhd_lya_absorb_cell(int nnu, const double *dnu, const double *Hv, con
                                const double cell[8], double dt, double c_tilde, double e_old, double jeps,
                                double out[13]);
 
+double orc_find_rsl_lya(int nr, int nz, const double *r, const double *Z, const double *u_r, const double *u_Z,
+                        const double *P, const double *rho, const double *gamma_ad, const double *T,
+                        const double *xHII, const double *xH2, const double *rho_d, const double *pd,
+                        const double kappa_abs[3], double eps_rsl, double X_over_mH, double ct_old,
+                        double ct_min);
+
 int    orc_num_threads(void);
 void   orc_set_num_threads(int n);
 

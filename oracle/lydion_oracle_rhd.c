@@ -179,3 +179,41 @@ int orc_rhd_lya_absorb_cell(int nnu, const double *dnu, const double *Hv, const 
     out[12] = dt_lya;
     return ((de > TOL_ABS && dt > TOL_ABS * dt_lya) || !isfinite(de)) ? 1 : 0;
 }
+
+/* FindRSL_LyaRT, src/PhotoChemistryAndCooling/PhotoThermoChemistry.jl:614-711, on a single
+ * cloud: cell arrays of nr*nz (i fastest), rho_d [3][nr*nz], interfaces r (nr+1) and Z (nz+1). */
+double orc_find_rsl_lya(int nr, int nz, const double *r, const double *Z, const double *u_r, const double *u_Z,
+                        const double *P, const double *rho, const double *gamma_ad, const double *T,
+                        const double *xHII, const double *xH2, const double *rho_d, const double *pd,
+                        const double kappa_abs[3], double eps_rsl, double X_over_mH, double ct_old,
+                        double ct_min) {
+    const size_t n = (size_t)nr * nz;
+    double ct = 0.0;
+    for (int j = 0; j < nz; j++) {
+        const double dZ = Z[j + 1] - Z[j];
+        for (int i = 0; i < nr; i++) {
+            const size_t c = (size_t)i + (size_t)nr * j;
+            const double dr = r[i + 1] - r[i];
+            const double cs = sqrt(gamma_ad[c] * P[c] / rho[c]);
+            double xHI = 1.0 - xHII[c] - 2.0 * xH2[c];
+            xHI = xHI > 0.0 ? xHI : 0.0;
+            const double nHI = xHI * X_over_mH * rho[c];
+            const double alpha = nHI * orc_compute_sigma0(T[c]);
+            const double dX = dr > dZ ? dr : dZ;
+            const double tau = alpha * dX;
+            const double tauc = (kappa_abs[0] * rho_d[c] + kappa_abs[1] * rho_d[n + c] + kappa_abs[2] * rho_d[2 * n + c]) * dX;
+            const double at = orc_compute_a(T[c]) * tau;
+            const double at13 = pow(at, 1.0 / 3.0);
+            const double fabs_ = 1.0 / (1.0 + at13 * tauc + 0.6 * pd[c] * tau);
+            const double u = hypot(u_r[c], u_Z[c]);
+            const double f = at13 * fabs_;
+            const double v = eps_rsl * (f > 1.0 ? f : 1.0) * (u > cs ? u : cs);
+            ct = v > ct ? v : ct;
+        }
+    }
+    ct = ct < ct_min ? ct_min : ct;
+    ct = ct < R_C_LIGHT ? ct : R_C_LIGHT;
+    if (ct < ct_old) ct = ct > 0.75 * ct_old ? ct : 0.75 * ct_old;
+    if (ct > ct_old) ct = ct < 4.0 * ct_old ? ct : 4.0 * ct_old;
+    return ct;
+}

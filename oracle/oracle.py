@@ -101,6 +101,7 @@ def _declare(L):
         "orc_js_rec_lya": (D, [D, D, D, I]), "orc_js_coll_lya": (D, [D, D, D]),
         "orc_rhd_lya_prepare_cell": (None, [P, C.c_void_p, D, I, I, P]),
         "orc_rhd_lya_absorb_cell": (I, [I, P, P, P, P, P, P, P, P, P, P, D, D, D, D, P]),
+        "orc_find_rsl_lya": (D, [I, I] + [P] * 13 + [D, D, D, D]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -370,3 +371,16 @@ def rhd_lya_absorb(state, acF, dF, dt, c_tilde, e_lya, jeps=1e-60, commit=False)
                     state.J_old[j, i], state.H_r_old[j, i], state.H_Z_old[j, i] = J, Hr, HZ
                     e_lya[j, i] = out[0]
     return res
+
+
+def find_rsl_lya(geom, hydro, rho_d, pd, kappa_abs, eps_rsl, X_over_mH, ct_old, ct_min):
+    """FindRSL_LyaRT on one cloud: hydro holds u_r, u_Z, P, rho, gamma_ad, T, xHII, xH2 ((n_z, n_r) each)."""
+    a = [np.ascontiguousarray(hydro[k], dtype=np.float64) for k in
+         ("u_r", "u_Z", "P", "rho", "gamma_ad", "T", "xHII", "xH2")]
+    rd = np.ascontiguousarray(rho_d, dtype=np.float64)
+    pdc = np.ascontiguousarray(pd, dtype=np.float64)
+    ka = np.ascontiguousarray(kappa_abs, dtype=np.float64)
+    r = np.ascontiguousarray(geom.r, dtype=np.float64)
+    Z = np.ascontiguousarray(geom.Z, dtype=np.float64)
+    return lib().orc_find_rsl_lya(geom.nr, geom.nz, _p(r), _p(Z), *[_p(x) for x in a], _p(rd), _p(pdc), _p(ka),
+                                  float(eps_rsl), float(X_over_mH), float(ct_old), float(ct_min))

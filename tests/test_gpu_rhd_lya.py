@@ -101,3 +101,27 @@ def test_absorb_needs_prepare():
     with pytest.raises(LydionError):
         ctx.rhd_lya_absorb(np.full((cl.nz, cl.nr), 1e3), C_TILDE)
     ctx.close()
+
+
+# (previous c~, c~_min): the cell maximum (~5.3e8 cm/s here) unclamped, capped at 4x the previous
+# value, floored at 0.75x, and raised to c~_min
+@pytest.mark.parametrize("ct_old,ct_min", [(3e8, 1e7), (1e7, 1e7), (3e9, 1e7), (1e9, 1e9)])
+def test_find_rsl_matches_oracle(ct_old, ct_min):
+    """FindRSL_LyaRT on the device against the oracle, on the seeded gas state with random flows
+    and pressures, through each of its clamps."""
+    from oracle import oracle as O
+    cl, st, ctx, acF, dF, _ = matched(PREC_FP64, 31)
+    rng = np.random.default_rng(9)
+    shape = (cl.nz, cl.nr)
+    sp, rho_d = W.rhd_gas_state(cl, 31)
+    from lydion_b200 import constants as K
+    nH = sp["nHI"] + sp["nHII"]
+    hydro = {"u_r": 1e6 * rng.normal(size=shape), "u_Z": 1e6 * rng.normal(size=shape),
+             "rho": nH * K.mH / K.X_H, "gamma_ad": np.full(shape, 5.0 / 3.0), "T": sp["T"],
+             "xHII": sp["nHII"] / nH, "xH2": 0.5 * sp["nH2"] / nH}
+    hydro["P"] = 2.0 * nH * K.kB * sp["T"] * rng.uniform(0.5, 2.0, size=shape)
+    ref = O.find_rsl_lya(cl.geom, hydro, rho_d, st.pd, KAPPA_ABS, 4.0, K.X_H / K.mH, ct_old, ct_min)
+    got = ctx.find_rsl_lya(ct_old, ct_min, hydro["u_r"], hydro["u_Z"], hydro["P"], hydro["rho"], hydro["gamma_ad"],
+                           hydro["T"], hydro["xHII"], hydro["xH2"], rho_d, KAPPA_ABS)
+    assert abs(got - ref) <= 1e-13 * ref, (got, ref)
+    ctx.close()
