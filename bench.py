@@ -341,6 +341,40 @@ def c5_form(args, stream_of, local):
     return out
 
 
+def dd_form(args, stream_of, local, world, rank):
+    """The 1024 x 1024 x 128 field split into Z slabs over the ranks (lydion_b200.domain; one
+    slab per GPU, halo rows exchanged and reduction columns all-reduced through torch.distributed),
+    mixed precision, strong scaling: the whole field's cell-bin updates over the slowest rank's
+    device time."""
+    import torch
+    from lydion_b200 import domain as D
+    from lydion_b200 import sharding
+    from lydion_b200 import workloads as W
+    from lydion_b200._lib import PREC_MIXED
+    cl = W.config_c5()
+    p = (cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+    steps = max(3, min(10, args.steps // 300))
+    r = D.SlabRank(cl, world, rank, precision=PREC_MIXED, device=local)
+    drv = D.SlabDriver([r], D.TorchComm() if world > 1 else D.LocalComm())
+    drv.find_active()
+    for _ in range(2):
+        drv.step(*p)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        drv.step(*p)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = sharding.max_over_ranks(e0.elapsed_time(e1), device="cuda")
+    r.ctx.close()
+    return {"workload": "c5_rhd_snapshot_1024x1024x128_zslabs", "ranks": world, "rows_per_rank": r.j1 - r.j0,
+            "steps": steps, "precision": "mixed", "scaling": "strong",
+            "value": steps * cl.cell_bins / (ms * 1e-3), "ms_per_step": ms / steps}
+
+
 def adjoint_form(args, stream_of, local):
     """Adjoint over forward cost on the turbulent cloud (128 x 128 x 48, lognormal n_H, dust,
     v_max = 50 km/s): N forward steps from the graph-replayed step against lyd_adjoint_run of
@@ -409,6 +443,7 @@ def run_gpu(args):
     adj = None if (args.no_adjoint or world > 1) else adjoint_form(args, stream_of, local)
     c5 = None if (args.no_c5 or world > 1) else c5_form(args, stream_of, local)
     rhd = None if (args.no_rhd or world > 1) else rhd_form(args, stream_of, local)
+    dd = dd_form(args, stream_of, local, world, rank) if args.dd_field else None
 
     # roofline of the dominant kernel of the headline (mixed) form
     names = ["advect", "freq", "reduce"]
@@ -438,6 +473,7 @@ def run_gpu(args):
                 "adjoint": adj,
                 "largest_field": c5,
                 "rhd_lya_block": rhd,
+                "largest_field_zslabs": dd,
                 "batch": batch,
                 "roofline": {"bound": "hbm", "kernel": "k_" + names[dom], "achieved": achieved,
                              "peak": peaks["hbm_gbs"], "peak_source": src, "unit": "GB/s",
@@ -470,6 +506,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of the autotuner")
     ap.add_argument("--no-c5", action="store_true", help="skip the 1024x1024x128 field")
     ap.add_argument("--no-rhd", action="store_true", help="skip the RHD-side Lyman-alpha block")
+    ap.add_argument("--dd-field", action="store_true",
+                    help="also step the 1024x1024x128 field split into Z slabs over the ranks (strong scaling)")
     ap.add_argument("--only-mixed", action="store_true", help="measure the mixed-precision form only")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -307,6 +307,30 @@ int  lyd_cfl_dt(lyd_ctx *ctx, double c_tilde, const double *u_r, const double *u
  * n_edge = (n_z-2) + 2*(n_r-3) cells; raw and normalised are (n_edge, n_nu) row-major. */
 int  lyd_edge_count(int32_t n_r, int32_t n_z);
 int  lyd_edge_spectra(lyd_ctx *ctx, double *raw, double *norm, int32_t *r_index, int32_t *z_index);
+/* ---- Z-slab domain decomposition of one field --------------------------------------------------
+ * One large field split into slabs of rows over ranks (one GPU each). A rank's context holds its
+ * rows plus two halo rows on each side that has a neighbour; its geometry, frequency grid and
+ * per-cell inputs are the global ones sliced to those rows. Per step, with the communication done
+ * by the caller (all-reduce of the column sums, exchange of the halo rows; e.g. NCCL through
+ * torch.distributed) on buffers in device memory:
+ *   lyd_dd_step_partials -> all-reduce(colsum) -> lyd_dd_finish -> lyd_dd_halo(pack) ->
+ *   exchange -> lyd_dd_halo(unpack)
+ * and once before the first step lyd_dd_find_active_partials -> all-reduce -> lyd_dd_finish(step
+ * = 0). The advection updates only the owned rows; its stencil reads the halo rows; the
+ * frequency step, FindActiveBins and the diagnostics run on the owned cells, and the window and
+ * diagnostics come from the all-reduced sums, so every rank takes the same window. There is no
+ * counterpart in the reference, which runs one field on one node. */
+int  lyd_dd_set_halo(lyd_ctx *ctx, int32_t h_bot, int32_t h_top);   /* 0 or 2 rows each */
+int  lyd_dd_columns(lyd_ctx *ctx);   /* length of the column-sum vector (n_nu + 6 doubles) */
+int  lyd_dd_find_active_partials(lyd_ctx *ctx, double *colsum_dev);
+int  lyd_dd_step_partials(lyd_ctx *ctx, const lyd_step_params *p, double *colsum_dev);
+/* the window of the next step from the all-reduced sums, and with step != 0 the step's record */
+int  lyd_dd_finish(lyd_ctx *ctx, const double *colsum_dev, int32_t step, lyd_diag *rec);
+/* side 0: lower neighbour, 1: upper; pack copies the two owned rows next to that neighbour, unpack
+ * fills the two halo rows; buf_dev holds J, H_r, H_Z of two rows (6 n_r n_nu values in the
+ * storage type: 8 bytes in FP64 and mixed, 4 in FP32). */
+int  lyd_dd_halo(lyd_ctx *ctx, int32_t side, int32_t pack, void *buf_dev);
+
 /* ---- RHD-side Lyman-alpha block ---------------------------------------------------------------
  * The Lya part of the per-cell photo-thermochemistry sub-cycle of the RHD drivers, on the device
  * for every cell of the context at once, so that an RHD code whose chemistry runs on the GPU

@@ -135,6 +135,12 @@ SIGNATURES = {
     "lyd_rhd_lya_prepare": (C.c_int, [VP, P, P, P, P, P, P, P, P, P, C.POINTER(DustLya), D, I32, I32]),
     "lyd_rhd_lya_absorb": (C.c_int, [VP, P, D, I32, C.POINTER(RhdLyaOut)]),
     "lyd_find_rsl_lya": (C.c_int, [VP, D, D, P, P, P, P, P, P, P, P, P, C.POINTER(DustLya), D, D, P]),
+    "lyd_dd_set_halo": (C.c_int, [VP, I32, I32]),
+    "lyd_dd_columns": (C.c_int, [VP]),
+    "lyd_dd_find_active_partials": (C.c_int, [VP, VP]),
+    "lyd_dd_step_partials": (C.c_int, [VP, C.POINTER(StepParams), VP]),
+    "lyd_dd_finish": (C.c_int, [VP, VP, I32, C.POINTER(Diag)]),
+    "lyd_dd_halo": (C.c_int, [VP, I32, I32, VP]),
     "lyd_cfl_dt": (C.c_int, [VP, D, P, P, D, P]),
     "lyd_edge_count": (C.c_int, [I32, I32]),
     "lyd_edge_spectra": (C.c_int, [VP, P, P, C.POINTER(I32), C.POINTER(I32)]),

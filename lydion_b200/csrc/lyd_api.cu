@@ -71,6 +71,7 @@ struct lyd_ctx {
     double *Ff[3] = {nullptr, nullptr, nullptr};
     bool ff_valid = false;
     double *cellf[CF_N] = {};
+    CloudDesc *dd_cl = nullptr;    // device record of lyd_dd_finish (the all-reduced columns)
     double *dust_F = nullptr;      // [3][ncell] dust flux opacities of the RHD Lya block (set by
                                    // lyd_rhd_lya_prepare)
     double *u_r_star = nullptr, *u_Z_star = nullptr;
@@ -197,13 +198,13 @@ static int build_work(lyd_ctx *c) {
     const int nkb = (c->nnu + 31) / 32;
     for (int q = 0; q < c->ncl; q++)
         for (int kb = 0; kb < nkb; kb++)
-            for (int j0 = 0; j0 < c->nz[q]; j0 += rows)
+            for (int j0 = c->desc[q].j_own0; j0 < c->desc[q].j_own1; j0 += rows)
                 for (int i0 = 0; i0 < c->nr[q]; i0 += kTileCols) t.push_back(make_int4(q, i0, j0, 32 * kb));
     const int cpb = cells_per_block(c);
     for (int q = 0; q < c->ncl; q++) {
-        const int nc = c->nr[q] * c->nz[q];
+        const int b0 = c->nr[q] * c->desc[q].j_own0, nc = c->nr[q] * c->desc[q].j_own1;   // owned cells
         c->desc[q].pb0 = (int)it.size();
-        for (int b = 0; b < nc; b += cpb) it.push_back(make_int4(q, b, std::min(nc, b + cpb), 0));
+        for (int b = b0; b < nc; b += cpb) it.push_back(make_int4(q, b, std::min(nc, b + cpb), 0));
         c->desc[q].npb = (int)it.size() - c->desc[q].pb0;
     }
     cudaFree(c->tiles);
@@ -279,6 +280,7 @@ int lyd_batch_create(lyd_ctx **out, int32_t ncl, const int32_t *n_r, const int32
         d.orint = (int)c->nrint; d.ozint = (int)c->nzint;
         d.orif = (int)c->nrif; d.ozif = (int)c->nzif;
         d.nr = nr; d.nz = nz;
+        d.j_own0 = 0; d.j_own1 = nz;
         d.ctdt = d.dt = d.c_tilde = 1.0;
         c->ncell += (size_t)nr * nz;
         c->n3 += (size_t)nr * nz * n_nu;
@@ -354,6 +356,7 @@ int lyd_destroy(lyd_ctx *c) {
     for (void *p : ps) cudaFree(p);
     for (int q = 0; q < CF_N; q++) cudaFree(c->cellf[q]);
     cudaFree(c->dust_F);
+    cudaFree(c->dd_cl);
     for (int q = 0; q < 8; q++)
         if (c->ev[q]) cudaEventDestroy(c->ev[q]);
     if (c->st) cudaStreamDestroy(c->st);
@@ -963,7 +966,7 @@ template <typename S>
 // read s_n from and write s_{n+1} into its own storage instead, and `ff` to keep the frequency
 // factors F+, F, F- (n3 apart).
 static int enqueue_step(lyd_ctx *c, bool timed, double *tape = nullptr, const S *in = nullptr, S *out = nullptr,
-                        double *ff = nullptr) {
+                        double *ff = nullptr, bool reduce = true) {
     const int A = c->cur, B = 1 - c->cur;
     AdvArgs<S> aa;
     fill_adv<S>(c, aa, A, B);
@@ -989,7 +992,7 @@ static int enqueue_step(lyd_ctx *c, bool timed, double *tape = nullptr, const S 
     if (timed) cudaEventRecord(c->ev[1], c->st);
     launch_freq(prec, &fa, c->nnu, c->nitems, c->st);
     if (timed) cudaEventRecord(c->ev[2], c->st);
-    launch_reduce(ra, c->st);
+    if (reduce) launch_reduce(ra, c->st);
     if (timed) cudaEventRecord(c->ev[3], c->st);
     LYD_CU(c, cudaGetLastError());
     return LYD_OK;
@@ -1085,6 +1088,102 @@ int lyd_static_steps(lyd_ctx *c, const lyd_step_params *p, lyd_diag *hist_out) {
     for (CloudDesc &d : c->desc) d.z_center = p->z_center;
     bcs_all(c, c->cfg.bc_r_left, p->bc_r_right, p->bc_z_bot, p->bc_z_top);
     return run_steps(c, p->n_steps, hist_out);
+}
+
+// ---- Z-slab domain decomposition -------------------------------------------------------------
+int lyd_dd_set_halo(lyd_ctx *c, int32_t h_bot, int32_t h_top) {
+    if (!c) return LYD_ERR_ARG;
+    LYD_TRY(single_cloud(c, "lyd_dd_set_halo"));
+    cudaSetDevice(c->dev);
+    const int nz = c->nz[0];
+    if ((h_bot != 0 && h_bot != 2) || (h_top != 0 && h_top != 2) || nz - h_bot - h_top < 2)
+        return fail(c, LYD_ERR_ARG, "halos are 0 or 2 rows and at least 2 rows must be owned");
+    c->desc[0].j_own0 = h_bot;
+    c->desc[0].j_own1 = nz - h_top;
+    c->active_valid = false;
+    return build_work(c);
+}
+
+int lyd_dd_columns(lyd_ctx *c) { return c ? c->nnu + kExtraCols : LYD_ERR_ARG; }
+
+int lyd_dd_find_active_partials(lyd_ctx *c, double *colsum) {
+    if (!c || !colsum) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    LYD_TRY(need_inputs(c, false, false));
+    LYD_TRY(sync_desc(c));
+    launch_find_active(c->sprec, Jc(c, 0), c->nnu, c->dnu, c->dV, c->cl, c->items, c->nitems, c->jeps_s, c->partials,
+                       c->st);
+    launch_column_sums(c->partials, c->nnu + kExtraCols, c->nitems, colsum, c->st);
+    LYD_CU(c, cudaGetLastError());
+    return LYD_OK;
+}
+
+int lyd_dd_step_partials(lyd_ctx *c, const lyd_step_params *p, double *colsum) {
+    if (!c || !p || !colsum) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    LYD_TRY(check_bcs(c, c->cfg.bc_r_left, p->bc_r_right, p->bc_z_bot, p->bc_z_top));
+    if (!(p->c_tilde > 0.0) || !(p->dt > 0.0)) return fail(c, LYD_ERR_ARG, "bad step parameters");
+    if (!c->active_valid) return fail(c, LYD_ERR_STATE, "no active window: run lyd_dd_find_active_partials and lyd_dd_finish first");
+    LYD_TRY(need_inputs(c, true, true));
+    params_all(c, p->c_tilde, p->dt, p->c_tilde * p->dt);
+    for (CloudDesc &d : c->desc) d.z_center = p->z_center;
+    bcs_all(c, c->cfg.bc_r_left, p->bc_r_right, p->bc_z_bot, p->bc_z_top);
+    LYD_TRY(sync_desc(c));
+    LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_R], 0, c->ncell * 8, c->st));
+    LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_Z], 0, c->ncell * 8, c->st));
+    int r = c->sprec == 0 ? enqueue_step<double>(c, false, nullptr, nullptr, nullptr, nullptr, false)
+                          : enqueue_step<float>(c, false, nullptr, nullptr, nullptr, nullptr, false);
+    if (r != LYD_OK) return r;
+    launch_column_sums(c->partials, c->nnu + kExtraCols, c->nitems, colsum, c->st);
+    LYD_CU(c, cudaGetLastError());
+    c->active_valid = false;   // until lyd_dd_finish decides the next window
+    return LYD_OK;
+}
+
+int lyd_dd_finish(lyd_ctx *c, const double *colsum, int32_t step, lyd_diag *rec) {
+    if (!c || !colsum) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    if (!c->dd_cl) LYD_TRY(dalloc(c, (void **)&c->dd_cl, sizeof(CloudDesc)));
+    CloudDesc d = c->desc[0];
+    d.pb0 = 0;
+    d.npb = 1;                 // the all-reduced column sums: one "block"
+    LYD_CU(c, cudaMemcpyAsync(c->dd_cl, &d, sizeof(d), cudaMemcpyHostToDevice, c->st));
+    RedArgs ra = red_args(c, step ? (PART_ACTIVE | PART_DIAG) : PART_ACTIVE);
+    ra.partials = colsum;
+    ra.nblocks = 1;
+    ra.cl = c->dd_cl;
+    launch_reduce(ra, c->st);
+    LYD_CU(c, cudaGetLastError());
+    c->active_valid = true;
+    if (rec) {
+        double h[7];
+        int kw[2];
+        LYD_CU(c, cudaMemcpyAsync(h, c->last, sizeof(h), cudaMemcpyDeviceToHost, c->st));
+        LYD_CU(c, cudaMemcpyAsync(kw, c->kwin, sizeof(kw), cudaMemcpyDeviceToHost, c->st));
+        LYD_CU(c, cudaStreamSynchronize(c->st));
+        rec->M_F = h[0]; rec->M_F_radial_net = h[1]; rec->M_F_radial_out = h[2]; rec->L_tot = h[3]; rec->f_esc = h[4];
+        if (step) { rec->kmin = (int32_t)h[5]; rec->kmax = (int32_t)h[6]; }
+        else { rec->kmin = kw[0]; rec->kmax = kw[1]; }
+    }
+    return check_err(c);
+}
+
+int lyd_dd_halo(lyd_ctx *c, int32_t side, int32_t pack, void *buf) {
+    if (!c || !buf || (side != 0 && side != 1)) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    const CloudDesc &d = c->desc[0];
+    const int hb = d.j_own0, ht = d.nz - d.j_own1;
+    if ((side == 0 && hb != 2) || (side == 1 && ht != 2)) return fail(c, LYD_ERR_STATE, "no halo on that side");
+    // pack: the two owned rows next to the neighbour; unpack: the two halo rows
+    const int row = pack ? (side == 0 ? d.j_own0 : d.j_own1 - 2) : (side == 0 ? d.j_own0 - 2 : d.j_own1);
+    const size_t n2 = (size_t)2 * d.nr * c->nnu, off = (size_t)row * d.nr * c->nnu;
+    for (int q = 0; q < 3; q++) {
+        char *dev = static_cast<char *>(Jc(c, q)) + off * c->ssz;
+        char *b = static_cast<char *>(buf) + (size_t)q * n2 * c->ssz;
+        if (pack) LYD_CU(c, cudaMemcpyAsync(b, dev, n2 * c->ssz, cudaMemcpyDeviceToDevice, c->st));
+        else LYD_CU(c, cudaMemcpyAsync(dev, b, n2 * c->ssz, cudaMemcpyDeviceToDevice, c->st));
+    }
+    return LYD_OK;
 }
 
 int lyd_batch_steps(lyd_ctx *c, const lyd_cloud_params *p, int32_t n_steps, lyd_diag *hist_out) {

@@ -23,6 +23,8 @@ struct CloudDesc {
     int orif, ozif;      // interface coordinates (n_r+1, n_z+1)
     int nr, nz;
     int bc_r_left, bc_r_right, bc_z_bot, bc_z_top;
+    int j_own0, j_own1;  // rows this context updates; outside them, halo rows of a Z-slab
+                         // decomposition (domain neighbours' rows, read by the stencil only)
     int pb0, npb;        // this cloud's blocks in the frequency-kernel work list / partials
     double ctdt, dt, c_tilde, z_center;
 };

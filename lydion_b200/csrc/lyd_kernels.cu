@@ -29,6 +29,7 @@ struct View {
     long long o3, oc, orf, ozf;
     int ocol, orow, orint, ozint;
     int nr, nz, bcl, bcr, bzb, bzt;
+    int jend;            // end of the rows the tiles update
     double ctdt;
 };
 
@@ -36,6 +37,7 @@ __device__ __forceinline__ void load_view(const CloudDesc &d, View &v) {
     v.o3 = d.o3; v.oc = d.oc; v.orf = d.orf; v.ozf = d.ozf;
     v.ocol = d.ocol; v.orow = d.orow; v.orint = d.orint; v.ozint = d.ozint;
     v.nr = d.nr; v.nz = d.nz; v.bcl = d.bc_r_left; v.bcr = d.bc_r_right; v.bzb = d.bc_z_bot; v.bzt = d.bc_z_top;
+    v.jend = d.j_own1;
     v.ctdt = d.ctdt;
 }
 
@@ -255,7 +257,7 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
     View v;
     load_view(a.cl[t.x], v);
     const int i0 = t.y, j0 = t.z, kb = t.w;
-    const int j1 = (j0 + a.rows < v.nz) ? j0 + a.rows : v.nz;
+    const int j1 = (j0 + a.rows < v.jend) ? j0 + a.rows : v.jend;
     const int k = kb + lane;
     const int kmin = a.kwin[2 * t.x], kmax = a.kwin[2 * t.x + 1];
     const bool kact = (k >= kmin) && (k <= kmax) && (k < a.nnu);

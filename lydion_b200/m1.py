@@ -239,6 +239,31 @@ class M1Context:
         self._ck(lib().lyd_pd_lya(self._h, out.size, *[_dp(a) for a in arrs], float(z), _dp(out)))
         return out.reshape(np.shape(nHII))
 
+    # -- Z-slab domain decomposition (see lydion_b200/domain.py) ---------------------------
+    def dd_set_halo(self, h_bot, h_top):
+        self._ck(lib().lyd_dd_set_halo(self._h, int(h_bot), int(h_top)))
+
+    def dd_columns(self):
+        return int(lib().lyd_dd_columns(self._h))
+
+    def dd_find_active_partials(self, colsum):
+        self._ck(lib().lyd_dd_find_active_partials(self._h, C.c_void_p(colsum.data_ptr())))
+
+    def dd_step_partials(self, colsum, c_tilde, dt, z_center, bc_r_right=BC_OUTFLOW, bc_z_bot=BC_REFLECT,
+                         bc_z_top=BC_OUTFLOW):
+        p = _lib.StepParams(float(c_tilde), float(dt), float(z_center), bc_r_right, bc_z_bot, bc_z_top, 1)
+        self._ck(lib().lyd_dd_step_partials(self._h, C.byref(p), C.c_void_p(colsum.data_ptr())))
+
+    def dd_finish(self, colsum, step=True):
+        """The next window (and the step's record) from the all-reduced column sums: returns
+        [M_F, radial net, radial out, L, f_esc, kmin, kmax]."""
+        d = _lib.Diag()
+        self._ck(lib().lyd_dd_finish(self._h, C.c_void_p(colsum.data_ptr()), int(bool(step)), C.byref(d)))
+        return [d.M_F, d.M_F_radial_net, d.M_F_radial_out, d.L_tot, d.f_esc, d.kmin, d.kmax]
+
+    def dd_halo(self, side, pack, buf):
+        self._ck(lib().lyd_dd_halo(self._h, int(side), int(bool(pack)), C.c_void_p(buf.data_ptr())))
+
     # -- RHD-side Lyman-alpha block --------------------------------------------------------
     def rhd_lya_prepare(self, T, nHI, nH2, nHII, nHeI, ne, nOHx, nCHx, rho_d, kappa_abs, kappa_F, rho_ignore,
                         z=0.0, ots=True, destruction=True):
