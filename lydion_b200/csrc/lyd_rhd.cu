@@ -59,7 +59,7 @@ __device__ __forceinline__ double wsum_rhd(double v) {
 }
 
 template <typename S>
-__global__ void k_rhd_absorb(RhdAbsorbArgs<S> a) {
+__global__ void __launch_bounds__(256, 3) k_rhd_absorb(RhdAbsorbArgs<S> a) {
     const int lane = threadIdx.x & 31;
     const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
     const double ct = a.c_tilde, ic = 1.0 / ct;
@@ -72,10 +72,8 @@ __global__ void k_rhd_absorb(RhdAbsorbArgs<S> a) {
         const double pd_a = pd * alpha;
         const size_t base = c * (size_t)a.nnu;
         double intJ = 0.0, dr = 0.0, dz = 0.0, sp[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        for (int k = lane; k < a.nnu; k += 32) {
+        auto body = [&](int k, double Hv, double Jo, double Hro, double HZo) {
             const size_t x = base + k;
-            const double Hv = double(a.Hv[x]);
-            const double Jo = double(a.Jold[x]), Hro = double(a.Hrold[x]), HZo = double(a.HZold[x]);
             const double dJdt = ct_js * (Hv * pinv);
             const double a_abs = ac + pd_a * Hv;
             double Jn = (Jo + dJdt * dt) / (1.0 + a_abs * ct * dt);
@@ -100,6 +98,18 @@ __global__ void k_rhd_absorb(RhdAbsorbArgs<S> a) {
             sp[0] += f0 * mr; sp[1] += f0 * mz; sp[2] += f1 * mr; sp[3] += f1 * mz;
             sp[4] += f2 * mr; sp[5] += f2 * mz; sp[6] += f3 * mr; sp[7] += f3 * mz;
             intJ += a.dnu[k] * double(S(Jn));
+        };
+        // two bins per lane per pass, their loads issued together
+        for (int kb = 0; kb < a.nnu; kb += 64) {
+            const int k0 = kb + lane, k1 = kb + 32 + lane;
+            const bool v0 = k0 < a.nnu, v1 = k1 < a.nnu;
+            const size_t x0 = base + k0, x1 = base + k1;
+            const double Hv0 = v0 ? double(a.Hv[x0]) : 0.0, Hv1 = v1 ? double(a.Hv[x1]) : 0.0;
+            const double Jo0 = v0 ? double(a.Jold[x0]) : 0.0, Jo1 = v1 ? double(a.Jold[x1]) : 0.0;
+            const double Hr0 = v0 ? double(a.Hrold[x0]) : 0.0, Hr1 = v1 ? double(a.Hrold[x1]) : 0.0;
+            const double HZ0 = v0 ? double(a.HZold[x0]) : 0.0, HZ1 = v1 ? double(a.HZold[x1]) : 0.0;
+            if (v0) body(k0, Hv0, Jo0, Hr0, HZ0);
+            if (v1) body(k1, Hv1, Jo1, Hr1, HZ1);
         }
         intJ = wsum_rhd(intJ);
         dr = wsum_rhd(dr);
