@@ -217,6 +217,25 @@ def measure_form(cloud, prec, args, barrier, stream_of, local, world, clk=None):
                  "clocks": clocks, "active_fraction": active}
 
 
+def mixed_error_form(cloud, local, n_steps=2000):
+    """Error of the mixed form against FP64 on the headline cloud: both forms run n_steps from
+    the same set-up state; M_F at the last step and over the run, the emergent edge-ring
+    spectrum and the final J, each relative to the FP64 quantity's maximum."""
+    from lydion_b200._lib import PREC_FP64, PREC_MIXED
+    from lydion_b200.m1 import context_for_cloud
+    p = (cloud.c_tilde, cloud.dt, cloud.z_center, cloud.bc_r_right, cloud.bc_z_bot, cloud.bc_z_top)
+    res = {}
+    for prec in (PREC_FP64, PREC_MIXED):
+        ctx = context_for_cloud(cloud, precision=prec, device=local)
+        h = ctx.static_steps(n_steps, *p, history=True)
+        res[prec] = (h[:, 0].copy(), ctx.edge_spectra()[0].mean(0), ctx.download("J"))
+        ctx.close()
+    (ma, sa, Ja), (mb, sb, Jb) = res[PREC_FP64], res[PREC_MIXED]
+    rel = lambda b, a: float(np.max(np.abs(b - a)) / np.max(np.abs(a)))
+    return {"steps": n_steps, "M_F_last": float(abs(mb[-1] - ma[-1]) / abs(ma[-1])), "M_F_run": rel(mb, ma),
+            "edge_spectrum": rel(sb, sa), "J": rel(Jb, Ja), "spec": 1e-5}
+
+
 def e2e_form(ctx, cloud, args, barrier, stream_of, world):
     """End to end through the public API with host buffers: per step, J / H_r / H_Z up from
     pinned host memory, one step with its diagnostics record, J / H_r / H_Z back."""
@@ -443,6 +462,7 @@ def run_gpu(args):
     adj = None if (args.no_adjoint or world > 1) else adjoint_form(args, stream_of, local)
     c5 = None if (args.no_c5 or world > 1) else c5_form(args, stream_of, local)
     rhd = None if (args.no_rhd or world > 1) else rhd_form(args, stream_of, local)
+    err = None if (args.no_error or world > 1) else mixed_error_form(cloud, local)
     dd = dd_form(args, stream_of, local, world, rank) if args.dd_field else None
 
     # roofline of the dominant kernel of the headline (mixed) form
@@ -469,6 +489,7 @@ def run_gpu(args):
                     "value": f64["value"], "ms_per_step": f64["ms_per_step"], "tuning": f64["tuning"],
                     "kernel_ms_per_step": {n: float(v) for n, v in zip(names, f64["kernel_ms"])}},
                 "mixed_over_fp64": None if f64 is None else mix["value"] / f64["value"],
+                "mixed_error": err,
                 "adjoint_over_forward": adj["ratio_auto"] if adj else None,
                 "adjoint": adj,
                 "largest_field": c5,
@@ -506,6 +527,7 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of the autotuner")
     ap.add_argument("--no-c5", action="store_true", help="skip the 1024x1024x128 field")
     ap.add_argument("--no-rhd", action="store_true", help="skip the RHD-side Lyman-alpha block")
+    ap.add_argument("--no-error", action="store_true", help="skip the mixed-against-FP64 error run")
     ap.add_argument("--dd-field", action="store_true",
                     help="also step the 1024x1024x128 field split into Z slabs over the ranks (strong scaling)")
     ap.add_argument("--only-mixed", action="store_true", help="measure the mixed-precision form only")

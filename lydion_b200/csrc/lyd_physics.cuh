@@ -60,7 +60,10 @@ __device__ __forceinline__ float rsq(float x) { return sqrtf(x); }
 // refined by two Newton-Raphson steps for 1/y, x <- x + x (1 - y x), each written as two
 // fused multiply-adds; every step squares the relative error (Markstein, IBM J. Res. Dev. 34
 // (1990) 111-119). No special-case branches: the callers divide by positive normal numbers
-// whose reciprocals are normal. FP32: the IEEE division.
+// whose reciprocals are normal. FP32: the hardware's approximate reciprocal alone (PTX
+// rcp.approx.ftz.f32, relative error within 2^-23 over the normal range, subnormals flushed),
+// one instruction in place of the IEEE division's refinement sequence; the FP32 arithmetic of
+// the mixed and FP32-storage forms already carries a 2^-24 rounding per operation.
 template <typename R> __device__ __forceinline__ R rcp(R y);
 template <> __device__ __forceinline__ double rcp<double>(double y) {
     double x;
@@ -70,7 +73,11 @@ template <> __device__ __forceinline__ double rcp<double>(double y) {
     e = fma(-y, x, 1.0);
     return fma(x, e, x);
 }
-template <> __device__ __forceinline__ float rcp<float>(float y) { return 1.0f / y; }
+template <> __device__ __forceinline__ float rcp<float>(float y) {
+    float x;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(x) : "f"(y));
+    return x;
+}
 
 // MinMod, src/ConstantsAndFunctions.jl:1571-1582
 template <typename R>
