@@ -186,11 +186,18 @@ def measure_form(cloud, prec, args, barrier, stream_of, local, world, clk=None):
     ctx = context_for_cloud(cloud, precision=prec, device=local)
     p = (cloud.c_tilde, cloud.dt, cloud.z_center, cloud.bc_r_right, cloud.bc_z_bot, cloud.bc_z_top)
     run = lambda n: ctx.static_steps(n, *p, history=False)
+    init = {n: ctx.download(n) for n in ("J", "H_r", "H_Z")}
+
+    def reset():   # the set-up state (and with it the set-up active window)
+        for n, x in init.items():
+            ctx.upload(n, x)
+
     if args.no_tune:
         tuning = ctx.tuning()
     else:
-        tuning = autotune.autotune(ctx, run, steps=5, device=local,
+        tuning = autotune.autotune(ctx, run, steps=10, device=local, reset=reset,
                                    cache=os.path.join(tempfile.gettempdir(), "lydion_bench_tuning.json"))
+        reset()
     run(args.warmup)
     barrier(ctx)
     if clk is not None:

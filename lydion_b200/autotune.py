@@ -13,7 +13,9 @@ library's per-kernel CUDA events (lyd_set_timing) over a few real steps of the c
 workload, after one untimed step that applies the new shape.
 
 Tuning advances the context's state by the steps it runs: tune a scratch context built from
-the same workload when the state must stay untouched. Results are cached as JSON, keyed by
+the same workload when the state must stay untouched, or pass `reset`, which is called before
+every candidate to put the same state back (the advection's tile count against the SMs' CTA
+slots, and the active window, make the shapes' times depend on the state they run from). Results are cached as JSON, keyed by
 the GPU name and the workload's shape, in $LYDION_TUNE_CACHE or
 ~/.cache/lydion_b200/tuning.json.
 """
@@ -23,7 +25,7 @@ import os
 
 import numpy as np
 
-ROWS = (4, 8, 16, 32)
+ROWS = (4, 8, 12, 16, 20, 24, 32, 40, 48)
 CTAS = (2, 3, 4)
 CELLS = (0, 16, 32, 64, 128, 256, 512)
 SOLVERS = (0, 1)
@@ -81,8 +83,9 @@ def _measure(ctx, run, tuning, steps):
     return ms
 
 
-def search(ctx, run, steps=10, rows=ROWS, cells=CELLS, solvers=SOLVERS, ctas=CTAS):
-    """Time every candidate; return (best tuning tuple, table of (tuning, ms[3]))."""
+def search(ctx, run, steps=10, rows=ROWS, cells=CELLS, solvers=SOLVERS, ctas=CTAS, reset=None):
+    """Time every candidate (each after `reset()`, when given); return (best tuning tuple, table
+    of (tuning, ms[3]))."""
     table = []
     if getattr(ctx, "precision", 0) == 0:
         ctas = tuple(o for o in ctas if o in (2, 3)) or (0,)   # FP64 arithmetic: 2 or 3 CTAs per SM
@@ -90,6 +93,8 @@ def search(ctx, run, steps=10, rows=ROWS, cells=CELLS, solvers=SOLVERS, ctas=CTA
     for r in rows:
         for o in ctas:
             t = (r, 0, 0, o)
+            if reset:
+                reset()
             ms = _measure(ctx, run, t, steps)
             table.append((t, ms.tolist()))
             if ms[0] < best_adv:
@@ -98,6 +103,8 @@ def search(ctx, run, steps=10, rows=ROWS, cells=CELLS, solvers=SOLVERS, ctas=CTA
     for s in solvers:
         for cb in cells:
             t = (best_rows[0], cb, s, best_rows[1])
+            if reset:
+                reset()
             ms = _measure(ctx, run, t, steps)
             table.append((t, ms.tolist()))
             if ms[1] + ms[2] < best_f:

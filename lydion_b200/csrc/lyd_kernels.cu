@@ -183,11 +183,17 @@ __device__ __forceinline__ CellF<R> staged(const R *A, int slot, int lc, int lan
     return c;
 }
 
+// With FP32 arithmetic the faces read u* (`up`) and the Z face's PLM intervals (`ivz`) where the
+// caller points, the warp's row slot in shared memory (see GEO_N below); with FP64 arithmetic
+// they load them from global memory where they are used and ignore the two pointers.
 // r face f (between cells f-1 and f) of row j held in ring slot `slot`; wl = f - i0 is the
 // staged column of the stencil's first cell (src/AdvectJandH.jl:641-968).
 template <typename S, typename R, int FLUX>
 __device__ __forceinline__ void face_r_staged(const AdvArgs<S> &a, const View &v, const R *A, int slot, int wl,
-                                              int f, int j, int k, int lane, R jeps, R *F, R &kL, R &kR) {
+                                              int f, int j, int k, int lane, R jeps, const double *up, R *F,
+                                              R &kL, R &kR) {
+    double us = 0.0;
+    if constexpr (sizeof(R) == 4) us = *up;
     R d0, aFi, aFp, d3;
     CellF<R> cm1 = staged<R>(A, slot, wl, lane, d0);
     CellF<R> ci = staged<R>(A, slot, wl + 1, lane, aFi);
@@ -207,7 +213,8 @@ __device__ __forceinline__ void face_r_staged(const AdvArgs<S> &a, const View &v
     R FJ, FHr, FHZ;
     m1_flux<R, FLUX, false>(q.Hr_L, q.Hr_R, DrrL * q.J_L, DrrR * q.J_R, DrZL * q.J_L, DrZR * q.J_R, q, ci.J, cp1.J,
                             FJ, FHr, FHZ);
-    R uc = R(__ldg(a.u_r_star + v.orf + f + (long long)(v.nr + 1) * j) * kInvC);
+    if constexpr (sizeof(R) != 4) us = __ldg(a.u_r_star + v.orf + f + (long long)(v.nr + 1) * j);
+    R uc = R(us * kInvC);
     F[0] = FJ + adv_flux(uc, q.J_L, q.J_R);
     F[1] = FHr + adv_flux(uc, q.Hr_L, q.Hr_R);
     F[2] = FHZ + adv_flux(uc, q.HZ_L, q.HZ_R);
@@ -218,7 +225,9 @@ __device__ __forceinline__ void face_r_staged(const AdvArgs<S> &a, const View &v
 // Z face f (between rows f-1 and f) of column i, staged column lc (src/AdvectJandH.jl:978-1289).
 template <typename S, typename R, int FLUX>
 __device__ __forceinline__ void face_z_staged(const AdvArgs<S> &a, const View &v, const R *A, int lc, int i, int f,
-                                              int k, int lane, R jeps, R *F) {
+                                              int k, int lane, R jeps, const double *ivz, const double *up, R *F) {
+    double us = 0.0;
+    if constexpr (sizeof(R) == 4) us = *up;
     R d0, aFi, aFp, d3;
     CellF<R> cm1 = staged<R>(A, (f + 2) & (RING - 1), lc, lane, d0);     // row f-2
     CellF<R> ci = staged<R>(A, (f + 3) & (RING - 1), lc, lane, aFi);     // row f-1
@@ -230,7 +239,10 @@ __device__ __forceinline__ void face_z_staged(const AdvArgs<S> &a, const View &v
     }
     R iv[5];
 #pragma unroll
-    for (int t = 0; t < 5; t++) iv[t] = R(__ldg(a.zint + v.ozint + 5 * f + t));
+    for (int t = 0; t < 5; t++) {
+        if constexpr (sizeof(R) == 4) iv[t] = R(ivz[t]);
+        else iv[t] = R(__ldg(a.zint + v.ozint + 5 * f + t));
+    }
     Recon<R> q = reconstruct_f<R>(cm1, ci, cp1, cp2, iv, aFi, aFp, jeps);
     R DrrL, DZZL, DrZL, DrrR, DZZR, DrZR;
     D_from_f_n<R>(q.f_L, q.nr_L, q.nZ_L, DrrL, DZZL, DrZL);
@@ -238,10 +250,59 @@ __device__ __forceinline__ void face_z_staged(const AdvArgs<S> &a, const View &v
     R FJ, FHr, FHZ;
     m1_flux<R, FLUX, true>(q.HZ_L, q.HZ_R, DrZL * q.J_L, DrZR * q.J_R, DZZL * q.J_L, DZZR * q.J_R, q, ci.J, cp1.J,
                            FJ, FHr, FHZ);
-    R uc = R(__ldg(a.u_Z_star + v.ozf + i + (long long)v.nr * f) * kInvC);
+    if constexpr (sizeof(R) != 4) us = __ldg(a.u_Z_star + v.ozf + i + (long long)v.nr * f);
+    R uc = R(us * kInvC);
     F[0] = FJ + adv_flux(uc, q.J_L, q.J_R);
     F[1] = FHr + adv_flux(uc, q.Hr_L, q.Hr_R);
     F[2] = FHZ + adv_flux(uc, q.HZ_L, q.HZ_R);
+}
+
+// The per-row scalars a warp needs: the cell's geometry and velocity gradients (0..10), u*_r of
+// the warp's r face (11), u*_Z of its Z face above the row (12), that face's PLM intervals
+// (13..17). With FP32 arithmetic they are fetched one per lane a row ahead of their use and
+// parked in shared memory, so their loads overlap a whole row's work instead of stalling the
+// faces and the cell update (mixed advection 0.233 -> 0.226 ms at 256^2 x 64). The FP64 tile
+// loads them where they are used: it runs at its register limit, and the registers that carry
+// the next row's scalar and its address across the row spill there (0.330 -> 0.335 ms).
+constexpr int GEO_N = 18;
+enum { G_ARL, G_ARR, G_AZL, G_AZR, G_IDV, G_DURDR, G_DURDZ, G_DUZDR, G_DUZDZ, G_UROR, G_IRC, G_UR, G_UZ, G_ZIV };
+
+// Where lane `lane` finds its scalar of row j for warp column `col` (the r face of warp w is
+// face col too): src + j * stride, or nowhere (src null). Each lane gets one address, so a row's
+// scalars come in with one load instruction per warp. The ranges are those of the consumers:
+// the cell update and the Z face run for own columns col < n_r, the r face for faces col <= n_r.
+template <typename S>
+__device__ __forceinline__ void geo_source(const AdvArgs<S> &a, const View &v, int lane, int col, bool own,
+                                           const double *&src, int &stride) {
+    src = nullptr;
+    stride = 0;
+    if (lane == G_UR) {
+        if (col <= v.nr) { src = a.u_r_star + v.orf + col; stride = v.nr + 1; }
+        return;
+    }
+    if (!own || col >= v.nr || lane >= GEO_N) return;
+    const long long c = v.oc + col;
+    stride = v.nr;
+    switch (lane) {
+        case G_ARL: src = a.A_r + v.orf + col; stride = v.nr + 1; break;
+        case G_ARR: src = a.A_r + v.orf + col + 1; stride = v.nr + 1; break;
+        case G_AZL: src = a.A_Z + v.ozf + col; break;
+        case G_AZR: src = a.A_Z + v.ozf + col + v.nr; break;
+        case G_IDV: src = a.inv_dV + c; break;
+        case G_DURDR: src = a.dur_dr + c; break;
+        case G_DURDZ: src = a.dur_dZ + c; break;
+        case G_DUZDR: src = a.duZ_dr + c; break;
+        case G_DUZDZ: src = a.duZ_dZ + c; break;
+        case G_UROR: src = a.ur_over_r + c; break;
+        case G_IRC: src = a.inv_r_cell + v.ocol + col; stride = 0; break;
+        case G_UZ: src = a.u_Z_star + v.ozf + col + v.nr; break;                 // face j+1
+        default: src = a.zint + v.ozint + 5 + (lane - G_ZIV); stride = 5; break;   // face j+1
+    }
+}
+
+// Row j's scalar of this lane; rows at or beyond the tile's end j1 (<= n_z) fetch nothing.
+__device__ __forceinline__ double geo_fetch(const double *src, int stride, int j, int j1) {
+    return (src != nullptr && j < j1) ? __ldg(src + (long long)stride * j) : 0.0;
 }
 
 template <typename S, typename R, int FLUX, int MINB>
@@ -252,6 +313,7 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
     R *A = reinterpret_cast<R *>(adv_smem);                            // [RING][MCOL][NF][32]
     S *Hh = reinterpret_cast<S *>(A + RING * MCOL * NF * 32);           // [RING][MT][HF][32]
     R *Fr = reinterpret_cast<R *>(Hh + RING * MT * HF * 32);            // [MT+1][5][32]
+    double *geo = reinterpret_cast<double *>(Fr + (MT + 1) * 5 * 32);  // [MWARPS][GEO_N], FP32 arithmetic only
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int4 t = a.tiles[blockIdx.x];
     View v;
@@ -284,13 +346,25 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
             stage_cell<S, R>(a, v, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps);
         }
     }
+    constexpr bool PRE = sizeof(R) == 4;   // per-row scalars fetched a row ahead
+    const double *gsrc = nullptr;
+    int gstr = 0;
+    double *g = geo + w * GEO_N;
+    if constexpr (PRE) {
+        geo_source<S>(a, v, lane, col, own, gsrc, gstr);
+        if (lane < GEO_N) g[lane] = geo_fetch(gsrc, gstr, j0, j1);
+    }
     __syncthreads();
     R zL[3] = {R(0), R(0), R(0)};
-    if (own && kact && col < v.nr) face_z_staged<S, R, FLUX>(a, v, A, w + 2, col, j0, k, lane, jeps, zL);
+    if (own && kact && col < v.nr)
+        face_z_staged<S, R, FLUX>(a, v, A, w + 2, col, j0, k, lane, jeps, a.zint + v.ozint + 5 * j0,
+                                  a.u_Z_star + v.ozf + col + (long long)v.nr * j0, zL);   // face j0
 
     const double ctdt = v.ctdt;
     const double ctdt_c = ctdt * kInvC;
     for (int j = j0; j < j1; j++) {
+        double gnext = 0.0;
+        if constexpr (PRE) gnext = geo_fetch(gsrc, gstr, j + 1, j1);
         // (A) stage row j+2 of the own column; warp 8 stages the halo columns of row j
         if (kact) {
             if (own) {
@@ -313,11 +387,12 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
         R zR[3] = {R(0), R(0), R(0)};
         if (kact && f <= v.nr) {
             R F[3], kL, kR;
-            face_r_staged<S, R, FLUX>(a, v, A, j & (RING - 1), w, f, j, k, lane, jeps, F, kL, kR);
+            face_r_staged<S, R, FLUX>(a, v, A, j & (RING - 1), w, f, j, k, lane, jeps, g + G_UR, F, kL, kR);
             R *p = Fr + (w * 5) * 32 + lane;
             p[0] = F[0]; p[32] = F[1]; p[64] = F[2]; p[96] = kL; p[128] = kR;
         }
-        if (own && kact && col < v.nr) face_z_staged<S, R, FLUX>(a, v, A, w + 2, col, j + 1, k, lane, jeps, zR);
+        if (own && kact && col < v.nr)
+            face_z_staged<S, R, FLUX>(a, v, A, w + 2, col, j + 1, k, lane, jeps, g + G_ZIV, g + G_UZ, zR);
         __syncthreads();
         // (C) cell update, src/AdvectJandH.jl:1302-1382
         if (own && col < v.nr && k < a.nnu) {
@@ -336,10 +411,16 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
                 D_edd<R>(sHr, sHZ, sJ, jeps, R(a.heps2), Drr, DZZ, DrZ);
                 const R *FL = Fr + (w * 5) * 32 + lane;
                 const R *FR = FL + 5 * 32;
-                double ArL = __ldg(a.A_r + v.orf + i + (long long)(v.nr + 1) * j);
-                double ArR = __ldg(a.A_r + v.orf + i + 1 + (long long)(v.nr + 1) * j);
-                double AZL = __ldg(a.A_Z + v.ozf + cl), AZR = __ldg(a.A_Z + v.ozf + cl + v.nr);
-                double fac = ctdt * __ldg(a.inv_dV + c);
+                double ArL, ArR, AZL, AZR, fac;
+                if constexpr (PRE) {
+                    ArL = g[G_ARL]; ArR = g[G_ARR]; AZL = g[G_AZL]; AZR = g[G_AZR];
+                    fac = ctdt * g[G_IDV];
+                } else {
+                    ArL = __ldg(a.A_r + v.orf + i + (long long)(v.nr + 1) * j);
+                    ArR = __ldg(a.A_r + v.orf + i + 1 + (long long)(v.nr + 1) * j);
+                    AZL = __ldg(a.A_Z + v.ozf + cl); AZR = __ldg(a.A_Z + v.ozf + cl + v.nr);
+                    fac = ctdt * __ldg(a.inv_dV + c);
+                }
                 // increments in R, accumulated into the state in S
                 S Jn, Hrn, HZn;
                 const S ujeps = S(a.jeps);
@@ -356,14 +437,19 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
                 }
                 const S Jn0 = Jn;
                 Jn = Jn > ujeps ? Jn : ujeps;
-                R ga = R(__ldg(a.dur_dr + c)), gb = R(__ldg(a.dur_dZ + c)), gc = R(__ldg(a.duZ_dr + c));
-                R gd = R(__ldg(a.duZ_dZ + c)), ge = R(__ldg(a.ur_over_r + c));
+                R ga, gb, gc, gd, ge;
+                if constexpr (PRE) {
+                    ga = R(g[G_DURDR]); gb = R(g[G_DURDZ]); gc = R(g[G_DUZDR]); gd = R(g[G_DUZDZ]); ge = R(g[G_UROR]);
+                } else {
+                    ga = R(__ldg(a.dur_dr + c)); gb = R(__ldg(a.dur_dZ + c)); gc = R(__ldg(a.duZ_dr + c));
+                    gd = R(__ldg(a.duZ_dZ + c)); ge = R(__ldg(a.ur_over_r + c));
+                }
                 R DdU = d_colon_grad_u<R>(Drr, DrZ, DZZ, ga, gb, gc, gd, ge);
                 R Kav = R(0.5) * (FL[128] + FR[96]);
                 if (sizeof(R) == 8)
                     Hrn += S(R(ctdt) * Kav * R(__ldg(a.inv_r_cell + v.ocol + i)));
                 else
-                    Hrn += S(R(ctdt * __ldg(a.inv_r_cell + v.ocol + i)) * Kav);
+                    Hrn += S(R(ctdt * g[G_IRC]) * Kav);
                 R cc = R(ctdt_c);
                 R dHr = -cc * (sHr * ga + sHZ * gb);
                 R dHZ = -cc * (sHr * gc + sHZ * gd);
@@ -390,6 +476,12 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
             }
         }
         zL[0] = zR[0]; zL[1] = zR[1]; zL[2] = zR[2];
+        // the next row's scalars replace this row's once every lane of the warp has read them;
+        // the next row's first barrier publishes them
+        if constexpr (PRE) {
+            __syncwarp();
+            if (lane < GEO_N) g[lane] = gnext;
+        }
     }
 }
 
@@ -1155,7 +1247,8 @@ __global__ void __launch_bounds__(1024) k_reduce(RedArgs a) {
 template <typename S, typename R>
 static size_t adv_smem_bytes() {
     constexpr int HF = sizeof(S) == sizeof(R) ? 2 : 3;
-    return sizeof(R) * 32 * (RING * MCOL * nf<R>() + (MT + 1) * 5) + sizeof(S) * 32 * RING * MT * HF;
+    return sizeof(R) * 32 * (RING * MCOL * nf<R>() + (MT + 1) * 5) + sizeof(S) * 32 * RING * MT * HF +
+           (sizeof(R) == 4 ? sizeof(double) * MWARPS * GEO_N : 0);   // the row slots (FP32 arithmetic)
 }
 
 template <typename S, typename R, int FLUX, int MINB>

@@ -4,6 +4,8 @@
                                                   # adjoint of 6 steps (every step kept)
     python -m lydion_b200.profile_cases rhd       # RHD Lya block on the 256x256x64 grid: prepare,
                                                   # then 4 absorption sub-steps of 0.1 t_abs
+    python -m lydion_b200.profile_cases step      # the dusty-outflow 256x256x64 cloud, mixed form,
+                                                  # 16 rows per advection tile, 4 CTAs/SM: 20 steps
 """
 import sys
 
@@ -41,6 +43,18 @@ def rhd_case():
     return 0.0
 
 
+def step_case():
+    from . import workloads as W
+    from ._lib import PREC_MIXED
+    from .m1 import context_for_cloud
+    cl = W.config_c2()
+    ctx = context_for_cloud(cl, precision=PREC_MIXED)
+    ctx.set_tuning(16, 0, 0, 4)
+    h = ctx.static_steps(20, cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+    ctx.close()
+    return float(h[-1, 0])
+
+
 if __name__ == "__main__":
     case = sys.argv[1] if len(sys.argv) > 1 else "adjoint"
-    print(case, {"adjoint": adjoint_case, "rhd": rhd_case}[case]())
+    print(case, {"adjoint": adjoint_case, "rhd": rhd_case, "step": step_case}[case]())
