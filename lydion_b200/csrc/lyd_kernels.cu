@@ -466,7 +466,14 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
                 Jn = Jn > ujeps ? Jn : ujeps;
                 S H2 = Hrn * Hrn + HZn * HZn;
                 if (H2 > Jn * Jn) {
-                    S fsc = Jn / rsq(H2);
+                    S fsc;
+                    if constexpr (sizeof(S) == 4) {
+                        // a flushed (zero) root of a subnormal |H|^2 scales H to zero
+                        const S Hm = rsq(H2);
+                        fsc = Hm > S(0) ? Jn / Hm : S(0);
+                    } else {
+                        fsc = Jn / rsq(H2);
+                    }
                     Hrn *= fsc;
                     HZn *= fsc;
                 }

@@ -64,3 +64,21 @@ def test_mixed_batch_matches_fp64_batch():
     for q in range(len(clouds)):
         assert float(np.max(np.abs(hb[:, q, 0] - ha[:, q, 0]))) <= 1e-5 * float(np.max(np.abs(ha[:, q, 0]))), q
         assert norm_err(b.download_cloud(q, "J"), a.download_cloud(q, "J")) < 2e-5, q
+
+
+@pytest.mark.parametrize("prec_name,tol", [("PREC_MIXED", 1e-5), ("PREC_FP32", 1e-4)])
+def test_reduced_precision_on_rhd_snapshot(prec_name, tol):
+    """The synthetic RHD snapshot (photoionised bubble in neutral 100 K gas, 128 bins) carries
+    fluxes whose squares fall below FP32's normal range in the far wings: the FP32 arithmetic
+    must stay finite there and keep M_F within its tolerance of the FP64 step."""
+    from lydion_b200 import _lib
+    from lydion_b200.m1 import context_for_cloud
+    cl = W.rhd_snapshot_cloud(n=128, n_nu=128)
+    a = context_for_cloud(cl)
+    b = context_for_cloud(cl, precision=getattr(_lib, prec_name))
+    n = 200
+    ha, hb = _run(a, cl, n), _run(b, cl, n)
+    assert np.isfinite(hb).all()
+    for f in ("J", "H_r", "H_Z"):
+        assert np.isfinite(b.download(f)).all(), f
+    assert float(np.max(np.abs(hb[:, 0] - ha[:, 0]))) <= tol * float(np.max(np.abs(ha[:, 0])))
