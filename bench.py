@@ -484,7 +484,7 @@ def run_gpu(args):
     ab = algorithmic_bytes(cloud.n_nu, 8)[names[dom]] * cloud.cell_bins
     peaks, src = measured_peaks()
     achieved = ab / (kms[dom] * 1e-3) / 1e9
-    variant = {"advect": "mixed", "freq": "fp64"}[names[dom]]   # the mixed form runs the FP64 frequency kernel
+    variant = "mixed"
     traffic = profile_traffic("k_" + names[dom], variant)
     cpu = cpu_baseline(cloud) if (rank == 0 and world == 1 and not args.no_cpu) else None
     if rank == 0:

@@ -763,7 +763,14 @@ __device__ __forceinline__ void warp_cell_run(int4 it, int warp, int nw, int &wb
 // Up to four bins per lane the kernel is held to 2 CTAs per SM (128 registers). Four bins:
 // ~230 B of spills, measured 1.4x faster than 1 CTA at 172 registers. Two bins: 1.8x faster
 // than the 164 registers ptxas picks when only the block size bounds it.
-template <typename S, typename R, int M>
+// RC is the arithmetic of the cell-centre closure D(J, H) and of D:grad u that enter the Doppler
+// term of the frequency factors: R in the FP64 and FP32-storage forms, FP32 in the mixed form.
+// The closure only sets the velocity of the Peclet numbers; every factor is then formed in FP64
+// from that one velocity, so its rounding moves the step like a velocity field off by 1e-7
+// relative, not like the rounding of F against F+ + F- that the factors themselves cannot take
+// (mixed frequency kernel at 256^2 x 64: 0.259 -> 0.246 ms; the mixed form's M_F after 2000
+// steps 5.93e-7 -> 5.95e-7 from FP64).
+template <typename S, typename R, int M, typename RC = R>
 __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<S> a) {
     extern __shared__ __align__(16) double fsm[];
     constexpr int NP = 32 * M;
@@ -962,9 +969,10 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
                     int k = lane * M + m;
                     Fp[m] = 0.0; F0[m] = 0.0; Fm[m] = 0.0;
                     if (k < 1 || k > nnu - 2) continue;
-                    R Drr, DZZ, DrZ;
-                    D_edd<R>(R(Hr[m]), R(HZ[m]), R(J[m]), R(jeps), R(a.heps2), Drr, DZZ, DrZ);
-                    double vel = double(d_colon_grad_u<R>(Drr, DrZ, DZZ, ga, gb, gc, gd, ge)) * kInvC;
+                    RC Drr, DZZ, DrZ;
+                    D_edd<RC>(RC(Hr[m]), RC(HZ[m]), RC(J[m]), RC(jeps), RC(a.heps2), Drr, DZZ, DrZ);
+                    double vel =
+                        double(d_colon_grad_u<RC>(Drr, DrZ, DZZ, RC(ga), RC(gb), RC(gc), RC(gd), RC(ge))) * kInvC;
                     double Kk = Kb[m];
                     double Kkm = (m > 0) ? Kb[m - 1] : K_up;
                     double Kkp = (m < M - 1) ? Kb[m + 1] : K_dn;
@@ -1311,35 +1319,37 @@ int freq_blocks(int ncell, int dev) {
     return want < cap ? (want > 0 ? want : 1) : cap;
 }
 
-template <typename S, typename R, int M>
+template <typename S, typename R, int M, typename RC>
 static void freq_launch(const void *args, int nitems, cudaStream_t st) {
     const FreqArgs<S> &fa = *static_cast<const FreqArgs<S> *>(args);
     const size_t sm = sizeof(double) * freq_smem_doubles<M>(FREQ_THREADS / 32, fa.solver == SOLVER_THOMAS);
     static bool attr = false;
     if (!attr) {
         const size_t smax = sizeof(double) * freq_smem_doubles<M>(FREQ_THREADS / 32, true);
-        cudaFuncSetAttribute(k_freq<S, R, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
+        cudaFuncSetAttribute(k_freq<S, R, M, RC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
         attr = true;
     }
-    k_freq<S, R, M><<<nitems, FREQ_THREADS, sm, st>>>(fa);
+    k_freq<S, R, M, RC><<<nitems, FREQ_THREADS, sm, st>>>(fa);
 }
 
 void launch_freq(int prec, const void *args, int nnu, int nitems, cudaStream_t st) {
     if (nitems <= 0) return;
     int M = bins_per_lane(nnu);
-#define LYD_FQ(S_, R_)                                             \
-    switch (M) {                                                   \
-    case 1: freq_launch<S_, R_, 1>(args, nitems, st); break;       \
-    case 2: freq_launch<S_, R_, 2>(args, nitems, st); break;       \
-    case 4: freq_launch<S_, R_, 4>(args, nitems, st); break;       \
-    default: freq_launch<S_, R_, 8>(args, nitems, st); break;      \
+#define LYD_FQ(S_, R_, RC_)                                              \
+    switch (M) {                                                         \
+    case 1: freq_launch<S_, R_, 1, RC_>(args, nitems, st); break;        \
+    case 2: freq_launch<S_, R_, 2, RC_>(args, nitems, st); break;        \
+    case 4: freq_launch<S_, R_, 4, RC_>(args, nitems, st); break;        \
+    default: freq_launch<S_, R_, 8, RC_>(args, nitems, st); break;       \
     }
-    // the mixed variant keeps the whole frequency step in FP64 (its state, factors and solve
-    // need it; its closure and emission are a small part of the kernel's time)
+    // the mixed variant keeps the frequency step in FP64 (its state, factors and solve need
+    // it) except the closure that sets the Doppler velocity (see k_freq)
     if (prec == PREC_K_FP32) {
-        LYD_FQ(float, float)
+        LYD_FQ(float, float, float)
+    } else if (prec == PREC_K_MIXED) {
+        LYD_FQ(double, double, float)
     } else {
-        LYD_FQ(double, double)
+        LYD_FQ(double, double, double)
     }
 #undef LYD_FQ
 }
