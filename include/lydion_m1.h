@@ -47,7 +47,8 @@ extern "C" {
 #define LYD_PREC_MIXED  1   /* FP64 state storage; the advection's reconstruction, closure,
                                fluxes and limiters in FP32 with the cell update accumulated
                                in FP64; the frequency step (factors, tridiagonal solve) and
-                               all reductions in FP64                                        */
+                               all reductions in FP64, bar the cell-centre closure that sets
+                               the Doppler velocity of the factors (FP32)                    */
 #define LYD_PREC_FP32   2   /* FP32 storage and bulk arithmetic; FP64 tridiagonal solve and
                                reductions (fastest, least accurate: weak bins lose digits)  */
 
