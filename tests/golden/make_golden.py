@@ -10,7 +10,10 @@ Run from the repository root:  python tests/golden/make_golden.py
   Voigt look-up-table nodes x_i = -1000 + 0.01 i (src/FastInterpolations.jl:175-197); scipy's
   dawsn and SpecialFunctions.jl's dawson both evaluate the Faddeeva-package algorithm.
 * analytic_spectra.npz -- the analytic emergent spectra J_sphere_point / J_sphere_uni of
-  src/ConstantsAndFunctions.jl:1018-1049 on an x grid, for physics-level checks.
+  src/ConstantsAndFunctions.jl:1018-1049 on an x grid, for physics-level checks, and the
+  reference's tabulated analytic force multiplier M_F / (a tau_cl)^(1/3) of a uniform source
+  against the dust parameter eps_1 (EscapeFractionTest_StaticCloud/AnalyticalMF_UniformSource.txt,
+  read as text; its first rows are the dust-free limit).
 """
 import os
 import sys
@@ -84,6 +87,9 @@ def analytic_spectra():
             un = -np.sqrt(6 / np.pi) * (x ** 2 / at) * np.log(1 - np.exp(-np.sqrt(2 * np.pi ** 3 / 27) * np.abs(x ** 3) / at))
         out[f"point_T{T:g}_tau{tau:g}"] = np.nan_to_num(pt, nan=0.0)
         out[f"uni_T{T:g}_tau{tau:g}"] = np.nan_to_num(un, nan=0.0)
+    mf = np.loadtxt(os.path.join("/root/reference", "EscapeFractionTest_StaticCloud", "AnalyticalMF_UniformSource.txt"))
+    out["mf_uniform_eps1"] = mf[:8, 0]
+    out["mf_uniform_over_atau13"] = mf[:8, 1]
     np.savez_compressed(os.path.join(HERE, "analytic_spectra.npz"), **out)
 
 
