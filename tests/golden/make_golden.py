@@ -13,7 +13,9 @@ Run from the repository root:  python tests/golden/make_golden.py
   src/ConstantsAndFunctions.jl:1018-1049 on an x grid, for physics-level checks, and the
   reference's tabulated analytic force multiplier M_F / (a tau_cl)^(1/3) of a uniform source
   against the dust parameter eps_1 (EscapeFractionTest_StaticCloud/AnalyticalMF_UniformSource.txt,
-  read as text; its first rows are the dust-free limit).
+  read as text; its first rows are the dust-free limit), and its analytic escape fractions of
+  dusty point- and uniform-source clouds against eps_1 = 0.4707 (a tau_cl)^(1/3) tau_abs
+  (AnalyticalEscapeFraction_{Point,Uniform}Source.txt, stored as -f_esc there).
 """
 import os
 import sys
@@ -90,6 +92,10 @@ def analytic_spectra():
     mf = np.loadtxt(os.path.join("/root/reference", "EscapeFractionTest_StaticCloud", "AnalyticalMF_UniformSource.txt"))
     out["mf_uniform_eps1"] = mf[:8, 0]
     out["mf_uniform_over_atau13"] = mf[:8, 1]
+    for kind, fn in (("point", "PointSource"), ("uni", "UniformSource")):
+        t = np.loadtxt(os.path.join("/root/reference", "EscapeFractionTest_StaticCloud", f"AnalyticalEscapeFraction_{fn}.txt"))
+        out[f"fesc_{kind}_eps1"] = t[:, 0]
+        out[f"fesc_{kind}"] = -t[:, 1]
     np.savez_compressed(os.path.join(HERE, "analytic_spectra.npz"), **out)
 
 
