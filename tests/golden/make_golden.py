@@ -15,7 +15,9 @@ Run from the repository root:  python tests/golden/make_golden.py
   against the dust parameter eps_1 (EscapeFractionTest_StaticCloud/AnalyticalMF_UniformSource.txt,
   read as text; its first rows are the dust-free limit), and its analytic escape fractions of
   dusty point- and uniform-source clouds against eps_1 = 0.4707 (a tau_cl)^(1/3) tau_abs
-  (AnalyticalEscapeFraction_{Point,Uniform}Source.txt, stored as -f_esc there).
+  (AnalyticalEscapeFraction_{Point,Uniform}Source.txt, stored as -f_esc there), and the
+  reference's MCRT comoving spectra of expanding uniform-source clouds with v_max = 10 and
+  200 km/s (VelocityGradientsTest/comoving_MCRT_uniform_{10,200}.txt).
 """
 import os
 import sys
@@ -96,6 +98,10 @@ def analytic_spectra():
         t = np.loadtxt(os.path.join("/root/reference", "EscapeFractionTest_StaticCloud", f"AnalyticalEscapeFraction_{fn}.txt"))
         out[f"fesc_{kind}_eps1"] = t[:, 0]
         out[f"fesc_{kind}"] = -t[:, 1]
+    for v in (10, 200):
+        t = np.loadtxt(os.path.join("/root/reference", "VelocityGradientsTest", f"comoving_MCRT_uniform_{v}.txt"))
+        out[f"mcrt_v{v}_x"] = t[:, 0]
+        out[f"mcrt_v{v}"] = t[:, 1]
     np.savez_compressed(os.path.join(HERE, "analytic_spectra.npz"), **out)
 
 
