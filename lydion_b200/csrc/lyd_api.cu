@@ -89,6 +89,8 @@ struct lyd_ctx {
     double *hist = nullptr;
     int hist_cap = 0;                  // steps
     int *step_ctr = nullptr;           // [0] record index, [1] completion counter
+    double *red_cols = nullptr;        // column sums of the reduction [cloud][N_nu + kExtraCols]
+    int *red_cnt = nullptr;            // per-cloud CTA counters of the reduction (zero between launches)
     double *last = nullptr;
     int *err = nullptr;
     double *lut = nullptr;
@@ -318,6 +320,8 @@ int lyd_batch_create(lyd_ctx **out, int32_t ncl, const int32_t *n_r, const int32
     A((void **)&c->cl, (size_t)ncl * sizeof(CloudDesc));
     A((void **)&c->kwin, (size_t)2 * ncl * sizeof(int));
     A((void **)&c->step_ctr, 2 * sizeof(int));
+    A((void **)&c->red_cols, (size_t)ncl * (c->nnu + kExtraCols) * sizeof(double));
+    A((void **)&c->red_cnt, (size_t)ncl * sizeof(int));
     A((void **)&c->last, (size_t)7 * ncl * sizeof(double));
     A((void **)&c->err, sizeof(int));
     A((void **)&c->small, 512 * 8);
@@ -352,7 +356,8 @@ int lyd_destroy(lyd_ctx *c) {
     void *ps[] = {c->Hv, c->phi, c->phi_inv, c->aF, c->Ff[0], c->Ff[1], c->Ff[2], c->u_r_star, c->u_Z_star, c->dV,
                   c->inv_dV, c->A_r, c->A_Z, c->inv_r_cell, c->rCoM, c->ZCoM, c->rint, c->zint, c->r_if, c->Z_if,
                   c->nu, c->nuC, c->dnu, c->inv_dnu, c->inv_nuC, c->partials, c->kwin, c->hist, c->step_ctr,
-                  c->last, c->err, c->lut, c->stage, c->small, c->cl, c->tiles, c->items, c->adj_ws};
+                  c->last, c->err, c->lut, c->stage, c->small, c->cl, c->tiles, c->items, c->adj_ws,
+                  c->red_cols, c->red_cnt};
     for (void *p : ps) cudaFree(p);
     for (int q = 0; q < CF_N; q++) cudaFree(c->cellf[q]);
     cudaFree(c->dust_F);
@@ -685,6 +690,7 @@ static RedArgs red_args(lyd_ctx *c, int parts) {
     r.partials = c->partials; r.nblocks = c->nitems; r.nnu = c->nnu; r.nclouds = c->ncl; r.parts = parts;
     r.kcore_min = c->cfg.kcore_min; r.kcore_max = c->cfg.kcore_max;
     r.j_scale = c->jscale; r.cl = c->cl; r.kwin = c->kwin; r.last = c->last;
+    r.colsum = c->red_cols; r.cnt = c->red_cnt;
     return r;
 }
 
@@ -1152,6 +1158,8 @@ int lyd_dd_finish(lyd_ctx *c, const double *colsum, int32_t step, lyd_diag *rec)
     ra.partials = colsum;
     ra.nblocks = 1;
     ra.cl = c->dd_cl;
+    ra.colsum = nullptr;   // the input is already the column sums: one CTA reads them
+    ra.cnt = nullptr;
     launch_reduce(ra, c->st);
     LYD_CU(c, cudaGetLastError());
     c->active_valid = true;

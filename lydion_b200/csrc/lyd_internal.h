@@ -117,6 +117,11 @@ struct RedArgs {
     int *done;                   // completion counter of the CTAs of one launch
     int hist_capacity;           // steps
     double *last;                // out: latest record per cloud [cloud][7]
+    // Column sums over several CTAs per cloud (8 columns each), the last CTA of a cloud to
+    // finish taking the decision: the sums [cloud][N_nu + kExtraCols] and the per-cloud CTA
+    // counters (zero between launches). Both null: one CTA per cloud sums every column.
+    double *colsum;
+    int *cnt;
 };
 
 // error bits

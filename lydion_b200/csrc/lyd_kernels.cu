@@ -1194,22 +1194,47 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_find_active(const S *J, int nn
     }
 }
 
-// One CTA per cloud: column sums of the cloud's partials (one warp per column, fixed order),
-// then FindActiveBins' decision and the diagnostics of Update_f_Lya_MF_L_Lya! /
-// Compute_f_esc_Lya_Cylindrical. The last CTA to finish advances the record index.
+// Column sums of each cloud's partials (one warp per column, a fixed order), then, by one thread
+// per cloud, FindActiveBins' decision and the diagnostics of Update_f_Lya_MF_L_Lya! /
+// Compute_f_esc_Lya_Cylindrical. With a.cnt set, each cloud's columns are spread over CTAs of
+// 8 warps, one column per warp, whose sums go through a.colsum; the last CTA of the cloud to
+// finish takes the decision. Without, one CTA per cloud sums every column. The last decision
+// of the launch advances the record index.
 __global__ void __launch_bounds__(1024) k_reduce(RedArgs a) {
     __shared__ double col[256 + kExtraCols];
+    __shared__ int is_last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int cloud = blockIdx.x;
-    const CloudDesc &cd = a.cl[cloud];
     const int ncols = a.nnu + kExtraCols;
-    for (int cc = warp; cc < ncols; cc += nw) {
+    const bool split = a.cnt != nullptr;
+    const int nchunks = split ? (ncols + nw - 1) / nw : 1;
+    const int cloud = blockIdx.x / nchunks, chunk = blockIdx.x % nchunks;
+    const CloudDesc &cd = a.cl[cloud];
+    const int npb = cd.npb;
+    const double *pbase = a.partials + cd.pb0;
+    const int c0 = split ? chunk * nw : 0, c1 = split ? min(ncols, c0 + nw) : ncols;
+    for (int cc = c0 + warp; cc < c1; cc += nw) {
         bool need = (cc < a.nnu + 1) ? (a.parts & PART_ACTIVE) : (a.parts & PART_DIAG);
         double s = 0.0;
-        if (need)
-            for (int b = lane; b < cd.npb; b += 32) s += a.partials[(size_t)cc * a.nblocks + cd.pb0 + b];
+        if (need) {
+            const double *p = pbase + (size_t)cc * a.nblocks;
+            for (int b = lane; b < npb; b += 32) s += p[b];
+        }
         s = warp_sum(s);
-        if (lane == 0) col[cc] = s;
+        if (lane == 0) {
+            col[cc] = s;
+            if (split) a.colsum[(size_t)cloud * ncols + cc] = s;
+        }
+    }
+    if (split) {
+        // the last CTA of this cloud gathers the other CTAs' sums (threadfence reduction)
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) is_last = atomicAdd(a.cnt + cloud, 1) == nchunks - 1;
+        __syncthreads();
+        if (!is_last) return;
+        __threadfence();
+        for (int cc = threadIdx.x; cc < ncols; cc += blockDim.x) col[cc] = __ldcg(a.colsum + (size_t)cloud * ncols + cc);
+        if (threadIdx.x == 0) a.cnt[cloud] = 0;
     }
     __syncthreads();
     if (threadIdx.x != 0) return;
@@ -1378,7 +1403,15 @@ void launch_find_active(int sprec, const void *J, int nnu, const double *dnu, co
 }
 
 void launch_reduce(const RedArgs &a, cudaStream_t st) {
-    if (a.nclouds > 0) k_reduce<<<a.nclouds, 1024, 0, st>>>(a);
+    if (a.nclouds <= 0) return;
+    if (a.cnt && a.colsum) {
+        const int nchunks = (a.nnu + kExtraCols + 7) / 8;
+        k_reduce<<<a.nclouds * nchunks, 256, 0, st>>>(a);
+    } else {
+        RedArgs b = a;
+        b.cnt = nullptr;
+        k_reduce<<<a.nclouds, 1024, 0, st>>>(b);
+    }
 }
 
 }  // namespace lyd
