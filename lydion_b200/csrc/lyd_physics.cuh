@@ -92,6 +92,17 @@ template <> __device__ __forceinline__ float rcp<float>(float y) {
     return x;
 }
 
+// Reciprocal square root 1 / sqrt(x) for FP32 arithmetic: the hardware's approximation alone
+// (PTX rsqrt.approx.ftz.f32, relative error within 2^-22.9 over the normal range; a subnormal
+// or zero argument gives +inf, so callers check x against FLT_MIN first). One transcendental
+// operation gives both a length, x * rsqf(x), and its reciprocal.
+__device__ __forceinline__ float rsqf(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float kFltMinNormal = 1.17549435e-38f;
+
 // MinMod, src/ConstantsAndFunctions.jl:1571-1582
 template <typename R>
 __device__ __forceinline__ R minmod(R a, R b) {
@@ -99,10 +110,17 @@ __device__ __forceinline__ R minmod(R a, R b) {
 }
 
 // Levermore closure chi(f), src/M1Closure.jl:28-33
+// With FP32 arithmetic it is evaluated as (5 - 2 sqrt(4 - 3 f^2)) / 3, the same function
+// (multiply numerator and denominator by 5 - 2 sqrt(4 - 3 f^2): the denominator becomes
+// 3 (3 + 4 f^2)), with one square root and no reciprocal; 5 - 2 sqrt(..) >= 1 for f <= 1, so
+// nothing cancels.
 template <typename R>
 __device__ __forceinline__ R chi_L84(R f) {
     R f2 = f * f;
-    return (R(3) + R(4) * f2) * rcp<R>(R(5) + R(2) * rsq(R(4) - R(3) * f2));
+    if constexpr (sizeof(R) == 4)
+        return (R(5) - R(2) * rsq(R(4) - R(3) * f2)) * R(1.0f / 3.0f);
+    else
+        return (R(3) + R(4) * f2) * rcp<R>(R(5) + R(2) * rsq(R(4) - R(3) * f2));
 }
 
 // Compute_D_Edd_from_f_n, src/M1Closure.jl:91-119
@@ -131,17 +149,21 @@ __device__ __forceinline__ void D_edd(R Hr, R HZ, R J, R jeps, R heps2, R &Drr, 
         Drr = Num<R>::third(); DZZ = Num<R>::third(); DrZ = R(0);
         return;
     }
-    R Hmag = rsq(H2);
+    R Hmag, inv_H;
     if constexpr (sizeof(R) == 4) {
-        if (!(Hmag > R(0))) {   // |H|^2 below FP32's normal range (flushed root): no direction
+        if (!(H2 >= kFltMinNormal)) {   // |H|^2 below FP32's normal range: no direction
             Drr = Num<R>::third(); DZZ = Num<R>::third(); DrZ = R(0);
             return;
         }
+        inv_H = rsqf(H2);
+        Hmag = H2 * inv_H;
+    } else {
+        Hmag = rsq(H2);
+        inv_H = rcp<R>(Hmag);
     }
     R f = Hmag * rcp<R>(J);
     f = f < Num<R>::fmin() ? Num<R>::fmin() : (f > Num<R>::fmax() ? Num<R>::fmax() : f);
     R chi = chi_L84(f);
-    R inv_H = rcp<R>(Hmag);
     R a = (R(1) - chi) * R(0.5);
     R b = (R(3) * chi - R(1)) * R(0.5);
     R nr = Hr * inv_H, nZ = HZ * inv_H;
@@ -158,8 +180,14 @@ __device__ __forceinline__ void hll_eigen(R f, R mu, R &l1, R &l3) {
     mu = mu < R(-1) ? R(-1) : (mu > R(1) ? R(1) : mu);
     R f2 = f * f, mu2 = mu * mu, muf = mu * f;
     R t = R(4) - R(3) * f2;
-    R sq = rsq(t > R(0) ? t : R(0));
-    R inv_sq = rcp<R>(sq);
+    R sq, inv_sq;
+    if constexpr (sizeof(R) == 4) {   // t >= 1 (f <= fmax < 1): one reciprocal square root
+        inv_sq = rsqf(t);
+        sq = t * inv_sq;
+    } else {
+        sq = rsq(t > R(0) ? t : R(0));
+        inv_sq = rcp<R>(sq);
+    }
     R g = R(2) / R(3) * (R(4) - R(3) * f2 - sq) + R(2) * mu2 * (R(2) - f2 - sq);
     R fac = rsq(g > R(0) ? g : R(0));
     R x1 = (muf - fac) * inv_sq, x3 = (muf + fac) * inv_sq;
@@ -214,6 +242,22 @@ __device__ __forceinline__ Recon<R> reconstruct_f(const CellF<R> &cm1, const Cel
     R frL = ci.fr + dfrL * dL, frR = cp1.fr - dfrR * dR;
     R fZL = ci.fZ + dfZL * dL, fZR = cp1.fZ - dfZR * dR;
 
+    if constexpr (sizeof(R) == 4) {
+        // one reciprocal square root gives |f| and 1/|f|; |f|^2 below FP32's normal range
+        // counts as no flux (no direction)
+        const R sL = frL * frL + fZL * fZL, sR = frR * frR + fZR * fZR;
+        const bool nzL = sL >= kFltMinNormal, nzR = sR >= kFltMinNormal;
+        R iL = nzL ? rsqf(sL) : R(0), iR = nzR ? rsqf(sR) : R(0);
+        R fL = sL * iL, fR = sR * iR;
+        if (fL > R(1)) { frL *= iL; fZL *= iL; fL = R(1); iL = R(1); }
+        if (fR > R(1)) { frR *= iR; fZR *= iR; fR = R(1); iR = R(1); }
+        o.Hr_L = frL * o.J_L; o.Hr_R = frR * o.J_R;
+        o.HZ_L = fZL * o.J_L; o.HZ_R = fZR * o.J_R;
+        o.nr_L = frL * iL; o.nZ_L = fZL * iL;
+        o.nr_R = frR * iR; o.nZ_R = fZR * iR;
+        o.f_L = fL; o.f_R = fR;
+        return o;
+    }
     R fL = rsq(frL * frL + fZL * fZL);
     if (fL > R(1)) { R inv = rcp<R>(fL); frL *= inv; fZL *= inv; fL = R(1); }
     R fR = rsq(frR * frR + fZR * fZR);
