@@ -144,12 +144,15 @@ def main():
         ctx = context_for_cloud(cl)
         p = (cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
         run = lambda n: ctx.static_steps(n, *p, history=False)
+        init = {n: ctx.download(n) for n in ("J", "H_r", "H_Z")}
+        reset = lambda: [ctx.upload(n, x) for n, x in init.items()]
     else:
         clouds = W.config_c3()
         ctx = batch_for_clouds(clouds)
         pp = cloud_params(clouds)
         run = lambda n: ctx.batch_steps(n, pp, history=False)
-    t = autotune(ctx, run, steps=args.steps, force=args.force)
+        reset = None
+    t = autotune(ctx, run, steps=args.steps, force=args.force, reset=reset)
     print(json.dumps({"workload": args.workload, "tuning": list(t), "cache": cache_path()}))
     ctx.close()
 
