@@ -28,6 +28,7 @@ from scipy.special import erf, dawsn
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
+REF = "/root/reference"   # the reference checkout whose data files are read as text
 
 
 def dgtsv_cases():
@@ -91,15 +92,15 @@ def analytic_spectra():
             un = -np.sqrt(6 / np.pi) * (x ** 2 / at) * np.log(1 - np.exp(-np.sqrt(2 * np.pi ** 3 / 27) * np.abs(x ** 3) / at))
         out[f"point_T{T:g}_tau{tau:g}"] = np.nan_to_num(pt, nan=0.0)
         out[f"uni_T{T:g}_tau{tau:g}"] = np.nan_to_num(un, nan=0.0)
-    mf = np.loadtxt(os.path.join("/root/reference", "EscapeFractionTest_StaticCloud", "AnalyticalMF_UniformSource.txt"))
+    mf = np.loadtxt(os.path.join(REF, "EscapeFractionTest_StaticCloud", "AnalyticalMF_UniformSource.txt"))
     out["mf_uniform_eps1"] = mf[:8, 0]
     out["mf_uniform_over_atau13"] = mf[:8, 1]
     for kind, fn in (("point", "PointSource"), ("uni", "UniformSource")):
-        t = np.loadtxt(os.path.join("/root/reference", "EscapeFractionTest_StaticCloud", f"AnalyticalEscapeFraction_{fn}.txt"))
+        t = np.loadtxt(os.path.join(REF, "EscapeFractionTest_StaticCloud", f"AnalyticalEscapeFraction_{fn}.txt"))
         out[f"fesc_{kind}_eps1"] = t[:, 0]
         out[f"fesc_{kind}"] = -t[:, 1]
     for v in (10, 200):
-        t = np.loadtxt(os.path.join("/root/reference", "VelocityGradientsTest", f"comoving_MCRT_uniform_{v}.txt"))
+        t = np.loadtxt(os.path.join(REF, "VelocityGradientsTest", f"comoving_MCRT_uniform_{v}.txt"))
         out[f"mcrt_v{v}_x"] = t[:, 0]
         out[f"mcrt_v{v}"] = t[:, 1]
     np.savez_compressed(os.path.join(HERE, "analytic_spectra.npz"), **out)
