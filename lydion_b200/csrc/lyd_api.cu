@@ -970,9 +970,10 @@ template <typename S>
 // One step from set[cur] back into set[cur] (x_A in the other set). The adjoint's forward sweep
 // passes `tape` to record the advection's tape, `in` / `out` (three fields each, n3 apart) to
 // read s_n from and write s_{n+1} into its own storage instead, and `ff` to keep the frequency
-// factors F+, F, F- (n3 apart).
+// factors F+, F, F- (n3 apart), and `win_next` to receive the window the step decides for the
+// next one.
 static int enqueue_step(lyd_ctx *c, bool timed, double *tape = nullptr, const S *in = nullptr, S *out = nullptr,
-                        double *ff = nullptr, bool reduce = true) {
+                        double *ff = nullptr, bool reduce = true, int *win_next = nullptr) {
     const int A = c->cur, B = 1 - c->cur;
     AdvArgs<S> aa;
     fill_adv<S>(c, aa, A, B);
@@ -992,6 +993,7 @@ static int enqueue_step(lyd_ctx *c, bool timed, double *tape = nullptr, const S 
     if (ff) { fa.Fkp = ff; fa.Fk = ff + c->n3; fa.Fkm = ff + 2 * c->n3; }
     RedArgs ra = red_args(c, PART_ACTIVE | PART_DIAG);
     ra.diag = c->hist; ra.step_counter = c->step_ctr; ra.done = c->step_ctr + 1; ra.hist_capacity = c->hist_cap;
+    ra.kwin_copy = win_next;
     const int prec = c->prec;
     if (timed) cudaEventRecord(c->ev[0], c->st);
     launch_advect(prec, c->cfg.flux_method, &aa, c->ntiles, c->tune.adv_ctas_per_sm, c->st);
@@ -1570,21 +1572,24 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_R], 0, nc * 8, c->st));
     LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_Z], 0, nc * 8, c->st));
     if (!c->active_valid) LYD_TRY(run_find_active(c));
+    // win[2n..2n+1] is step n's window: step 0's is copied here, each step's reduction writes
+    // the next one's beside the context's own (no copy between the steps' kernels)
+    LYD_CU(c, cudaMemcpyAsync(win, c->kwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
     if (store_all) {
         // every state lives in the checkpoint storage: step n reads slot n and writes slot n + 1
         // (the last step writes the context's state)
         LYD_TRY(copy_state(ck, c->cur));
         for (int n = 0; n < N; n++) {
-            LYD_CU(c, cudaMemcpyAsync(win + 2 * n, c->kwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
             double *out = n + 1 < N ? ck + (size_t)(n + 1) * S : nullptr;
             LYD_TRY(enqueue_step<double>(c, false, segT + (size_t)n * 4 * n3, ck + (size_t)n * S, out,
-                                         ffs ? ffs + (size_t)n * 3 * n3 : nullptr));
+                                         ffs ? ffs + (size_t)n * 3 * n3 : nullptr, true,
+                                         n + 1 < N ? win + 2 * (n + 1) : nullptr));
         }
     } else {
         for (int n = 0; n < N; n++) {
             if (n % K == 0) LYD_TRY(copy_state(ck + (size_t)(n / K) * S, c->cur));
-            LYD_CU(c, cudaMemcpyAsync(win + 2 * n, c->kwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
-            LYD_TRY(enqueue_step<double>(c, false));
+            LYD_TRY(enqueue_step<double>(c, false, nullptr, nullptr, nullptr, nullptr, true,
+                                         n + 1 < N ? win + 2 * (n + 1) : nullptr));
         }
     }
     LYD_TRY(copy_state(fin, c->cur));

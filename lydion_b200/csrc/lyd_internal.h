@@ -122,6 +122,7 @@ struct RedArgs {
     // counters (zero between launches). Both null: one CTA per cloud sums every column.
     double *colsum;
     int *cnt;
+    int *kwin_copy;              // optional second destination of the decided window [cloud][2]
 };
 
 // error bits

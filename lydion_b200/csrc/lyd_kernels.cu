@@ -1253,6 +1253,10 @@ __global__ void __launch_bounds__(1024) k_reduce(RedArgs a) {
         kmin = kmin < a.kcore_min ? kmin : a.kcore_min;
         kw[0] = kmin;
         kw[1] = kmax;
+        if (a.kwin_copy) {
+            a.kwin_copy[2 * cloud] = kmin;
+            a.kwin_copy[2 * cloud + 1] = kmax;
+        }
     }
     if (a.parts & PART_DIAG) {
         double MF = col[a.nnu + 1], net = col[a.nnu + 2], outw = col[a.nnu + 3];
