@@ -22,6 +22,7 @@ the GPU name and the workload's shape, in $LYDION_TUNE_CACHE or
 import hashlib
 import json
 import os
+import tempfile
 
 import numpy as np
 
@@ -62,11 +63,19 @@ def _load(path):
 
 
 def _save(path, data):
-    os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
-    tmp = path + ".tmp"
-    with open(tmp, "w") as f:
-        json.dump(data, f, indent=1, sort_keys=True)
-    os.replace(tmp, path)
+    """Atomic write through a temporary file of this process's own, so ranks that tune at the
+    same time (one process per GPU) each replace the cache whole; the last one wins."""
+    d = os.path.dirname(path) or "."
+    os.makedirs(d, exist_ok=True)
+    fd, tmp = tempfile.mkstemp(prefix=os.path.basename(path) + ".", suffix=".tmp", dir=d)
+    try:
+        with os.fdopen(fd, "w") as f:
+            json.dump(data, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except BaseException:
+        if os.path.exists(tmp):
+            os.unlink(tmp)
+        raise
 
 
 def _measure(ctx, run, tuning, steps):

@@ -70,3 +70,33 @@ def test_batch_key_depends_on_sizes(monkeypatch):
     assert A.workload_key(a) != A.workload_key(b)
     b.sizes = [(64, 64), (32, 48)]
     assert A.workload_key(a) == A.workload_key(b)
+
+
+def test_reset_runs_before_every_candidate():
+    ctx = FakeCtx()
+    calls = []
+    best, table = A.search(ctx, ctx.run, steps=5, reset=lambda: calls.append(ctx.t))
+    assert len(calls) == len(table)
+
+
+def _writer(path, rank, n):
+    from lydion_b200 import autotune as A_
+    for k in range(n):
+        A_._save(path, {"rank": rank, "k": k})
+
+
+def test_concurrent_cache_writes_stay_whole(tmp_path):
+    """Under torchrun every rank tunes its own GPU and writes the same cache file at once."""
+    import multiprocessing as mp
+    import os
+    path = str(tmp_path / "tuning.json")
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_writer, args=(path, r, 100)) for r in range(4)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+    assert [p.exitcode for p in procs] == [0, 0, 0, 0]
+    data = json.load(open(path))            # one writer's whole record: the last one wins
+    assert data["k"] == 99 and data["rank"] in range(4)
+    assert os.listdir(tmp_path) == ["tuning.json"]   # no temporary file left behind
