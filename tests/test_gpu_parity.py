@@ -305,6 +305,24 @@ def test_full_size_c2_steps_match_oracle(oracle_mod):
         assert norm_err(ctx.download(f), getattr(st, f)) < 1e-9, f
 
 
+def test_c1_point_source_1000_steps_match_oracle(oracle_mod):
+    """The plain-FP64 point-source cloud (64 x 64 x 64, tau0 = 1e6, recoil on) over the 1000
+    steps it is specified with, against the oracle: the active window of every step, M_F, the
+    final J and H and the edge-ring spectra."""
+    cl = W.config_c1()
+    st, ctx = matched_pair(oracle_mod, cl)
+    n = 1000
+    d_o = st.run(n)
+    d_g = ctx.static_steps(n, cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+    np.testing.assert_array_equal(d_g[:, 5:7], d_o[:, 5:7])
+    assert max_rel(d_g[1:, 0], d_o[1:, 0]) < 1e-9
+    for f in ("J", "H_r", "H_Z"):
+        assert norm_err(ctx.download(f), getattr(st, f)) < 1e-9, f
+    raw_g = ctx.edge_spectra()[0]
+    raw_o = st.edge_spectra()[0]
+    assert norm_err(raw_g, raw_o) < 1e-9
+
+
 def test_rhd_snapshot_field_matches_oracle(oracle_mod):
     """The synthetic RHD snapshot (lognormal n_H, photoionised bubble with p_d from pd_Lya,
     shell outflow, dust) at 64 x 64 x 16: a few full steps against the oracle."""
