@@ -2,10 +2,11 @@
 dusty outflowing cloud (tau0 = 1e8, tau_abs = 1, uniform source r_s = 0.5 R_cl, Hubble
 outflow v_max = 200 km/s), one static-cloud driver iteration per step.
 
-The headline value is the mixed-precision form (FP64 state, FP32 advection arithmetic); the
-same line carries the plain-FP64 form, their ratio, the ragged batch of 512 clouds (48 bins,
-sides 32..256) in both forms, the adjoint/forward cost on the 128x128x48 turbulent cloud, and
-the 1024x1024x128 field in both forms.
+The headline value is the FP64 form, the reference's arithmetic. The same line carries the
+reduced-precision forms (FP32 flux arithmetic over FP64 storage; FP32 storage) with their
+ratio to FP64 and their error against it over 2000 steps, the ragged batch of 512 clouds (48
+bins, sides 32..256), the adjoint/forward cost on the 128x128x48 turbulent cloud over 2000
+steps with checkpoints every 100 steps, and the 1024x1024x128 field.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -143,7 +144,7 @@ def run_reference(args):
     st.setup_profiles()
     # one step of the reference arm is one full FP64 step of the whole cloud on the host;
     # the timed count is capped so the run stays within a few minutes of wall clock
-    for _ in range(min(args.warmup, 2)):
+    for _ in range(args.warmup):
         st.step()
     t0 = time.perf_counter()
     n = 0
@@ -224,23 +225,32 @@ def measure_form(cloud, prec, args, barrier, stream_of, local, world, clk=None):
                  "clocks": clocks, "active_fraction": active}
 
 
-def mixed_error_form(cloud, local, n_steps=2000):
-    """Error of the mixed form against FP64 on the headline cloud: both forms run n_steps from
-    the same set-up state; M_F at the last step and over the run, the emergent edge-ring
-    spectrum and the final J, each relative to the FP64 quantity's maximum."""
-    from lydion_b200._lib import PREC_FP64, PREC_MIXED
+def form_errors(cloud, local, precs, n_steps=2000):
+    """Error of each reduced-precision form against FP64 on the headline cloud: every form runs
+    n_steps from the same set-up state. Reported per form: M_F at the last step and over the
+    run, the emergent edge-ring spectrum and the final J, each relative to the FP64 quantity's
+    maximum, and the spectrum per bin relative to the FP64 bin with a floor of 1e-6 of the
+    spectrum's maximum (the wing bins carry the escaping flux)."""
+    from lydion_b200._lib import PREC_FP64
     from lydion_b200.m1 import context_for_cloud
     p = (cloud.c_tilde, cloud.dt, cloud.z_center, cloud.bc_r_right, cloud.bc_z_bot, cloud.bc_z_top)
     res = {}
-    for prec in (PREC_FP64, PREC_MIXED):
+    for prec in (PREC_FP64, *precs.values()):
         ctx = context_for_cloud(cloud, precision=prec, device=local)
         h = ctx.static_steps(n_steps, *p, history=True)
         res[prec] = (h[:, 0].copy(), ctx.edge_spectra()[0].mean(0), ctx.download("J"))
         ctx.close()
-    (ma, sa, Ja), (mb, sb, Jb) = res[PREC_FP64], res[PREC_MIXED]
+    ma, sa, Ja = res[PREC_FP64]
     rel = lambda b, a: float(np.max(np.abs(b - a)) / np.max(np.abs(a)))
-    return {"steps": n_steps, "M_F_last": float(abs(mb[-1] - ma[-1]) / abs(ma[-1])), "M_F_run": rel(mb, ma),
-            "edge_spectrum": rel(sb, sa), "J": rel(Jb, Ja), "spec": 1e-5}
+    floor = 1e-6 * np.max(np.abs(sa))
+    out = {}
+    for name, prec in precs.items():
+        mb, sb, Jb = res[prec]
+        out[name] = {"steps": n_steps, "M_F_last": float(abs(mb[-1] - ma[-1]) / abs(ma[-1])), "M_F_run": rel(mb, ma),
+                     "edge_spectrum": rel(sb, sa),
+                     "edge_spectrum_per_bin": float(np.max(np.abs(sb - sa) / np.maximum(np.abs(sa), floor))),
+                     "J": rel(Jb, Ja), "spec": 1e-5}
+    return out
 
 
 def e2e_form(ctx, cloud, args, barrier, stream_of, world):
@@ -412,7 +422,7 @@ def adjoint_form(args, stream_of, local):
     from lydion_b200 import workloads as W
     from lydion_b200.m1 import context_for_cloud
     cl = W.config_c4()
-    n = max(100, min(2000, args.steps))
+    n = 2000      # the adjoint run's specified length, whatever --steps is
     p = (cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
     ctx = context_for_cloud(cl, device=local)
     run = lambda k: ctx.static_steps(k, *p, history=False)
@@ -452,7 +462,7 @@ def run_gpu(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from lydion_b200 import workloads as W
-    from lydion_b200._lib import PREC_FP64, PREC_MIXED
+    from lydion_b200._lib import PREC_FP32, PREC_FP64, PREC_MIXED
     cloud = W.config_c2()
 
     def barrier(ctx):
@@ -462,47 +472,57 @@ def run_gpu(args):
         ctx.synchronize()
 
     stream_of = lambda ctx: torch.cuda.ExternalStream(ctx.stream(), device=local)
-    if args.only_mixed:
-        f64 = None
-    else:
-        ctx64, f64 = measure_form(cloud, PREC_FP64, args, barrier, stream_of, local, world)
-        ctx64.close()
-    ctxm, mix = measure_form(cloud, PREC_MIXED, args, barrier, stream_of, local, world, clk=ClockSampler(local))
-    e2e = e2e_form(ctxm, cloud, args, barrier, stream_of, world)
-    ctxm.close()
+    # the headline: the FP64 form, the reference's arithmetic
+    ctx64, f64 = measure_form(cloud, PREC_FP64, args, barrier, stream_of, local, world, clk=ClockSampler(local))
+    e2e = e2e_form(ctx64, cloud, args, barrier, stream_of, world)
+    ctx64.close()
+    names = ["advect", "freq", "reduce"]
+    # the reduced-precision forms: FP32 flux arithmetic over FP64 storage, and FP32 storage
+    forms = {}
+    for fname, prec in (("mixed", PREC_MIXED), ("fp32_storage", PREC_FP32)):
+        if args.only_fp64:
+            break
+        c, m = measure_form(cloud, prec, args, barrier, stream_of, local, world)
+        c.close()
+        forms[fname] = {"value": m["value"], "ms_per_step": m["ms_per_step"], "tuning": m["tuning"],
+                        "kernel_ms_per_step": {n: float(v) for n, v in zip(names, m["kernel_ms"])},
+                        "over_fp64": m["value"] / f64["value"]}
     batch = None if args.no_batch else batch_form(args, barrier, stream_of, local, world)
     adj = None if (args.no_adjoint or world > 1) else adjoint_form(args, stream_of, local)
     c5 = None if (args.no_c5 or world > 1) else c5_form(args, stream_of, local)
     rhd = None if (args.no_rhd or world > 1) else rhd_form(args, stream_of, local)
-    err = None if (args.no_error or world > 1) else mixed_error_form(cloud, local)
+    err = None if (args.no_error or world > 1 or args.only_fp64) else form_errors(
+        cloud, local, {"mixed": PREC_MIXED, "fp32_storage": PREC_FP32})
     dd = dd_form(args, stream_of, local, world, rank) if args.dd_field else None
 
-    # roofline of the dominant kernel of the headline (mixed) form
-    names = ["advect", "freq", "reduce"]
-    kms = mix["kernel_ms"]
+    # roofline of the dominant kernel of the headline (FP64) form
+    kms = f64["kernel_ms"]
     dom = int(np.argmax(kms[:2]))
     ab = algorithmic_bytes(cloud.n_nu, 8)[names[dom]] * cloud.cell_bins
     peaks, src = measured_peaks()
     achieved = ab / (kms[dom] * 1e-3) / 1e9
-    variant = "mixed"
+    variant = "fp64"
     traffic = profile_traffic("k_" + names[dom], variant)
     cpu = cpu_baseline(cloud) if (rank == 0 and world == 1 and not args.no_cpu) else None
     if rank == 0:
-        line = {"metric": METRIC, "value": mix["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": mix["ms_per_step"], "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64 state, f32 advection arithmetic",
+        mixed = forms.get("mixed")
+        line = {"metric": METRIC, "value": f64["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": f64["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded static cloud set-up, no dataset)",
                 "config": {"workload": WORKLOAD, "cells": [cloud.nr, cloud.nz], "bins": cloud.n_nu, "tau0": 1e8,
-                           "tau_abs": 1.0, "source_radius": 0.5, "v_max_kms": 200.0, "precision": "mixed",
+                           "tau_abs": 1.0, "source_radius": 0.5, "v_max_kms": 200.0, "precision": "fp64",
                            "parallelism": f"{world} independent clouds (one per GPU)" if world > 1 else "single GPU",
                            "l2": "inputs larger than L2: 7 FP64 fields x 33.5 MB resident, 56 B/cell-bin streamed per kernel",
-                           "tuning": mix["tuning"]},
-                "fp64": None if f64 is None else {
-                    "value": f64["value"], "ms_per_step": f64["ms_per_step"], "tuning": f64["tuning"],
-                    "kernel_ms_per_step": {n: float(v) for n, v in zip(names, f64["kernel_ms"])}},
-                "mixed_over_fp64": None if f64 is None else mix["value"] / f64["value"],
-                "mixed_error": err,
-                "adjoint_over_forward": adj["ratio_auto"] if adj else None,
+                           "tuning": f64["tuning"]},
+                "kernel_ms_per_step": {n: float(v) for n, v in zip(names, kms)},
+                "mixed": mixed,
+                "mixed_over_fp64": mixed["over_fp64"] if mixed else None,
+                "fp32_storage": forms.get("fp32_storage"),
+                "form_errors": err,
+                "adjoint_over_forward": adj["ratio_every_100"] if adj else None,
+                "adjoint_over_forward_mode": "checkpoints every 100 steps, 2000 steps" if adj else None,
+                "adjoint_over_forward_keep_all": adj["ratio_auto"] if adj else None,
                 "adjoint": adj,
                 "largest_field": c5,
                 "rhd_lya_block": rhd,
@@ -512,14 +532,13 @@ def run_gpu(args):
                              "peak": peaks["hbm_gbs"], "peak_source": src, "unit": "GB/s",
                              "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                              "algorithmic_bytes_per_launch": ab, "ms_per_launch": float(kms[dom]),
-                             "kernel_ms_per_step": {n: float(v) for n, v in zip(names, kms)},
                              "ncu_fp64_pipe_pct": profile_figure("k_" + names[dom], variant, "fp64_pipe_pct"),
                              "ncu_fma_pipe_pct": profile_figure("k_" + names[dom], variant, "fma_pipe_pct")},
-                "active_fraction": mix["active_fraction"],
+                "active_fraction": f64["active_fraction"],
                 "cpu_baseline": cpu,
                 "e2e": e2e,
                 "gpu_launches": 3 * args.steps,
-                "clocks": mix["clocks"]}
+                "clocks": f64["clocks"]}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -542,7 +561,7 @@ def main():
     ap.add_argument("--no-error", action="store_true", help="skip the mixed-against-FP64 error run")
     ap.add_argument("--dd-field", action="store_true",
                     help="also step the 1024x1024x128 field split into Z slabs over the ranks (strong scaling)")
-    ap.add_argument("--only-mixed", action="store_true", help="measure the mixed-precision form only")
+    ap.add_argument("--only-fp64", action="store_true", help="measure the FP64 form only")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

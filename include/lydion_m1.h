@@ -13,7 +13,7 @@
  * own CUDA stream; lyd_download* and the diagnostic calls return after the stream drains.
  *
  * Each step entry point names the Julia function of LYDION it replaces (path:line within
- * the LYDION source tree). The Julia ccall bindings are given in INTEGRATION.md.
+ * the LYDION source tree), whose argument meaning it keeps.
  */
 #ifndef LYDION_M1_H
 #define LYDION_M1_H
@@ -395,8 +395,9 @@ int  lyd_voigt_tables(double *out, int32_t n, double xmax);
  * No counterpart in the reference. For callers that may not allocate device memory (a host
  * framework that owns every allocation through its own pool, a plugin inside a fixed memory
  * budget, a time loop that must not allocate): computes the active-bin window of
- * FindActiveBins from caller-owned device arrays J (n_nu*n_r*n_z, FP64, [k,i,j]), dnu (n_nu)
- * and dV (n_r*n_z), on `stream` (a cudaStream_t; NULL is the legacy default stream), and
+ * FindActiveBins from caller-owned device arrays J (n_nu*n_r*n_z, FP64 in physical units,
+ * [k,i,j]: the Jeps floor of 1e-60 applies to J as given, so a state a context holds as
+ * value / j_scale must be scaled back first), dnu (n_nu) and dV (n_r*n_z), on `stream` (a cudaStream_t; NULL is the legacy default stream), and
  * returns kmin/kmax (0-based) to the host after synchronising that stream. It creates no
  * context and calls no cudaMalloc/cudaFree: its scratch is a file-scope 1 MiB device array
  * (131072 FP64 partial sums) that every GPU loading the library holds until exit. The first

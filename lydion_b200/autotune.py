@@ -62,20 +62,31 @@ def _load(path):
         return {}
 
 
-def _save(path, data):
-    """Atomic write through a temporary file of this process's own, so ranks that tune at the
-    same time (one process per GPU) each replace the cache whole; the last one wins."""
+def _save(path, entries):
+    """Merge `entries` (workload key -> record) into the cache file. Ranks that tune at the same
+    time (one process per GPU) may hold different keys: under an exclusive lock on a sidecar
+    file each writer re-reads the cache, adds its own keys and replaces the file atomically
+    through a temporary file of its own, so no writer drops another's entries and no reader
+    ever sees a torn file."""
+    import fcntl
     d = os.path.dirname(path) or "."
     os.makedirs(d, exist_ok=True)
-    fd, tmp = tempfile.mkstemp(prefix=os.path.basename(path) + ".", suffix=".tmp", dir=d)
-    try:
-        with os.fdopen(fd, "w") as f:
-            json.dump(data, f, indent=1, sort_keys=True)
-        os.replace(tmp, path)
-    except BaseException:
-        if os.path.exists(tmp):
-            os.unlink(tmp)
-        raise
+    with open(path + ".lock", "a") as lk:
+        fcntl.flock(lk, fcntl.LOCK_EX)
+        try:
+            data = _load(path)
+            data.update(entries)
+            fd, tmp = tempfile.mkstemp(prefix=os.path.basename(path) + ".", suffix=".tmp", dir=d)
+            try:
+                with os.fdopen(fd, "w") as f:
+                    json.dump(data, f, indent=1, sort_keys=True)
+                os.replace(tmp, path)
+            except BaseException:
+                if os.path.exists(tmp):
+                    os.unlink(tmp)
+                raise
+        finally:
+            fcntl.flock(lk, fcntl.LOCK_UN)
 
 
 def _measure(ctx, run, tuning, steps):
@@ -134,8 +145,7 @@ def autotune(ctx, run, steps=10, device=0, cache=None, force=False, **grid):
         return t
     best, table = search(ctx, run, steps=steps, **grid)
     ctx.set_tuning(*best)
-    data[key] = {"tuning": list(best), "table": [[list(t), ms] for t, ms in table], "steps": steps}
-    _save(path, data)
+    _save(path, {key: {"tuning": list(best), "table": [[list(t), ms] for t, ms in table], "steps": steps}})
     return best
 
 

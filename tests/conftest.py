@@ -24,6 +24,9 @@ def gpu_available():
 
 
 def pytest_collection_modifyitems(config, items):
+    # the oracle parity tests of the step run first, so a run stopped at the first failure
+    # has always checked the step itself; every other file keeps its collection order
+    items.sort(key=lambda it: 0 if os.path.basename(str(it.fspath)) == "test_gpu_parity.py" else 1)
     if gpu_available():
         return
     skip = pytest.mark.skip(reason="no CUDA device in this environment")

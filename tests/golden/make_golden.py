@@ -1,6 +1,9 @@
 """Generates the committed golden fixtures that pin the oracle's third-party pieces.
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py <path of the LYDION checkout>
+
+The checkout path may also come from the environment variable LYDION_REFERENCE; its data
+files are read as text.
 
 * dgtsv_cases.npz -- tridiagonal systems (random, diagonally dominant, pivot-forcing, and
   systems taken from a stiff tau0 = 1e8 cloud) with the solutions and INFO returned by
@@ -28,7 +31,15 @@ from scipy.special import erf, dawsn
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference"   # the reference checkout whose data files are read as text
+
+
+def reference_root():
+    """The LYDION checkout whose data files are read as text: the first command-line argument,
+    else $LYDION_REFERENCE."""
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LYDION_REFERENCE")
+    if not root or not os.path.isdir(root):
+        raise SystemExit("usage: python tests/golden/make_golden.py <LYDION checkout> (or set LYDION_REFERENCE)")
+    return root
 
 
 def dgtsv_cases():
@@ -92,21 +103,23 @@ def analytic_spectra():
             un = -np.sqrt(6 / np.pi) * (x ** 2 / at) * np.log(1 - np.exp(-np.sqrt(2 * np.pi ** 3 / 27) * np.abs(x ** 3) / at))
         out[f"point_T{T:g}_tau{tau:g}"] = np.nan_to_num(pt, nan=0.0)
         out[f"uni_T{T:g}_tau{tau:g}"] = np.nan_to_num(un, nan=0.0)
-    mf = np.loadtxt(os.path.join(REF, "EscapeFractionTest_StaticCloud", "AnalyticalMF_UniformSource.txt"))
+    ref = reference_root()
+    mf = np.loadtxt(os.path.join(ref, "EscapeFractionTest_StaticCloud", "AnalyticalMF_UniformSource.txt"))
     out["mf_uniform_eps1"] = mf[:8, 0]
     out["mf_uniform_over_atau13"] = mf[:8, 1]
     for kind, fn in (("point", "PointSource"), ("uni", "UniformSource")):
-        t = np.loadtxt(os.path.join(REF, "EscapeFractionTest_StaticCloud", f"AnalyticalEscapeFraction_{fn}.txt"))
+        t = np.loadtxt(os.path.join(ref, "EscapeFractionTest_StaticCloud", f"AnalyticalEscapeFraction_{fn}.txt"))
         out[f"fesc_{kind}_eps1"] = t[:, 0]
         out[f"fesc_{kind}"] = -t[:, 1]
     for v in (10, 200):
-        t = np.loadtxt(os.path.join(REF, "VelocityGradientsTest", f"comoving_MCRT_uniform_{v}.txt"))
+        t = np.loadtxt(os.path.join(ref, "VelocityGradientsTest", f"comoving_MCRT_uniform_{v}.txt"))
         out[f"mcrt_v{v}_x"] = t[:, 0]
         out[f"mcrt_v{v}"] = t[:, 1]
     np.savez_compressed(os.path.join(HERE, "analytic_spectra.npz"), **out)
 
 
 if __name__ == "__main__":
+    reference_root()
     dgtsv_cases()
     voigt_samples()
     analytic_spectra()

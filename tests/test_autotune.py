@@ -82,21 +82,23 @@ def test_reset_runs_before_every_candidate():
 def _writer(path, rank, n):
     from lydion_b200 import autotune as A_
     for k in range(n):
-        A_._save(path, {"rank": rank, "k": k})
+        A_._save(path, {f"rank{rank}|k{k}": {"rank": rank, "k": k}})
 
 
-def test_concurrent_cache_writes_stay_whole(tmp_path):
-    """Under torchrun every rank tunes its own GPU and writes the same cache file at once."""
+def test_concurrent_cache_writes_keep_every_key(tmp_path):
+    """Under torchrun every rank tunes its own GPU (its own workload keys) and writes the same
+    cache file at once: every key of every writer survives, and no temporary file is left."""
     import multiprocessing as mp
     import os
     path = str(tmp_path / "tuning.json")
     ctx = mp.get_context("spawn")
-    procs = [ctx.Process(target=_writer, args=(path, r, 100)) for r in range(4)]
+    procs = [ctx.Process(target=_writer, args=(path, r, 50)) for r in range(4)]
     for p in procs:
         p.start()
     for p in procs:
         p.join(120)
     assert [p.exitcode for p in procs] == [0, 0, 0, 0]
-    data = json.load(open(path))            # one writer's whole record: the last one wins
-    assert data["k"] == 99 and data["rank"] in range(4)
-    assert os.listdir(tmp_path) == ["tuning.json"]   # no temporary file left behind
+    data = json.load(open(path))
+    assert sorted(data) == sorted(f"rank{r}|k{k}" for r in range(4) for k in range(50))
+    assert all(data[f"rank{r}|k{k}"] == {"rank": r, "k": k} for r in range(4) for k in range(50))
+    assert sorted(os.listdir(tmp_path)) == ["tuning.json", "tuning.json.lock"]
