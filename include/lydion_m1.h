@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define LYD_ABI_VERSION 3
+#define LYD_ABI_VERSION 4
 
 /* status codes */
 #define LYD_OK              0
@@ -35,6 +35,8 @@ extern "C" {
 #define LYD_ERR_SOLVE      -4   /* a frequency tridiagonal system had a zero pivot      */
 #define LYD_ERR_STATE      -5   /* call needs an input that was never provided           */
 #define LYD_ERR_NOMEM      -6   /* device allocation failed                              */
+#define LYD_ERR_TIMEOUT    -7   /* a bounded wait inside a kernel ran out (a bulk copy
+                                   never completed); the kernel skipped its remaining work  */
 
 /* boundary conditions (Symbol :Reflect / :Outflow in the reference) */
 #define LYD_BC_REFLECT 0
@@ -240,11 +242,16 @@ int  lyd_batch_steps(lyd_ctx *ctx, const lyd_cloud_params *params, int32_t n_ste
 /* Launch-shape knobs chosen by the autotuner (lydion_b200/autotune.py): rows of the
  * advection tile (4..64), cells per frequency-kernel block (8..1024, or 0 for automatic), the
  * frequency solver (0: parallel cyclic reduction across the warp; 1: lane-serial
- * elimination), and the advection kernel's resident CTAs per SM (2..4 with FP32 arithmetic,
- * 2..3 with FP64, or 0 for the default: 4 and 3). lyd_get_tuning reports an automatic cell
- * count as its negative. */
+ * elimination), the advection kernel's resident CTAs per SM (2..4 with FP32 arithmetic,
+ * 2..3 with FP64, or 0 for the default: 4 and 3), and how the advection stages its rows
+ * (LYD_STAGING_*). lyd_get_tuning reports an automatic cell count as its negative and the
+ * staging actually used. */
+#define LYD_STAGING_AUTO   0   /* the library's choice for the precision and layout            */
+#define LYD_STAGING_LANES  1   /* per-lane loads of every staged cell                         */
+#define LYD_STAGING_TMA    2   /* bulk tensor copies (TMA) of each row's 32-bin x 12-column box,
+                                  a row ahead, when a row of n_nu bins is a multiple of 16 bytes */
 typedef struct lyd_tuning {
-    int32_t rows_per_tile, cells_per_block, solver, adv_ctas_per_sm;
+    int32_t rows_per_tile, cells_per_block, solver, adv_ctas_per_sm, adv_staging;
 } lyd_tuning;
 int  lyd_set_tuning(lyd_ctx *ctx, const lyd_tuning *t);
 int  lyd_get_tuning(lyd_ctx *ctx, lyd_tuning *t);

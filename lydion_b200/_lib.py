@@ -10,6 +10,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "liblydion_m1.so")
 
 LYD_OK = 0
 LYD_ERR_ARG, LYD_ERR_CUDA, LYD_ERR_NONFINITE, LYD_ERR_SOLVE, LYD_ERR_STATE, LYD_ERR_NOMEM = -1, -2, -3, -4, -5, -6
+LYD_ERR_TIMEOUT = -7
 BC_REFLECT, BC_OUTFLOW = 0, 1
 FLUX_GLF, FLUX_HLL = 0, 1
 GEOM_CYLINDRICAL, GEOM_CARTESIAN = 0, 1
@@ -67,7 +68,10 @@ class CloudParams(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("rows_per_tile", C.c_int32), ("cells_per_block", C.c_int32), ("solver", C.c_int32),
-                ("adv_ctas_per_sm", C.c_int32)]
+                ("adv_ctas_per_sm", C.c_int32), ("adv_staging", C.c_int32)]
+
+
+STAGING_AUTO, STAGING_LANES, STAGING_TMA = 0, 1, 2
 
 
 SOLVER_PCR, SOLVER_THOMAS = 0, 1

@@ -15,6 +15,7 @@
 // sets swap; the emission and frequency kernels work per cell in place. The fused
 // static-cloud step advects cur -> spare and then runs emission + frequency spare -> cur,
 // so a step starts and ends in the same set and one CUDA graph replays every step.
+#include <cuda.h>   // CUtensorMap and its enums (types only: the driver entry point is fetched at run time)
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -80,7 +81,9 @@ struct lyd_ctx {
     double *nu = nullptr, *nuC = nullptr, *dnu = nullptr, *inv_dnu = nullptr, *inv_nuC = nullptr;
     bool freq_set = false;
     // work lists
-    lyd_tuning tune{kDefaultRows, 0, SOLVER_PCR, 0};
+    lyd_tuning tune{kDefaultRows, 0, SOLVER_PCR, 0, LYD_STAGING_AUTO};
+    unsigned char *tmaps = nullptr;    // tensor maps of J, H_r, H_Z: [set][cloud][3] (TMA staging)
+    bool tma_ok = false;               // every map encoded (the layout allows bulk tensor copies)
     int4 *tiles = nullptr, *items = nullptr;
     int ntiles = 0, nitems = 0;
     double *partials = nullptr;
@@ -160,6 +163,8 @@ static int check_err(lyd_ctx *c) {
     LYD_CU(c, cudaStreamSynchronize(c->st));
     if (h) {
         LYD_CU(c, cudaMemsetAsync(c->err, 0, sizeof(int), c->st));
+        if (h & ERRB_TIMEOUT)
+            return fail(c, LYD_ERR_TIMEOUT, "a bulk copy of the advection's staging did not complete in time");
         if (h & ERRB_NONFINITE) return fail(c, LYD_ERR_NONFINITE, "non-finite value in J or H");
         return fail(c, LYD_ERR_SOLVE, "zero pivot in a frequency tridiagonal system");
     }
@@ -240,6 +245,67 @@ static int ensure_stage(lyd_ctx *c, size_t n) {
 // Every lyd_* definition below has C linkage through its declaration in lydion_m1.h.
 
 int lyd_abi_version(void) { return LYD_ABI_VERSION; }
+
+// cuTensorMapEncodeTiled, fetched from the driver at run time (the library links no libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// Tensor maps for the advection's bulk-copy staging: one per cloud, field (J, H_r, H_Z) and
+// buffer set, over the cloud's [n_nu][n_r][n_z] block with a box of 32 bins x (tile columns + 4
+// halo columns) x 1 row. A map needs its block to start on a 16-byte boundary and a row of
+// n_nu elements to be a multiple of 16 bytes; cloud blocks are sums of whole rows, so the
+// second implies the first. When that fails, or the driver lacks the encoder, the advection
+// stages with per-lane loads.
+static int encode_tmaps(lyd_ctx *c) {
+    static_assert(sizeof(CUtensorMap) == kTensorMapBytes, "tensor map size");
+    c->tma_ok = false;
+    const size_t es = c->ssz;
+    if ((c->nnu * es) % 16 != 0) return LYD_OK;
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn) return LYD_OK;
+    std::vector<CUtensorMap> maps((size_t)2 * c->ncl * 3);
+    for (int s = 0; s < 2; s++)
+        for (int q = 0; q < c->ncl; q++)
+            for (int f = 0; f < 3; f++) {
+                const CloudDesc &d = c->desc[q];
+                void *base = static_cast<char *>(c->set[s][f]) + (size_t)d.o3 * es;
+                const cuuint64_t dims[3] = {(cuuint64_t)c->nnu, (cuuint64_t)d.nr, (cuuint64_t)d.nz};
+                const cuuint64_t strides[2] = {(cuuint64_t)c->nnu * es, (cuuint64_t)c->nnu * d.nr * es};
+                const cuuint32_t box[3] = {32u, (cuuint32_t)(kTileCols + 4), 1u};
+                const cuuint32_t estr[3] = {1u, 1u, 1u};
+                CUresult e = fn(&maps[((size_t)s * c->ncl + q) * 3 + f],
+                                es == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base,
+                                dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                if (e != CUDA_SUCCESS) return LYD_OK;
+            }
+    LYD_TRY(dalloc(c, (void **)&c->tmaps, maps.size() * sizeof(CUtensorMap)));
+    LYD_CU(c, cudaMemcpyAsync(c->tmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
+                              c->st));
+    LYD_CU(c, cudaStreamSynchronize(c->st));
+    c->tma_ok = true;
+    return LYD_OK;
+}
+
+// The staging the advection uses: bulk copies when asked for and the maps exist.
+static int staging_used(const lyd_ctx *c) {
+    const int want = c->tune.adv_staging != LYD_STAGING_AUTO ? c->tune.adv_staging : LYD_STAGING_LANES;
+    return (want == LYD_STAGING_TMA && c->tma_ok) ? LYD_STAGING_TMA : LYD_STAGING_LANES;
+}
 
 const char *lyd_last_error(const lyd_ctx *c) { return c ? c->msg.c_str() : "null context"; }
 
@@ -328,6 +394,7 @@ int lyd_batch_create(lyd_ctx **out, int32_t ncl, const int32_t *n_r, const int32
     if (cfg->keep_freq_factors)
         for (int q = 0; q < 3; q++) A((void **)&c->Ff[q], c->n3 * 8);
     if (r == LYD_OK) r = build_work(c);
+    if (r == LYD_OK) r = encode_tmaps(c);
     if (r != LYD_OK) {
         lyd_destroy(c);
         return r;
@@ -353,6 +420,7 @@ int lyd_destroy(lyd_ctx *c) {
     drop_graph(c);
     for (int s = 0; s < 2; s++)
         for (int q = 0; q < 3; q++) cudaFree(c->set[s][q]);
+    cudaFree(c->tmaps);
     void *ps[] = {c->Hv, c->phi, c->phi_inv, c->aF, c->Ff[0], c->Ff[1], c->Ff[2], c->u_r_star, c->u_Z_star, c->dV,
                   c->inv_dV, c->A_r, c->A_Z, c->inv_r_cell, c->rCoM, c->ZCoM, c->rint, c->zint, c->r_if, c->Z_if,
                   c->nu, c->nuC, c->dnu, c->inv_dnu, c->inv_nuC, c->partials, c->kwin, c->hist, c->step_ctr,
@@ -396,6 +464,8 @@ int lyd_set_tuning(lyd_ctx *c, const lyd_tuning *t) {
     if (t->solver != SOLVER_PCR && t->solver != SOLVER_THOMAS) return fail(c, LYD_ERR_ARG, "unknown solver");
     if (t->adv_ctas_per_sm != 0 && (t->adv_ctas_per_sm < 2 || t->adv_ctas_per_sm > 4))
         return fail(c, LYD_ERR_ARG, "adv_ctas_per_sm outside 2..4");
+    if (t->adv_staging < LYD_STAGING_AUTO || t->adv_staging > LYD_STAGING_TMA)
+        return fail(c, LYD_ERR_ARG, "unknown adv_staging");
     cudaSetDevice(c->dev);
     LYD_CU(c, cudaStreamSynchronize(c->st));
     c->tune = *t;
@@ -407,6 +477,7 @@ int lyd_get_tuning(lyd_ctx *c, lyd_tuning *t) {
     *t = c->tune;
     if (t->cells_per_block == 0) t->cells_per_block = -cells_per_block(c);   // negative: chosen automatically
     t->adv_ctas_per_sm = adv_ctas_per_sm(c->prec, t->adv_ctas_per_sm);
+    t->adv_staging = staging_used(c);
     return LYD_OK;
 }
 
@@ -641,6 +712,8 @@ static void fill_adv(lyd_ctx *c, AdvArgs<S> &a, int in_set, int out_set) {
     a.rows = c->tune.rows_per_tile;
     a.nnu = c->nnu;
     a.jeps = c->jeps_s; a.heps2 = c->heps2_s;
+    a.err = c->err;
+    a.tmaps = staging_used(c) == LYD_STAGING_TMA ? c->tmaps + (size_t)in_set * c->ncl * 3 * kTensorMapBytes : nullptr;
 }
 
 template <typename S>
@@ -979,7 +1052,7 @@ static int enqueue_step(lyd_ctx *c, bool timed, double *tape = nullptr, const S 
     fill_adv<S>(c, aa, A, B);
     aa.tape = tape;
     aa.tape_stride = (long long)c->n3;
-    if (in) { aa.J = in; aa.Hr = in + c->n3; aa.HZ = in + 2 * c->n3; }
+    if (in) { aa.J = in; aa.Hr = in + c->n3; aa.HZ = in + 2 * c->n3; aa.tmaps = nullptr; }
     FreqArgs<S> fa;
     if (out)
         fill_freq<S>(c, fa, c->set[B][0], c->set[B][1], c->set[B][2], c->set[B][0], out, out + c->n3,
@@ -1642,6 +1715,7 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
             AdvArgs<double> aa;
             fill_adv<double>(c, aa, c->cur, B);
             aa.J = sn; aa.Hr = sn + n3; aa.HZ = sn + 2 * n3;
+            aa.tmaps = nullptr;     // the maps cover the context's buffer sets, not the workspace
             aa.Jo = xA; aa.Hro = xA + n3; aa.HZo = xA + 2 * n3;
             aa.kwin = win + 2 * n;
             aa.tape = segT + (size_t)(n - n0) * 4 * n3;

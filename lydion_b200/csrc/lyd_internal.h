@@ -66,6 +66,9 @@ struct AdvArgs {
     double *tape;                // adjoint recomputation: the cell update's values before its
                                  // floors and limiter, 4 fields of tape_stride (or nullptr)
     long long tape_stride;
+    const unsigned char *tmaps;  // tensor maps of the input J, H_r, H_Z, [cloud][3] of
+                                 // kTensorMapBytes each in device memory, or nullptr: per-lane loads
+    int *err;                    // device error bits (ERRB_TIMEOUT)
 };
 
 // Emission/absorption + frequency step + flux correction (+ partial reductions).
@@ -97,6 +100,7 @@ struct FreqArgs {
     int *err;                    // device error bits
     int nnu;
     int solver;                  // SOLVER_*
+    int vec16;                   // set by the launcher: rows move as whole 16-byte words
 };
 
 enum { SOLVER_PCR = 0, SOLVER_THOMAS = 1 };
@@ -126,7 +130,9 @@ struct RedArgs {
 };
 
 // error bits
-enum { ERRB_NONFINITE = 1, ERRB_SOLVE = 2 };
+enum { ERRB_NONFINITE = 1, ERRB_SOLVE = 2, ERRB_TIMEOUT = 4 };
+// size of one CUtensorMap (an opaque 64-byte-aligned record)
+constexpr int kTensorMapBytes = 128;
 
 int bins_per_lane(int nnu);
 // `prec` of the step launches is a PREC_K_* variant; `sprec` of the others is the storage

@@ -119,6 +119,49 @@ __device__ __forceinline__ R alpha_F(const AdvArgs<S> &a, const View &v, int i, 
     return val;
 }
 
+// ---- bulk tensor copies (TMA) into shared memory, completed on an mbarrier -------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+// One arrival that also announces `bytes` of copies that will complete on the barrier.
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Wait for the phase `parity` of the barrier to complete; gives up after a bounded number of
+// polls (each poll itself returns after a short hardware time limit) and reports false.
+constexpr int kMbarPolls = 1 << 20;
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity) {
+    for (int it = 0; it < kMbarPolls; it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// Orders this thread's view of earlier generic-proxy shared-memory accesses (made visible to
+// it by a barrier) before the bulk copies it issues next into the same memory.
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// A 3-D tile of a tensor in this GPU's global memory (the map's own buffer) into shared memory;
+// x, y, z are the element coordinates of the tile's first element (x * element size a multiple
+// of 16 bytes; y may be negative, out-of-range elements read as zero). No multicast.
+__device__ __forceinline__ void tma_load_3d(void *dst, const void *map, int x, int y, int z,
+                                            unsigned long long *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::
+            "r"(smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
 // ---- k_advect: one CTA = 8 columns (r) x `rows` rows (Z) x 32 bins, marching up in Z --------
 //
 // A ring of four rows holds, for the 8 own columns and the 2 + 2 halo columns of each row, the
@@ -166,6 +209,57 @@ __device__ __forceinline__ void stage_cell(const AdvArgs<S> &a, const View &v, R
     if (nf<R>() == 4) p[96] = aF;
     if (lc >= 2 && lc < 2 + MT) {
         // the state in S; with S == R the ring's J is the state's J
+        constexpr int HF = sizeof(S) == sizeof(R) ? 2 : 3;
+        S *q = Hh + ((slot * MT + (lc - 2)) * HF) * 32 + lane;
+        q[0] = c.Hr; q[32] = c.HZ;
+        if (HF == 3) q[64] = c.J;
+    }
+}
+
+// The raw tile a bulk tensor copy lands for one row: J, H_r, H_Z of the staged columns
+// i0-2 .. i0+MT+1 and 32 bins, [field][column][bin] (the copy box is 32 bins x MCOL columns).
+// Columns outside 0..n_r-1 land as zeros; for a ghost row (row >= n_z) the copy fetched the row
+// it mirrors.
+template <typename S>
+__host__ __device__ constexpr int raw_tile_bytes() { return 3 * MCOL * 32 * (int)sizeof(S); }
+
+// Stage cell (col, row) into ring slot `slot` from the raw tile, applying the ghost-cell rules
+// of r_cell / z_cell: a ghost column takes the column it mirrors from the same tile (every such
+// column lies in the tile: i0 < n_r), a ghost row's H_Z gets the rule of its boundary.
+template <typename S, typename R>
+__device__ __forceinline__ void stage_from_raw(const AdvArgs<S> &a, const View &v, const S *raw, R *A, S *Hh,
+                                               int slot, int lc, int col, int row, int k, int lane, R jeps, int i0) {
+    int sc = lc;
+    int rule = 0;   // H_r: 1 negate, 2 keep the inward (<= 0) part, 3 keep the outward (>= 0) part
+    if (col < 0) {
+        if (v.bcl == 0) { sc = (-1 - col) - i0 + 2; rule = 1; }
+        else { sc = -i0 + 2; rule = 2; }
+    } else if (col >= v.nr) {
+        if (v.bcr == 0) { sc = (2 * v.nr - 1 - col) - i0 + 2; rule = 1; }
+        else { sc = (v.nr - 1) - i0 + 2; rule = 3; }
+    }
+    Cell<S> c;
+    c.J = raw[(0 * MCOL + sc) * 32 + lane];
+    c.Hr = raw[(1 * MCOL + sc) * 32 + lane];
+    c.HZ = raw[(2 * MCOL + sc) * 32 + lane];
+    if (rule == 1) c.Hr = -c.Hr;
+    else if (rule == 2) c.Hr = c.Hr < S(0) ? c.Hr : S(0);
+    else if (rule == 3) c.Hr = c.Hr > S(0) ? c.Hr : S(0);
+    if (row >= v.nz) {
+        if (v.bzt == 0) c.HZ = -c.HZ;
+        else c.HZ = c.HZ > S(0) ? c.HZ : S(0);
+    }
+    R aF = R(0);
+    if (nf<R>() == 4) {
+        int cc = col < 0 ? 0 : (col >= v.nr ? v.nr - 1 : col);
+        int rr = row >= v.nz ? v.nz - 1 : row;
+        aF = alpha_F<S, R>(a, v, cc, rr, k);
+    }
+    CellF<R> f = cell_f<R>(R(c.J), R(c.Hr), R(c.HZ), jeps);
+    R *p = A + ((slot * MCOL + lc) * nf<R>()) * 32 + lane;
+    p[0] = f.J; p[32] = f.fr; p[64] = f.fZ;
+    if (nf<R>() == 4) p[96] = aF;
+    if (lc >= 2 && lc < 2 + MT) {
         constexpr int HF = sizeof(S) == sizeof(R) ? 2 : 3;
         S *q = Hh + ((slot * MT + (lc - 2)) * HF) * 32 + lane;
         q[0] = c.Hr; q[32] = c.HZ;
@@ -305,21 +399,49 @@ __device__ __forceinline__ double geo_fetch(const double *src, int stride, int j
     return (src != nullptr && j < j1) ? __ldg(src + (long long)stride * j) : 0.0;
 }
 
-template <typename S, typename R, int FLUX, int MINB>
+// Shared memory of the advection tile before the bulk-copy staging area, in bytes.
+template <typename S, typename R>
+__host__ __device__ constexpr size_t adv_smem_base() {
+    return sizeof(R) * 32 * (RING * MCOL * nf<R>() + (MT + 1) * 5) +
+           sizeof(S) * 32 * RING * MT * (sizeof(S) == sizeof(R) ? 2 : 3) +
+           (sizeof(R) == 4 ? sizeof(double) * MWARPS * GEO_N : 0);   // the row slots (FP32 arithmetic)
+}
+__host__ __device__ constexpr size_t adv_tma_off(size_t base) { return (base + 127) / 128 * 128; }
+
+// TMA: rows j0+2 .. of the tile arrive as bulk tensor copies (one 32-bin x MCOL-column box per
+// field, issued by one thread a row ahead of their use into one raw tile, completed on an
+// mbarrier) instead of per-lane loads; the converting warps apply the ghost-cell rules. The
+// first rows (j0-2 .. j0+1) are staged by per-lane loads while the first copy is in flight.
+template <typename S, typename R, int FLUX, int MINB, bool TMA>
 __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
-    extern __shared__ __align__(16) unsigned char adv_smem[];
+    extern __shared__ __align__(128) unsigned char adv_smem[];
     constexpr int HF = sizeof(S) == sizeof(R) ? 2 : 3;
     constexpr int NF = nf<R>();
     R *A = reinterpret_cast<R *>(adv_smem);                            // [RING][MCOL][NF][32]
     S *Hh = reinterpret_cast<S *>(A + RING * MCOL * NF * 32);           // [RING][MT][HF][32]
     R *Fr = reinterpret_cast<R *>(Hh + RING * MT * HF * 32);            // [MT+1][5][32]
     double *geo = reinterpret_cast<double *>(Fr + (MT + 1) * 5 * 32);  // [MWARPS][GEO_N], FP32 arithmetic only
+    constexpr size_t toff = adv_tma_off(adv_smem_base<S, R>());
+    S *raw = reinterpret_cast<S *>(adv_smem + toff);                                   // [3][MCOL][32]
+    unsigned long long *bar = reinterpret_cast<unsigned long long *>(adv_smem + toff + raw_tile_bytes<S>());
+    int *abort_flag = reinterpret_cast<int *>(bar + 1);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int4 t = a.tiles[blockIdx.x];
     View v;
     load_view(a.cl[t.x], v);
     const int i0 = t.y, j0 = t.z, kb = t.w;
     const int j1 = (j0 + a.rows < v.jend) ? j0 + a.rows : v.jend;
+    // the last row a tile stages: the Z face j1 - 1/2 reads rows up to j1 + 1 (ghosts beyond n_z + 1 unused)
+    const int rlast = (j1 + 1 < v.nz + 1) ? j1 + 1 : v.nz + 1;
+    // one bulk copy per field of row r (a ghost row fetches the row it mirrors)
+    auto issue_row = [&](int r) {
+        const int src = r < v.nz ? r : (v.bzt == 0 ? 2 * v.nz - 1 - r : v.nz - 1);
+        const unsigned char *maps = a.tmaps + (size_t)t.x * 3 * kTensorMapBytes;
+        fence_proxy_async_smem();
+        mbar_expect_tx(bar, (unsigned)raw_tile_bytes<S>());
+#pragma unroll
+        for (int f = 0; f < 3; f++) tma_load_3d(raw + f * MCOL * 32, maps + f * kTensorMapBytes, kb, i0 - 2, src, bar);
+    };
     const int k = kb + lane;
     const int kmin = a.kwin[2 * t.x], kmax = a.kwin[2 * t.x + 1];
     const bool kact = (k >= kmin) && (k <= kmax) && (k < a.nnu);
@@ -338,12 +460,34 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
         return;
     }
 
+    if constexpr (TMA) {
+        if (threadIdx.x == 0) {
+            mbar_init(bar, 1);
+            *abort_flag = 0;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && j0 + 2 <= rlast) issue_row(j0 + 2);
+    }
     // prologue: own columns, rows j0-2 .. j0+1
     if (own && kact && col <= v.nr + 1) {
         for (int r = j0 - 2; r <= j0 + 1; r++) {
             bool gcol = col >= v.nr, grow = (r < 0 || r >= v.nz);
             if (r < -2 || r > v.nz + 1 || (gcol && grow)) continue;
             stage_cell<S, R>(a, v, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps);
+        }
+    }
+    if constexpr (TMA) {
+        // with bulk copies the halo columns of a row come with its copy, two rows before the
+        // r faces read them: the prologue stages those of rows j0 and j0+1
+        if (!own && kact) {
+            const int hl[4] = {0, 1, MT + 2, MT + 3};
+            for (int r = j0; r <= j0 + 1 && r < j1 && r < v.nz; r++) {
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    int c2 = i0 - 2 + hl[q];
+                    if (c2 <= v.nr + 1) stage_cell<S, R>(a, v, A, Hh, r & (RING - 1), hl[q], c2, r, k, lane, jeps);
+                }
+            }
         }
     }
     constexpr bool PRE = sizeof(R) == 4;   // per-row scalars fetched a row ahead
@@ -365,23 +509,57 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
     for (int j = j0; j < j1; j++) {
         double gnext = 0.0;
         if constexpr (PRE) gnext = geo_fetch(gsrc, gstr, j + 1, j1);
-        // (A) stage row j+2 of the own column; warp 8 stages the halo columns of row j
-        if (kact) {
-            if (own) {
-                int r = j + 2;
-                bool gcol = col >= v.nr, grow = r >= v.nz;
-                if (col <= v.nr + 1 && r <= v.nz + 1 && !(gcol && grow))
-                    stage_cell<S, R>(a, v, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps);
-            } else {
-                const int hl[4] = {0, 1, MT + 2, MT + 3};
+        if constexpr (TMA) {
+            // (A) row j+2 from its bulk copy: the own column, and (warp 8) the halo columns
+            const int r = j + 2;
+            if (r <= rlast) {
+                if (!mbar_wait_bounded(bar, (unsigned)((r - (j0 + 2)) & 1))) {
+                    *abort_flag = 1;
+                    atomicOr(a.err, ERRB_TIMEOUT);
+                } else if (kact) {
+                    const bool grow = r >= v.nz;
+                    if (own) {
+                        if (col <= v.nr + 1 && !(col >= v.nr && grow))
+                            stage_from_raw<S, R>(a, v, raw, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps, i0);
+                    } else if (!grow && r < j1) {
+                        const int hl[4] = {0, 1, MT + 2, MT + 3};
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    int c2 = i0 - 2 + hl[q];
-                    if (c2 <= v.nr + 1) stage_cell<S, R>(a, v, A, Hh, j & (RING - 1), hl[q], c2, j, k, lane, jeps);
+                        for (int q = 0; q < 4; q++) {
+                            int c2 = i0 - 2 + hl[q];
+                            if (c2 <= v.nr + 1)
+                                stage_from_raw<S, R>(a, v, raw, A, Hh, r & (RING - 1), hl[q], c2, r, k, lane, jeps, i0);
+                        }
+                    }
                 }
             }
+            __syncthreads();
+            if (*reinterpret_cast<volatile int *>(abort_flag)) {
+                // a copy never arrived: wait once more (bounded) for it, then leave the tile
+                if (threadIdx.x == 0) mbar_wait_bounded(bar, (unsigned)((r - (j0 + 2)) & 1));
+                return;
+            }
+            // the raw tile is free again: fetch row j+3 while this row's faces and update run
+            if (threadIdx.x == 0 && j + 3 <= rlast) issue_row(j + 3);
+        } else {
+            // (A) stage row j+2 of the own column; warp 8 stages the halo columns of row j
+            if (kact) {
+                if (own) {
+                    int r = j + 2;
+                    bool gcol = col >= v.nr, grow = r >= v.nz;
+                    if (col <= v.nr + 1 && r <= v.nz + 1 && !(gcol && grow))
+                        stage_cell<S, R>(a, v, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps);
+                } else {
+                    const int hl[4] = {0, 1, MT + 2, MT + 3};
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        int c2 = i0 - 2 + hl[q];
+                        if (c2 <= v.nr + 1)
+                            stage_cell<S, R>(a, v, A, Hh, j & (RING - 1), hl[q], c2, j, k, lane, jeps);
+                    }
+                }
+            }
+            __syncthreads();
         }
-        __syncthreads();
         // (B) the r face left of the own column (warp 8: the tile's right face), the Z face j+1/2
         const int f = i0 + w;
         R zR[3] = {R(0), R(0), R(0)};
@@ -714,8 +892,10 @@ __device__ __forceinline__ double warp_sum(double v) {
 enum { KC_NCK, KC_NCKP, KC_NCKM, KC_DNKP, KC_DNK, KC_DNKM, KC_IDNU, KC_ICK, KC_ICKP, KC_ICKM, KC_DNU, KC_N };
 
 // Per-cell inputs staged in shared memory, 32 cells at a time per warp.
+// CS_SUM_R / CS_SUM_Z receive each cell's sum over bins of dnu (H_old - H), which the warp's
+// lanes turn into the cell's momentum, force and diagnostics once per 32 cells, one cell per lane.
 enum { CS_ALPHA, CS_ALPHA_C, CS_PD, CS_JS, CS_PHI_INV, CS_ALPHA_CF, CS_T, CS_DUR_DR, CS_DUR_DZ, CS_DUZ_DR,
-       CS_DUZ_DZ, CS_UR_OVER_R, CS_DV, CS_DRU_R, CS_DRU_Z, CS_N };
+       CS_DUZ_DZ, CS_UR_OVER_R, CS_DV, CS_DRU_R, CS_DRU_Z, CS_SUM_R, CS_SUM_Z, CS_N };
 
 // The next cell's bin rows (J, H_r, H_Z, H_voigt, J_old) are prefetched into a per-warp double
 // buffer while the current cell computes, up to two bins per lane (four or more would leave
@@ -748,7 +928,39 @@ __device__ __forceinline__ void cp_async_el(T *dst, const T *src) {
     else
         asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(src) : "memory");
 }
+// Asynchronous global -> shared copy of 16 bytes (cp.async.cg: L2 only, the rows are streamed).
+__device__ __forceinline__ void cp_async_16(void *dst, const void *src) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+// A lane's M contiguous bins of one row as whole 16-byte words, when the row layout allows it
+// (k_freq's `vec` path): loads from shared memory and stores to global memory.
+template <typename S, int M>
+struct LaneRow {
+    static constexpr bool ok = (M * sizeof(S)) % 16 == 0;
+    static constexpr int words = (M * (int)sizeof(S)) / 16;
+    __device__ __forceinline__ static void load(const S *src, S (&v)[M]) {
+        if constexpr (ok) {
+#pragma unroll
+            for (int w = 0; w < words; w++) {
+                const float4 t = reinterpret_cast<const float4 *>(src)[w];
+                memcpy(&v[w * (16 / sizeof(S))], &t, 16);
+            }
+        }
+    }
+    __device__ __forceinline__ static void store(S *dst, const S (&v)[M]) {
+        if constexpr (ok) {
+#pragma unroll
+            for (int w = 0; w < words; w++) {
+                float4 t;
+                memcpy(&t, &v[w * (16 / sizeof(S))], 16);
+                reinterpret_cast<float4 *>(dst)[w] = t;
+            }
+        }
+    }
+};
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
@@ -816,10 +1028,34 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
     S *pf = reinterpret_cast<S *>(fsm + freq_smem_off_pf<M>(nw)) + warp * 2 * 5 * NP;  // [2][5][NP]
     const bool jo_alias = a.Jold == a.Jin;
     const bool need_ff = a.do_freq && a.update_ff, need_js = a.do_emission || (a.parts & PART_DIAG);
-    // copies of cell cl's bin rows into prefetch buffer b (element k of lane l, bin m at m*32+l)
+    // With `vec`, every lane's M bins of a row are whole 16-byte words in global and shared
+    // memory (row starts 16-byte aligned, n_nu a multiple of M): rows move as 16-byte copies,
+    // loads and stores, bin m of lane l at l*M + m. Otherwise element by element, bin m of
+    // lane l at m*32 + l.
+    using LR = LaneRow<S, M>;
+    const bool vec = LR::ok && a.vec16;
+    // copies of cell cl's bin rows into prefetch buffer b
     auto issue = [&](int cl, int b) {
         const long long base = o3 + (long long)cl * nnu;
         S *d = pf + b * 5 * NP;
+        if constexpr (LR::ok) {
+            if (vec) {
+                if (lane * M < nnu) {
+                    const long long g = base + lane * M;
+                    const int q = lane * M;
+                    constexpr int per = 16 / sizeof(S);
+#pragma unroll
+                    for (int w = 0; w < LR::words; w++) {
+                        cp_async_16(d + q + w * per, a.Jin + g + w * per);
+                        cp_async_16(d + NP + q + w * per, a.Hrin + g + w * per);
+                        cp_async_16(d + 2 * NP + q + w * per, a.HZin + g + w * per);
+                        cp_async_16(d + 3 * NP + q + w * per, a.Hv + g + w * per);
+                        if (!jo_alias) cp_async_16(d + 4 * NP + q + w * per, a.Jold + g + w * per);
+                    }
+                }
+                return;
+            }
+        }
 #pragma unroll
         for (int m = 0; m < M; m++) {
             const int k = lane * M + m, q = m * 32 + lane;
@@ -832,6 +1068,39 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
             }
         }
     };
+    const double k4 = kFourPiOverC * (1.0 / c_tilde) * a.j_scale;
+    const double inv_dt = 1.0 / dt;
+    // the per-cell part of the epilogue for cells [gb, ge) of the run (ge - gb <= 32), one
+    // cell per lane: the momentum Delta rho u, this step's force, and the M_F, L and radial
+    // partials (Update_f_Lya_MF_L_Lya!, src/ConstantsAndFunctions.jl:588-674)
+    auto flush = [&](int gb, int ge) {
+        __syncwarp();
+        const int cl = gb + lane;
+        if (cl >= ge) return;
+        const long long c = oc + cl;
+        const double drs = cs[CS_SUM_R * 32 + lane], dzs = cs[CS_SUM_Z * 32 + lane];
+        if (a.do_emission && a.dru_r) {
+            a.dru_r[c] = cs[CS_DRU_R * 32 + lane] + k4 * drs;
+            a.dru_Z[c] = cs[CS_DRU_Z * 32 + lane] + k4 * dzs;
+        }
+        if (a.parts & PART_DIAG) {
+            const int i = cl % nr, j = cl / nr;
+            const double dV = cs[CS_DV * 32 + lane];
+            double fr = (k4 * drs) * inv_dt, fz = (k4 * dzs) * inv_dt;
+            if (a.f_r) { a.f_r[c] = fr; a.f_Z[c] = fz; }
+            acc_mf += dV * sqrt(fr * fr + fz * fz);
+            acc_L += kFourPi * dV * cs[CS_JS * 32 + lane];
+            double drr = __ldg(a.rCoM + cd.ocol + i), dzz = __ldg(a.ZCoM + cd.orow + j) - z_center;
+            double dist = sqrt(drr * drr + dzz * dzz);
+            double frad = 0.0;
+            if (dist > 0.0) {
+                double id = 1.0 / dist;
+                frad = fr * (drr * id) + fz * (dzz * id);
+            }
+            acc_net += dV * frad;
+            acc_out += dV * (frad > 0.0 ? frad : 0.0);
+        }
+    };
     if constexpr (PF) {
         if (wbeg < wend) issue(wbeg, 0);
         cp_async_commit();
@@ -842,6 +1111,7 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
         const long long c = oc + cl;
         const long long base = o3 + (long long)cl * nnu;
         if (((cl - wbeg) & 31) == 0) {
+            if (cl > wbeg) flush(g0, cl);
             // stage the per-cell inputs of the next 32 cells of the run (one coalesced load per
             // field instead of a dependent load per cell)
             g0 = cl;
@@ -876,15 +1146,37 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
             cp_async_commit();
             cp_async_wait<1>();                   // this cell's copies (each lane reads its own)
             const S *d = pf + b * 5 * NP;
+            bool done = false;
+            if constexpr (LR::ok) {
+                if (vec) {
+                    if (lane * M < nnu) {
+                        const int q = lane * M;
+                        S hv[M], jo[M];
+                        LR::load(d + q, J);
+                        LR::load(d + NP + q, Hr);
+                        LR::load(d + 2 * NP + q, HZ);
+                        LR::load(d + 3 * NP + q, hv);
+                        LR::load(d + (jo_alias ? 0 : 4 * NP) + q, jo);
 #pragma unroll
-            for (int m = 0; m < M; m++) {
-                const int k = lane * M + m, q = m * 32 + lane;
-                const bool vld = k < nnu;
-                J[m] = vld ? d[q] : S(0);
-                Hr[m] = vld ? d[NP + q] : S(0);
-                HZ[m] = vld ? d[2 * NP + q] : S(0);
-                Hv[m] = vld ? R(d[3 * NP + q]) : R(0);
-                Jo[m] = vld ? double(jo_alias ? d[q] : d[4 * NP + q]) : 0.0;
+                        for (int m = 0; m < M; m++) { Hv[m] = R(hv[m]); Jo[m] = double(jo[m]); }
+                    } else {
+#pragma unroll
+                        for (int m = 0; m < M; m++) { J[m] = Hr[m] = HZ[m] = S(0); Hv[m] = R(0); Jo[m] = 0.0; }
+                    }
+                    done = true;
+                }
+            }
+            if (!done) {
+#pragma unroll
+                for (int m = 0; m < M; m++) {
+                    const int k = lane * M + m, q = m * 32 + lane;
+                    const bool vld = k < nnu;
+                    J[m] = vld ? d[q] : S(0);
+                    Hr[m] = vld ? d[NP + q] : S(0);
+                    HZ[m] = vld ? d[2 * NP + q] : S(0);
+                    Hv[m] = vld ? R(d[3 * NP + q]) : R(0);
+                    Jo[m] = vld ? double(jo_alias ? d[q] : d[4 * NP + q]) : 0.0;
+                }
             }
         } else {
 #pragma unroll
@@ -930,11 +1222,10 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
             }
             dr_sum = warp_sum(dr_sum);
             dz_sum = warp_sum(dz_sum);
-            if (lane == 0 && a.dru_r) {
-                const double k4 = kFourPiOverC * (1.0 / c_tilde) * a.j_scale;
-                a.dru_r[c] = cv[CS_DRU_R * 32] + k4 * dr_sum;
-                a.dru_Z[c] = cv[CS_DRU_Z * 32] + k4 * dz_sum;
-            }
+        }
+        if (lane == 0) {     // turned into the cell's momentum and diagnostics by flush()
+            cs[CS_SUM_R * 32 + (cl - g0)] = dr_sum;
+            cs[CS_SUM_Z * 32 + (cl - g0)] = dz_sum;
         }
         // ---- FrequencyUpdateJLya_AllCells! (src/UpdateLyaJandH.jl:231-391) ----
         if (a.do_freq) {
@@ -1059,15 +1350,27 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
             }
         }
         // ---- store ----
+        if (LR::ok && vec) {
+            if (lane * M < nnu) {
 #pragma unroll
-        for (int m = 0; m < M; m++) {
-            int k = lane * M + m;
-            if (k >= nnu) continue;
-            S js = S(J[m]), hs = S(Hr[m]), zs = S(HZ[m]);
-            if (!isfinite(double(js)) || !isfinite(double(hs)) || !isfinite(double(zs))) bad |= ERRB_NONFINITE;
-            a.Jout[base + k] = js;
-            a.Hrout[base + k] = hs;
-            a.HZout[base + k] = zs;
+                for (int m = 0; m < M; m++)
+                    if (!isfinite(double(J[m])) || !isfinite(double(Hr[m])) || !isfinite(double(HZ[m])))
+                        bad |= ERRB_NONFINITE;
+                LR::store(a.Jout + base + lane * M, J);
+                LR::store(a.Hrout + base + lane * M, Hr);
+                LR::store(a.HZout + base + lane * M, HZ);
+            }
+        } else {
+#pragma unroll
+            for (int m = 0; m < M; m++) {
+                int k = lane * M + m;
+                if (k >= nnu) continue;
+                S js = S(J[m]), hs = S(Hr[m]), zs = S(HZ[m]);
+                if (!isfinite(double(js)) || !isfinite(double(hs)) || !isfinite(double(zs))) bad |= ERRB_NONFINITE;
+                a.Jout[base + k] = js;
+                a.Hrout[base + k] = hs;
+                a.HZout[base + k] = zs;
+            }
         }
         // ---- epilogue partials ----
         if (a.parts & PART_ACTIVE) {
@@ -1103,26 +1406,9 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
                 }
             }
             acc_esc += esc;
-            if (lane == 0) {
-                const double dV = cv[CS_DV * 32];
-                const double k4 = kFourPiOverC * (1.0 / c_tilde) * a.j_scale;
-                const double inv_dt = 1.0 / dt;
-                double fr = (k4 * dr_sum) * inv_dt, fz = (k4 * dz_sum) * inv_dt;
-                if (a.f_r) { a.f_r[c] = fr; a.f_Z[c] = fz; }
-                acc_mf += dV * sqrt(fr * fr + fz * fz);
-                acc_L += kFourPi * dV * cv[CS_JS * 32];
-                double drr = __ldg(a.rCoM + cd.ocol + i), dzz = __ldg(a.ZCoM + cd.orow + j) - z_center;
-                double dist = sqrt(drr * drr + dzz * dzz);
-                double frad = 0.0;
-                if (dist > 0.0) {
-                    double id = 1.0 / dist;
-                    frad = fr * (drr * id) + fz * (dzz * id);
-                }
-                acc_net += dV * frad;
-                acc_out += dV * (frad > 0.0 ? frad : 0.0);
-            }
         }
     }
+    if (wbeg < wend) flush(g0, wend);
     if constexpr (PF) cp_async_wait<0>();
     if (bad) atomicOr(a.err, bad);
     if (!a.parts) return;
@@ -1132,6 +1418,10 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
     for (int m = 0; m < M; m++) red[warp * stride + lane * M + m] = acc_e[m];
     acc_tot = warp_sum(acc_tot);
     acc_esc = warp_sum(acc_esc);
+    acc_mf = warp_sum(acc_mf);
+    acc_net = warp_sum(acc_net);
+    acc_out = warp_sum(acc_out);
+    acc_L = warp_sum(acc_L);
     if (lane == 0) {
         red[warp * stride + NP + 0] = acc_tot;
         red[warp * stride + NP + 1] = acc_mf;
@@ -1288,22 +1578,28 @@ __global__ void __launch_bounds__(1024) k_reduce(RedArgs a) {
 }
 
 // ---- launch wrappers ----------------------------------------------------------------------
-template <typename S, typename R>
+template <typename S, typename R, bool TMA>
 static size_t adv_smem_bytes() {
-    constexpr int HF = sizeof(S) == sizeof(R) ? 2 : 3;
-    return sizeof(R) * 32 * (RING * MCOL * nf<R>() + (MT + 1) * 5) + sizeof(S) * 32 * RING * MT * HF +
-           (sizeof(R) == 4 ? sizeof(double) * MWARPS * GEO_N : 0);   // the row slots (FP32 arithmetic)
+    if (!TMA) return adv_smem_base<S, R>();
+    return adv_tma_off(adv_smem_base<S, R>()) + raw_tile_bytes<S>() + 16;   // raw tile, mbarrier, abort flag
 }
 
-template <typename S, typename R, int FLUX, int MINB>
-static void adv_launch(const void *args, int ntiles, cudaStream_t st) {
+template <typename S, typename R, int FLUX, int MINB, bool TMA>
+static void adv_launch_t(const void *args, int ntiles, cudaStream_t st) {
     static bool attr = false;
-    size_t sm = adv_smem_bytes<S, R>();
+    size_t sm = adv_smem_bytes<S, R, TMA>();
     if (!attr) {
-        cudaFuncSetAttribute(k_advect<S, R, FLUX, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        cudaFuncSetAttribute(k_advect<S, R, FLUX, MINB, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         attr = true;
     }
-    k_advect<S, R, FLUX, MINB><<<ntiles, MTHREADS, sm, st>>>(*static_cast<const AdvArgs<S> *>(args));
+    k_advect<S, R, FLUX, MINB, TMA><<<ntiles, MTHREADS, sm, st>>>(*static_cast<const AdvArgs<S> *>(args));
+}
+
+// the bulk-copy staging runs when the caller encoded tensor maps for this launch's input state
+template <typename S, typename R, int FLUX, int MINB>
+static void adv_launch(const void *args, int ntiles, cudaStream_t st) {
+    if (static_cast<const AdvArgs<S> *>(args)->tmaps) adv_launch_t<S, R, FLUX, MINB, true>(args, ntiles, st);
+    else adv_launch_t<S, R, FLUX, MINB, false>(args, ntiles, st);
 }
 
 template <typename S, typename R, int FLUX>
@@ -1348,9 +1644,16 @@ int freq_blocks(int ncell, int dev) {
     return want < cap ? (want > 0 ? want : 1) : cap;
 }
 
+static bool al16(const void *p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
 template <typename S, typename R, int M, typename RC>
 static void freq_launch(const void *args, int nitems, cudaStream_t st) {
-    const FreqArgs<S> &fa = *static_cast<const FreqArgs<S> *>(args);
+    FreqArgs<S> fa = *static_cast<const FreqArgs<S> *>(args);
+    // every row of every cloud starts on a 16-byte boundary when the buffers do and a row
+    // (n_nu elements) is a multiple of 16 bytes: cloud offsets are sums of whole rows
+    fa.vec16 = LaneRow<S, M>::ok && fa.nnu % M == 0 && (fa.nnu * sizeof(S)) % 16 == 0 && al16(fa.Jin) &&
+               al16(fa.Hrin) && al16(fa.HZin) && al16(fa.Jold) && al16(fa.Hv) && al16(fa.Jout) && al16(fa.Hrout) &&
+               al16(fa.HZout);
     const size_t sm = sizeof(double) * freq_smem_doubles<M>(FREQ_THREADS / 32, fa.solver == SOLVER_THOMAS);
     static bool attr = false;
     if (!attr) {

@@ -351,35 +351,38 @@ __device__ __forceinline__ R d_colon_grad_u(R Drr, R DrZ, R DZZ, R a, R b, R c, 
 }
 
 // OneMinusphi_L_and_chi_L / OneMinusphi_R_and_chi_R, src/FreqFactors.jl:54-133, in FP64.
+// Every caller clamps P to [-Pmax, Pmax] first (src/FreqFactors.jl:248-250), so the reference's
+// |P| >= Pmax branches only ever see P = +-Pmax, where they return exp(-+Pmax) and
+// (1 - exp(-+Pmax)) / +-Pmax: the general expression at that P. What remains is the choice
+// between the exponential and the second-order Taylor form below |P| = Pmin, taken here by a
+// select on values the warp computes for every lane, so lanes of one warp never take
+// different paths (at P = 0 the unused general value is not finite; the select drops it).
 __device__ __forceinline__ void omphi_L(double P, double &omp, double &chi) {
-    if (P >= kPmax) { omp = exp(-kPmax); chi = (1.0 - omp) / kPmax; return; }
-    if (P <= -kPmax) { omp = exp(kPmax); chi = (1.0 - omp) / (-kPmax); return; }
-    if (fabs(P) < kPmin) { omp = 1.0 - P + 0.5 * (P * P); chi = 1.0 - 0.5 * P; return; }
-    omp = exp(-P);
-    chi = (1.0 - omp) * rcp<double>(P);
+    const double e = exp(-P);
+    const double x = (1.0 - e) * rcp<double>(P);
+    const bool tay = fabs(P) < kPmin;
+    omp = tay ? 1.0 - P + 0.5 * (P * P) : e;
+    chi = tay ? 1.0 - 0.5 * P : x;
 }
 __device__ __forceinline__ void omphi_R(double P, double &omp, double &chi) {
-    if (P >= kPmax) { omp = exp(kPmax); chi = (1.0 - omp) / kPmax; return; }
-    if (P <= -kPmax) { omp = exp(-kPmax); chi = (1.0 - omp) / (-kPmax); return; }
-    if (fabs(P) < kPmin) { omp = 1.0 + P + 0.5 * (P * P); chi = -1.0 - 0.5 * P; return; }
-    omp = exp(P);
-    chi = (1.0 - omp) * rcp<double>(P);
+    const double e = exp(P);
+    const double x = (1.0 - e) * rcp<double>(P);
+    const bool tay = fabs(P) < kPmin;
+    omp = tay ? 1.0 + P + 0.5 * (P * P) : e;
+    chi = tay ? -1.0 - 0.5 * P : x;
 }
 // Both of the above at once for the same P (used for P_k, which needs phi^L and phi^R):
-// one exponential and one reciprocal of P serve the two branches.
+// one exponential and one reciprocal of P serve the two.
 __device__ __forceinline__ void omphi_LR(double P, double &oL, double &xL, double &oR, double &xR) {
-    if (P >= kPmax || P <= -kPmax || fabs(P) < kPmin) {
-        omphi_L(P, oL, xL);
-        omphi_R(P, oR, xR);
-        return;
-    }
-    double e = exp(-P);
-    double ie = rcp<double>(e);
-    double iP = rcp<double>(P);
-    oL = e;
-    xL = (1.0 - e) * iP;
-    oR = ie;
-    xR = (1.0 - ie) * iP;
+    const double e = exp(-P);
+    const double ie = rcp<double>(e);
+    const double iP = rcp<double>(P);
+    const bool tay = fabs(P) < kPmin;
+    const double h = 0.5 * (P * P);
+    oL = tay ? 1.0 - P + h : e;
+    xL = tay ? 1.0 - 0.5 * P : (1.0 - e) * iP;
+    oR = tay ? 1.0 + P + h : ie;
+    xR = tay ? -1.0 - 0.5 * P : (1.0 - ie) * iP;
 }
 // Thermal velocity, Doppler width, Voigt parameter (src/ConstantsAndFunctions.jl:282-314)
 __host__ __device__ __forceinline__ double compute_b(double T) { return sqrt(2.0 * kKBoltz / kMH) * sqrt(T); }

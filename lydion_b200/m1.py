@@ -174,16 +174,18 @@ class M1Context:
         self._ck(lib().lyd_get_timing(self._h, _dp(ms)))
         return ms
 
-    def set_tuning(self, rows_per_tile=16, cells_per_block=0, solver=_lib.SOLVER_PCR, adv_ctas_per_sm=0):
-        t = _lib.Tuning(int(rows_per_tile), int(cells_per_block), int(solver), int(adv_ctas_per_sm))
+    def set_tuning(self, rows_per_tile=16, cells_per_block=0, solver=_lib.SOLVER_PCR, adv_ctas_per_sm=0,
+                   adv_staging=_lib.STAGING_AUTO):
+        t = _lib.Tuning(int(rows_per_tile), int(cells_per_block), int(solver), int(adv_ctas_per_sm), int(adv_staging))
         self._ck(lib().lyd_set_tuning(self._h, C.byref(t)))
 
     def tuning(self):
-        """(rows_per_tile, cells_per_block, solver, adv_ctas_per_sm); cells_per_block < 0 when
-        chosen automatically."""
+        """(rows_per_tile, cells_per_block, solver, adv_ctas_per_sm, adv_staging); cells_per_block
+        < 0 when chosen automatically; adv_staging is the staging the advection uses
+        (STAGING_LANES or STAGING_TMA)."""
         t = _lib.Tuning()
         self._ck(lib().lyd_get_tuning(self._h, C.byref(t)))
-        return t.rows_per_tile, t.cells_per_block, t.solver, t.adv_ctas_per_sm
+        return t.rows_per_tile, t.cells_per_block, t.solver, t.adv_ctas_per_sm, t.adv_staging
 
     # -- adjoint ---------------------------------------------------------------------------
     def adjoint(self, n_steps, c_tilde, dt, z_center, bc_r_right=BC_OUTFLOW, bc_z_bot=BC_REFLECT,

@@ -47,6 +47,38 @@ def max_rel(a, b, floor=0.0):
     return float(np.max(np.abs(a - b)[m] / scale[m]))
 
 
+def escaping_flux_per_bin(H_r, H_Z, geom, bc_z_bot):
+    """Outward flux per frequency bin through the outer r face, the top face and (when it lets
+    flow out) the bottom face: the per-bin sum behind Compute_f_esc_Lya_Cylindrical
+    (src/ConstantsAndFunctions.jl:969-993), before the bin widths and 1/L. H arrays are [j, i, k]."""
+    esc = np.einsum("j,jk->k", geom.A_r[:, -1], np.maximum(H_r[:, -1, :], 0.0))
+    esc += np.einsum("i,ik->k", geom.A_Z[-1, :], np.maximum(H_Z[-1, :, :], 0.0))
+    if bc_z_bot == W.BC_OUTFLOW:
+        esc += np.einsum("i,ik->k", geom.A_Z[0, :], np.maximum(-H_Z[0, :, :], 0.0))
+    return esc
+
+
+def wing_checks(ctx, st, cloud, floor=1e-6):
+    """Per-element errors relative to each element, with a floor of `floor` times the quantity's
+    maximum, so faint wing bins are held to the same relative bound as the line centre until
+    they fall below the floor: J, the flux fractions H_r/J and H_Z/J, the edge-ring spectrum
+    and the per-bin escaping flux of the CUDA state against the oracle's."""
+    out = {}
+    Jo = st.J
+    Jfloor = np.maximum(Jo, floor * Jo.max())
+    out["J"] = max_rel(ctx.download("J"), Jo, floor=floor * Jo.max())
+    # H changes sign, so near its zeros an error relative to H itself means nothing; it is
+    # held relative to the same element's J instead, i.e. as an error of the flux fraction H/J
+    for f in ("H_r", "H_Z"):
+        out[f] = float(np.max(np.abs(ctx.download(f) - getattr(st, f)) / Jfloor))
+    raw_g, raw_o = ctx.edge_spectra()[0], st.edge_spectra()[0]
+    out["edge_spectrum"] = max_rel(raw_g, raw_o, floor=floor * np.abs(raw_o).max())
+    eg = escaping_flux_per_bin(ctx.download("H_r"), ctx.download("H_Z"), cloud.geom, cloud.bc_z_bot)
+    eo = escaping_flux_per_bin(st.H_r, st.H_Z, cloud.geom, cloud.bc_z_bot)
+    out["escaping_flux"] = max_rel(eg, eo, floor=floor * np.abs(eo).max())
+    return out
+
+
 def norm_err(a, b):
     """max |a - b| / max |b| (error relative to the field's scale)."""
     a = np.asarray(a, dtype=np.float64)

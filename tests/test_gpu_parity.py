@@ -9,7 +9,7 @@ conditioning of the system (~1e-9 relative at F/dw ~ 4e8, tau0 = 1e8, measured a
 import numpy as np
 import pytest
 
-from helpers import CLOUDS, matched_pair, max_rel, norm_err, random_state
+from helpers import CLOUDS, matched_pair, max_rel, norm_err, random_state, wing_checks
 from lydion_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
@@ -294,21 +294,31 @@ def test_bad_arguments_are_rejected(oracle_mod):
 
 
 def test_full_size_c2_steps_match_oracle(oracle_mod):
-    """The headline 256x256x64 cloud: 6 fused steps against the oracle."""
+    """The headline 256x256x64 cloud over 200 fused steps against the oracle: every step's
+    active window and M_F; the final J, the flux fractions and the edge-ring spectrum per
+    element with a floor of 1e-6 of the maximum (the wing bins); the per-bin escaping flux.
+    The escaping flux sums max(H, 0) over the boundary faces: where a boundary cell's H
+    changes sign the clipped sum keeps the cancellation error of H, so its bound is looser."""
     cl = W.config_c2()
     st, ctx = matched_pair(oracle_mod, cl)
-    d_o = st.run(6)
-    d_g = ctx.static_steps(6, cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+    n = 200
+    d_o = st.run(n)
+    d_g = ctx.static_steps(n, cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
     np.testing.assert_array_equal(d_g[:, 5:7], d_o[:, 5:7])
-    assert max_rel(d_g[1:, 0], d_o[1:, 0]) < 1e-9
+    assert max_rel(d_g[1:, 0], d_o[1:, 0]) < 1e-8
     for f in ("J", "H_r", "H_Z"):
-        assert norm_err(ctx.download(f), getattr(st, f)) < 1e-9, f
+        assert norm_err(ctx.download(f), getattr(st, f)) < 1e-8, f
+    w = wing_checks(ctx, st, cl)
+    for q in ("J", "H_r", "H_Z", "edge_spectrum"):
+        assert w[q] < 1e-8, (q, w[q])
+    assert w["escaping_flux"] < 1e-5, w["escaping_flux"]
 
 
 def test_c1_point_source_1000_steps_match_oracle(oracle_mod):
     """The plain-FP64 point-source cloud (64 x 64 x 64, tau0 = 1e6, recoil on) over the 1000
-    steps it is specified with, against the oracle: the active window of every step, M_F, the
-    final J and H and the edge-ring spectra."""
+    steps it is specified with, against the oracle: the active window of every step, M_F, and
+    per element with a floor of 1e-6 of the maximum, the final J, the flux fractions, the
+    edge-ring spectrum and the per-bin escaping flux."""
     cl = W.config_c1()
     st, ctx = matched_pair(oracle_mod, cl)
     n = 1000
@@ -318,9 +328,31 @@ def test_c1_point_source_1000_steps_match_oracle(oracle_mod):
     assert max_rel(d_g[1:, 0], d_o[1:, 0]) < 1e-9
     for f in ("J", "H_r", "H_Z"):
         assert norm_err(ctx.download(f), getattr(st, f)) < 1e-9, f
-    raw_g = ctx.edge_spectra()[0]
-    raw_o = st.edge_spectra()[0]
-    assert norm_err(raw_g, raw_o) < 1e-9
+    w = wing_checks(ctx, st, cl)
+    for q in ("J", "H_r", "H_Z", "edge_spectrum", "escaping_flux"):
+        assert w[q] < 1e-8, (q, w[q])
+
+
+def test_c5_slice_256x256x128_matches_oracle(oracle_mod):
+    """A 256 x 256 x 128-bin slice of the largest-field workload (the synthetic RHD snapshot:
+    lognormal n_H, photoionised bubble with p_d from pd_Lya on the device, shell outflow, dust)
+    over 20 steps against the oracle: windows, M_F, and J, the flux fractions and the edge
+    spectrum per element with a floor of 1e-6 of the maximum. After 20 steps no radiation has
+    reached the outer faces, so the escaping flux is not compared."""
+    from lydion_b200.m1 import context_for_cloud
+    cl = W.rhd_snapshot_cloud(n=256, n_nu=128, name="c5_slice_256x256x128")
+    ctx = context_for_cloud(cl)          # computes p_d on the device from the species
+    st = oracle_mod.OracleState(cl)
+    st.setup_profiles()
+    n = 20
+    d_o = st.run(n)
+    d_g = ctx.static_steps(n, cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+    np.testing.assert_array_equal(d_g[:, 5:7], d_o[:, 5:7])
+    assert max_rel(d_g[1:, 0], d_o[1:, 0]) < 1e-10
+    w = wing_checks(ctx, st, cl)
+    for q in ("J", "H_r", "H_Z", "edge_spectrum"):
+        assert w[q] < 1e-8, (q, w[q])
+    ctx.close()
 
 
 def test_rhd_snapshot_field_matches_oracle(oracle_mod):
