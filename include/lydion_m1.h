@@ -246,7 +246,8 @@ int  lyd_batch_steps(lyd_ctx *ctx, const lyd_cloud_params *params, int32_t n_ste
  * 2..3 with FP64, or 0 for the default: 4 and 3), and how the advection stages its rows
  * (LYD_STAGING_*). lyd_get_tuning reports an automatic cell count as its negative and the
  * staging actually used. */
-#define LYD_STAGING_AUTO   0   /* the library's choice for the precision and layout            */
+#define LYD_STAGING_AUTO   0   /* the library's choice: bulk copies with FP32 storage, per-lane
+                                  loads otherwise                                               */
 #define LYD_STAGING_LANES  1   /* per-lane loads of every staged cell                         */
 #define LYD_STAGING_TMA    2   /* bulk tensor copies (TMA) of each row's 32-bin x 12-column box,
                                   a row ahead, when a row of n_nu bins is a multiple of 16 bytes */

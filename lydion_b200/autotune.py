@@ -1,14 +1,16 @@
 """Launch-shape autotuner for the Lyman-alpha step.
 
-Four knobs of a context are tuned (lyd_set_tuning):
+Five knobs of a context are tuned (lyd_set_tuning):
   rows_per_tile    rows of the advection tile each CTA marches through (4..64);
   adv_ctas_per_sm  resident advection CTAs per SM (2..4 with FP32 arithmetic, 2..3 with FP64);
+  adv_staging      how the advection stages its rows: per-lane loads (1) or bulk tensor copies
+                   of each row's box completed on an mbarrier (2);
   cells_per_block  cells per frequency-kernel block (8..1024, or 0 = automatic);
   solver           frequency tridiagonal solver: 0 = parallel cyclic reduction across the warp,
                    1 = lane-serial elimination.
-The advection kernel depends only on rows_per_tile and adv_ctas_per_sm, the frequency kernel
-and the reductions only on the other two, so the search is two short sweeps: rows x CTAs
-first (advection time), then cells x solver (frequency + reduction time). Every candidate is timed on the device with the
+The advection kernel depends only on rows_per_tile, adv_ctas_per_sm and adv_staging, the
+frequency kernel and the reductions only on the other two, so the search is two short sweeps:
+rows x CTAs x staging first (advection time), then cells x solver (frequency + reduction time). Every candidate is timed on the device with the
 library's per-kernel CUDA events (lyd_set_timing) over a few real steps of the caller's
 workload, after one untimed step that applies the new shape.
 
@@ -30,6 +32,8 @@ ROWS = (4, 8, 12, 16, 20, 24, 32, 40, 48)
 CTAS = (2, 3, 4)
 CELLS = (0, 16, 32, 64, 128, 256, 512)
 SOLVERS = (0, 1)
+STAGING = (1, 2)        # per-lane loads, bulk tensor copies (the library falls back to the first
+                        # where the layout does not allow the second)
 
 
 def cache_path():
@@ -51,7 +55,7 @@ def workload_key(ctx, device=0):
     """GPU name + bins + precision + cloud sizes (hashed for batches)."""
     sizes = getattr(ctx, "sizes", None) or [(ctx.n_r, ctx.n_z)]
     h = hashlib.sha1(np.asarray(sorted(sizes), dtype=np.int64).tobytes()).hexdigest()[:12]
-    return f"{device_name(device)}|nnu={ctx.n_nu}|prec={ctx.precision}|clouds={len(sizes)}|sizes={h}"
+    return f"{device_name(device)}|nnu={ctx.n_nu}|prec={ctx.precision}|clouds={len(sizes)}|sizes={h}|knobs=5"
 
 
 def _load(path):
@@ -103,7 +107,7 @@ def _measure(ctx, run, tuning, steps):
     return ms
 
 
-def search(ctx, run, steps=10, rows=ROWS, cells=CELLS, solvers=SOLVERS, ctas=CTAS, reset=None):
+def search(ctx, run, steps=10, rows=ROWS, cells=CELLS, solvers=SOLVERS, ctas=CTAS, staging=STAGING, reset=None):
     """Time every candidate (each after `reset()`, when given); return (best tuning tuple, table
     of (tuning, ms[3]))."""
     table = []
@@ -112,17 +116,18 @@ def search(ctx, run, steps=10, rows=ROWS, cells=CELLS, solvers=SOLVERS, ctas=CTA
     best_rows, best_adv = None, np.inf
     for r in rows:
         for o in ctas:
-            t = (r, 0, 0, o)
-            if reset:
-                reset()
-            ms = _measure(ctx, run, t, steps)
-            table.append((t, ms.tolist()))
-            if ms[0] < best_adv:
-                best_rows, best_adv = (r, o), ms[0]
+            for g in staging:
+                t = (r, 0, 0, o, g)
+                if reset:
+                    reset()
+                ms = _measure(ctx, run, t, steps)
+                table.append((t, ms.tolist()))
+                if ms[0] < best_adv:
+                    best_rows, best_adv = (r, o, g), ms[0]
     best, best_f = None, np.inf
     for s in solvers:
         for cb in cells:
-            t = (best_rows[0], cb, s, best_rows[1])
+            t = (best_rows[0], cb, s, best_rows[1], best_rows[2])
             if reset:
                 reset()
             ms = _measure(ctx, run, t, steps)

@@ -9,13 +9,13 @@ class FakeCtx:
     n_nu, n_r, n_z, precision = 64, 256, 256, 0
 
     def __init__(self):
-        self.t = (16, 0, 0, 0)
+        self.t = (16, 0, 0, 0, 0)
         self.timing_on = False
         self.steps = 0
         self.applied = []
 
-    def set_tuning(self, r, c, s, o=0):
-        self.t = (r, c, s, o)
+    def set_tuning(self, r, c, s, o=0, g=0):
+        self.t = (r, c, s, o, g)
         self.applied.append(self.t)
 
     def synchronize(self):
@@ -25,8 +25,8 @@ class FakeCtx:
         self.timing_on = on
 
     def timing(self):
-        r, c, s, o = self.t
-        adv = 1.0 + abs(r - 8) * 0.1 + 0.05 * abs(o - 3)
+        r, c, s, o, g = self.t
+        adv = 1.0 + abs(r - 8) * 0.1 + 0.05 * abs(o - 3) + (0.02 if g == 1 else 0.0)
         freq = 2.0 + (0.5 if s == 1 else 0.0) + abs((c or 96) - 64) * 0.01
         return [adv * self.steps, freq * self.steps, 0.1 * self.steps]
 
@@ -37,29 +37,29 @@ class FakeCtx:
 def test_search_picks_the_fastest_shape():
     ctx = FakeCtx()
     best, table = A.search(ctx, ctx.run, steps=5)
-    assert best[:3] == (8, 64, 0)
-    assert len(table) == len(A.ROWS) * 2 + len(A.CELLS) * len(A.SOLVERS)
+    assert best[:3] == (8, 64, 0) and best[4] == 2
+    assert len(table) == len(A.ROWS) * 2 * len(A.STAGING) + len(A.CELLS) * len(A.SOLVERS)
     assert not ctx.timing_on
     ctx = FakeCtx()
     ctx.precision = 1
     best, table = A.search(ctx, ctx.run, steps=5)
-    assert best == (8, 64, 0, 3)
-    assert len(table) == len(A.ROWS) * len(A.CTAS) + len(A.CELLS) * len(A.SOLVERS)
+    assert best == (8, 64, 0, 3, 2)
+    assert len(table) == len(A.ROWS) * len(A.CTAS) * len(A.STAGING) + len(A.CELLS) * len(A.SOLVERS)
 
 
 def test_cache_round_trip(tmp_path, monkeypatch):
     monkeypatch.setattr(A, "device_name", lambda device=0: "fake-gpu")
     path = str(tmp_path / "tune.json")
     ctx = FakeCtx()
-    assert A.autotune(ctx, ctx.run, steps=3, cache=path) == (8, 64, 0, 3)
+    assert A.autotune(ctx, ctx.run, steps=3, cache=path) == (8, 64, 0, 3, 2)
     data = json.load(open(path))
     key = A.workload_key(ctx)
     assert key.startswith("fake-gpu|nnu=64|prec=0|clouds=1|")
-    assert data[key]["tuning"] == [8, 64, 0, 3]
+    assert data[key]["tuning"] == [8, 64, 0, 3, 2]
     # a second call applies the cached shape without timing anything
     ctx2 = FakeCtx()
-    assert A.autotune(ctx2, ctx2.run, steps=3, cache=path) == (8, 64, 0, 3)
-    assert ctx2.applied == [(8, 64, 0, 3)]
+    assert A.autotune(ctx2, ctx2.run, steps=3, cache=path) == (8, 64, 0, 3, 2)
+    assert ctx2.applied == [(8, 64, 0, 3, 2)]
 
 
 def test_batch_key_depends_on_sizes(monkeypatch):
