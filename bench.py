@@ -281,6 +281,65 @@ def e2e_form(ctx, cloud, args, barrier, stream_of, world):
             "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes + 7 * 8, "steps": n}
 
 
+def dropin_form(cloud, args, stream_of, local):
+    """End to end through the drop-in functions with the reference's signatures
+    (lydion_b200/lya.py): the static-cloud loop of src/StaticCloudTest.jl:362-392 called
+    phase by phase on host numpy arrays, FP64. In copy mode every call moves the state it
+    reads and writes (the host arrays are always current); in resident mode the state and the
+    inputs stay on the device and only the diagnostics come back. The bytes are those the
+    drop-ins moved, counted per step."""
+    from lydion_b200 import lya as D
+    from lydion_b200.m1 import context_for_cloud
+    ctx = context_for_cloud(cloud, device=local)
+    hv = ctx.download("Hvoigt")
+    state = {n: ctx.download(n) for n in ("J", "H_r", "H_Z")}
+    ctx.close()
+    # the emission profile over the core bins, normalised per cell (Update_phi_nu!,
+    # src/ConstantsAndFunctions.jl:362-393): the static driver's input, made on the host as there
+    fq = cloud.freq
+    core = slice(fq.kcore_min, fq.kcore_max + 1)
+    phi = np.zeros_like(hv)
+    phi[..., core] = hv[..., core] / np.sum(hv[..., core] * fq.dnu[core], axis=-1, keepdims=True)
+    out = {"workload": WORKLOAD, "precision": "fp64"}
+    for mode, n in (("copy_every_call", max(3, min(5, args.steps))), ("resident", max(10, min(50, args.steps)))):
+        S = D.generate_lya_arrays_from_saved(cloud.c_tilde, cloud.freq, cloud.geom, cloud.T, hv, phi,
+                                             recoil=cloud.recoil)
+        for name in ("alpha", "alpha_c", "pd", "js"):
+            getattr(S, name)[...] = getattr(cloud, name)
+        S.alpha_F[...] = S.alpha[:, :, None] * S.Hvoigt         # src/StaticCloudTest.jl:283-285
+        for name, a in state.items():
+            getattr(S, name)[...] = a
+            getattr(S, name + "_old")[...] = a
+        if mode == "resident":
+            D.set_resident(S)
+        g, ct, dt = cloud.geom, cloud.c_tilde, cloud.dt
+        vel = (cloud.u_r_star, cloud.u_Z_star, cloud.dur_dr, cloud.dur_dZ, cloud.duZ_dr, cloud.duZ_dZ,
+               cloud.ur_over_r)
+
+        def loop(k):
+            for _ in range(k):
+                D.advect_lya(ct * dt, S, g, *vel, "Reflect", "Outflow", "Reflect", "Outflow")
+                D.lya_emission_absorption_update(S.J, S.J_old, S.H_r, S.H_Z, S.H_r_old, S.H_Z_old, S.js, S.phi_nu,
+                                                 S.Hvoigt, S.alpha, S.alpha_c, S.alpha_F, S.pd, S.dru_r, S.dru_Z,
+                                                 S.dnu, ct, dt)
+                D.frequency_update_J_lya_all_cells(ct * dt, S, cloud.T, *vel[2:], True)
+                mf = D.update_f_lya_MF_L_lya(S.f_r, S.f_Z, S.dru_r, S.dru_Z, S.js, g.dV, g.rCoM, g.ZCoM, dt,
+                                             cloud.z_center, "Reflect")
+                S.M_F, S.M_F_radial_net, S.M_F_radial_out, S.L_lya = mf
+                S.f_esc_lya = D.compute_f_esc_lya_cylindrical(S.H_r, S.H_Z, g.A_r, g.A_Z, S.dnu, S.L_lya, "Reflect")
+                D.reset_dru(S.dru_r, S.dru_Z)
+
+        loop(1)
+        tw = D.twin_of(S)
+        u0, d0 = D.transfer_bytes(S)
+        ms = _timed(tw.ctx, loop, n, stream_of)
+        u1, d1 = D.transfer_bytes(S)
+        out[mode] = {"value": n * cloud.cell_bins / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / n, "steps": n,
+                     "h2d_bytes_per_step": (u1 - u0) // n, "d2h_bytes_per_step": (d1 - d0) // n}
+        D.release(S)
+    return out
+
+
 def batch_form(args, barrier, stream_of, local, world):
     """The ragged batch (512 static clouds x 48 bins, sides 32..256, per-cloud CFL step) in both
     forms: a few graph-replayed steps of the whole batch each."""
@@ -487,6 +546,7 @@ def run_gpu(args):
         forms[fname] = {"value": m["value"], "ms_per_step": m["ms_per_step"], "tuning": m["tuning"],
                         "kernel_ms_per_step": {n: float(v) for n, v in zip(names, m["kernel_ms"])},
                         "over_fp64": m["value"] / f64["value"]}
+    dropin = None if (args.no_dropin or world > 1) else dropin_form(cloud, args, stream_of, local)
     batch = None if args.no_batch else batch_form(args, barrier, stream_of, local, world)
     adj = None if (args.no_adjoint or world > 1) else adjoint_form(args, stream_of, local)
     c5 = None if (args.no_c5 or world > 1) else c5_form(args, stream_of, local)
@@ -537,6 +597,7 @@ def run_gpu(args):
                 "active_fraction": f64["active_fraction"],
                 "cpu_baseline": cpu,
                 "e2e": e2e,
+                "e2e_dropin": dropin,
                 "gpu_launches": 3 * args.steps,
                 "clocks": f64["clocks"]}
         print(json.dumps(line), flush=True)
@@ -554,6 +615,7 @@ def main():
     ap.add_argument("--impl", default="lydion", choices=["lydion", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-batch", action="store_true", help="skip the ragged-batch measurement")
+    ap.add_argument("--no-dropin", action="store_true", help="skip the end-to-end leg through the drop-in functions")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward measurement")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of the autotuner")
     ap.add_argument("--no-c5", action="store_true", help="skip the 1024x1024x128 field")

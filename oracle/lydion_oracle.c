@@ -1048,7 +1048,8 @@ void orc_static_step(orc_lya *s, const orc_geom *g, const orc_vel *v, double c_t
 void orc_static_run(orc_lya *s, const orc_geom *g, const orc_vel *v, double c_tilde, double dt,
                     double z_center, int bc_r_right, int bc_z_bot, int bc_z_top, int n_steps,
                     double *diag_hist) {
+    double scratch[7];
     for (int n = 0; n < n_steps; n++)
         orc_static_step(s, g, v, c_tilde, dt, z_center, bc_r_right, bc_z_bot, bc_z_top,
-                        diag_hist ? diag_hist + 7 * (size_t)n : (double[7]){0});
+                        diag_hist ? diag_hist + 7 * (size_t)n : scratch);
 }

@@ -114,6 +114,51 @@ def _p(a):
     return a.ctypes.data_as(P)
 
 
+_DUAL_PATH = os.path.join(_HERE, "build", "liblydion_oracle_dual.so")
+_dual = None
+
+
+def dual_lib():
+    """The oracle compiled with dual numbers (lydion_oracle_dual.cpp): forward-mode derivatives."""
+    global _dual
+    if _dual is None:
+        if not os.path.exists(_DUAL_PATH):
+            build()
+        _dual = C.CDLL(_DUAL_PATH)
+        _dual.orcd_objective_tangent.restype = C.c_int
+        _dual.orcd_objective_tangent.argtypes = [C.c_void_p] * 4 + [C.c_double] * 3 + [C.c_int] * 4 + \
+            [C.c_double] + [P] * 7 + [P]
+    return _dual
+
+
+def objective_tangent(st, n_steps, w_MF=1.0, w_spec=None, seeds=None):
+    """Forward-mode derivative of the static-driver objective w_MF * M_F(last step) +
+    sum_k w_spec[k] S_k(final J) over n_steps from the initial state held by the OracleState
+    `st` (its J, H_r, H_Z; H_voigt, phi_nu and alpha_F recomputed from T inside), along the
+    direction `seeds`: a dict with any of alpha, alpha_c, T (numpy [j, i]), u_r_star, u_Z_star
+    and J0. Returns (objective, directional derivative, M_F, its directional derivative)."""
+    seeds = seeds or {}
+    c = st.cloud
+    keep = []
+
+    def q(name):
+        a = seeds.get(name)
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        keep.append(a)
+        return _p(a)
+
+    ws = None if w_spec is None else np.ascontiguousarray(w_spec, dtype=np.float64)
+    lut = st.lut or OracleLUT()
+    out = np.zeros(4)
+    dual_lib().orcd_objective_tangent(C.byref(st.s), C.byref(st.g), C.byref(st.v), lut.ref, c.c_tilde, c.dt,
+                                      c.z_center, c.bc_r_right, c.bc_z_bot, c.bc_z_top, int(n_steps), float(w_MF),
+                                      None if ws is None else _p(ws), q("alpha"), q("alpha_c"), q("T"),
+                                      q("u_r_star"), q("u_Z_star"), q("J0"), _p(out))
+    return tuple(float(x) for x in out)
+
+
 # ---- Voigt look-up tables (src/FastInterpolations.jl:175-197) ----------------------------
 XMAX_VOIGT = 1000.0
 NX_VOIGT = 200001

@@ -195,3 +195,36 @@ def test_hll_initial_state_and_face_velocity_gradients(prob_hll):
                 continue
             adj = g["grad_" + field][idx] * v0
             assert abs(adj - d) <= 1e-4 * abs(d), (field, idx, adj, d)
+
+
+@pytest.mark.parametrize("flux", [W.FLUX_GLF, W.FLUX_HLL])
+def test_adjoint_matches_forward_mode_oracle(oracle_mod, flux):
+    """An independent derivative: the dual-number build of the oracle (forward mode, every
+    operation of the restated step differentiated by the chain rule, no hand-written
+    derivative) along random directions in alpha, alpha_c, T (with H_voigt(T), phi_nu and
+    alpha_F), the face velocities and the initial J, against the hand-written adjoint's gradient
+    dotted with the same direction. Both are exact derivatives of the same discrete step; they
+    differ by the rounding of two solves of the stiff frequency systems (cyclic reduction on the
+    GPU, pivoted elimination in the oracle) and of the two H_voigt tables."""
+    P = Problem(6, flux)
+    ctx, g = P.adjoint(every=1)
+    ctx.close()
+    cl = P.cl
+    rng = np.random.default_rng(17)
+    seeds = {"alpha": rng.normal(size=cl.alpha.shape) * cl.alpha,
+             "alpha_c": rng.normal(size=cl.alpha_c.shape) * cl.alpha_c,
+             "T": rng.normal(size=cl.T.shape) * cl.T,
+             "u_r_star": rng.normal(size=cl.u_r_star.shape) * cl.u_r_star,
+             "u_Z_star": rng.normal(size=cl.u_Z_star.shape) * cl.u_Z_star,
+             "J0": rng.normal(size=P.state[0].shape) * P.state[0]}
+    st = oracle_mod.OracleState(cl)
+    for name, a in zip(("J", "H_r", "H_Z"), P.state):
+        getattr(st, name)[...] = a
+        getattr(st, name + "_old")[...] = a
+    st.setup_profiles()
+    tol = {"alpha": 1e-8, "alpha_c": 1e-8, "T": 1e-8, "u_r_star": 1e-6, "u_Z_star": 1e-6, "J0": 1e-8}
+    for key, sd in seeds.items():
+        obj, tan, _, _ = oracle_mod.objective_tangent(st, P.n, 1.0, SS * P.w, {key: sd})
+        assert obj == pytest.approx(g["objective"], rel=1e-10)
+        adj = float(np.sum(g["grad_" + key] * sd))
+        assert adj == pytest.approx(tan, rel=tol[key]), (key, adj, tan)

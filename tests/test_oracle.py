@@ -233,3 +233,58 @@ def test_rhd_lya_oracle_pins():
     assert abs(js - L.orc_prob_lya_sh95(1e4, 3.0, 1) * L.orc_krec_hii(1e4, 1) * 2.0 * 3.0 * E) < 1e-12 * js
     # collisional excitation is negligible in cold gas and rises steeply with T
     assert L.orc_js_coll_lya(1e3, 1.0, 1.0) < 1e-40 < L.orc_js_coll_lya(1e4, 1.0, 1.0)
+
+
+def _dual_problem(oracle_mod, flux=0):
+    from helpers import random_state
+    cl = W.small_cloud(nr=8, nz=7, n_nu=16, flux_method=flux)
+    state = random_state(cl, 5)
+    rng = np.random.default_rng(11)
+    seeds = {"alpha": rng.normal(size=cl.alpha.shape) * cl.alpha,
+             "alpha_c": rng.normal(size=cl.alpha_c.shape) * cl.alpha_c,
+             "T": rng.normal(size=cl.T.shape) * cl.T,
+             "u_r_star": rng.normal(size=cl.u_r_star.shape) * cl.u_r_star,
+             "J0": rng.normal(size=state[0].shape) * state[0]}
+    w = np.random.default_rng(1).uniform(0.5, 1.5, cl.n_nu)
+    return cl, state, seeds, w
+
+
+def _plain_objective(oracle_mod, cl, state, n, w, ss, shift):
+    import copy
+    c = copy.deepcopy(cl)
+    st0 = list(state)
+    for k, d in shift.items():
+        if k == "J0":
+            st0[0] = state[0] + d
+        else:
+            setattr(c, k, getattr(cl, k) + d)
+    st = oracle_mod.OracleState(c)
+    for name, a in zip(("J", "H_r", "H_Z"), st0):
+        getattr(st, name)[...] = a
+        getattr(st, name + "_old")[...] = a
+    st.setup_profiles()
+    h = st.run(n)
+    return h[-1, 0] + ss * float(np.dot(w, st.edge_spectra()[0].mean(0)))
+
+
+@pytest.mark.parametrize("flux", [0, 1])
+@pytest.mark.parametrize("field,h", [("alpha", 1e-4), ("alpha_c", 1e-4), ("T", 1e-4), ("J0", 1e-5)])
+def test_dual_oracle_tangent_matches_central_differences(oracle_mod, flux, field, h):
+    """The dual-number build of the oracle (forward-mode derivatives) against central
+    differences of the plain oracle along the same direction, over 4 static steps: alpha,
+    alpha_c, T (through H_voigt, phi_nu and alpha_F too) and the initial J. The step h is the
+    one the difference resolves best: rounding in the stiff frequency solve dominates below it
+    (1e-6 gives differences noisy at 1e-4 relative), the objective's kinks above it."""
+    cl, state, seeds, w = _dual_problem(oracle_mod, flux)
+    sd = {field: seeds[field]}
+    ss, n = 1e12, 4
+    st = oracle_mod.OracleState(cl)
+    for name, a in zip(("J", "H_r", "H_Z"), state):
+        getattr(st, name)[...] = a
+        getattr(st, name + "_old")[...] = a
+    st.setup_profiles()
+    obj, tan, mf, dmf = oracle_mod.objective_tangent(st, n, 1.0, ss * w, sd)
+    assert obj == pytest.approx(_plain_objective(oracle_mod, cl, state, n, w, ss, {}), rel=1e-13)
+    fd = (_plain_objective(oracle_mod, cl, state, n, w, ss, {k: h * v for k, v in sd.items()}) -
+          _plain_objective(oracle_mod, cl, state, n, w, ss, {k: -h * v for k, v in sd.items()})) / (2 * h)
+    assert tan == pytest.approx(fd, rel=2e-6)
