@@ -473,10 +473,11 @@ def dd_form(args, stream_of, local, world, rank):
 def adjoint_form(args, stream_of, local):
     """Adjoint over forward cost on the turbulent cloud (128 x 128 x 48, lognormal n_H, dust,
     v_max = 50 km/s): N forward steps from the graph-replayed step against lyd_adjoint_run of
-    the same N steps. Two storage modes: automatic (every step's state and advection tape kept
-    from the forward sweep when they fit in device memory, so nothing is recomputed), and a
-    checkpoint every 100 steps with one recomputation of each segment. Each mode is timed on its
-    second call, after the call that allocates the workspace."""
+    the same N steps. Three storage modes: automatic (every step's state and advection tape kept
+    from the forward sweep when they fit in device memory, so nothing is recomputed), a
+    checkpoint every 100 steps with one recomputation of each segment, and the binomial
+    (Revolve) schedule with 62 state snapshots. Each mode is timed on its second call, after the
+    call that allocates the workspace."""
     from lydion_b200 import adjoint as A
     from lydion_b200 import workloads as W
     from lydion_b200.m1 import context_for_cloud
@@ -492,9 +493,10 @@ def adjoint_form(args, stream_of, local):
     w_MF, w_bins = A.objective_weights(cl.freq, 1.0, w64)
     out = {"workload": "c4_turbulent_128x128x48", "steps": n, "forward_ms": fwd}
     names = ("forward_sweep", "recompute_with_tapes", "frequency_adjoint", "advection_adjoint")
-    for every, label in ((0, "auto"), (100, "every_100")):
+    for every, label in ((0, "auto"), (100, "every_100"), (-1, "binomial")):
         # one untimed call first: the workspace (grow-only, kept by the context between calls;
-        # about 126 GB when every step is kept) is allocated by the first call that needs it
+        # about 126 GB when every step is kept) is allocated by the first call that needs it.
+        # binomial: 61 snapshots besides the initial state, no step advanced more than twice
         ctx.adjoint(n, *p, w_MF=w_MF, w_spec=1e12 * w_bins, checkpoint_every=every, want=("grad_alpha",))
         ctx.synchronize()
         adj = _timed(ctx, lambda k: ctx.adjoint(k, *p, w_MF=w_MF, w_spec=1e12 * w_bins, checkpoint_every=every,

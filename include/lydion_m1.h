@@ -264,7 +264,10 @@ int  lyd_get_tuning(lyd_ctx *ctx, lyd_tuning *t);
  * (7 doubles per cell-bin per step), the forward sweep keeps every step's state and advection
  * tape, plus its frequency factors when 10 doubles per cell-bin per step fit, and nothing is
  * recomputed; with checkpoint_every = K > 1 (0 otherwise: 100)
- * it stores the state every K steps and the reverse sweep recomputes each segment once. The
+ * it stores the state every K steps and the reverse sweep recomputes each segment once; with
+ * checkpoint_every < 0 it keeps `snapshots` + 1 states in Griewank's binomial (Revolve)
+ * schedule, advancing no step more than r times, r the least with C(snapshots + 1 + r, r) >=
+ * n_steps, and records each step's tape right before its reverse. The
  * reverse sweep runs hand-written adjoint kernels of the step (advection, emission/absorption,
  * frequency factors, transposed tridiagonal solve, flux correction). The active window of every step is the forward's.
  * Non-smooth points (MinMod, floors, clamps, limiters) take the derivative of the branch the
@@ -276,8 +279,11 @@ int  lyd_get_tuning(lyd_ctx *ctx, lyd_tuning *t);
  * parametrisation (alpha = x_HI n_H sigma0(T)). No counterpart exists in the reference. */
 typedef struct lyd_adjoint_cfg {
     lyd_step_params step;        /* c_tilde, dt, z_center, boundaries, n_steps */
-    int32_t checkpoint_every;
-    int32_t reserved;
+    int32_t checkpoint_every;    /* 1: keep every step; K > 1: a checkpoint every K steps; 0:
+                                    every step when it fits, else K = 100; < 0: the binomial
+                                    schedule with `snapshots` state snapshots */
+    int32_t snapshots;           /* binomial schedule: snapshots besides the initial state (0:
+                                    the fewest with which no step is advanced more than twice) */
     double w_MF;
     const double *w_spec;        /* n_nu weights, or NULL */
 } lyd_adjoint_cfg;

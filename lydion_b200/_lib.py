@@ -78,7 +78,7 @@ SOLVER_PCR, SOLVER_THOMAS = 0, 1
 
 
 class AdjointCfg(C.Structure):
-    _fields_ = [("step", StepParams), ("checkpoint_every", C.c_int32), ("reserved", C.c_int32), ("w_MF", C.c_double),
+    _fields_ = [("step", StepParams), ("checkpoint_every", C.c_int32), ("snapshots", C.c_int32), ("w_MF", C.c_double),
                 ("w_spec", P)]
 
 

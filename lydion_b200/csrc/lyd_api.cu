@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <functional>
 #include <cstring>
 #include <string>
 #include <type_traits>
@@ -1544,6 +1545,15 @@ int lyd_voigt_tables(double *out, int32_t n, double xmax) {
 // segments backwards, recomputes a segment's states from its checkpoint, then runs the
 // adjoint steps of that segment from its last step to its first.
 
+// C(s + r, s): the most steps s snapshots reverse with no step advanced more than r times
+// (Griewank, "Achieving logarithmic growth of temporal and spatial complexity in reverse
+// automatic differentiation", 1992), as a double (exact far beyond the step counts used here).
+static double binomial_reach(int s, int r) {
+    double b = 1.0;
+    for (int q = 1; q <= s; q++) b = b * (double)(r + q) / (double)q;
+    return b;
+}
+
 int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out) {
     if (!c || !cfg || !out) return LYD_ERR_ARG;
     cudaSetDevice(c->dev);
@@ -1564,13 +1574,25 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) { cudaGetLastError(); fr = 0; }
     const size_t avail = fr + c->adj_ws_bytes, margin = 16 * S * 8 + ((size_t)2 << 30);
+    // checkpoint_every < 0: the binomial schedule with `snapshots` state snapshots (0: the fewest
+    // for which no step is advanced more than twice in the reverse sweep)
+    const bool binom = cfg->checkpoint_every < 0;
     bool store_all = cfg->checkpoint_every == 1;
     if (cfg->checkpoint_every == 0) store_all = (size_t)N * (S + 4 * n3) * 8 + margin <= avail;
     const bool keep_ff = store_all && (size_t)N * (S + 7 * n3) * 8 + margin <= avail;
-    const int K = store_all ? 1
-                            : (cfg->checkpoint_every > 0 ? (cfg->checkpoint_every < N ? cfg->checkpoint_every : N)
-                                                         : (N < 100 ? N : 100));
-    const int nseg = (N + K - 1) / K;
+    int snaps = 0;
+    if (binom) {
+        if (cfg->snapshots < 0) return fail(c, LYD_ERR_ARG, "snapshots must be >= 0");
+        snaps = cfg->snapshots > 0 ? cfg->snapshots : 1;
+        if (cfg->snapshots == 0)
+            while (binomial_reach(snaps + 1, 2) < (double)N) snaps++;
+        if (snaps > N) snaps = N;
+    }
+    const int K = binom ? 1
+                        : store_all ? 1
+                                    : (cfg->checkpoint_every > 0 ? (cfg->checkpoint_every < N ? cfg->checkpoint_every : N)
+                                                                 : (N < 100 ? N : 100));
+    const int nseg = binom ? snaps + 1 : (N + K - 1) / K;
     const int nr = c->nr[0], nz = c->nz[0], nnu = c->nnu;
     params_all(c, p->c_tilde, p->dt, p->c_tilde * p->dt);
     for (CloudDesc &d : c->desc) d.z_center = p->z_center;
@@ -1666,7 +1688,7 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
         }
     } else {
         for (int n = 0; n < N; n++) {
-            if (n % K == 0) LYD_TRY(copy_state(ck + (size_t)(n / K) * S, c->cur));
+            if (binom ? n == 0 : n % K == 0) LYD_TRY(copy_state(ck + (size_t)(n / K) * S, c->cur));
             LYD_TRY(enqueue_step<double>(c, false, nullptr, nullptr, nullptr, nullptr, true,
                                          n + 1 < N ? win + 2 * (n + 1) : nullptr));
         }
@@ -1707,104 +1729,164 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
         launch_seed_spectrum(lam, wsp, nnu, nr, nz, c->st);
     }
     const int B = 1 - c->cur;
-    for (int g = nseg - 1; g >= 0; g--) {
-        const int n0 = g * K, n1 = (n0 + K < N) ? n0 + K : N;
-        if (!store_all) {
-            tick(0);
-            LYD_TRY(load_state(ck + (size_t)g * S, c->cur));
-        }
-        // recompute the segment: advection of s_n in the step's window into x_A with its tape,
-        // then (except after the last step) emission + frequency step x_A -> s_{n+1}
-        for (int n = n0; n < n1 && !store_all; n++) {
-            double *sn = seg + (size_t)(n - n0) * S, *xA = segA;
+    // One step forward from the state in the context's current set (or from `sn`, which then
+    // receives a copy of it), in the forward sweep's window of step n: the advection into x_A,
+    // with its tape when `tape` is given, then (with `freq`) emission + frequency step x_A -> the
+    // current set.
+    auto forward_step = [&](int n, double *sn, double *tape, bool freq) -> int {
+        double *xA = segA;
+        AdvArgs<double> aa;
+        fill_adv<double>(c, aa, c->cur, B);
+        if (sn) {
             LYD_TRY(copy_state(sn, c->cur));
-            AdvArgs<double> aa;
-            fill_adv<double>(c, aa, c->cur, B);
             aa.J = sn; aa.Hr = sn + n3; aa.HZ = sn + 2 * n3;
             aa.tmaps = nullptr;     // the maps cover the context's buffer sets, not the workspace
-            aa.Jo = xA; aa.Hro = xA + n3; aa.HZo = xA + 2 * n3;
-            aa.kwin = win + 2 * n;
-            aa.tape = segT + (size_t)(n - n0) * 4 * n3;
-            aa.tape_stride = (long long)n3;
-            launch_advect(LYD_PREC_FP64, c->cfg.flux_method, &aa, c->ntiles, 2, c->st);
-            if (n + 1 < n1) {
-                FreqArgs<double> fq;
-                fill_freq<double>(c, fq, xA, xA + n3, xA + 2 * n3, xA, c->set[c->cur][0], c->set[c->cur][1],
-                                  c->set[c->cur][2]);
-                fq.do_emission = 1; fq.do_freq = 1; fq.update_ff = 1;
-                fq.parts = 0;
-                launch_freq(LYD_PREC_FP64, &fq, nnu, c->nitems, c->st);
-            }
-            LYD_CU(c, cudaGetLastError());
         }
-        if (!store_all) {
+        aa.Jo = xA; aa.Hro = xA + n3; aa.HZo = xA + 2 * n3;
+        aa.kwin = win + 2 * n;
+        aa.tape = tape;
+        aa.tape_stride = (long long)n3;
+        launch_advect(LYD_PREC_FP64, c->cfg.flux_method, &aa, c->ntiles, 2, c->st);
+        if (freq) {
+            FreqArgs<double> fq;
+            fill_freq<double>(c, fq, xA, xA + n3, xA + 2 * n3, xA, c->set[c->cur][0], c->set[c->cur][1],
+                              c->set[c->cur][2]);
+            fq.do_emission = 1; fq.do_freq = 1; fq.update_ff = 1;
+            fq.parts = 0;
+            launch_freq(LYD_PREC_FP64, &fq, nnu, c->nitems, c->st);
+        }
+        LYD_CU(c, cudaGetLastError());
+        return LYD_OK;
+    };
+    // The adjoint of step n from its input state sn and advection tape: lambda_{n+1} -> lambda_n.
+    auto reverse_step = [&](int n, const double *sn, const double *tape) -> int {
+        tick(2);
+        tick(3);
+        // frequency step adjoint: lambda_{n+1} -> lambda of x_A
+        FreqAdjArgs fa;
+        memset(&fa, 0, sizeof(fa));
+        fa.J = sn; fa.Hr = sn + n3; fa.HZ = sn + 2 * n3;
+        fa.tape = tape; fa.tape_stride = (long long)n3;
+        fa.kmin = hwin[2 * n]; fa.kmax = hwin[2 * n + 1];
+        if (ffs) {
+            fa.Fkp = ffs + (size_t)n * 3 * n3;
+            fa.Fk = fa.Fkp + n3;
+            fa.Fkm = fa.Fkp + 2 * n3;
+        }
+        fa.Hv = (const double *)c->Hv;
+        fa.phi = c->phi ? (const double *)c->phi : nullptr;
+        fa.phi_inv = c->phi_inv; fa.phi_kmin = c->phi_kmin; fa.phi_kmax = c->phi_kmax;
+        fa.alpha = c->cellf[CF_ALPHA]; fa.alpha_c = c->cellf[CF_ALPHA_C];
+        fa.alpha_cF = any_have(c, 1u << CF_ALPHA_CF) ? c->cellf[CF_ALPHA_CF] : nullptr;
+        fa.pd = c->cellf[CF_PD]; fa.js = c->cellf[CF_JS]; fa.T = c->cellf[CF_T];
+        fa.dur_dr = c->cellf[CF_DUR_DR]; fa.dur_dZ = c->cellf[CF_DUR_DZ]; fa.duZ_dr = c->cellf[CF_DUZ_DR];
+        fa.duZ_dZ = c->cellf[CF_DUZ_DZ]; fa.ur_over_r = c->cellf[CF_UR_OVER_R];
+        fa.nu = c->nu; fa.nuC = c->nuC; fa.dnu = c->dnu; fa.inv_dnu = c->inv_dnu; fa.inv_nuC = c->inv_nuC;
+        fa.dV = c->dV; fa.cl = c->cl; fa.items = c->items;
+        fa.alpha_floor = c->cfg.alpha_floor; fa.jeps = c->jeps_s; fa.heps2 = c->heps2_s; fa.j_scale = c->jscale;
+        fa.recoil = c->cfg.recoil; fa.nnu = nnu; fa.ncell = (long long)nc;
+        fa.gJ = lam; fa.gHr = lam + n3; fa.gHZ = lam + 2 * n3;
+        fa.oJ = lamA; fa.oHr = lamA + n3; fa.oHZ = lamA + 2 * n3;
+        fa.g_alpha = g_alpha; fa.g_alpha_c = g_alpha_c; fa.g_T = g_T; fa.g_u = g_u; fa.g_Hv = gHv;
+        fa.mf_seed = (n == N - 1) && mf_w != 0.0;
+        fa.mf_w = mf_w;
+        launch_freq_adj(fa, c->nitems, c->st);
+        tick(4);
+        // advection adjoint: lambda of x_A -> lambda_n
+        AdjAdvArgs ad;
+        memset(&ad, 0, sizeof(ad));
+        ad.J = sn; ad.Hr = sn + n3; ad.HZ = sn + 2 * n3;
+        ad.tape = tape; ad.n3 = (long long)n3;
+        ad.gJ = lamA; ad.gHr = lamA + n3; ad.gHZ = lamA + 2 * n3;
+        ad.lJ = lamN; ad.lHr = lamN + n3; ad.lHZ = lamN + 2 * n3;
+        ad.pJ = pre; ad.pHr = pre + n3; ad.pHZ = pre + 2 * n3;
+        ad.Hv = (const double *)c->Hv; ad.alpha = c->cellf[CF_ALPHA]; ad.alpha_cF = fa.alpha_cF;
+        ad.A_r = c->A_r; ad.A_Z = c->A_Z; ad.inv_dV = c->inv_dV; ad.inv_r_cell = c->inv_r_cell;
+        ad.rint = c->rint; ad.zint = c->zint; ad.u_r_star = c->u_r_star; ad.u_Z_star = c->u_Z_star;
+        ad.dur_dr = fa.dur_dr; ad.dur_dZ = fa.dur_dZ; ad.duZ_dr = fa.duZ_dr; ad.duZ_dZ = fa.duZ_dZ;
+        ad.ur_over_r = fa.ur_over_r;
+        ad.g_aF = gaF; ad.g_u = g_u; ad.g_ur = g_ur; ad.g_uZ = g_uZ;
+        ad.nnu = nnu; ad.nr = nr; ad.nz = nz; ad.kmin = hwin[2 * n]; ad.kmax = hwin[2 * n + 1];
+        ad.bc_r_left = c->cfg.bc_r_left;
+        ad.bc_r_right = p->bc_r_right; ad.bc_z_bot = p->bc_z_bot; ad.bc_z_top = p->bc_z_top;
+        ad.ctdt = p->c_tilde * p->dt; ad.jeps = c->jeps_s; ad.heps2 = c->heps2_s;
+        ad.flux = c->cfg.flux_method == LYD_FLUX_HLL ? 1 : 0;
+        launch_adv_adj(ad, c->st);
+        tick(5);
+        tock(2, 3, 2);
+        tock(3, 4, 3);
+        tock(4, 5, 4);
+        LYD_CU(c, cudaGetLastError());
+        double *t = lam;
+        lam = lamN;
+        lamN = t;
+        return LYD_OK;
+    };
+    if (!binom) {
+        for (int g = nseg - 1; g >= 0; g--) {
+            const int n0 = g * K, n1 = (n0 + K < N) ? n0 + K : N;
+            if (!store_all) {
+                tick(0);
+                LYD_TRY(load_state(ck + (size_t)g * S, c->cur));
+                // recompute the segment, recording every step's input state and advection tape
+                for (int n = n0; n < n1; n++)
+                    LYD_TRY(forward_step(n, seg + (size_t)(n - n0) * S, segT + (size_t)(n - n0) * 4 * n3, n + 1 < n1));
+                tick(1);
+                tock(0, 1, 1);
+            }
+            for (int n = n1 - 1; n >= n0; n--) {
+                const double *sn = store_all ? ck + (size_t)n * S : seg + (size_t)(n - n0) * S;
+                const double *tape = segT + (size_t)(store_all ? n : n - n0) * 4 * n3;
+                LYD_TRY(reverse_step(n, sn, tape));
+            }
+        }
+    } else {
+        // Binomial checkpointing (Griewank's Revolve schedule): reverse steps [i0, i1) with the
+        // state s_i0 in snapshot `slot` and `nfree` more snapshots, s = nfree + 1 in all. With r
+        // the least repetition number for which C(s + r, s) >= i1 - i0, the next snapshot goes
+        // t steps ahead, t the least with i1 - i0 - t <= C(s - 1 + r, s - 1): the steps right
+        // of it are reversed with one snapshot fewer and up to r advances, those left of it
+        // (advanced once to place it) with the same snapshots and r - 1, so no step is advanced
+        // more than r times. Each step is recorded (its input state and tape) right before its
+        // reverse.
+        auto advance = [&](int slot, int i0, int n_to) -> int {
+            tick(0);
+            LYD_TRY(load_state(ck + (size_t)slot * S, c->cur));
+            for (int n = i0; n < n_to; n++) LYD_TRY(forward_step(n, nullptr, nullptr, true));
             tick(1);
             tock(0, 1, 1);
-        }
-        for (int n = n1 - 1; n >= n0; n--) {
-            const double *sn = store_all ? ck + (size_t)n * S : seg + (size_t)(n - n0) * S;
-            const double *tape = segT + (size_t)(store_all ? n : n - n0) * 4 * n3;
-            tick(2);
-            tick(3);
-            // frequency step adjoint: lambda_{n+1} -> lambda of x_A
-            FreqAdjArgs fa;
-            memset(&fa, 0, sizeof(fa));
-            fa.J = sn; fa.Hr = sn + n3; fa.HZ = sn + 2 * n3;
-            fa.tape = tape; fa.tape_stride = (long long)n3;
-            fa.kmin = hwin[2 * n]; fa.kmax = hwin[2 * n + 1];
-            if (ffs) {
-                fa.Fkp = ffs + (size_t)n * 3 * n3;
-                fa.Fk = fa.Fkp + n3;
-                fa.Fkm = fa.Fkp + 2 * n3;
+            return LYD_OK;
+        };
+        auto record_and_reverse = [&](int n) -> int {
+            tick(0);
+            LYD_TRY(forward_step(n, seg, segT, false));
+            tick(1);
+            tock(0, 1, 1);
+            return reverse_step(n, seg, segT);
+        };
+        std::function<int(int, int, int, int)> rev = [&](int i0, int i1, int slot, int nfree) -> int {
+            const int l = i1 - i0;
+            if (l == 1) {
+                LYD_TRY(advance(slot, i0, i0));
+                return record_and_reverse(i0);
             }
-            fa.Hv = (const double *)c->Hv;
-            fa.phi = c->phi ? (const double *)c->phi : nullptr;
-            fa.phi_inv = c->phi_inv; fa.phi_kmin = c->phi_kmin; fa.phi_kmax = c->phi_kmax;
-            fa.alpha = c->cellf[CF_ALPHA]; fa.alpha_c = c->cellf[CF_ALPHA_C];
-            fa.alpha_cF = any_have(c, 1u << CF_ALPHA_CF) ? c->cellf[CF_ALPHA_CF] : nullptr;
-            fa.pd = c->cellf[CF_PD]; fa.js = c->cellf[CF_JS]; fa.T = c->cellf[CF_T];
-            fa.dur_dr = c->cellf[CF_DUR_DR]; fa.dur_dZ = c->cellf[CF_DUR_DZ]; fa.duZ_dr = c->cellf[CF_DUZ_DR];
-            fa.duZ_dZ = c->cellf[CF_DUZ_DZ]; fa.ur_over_r = c->cellf[CF_UR_OVER_R];
-            fa.nu = c->nu; fa.nuC = c->nuC; fa.dnu = c->dnu; fa.inv_dnu = c->inv_dnu; fa.inv_nuC = c->inv_nuC;
-            fa.dV = c->dV; fa.cl = c->cl; fa.items = c->items;
-            fa.alpha_floor = c->cfg.alpha_floor; fa.jeps = c->jeps_s; fa.heps2 = c->heps2_s; fa.j_scale = c->jscale;
-            fa.recoil = c->cfg.recoil; fa.nnu = nnu; fa.ncell = (long long)nc;
-            fa.gJ = lam; fa.gHr = lam + n3; fa.gHZ = lam + 2 * n3;
-            fa.oJ = lamA; fa.oHr = lamA + n3; fa.oHZ = lamA + 2 * n3;
-            fa.g_alpha = g_alpha; fa.g_alpha_c = g_alpha_c; fa.g_T = g_T; fa.g_u = g_u; fa.g_Hv = gHv;
-            fa.mf_seed = (n == N - 1) && mf_w != 0.0;
-            fa.mf_w = mf_w;
-            launch_freq_adj(fa, c->nitems, c->st);
-            tick(4);
-            // advection adjoint: lambda of x_A -> lambda_n
-            AdjAdvArgs ad;
-            memset(&ad, 0, sizeof(ad));
-            ad.J = sn; ad.Hr = sn + n3; ad.HZ = sn + 2 * n3;
-            ad.tape = tape; ad.n3 = (long long)n3;
-            ad.gJ = lamA; ad.gHr = lamA + n3; ad.gHZ = lamA + 2 * n3;
-            ad.lJ = lamN; ad.lHr = lamN + n3; ad.lHZ = lamN + 2 * n3;
-            ad.pJ = pre; ad.pHr = pre + n3; ad.pHZ = pre + 2 * n3;
-            ad.Hv = (const double *)c->Hv; ad.alpha = c->cellf[CF_ALPHA]; ad.alpha_cF = fa.alpha_cF;
-            ad.A_r = c->A_r; ad.A_Z = c->A_Z; ad.inv_dV = c->inv_dV; ad.inv_r_cell = c->inv_r_cell;
-            ad.rint = c->rint; ad.zint = c->zint; ad.u_r_star = c->u_r_star; ad.u_Z_star = c->u_Z_star;
-            ad.dur_dr = fa.dur_dr; ad.dur_dZ = fa.dur_dZ; ad.duZ_dr = fa.duZ_dr; ad.duZ_dZ = fa.duZ_dZ;
-            ad.ur_over_r = fa.ur_over_r;
-            ad.g_aF = gaF; ad.g_u = g_u; ad.g_ur = g_ur; ad.g_uZ = g_uZ;
-            ad.nnu = nnu; ad.nr = nr; ad.nz = nz; ad.kmin = hwin[2 * n]; ad.kmax = hwin[2 * n + 1];
-            ad.bc_r_left = c->cfg.bc_r_left;
-            ad.bc_r_right = p->bc_r_right; ad.bc_z_bot = p->bc_z_bot; ad.bc_z_top = p->bc_z_top;
-            ad.ctdt = p->c_tilde * p->dt; ad.jeps = c->jeps_s; ad.heps2 = c->heps2_s;
-            ad.flux = c->cfg.flux_method == LYD_FLUX_HLL ? 1 : 0;
-            launch_adv_adj(ad, c->st);
-            tick(5);
-            tock(2, 3, 2);
-            tock(3, 4, 3);
-            tock(4, 5, 4);
-            LYD_CU(c, cudaGetLastError());
-            double *t = lam;
-            lam = lamN;
-            lamN = t;
-        }
+            if (nfree == 0) {
+                for (int n = i1 - 1; n >= i0; n--) {
+                    LYD_TRY(advance(slot, i0, n));
+                    LYD_TRY(record_and_reverse(n));
+                }
+                return LYD_OK;
+            }
+            int r = 1;
+            while (binomial_reach(nfree + 1, r) < (double)l) r++;
+            int t = l - (int)std::min((double)(l - 1), binomial_reach(nfree, r));
+            if (t < 1) t = 1;
+            LYD_TRY(advance(slot, i0, i0 + t));
+            LYD_TRY(copy_state(ck + (size_t)(slot + 1) * S, c->cur));
+            LYD_TRY(rev(i0 + t, i1, slot + 1, nfree - 1));
+            return rev(i0, i0 + t, slot, nfree);
+        };
+        LYD_TRY(rev(0, N, 0, snaps));
     }
     // alpha_F = alpha H_voigt ; H_voigt(T) when it was computed on the device
     launch_af_params(gaF, c->cellf[CF_ALPHA], (const double *)c->Hv, nnu, (long long)nc, g_alpha, gHv, c->st);

@@ -119,6 +119,25 @@ __device__ __forceinline__ R alpha_F(const AdvArgs<S> &a, const View &v, int i, 
     return val;
 }
 
+// Asynchronous global -> shared copy of one 4- or 8-byte element (cp.async, L1-allocating).
+template <typename T>
+__device__ __forceinline__ void cp_async_el(T *dst, const T *src) {
+    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "element size");
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    if constexpr (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(src) : "memory");
+}
+// Asynchronous global -> shared copy of 16 bytes (cp.async.cg: L2 only, the rows are streamed).
+__device__ __forceinline__ void cp_async_16(void *dst, const void *src) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // ---- bulk tensor copies (TMA) into shared memory, completed on an mbarrier -------------------
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
@@ -165,11 +184,10 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const void *map, int x, i
 // ---- k_advect: one CTA = 8 columns (r) x `rows` rows (Z) x 32 bins, marching up in Z --------
 //
 // A ring of four rows holds, for the 8 own columns and the 2 + 2 halo columns of each row, the
-// cell values every face needs: J and the reduced fluxes H/max(J, Jeps) (so the reciprocal of
-// J is taken once per cell, not once per face), plus the state of the own columns for the
-// cell update. With FP32 arithmetic the ring also holds alpha_F; with FP64 arithmetic alpha_F of
-// the two cells beside a face is formed at the face from alpha and H_voigt (L1-resident loads)
-// instead, which keeps the FP64 tile (65 KB) within three CTAs per SM. Warp w (0..7) owns
+// cell values every face needs: J, the reduced fluxes H/max(J, Jeps) (so the reciprocal of J is
+// taken once per cell, not once per face) and alpha_F (formed once per cell, not at each of the
+// four face sides that read it); a ring of three rows holds the state of the own columns for
+// the cell update. The FP64 tile (74 KB) runs at three CTAs per SM. Warp w (0..7) owns
 // column i0+w; warp 8 stages the halo columns and computes the tile's rightmost r face. Per row: stage row j+2 -> sync -> every warp
 // computes the r face on its left (warp 8: the right edge) into shared memory and its Z face
 // j+1/2 into registers -> sync -> the cell update of row j uses the two r faces from shared
@@ -179,8 +197,13 @@ constexpr int MWARPS = MT + 1;
 constexpr int MTHREADS = 32 * MWARPS;
 constexpr int MCOL = MT + 4;           // staged columns i0-2 .. i0+MT+1
 constexpr int RING = 4;
-// staged fields per cell: J, f_r, f_Z (+ alpha_F with FP32 arithmetic)
-template <typename R> __host__ __device__ constexpr int nf() { return sizeof(R) == 4 ? 4 : 3; }
+// staged fields per cell: J, f_r, f_Z and alpha_F (formed once per staged cell; four face sides
+// read each cell's)
+template <typename R> __host__ __device__ constexpr int nf() { return 4; }
+// The own columns' state (J, H_r, H_Z in the storage type) is kept for the rows j .. j+2 only
+// (staged at j+2, updated at j): a ring of three slots.
+constexpr int HRING = 3;
+__host__ __device__ constexpr int hslot(int r) { return ((r % HRING) + HRING) % HRING; }
 
 template <typename S, typename R>
 __device__ __forceinline__ Cell<R> raw_cell(const AdvArgs<S> &a, const View &v, int col, int row, int k) {
@@ -210,7 +233,7 @@ __device__ __forceinline__ void stage_cell(const AdvArgs<S> &a, const View &v, R
     if (lc >= 2 && lc < 2 + MT) {
         // the state in S; with S == R the ring's J is the state's J
         constexpr int HF = sizeof(S) == sizeof(R) ? 2 : 3;
-        S *q = Hh + ((slot * MT + (lc - 2)) * HF) * 32 + lane;
+        S *q = Hh + ((hslot(row) * MT + (lc - 2)) * HF) * 32 + lane;
         q[0] = c.Hr; q[32] = c.HZ;
         if (HF == 3) q[64] = c.J;
     }
@@ -261,7 +284,7 @@ __device__ __forceinline__ void stage_from_raw(const AdvArgs<S> &a, const View &
     if (nf<R>() == 4) p[96] = aF;
     if (lc >= 2 && lc < 2 + MT) {
         constexpr int HF = sizeof(S) == sizeof(R) ? 2 : 3;
-        S *q = Hh + ((slot * MT + (lc - 2)) * HF) * 32 + lane;
+        S *q = Hh + ((hslot(row) * MT + (lc - 2)) * HF) * 32 + lane;
         q[0] = c.Hr; q[32] = c.HZ;
         if (HF == 3) q[64] = c.J;
     }
@@ -284,22 +307,17 @@ __device__ __forceinline__ CellF<R> staged(const R *A, int slot, int lc, int lan
 // staged column of the stencil's first cell (src/AdvectJandH.jl:641-968).
 template <typename S, typename R, int FLUX>
 __device__ __forceinline__ void face_r_staged(const AdvArgs<S> &a, const View &v, const R *A, int slot, int wl,
-                                              int f, int j, int k, int lane, R jeps, const double *up, R *F,
-                                              R &kL, R &kR) {
-    double us = 0.0;
-    if constexpr (sizeof(R) == 4) us = *up;
+                                              int f, int j, int k, int lane, R jeps, const double *up,
+                                              const double *riv, R *F, R &kL, R &kR) {
+    const double us = *up;
     R d0, aFi, aFp, d3;
     CellF<R> cm1 = staged<R>(A, slot, wl, lane, d0);
     CellF<R> ci = staged<R>(A, slot, wl + 1, lane, aFi);
     CellF<R> cp1 = staged<R>(A, slot, wl + 2, lane, aFp);
     CellF<R> cp2 = staged<R>(A, slot, wl + 3, lane, d3);
-    if (nf<R>() == 3) {   // FP64 arithmetic: alpha_F formed here from alpha and H_voigt
-        aFi = alpha_F<S, R>(a, v, f - 1 < 0 ? 0 : (f - 1 >= v.nr ? v.nr - 1 : f - 1), j, k);
-        aFp = alpha_F<S, R>(a, v, f >= v.nr ? v.nr - 1 : f, j, k);
-    }
     R iv[5];
 #pragma unroll
-    for (int t = 0; t < 5; t++) iv[t] = R(__ldg(a.rint + v.orint + 5 * f + t));
+    for (int t = 0; t < 5; t++) iv[t] = R(riv[t]);
     Recon<R> q = reconstruct_f<R>(cm1, ci, cp1, cp2, iv, aFi, aFp, jeps);
     R DrrL, DZZL, DrZL, DrrR, DZZR, DrZR;
     D_from_f_n<R>(q.f_L, q.nr_L, q.nZ_L, DrrL, DZZL, DrZL);
@@ -307,7 +325,6 @@ __device__ __forceinline__ void face_r_staged(const AdvArgs<S> &a, const View &v
     R FJ, FHr, FHZ;
     m1_flux<R, FLUX, false>(q.Hr_L, q.Hr_R, DrrL * q.J_L, DrrR * q.J_R, DrZL * q.J_L, DrZR * q.J_R, q, ci.J, cp1.J,
                             FJ, FHr, FHZ);
-    if constexpr (sizeof(R) != 4) us = __ldg(a.u_r_star + v.orf + f + (long long)(v.nr + 1) * j);
     R uc = R(us * kInvC);
     F[0] = FJ + adv_flux(uc, q.J_L, q.J_R);
     F[1] = FHr + adv_flux(uc, q.Hr_L, q.Hr_R);
@@ -320,23 +337,15 @@ __device__ __forceinline__ void face_r_staged(const AdvArgs<S> &a, const View &v
 template <typename S, typename R, int FLUX>
 __device__ __forceinline__ void face_z_staged(const AdvArgs<S> &a, const View &v, const R *A, int lc, int i, int f,
                                               int k, int lane, R jeps, const double *ivz, const double *up, R *F) {
-    double us = 0.0;
-    if constexpr (sizeof(R) == 4) us = *up;
+    const double us = *up;
     R d0, aFi, aFp, d3;
     CellF<R> cm1 = staged<R>(A, (f + 2) & (RING - 1), lc, lane, d0);     // row f-2
     CellF<R> ci = staged<R>(A, (f + 3) & (RING - 1), lc, lane, aFi);     // row f-1
     CellF<R> cp1 = staged<R>(A, f & (RING - 1), lc, lane, aFp);          // row f
     CellF<R> cp2 = staged<R>(A, (f + 1) & (RING - 1), lc, lane, d3);     // row f+1
-    if (nf<R>() == 3) {
-        aFi = alpha_F<S, R>(a, v, i, f - 1 < 0 ? 0 : (f - 1 >= v.nz ? v.nz - 1 : f - 1), k);
-        aFp = alpha_F<S, R>(a, v, i, f >= v.nz ? v.nz - 1 : f, k);
-    }
     R iv[5];
 #pragma unroll
-    for (int t = 0; t < 5; t++) {
-        if constexpr (sizeof(R) == 4) iv[t] = R(ivz[t]);
-        else iv[t] = R(__ldg(a.zint + v.ozint + 5 * f + t));
-    }
+    for (int t = 0; t < 5; t++) iv[t] = R(ivz[t]);
     Recon<R> q = reconstruct_f<R>(cm1, ci, cp1, cp2, iv, aFi, aFp, jeps);
     R DrrL, DZZL, DrZL, DrrR, DZZR, DrZR;
     D_from_f_n<R>(q.f_L, q.nr_L, q.nZ_L, DrrL, DZZL, DrZL);
@@ -344,7 +353,6 @@ __device__ __forceinline__ void face_z_staged(const AdvArgs<S> &a, const View &v
     R FJ, FHr, FHZ;
     m1_flux<R, FLUX, true>(q.HZ_L, q.HZ_R, DrZL * q.J_L, DrZR * q.J_R, DZZL * q.J_L, DZZR * q.J_R, q, ci.J, cp1.J,
                            FJ, FHr, FHZ);
-    if constexpr (sizeof(R) != 4) us = __ldg(a.u_Z_star + v.ozf + i + (long long)v.nr * f);
     R uc = R(us * kInvC);
     F[0] = FJ + adv_flux(uc, q.J_L, q.J_R);
     F[1] = FHr + adv_flux(uc, q.Hr_L, q.Hr_R);
@@ -353,11 +361,10 @@ __device__ __forceinline__ void face_z_staged(const AdvArgs<S> &a, const View &v
 
 // The per-row scalars a warp needs: the cell's geometry and velocity gradients (0..10), u*_r of
 // the warp's r face (11), u*_Z of its Z face above the row (12), that face's PLM intervals
-// (13..17). With FP32 arithmetic they are fetched one per lane a row ahead of their use and
-// parked in shared memory, so their loads overlap a whole row's work instead of stalling the
-// faces and the cell update (mixed advection 0.233 -> 0.226 ms at 256^2 x 64). The FP64 tile
-// loads them where they are used: it runs at its register limit, and the registers that carry
-// the next row's scalar and its address across the row spill there (0.330 -> 0.335 ms).
+// (13..17). They are copied one per lane a row ahead of their use (cp.async into the other half
+// of a per-warp double buffer in shared memory, so no register carries them across the row),
+// and their loads overlap a whole row's work instead of stalling the faces and the cell update.
+// The r faces' PLM intervals depend on the column only: the tile stages its MT + 1 faces' once.
 constexpr int GEO_N = 18;
 enum { G_ARL, G_ARR, G_AZL, G_AZR, G_IDV, G_DURDR, G_DURDZ, G_DUZDR, G_DUZDZ, G_UROR, G_IRC, G_UR, G_UZ, G_ZIV };
 
@@ -403,8 +410,8 @@ __device__ __forceinline__ double geo_fetch(const double *src, int stride, int j
 template <typename S, typename R>
 __host__ __device__ constexpr size_t adv_smem_base() {
     return sizeof(R) * 32 * (RING * MCOL * nf<R>() + (MT + 1) * 5) +
-           sizeof(S) * 32 * RING * MT * (sizeof(S) == sizeof(R) ? 2 : 3) +
-           (sizeof(R) == 4 ? sizeof(double) * MWARPS * GEO_N : 0);   // the row slots (FP32 arithmetic)
+           sizeof(S) * 32 * HRING * MT * (sizeof(S) == sizeof(R) ? 2 : 3) +
+           sizeof(double) * (MWARPS * 2 * GEO_N + (MT + 1) * 5);   // the row slots, the r faces' intervals
 }
 __host__ __device__ constexpr size_t adv_tma_off(size_t base) { return (base + 127) / 128 * 128; }
 
@@ -418,9 +425,10 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
     constexpr int HF = sizeof(S) == sizeof(R) ? 2 : 3;
     constexpr int NF = nf<R>();
     R *A = reinterpret_cast<R *>(adv_smem);                            // [RING][MCOL][NF][32]
-    S *Hh = reinterpret_cast<S *>(A + RING * MCOL * NF * 32);           // [RING][MT][HF][32]
-    R *Fr = reinterpret_cast<R *>(Hh + RING * MT * HF * 32);            // [MT+1][5][32]
-    double *geo = reinterpret_cast<double *>(Fr + (MT + 1) * 5 * 32);  // [MWARPS][GEO_N], FP32 arithmetic only
+    S *Hh = reinterpret_cast<S *>(A + RING * MCOL * NF * 32);           // [HRING][MT][HF][32]
+    R *Fr = reinterpret_cast<R *>(Hh + HRING * MT * HF * 32);           // [MT+1][5][32]
+    double *geo = reinterpret_cast<double *>(Fr + (MT + 1) * 5 * 32);  // [MWARPS][2][GEO_N]: the row slots
+    double *riv = geo + MWARPS * 2 * GEO_N;                             // [MT+1][5]: the r faces' intervals
     constexpr size_t toff = adv_tma_off(adv_smem_base<S, R>());
     S *raw = reinterpret_cast<S *>(adv_smem + toff);                                   // [3][MCOL][32]
     unsigned long long *bar = reinterpret_cast<unsigned long long *>(adv_smem + toff + raw_tile_bytes<S>());
@@ -490,13 +498,16 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
             }
         }
     }
-    constexpr bool PRE = sizeof(R) == 4;   // per-row scalars fetched a row ahead
+    // per-row scalars: row j0 now, every next row a row ahead (the buffer of row j is
+    // g0 + ((j - j0) & 1) * GEO_N)
     const double *gsrc = nullptr;
     int gstr = 0;
-    double *g = geo + w * GEO_N;
-    if constexpr (PRE) {
-        geo_source<S>(a, v, lane, col, own, gsrc, gstr);
-        if (lane < GEO_N) g[lane] = geo_fetch(gsrc, gstr, j0, j1);
+    double *g0 = geo + w * 2 * GEO_N;
+    geo_source<S>(a, v, lane, col, own, gsrc, gstr);
+    if (lane < GEO_N) g0[lane] = geo_fetch(gsrc, gstr, j0, j1);
+    for (int t = threadIdx.x; t < (MT + 1) * 5; t += blockDim.x) {
+        const int f = i0 + t / 5;
+        riv[t] = f <= v.nr ? __ldg(a.rint + v.orint + 5 * f + t % 5) : 0.0;
     }
     __syncthreads();
     R zL[3] = {R(0), R(0), R(0)};
@@ -506,9 +517,24 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
 
     const double ctdt = v.ctdt;
     const double ctdt_c = ctdt * kInvC;
+    // FP32 arithmetic (56 registers at 4 CTAs per SM) holds the next row's scalar in a register
+    // and keeps one buffer; FP64 arithmetic, at its register limit, copies it with cp.async into
+    // the other buffer (mixed advection 0.183 ms with the register, 0.189 ms with the copy;
+    // FP64 advection 0.333 -> 0.320 ms with the copy, at 256^2 x 64)
+    constexpr bool GREG = sizeof(R) == 4;
     for (int j = j0; j < j1; j++) {
+        double *g = GREG ? g0 : g0 + ((j - j0) & 1) * GEO_N;
         double gnext = 0.0;
-        if constexpr (PRE) gnext = geo_fetch(gsrc, gstr, j + 1, j1);
+        if constexpr (GREG) {
+            gnext = geo_fetch(gsrc, gstr, j + 1, j1);
+        } else {
+            if (lane < GEO_N) {
+                double *gn = g0 + ((j + 1 - j0) & 1) * GEO_N;
+                if (gsrc != nullptr && j + 1 < j1) cp_async_el(gn + lane, gsrc + (long long)gstr * (j + 1));
+                else gn[lane] = 0.0;
+            }
+            cp_async_commit();
+        }
         if constexpr (TMA) {
             // (A) row j+2 from its bulk copy: the own column, and (warp 8) the halo columns
             const int r = j + 2;
@@ -565,7 +591,8 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
         R zR[3] = {R(0), R(0), R(0)};
         if (kact && f <= v.nr) {
             R F[3], kL, kR;
-            face_r_staged<S, R, FLUX>(a, v, A, j & (RING - 1), w, f, j, k, lane, jeps, g + G_UR, F, kL, kR);
+            face_r_staged<S, R, FLUX>(a, v, A, j & (RING - 1), w, f, j, k, lane, jeps, g + G_UR, riv + 5 * w, F,
+                                      kL, kR);
             R *p = Fr + (w * 5) * 32 + lane;
             p[0] = F[0]; p[32] = F[1]; p[64] = F[2]; p[96] = kL; p[128] = kR;
         }
@@ -576,12 +603,11 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
         if (own && col < v.nr && k < a.nnu) {
             const int i = col;
             long long cl = (long long)i + (long long)v.nr * j;
-            long long c = v.oc + cl;
             long long x = v.o3 + (long long)k + (long long)a.nnu * cl;
             if (!kact) {
                 a.Jo[x] = a.J[x]; a.Hro[x] = a.Hr[x]; a.HZo[x] = a.HZ[x];
             } else {
-                const S *pH = Hh + (((j & (RING - 1)) * MT + w) * HF) * 32 + lane;
+                const S *pH = Hh + ((hslot(j) * MT + w) * HF) * 32 + lane;
                 const S uHr = pH[0], uHZ = pH[32];
                 const S uJ = HF == 3 ? pH[64] : S(A[(((j & (RING - 1)) * MCOL + w + 2) * NF) * 32 + lane]);
                 const R sJ = R(uJ), sHr = R(uHr), sHZ = R(uHZ);
@@ -589,16 +615,8 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
                 D_edd<R>(sHr, sHZ, sJ, jeps, R(a.heps2), Drr, DZZ, DrZ);
                 const R *FL = Fr + (w * 5) * 32 + lane;
                 const R *FR = FL + 5 * 32;
-                double ArL, ArR, AZL, AZR, fac;
-                if constexpr (PRE) {
-                    ArL = g[G_ARL]; ArR = g[G_ARR]; AZL = g[G_AZL]; AZR = g[G_AZR];
-                    fac = ctdt * g[G_IDV];
-                } else {
-                    ArL = __ldg(a.A_r + v.orf + i + (long long)(v.nr + 1) * j);
-                    ArR = __ldg(a.A_r + v.orf + i + 1 + (long long)(v.nr + 1) * j);
-                    AZL = __ldg(a.A_Z + v.ozf + cl); AZR = __ldg(a.A_Z + v.ozf + cl + v.nr);
-                    fac = ctdt * __ldg(a.inv_dV + c);
-                }
+                const double ArL = g[G_ARL], ArR = g[G_ARR], AZL = g[G_AZL], AZR = g[G_AZR];
+                const double fac = ctdt * g[G_IDV];
                 // increments in R, accumulated into the state in S
                 S Jn, Hrn, HZn;
                 const S ujeps = S(a.jeps);
@@ -615,17 +633,12 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
                 }
                 const S Jn0 = Jn;
                 Jn = Jn > ujeps ? Jn : ujeps;
-                R ga, gb, gc, gd, ge;
-                if constexpr (PRE) {
-                    ga = R(g[G_DURDR]); gb = R(g[G_DURDZ]); gc = R(g[G_DUZDR]); gd = R(g[G_DUZDZ]); ge = R(g[G_UROR]);
-                } else {
-                    ga = R(__ldg(a.dur_dr + c)); gb = R(__ldg(a.dur_dZ + c)); gc = R(__ldg(a.duZ_dr + c));
-                    gd = R(__ldg(a.duZ_dZ + c)); ge = R(__ldg(a.ur_over_r + c));
-                }
+                const R ga = R(g[G_DURDR]), gb = R(g[G_DURDZ]), gc = R(g[G_DUZDR]), gd = R(g[G_DUZDZ]);
+                const R ge = R(g[G_UROR]);
                 R DdU = d_colon_grad_u<R>(Drr, DrZ, DZZ, ga, gb, gc, gd, ge);
                 R Kav = R(0.5) * (FL[128] + FR[96]);
                 if (sizeof(R) == 8)
-                    Hrn += S(R(ctdt) * Kav * R(__ldg(a.inv_r_cell + v.ocol + i)));
+                    Hrn += S(R(ctdt) * Kav * R(g[G_IRC]));
                 else
                     Hrn += S(R(ctdt * g[G_IRC]) * Kav);
                 R cc = R(ctdt_c);
@@ -661,12 +674,17 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
             }
         }
         zL[0] = zR[0]; zL[1] = zR[1]; zL[2] = zR[2];
-        // the next row's scalars replace this row's once every lane of the warp has read them;
-        // the next row's first barrier publishes them
-        if constexpr (PRE) {
+        if constexpr (GREG) {
+            // the next row's scalars replace this row's once every lane of the warp has read them
             __syncwarp();
             if (lane < GEO_N) g[lane] = gnext;
+        } else {
+            // the next row's scalars have landed (each lane waits for its own copy; the warp
+            // barrier shows them to the other lanes and keeps this row's buffer until every lane
+            // has read it)
+            cp_async_wait<0>();
         }
+        __syncwarp();
     }
 }
 
@@ -918,23 +936,6 @@ __host__ __device__ constexpr int freq_smem_doubles(int nwarps, bool thomas) {
     return freq_smem_off_tsm<M>(nwarps) + (thomas ? nwarps * 4 * 32 * M : 0);
 }
 
-// Asynchronous global -> shared copy of one 4- or 8-byte element (cp.async, L1-allocating).
-template <typename T>
-__device__ __forceinline__ void cp_async_el(T *dst, const T *src) {
-    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "element size");
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
-    if constexpr (sizeof(T) == 8)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(src) : "memory");
-}
-// Asynchronous global -> shared copy of 16 bytes (cp.async.cg: L2 only, the rows are streamed).
-__device__ __forceinline__ void cp_async_16(void *dst, const void *src) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-
 // A lane's M contiguous bins of one row as whole 16-byte words, when the row layout allows it
 // (k_freq's `vec` path): loads from shared memory and stores to global memory.
 template <typename S, int M>
@@ -961,8 +962,6 @@ struct LaneRow {
         }
     }
 };
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // The cells [wbeg, wend) of a work item that warp `warp` of `nw` handles: one contiguous run
 // per warp (k_freq and k_find_active sum their partials in this order).
@@ -1610,7 +1609,7 @@ static void adv_occ(const void *args, int ntiles, cudaStream_t st, int ctas) {
 }
 
 int adv_ctas_per_sm(int prec, int want) {
-    if (prec == PREC_K_FP64) return (want == 2) ? 2 : 3;   // FP64: 65 KB of shared memory, 72 registers
+    if (prec == PREC_K_FP64) return (want == 2) ? 2 : 3;   // FP64: 74 KB of shared memory, 72 registers
     return (want >= 2 && want <= 4) ? want : 4;
 }
 

@@ -189,17 +189,19 @@ class M1Context:
 
     # -- adjoint ---------------------------------------------------------------------------
     def adjoint(self, n_steps, c_tilde, dt, z_center, bc_r_right=BC_OUTFLOW, bc_z_bot=BC_REFLECT,
-                bc_z_top=BC_OUTFLOW, w_MF=1.0, w_spec=None, checkpoint_every=0, want=None):
+                bc_z_top=BC_OUTFLOW, w_MF=1.0, w_spec=None, checkpoint_every=0, want=None, snapshots=0):
         """Gradients of  w_MF * M_F(last step) + sum_k w_spec[k] * S_k(final J)  over n_steps
         static-driver steps from the current state (lyd_adjoint_run); the context ends in
-        the final state. Returns a dict: objective, M_F, spectrum and the gradients
+        the final state. checkpoint_every: 1 keeps every step, K > 1 a checkpoint every K steps,
+        0 every step when it fits (else K = 100), < 0 the binomial schedule with `snapshots`
+        snapshots (0: the fewest with at most two advances of any step). Returns a dict: objective, M_F, spectrum and the gradients
         grad_alpha, grad_alpha_c, grad_T, grad_Hv, grad_u_r_star, grad_u_Z_star,
         grad_dur_dr, grad_dur_dZ, grad_duZ_dr, grad_duZ_dZ, grad_ur_over_r, grad_J0,
         grad_H_r0, grad_H_Z0 (numpy arrays in the reference's memory order)."""
         nr, nz, nnu = self.n_r, self.n_z, self.n_nu
         p = _lib.StepParams(float(c_tilde), float(dt), float(z_center), bc_r_right, bc_z_bot, bc_z_top, int(n_steps))
         ws = None if w_spec is None else _c64(w_spec)
-        cfg = _lib.AdjointCfg(p, int(checkpoint_every), 0, float(w_MF), _dp(ws) if ws is not None else None)
+        cfg = _lib.AdjointCfg(p, int(checkpoint_every), int(snapshots), float(w_MF), _dp(ws) if ws is not None else None)
         shapes = {"objective": (1,), "M_F": (1,), "spectrum": (nnu,), "grad_alpha": (nz, nr),
                   "grad_alpha_c": (nz, nr), "grad_T": (nz, nr), "grad_Hv": (nz, nr, nnu),
                   "grad_u_r_star": (nz, nr + 1), "grad_u_Z_star": (nz + 1, nr),

@@ -140,11 +140,28 @@ def test_initial_state_gradients(prob):
 def test_checkpoint_spacing_does_not_change_gradients(prob):
     # the face adjoints scatter with FP64 atomics: equal to rounding, not bitwise. 0 and 1 keep
     # every step's state and tape from the forward sweep; 2 (the fixture), 4 and n recompute
+    # segments; -1 is the binomial schedule with 0 (automatic), 1 and 2 extra snapshots
     _, g = prob.ctx_g
-    for every in (0, 1, 4, prob.n):
-        _, g2 = prob.adjoint(every)
+    for every, snaps in ((0, 0), (1, 0), (4, 0), (prob.n, 0), (-1, 0), (-1, 1), (-1, 2)):
+        ctx = prob.ctx()
+        g2 = ctx.adjoint(prob.n, *prob.p, w_MF=1.0, w_spec=SS * prob.w, checkpoint_every=every, snapshots=snaps)
+        ctx.close()
+        assert g2["objective"] == g["objective"]
         for k in ("grad_alpha", "grad_T", "grad_J0", "grad_u_r_star"):
             np.testing.assert_allclose(g2[k], g[k], rtol=1e-10, atol=1e-11 * np.abs(g[k]).max())
+
+
+def test_binomial_schedule_on_a_longer_run():
+    """40 steps with 3 extra snapshots (no step advanced more than 4 times) give the gradients of
+    the run that keeps every step."""
+    P = Problem(40)
+    out = []
+    for every, snaps in ((1, 0), (-1, 3)):
+        ctx = P.ctx()
+        out.append(ctx.adjoint(P.n, *P.p, w_MF=1.0, w_spec=SS * P.w, checkpoint_every=every, snapshots=snaps))
+        ctx.close()
+    for k in ("grad_alpha", "grad_alpha_c", "grad_T", "grad_J0", "grad_u_Z_star"):
+        np.testing.assert_allclose(out[1][k], out[0][k], rtol=1e-10, atol=1e-11 * np.abs(out[0][k]).max())
 
 
 def test_adjoint_rejects_unsupported_forms():
