@@ -7,7 +7,8 @@ inputs:
 
 * cylindrical geometry -- src/SpatialGrid.jl:26-170 (centroids, volumes, areas, <1/r>),
   src/SpatialGrid.jl:516-586 (PLM intervals with mirrored / extrapolated ghost centroids),
-  src/SpatialGrid.jl:606-913 (uniform grid branch, LinRange interfaces);
+  src/SpatialGrid.jl:606-913 (uniform interfaces, and the logarithmic regions of N_r_log and
+  N_Z_log_side cells whose widths grow by the ratio bisection finds);
 * frequency grid -- src/SetupLymanAlphaArrays.jl:40-135 (symmetric, geometrically growing
   bins, core range), and the fixed-count variant used to inject a 48/64/128-bin grid
   through GenerateLyaArrays_FromSaved (src/SetupLymanAlphaArrays.jl:244-296).
@@ -155,6 +156,100 @@ def cartesian_geometry(X, Y):
 def uniform_cylindrical_geometry(rmax, zmax, nr, nz):
     """Uniform branch of SetupCylindricalGrid (N_r_log = N_Z_log_side = 0)."""
     return cylindrical_geometry(julia_linrange(0.0, rmax, nr + 1), julia_linrange(0.0, zmax, nz + 1))
+
+
+def _isapprox(a, b, rtol):
+    return abs(a - b) <= rtol * max(abs(a), abs(b))
+
+
+def geometric_ratio(L, d, n):
+    """The ratio q > 1 of n intervals d q, d q^2, ..., d q^n... that span L: the root of
+    f(q) = L - d (q^n - 1) / (q - 1), found as SetupCylindricalGrid finds it
+    (src/SpatialGrid.jl:693-716): a bracket [1 + 1e-14, 2] whose upper end doubles until
+    f < 0, then bisection until the bracket cannot be split further in FP64."""
+    f = lambda q: L - d * (q ** n - 1.0) / (q - 1.0)
+    lo, hi = 1.0 + 1e-14, 2.0
+    while f(hi) > 0.0:
+        hi *= 2.0
+        if hi > 1e12:
+            raise ValueError("failed to bracket the ratio of the logarithmic grid")
+    flo = f(lo)
+    while True:
+        mid = 0.5 * (lo + hi)
+        if mid <= lo or mid >= hi:
+            break
+        fm = f(mid)
+        if fm == 0.0:
+            return mid
+        if (fm > 0.0) == (flo > 0.0):
+            lo, flo = mid, fm
+        else:
+            hi = mid
+    return lo if abs(f(lo)) <= abs(f(hi)) else hi
+
+
+def _log_tail(x0, d, L, n, sign=1.0):
+    """The n - 1 interfaces beyond x0 (towards sign) of n cells spanning L that start at the
+    uniform width d and grow geometrically (or stay uniform when n d already spans L)."""
+    if _isapprox(L, n * d, 1e-12):
+        return np.array([x0 + sign * k * d for k in range(1, n)])
+    if L < n * d:
+        raise ValueError("can't find a consistent logarithmic grid: use a larger range or a uniform grid")
+    q = geometric_ratio(L, d, n)
+    return np.array([x0 + sign * d * (q ** k - 1.0) / (q - 1.0) for k in range(1, n)])
+
+
+def log_stretched_interfaces(rmax, rmax_lin, Zmax, LZ_uniform, N_r_lin, N_r_log, N_Z_lin, N_Z_log_side,
+                             bc_z_bot="Reflect"):
+    """Interfaces (r, Z) of SetupCylindricalGrid (src/SpatialGrid.jl:606-830): a uniform radial
+    grid of N_r_lin cells up to rmax_lin, then N_r_log cells growing geometrically to rmax; in Z
+    a uniform central region of N_Z_lin cells and length LZ_uniform with N_Z_log_side growing
+    cells on each open side (above it for a reflecting bottom at Z = 0; above and below it,
+    mirrored, for an outflowing bottom)."""
+    if not (rmax > 0.0 and Zmax > 0.0 and LZ_uniform > 0.0 and rmax_lin > 0.0 and LZ_uniform <= Zmax):
+        raise ValueError("SetupCylindricalGrid needs rmax, Zmax, LZ_uniform, rmax_lin > 0 and LZ_uniform <= Zmax")
+    outflow = str(bc_z_bot).strip(":") == "Outflow"
+    N_r = N_r_lin + N_r_log
+    N_Z = N_Z_lin + (2 if outflow else 1) * N_Z_log_side
+    if N_r < 3 or N_Z < 3:
+        raise ValueError("the M1 stencil needs N_r >= 3 and N_Z >= 3")
+    if outflow:
+        zmin_lin, zmax_lin = 0.5 * (Zmax - LZ_uniform), 0.5 * (Zmax + LZ_uniform)
+        Z_lin = julia_linrange(zmin_lin, zmax_lin, N_Z_lin + 1)
+        dZ = Z_lin[1] - Z_lin[0]
+        if N_Z_log_side >= 2:
+            L_lower, L_upper = zmin_lin, Zmax - zmax_lin
+            if not _isapprox(L_lower, L_upper, 1e-12):
+                raise ValueError("the two logarithmic Z regions differ in length")
+            up = _log_tail(zmax_lin, dZ, L_upper, N_Z_log_side)
+            low = (zmin_lin - (up - zmax_lin))[::-1]
+            Z = np.concatenate(([0.0], low, Z_lin, up, [Zmax]))
+        else:
+            Z = julia_linrange(0.0, Zmax, N_Z_lin + 1)
+    else:
+        Z_lin = julia_linrange(0.0, LZ_uniform, N_Z_lin + 1)
+        dZ = Z_lin[1] - Z_lin[0]
+        if N_Z_log_side >= 2:
+            Z = np.concatenate((Z_lin, _log_tail(LZ_uniform, dZ, Zmax - LZ_uniform, N_Z_log_side), [Zmax]))
+        else:
+            Z = julia_linrange(0.0, Zmax, N_Z_lin + 1)
+    r_lin = julia_linrange(0.0, rmax_lin, N_r_lin + 1)
+    dr = r_lin[1] - r_lin[0]
+    if N_r_log >= 2:
+        r = np.concatenate((r_lin, _log_tail(rmax_lin, dr, rmax - rmax_lin, N_r_log), [rmax]))
+    else:
+        r = julia_linrange(0.0, rmax, N_r_lin + 1)
+    if not (np.all(np.diff(r) > 0.0) and np.all(np.diff(Z) > 0.0)):
+        raise ValueError("interfaces are not increasing")
+    return r, Z
+
+
+def log_stretched_cylindrical_geometry(rmax, rmax_lin, Zmax, LZ_uniform, N_r_lin, N_r_log, N_Z_lin, N_Z_log_side,
+                                       bc_z_bot="Reflect"):
+    """SetupCylindricalGrid (src/SpatialGrid.jl:606-915) with its logarithmic regions: the
+    interfaces of log_stretched_interfaces and the geometry of cylindrical_geometry."""
+    return cylindrical_geometry(*log_stretched_interfaces(rmax, rmax_lin, Zmax, LZ_uniform, N_r_lin, N_r_log,
+                                                          N_Z_lin, N_Z_log_side, bc_z_bot))
 
 
 @dataclass

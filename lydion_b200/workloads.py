@@ -100,15 +100,18 @@ def cfl_dt(geom, c_tilde, u_r, u_Z, cfl):
 
 def static_cloud(nr, nz, n_nu, tau0, T0=1e4, tau_abs=0.0, pd0=0.0, rs=0.0, umax_kms=0.0,
                  recoil=True, bc_z_bot=BC_REFLECT, flux_method=FLUX_GLF, freq=None, name="cloud",
-                 cfl=0.4, x_max=600.0):
-    """Fields of SetupStaticCloudTest (src/StaticCloudTest.jl:117-306), uniform grid, no cone."""
+                 cfl=0.4, x_max=600.0, geom=None):
+    """Fields of SetupStaticCloudTest (src/StaticCloudTest.jl:117-306), no cone; on a uniform
+    grid of nr x nz cells over 1.1 R_cl, or on `geom` (whose sizes then replace nr, nz)."""
     L = 1e5 * K.Lsun
     Rcl = K.pc
-    Rmax = 1.1 * Rcl
-    Zmax = Rmax
+    Rmax = 1.1 * Rcl if geom is None else float(geom.r[-1])
+    Zmax = 1.1 * Rcl if geom is None else float(geom.Z[-1])
     Zc = 0.0 if bc_z_bot == BC_REFLECT else 0.5 * Zmax
     c_tilde = K.c
-    geom = uniform_cylindrical_geometry(Rmax, Zmax, nr, nz)
+    if geom is None:
+        geom = uniform_cylindrical_geometry(Rmax, Zmax, nr, nz)
+    nr, nz = geom.r.size - 1, geom.Z.size - 1
     if freq is None:
         freq = symmetric_frequency_grid(n_nu, x_max=x_max, T_ref=T0)
     rC, ZC = np.meshgrid(geom.rCoM, geom.ZCoM)            # [j, i]

@@ -389,3 +389,28 @@ def test_many_bins_per_lane_match_oracle(oracle_mod, n_nu, tol):
     assert max_rel(d_g[:, 0], d_o[:, 0]) < tol
     for f in ("J", "H_r", "H_Z"):
         assert norm_err(ctx.download(f), getattr(st, f)) < tol, f
+
+
+@pytest.mark.parametrize("bc_z_bot", [W.BC_REFLECT, W.BC_OUTFLOW])
+def test_log_stretched_grid_steps_match_oracle(oracle_mod, bc_z_bot):
+    """The step on a grid with logarithmic regions (SetupCylindricalGrid with N_r_log and
+    N_Z_log_side, src/SpatialGrid.jl:606-915): non-uniform PLM intervals, volumes and areas in
+    every kernel, 30 fused steps against the oracle."""
+    from lydion_b200 import constants as K
+    from lydion_b200 import grid as G
+    pc = K.pc
+    if bc_z_bot == W.BC_REFLECT:
+        geom = G.log_stretched_cylindrical_geometry(1.1 * pc, 0.6 * pc, 1.1 * pc, 0.5 * pc, 10, 6, 9, 5, "Reflect")
+    else:
+        geom = G.log_stretched_cylindrical_geometry(1.1 * pc, 0.6 * pc, 2.2 * pc, 0.8 * pc, 10, 6, 9, 4, "Outflow")
+    cl = W.static_cloud(0, 0, 32, tau0=1e6, tau_abs=0.5, rs=0.5, umax_kms=100.0, bc_z_bot=bc_z_bot,
+                        x_max=100.0, geom=geom, name="stretched")
+    st, ctx = matched_pair(oracle_mod, cl, seed=19)
+    n = 30
+    d_o = st.run(n)
+    d_g = ctx.static_steps(n, cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+    np.testing.assert_array_equal(d_g[:, 5:7], d_o[:, 5:7])
+    assert max_rel(d_g[1:, 0], d_o[1:, 0]) < 1e-9
+    for f in ("J", "H_r", "H_Z"):
+        assert norm_err(ctx.download(f), getattr(st, f)) < 1e-9, f
+    ctx.close()

@@ -125,6 +125,60 @@ def test_geometry_uniform_grid():
         G.uniform_cylindrical_geometry(1.0, 1.0, 2, 5)
 
 
+@pytest.mark.parametrize("bc", ["Reflect", "Outflow"])
+def test_log_stretched_grid_intervals(bc):
+    """SetupCylindricalGrid with logarithmic regions (src/SpatialGrid.jl:606-830): the uniform
+    part is the LinRange of its cells, the logarithmic part's widths start at the uniform width
+    and grow by one ratio q, q is the root of L - d (q^n - 1)/(q - 1), and the grid ends at
+    rmax / Zmax; with an outflowing bottom the lower Z region mirrors the upper one."""
+    pc = K.pc
+    rmax, rmax_lin, N_r_lin, N_r_log = 1.1 * pc, 0.6 * pc, 8, 6
+    Zmax, LZ, N_Z_lin, N_Z_log = (1.1 * pc, 0.5 * pc, 8, 5) if bc == "Reflect" else (2.2 * pc, 0.8 * pc, 8, 5)
+    r, Z = G.log_stretched_interfaces(rmax, rmax_lin, Zmax, LZ, N_r_lin, N_r_log, N_Z_lin, N_Z_log, bc)
+    assert r.size - 1 == N_r_lin + N_r_log
+    assert Z.size - 1 == N_Z_lin + (2 if bc == "Outflow" else 1) * N_Z_log
+    assert r[0] == 0.0 and Z[0] == 0.0 and r[-1] == rmax and Z[-1] == Zmax
+    np.testing.assert_array_equal(r[:N_r_lin + 1], G.julia_linrange(0.0, rmax_lin, N_r_lin + 1))
+    d = r[1] - r[0]
+    q = G.geometric_ratio(rmax - rmax_lin, d, N_r_log)
+    assert abs((rmax - rmax_lin) - d * (q ** N_r_log - 1) / (q - 1)) <= 1e-12 * rmax
+    w = np.diff(r)[N_r_lin:]
+    np.testing.assert_allclose(w, d * q ** np.arange(N_r_log), rtol=1e-10)
+    wz = np.diff(Z)
+    if bc == "Outflow":
+        np.testing.assert_allclose(wz[:N_Z_log], wz[::-1][:N_Z_log], rtol=1e-10)
+        dz = wz[N_Z_log]
+        qz = G.geometric_ratio(0.5 * (Zmax - LZ), dz, N_Z_log)
+        np.testing.assert_allclose(wz[N_Z_log + N_Z_lin:], dz * qz ** np.arange(N_Z_log), rtol=1e-10)
+        np.testing.assert_allclose(Z[N_Z_log:N_Z_log + N_Z_lin + 1],
+                                   G.julia_linrange(0.5 * (Zmax - LZ), 0.5 * (Zmax + LZ), N_Z_lin + 1), rtol=1e-15)
+    else:
+        dz = wz[0]
+        qz = G.geometric_ratio(Zmax - LZ, dz, N_Z_log)
+        np.testing.assert_allclose(wz[N_Z_lin:], dz * qz ** np.arange(N_Z_log), rtol=1e-10)
+    # the PLM intervals of the stretched grid: L = r_{i+1/2} - rCoM_i, R = rCoM_{i+1} - r_{i+1/2}
+    g = G.log_stretched_cylindrical_geometry(rmax, rmax_lin, Zmax, LZ, N_r_lin, N_r_log, N_Z_lin, N_Z_log, bc)
+    np.testing.assert_allclose(g.dr_L, r[1:] - g.rCoM, rtol=1e-14)
+    np.testing.assert_allclose(g.dr_R[:-1], g.rCoM[1:] - r[1:-1], rtol=1e-14)
+    np.testing.assert_allclose(g.inv_dr_ip1_i[:-1], 1.0 / np.diff(g.rCoM), rtol=1e-14)
+    assert g.dV.sum() == pytest.approx(np.pi * rmax ** 2 * Zmax, rel=1e-13)
+
+
+def test_log_stretched_grid_edge_cases():
+    pc = K.pc
+    # a "logarithmic" region that n uniform cells already span stays uniform
+    r, Z = G.log_stretched_interfaces(1.0 * pc, 0.5 * pc, 1.0 * pc, 0.5 * pc, 5, 5, 5, 5, "Reflect")
+    np.testing.assert_allclose(np.diff(r), 0.1 * pc, rtol=1e-12)
+    # a region too short for its cells at the uniform width is rejected
+    with pytest.raises(ValueError):
+        G.log_stretched_interfaces(1.0 * pc, 0.8 * pc, 1.0 * pc, 0.5 * pc, 4, 5, 5, 5, "Reflect")
+    with pytest.raises(ValueError):
+        G.log_stretched_interfaces(1.0 * pc, 0.5 * pc, 1.0 * pc, 1.5 * pc, 5, 5, 5, 5, "Reflect")
+    # one logarithmic cell or none: the whole axis is uniform
+    r, Z = G.log_stretched_interfaces(1.0 * pc, 0.5 * pc, 1.0 * pc, 0.5 * pc, 6, 1, 6, 0, "Reflect")
+    np.testing.assert_array_equal(r, G.julia_linrange(0.0, 1.0 * pc, 7))
+
+
 def test_frequency_grids():
     fq = G.symmetric_frequency_grid(64)
     assert fq.n_nu == 64
