@@ -188,7 +188,8 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const void *map, int x, i
 // taken once per cell, not once per face) and alpha_F (formed once per cell, not at each of the
 // four face sides that read it); a ring of three rows holds the state of the own columns for
 // the cell update. The FP64 tile (74 KB) runs at three CTAs per SM. Warp w (0..7) owns
-// column i0+w; warp 8 stages the halo columns and computes the tile's rightmost r face. Per row: stage row j+2 -> sync -> every warp
+// column i0+w; warp 8 computes the tile's rightmost r face, and it and warps 0..2 stage one halo
+// cell each. Per row: stage row j+2 -> sync -> every warp
 // computes the r face on its left (warp 8: the right edge) into shared memory and its Z face
 // j+1/2 into registers -> sync -> the cell update of row j uses the two r faces from shared
 // memory and the Z faces j-1/2 (carried from the previous row) and j+1/2.
@@ -487,15 +488,12 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
     if constexpr (TMA) {
         // with bulk copies the halo columns of a row come with its copy, two rows before the
         // r faces read them: the prologue stages those of rows j0 and j0+1
-        if (!own && kact) {
-            const int hl[4] = {0, 1, MT + 2, MT + 3};
-            for (int r = j0; r <= j0 + 1 && r < j1 && r < v.nz; r++) {
-#pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    int c2 = i0 - 2 + hl[q];
-                    if (c2 <= v.nr + 1) stage_cell<S, R>(a, v, A, Hh, r & (RING - 1), hl[q], c2, r, k, lane, jeps);
-                }
-            }
+        const int hq = own ? (w < 3 ? w + 1 : -1) : 0;
+        if (hq >= 0 && kact) {
+            const int hl = hq < 2 ? hq : MT + hq;
+            const int c2 = i0 - 2 + hl;
+            for (int r = j0; r <= j0 + 1 && r < j1 && r < v.nz; r++)
+                if (c2 <= v.nr + 1) stage_cell<S, R>(a, v, A, Hh, r & (RING - 1), hl, c2, r, k, lane, jeps);
         }
     }
     // per-row scalars: row j0 now, every next row a row ahead (the buffer of row j is
@@ -547,14 +545,14 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
                     if (own) {
                         if (col <= v.nr + 1 && !(col >= v.nr && grow))
                             stage_from_raw<S, R>(a, v, raw, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps, i0);
-                    } else if (!grow && r < j1) {
-                        const int hl[4] = {0, 1, MT + 2, MT + 3};
-#pragma unroll
-                        for (int q = 0; q < 4; q++) {
-                            int c2 = i0 - 2 + hl[q];
-                            if (c2 <= v.nr + 1)
-                                stage_from_raw<S, R>(a, v, raw, A, Hh, r & (RING - 1), hl[q], c2, r, k, lane, jeps, i0);
-                        }
+                    }
+                    // the halo cells: warp 8 and warps 0..2, one each
+                    const int hq = own ? (w < 3 ? w + 1 : -1) : 0;
+                    if (hq >= 0 && !grow && r < j1) {
+                        const int hl = hq < 2 ? hq : MT + hq;
+                        const int c2 = i0 - 2 + hl;
+                        if (c2 <= v.nr + 1)
+                            stage_from_raw<S, R>(a, v, raw, A, Hh, r & (RING - 1), hl, c2, r, k, lane, jeps, i0);
                     }
                 }
             }
@@ -567,21 +565,21 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
             // the raw tile is free again: fetch row j+3 while this row's faces and update run
             if (threadIdx.x == 0 && j + 3 <= rlast) issue_row(j + 3);
         } else {
-            // (A) stage row j+2 of the own column; warp 8 stages the halo columns of row j
+            // (A) stage row j+2 of the own column, and the four halo cells of row j: warp 8
+            // takes the first and warps 0..2 one more each, so that no warp stages more than two
+            // cells while the others wait at the barrier
             if (kact) {
                 if (own) {
                     int r = j + 2;
                     bool gcol = col >= v.nr, grow = r >= v.nz;
                     if (col <= v.nr + 1 && r <= v.nz + 1 && !(gcol && grow))
                         stage_cell<S, R>(a, v, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps);
-                } else {
-                    const int hl[4] = {0, 1, MT + 2, MT + 3};
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        int c2 = i0 - 2 + hl[q];
-                        if (c2 <= v.nr + 1)
-                            stage_cell<S, R>(a, v, A, Hh, j & (RING - 1), hl[q], c2, j, k, lane, jeps);
-                    }
+                }
+                const int hq = own ? (w < 3 ? w + 1 : -1) : 0;
+                if (hq >= 0) {
+                    const int hl = hq < 2 ? hq : MT + hq;      // staged columns 0, 1, MT+2, MT+3
+                    const int c2 = i0 - 2 + hl;
+                    if (c2 <= v.nr + 1) stage_cell<S, R>(a, v, A, Hh, j & (RING - 1), hl, c2, j, k, lane, jeps);
                 }
             }
             __syncthreads();
