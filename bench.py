@@ -342,7 +342,8 @@ def dropin_form(cloud, args, stream_of, local):
 
 def batch_form(args, barrier, stream_of, local, world):
     """The ragged batch (512 static clouds x 48 bins, sides 32..256, per-cloud CFL step) in both
-    forms: a few graph-replayed steps of the whole batch each."""
+    forms: graph-replayed steps of the whole batch (--steps of them, 20 to 500), and the three
+    kernels' own share of the step."""
     from lydion_b200 import autotune, sharding
     from lydion_b200 import workloads as W
     from lydion_b200._lib import PREC_FP64, PREC_MIXED
@@ -353,7 +354,8 @@ def batch_form(args, barrier, stream_of, local, world):
     pp = cloud_params(mine)
     out = {"workload": "c3_ragged_batch_512_clouds_x48", "clouds": len(clouds),
            "cell_bins": int(sum(c.cell_bins for c in clouds))}
-    steps = max(3, min(20, args.steps // 150))
+    # timed steps: --steps, at least 20 and at most the 500 of the batch configuration
+    steps = max(20, min(500, args.steps))
     for name, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
         b = batch_for_clouds(mine, precision=prec, device=local)
         run = lambda n: b.batch_steps(n, pp, history=False)
@@ -362,10 +364,26 @@ def batch_form(args, barrier, stream_of, local, world):
         run(3)
         barrier(b)
         ms = sharding.max_over_ranks(_timed(b, run, steps, stream_of), device="cuda")
+        # the three kernels' own device time per step: what is left of the step is launch gaps,
+        # all a single persistent kernel could remove
+        b.set_timing(True)
+        run(2)
+        b.synchronize()
+        kms = b.timing() / 2
+        b.set_timing(False)
+        # the same steps as one persistent cooperative launch each (lyd_batch_steps_persistent)
+        runp = lambda n: b.batch_steps(n, pp, history=False, persistent=True)
+        runp(3)
+        barrier(b)
+        pms = sharding.max_over_ranks(_timed(b, runp, steps, stream_of), device="cuda")
         # every rank advances its share of the 512 clouds: the whole batch's cell-bins over the
         # slowest rank's time
         out[name] = {"value": steps * out["cell_bins"] / (ms * 1e-3), "ms_per_step": ms / steps, "steps": steps,
-                     "tuning": list(tuning)}
+                     "tuning": list(tuning),
+                     "kernel_ms_per_step": {"advect": float(kms[0]), "freq": float(kms[1]), "reduce": float(kms[2])},
+                     "launch_gap_fraction": float(max(0.0, 1.0 - float(np.sum(kms)) / (ms / steps))),
+                     "persistent": {"ms_per_step": pms / steps, "graph": b.persistent_graph(),
+                                    "over_three_launches": ms / pms}}
         b.close()
     out["mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
     return out

@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define LYD_ABI_VERSION 4
+#define LYD_ABI_VERSION 5
 
 /* status codes */
 #define LYD_OK              0
@@ -36,7 +36,8 @@ extern "C" {
 #define LYD_ERR_STATE      -5   /* call needs an input that was never provided           */
 #define LYD_ERR_NOMEM      -6   /* device allocation failed                              */
 #define LYD_ERR_TIMEOUT    -7   /* a bounded wait inside a kernel ran out (a bulk copy
-                                   never completed); the kernel skipped its remaining work  */
+                                   never completed, or a grid barrier of the persistent
+                                   step); the kernel skipped its remaining work             */
 
 /* boundary conditions (Symbol :Reflect / :Outflow in the reference) */
 #define LYD_BC_REFLECT 0
@@ -238,6 +239,18 @@ typedef struct lyd_cloud_params {
 /* n_steps static-driver iterations of every cloud, cloud q with params[q]; hist (may be NULL)
  * receives n_steps * n_clouds records, step-major. */
 int  lyd_batch_steps(lyd_ctx *ctx, const lyd_cloud_params *params, int32_t n_steps, lyd_diag *hist);
+/* lyd_batch_steps with each step as ONE cooperative launch of a persistent kernel (a grid of
+ * resident CTAs runs the advection tiles, the frequency-kernel cells and the reduction, with
+ * a grid barrier between the phases) instead of three launches; the results are bit-for-bit
+ * those of lyd_batch_steps. A CTA that waits at a barrier for more than barrier_polls polls
+ * (~0.1 us each) gives up and the call reports LYD_ERR_TIMEOUT (at the next synchronising
+ * call when hist is NULL); the state is then undefined and the context stays usable.
+ * barrier_polls must be positive; 1 << 24 is ample. The rows are staged by per-lane loads. */
+int  lyd_batch_steps_persistent(lyd_ctx *ctx, const lyd_cloud_params *params, int32_t n_steps,
+                                int64_t barrier_polls, lyd_diag *hist);
+/* Whether the persistent step is replayed from a CUDA graph: 1 yes, -1 launched directly (the
+ * runtime refused to capture it), 0 not run yet. */
+int  lyd_persistent_info(lyd_ctx *ctx, int32_t *graph);
 
 /* Launch-shape knobs chosen by the autotuner (lydion_b200/autotune.py): rows of the
  * advection tile (4..64), cells per frequency-kernel block (8..1024, or 0 for automatic), the

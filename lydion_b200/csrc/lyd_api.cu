@@ -103,6 +103,9 @@ struct lyd_ctx {
     double *small = nullptr;           // device scratch (512 doubles)
     cudaGraphExec_t gexec = nullptr;
     int gkey_cur = -1;
+    long long gkey_polls = 0;          // 0: the three-launch step graph; else the persistent step's poll limit
+    unsigned *bar = nullptr;           // grid barrier of the persistent step: arrivals, generation
+    int persist_graph = 0;             // persistent step replayed from a graph: 1 yes, -1 no (capture refused)
     bool timing = false;
     cudaEvent_t ev[8] = {};
     double ms[3] = {0, 0, 0};
@@ -164,8 +167,16 @@ static int check_err(lyd_ctx *c) {
     LYD_CU(c, cudaStreamSynchronize(c->st));
     if (h) {
         LYD_CU(c, cudaMemsetAsync(c->err, 0, sizeof(int), c->st));
-        if (h & ERRB_TIMEOUT)
-            return fail(c, LYD_ERR_TIMEOUT, "a bulk copy of the advection's staging did not complete in time");
+        if (h & ERRB_TIMEOUT) {
+            // a persistent step whose CTAs left early may leave the reduction's counters part-way
+            LYD_CU(c, cudaMemsetAsync(c->red_cnt, 0, (size_t)c->ncl * sizeof(int), c->st));
+            LYD_CU(c, cudaMemsetAsync(c->step_ctr + 1, 0, sizeof(int), c->st));
+            LYD_CU(c, cudaStreamSynchronize(c->st));
+            c->active_valid = false;
+            return fail(c, LYD_ERR_TIMEOUT,
+                        "a bounded wait ran out (a bulk copy of the advection's staging or a grid barrier of the "
+                        "persistent step)");
+        }
         if (h & ERRB_NONFINITE) return fail(c, LYD_ERR_NONFINITE, "non-finite value in J or H");
         return fail(c, LYD_ERR_SOLVE, "zero pivot in a frequency tridiagonal system");
     }
@@ -398,6 +409,7 @@ int lyd_batch_create(lyd_ctx **out, int32_t ncl, const int32_t *n_r, const int32
     A((void **)&c->last, (size_t)7 * ncl * sizeof(double));
     A((void **)&c->err, sizeof(int));
     A((void **)&c->small, 512 * 8);
+    A((void **)&c->bar, 2 * sizeof(unsigned));
     if (cfg->keep_freq_factors)
         for (int q = 0; q < 3; q++) A((void **)&c->Ff[q], c->n3 * 8);
     if (r == LYD_OK) r = build_work(c);
@@ -432,7 +444,7 @@ int lyd_destroy(lyd_ctx *c) {
                   c->inv_dV, c->A_r, c->A_Z, c->inv_r_cell, c->rCoM, c->ZCoM, c->rint, c->zint, c->r_if, c->Z_if,
                   c->nu, c->nuC, c->dnu, c->inv_dnu, c->inv_nuC, c->partials, c->kwin, c->hist, c->step_ctr,
                   c->last, c->err, c->lut, c->stage, c->small, c->cl, c->tiles, c->items, c->adj_ws,
-                  c->red_cols, c->red_cnt};
+                  c->red_cols, c->red_cnt, c->bar};
     for (void *p : ps) cudaFree(p);
     for (int q = 0; q < CF_N; q++) cudaFree(c->cellf[q]);
     cudaFree(c->dust_F);
@@ -1052,8 +1064,10 @@ template <typename S>
 // read s_n from and write s_{n+1} into its own storage instead, and `ff` to keep the frequency
 // factors F+, F, F- (n3 apart), and `win_next` to receive the window the step decides for the
 // next one.
+// `polls` > 0 runs the step as one cooperative launch of the persistent kernel whose grid
+// barriers give up after that many polls.
 static int enqueue_step(lyd_ctx *c, bool timed, double *tape = nullptr, const S *in = nullptr, S *out = nullptr,
-                        double *ff = nullptr, bool reduce = true, int *win_next = nullptr) {
+                        double *ff = nullptr, bool reduce = true, int *win_next = nullptr, long long polls = 0) {
     const int A = c->cur, B = 1 - c->cur;
     AdvArgs<S> aa;
     fill_adv<S>(c, aa, A, B);
@@ -1075,6 +1089,16 @@ static int enqueue_step(lyd_ctx *c, bool timed, double *tape = nullptr, const S 
     ra.diag = c->hist; ra.step_counter = c->step_ctr; ra.done = c->step_ctr + 1; ra.hist_capacity = c->hist_cap;
     ra.kwin_copy = win_next;
     const int prec = c->prec;
+    if (polls > 0) {
+        if (timed) cudaEventRecord(c->ev[0], c->st);
+        cudaError_t e = launch_persistent(prec, c->cfg.flux_method, &aa, &fa, ra, c->nnu, c->ntiles, c->nitems, c->bar,
+                                          polls, c->err, c->st);
+        if (timed)
+            for (int q = 1; q < 4; q++) cudaEventRecord(c->ev[q], c->st);
+        if (e != cudaSuccess) return fail(c, LYD_ERR_CUDA, std::string("persistent step: ") + cudaGetErrorString(e));
+        LYD_CU(c, cudaGetLastError());
+        return LYD_OK;
+    }
     if (timed) cudaEventRecord(c->ev[0], c->st);
     launch_advect(prec, c->cfg.flux_method, &aa, c->ntiles, c->tune.adv_ctas_per_sm, c->st);
     if (timed) cudaEventRecord(c->ev[1], c->st);
@@ -1098,8 +1122,9 @@ int lyd_get_timing(lyd_ctx *c, double ms[3]) {
     return LYD_OK;
 }
 
-// n_steps fused steps with the parameters already in the host descriptors.
-static int run_steps(lyd_ctx *c, int n_steps, lyd_diag *hist_out) {
+// n_steps fused steps with the parameters already in the host descriptors; `polls` > 0 runs
+// each step as one persistent cooperative launch (see enqueue_step).
+static int run_steps(lyd_ctx *c, int n_steps, lyd_diag *hist_out, long long polls = 0) {
     LYD_TRY(need_inputs(c, true, true));
     if (n_steps == 0) return LYD_OK;
     if (n_steps > c->hist_cap) {
@@ -1121,7 +1146,8 @@ static int run_steps(lyd_ctx *c, int n_steps, lyd_diag *hist_out) {
     if (c->timing) {
         double acc[3] = {0, 0, 0};
         for (int n = 0; n < n_steps; n++) {
-            int r = c->sprec == 0 ? enqueue_step<double>(c, true) : enqueue_step<float>(c, true);
+            int r = c->sprec == 0 ? enqueue_step<double>(c, true, nullptr, nullptr, nullptr, nullptr, true, nullptr, polls)
+                                  : enqueue_step<float>(c, true, nullptr, nullptr, nullptr, nullptr, true, nullptr, polls);
             if (r != LYD_OK) return r;
             LYD_CU(c, cudaEventSynchronize(c->ev[3]));
             for (int q = 0; q < 3; q++) {
@@ -1131,19 +1157,37 @@ static int run_steps(lyd_ctx *c, int n_steps, lyd_diag *hist_out) {
             }
         }
         for (int q = 0; q < 3; q++) c->ms[q] = acc[q];
+    } else if (polls > 0 && c->persist_graph < 0) {
+        // the runtime refused to capture the cooperative launch: one launch per step
+        for (int n = 0; n < n_steps; n++) {
+            int r = c->sprec == 0 ? enqueue_step<double>(c, false, nullptr, nullptr, nullptr, nullptr, true, nullptr, polls)
+                                  : enqueue_step<float>(c, false, nullptr, nullptr, nullptr, nullptr, true, nullptr, polls);
+            if (r != LYD_OK) return r;
+        }
     } else {
-        if (!c->gexec || c->gkey_cur != c->cur) {
+        if (!c->gexec || c->gkey_cur != c->cur || c->gkey_polls != polls) {
             drop_graph(c);
-            cudaGraph_t g;
+            cudaGraph_t g = nullptr;
             LYD_CU(c, cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-            int r = c->sprec == 0 ? enqueue_step<double>(c, false) : enqueue_step<float>(c, false);
+            int r = c->sprec == 0 ? enqueue_step<double>(c, false, nullptr, nullptr, nullptr, nullptr, true, nullptr, polls)
+                                  : enqueue_step<float>(c, false, nullptr, nullptr, nullptr, nullptr, true, nullptr, polls);
             cudaError_t e = cudaStreamEndCapture(c->st, &g);
+            if (e == cudaSuccess && r == LYD_OK) {
+                e = cudaGraphInstantiate(&c->gexec, g, 0);
+                if (e != cudaSuccess) c->gexec = nullptr;
+            }
+            if (g) cudaGraphDestroy(g);
+            if (polls > 0 && (r != LYD_OK || e != cudaSuccess)) {
+                // capture of the cooperative launch refused: launch it directly from now on
+                cudaGetLastError();
+                c->persist_graph = -1;
+                return run_steps(c, n_steps, hist_out, polls);
+            }
             if (r != LYD_OK) return r;
             if (e != cudaSuccess) return fail(c, LYD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-            e = cudaGraphInstantiate(&c->gexec, g, 0);
-            cudaGraphDestroy(g);
-            if (e != cudaSuccess) return fail(c, LYD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
             c->gkey_cur = c->cur;
+            c->gkey_polls = polls;
+            if (polls > 0) c->persist_graph = 1;
         }
         for (int n = 0; n < n_steps; n++) LYD_CU(c, cudaGraphLaunch(c->gexec, c->st));
     }
@@ -1276,10 +1320,8 @@ int lyd_dd_halo(lyd_ctx *c, int32_t side, int32_t pack, void *buf) {
     return LYD_OK;
 }
 
-int lyd_batch_steps(lyd_ctx *c, const lyd_cloud_params *p, int32_t n_steps, lyd_diag *hist_out) {
-    if (!c || !p) return LYD_ERR_ARG;
-    cudaSetDevice(c->dev);
-    if (n_steps < 0) return fail(c, LYD_ERR_ARG, "bad step count");
+// per-cloud step parameters into the host descriptors
+static int batch_params(lyd_ctx *c, const lyd_cloud_params *p) {
     for (int q = 0; q < c->ncl; q++) {
         LYD_TRY(check_bcs(c, c->cfg.bc_r_left, p[q].bc_r_right, p[q].bc_z_bot, p[q].bc_z_top));
         if (!(p[q].c_tilde > 0.0) || !(p[q].dt > 0.0)) return fail(c, LYD_ERR_ARG, "bad step parameters");
@@ -1290,7 +1332,31 @@ int lyd_batch_steps(lyd_ctx *c, const lyd_cloud_params *p, int32_t n_steps, lyd_
         d.bc_r_left = c->cfg.bc_r_left;
         d.bc_r_right = p[q].bc_r_right; d.bc_z_bot = p[q].bc_z_bot; d.bc_z_top = p[q].bc_z_top;
     }
+    return LYD_OK;
+}
+
+int lyd_batch_steps(lyd_ctx *c, const lyd_cloud_params *p, int32_t n_steps, lyd_diag *hist_out) {
+    if (!c || !p) return LYD_ERR_ARG;
+    cudaSetDevice(c->dev);
+    if (n_steps < 0) return fail(c, LYD_ERR_ARG, "bad step count");
+    LYD_TRY(batch_params(c, p));
     return run_steps(c, n_steps, hist_out);
+}
+
+int lyd_batch_steps_persistent(lyd_ctx *c, const lyd_cloud_params *p, int32_t n_steps, int64_t barrier_polls,
+                               lyd_diag *hist_out) {
+    if (!c || !p) return LYD_ERR_ARG;
+    if (barrier_polls < 1) return fail(c, LYD_ERR_ARG, "barrier_polls must be positive");
+    cudaSetDevice(c->dev);
+    if (n_steps < 0) return fail(c, LYD_ERR_ARG, "bad step count");
+    LYD_TRY(batch_params(c, p));
+    return run_steps(c, n_steps, hist_out, (long long)barrier_polls);
+}
+
+int lyd_persistent_info(lyd_ctx *c, int32_t *graph) {
+    if (!c || !graph) return LYD_ERR_ARG;
+    *graph = c->persist_graph;
+    return LYD_OK;
 }
 
 // ---- set-up helpers ------------------------------------------------------------------------------

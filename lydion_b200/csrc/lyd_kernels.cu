@@ -188,8 +188,7 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const void *map, int x, i
 // taken once per cell, not once per face) and alpha_F (formed once per cell, not at each of the
 // four face sides that read it); a ring of three rows holds the state of the own columns for
 // the cell update. The FP64 tile (74 KB) runs at three CTAs per SM. Warp w (0..7) owns
-// column i0+w; warp 8 computes the tile's rightmost r face, and it and warps 0..2 stage one halo
-// cell each. Per row: stage row j+2 -> sync -> every warp
+// column i0+w; warp 8 stages the halo columns and computes the tile's rightmost r face. Per row: stage row j+2 -> sync -> every warp
 // computes the r face on its left (warp 8: the right edge) into shared memory and its Z face
 // j+1/2 into registers -> sync -> the cell update of row j uses the two r faces from shared
 // memory and the Z faces j-1/2 (carried from the previous row) and j+1/2.
@@ -420,9 +419,11 @@ __host__ __device__ constexpr size_t adv_tma_off(size_t base) { return (base + 1
 // field, issued by one thread a row ahead of their use into one raw tile, completed on an
 // mbarrier) instead of per-lane loads; the converting warps apply the ghost-cell rules. The
 // first rows (j0-2 .. j0+1) are staged by per-lane loads while the first copy is in flight.
-template <typename S, typename R, int FLUX, int MINB, bool TMA>
-__global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
-    extern __shared__ __align__(128) unsigned char adv_smem[];
+// One tile of the advection (tile `tile` of the work list) by the calling CTA of MTHREADS
+// threads, in dynamic shared memory `adv_smem`: the body of k_advect, also run by the persistent
+// batch kernel.
+template <typename S, typename R, int FLUX, bool TMA>
+__device__ __forceinline__ void advect_tile(const AdvArgs<S> &a, int tile, unsigned char *adv_smem) {
     constexpr int HF = sizeof(S) == sizeof(R) ? 2 : 3;
     constexpr int NF = nf<R>();
     R *A = reinterpret_cast<R *>(adv_smem);                            // [RING][MCOL][NF][32]
@@ -435,7 +436,7 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
     unsigned long long *bar = reinterpret_cast<unsigned long long *>(adv_smem + toff + raw_tile_bytes<S>());
     int *abort_flag = reinterpret_cast<int *>(bar + 1);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int4 t = a.tiles[blockIdx.x];
+    const int4 t = a.tiles[tile];
     View v;
     load_view(a.cl[t.x], v);
     const int i0 = t.y, j0 = t.z, kb = t.w;
@@ -488,12 +489,15 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
     if constexpr (TMA) {
         // with bulk copies the halo columns of a row come with its copy, two rows before the
         // r faces read them: the prologue stages those of rows j0 and j0+1
-        const int hq = own ? (w < 3 ? w + 1 : -1) : 0;
-        if (hq >= 0 && kact) {
-            const int hl = hq < 2 ? hq : MT + hq;
-            const int c2 = i0 - 2 + hl;
-            for (int r = j0; r <= j0 + 1 && r < j1 && r < v.nz; r++)
-                if (c2 <= v.nr + 1) stage_cell<S, R>(a, v, A, Hh, r & (RING - 1), hl, c2, r, k, lane, jeps);
+        if (!own && kact) {
+            const int hl[4] = {0, 1, MT + 2, MT + 3};
+            for (int r = j0; r <= j0 + 1 && r < j1 && r < v.nz; r++) {
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    int c2 = i0 - 2 + hl[q];
+                    if (c2 <= v.nr + 1) stage_cell<S, R>(a, v, A, Hh, r & (RING - 1), hl[q], c2, r, k, lane, jeps);
+                }
+            }
         }
     }
     // per-row scalars: row j0 now, every next row a row ahead (the buffer of row j is
@@ -545,14 +549,14 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
                     if (own) {
                         if (col <= v.nr + 1 && !(col >= v.nr && grow))
                             stage_from_raw<S, R>(a, v, raw, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps, i0);
-                    }
-                    // the halo cells: warp 8 and warps 0..2, one each
-                    const int hq = own ? (w < 3 ? w + 1 : -1) : 0;
-                    if (hq >= 0 && !grow && r < j1) {
-                        const int hl = hq < 2 ? hq : MT + hq;
-                        const int c2 = i0 - 2 + hl;
-                        if (c2 <= v.nr + 1)
-                            stage_from_raw<S, R>(a, v, raw, A, Hh, r & (RING - 1), hl, c2, r, k, lane, jeps, i0);
+                    } else if (!grow && r < j1) {
+                        const int hl[4] = {0, 1, MT + 2, MT + 3};
+#pragma unroll
+                        for (int q = 0; q < 4; q++) {
+                            int c2 = i0 - 2 + hl[q];
+                            if (c2 <= v.nr + 1)
+                                stage_from_raw<S, R>(a, v, raw, A, Hh, r & (RING - 1), hl[q], c2, r, k, lane, jeps, i0);
+                        }
                     }
                 }
             }
@@ -565,21 +569,23 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
             // the raw tile is free again: fetch row j+3 while this row's faces and update run
             if (threadIdx.x == 0 && j + 3 <= rlast) issue_row(j + 3);
         } else {
-            // (A) stage row j+2 of the own column, and the four halo cells of row j: warp 8
-            // takes the first and warps 0..2 one more each, so that no warp stages more than two
-            // cells while the others wait at the barrier
+            // (A) stage row j+2 of the own column; warp 8 stages the halo columns of row j (spread
+            // over four warps instead, one halo cell each, the FP64 advection took 0.336 ms
+            // against 0.322 ms at 256^2 x 64)
             if (kact) {
                 if (own) {
                     int r = j + 2;
                     bool gcol = col >= v.nr, grow = r >= v.nz;
                     if (col <= v.nr + 1 && r <= v.nz + 1 && !(gcol && grow))
                         stage_cell<S, R>(a, v, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps);
-                }
-                const int hq = own ? (w < 3 ? w + 1 : -1) : 0;
-                if (hq >= 0) {
-                    const int hl = hq < 2 ? hq : MT + hq;      // staged columns 0, 1, MT+2, MT+3
-                    const int c2 = i0 - 2 + hl;
-                    if (c2 <= v.nr + 1) stage_cell<S, R>(a, v, A, Hh, j & (RING - 1), hl, c2, j, k, lane, jeps);
+                } else {
+                    const int hl[4] = {0, 1, MT + 2, MT + 3};
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        int c2 = i0 - 2 + hl[q];
+                        if (c2 <= v.nr + 1)
+                            stage_cell<S, R>(a, v, A, Hh, j & (RING - 1), hl[q], c2, j, k, lane, jeps);
+                    }
                 }
             }
             __syncthreads();
@@ -684,6 +690,12 @@ __global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
         }
         __syncwarp();
     }
+}
+
+template <typename S, typename R, int FLUX, int MINB, bool TMA>
+__global__ void __launch_bounds__(MTHREADS, MINB) k_advect(AdvArgs<S> a) {
+    extern __shared__ __align__(128) unsigned char adv_smem[];
+    advect_tile<S, R, FLUX, TMA>(a, blockIdx.x, adv_smem);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -979,11 +991,13 @@ __device__ __forceinline__ void warp_cell_run(int4 it, int warp, int nw, int &wb
 // relative, not like the rounding of F against F+ + F- that the factors themselves cannot take
 // (mixed frequency kernel at 256^2 x 64: 0.259 -> 0.246 ms; the mixed form's M_F after 2000
 // steps 5.93e-7 -> 5.95e-7 from FP64).
-template <typename S, typename R, int M, typename RC = R>
-__global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<S> a) {
-    extern __shared__ __align__(16) double fsm[];
+//
+// freq_item is one work item (`item` of `nitems`) by the calling CTA, whose first `nw` warps take
+// its cells (the others only meet its barriers), in dynamic shared memory `fsm`: the body of
+// k_freq, also run by the persistent batch kernel.
+template <typename S, typename R, int M, typename RC>
+__device__ __forceinline__ void freq_item(const FreqArgs<S> &a, int item, int nitems, double *fsm, int nw) {
     constexpr int NP = 32 * M;
-    const int nw = blockDim.x >> 5;
     constexpr bool PF = freq_prefetch<M>();
     double *kc = fsm;                              // [KC_N][NP]
     double *red = fsm + KC_N * NP;                 // [nwarps][NP + 8]
@@ -1006,7 +1020,7 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
     }
     __syncthreads();
 
-    const int4 it = a.items[blockIdx.x];
+    const int4 it = a.items[item];
     const CloudDesc &cd = a.cl[it.x];
     const long long o3 = cd.o3, oc = cd.oc;
     const int nr = cd.nr, nz = cd.nz, bzb = cd.bc_z_bot;
@@ -1411,15 +1425,17 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
     if (!a.parts) return;
     // ---- CTA reduction of the partials, fixed order ----
     const int stride = NP + 8;
+    if (warp < nw) {
 #pragma unroll
-    for (int m = 0; m < M; m++) red[warp * stride + lane * M + m] = acc_e[m];
+        for (int m = 0; m < M; m++) red[warp * stride + lane * M + m] = acc_e[m];
+    }
     acc_tot = warp_sum(acc_tot);
     acc_esc = warp_sum(acc_esc);
     acc_mf = warp_sum(acc_mf);
     acc_net = warp_sum(acc_net);
     acc_out = warp_sum(acc_out);
     acc_L = warp_sum(acc_L);
-    if (lane == 0) {
+    if (lane == 0 && warp < nw) {
         red[warp * stride + NP + 0] = acc_tot;
         red[warp * stride + NP + 1] = acc_mf;
         red[warp * stride + NP + 2] = acc_net;
@@ -1433,8 +1449,14 @@ __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<
         int src = col < nnu ? col : NP + (col - nnu);
         double s = 0.0;
         for (int w2 = 0; w2 < nw; w2++) s += red[w2 * stride + src];
-        a.partials[(size_t)col * gridDim.x + blockIdx.x] = s;
+        a.partials[(size_t)col * nitems + item] = s;
     }
+}
+
+template <typename S, typename R, int M, typename RC = R>
+__global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<S> a) {
+    extern __shared__ __align__(16) double fsm[];
+    freq_item<S, R, M, RC>(a, blockIdx.x, gridDim.x, fsm, blockDim.x >> 5);
 }
 
 // FindActiveBins partials of the current J (src/UpdateLyaJandH.jl:47-97): one warp per cell,
@@ -1487,14 +1509,16 @@ __global__ void __launch_bounds__(FREQ_THREADS) k_find_active(const S *J, int nn
 // 8 warps, one column per warp, whose sums go through a.colsum; the last CTA of the cloud to
 // finish takes the decision. Without, one CTA per cloud sums every column. The last decision
 // of the launch advances the record index.
-__global__ void __launch_bounds__(1024) k_reduce(RedArgs a) {
+// reduce_block is block `vb` of that launch by the calling CTA (all its warps): the body of
+// k_reduce, also run by the persistent batch kernel.
+__device__ __forceinline__ void reduce_block(const RedArgs &a, int vb) {
     __shared__ double col[256 + kExtraCols];
     __shared__ int is_last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const int ncols = a.nnu + kExtraCols;
     const bool split = a.cnt != nullptr;
     const int nchunks = split ? (ncols + nw - 1) / nw : 1;
-    const int cloud = blockIdx.x / nchunks, chunk = blockIdx.x % nchunks;
+    const int cloud = vb / nchunks, chunk = vb % nchunks;
     const CloudDesc &cd = a.cl[cloud];
     const int npb = cd.npb;
     const double *pbase = a.partials + cd.pb0;
@@ -1571,6 +1595,82 @@ __global__ void __launch_bounds__(1024) k_reduce(RedArgs a) {
                 *a.done = 0;
             }
         }
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_reduce(RedArgs a) { reduce_block(a, blockIdx.x); }
+
+// ---- the persistent step: one cooperative launch runs the three phases -----------------------
+//
+// A grid barrier with a bounded wait: the CTAs of the launch arrive on a counter; the last to
+// arrive resets it and advances the generation the others wait on. A wait that outlasts `polls`
+// polls sets ERRB_TIMEOUT and the CTA leaves the launch (the others then time out at this or
+// the next barrier), so a launch never hangs. Fences order each CTA's writes of one phase before
+// the other CTAs' reads of the next.
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned nblocks, long long polls, int *err) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = bar + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        int good = 1;
+        if (atomicAdd(bar, 1u) + 1u == nblocks) {
+            bar[0] = 0u;
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            long long it = 0;
+            while (*gen == g) {
+                if (++it > polls) {
+                    good = 0;
+                    atomicOr(err, ERRB_TIMEOUT);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// One fused static step of every cloud of a batch in one launch: the advection tiles, a grid
+// barrier, the frequency-kernel items (8 of the CTA's 9 warps take the cells, as in k_freq), a
+// grid barrier, the reduction blocks; each CTA walks the work lists with a grid stride. The rows
+// are staged by per-lane loads. Within a launch every buffer one phase reads was written by an
+// earlier launch or after a barrier, so no read meets a stale copy: the advection reads the set
+// the previous launch's frequency phase wrote.
+template <typename S>
+struct PersistArgs {
+    AdvArgs<S> adv;
+    FreqArgs<S> freq;
+    RedArgs red;
+    int ntiles, nitems, nred;
+    unsigned *bar;          // [0] arrivals, [1] generation; [0] zero before the launch
+    long long polls;
+    int *err;
+};
+
+// RA: arithmetic of the advection; RF, RC: of the frequency step and its closure (as k_freq).
+template <typename S, typename RA, typename RF, typename RC, int FLUX, int M>
+__global__ void __launch_bounds__(MTHREADS, 2) k_step_persistent(PersistArgs<S> p) {
+    extern __shared__ __align__(128) unsigned char psm[];
+    for (int t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
+        advect_tile<S, RA, FLUX, false>(p.adv, t, psm);
+        __syncthreads();
+    }
+    if (!grid_barrier(p.bar, gridDim.x, p.polls, p.err)) return;
+    for (int it = blockIdx.x; it < p.nitems; it += gridDim.x) {
+        freq_item<S, RF, M, RC>(p.freq, it, p.nitems, reinterpret_cast<double *>(psm), FREQ_THREADS / 32);
+        __syncthreads();
+    }
+    if (!grid_barrier(p.bar, gridDim.x, p.polls, p.err)) return;
+    for (int vb = blockIdx.x; vb < p.nred; vb += gridDim.x) {
+        reduce_block(p.red, vb);
+        __syncthreads();
     }
 }
 
@@ -1704,6 +1804,77 @@ void launch_find_active(int sprec, const void *J, int nnu, const double *dnu, co
                      case 4: LYD_ACT(float, 4); break; default: LYD_ACT(float, 8); break; }
     }
 #undef LYD_ACT
+}
+
+template <typename S, typename RA, typename RF, typename RC, int FLUX, int M>
+static cudaError_t persist_launch(const void *adv, const void *freq, const RedArgs &red, int ntiles, int nitems,
+                                  unsigned *bar, long long polls, int *err, cudaStream_t st) {
+    PersistArgs<S> p;
+    p.adv = *static_cast<const AdvArgs<S> *>(adv);
+    p.adv.tmaps = nullptr;
+    p.freq = *static_cast<const FreqArgs<S> *>(freq);
+    p.freq.vec16 = LaneRow<S, M>::ok && p.freq.nnu % M == 0 && (p.freq.nnu * sizeof(S)) % 16 == 0 && al16(p.freq.Jin) &&
+                   al16(p.freq.Hrin) && al16(p.freq.HZin) && al16(p.freq.Jold) && al16(p.freq.Hv) &&
+                   al16(p.freq.Jout) && al16(p.freq.Hrout) && al16(p.freq.HZout);
+    p.red = red;
+    if (!red.colsum) p.red.cnt = nullptr;
+    const int ncols = red.nnu + kExtraCols, rw = MTHREADS / 32;
+    p.ntiles = ntiles;
+    p.nitems = nitems;
+    p.nred = p.red.cnt ? red.nclouds * ((ncols + rw - 1) / rw) : red.nclouds;
+    p.bar = bar;
+    p.polls = polls;
+    p.err = err;
+    auto kern = k_step_persistent<S, RA, RF, RC, FLUX, M>;
+    const size_t sa = adv_smem_bytes<S, RA, false>();
+    const size_t sf = sizeof(double) * freq_smem_doubles<M>(FREQ_THREADS / 32, p.freq.solver == SOLVER_THOMAS);
+    const size_t sm = sa > sf ? sa : sf;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, MTHREADS, sm);
+    if (e != cudaSuccess) return e;
+    if (per < 1) return cudaErrorInvalidConfiguration;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(per * sms));
+    cfg.blockDim = dim3(MTHREADS);
+    cfg.dynamicSmemBytes = sm;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    e = cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st);
+    if (e != cudaSuccess) return e;
+    return cudaLaunchKernelEx(&cfg, kern, p);
+}
+
+cudaError_t launch_persistent(int prec, int flux, const void *adv, const void *freq, const RedArgs &red, int nnu,
+                              int ntiles, int nitems, unsigned *bar, long long polls, int *err, cudaStream_t st) {
+    const int M = bins_per_lane(nnu);
+#define LYD_PS1(S_, RA_, RF_, RC_, M_)                                                                     \
+    return flux == 0 ? persist_launch<S_, RA_, RF_, RC_, 0, M_>(adv, freq, red, ntiles, nitems, bar, polls, err, st) \
+                     : persist_launch<S_, RA_, RF_, RC_, 1, M_>(adv, freq, red, ntiles, nitems, bar, polls, err, st);
+#define LYD_PS(S_, RA_, RF_, RC_)                                                                         \
+    switch (M) {                                                                                          \
+    case 1: LYD_PS1(S_, RA_, RF_, RC_, 1)                                                                 \
+    case 2: LYD_PS1(S_, RA_, RF_, RC_, 2)                                                                 \
+    case 4: LYD_PS1(S_, RA_, RF_, RC_, 4)                                                                 \
+    default: LYD_PS1(S_, RA_, RF_, RC_, 8)                                                                \
+    }
+    // the arithmetic of each phase as in launch_advect and launch_freq
+    if (prec == PREC_K_FP32) {
+        LYD_PS(float, float, float, float)
+    } else if (prec == PREC_K_MIXED) {
+        LYD_PS(double, float, double, float)
+    } else {
+        LYD_PS(double, double, double, double)
+    }
+#undef LYD_PS
+#undef LYD_PS1
 }
 
 void launch_reduce(const RedArgs &a, cudaStream_t st) {

@@ -391,20 +391,33 @@ class M1Batch(M1Context):
         self._ck(lib().lyd_find_active_bins(self._h, a, b))
         return np.array(a[:]), np.array(b[:])
 
-    def batch_steps(self, n_steps, params, history=True):
+    def batch_steps(self, n_steps, params, history=True, persistent=False, barrier_polls=1 << 24):
         """params: one (c_tilde, dt, z_center, bc_r_right, bc_z_bot, bc_z_top) per cloud.
-        Returns the (n_steps, n_clouds, 7) records when history is set."""
+        Returns the (n_steps, n_clouds, 7) records when history is set. `persistent` runs each
+        step as one cooperative launch whose grid barriers give up after `barrier_polls` polls
+        (lyd_batch_steps_persistent)."""
         arr = (_lib.CloudParams * self.n_clouds)()
         for q, (ct, dt, zc, br, bb, bt) in enumerate(params):
             arr[q] = _lib.CloudParams(float(ct), float(dt), float(zc), int(br), int(bb), int(bt), 0)
+        if persistent:
+            call = lambda h: lib().lyd_batch_steps_persistent(self._h, arr, int(n_steps), int(barrier_polls), h)
+        else:
+            call = lambda h: lib().lyd_batch_steps(self._h, arr, int(n_steps), h)
         if history:
             hist = (_lib.Diag * max(1, n_steps * self.n_clouds))()
-            self._ck(lib().lyd_batch_steps(self._h, arr, int(n_steps), hist))
+            self._ck(call(hist))
             out = np.array([[d.M_F, d.M_F_radial_net, d.M_F_radial_out, d.L_tot, d.f_esc, d.kmin, d.kmax]
                             for d in hist[:n_steps * self.n_clouds]])
             return out.reshape(n_steps, self.n_clouds, 7)
-        self._ck(lib().lyd_batch_steps(self._h, arr, int(n_steps), None))
+        self._ck(call(None))
         return None
+
+    def persistent_graph(self):
+        """1 when the persistent step replays from a CUDA graph, -1 when it is launched directly
+        (capture refused by the runtime), 0 before its first run."""
+        g = C.c_int32(0)
+        self._ck(lib().lyd_persistent_info(self._h, C.byref(g)))
+        return g.value
 
     def edge_spectra(self, cloud=0):
         nr, nz = self.sizes[cloud]
