@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 2) k_freq_adj(FreqAdjArgs a) {
                 const double Jn = t1 > jeps ? t1 : jeps;
                 const double H2 = hr * hr + hz * hz;
                 if (H2 > Jn * Jn) {
-                    const double fsc = Jn / sqrt(H2);
+                    const double fsc = Jn * rsqrt_nr(H2);
                     hr *= fsc;
                     hz *= fsc;
                 }

@@ -10,17 +10,14 @@
 
 namespace lyd {
 
-// chi_L84(f) and its derivative together, src/M1Closure.jl:28-33: chi = (3 + 4f^2) / (5 + 2s),
-// s = sqrt(4 - 3f^2), chi' = (8f (5 + 2s) + 6 (3 + 4f^2) f / s) / (5 + 2s)^2; chi is formed as
-// chi_L84 forms it.
+// chi_L84(f) and its derivative together, src/M1Closure.jl:28-33: chi = (3 + 4f^2) / (5 + 2s)
+// = (5 - 2s) / 3 with s = sqrt(4 - 3f^2), formed as chi_L84 forms it; chi' = -(2/3) s' = 2f / s.
 __device__ __forceinline__ void chi_dchi_L84(double f, double &chi, double &dchi) {
     const double f2 = f * f;
-    const double s = sqrt(4.0 - 3.0 * f2);
-    const double den = 5.0 + 2.0 * s;
-    const double num = 3.0 + 4.0 * f2;
-    const double iden = rcp<double>(den);
-    chi = num * iden;
-    dchi = (8.0 * f * den + 6.0 * num * f * rcp<double>(s)) * (iden * iden);
+    const double t = 4.0 - 3.0 * f2;
+    const double is = rsqrt_nr(t);
+    chi = fma(-2.0 * t, is, 5.0) * (1.0 / 3.0);
+    dchi = 2.0 * f * is;
 }
 
 __device__ __forceinline__ void adj_minmod(double a, double b, double g, double &ga, double &gb) {
@@ -51,8 +48,9 @@ __device__ __forceinline__ void adj_D_edd(double Hr, double HZ, double J, double
                                           double gDZZ, double gDrZ, double &gHr, double &gHZ, double &gJ) {
     double H2 = Hr * Hr + HZ * HZ;
     const double fmin2 = kFmin * kFmin;
-    if (J <= jeps || H2 <= heps2 || H2 <= fmin2 * J * J) return;
-    double Hm = sqrt(H2);
+    if (J <= jeps || H2 <= heps2 || H2 <= fmin2 * J * J || !(H2 >= kDblMinNormal)) return;
+    const double iH = rsqrt_nr(H2);   // |H| and 1/|H| as D_edd forms them
+    const double Hm = H2 * iH;
     const double iJ = rcp<double>(J);
     double fr = Hm * iJ;
     const bool inside = fr > kFmin && fr < kFmax;
@@ -60,7 +58,6 @@ __device__ __forceinline__ void adj_D_edd(double Hr, double HZ, double J, double
     double chi, dchi;
     chi_dchi_L84(f, chi, dchi);
     double b = (3.0 * chi - 1.0) * 0.5;
-    double iH = rcp<double>(Hm);
     double nr = Hr * iH, nZ = HZ * iH;
     double ga = gDrr + gDZZ;
     double gb = gDrr * nr * nr + gDZZ * nZ * nZ + gDrZ * nr * nZ;
@@ -129,18 +126,19 @@ __device__ __forceinline__ void recon_fwd(const CellF<double> &cm1, const CellF<
     t.fZL0 = ci.fZ + dfZL * dL;
     t.fZR0 = cp1.fZ - dfZR * dR;
     double frL = t.frL0, fZL = t.fZL0, frR = t.frR0, fZR = t.fZR0;
-    double fL = sqrt(frL * frL + fZL * fZL);
+    // |f| and 1/|f| from one reciprocal square root, as reconstruct_f forms them
+    const double sL = frL * frL + fZL * fZL, sR = frR * frR + fZR * fZR;
+    double iL = sL >= kDblMinNormal ? rsqrt_nr(sL) : 0.0;
+    double iR = sR >= kDblMinNormal ? rsqrt_nr(sR) : 0.0;
+    double fL = sL * iL, fR = sR * iR;
     t.fL0 = fL;
-    if (fL > 1.0) { double inv = rcp<double>(fL); frL *= inv; fZL *= inv; fL = 1.0; }
-    double fR = sqrt(frR * frR + fZR * fZR);
     t.fR0 = fR;
-    if (fR > 1.0) { double inv = rcp<double>(fR); frR *= inv; fZR *= inv; fR = 1.0; }
+    if (fL > 1.0) { frL *= iL; fZL *= iL; fL = 1.0; iL = 1.0; }
+    if (fR > 1.0) { frR *= iR; fZR *= iR; fR = 1.0; iR = 1.0; }
     o.Hr_L = frL * o.J_L; o.Hr_R = frR * o.J_R;
     o.HZ_L = fZL * o.J_L; o.HZ_R = fZR * o.J_R;
-    if (fL > 0.0) { double inv = rcp<double>(fL); o.nr_L = frL * inv; o.nZ_L = fZL * inv; }
-    else { o.nr_L = 0.0; o.nZ_L = 0.0; }
-    if (fR > 0.0) { double inv = rcp<double>(fR); o.nr_R = frR * inv; o.nZ_R = fZR * inv; }
-    else { o.nr_R = 0.0; o.nZ_R = 0.0; }
+    o.nr_L = frL * iL; o.nZ_L = fZL * iL;
+    o.nr_R = frR * iR; o.nZ_R = fZR * iR;
     o.f_L = fL; o.f_R = fR;
 }
 
@@ -233,9 +231,9 @@ __device__ __forceinline__ void adj_hll_eigen(double f0, double mu0, double gl1,
     double mu = mu0 < -1.0 ? -1.0 : (mu0 > 1.0 ? 1.0 : mu0);
     double f2 = f * f, mu2 = mu * mu, muf = mu * f;
     double t = 4.0 - 3.0 * f2;
-    const bool tpos = t > 0.0;
-    double sq = sqrt(tpos ? t : 0.0);
-    double inv_sq = rcp<double>(sq);
+    const bool tpos = t > 0.0;      // always (t >= 1): the root and its reciprocal as hll_eigen forms them
+    double inv_sq = rsqrt_nr(t);
+    double sq = t * inv_sq;
     double g = (2.0 / 3.0) * (4.0 - 3.0 * f2 - sq) + 2.0 * mu2 * (2.0 - f2 - sq);
     const bool gpos = g > 0.0;
     double fac = sqrt(gpos ? g : 0.0);

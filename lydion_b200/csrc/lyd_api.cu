@@ -329,6 +329,21 @@ const char *lyd_last_error(const lyd_ctx *c) { return c ? c->msg.c_str() : "null
 
 int lyd_edge_count(int32_t n_r, int32_t n_z) { return (n_z - 2) + 2 * (n_r - 3); }
 
+int lyd_math_check(int32_t fn, const double *x, double *y, size_t n) {
+    if (fn < 0 || fn > 3 || !x || !y) return LYD_ERR_ARG;
+    if (n == 0) return LYD_OK;
+    double *d = nullptr;
+    if (cudaMalloc(&d, 2 * n * sizeof(double)) != cudaSuccess) return LYD_ERR_NOMEM;
+    cudaError_t e = cudaMemcpy(d, x, n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        launch_math(fn, d, d + n, n, 0);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(y, d + n, n * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? LYD_OK : LYD_ERR_CUDA;
+}
+
 int lyd_batch_create(lyd_ctx **out, int32_t ncl, const int32_t *n_r, const int32_t *n_z, int32_t n_nu,
                      const lyd_config *cfg) {
     if (!out || !cfg || !n_r || !n_z) return LYD_ERR_ARG;

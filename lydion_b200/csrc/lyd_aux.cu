@@ -356,4 +356,22 @@ void launch_edge(int prec, const void *J, const double *dnu, int nnu, int nr, in
     else k_edge<float><<<64, 256, 0, st>>>(static_cast<const float *>(J), dnu, nnu, nr, nz, j_scale, raw, norm);
 }
 
+// ---- the FP64 arithmetic helpers on host-given arguments, for their accuracy checks ---------
+__global__ void k_math(int fn, const double *x, double *y, size_t n) {
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const double v = x[q];
+        double r;
+        switch (fn) {
+            case 0: r = rsqrt_nr(v); break;
+            case 1: r = rcp<double>(v); break;
+            case 2: r = v * rsqrt_nr(v); break;
+            default: r = chi_L84<double>(v); break;
+        }
+        y[q] = r;
+    }
+}
+void launch_math(int fn, const double *x, double *y, size_t n, cudaStream_t st) {
+    k_math<<<grid_for(n), 256, 0, st>>>(fn, x, y, n);
+}
+
 }  // namespace lyd

@@ -667,7 +667,8 @@ __device__ __forceinline__ void advect_tile(const AdvArgs<S> &a, int tile, unsig
                         const S Hm = rsq(H2);
                         fsc = Hm > S(0) ? Jn / Hm : S(0);
                     } else {
-                        fsc = Jn / rsq(H2);
+                        // |H|^2 > J^2 >= jeps^2, far inside the normal range
+                        fsc = Jn * rsqrt_nr(H2);
                     }
                     Hrn *= fsc;
                     HZn *= fsc;
@@ -1351,7 +1352,7 @@ __device__ __forceinline__ void freq_item(const FreqArgs<S> &a, int item, int ni
                 double hr = double(Hr[m]) * ratio, hz = double(HZ[m]) * ratio;
                 double H2 = hr * hr + hz * hz;
                 if (H2 > Jf * Jf) {
-                    double fsc = Jf / sqrt(H2);
+                    double fsc = Jf * rsqrt_nr(H2);   // |H|^2 > J^2 >= jeps^2: normal
                     hr *= fsc;
                     hz *= fsc;
                 }

@@ -92,6 +92,23 @@ template <> __device__ __forceinline__ float rcp<float>(float y) {
     return x;
 }
 
+// Reciprocal square root 1 / sqrt(x) for FP64 arithmetic and x >= DBL_MIN: the hardware's
+// approximate reciprocal square root (PTX rsqrt.approx.ftz.f64) refined by two Newton-Raphson
+// steps for 1/sqrt(x), y <- y + y (1/2 - (x/2) y^2), each a multiply and two fused
+// multiply-adds; every step squares the relative error (Markstein, IBM J. Res. Dev. 34 (1990)
+// 111-119). x * rsqrt_nr(x) is then sqrt(x) to about an ulp, and one such root gives both a
+// length and its reciprocal where the IEEE root needs a root and a reciprocal.
+__device__ __forceinline__ double rsqrt_nr(double x) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double h = 0.5 * x;
+    double r = fma(-(h * y), y, 0.5);
+    y = fma(y, r, y);
+    r = fma(-(h * y), y, 0.5);
+    return fma(y, r, y);
+}
+constexpr double kDblMinNormal = 2.2250738585072014e-308;
+
 // Reciprocal square root 1 / sqrt(x) for FP32 arithmetic: the hardware's approximation alone
 // (PTX rsqrt.approx.ftz.f32, relative error within 2^-22.9 over the normal range; a subnormal
 // or zero argument gives +inf, so callers check x against FLT_MIN first). One transcendental
@@ -109,18 +126,19 @@ __device__ __forceinline__ R minmod(R a, R b) {
     return (a * b <= R(0)) ? R(0) : (fabs(a) < fabs(b) ? a : b);
 }
 
-// Levermore closure chi(f), src/M1Closure.jl:28-33
-// With FP32 arithmetic it is evaluated as (5 - 2 sqrt(4 - 3 f^2)) / 3, the same function
-// (multiply numerator and denominator by 5 - 2 sqrt(4 - 3 f^2): the denominator becomes
-// 3 (3 + 4 f^2)), with one square root and no reciprocal; 5 - 2 sqrt(..) >= 1 for f <= 1, so
-// nothing cancels.
+// Levermore closure chi(f), src/M1Closure.jl:28-33, evaluated as (5 - 2 sqrt(4 - 3 f^2)) / 3,
+// the same function (multiply numerator and denominator by 5 - 2 sqrt(4 - 3 f^2): the
+// denominator becomes 3 (3 + 4 f^2)), with one square root and no reciprocal; 5 - 2 sqrt(..)
+// >= 1 for f <= 1, so at most a factor 4 cancels (f = 0: 5 - 4). In FP64 the root of
+// t = 4 - 3 f^2, in [1, 4], is t * rsqrt_nr(t), folded into 5 - 2 s by one fused multiply-add.
 template <typename R>
 __device__ __forceinline__ R chi_L84(R f) {
     R f2 = f * f;
+    R t = R(4) - R(3) * f2;
     if constexpr (sizeof(R) == 4)
-        return (R(5) - R(2) * rsq(R(4) - R(3) * f2)) * R(1.0f / 3.0f);
+        return (R(5) - R(2) * rsq(t)) * R(1.0f / 3.0f);
     else
-        return (R(3) + R(4) * f2) * rcp<R>(R(5) + R(2) * rsq(R(4) - R(3) * f2));
+        return fma(-2.0 * t, rsqrt_nr(t), 5.0) * (1.0 / 3.0);
 }
 
 // Compute_D_Edd_from_f_n, src/M1Closure.jl:91-119
@@ -150,17 +168,22 @@ __device__ __forceinline__ void D_edd(R Hr, R HZ, R J, R jeps, R heps2, R &Drr, 
         return;
     }
     R Hmag, inv_H;
+    // one reciprocal square root gives |H| and 1/|H|; |H|^2 below the type's normal range
+    // counts as no direction
     if constexpr (sizeof(R) == 4) {
-        if (!(H2 >= kFltMinNormal)) {   // |H|^2 below FP32's normal range: no direction
+        if (!(H2 >= kFltMinNormal)) {
             Drr = Num<R>::third(); DZZ = Num<R>::third(); DrZ = R(0);
             return;
         }
         inv_H = rsqf(H2);
-        Hmag = H2 * inv_H;
     } else {
-        Hmag = rsq(H2);
-        inv_H = rcp<R>(Hmag);
+        if (!(H2 >= kDblMinNormal)) {
+            Drr = Num<R>::third(); DZZ = Num<R>::third(); DrZ = R(0);
+            return;
+        }
+        inv_H = rsqrt_nr(H2);
     }
+    Hmag = H2 * inv_H;
     R f = Hmag * rcp<R>(J);
     f = f < Num<R>::fmin() ? Num<R>::fmin() : (f > Num<R>::fmax() ? Num<R>::fmax() : f);
     R chi = chi_L84(f);
@@ -180,14 +203,11 @@ __device__ __forceinline__ void hll_eigen(R f, R mu, R &l1, R &l3) {
     mu = mu < R(-1) ? R(-1) : (mu > R(1) ? R(1) : mu);
     R f2 = f * f, mu2 = mu * mu, muf = mu * f;
     R t = R(4) - R(3) * f2;
-    R sq, inv_sq;
-    if constexpr (sizeof(R) == 4) {   // t >= 1 (f <= fmax < 1): one reciprocal square root
-        inv_sq = rsqf(t);
-        sq = t * inv_sq;
-    } else {
-        sq = rsq(t > R(0) ? t : R(0));
-        inv_sq = rcp<R>(sq);
-    }
+    // t >= 1 (f <= fmax < 1): one reciprocal square root gives the root and its reciprocal
+    R inv_sq;
+    if constexpr (sizeof(R) == 4) inv_sq = rsqf(t);
+    else inv_sq = rsqrt_nr(t);
+    const R sq = t * inv_sq;
     R g = R(2) / R(3) * (R(4) - R(3) * f2 - sq) + R(2) * mu2 * (R(2) - f2 - sq);
     R fac = rsq(g > R(0) ? g : R(0));
     R x1 = (muf - fac) * inv_sq, x3 = (muf + fac) * inv_sq;
@@ -242,33 +262,24 @@ __device__ __forceinline__ Recon<R> reconstruct_f(const CellF<R> &cm1, const Cel
     R frL = ci.fr + dfrL * dL, frR = cp1.fr - dfrR * dR;
     R fZL = ci.fZ + dfZL * dL, fZR = cp1.fZ - dfZR * dR;
 
+    // one reciprocal square root gives |f| and 1/|f|; |f|^2 below the type's normal range
+    // counts as no flux (no direction)
+    const R sL = frL * frL + fZL * fZL, sR = frR * frR + fZR * fZR;
+    R iL, iR;
     if constexpr (sizeof(R) == 4) {
-        // one reciprocal square root gives |f| and 1/|f|; |f|^2 below FP32's normal range
-        // counts as no flux (no direction)
-        const R sL = frL * frL + fZL * fZL, sR = frR * frR + fZR * fZR;
-        const bool nzL = sL >= kFltMinNormal, nzR = sR >= kFltMinNormal;
-        R iL = nzL ? rsqf(sL) : R(0), iR = nzR ? rsqf(sR) : R(0);
-        R fL = sL * iL, fR = sR * iR;
-        if (fL > R(1)) { frL *= iL; fZL *= iL; fL = R(1); iL = R(1); }
-        if (fR > R(1)) { frR *= iR; fZR *= iR; fR = R(1); iR = R(1); }
-        o.Hr_L = frL * o.J_L; o.Hr_R = frR * o.J_R;
-        o.HZ_L = fZL * o.J_L; o.HZ_R = fZR * o.J_R;
-        o.nr_L = frL * iL; o.nZ_L = fZL * iL;
-        o.nr_R = frR * iR; o.nZ_R = fZR * iR;
-        o.f_L = fL; o.f_R = fR;
-        return o;
+        iL = sL >= kFltMinNormal ? rsqf(sL) : R(0);
+        iR = sR >= kFltMinNormal ? rsqf(sR) : R(0);
+    } else {
+        iL = sL >= kDblMinNormal ? rsqrt_nr(sL) : R(0);
+        iR = sR >= kDblMinNormal ? rsqrt_nr(sR) : R(0);
     }
-    R fL = rsq(frL * frL + fZL * fZL);
-    if (fL > R(1)) { R inv = rcp<R>(fL); frL *= inv; fZL *= inv; fL = R(1); }
-    R fR = rsq(frR * frR + fZR * fZR);
-    if (fR > R(1)) { R inv = rcp<R>(fR); frR *= inv; fZR *= inv; fR = R(1); }
-
+    R fL = sL * iL, fR = sR * iR;
+    if (fL > R(1)) { frL *= iL; fZL *= iL; fL = R(1); iL = R(1); }
+    if (fR > R(1)) { frR *= iR; fZR *= iR; fR = R(1); iR = R(1); }
     o.Hr_L = frL * o.J_L; o.Hr_R = frR * o.J_R;
     o.HZ_L = fZL * o.J_L; o.HZ_R = fZR * o.J_R;
-    if (fL > R(0)) { R inv = rcp<R>(fL); o.nr_L = frL * inv; o.nZ_L = fZL * inv; }
-    else { o.nr_L = R(0); o.nZ_L = R(0); }
-    if (fR > R(0)) { R inv = rcp<R>(fR); o.nr_R = frR * inv; o.nZ_R = fZR * inv; }
-    else { o.nr_R = R(0); o.nZ_R = R(0); }
+    o.nr_L = frL * iL; o.nZ_L = fZL * iL;
+    o.nr_R = frR * iR; o.nZ_R = fZR * iR;
     o.f_L = fL; o.f_R = fR;
     return o;
 }
