@@ -158,7 +158,8 @@ int  lyd_abi_version(void);
 /* The device's FP64 arithmetic helpers on n host values (device 0 or the current device), for
  * checks of their accuracy: fn 0: 1/sqrt(x) (approximation refined by Newton steps; x normal,
  * positive), 1: 1/x (likewise; x normal, nonzero), 2: sqrt(x) as x * (1/sqrt(x)), 3: the
- * closure chi(f) = (5 - 2 sqrt(4 - 3 f^2)) / 3 for f in [0, 1]. */
+ * closure chi(f) = (5 - 2 sqrt(4 - 3 f^2)) / 3 for f in [0, 1], 4: exp(x) for |x| <= 40 (the
+ * table-driven form of the frequency factors). */
 int  lyd_math_check(int32_t fn, const double *x, double *y, size_t n);
 int  lyd_set_geometry(lyd_ctx *ctx, const lyd_geometry *g);
 int  lyd_set_freq_grid(lyd_ctx *ctx, const lyd_freq_grid *f);

@@ -225,7 +225,8 @@ __device__ __forceinline__ void omphi_d_LR(double P, Omphi &L, Omphi &R_) {
     R_.o = ie; R_.x = (1.0 - ie) * iP; R_.d_o = ie; R_.d_x = (-ie - R_.x) * iP;
 }
 
-__device__ __forceinline__ void ff_fwd(const FfIn &q, double &Fp, double &F0, double &Fm) {
+// `tab`: exp_tab's table (the forward frequency kernel's exponentials).
+__device__ __forceinline__ void ff_fwd(const FfIn &q, double &Fp, double &F0, double &Fm, const double *tab) {
     double iKkm = rcp<double>(q.Kkm), iKk = rcp<double>(q.Kk), iKkp = rcp<double>(q.Kkp);
     double Ckp = q.vel * q.nCkp, Ck = q.vel * q.nCk, Ckm = q.vel * q.nCkm;
     if (q.recoil) {
@@ -238,9 +239,9 @@ __device__ __forceinline__ void ff_fwd(const FfIn &q, double &Fp, double &F0, do
     double Pk = fmin(fmax(Ck * rk, -kPmax), kPmax);
     double Pkm = fmin(fmax(Ckm * rkm, -kPmax), kPmax);
     double oRkp, xRkp, oLk, xLk, oRk, xRk, oLkm, xLkm;
-    omphi_R(Pkp, oRkp, xRkp);
-    omphi_LR(Pk, oLk, xLk, oRk, xRk);
-    omphi_L(Pkm, oLkm, xLkm);
+    omphi_R(Pkp, oRkp, xRkp, tab);
+    omphi_LR(Pk, oLk, xLk, oRk, xRk, tab);
+    omphi_L(Pkm, oLkm, xLkm, tab);
     double dkp = q.idn * rcp<double>(xLk * rk - xRkp * rkp);
     double dkm = q.idn * rcp<double>(xLkm * rkm - xRk * rk);
     Fp = oRkp * dkp;
@@ -308,6 +309,9 @@ __global__ void __launch_bounds__(ADJ_THREADS, 2) k_freq_adj(FreqAdjArgs a) {
     const CloudDesc &cd = a.cl[it.x];
     const double c_tilde = cd.c_tilde, dt = cd.dt, ctdt = cd.ctdt;
     const double jeps = a.jeps, dw = 1.0 / ctdt;
+    __shared__ double etab[32];
+    if (threadIdx.x < 32) etab[threadIdx.x] = kExp2Tab[threadIdx.x];
+    __syncthreads();
     for (int cl = it.y + warp; cl < it.z; cl += nw) {
         const long long c = cd.oc + cl;
         const long long base = cd.o3 + (long long)cl * nnu;
@@ -400,7 +404,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 2) k_freq_adj(FreqAdjArgs a) {
                     q.DNKM = a.nu[k] - a.nuC[k - 1]; q.DNK = a.nu[k + 1] - a.nuC[k];
                     q.DNKP = a.nuC[k + 1] - a.nu[k + 1];
                     q.idn = a.inv_dnu[k]; q.rec0 = rec0; q.recoil = a.recoil;
-                    ff_fwd(q, Fp[m], F0[m], Fm[m]);
+                    ff_fwd(q, Fp[m], F0[m], Fm[m], etab);
                 }
             }
             bool in = (k >= 1 && k <= nnu - 2);

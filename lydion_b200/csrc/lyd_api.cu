@@ -330,7 +330,7 @@ const char *lyd_last_error(const lyd_ctx *c) { return c ? c->msg.c_str() : "null
 int lyd_edge_count(int32_t n_r, int32_t n_z) { return (n_z - 2) + 2 * (n_r - 3); }
 
 int lyd_math_check(int32_t fn, const double *x, double *y, size_t n) {
-    if (fn < 0 || fn > 3 || !x || !y) return LYD_ERR_ARG;
+    if (fn < 0 || fn > 4 || !x || !y) return LYD_ERR_ARG;
     if (n == 0) return LYD_OK;
     double *d = nullptr;
     if (cudaMalloc(&d, 2 * n * sizeof(double)) != cudaSuccess) return LYD_ERR_NOMEM;

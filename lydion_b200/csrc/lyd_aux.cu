@@ -365,7 +365,8 @@ __global__ void k_math(int fn, const double *x, double *y, size_t n) {
             case 0: r = rsqrt_nr(v); break;
             case 1: r = rcp<double>(v); break;
             case 2: r = v * rsqrt_nr(v); break;
-            default: r = chi_L84<double>(v); break;
+            case 3: r = chi_L84<double>(v); break;
+            default: r = exp_tab(v, kExp2Tab); break;
         }
         y[q] = r;
     }

@@ -142,7 +142,7 @@ void launch_find_active(int sprec, const void *J, int nnu, const double *dnu, co
 void launch_advect(int prec, int flux, const void *args, int ntiles, int ctas_per_sm, cudaStream_t st);
 int adv_ctas_per_sm(int prec, int want);   // the occupancy variant launch_advect uses
 void launch_freq(int prec, const void *args, int nnu, int nitems, cudaStream_t st);
-// fn 0: rsqrt_nr, 1: rcp<double>, 2: x * rsqrt_nr(x), 3: chi_L84<double>
+// fn 0: rsqrt_nr, 1: rcp<double>, 2: x * rsqrt_nr(x), 3: chi_L84<double>, 4: exp_tab
 void launch_math(int fn, const double *x, double *y, size_t n, cudaStream_t st);
 // one fused step in one cooperative launch (advection, frequency step, reduction, with bounded
 // grid barriers between them); bar: two unsigned of device memory

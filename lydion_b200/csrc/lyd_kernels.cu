@@ -918,7 +918,8 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // Per-k constants of UpdateFreqFactors! staged in shared memory once per CTA.
-enum { KC_NCK, KC_NCKP, KC_NCKM, KC_DNKP, KC_DNK, KC_DNKM, KC_IDNU, KC_ICK, KC_ICKP, KC_ICKM, KC_DNU, KC_N };
+// KC_EXP2: the 32 entries of exp_tab's table.
+enum { KC_NCK, KC_NCKP, KC_NCKM, KC_DNKP, KC_DNK, KC_DNKM, KC_IDNU, KC_ICK, KC_ICKP, KC_ICKM, KC_DNU, KC_EXP2, KC_N };
 
 // Per-cell inputs staged in shared memory, 32 cells at a time per warp.
 // CS_SUM_R / CS_SUM_Z receive each cell's sum over bins of dnu (H_old - H), which the warp's
@@ -1018,6 +1019,7 @@ __device__ __forceinline__ void freq_item(const FreqArgs<S> &a, int item, int ni
         kc[KC_ICKP * NP + t] = in ? a.inv_nuC[t + 1] : 0.0;
         kc[KC_ICKM * NP + t] = in ? a.inv_nuC[t - 1] : 0.0;
         kc[KC_DNU * NP + t] = (t < nnu) ? a.dnu[t] : 0.0;
+        kc[KC_EXP2 * NP + t] = (t < 32) ? kExp2Tab[t] : 0.0;
     }
     __syncthreads();
 
@@ -1295,9 +1297,10 @@ __device__ __forceinline__ void freq_item(const FreqArgs<S> &a, int item, int ni
                     double Pk = fmin(fmax(Ck * rk, -kPmax), kPmax);
                     double Pkm = fmin(fmax(Ckm * rkm, -kPmax), kPmax);
                     double oRkp, xRkp, oLk, xLk, oRk, xRk, oLkm, xLkm;
-                    omphi_R(Pkp, oRkp, xRkp);
-                    omphi_LR(Pk, oLk, xLk, oRk, xRk);
-                    omphi_L(Pkm, oLkm, xLkm);
+                    const double *etab = kc + KC_EXP2 * NP;
+                    omphi_R(Pkp, oRkp, xRkp, etab);
+                    omphi_LR(Pk, oLk, xLk, oRk, xRk, etab);
+                    omphi_L(Pkm, oLkm, xLkm, etab);
                     double idn = kc[KC_IDNU * NP + k];
                     double dkp = idn * rcp<double>(xLk * rk - xRkp * rkp);
                     double dkm = idn * rcp<double>(xLkm * rkm - xRk * rk);

@@ -361,6 +361,42 @@ __device__ __forceinline__ R d_colon_grad_u(R Drr, R DrZ, R DZZ, R a, R b, R c, 
     return Drr * a + DrZ * (b + c) + DZZ * d + Dpp * e;
 }
 
+// exp(x) for |x| <= 40 in FP64 by the table-driven method of P. T. P. Tang (ACM Trans. Math.
+// Softw. 15 (1989) 144-157): x = (32 m + j) ln2/32 + r with |r| <= ln2/64, exp(x) = 2^m 2^(j/32)
+// e^r. The 32 values 2^(j/32) are correctly rounded (generated in 80-digit decimal arithmetic),
+// e^r - 1 is its Taylor polynomial to degree 6 (truncation below 4e-18 relative) and the
+// result is 2^m (T + T (e^r - 1)) with one rounding: within about an ulp. round(32 x / ln2)
+// comes out of one fused multiply-add with 1.5 * 2^52 (its low bits then hold the integer);
+// ln2/32 is split in a 40-bit head, whose products with |32 x / ln2| < 2^13 are exact, and a
+// tail. `tab` is kExp2Tab, or a copy of it in shared memory.
+static __constant__ double kExp2Tab[32] = {
+    0x1.0000000000000p+0, 0x1.059b0d3158574p+0, 0x1.0b5586cf9890fp+0, 0x1.11301d0125b51p+0,
+    0x1.172b83c7d517bp+0, 0x1.1d4873168b9aap+0, 0x1.2387a6e756238p+0, 0x1.29e9df51fdee1p+0,
+    0x1.306fe0a31b715p+0, 0x1.371a7373aa9cbp+0, 0x1.3dea64c123422p+0, 0x1.44e086061892dp+0,
+    0x1.4bfdad5362a27p+0, 0x1.5342b569d4f82p+0, 0x1.5ab07dd485429p+0, 0x1.6247eb03a5585p+0,
+    0x1.6a09e667f3bcdp+0, 0x1.71f75e8ec5f74p+0, 0x1.7a11473eb0187p+0, 0x1.82589994cce13p+0,
+    0x1.8ace5422aa0dbp+0, 0x1.93737b0cdc5e5p+0, 0x1.9c49182a3f090p+0, 0x1.a5503b23e255dp+0,
+    0x1.ae89f995ad3adp+0, 0x1.b7f76f2fb5e47p+0, 0x1.c199bdd85529cp+0, 0x1.cb720dcef9069p+0,
+    0x1.d5818dcfba487p+0, 0x1.dfc97337b9b5fp+0, 0x1.ea4afa2a490dap+0, 0x1.f50765b6e4540p+0};
+__device__ __forceinline__ double exp_tab(double x, const double *tab) {
+    constexpr double kShift = 0x1.8p52, kInvL = 0x1.71547652b82fep+5;
+    constexpr double kLhi = 0x1.62e42fefa2000p-6, kLlo = 0x1.9ef35793c7673p-46;
+    const double t = fma(x, kInvL, kShift);
+    const int N = __double2loint(t);
+    const double Nd = t - kShift;
+    double r = fma(-Nd, kLhi, x);
+    r = fma(-Nd, kLlo, r);
+    double q = fma(r, 1.0 / 720.0, 1.0 / 120.0);
+    q = fma(q, r, 1.0 / 24.0);
+    q = fma(q, r, 1.0 / 6.0);
+    q = fma(q, r, 0.5);
+    q = fma(q, r, 1.0);
+    q *= r;
+    const double T = tab[N & 31];
+    const double s = __hiloint2double(((N >> 5) + 1023) << 20, 0);
+    return fma(T, q, T) * s;
+}
+
 // OneMinusphi_L_and_chi_L / OneMinusphi_R_and_chi_R, src/FreqFactors.jl:54-133, in FP64.
 // Every caller clamps P to [-Pmax, Pmax] first (src/FreqFactors.jl:248-250), so the reference's
 // |P| >= Pmax branches only ever see P = +-Pmax, where they return exp(-+Pmax) and
@@ -368,15 +404,16 @@ __device__ __forceinline__ R d_colon_grad_u(R Drr, R DrZ, R DZZ, R a, R b, R c, 
 // between the exponential and the second-order Taylor form below |P| = Pmin, taken here by a
 // select on values the warp computes for every lane, so lanes of one warp never take
 // different paths (at P = 0 the unused general value is not finite; the select drops it).
-__device__ __forceinline__ void omphi_L(double P, double &omp, double &chi) {
-    const double e = exp(-P);
+// The exponentials are exp_tab's (|P| <= Pmax = 40) with the table at `tab`.
+__device__ __forceinline__ void omphi_L(double P, double &omp, double &chi, const double *tab) {
+    const double e = exp_tab(-P, tab);
     const double x = (1.0 - e) * rcp<double>(P);
     const bool tay = fabs(P) < kPmin;
     omp = tay ? 1.0 - P + 0.5 * (P * P) : e;
     chi = tay ? 1.0 - 0.5 * P : x;
 }
-__device__ __forceinline__ void omphi_R(double P, double &omp, double &chi) {
-    const double e = exp(P);
+__device__ __forceinline__ void omphi_R(double P, double &omp, double &chi, const double *tab) {
+    const double e = exp_tab(P, tab);
     const double x = (1.0 - e) * rcp<double>(P);
     const bool tay = fabs(P) < kPmin;
     omp = tay ? 1.0 + P + 0.5 * (P * P) : e;
@@ -384,8 +421,9 @@ __device__ __forceinline__ void omphi_R(double P, double &omp, double &chi) {
 }
 // Both of the above at once for the same P (used for P_k, which needs phi^L and phi^R):
 // one exponential and one reciprocal of P serve the two.
-__device__ __forceinline__ void omphi_LR(double P, double &oL, double &xL, double &oR, double &xR) {
-    const double e = exp(-P);
+__device__ __forceinline__ void omphi_LR(double P, double &oL, double &xL, double &oR, double &xR,
+                                         const double *tab) {
+    const double e = exp_tab(-P, tab);
     const double ie = rcp<double>(e);
     const double iP = rcp<double>(P);
     const bool tay = fabs(P) < kPmin;

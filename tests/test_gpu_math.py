@@ -1,7 +1,8 @@
 """Accuracy of the device's FP64 arithmetic helpers (lyd_math_check) against the host's
 extended-precision arithmetic: the Newton-refined reciprocal and reciprocal square root the
 kernels use in place of IEEE division and square root, the root formed from the latter, and the
-closure chi(f) in the form the kernels evaluate."""
+closure chi(f) in the form the kernels evaluate, and the table-driven exponential of the
+frequency factors."""
 import numpy as np
 import pytest
 
@@ -53,3 +54,11 @@ def test_closure_chi():
     fl = f.astype(np.longdouble)
     want = (3 + 4 * fl * fl) / (5 + 2 * np.sqrt(4 - 3 * fl * fl))
     assert _rel(_run(3, f), want) < 5.0 * ULP
+
+
+def test_exponential_of_the_clamped_peclet_range():
+    rng = np.random.default_rng(5)
+    x = np.concatenate([np.linspace(-40.0, 40.0, 400_001), rng.uniform(-40.0, 40.0, 200_000),
+                        rng.uniform(-1e-3, 1e-3, 10_000), [0.0, -0.0, 40.0, -40.0]])
+    # half an ulp from the table entry, half from the final rounding, a little from e^r - 1
+    assert _rel(_run(4, x), np.exp(x.astype(np.longdouble))) < 1.5 * ULP
