@@ -187,14 +187,15 @@ struct FfIn {
 // phi / chi of one P and their P-derivatives with one exponential and one reciprocal
 // (OneMinusphi_L/R_and_chi_L/R, src/FreqFactors.jl:54-133). L: omp = e^-P, chi = (1 - omp)/P;
 // R: omp = e^P, chi = (1 - omp)/P; the clamp and Taylor branches as the forward takes them.
+// The exponentials are exp_tab's, as in the forward, with its table at `tab`.
 struct Omphi { double o, x, d_o, d_x; };
 template <bool LEFT>
-__device__ __forceinline__ Omphi omphi_d(double P) {
+__device__ __forceinline__ Omphi omphi_d(double P, const double *tab) {
     Omphi r;
     const double sg = LEFT ? -1.0 : 1.0;
     if (P >= kPmax || P <= -kPmax) {
         const double Pc = P >= kPmax ? kPmax : -kPmax;
-        r.o = exp(sg * Pc);
+        r.o = exp_tab(sg * Pc, tab);
         r.x = (1.0 - r.o) / Pc;
         r.d_o = 0.0; r.d_x = 0.0;
         return r;
@@ -206,7 +207,7 @@ __device__ __forceinline__ Omphi omphi_d(double P) {
         r.d_x = -0.5;
         return r;
     }
-    r.o = exp(sg * P);
+    r.o = exp_tab(sg * P, tab);
     const double iP = rcp<double>(P);
     r.x = (1.0 - r.o) * iP;
     r.d_o = sg * r.o;
@@ -214,13 +215,13 @@ __device__ __forceinline__ Omphi omphi_d(double P) {
     return r;
 }
 // Both sides of the same P: e^P = 1 / e^-P and one reciprocal of P serve the two.
-__device__ __forceinline__ void omphi_d_LR(double P, Omphi &L, Omphi &R_) {
+__device__ __forceinline__ void omphi_d_LR(double P, Omphi &L, Omphi &R_, const double *tab) {
     if (P >= kPmax || P <= -kPmax || fabs(P) < kPmin) {
-        L = omphi_d<true>(P);
-        R_ = omphi_d<false>(P);
+        L = omphi_d<true>(P, tab);
+        R_ = omphi_d<false>(P, tab);
         return;
     }
-    const double e = exp(-P), ie = rcp<double>(e), iP = rcp<double>(P);
+    const double e = exp_tab(-P, tab), ie = rcp<double>(e), iP = rcp<double>(P);
     L.o = e; L.x = (1.0 - e) * iP; L.d_o = -e; L.d_x = (e - L.x) * iP;
     R_.o = ie; R_.x = (1.0 - ie) * iP; R_.d_o = ie; R_.d_x = (-ie - R_.x) * iP;
 }
@@ -250,7 +251,7 @@ __device__ __forceinline__ void ff_fwd(const FfIn &q, double &Fp, double &F0, do
 }
 
 __device__ __forceinline__ void ff_adj(const FfIn &q, double gFp, double gF0, double gFm, double &gvel, double &gKkm,
-                                       double &gKk, double &gKkp, double &grec0) {
+                                       double &gKk, double &gKkp, double &grec0, const double *tab) {
     double iKkm = rcp<double>(q.Kkm), iKk = rcp<double>(q.Kk), iKkp = rcp<double>(q.Kkp);
     double Ckp = q.vel * q.nCkp, Ck = q.vel * q.nCk, Ckm = q.vel * q.nCkm;
     const double ekp = q.rec0 - 2.0 * q.ICkp, ek = q.rec0 - 2.0 * q.ICk, ekm = q.rec0 - 2.0 * q.ICkm;
@@ -264,9 +265,9 @@ __device__ __forceinline__ void ff_adj(const FfIn &q, double gFp, double gF0, do
     double Pkp = fmin(fmax(Pkp0, -kPmax), kPmax);
     double Pk = fmin(fmax(Pk0, -kPmax), kPmax);
     double Pkm = fmin(fmax(Pkm0, -kPmax), kPmax);
-    const Omphi Rkp = omphi_d<false>(Pkp), Lkm = omphi_d<true>(Pkm);
+    const Omphi Rkp = omphi_d<false>(Pkp, tab), Lkm = omphi_d<true>(Pkm, tab);
     Omphi Lk, Rk;
-    omphi_d_LR(Pk, Lk, Rk);
+    omphi_d_LR(Pk, Lk, Rk, tab);
     double Dp = Lk.x * rk - Rkp.x * rkp, Dm = Lkm.x * rkm - Rk.x * rk;
     const double iDp = rcp<double>(Dp), iDm = rcp<double>(Dm);
     double dkp = q.idn * iDp, dkm = q.idn * iDm;
@@ -503,7 +504,7 @@ __global__ void __launch_bounds__(ADJ_THREADS, 2) k_freq_adj(FreqAdjArgs a) {
             q.DNKM = a.nu[k] - a.nuC[k - 1]; q.DNK = a.nu[k + 1] - a.nuC[k]; q.DNKP = a.nuC[k + 1] - a.nu[k + 1];
             q.idn = a.inv_dnu[k]; q.rec0 = rec0; q.recoil = a.recoil;
             double gvel = 0.0;
-            ff_adj(q, Fp[m], F0[m], Fm[m], gvel, gKtoM[m], gKown[m], gKtoP[m], grec0);
+            ff_adj(q, Fp[m], F0[m], Fm[m], gvel, gKtoM[m], gKown[m], gKtoP[m], grec0, etab);
             // vel = D:grad u / c with D from (H_r, H_Z, J) after emission
             double Drr, DZZ, DrZ;
             D_edd<double>(Hr1[m], HZ1[m], J1[m], jeps, a.heps2, Drr, DZZ, DrZ);

@@ -462,24 +462,4 @@ __device__ __forceinline__ void adj_cell_f(double J, double Hr, double HZ, doubl
     if (jf) gJ += -(g.fr * Hr + g.fZ * HZ) * iJ * iJ;
 }
 
-// OneMinusphi_{L,R}_and_chi_{L,R} derivatives (src/FreqFactors.jl:54-133): d omp/dP, d chi/dP
-__device__ __forceinline__ void d_omphi_L(double P, double &domp, double &dchi) {
-    if (P >= kPmax || P <= -kPmax) { domp = 0.0; dchi = 0.0; return; }
-    if (fabs(P) < kPmin) { domp = -1.0 + P; dchi = -0.5; return; }
-    double omp = exp(-P);
-    const double iP = rcp<double>(P);
-    double chi = (1.0 - omp) * iP;
-    domp = -omp;
-    dchi = (omp - chi) * iP;
-}
-__device__ __forceinline__ void d_omphi_R(double P, double &domp, double &dchi) {
-    if (P >= kPmax || P <= -kPmax) { domp = 0.0; dchi = 0.0; return; }
-    if (fabs(P) < kPmin) { domp = 1.0 + P; dchi = -0.5; return; }
-    double omp = exp(P);
-    const double iP = rcp<double>(P);
-    double chi = (1.0 - omp) * iP;
-    domp = omp;
-    dchi = (-omp - chi) * iP;
-}
-
 }  // namespace lyd
