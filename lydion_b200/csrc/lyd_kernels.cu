@@ -932,20 +932,34 @@ enum { CS_ALPHA, CS_ALPHA_C, CS_PD, CS_JS, CS_PHI_INV, CS_ALPHA_CF, CS_T, CS_DUR
 // shared memory for one CTA per SM).
 template <int M> __host__ __device__ constexpr bool freq_prefetch() { return M <= 2; }
 
-// Shared memory of the frequency kernel, in doubles: FP64 per-k constants, per-warp reduction
-// rows, per-warp staged cell inputs, the per-warp prefetch buffers, and the lane-serial
-// solver rows when that solver runs.
+// Shared memory of the frequency kernel, in doubles: FP64 per-k constants, the per-warp
+// reduction rows (without prefetch; with it, each warp's row lies in its own prefetch area,
+// free once the warp's cells are done), per-warp staged cell inputs, the per-warp prefetch
+// buffers (two slots of `ns` rows: 4, or 5 when J_old is not J's own buffer), and the
+// lane-serial solver rows when that solver runs: 72 KB per CTA at two bins per lane with J_old
+// aliased (86.5 KB before the overlay and the fourth row), which leaves L1 the difference. A
+// third CTA per SM would fit, but its 80-register bound spills in the cell loop (FP64 at
+// 256^2 x 64: 0.258 ms against 0.184 ms at two CTAs).
 template <int M>
-__host__ __device__ constexpr int freq_smem_off_cs(int nwarps) { return KC_N * 32 * M + nwarps * (32 * M + 8); }
+__host__ __device__ constexpr int freq_smem_off_cs(int nwarps) {
+    return KC_N * 32 * M + (freq_prefetch<M>() ? 0 : nwarps * (32 * M + 8));
+}
 template <int M>
 __host__ __device__ constexpr int freq_smem_off_pf(int nwarps) { return freq_smem_off_cs<M>(nwarps) + nwarps * CS_N * 32; }
 template <int M>
-__host__ __device__ constexpr int freq_smem_off_tsm(int nwarps) {
-    return freq_smem_off_pf<M>(nwarps) + (freq_prefetch<M>() ? nwarps * 2 * 5 * 32 * M : 0);
+__host__ __device__ constexpr int freq_pf_warp(int ns) { return 2 * ns * 32 * M; }   // doubles per warp
+template <int M>
+__host__ __device__ constexpr int freq_smem_off_tsm(int nwarps, int ns) {
+    return freq_smem_off_pf<M>(nwarps) + (freq_prefetch<M>() ? nwarps * freq_pf_warp<M>(ns) : 0);
 }
 template <int M>
-__host__ __device__ constexpr int freq_smem_doubles(int nwarps, bool thomas) {
-    return freq_smem_off_tsm<M>(nwarps) + (thomas ? nwarps * 4 * 32 * M : 0);
+__host__ __device__ constexpr int freq_smem_doubles(int nwarps, bool thomas, int ns) {
+    return freq_smem_off_tsm<M>(nwarps, ns) + (thomas ? nwarps * 4 * 32 * M : 0);
+}
+template <int M>
+__host__ __device__ inline double *freq_red_row(double *fsm, int nwarps, int ns, int w) {
+    return freq_prefetch<M>() ? fsm + freq_smem_off_pf<M>(nwarps) + w * freq_pf_warp<M>(ns)
+                              : fsm + KC_N * 32 * M + w * (32 * M + 8);
 }
 
 // A lane's M contiguous bins of one row as whole 16-byte words, when the row layout allows it
@@ -1001,9 +1015,10 @@ template <typename S, typename R, int M, typename RC>
 __device__ __forceinline__ void freq_item(const FreqArgs<S> &a, int item, int nitems, double *fsm, int nw) {
     constexpr int NP = 32 * M;
     constexpr bool PF = freq_prefetch<M>();
-    double *kc = fsm;                              // [KC_N][NP]
-    double *red = fsm + KC_N * NP;                 // [nwarps][NP + 8]
-    double *tsm = fsm + freq_smem_off_tsm<M>(nw);  // [nwarps][4][NP] (lane-serial solver)
+    const bool jo_alias = a.Jold == a.Jin;
+    const int ns = jo_alias ? 4 : 5;               // prefetched rows per cell
+    double *kc = fsm;                                  // [KC_N][NP]
+    double *tsm = fsm + freq_smem_off_tsm<M>(nw, ns);  // [nwarps][4][NP] (lane-serial solver)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nnu = a.nnu;
     for (int t = threadIdx.x; t < NP; t += blockDim.x) {
@@ -1039,8 +1054,7 @@ __device__ __forceinline__ void freq_item(const FreqArgs<S> &a, int item, int ni
     int wbeg, wend;
     warp_cell_run(it, warp, nw, wbeg, wend);
     double *cs = fsm + freq_smem_off_cs<M>(nw) + warp * CS_N * 32;      // [CS_N][32]
-    S *pf = reinterpret_cast<S *>(fsm + freq_smem_off_pf<M>(nw)) + warp * 2 * 5 * NP;  // [2][5][NP]
-    const bool jo_alias = a.Jold == a.Jin;
+    S *pf = reinterpret_cast<S *>(fsm + freq_smem_off_pf<M>(nw) + warp * freq_pf_warp<M>(ns));  // [2][ns][NP]
     const bool need_ff = a.do_freq && a.update_ff, need_js = a.do_emission || (a.parts & PART_DIAG);
     // With `vec`, every lane's M bins of a row are whole 16-byte words in global and shared
     // memory (row starts 16-byte aligned, n_nu a multiple of M): rows move as 16-byte copies,
@@ -1051,7 +1065,7 @@ __device__ __forceinline__ void freq_item(const FreqArgs<S> &a, int item, int ni
     // copies of cell cl's bin rows into prefetch buffer b
     auto issue = [&](int cl, int b) {
         const long long base = o3 + (long long)cl * nnu;
-        S *d = pf + b * 5 * NP;
+        S *d = pf + b * ns * NP;
         if constexpr (LR::ok) {
             if (vec) {
                 if (lane * M < nnu) {
@@ -1159,7 +1173,7 @@ __device__ __forceinline__ void freq_item(const FreqArgs<S> &a, int item, int ni
             if (cl + 1 < wend) issue(cl + 1, b ^ 1);
             cp_async_commit();
             cp_async_wait<1>();                   // this cell's copies (each lane reads its own)
-            const S *d = pf + b * 5 * NP;
+            const S *d = pf + b * ns * NP;
             bool done = false;
             if constexpr (LR::ok) {
                 if (vec) {
@@ -1428,10 +1442,13 @@ __device__ __forceinline__ void freq_item(const FreqArgs<S> &a, int item, int ni
     if (bad) atomicOr(a.err, bad);
     if (!a.parts) return;
     // ---- CTA reduction of the partials, fixed order ----
-    const int stride = NP + 8;
+    // (the warp's own row: with prefetch it overlays the warp's prefetch area, whose last copies
+    // landed above)
+    double *red = freq_red_row<M>(fsm, nw, ns, warp);
+    __syncwarp();
     if (warp < nw) {
 #pragma unroll
-        for (int m = 0; m < M; m++) red[warp * stride + lane * M + m] = acc_e[m];
+        for (int m = 0; m < M; m++) red[lane * M + m] = acc_e[m];
     }
     acc_tot = warp_sum(acc_tot);
     acc_esc = warp_sum(acc_esc);
@@ -1440,19 +1457,19 @@ __device__ __forceinline__ void freq_item(const FreqArgs<S> &a, int item, int ni
     acc_out = warp_sum(acc_out);
     acc_L = warp_sum(acc_L);
     if (lane == 0 && warp < nw) {
-        red[warp * stride + NP + 0] = acc_tot;
-        red[warp * stride + NP + 1] = acc_mf;
-        red[warp * stride + NP + 2] = acc_net;
-        red[warp * stride + NP + 3] = acc_out;
-        red[warp * stride + NP + 4] = acc_L;
-        red[warp * stride + NP + 5] = acc_esc;
+        red[NP + 0] = acc_tot;
+        red[NP + 1] = acc_mf;
+        red[NP + 2] = acc_net;
+        red[NP + 3] = acc_out;
+        red[NP + 4] = acc_L;
+        red[NP + 5] = acc_esc;
     }
     __syncthreads();
     const int ncols = nnu + kExtraCols;
     for (int col = threadIdx.x; col < ncols; col += blockDim.x) {
         int src = col < nnu ? col : NP + (col - nnu);
         double s = 0.0;
-        for (int w2 = 0; w2 < nw; w2++) s += red[w2 * stride + src];
+        for (int w2 = 0; w2 < nw; w2++) s += freq_red_row<M>(fsm, nw, ns, w2)[src];
         a.partials[(size_t)col * nitems + item] = s;
     }
 }
@@ -1755,10 +1772,11 @@ static void freq_launch(const void *args, int nitems, cudaStream_t st) {
     fa.vec16 = LaneRow<S, M>::ok && fa.nnu % M == 0 && (fa.nnu * sizeof(S)) % 16 == 0 && al16(fa.Jin) &&
                al16(fa.Hrin) && al16(fa.HZin) && al16(fa.Jold) && al16(fa.Hv) && al16(fa.Jout) && al16(fa.Hrout) &&
                al16(fa.HZout);
-    const size_t sm = sizeof(double) * freq_smem_doubles<M>(FREQ_THREADS / 32, fa.solver == SOLVER_THOMAS);
+    const int ns = fa.Jold == fa.Jin ? 4 : 5;
+    const size_t sm = sizeof(double) * freq_smem_doubles<M>(FREQ_THREADS / 32, fa.solver == SOLVER_THOMAS, ns);
     static bool attr = false;
     if (!attr) {
-        const size_t smax = sizeof(double) * freq_smem_doubles<M>(FREQ_THREADS / 32, true);
+        const size_t smax = sizeof(double) * freq_smem_doubles<M>(FREQ_THREADS / 32, true, 5);
         cudaFuncSetAttribute(k_freq<S, R, M, RC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
         attr = true;
     }
@@ -1831,7 +1849,8 @@ static cudaError_t persist_launch(const void *adv, const void *freq, const RedAr
     p.err = err;
     auto kern = k_step_persistent<S, RA, RF, RC, FLUX, M>;
     const size_t sa = adv_smem_bytes<S, RA, false>();
-    const size_t sf = sizeof(double) * freq_smem_doubles<M>(FREQ_THREADS / 32, p.freq.solver == SOLVER_THOMAS);
+    const size_t sf = sizeof(double) * freq_smem_doubles<M>(FREQ_THREADS / 32, p.freq.solver == SOLVER_THOMAS,
+                                                            p.freq.Jold == p.freq.Jin ? 4 : 5);
     const size_t sm = sa > sf ? sa : sf;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
