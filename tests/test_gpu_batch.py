@@ -159,3 +159,30 @@ def test_autotune_applies_a_valid_shape(tmp_path):
     assert t[1] == 0 and got[1] < 0 or got[1] == t[1]
     h = b.batch_steps(2, pp)
     assert np.isfinite(h).all()
+
+
+def test_ragged_batch_distribution_matches_oracle(oracle_mod):
+    """The first 32 clouds of the 512-cloud ragged batch (its own generator and seed: sides
+    32..256 drawn independently in r and Z, tau0 1e4..1e8, T 1e2..1e4 K, dust, outflows up to
+    100 km/s; 48 bins; 20.3M cell-bins), 20 steps in one batch context, against the oracle
+    cloud by cloud: windows exact, L to 1e-13, the force multipliers floored to 1e-9, J and H
+    to 1e-9 of their maxima. The net radial multiplier is a signed sum that crosses zero in
+    some clouds (cloud 20: from -1.8e-3 to +1.5e-3 between two steps, against outward and
+    inward parts of 1.3 each), so it is held to 1e-9 of the same step's M_F, the sum of the
+    magnitudes of its terms."""
+    from lydion_b200.m1 import cloud_params
+    clouds = W.batch_clouds(n_clouds=32)
+    b, states = _batch(oracle_mod, clouds, seed=17)
+    n = 20
+    hist = b.batch_steps(n, cloud_params(clouds))
+    for q, (c, st) in enumerate(zip(clouds, states)):
+        d_o = st.run(n)
+        d_g = hist[:, q, :]
+        np.testing.assert_array_equal(d_g[:, 5:7], d_o[:, 5:7], err_msg=str(q))
+        np.testing.assert_allclose(d_g[:, 3], d_o[:, 3], rtol=1e-13, err_msg=str(q))
+        for col in (0, 2):
+            assert max_rel(d_g[5:, col], d_o[5:, col], floor=1e-9 * np.abs(d_o[:, col]).max()) < 1e-9, (q, col)
+        assert np.all(np.abs(d_g[:, 1] - d_o[:, 1]) <= 1e-9 * d_o[:, 0]), (q, d_g[:, 1] - d_o[:, 1])
+        for f in ("J", "H_r", "H_Z"):
+            assert norm_err(b.download_cloud(q, f), getattr(st, f)) < 1e-9, (q, f)
+    b.close()
