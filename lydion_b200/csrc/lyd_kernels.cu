@@ -205,6 +205,21 @@ template <typename R> __host__ __device__ constexpr int nf() { return 4; }
 constexpr int HRING = 3;
 __host__ __device__ constexpr int hslot(int r) { return ((r % HRING) + HRING) % HRING; }
 
+// The staged-cell ring A: [RING][MCOL][nf][32] (staged column lc, ring slot of the row), or with
+// H1 the own columns' ring [RING][MT][nf][32] followed by one row of the four halo columns
+// (lc 0, 1, MT+2, MT+3) [4][nf][32]: with per-lane staging the halo of row j is staged for and
+// read by row j's r faces alone, so one row of it suffices (12 KB less in FP64).
+template <typename R, bool H1>
+__device__ __forceinline__ R *a_cell(R *A, int slot, int lc) {
+    if constexpr (H1) {
+        if (lc >= 2 && lc < MT + 2) return A + ((slot * MT + (lc - 2)) * nf<R>()) * 32;
+        return A + ((RING * MT + (lc < 2 ? lc : lc - MT)) * nf<R>()) * 32;
+    } else {
+        return A + ((slot * MCOL + lc) * nf<R>()) * 32;
+    }
+}
+template <typename R, bool H1> __host__ __device__ constexpr int a_cells() { return H1 ? RING * MT + 4 : RING * MCOL; }
+
 template <typename S, typename R>
 __device__ __forceinline__ Cell<R> raw_cell(const AdvArgs<S> &a, const View &v, int col, int row, int k) {
     if (col < 0 || col >= v.nr) return r_cell<S, R>(a, v, col, row, k);
@@ -215,7 +230,7 @@ __device__ __forceinline__ Cell<R> raw_cell(const AdvArgs<S> &a, const View &v, 
 // Stage cell (col, row) into ring slot `slot`, staged column lc (= col - i0 + 2): the flux
 // inputs in the arithmetic type R, and for the tile's own columns the state (J, H_r, H_Z) in
 // the storage type S, which the cell update accumulates into.
-template <typename S, typename R>
+template <typename S, typename R, bool H1>
 __device__ __forceinline__ void stage_cell(const AdvArgs<S> &a, const View &v, R *A, S *Hh, int slot, int lc,
                                            int col, int row, int k, int lane, R jeps) {
     Cell<S> c = raw_cell<S, S>(a, v, col, row, k);
@@ -227,11 +242,93 @@ __device__ __forceinline__ void stage_cell(const AdvArgs<S> &a, const View &v, R
         aF = alpha_F<S, R>(a, v, cc, rr, k);
     }
     CellF<R> f = cell_f<R>(R(c.J), R(c.Hr), R(c.HZ), jeps);
-    R *p = A + ((slot * MCOL + lc) * nf<R>()) * 32 + lane;
+    R *p = a_cell<R, H1>(A, slot, lc) + lane;
     p[0] = f.J; p[32] = f.fr; p[64] = f.fZ;
     if (nf<R>() == 4) p[96] = aF;
     if (lc >= 2 && lc < 2 + MT) {
         // the state in S; with S == R the ring's J is the state's J
+        constexpr int HF = sizeof(S) == sizeof(R) ? 2 : 3;
+        S *q = Hh + ((hslot(row) * MT + (lc - 2)) * HF) * 32 + lane;
+        q[0] = c.Hr; q[32] = c.HZ;
+        if (HF == 3) q[64] = c.J;
+    }
+}
+
+// ---- a row ahead by cp.async (FP64 arithmetic with per-lane staging) ----
+// The cell a staged stencil cell (col, row) copies, and the boundary rules that r_cell / z_cell
+// apply to the copy: rr for H_r, rz for H_Z (1: negate; 2: keep the part <= 0; 3: keep the
+// part >= 0). A corner cell (ghost in both directions) is never staged.
+struct CellSrc { int i, j, rr, rz; };
+__device__ __forceinline__ CellSrc cell_src(const View &v, int col, int row) {
+    CellSrc s{col, row, 0, 0};
+    if (col < 0) {
+        if (v.bcl == 0) { s.i = -1 - col; s.rr = 1; } else { s.i = 0; s.rr = 2; }
+    } else if (col >= v.nr) {
+        if (v.bcr == 0) { s.i = 2 * v.nr - 1 - col; s.rr = 1; } else { s.i = v.nr - 1; s.rr = 3; }
+    } else if (row < 0) {
+        if (v.bzb == 0) { s.j = -1 - row; s.rz = 1; } else { s.j = 0; s.rz = 2; }
+    } else if (row >= v.nz) {
+        if (v.bzt == 0) { s.j = 2 * v.nz - 1 - row; s.rz = 1; } else { s.j = v.nz - 1; s.rz = 3; }
+    }
+    return s;
+}
+template <typename S>
+__device__ __forceinline__ S bc_rule(S h, int rule) {
+    if (rule == 1) return -h;
+    if (rule == 2) return h < S(0) ? h : S(0);
+    if (rule == 3) return h > S(0) ? h : S(0);
+    return h;
+}
+// A raw slot holds one staged cell's inputs as copied: [4][32] values of the storage type
+// (J, H_r, H_Z of the cell it mirrors, and alpha_F, or H_voigt when alpha_F is derived, of the
+// in-grid cell it clamps to) and two doubles (alpha and alpha_cF of that cell).
+constexpr int RAW_SLOT = 4 * 32 + 2;   // doubles (storage FP64)
+
+// Copies of staged cell (col, row)'s inputs into the raw slot `dst` (cp.async, one 8-byte copy
+// per value; lanes outside the active bins copy no bin values; lane 0 copies the per-cell ones).
+template <typename S>
+__device__ __forceinline__ void raw_issue(const AdvArgs<S> &a, const View &v, S *dst, int col, int row, int k,
+                                          int lane, bool kact) {
+    const CellSrc s = cell_src(v, col, row);
+    const int cc = col < 0 ? 0 : (col >= v.nr ? v.nr - 1 : col);
+    const int rr = row < 0 ? 0 : (row >= v.nz ? v.nz - 1 : row);
+    const long long cla = (long long)cc + (long long)v.nr * rr;
+    if (kact) {
+        const long long x = v.o3 + (long long)k + (long long)a.nnu * ((long long)s.i + (long long)v.nr * s.j);
+        const long long xa = v.o3 + (long long)k + (long long)a.nnu * cla;
+        cp_async_el(dst + lane, a.J + x);
+        cp_async_el(dst + 32 + lane, a.Hr + x);
+        cp_async_el(dst + 64 + lane, a.HZ + x);
+        cp_async_el(dst + 96 + lane, a.aF ? a.aF + xa : a.Hv + xa);
+    }
+    if (lane == 0 && !a.aF) {
+        double *dsc = reinterpret_cast<double *>(dst + 128);
+        cp_async_el(dsc, a.alpha + v.oc + cla);
+        if (a.alpha_cF) cp_async_el(dsc + 1, a.alpha_cF + v.oc + cla);
+    }
+}
+// stage_cell from a raw slot that raw_issue filled (its copies complete and visible to the
+// warp): the same values through the same arithmetic.
+template <typename S, typename R, bool H1>
+__device__ __forceinline__ void stage_raw(const AdvArgs<S> &a, const View &v, const S *src, R *A, S *Hh, int slot,
+                                          int lc, int col, int row, int lane, R jeps) {
+    const CellSrc s = cell_src(v, col, row);
+    Cell<S> c;
+    c.J = src[lane];
+    c.Hr = bc_rule(src[32 + lane], s.rr);
+    c.HZ = bc_rule(src[64 + lane], s.rz);
+    R aF;
+    if (a.aF) {
+        aF = R(src[96 + lane]);
+    } else {
+        const double *dsc = reinterpret_cast<const double *>(src + 128);
+        aF = R(dsc[0]) * R(src[96 + lane]);
+        if (a.alpha_cF) aF = aF + R(dsc[1]);
+    }
+    CellF<R> f = cell_f<R>(R(c.J), R(c.Hr), R(c.HZ), jeps);
+    R *p = a_cell<R, H1>(A, slot, lc) + lane;
+    p[0] = f.J; p[32] = f.fr; p[64] = f.fZ; p[96] = aF;
+    if (lc >= 2 && lc < 2 + MT) {
         constexpr int HF = sizeof(S) == sizeof(R) ? 2 : 3;
         S *q = Hh + ((hslot(row) * MT + (lc - 2)) * HF) * 32 + lane;
         q[0] = c.Hr; q[32] = c.HZ;
@@ -249,7 +346,7 @@ __host__ __device__ constexpr int raw_tile_bytes() { return 3 * MCOL * 32 * (int
 // Stage cell (col, row) into ring slot `slot` from the raw tile, applying the ghost-cell rules
 // of r_cell / z_cell: a ghost column takes the column it mirrors from the same tile (every such
 // column lies in the tile: i0 < n_r), a ghost row's H_Z gets the rule of its boundary.
-template <typename S, typename R>
+template <typename S, typename R, bool H1>
 __device__ __forceinline__ void stage_from_raw(const AdvArgs<S> &a, const View &v, const S *raw, R *A, S *Hh,
                                                int slot, int lc, int col, int row, int k, int lane, R jeps, int i0) {
     int sc = lc;
@@ -279,7 +376,7 @@ __device__ __forceinline__ void stage_from_raw(const AdvArgs<S> &a, const View &
         aF = alpha_F<S, R>(a, v, cc, rr, k);
     }
     CellF<R> f = cell_f<R>(R(c.J), R(c.Hr), R(c.HZ), jeps);
-    R *p = A + ((slot * MCOL + lc) * nf<R>()) * 32 + lane;
+    R *p = a_cell<R, H1>(A, slot, lc) + lane;
     p[0] = f.J; p[32] = f.fr; p[64] = f.fZ;
     if (nf<R>() == 4) p[96] = aF;
     if (lc >= 2 && lc < 2 + MT) {
@@ -291,9 +388,9 @@ __device__ __forceinline__ void stage_from_raw(const AdvArgs<S> &a, const View &
 }
 
 // A staged cell; with FP32 arithmetic also its alpha_F from the ring.
-template <typename R>
+template <typename R, bool H1>
 __device__ __forceinline__ CellF<R> staged(const R *A, int slot, int lc, int lane, R &aF) {
-    const R *p = A + ((slot * MCOL + lc) * nf<R>()) * 32 + lane;
+    const R *p = a_cell<R, H1>(const_cast<R *>(A), slot, lc) + lane;
     CellF<R> c;
     c.J = p[0]; c.fr = p[32]; c.fZ = p[64];
     if (nf<R>() == 4) aF = p[96];
@@ -305,16 +402,16 @@ __device__ __forceinline__ CellF<R> staged(const R *A, int slot, int lc, int lan
 // they load them from global memory where they are used and ignore the two pointers.
 // r face f (between cells f-1 and f) of row j held in ring slot `slot`; wl = f - i0 is the
 // staged column of the stencil's first cell (src/AdvectJandH.jl:641-968).
-template <typename S, typename R, int FLUX>
+template <typename S, typename R, int FLUX, bool H1>
 __device__ __forceinline__ void face_r_staged(const AdvArgs<S> &a, const View &v, const R *A, int slot, int wl,
                                               int f, int j, int k, int lane, R jeps, const double *up,
                                               const double *riv, R *F, R &kL, R &kR) {
     const double us = *up;
     R d0, aFi, aFp, d3;
-    CellF<R> cm1 = staged<R>(A, slot, wl, lane, d0);
-    CellF<R> ci = staged<R>(A, slot, wl + 1, lane, aFi);
-    CellF<R> cp1 = staged<R>(A, slot, wl + 2, lane, aFp);
-    CellF<R> cp2 = staged<R>(A, slot, wl + 3, lane, d3);
+    CellF<R> cm1 = staged<R, H1>(A, slot, wl, lane, d0);
+    CellF<R> ci = staged<R, H1>(A, slot, wl + 1, lane, aFi);
+    CellF<R> cp1 = staged<R, H1>(A, slot, wl + 2, lane, aFp);
+    CellF<R> cp2 = staged<R, H1>(A, slot, wl + 3, lane, d3);
     R iv[5];
 #pragma unroll
     for (int t = 0; t < 5; t++) iv[t] = R(riv[t]);
@@ -334,15 +431,15 @@ __device__ __forceinline__ void face_r_staged(const AdvArgs<S> &a, const View &v
 }
 
 // Z face f (between rows f-1 and f) of column i, staged column lc (src/AdvectJandH.jl:978-1289).
-template <typename S, typename R, int FLUX>
+template <typename S, typename R, int FLUX, bool H1>
 __device__ __forceinline__ void face_z_staged(const AdvArgs<S> &a, const View &v, const R *A, int lc, int i, int f,
                                               int k, int lane, R jeps, const double *ivz, const double *up, R *F) {
     const double us = *up;
     R d0, aFi, aFp, d3;
-    CellF<R> cm1 = staged<R>(A, (f + 2) & (RING - 1), lc, lane, d0);     // row f-2
-    CellF<R> ci = staged<R>(A, (f + 3) & (RING - 1), lc, lane, aFi);     // row f-1
-    CellF<R> cp1 = staged<R>(A, f & (RING - 1), lc, lane, aFp);          // row f
-    CellF<R> cp2 = staged<R>(A, (f + 1) & (RING - 1), lc, lane, d3);     // row f+1
+    CellF<R> cm1 = staged<R, H1>(A, (f + 2) & (RING - 1), lc, lane, d0);     // row f-2
+    CellF<R> ci = staged<R, H1>(A, (f + 3) & (RING - 1), lc, lane, aFi);     // row f-1
+    CellF<R> cp1 = staged<R, H1>(A, f & (RING - 1), lc, lane, aFp);          // row f
+    CellF<R> cp2 = staged<R, H1>(A, (f + 1) & (RING - 1), lc, lane, d3);     // row f+1
     R iv[5];
 #pragma unroll
     for (int t = 0; t < 5; t++) iv[t] = R(ivz[t]);
@@ -407,11 +504,21 @@ __device__ __forceinline__ double geo_fetch(const double *src, int stride, int j
 }
 
 // Shared memory of the advection tile before the bulk-copy staging area, in bytes.
-template <typename S, typename R>
+// PFR: every staged input copied a row ahead by per-lane cp.async into raw slots (the own
+// column's row j+3 and warp 8's halo cells of row j+1, while row j's faces and update run),
+// with the one-row halo ring of a_cell paying for the slots: FP64 arithmetic with per-lane
+// staging, 76 KB per CTA, three CTAs per SM. FP64 advection 0.288 -> 0.282 ms at 256^2 x 64,
+// 1.219 -> 1.169 ms at 512^2 x 128, 4.82 -> 4.64 ms at 1024^2 x 128; bit for bit unchanged.
+template <typename R, bool TMA> __host__ __device__ constexpr bool adv_pfr() { return !TMA && sizeof(R) == 8; }
+
+// Shared memory of the advection tile before the bulk-copy staging area, in bytes (with PFR
+// the one-row halo ring and the raw slots).
+template <typename S, typename R, bool PFR>
 __host__ __device__ constexpr size_t adv_smem_base() {
-    return sizeof(R) * 32 * (RING * MCOL * nf<R>() + (MT + 1) * 5) +
+    return sizeof(R) * 32 * (a_cells<R, PFR>() * nf<R>() + (MT + 1) * 5) +
            sizeof(S) * 32 * HRING * MT * (sizeof(S) == sizeof(R) ? 2 : 3) +
-           sizeof(double) * (MWARPS * 2 * GEO_N + (MT + 1) * 5);   // the row slots, the r faces' intervals
+           sizeof(double) * (MWARPS * 2 * GEO_N + (MT + 1) * 5) +
+           (PFR ? sizeof(double) * (MT + 4) * RAW_SLOT : 0);
 }
 __host__ __device__ constexpr size_t adv_tma_off(size_t base) { return (base + 127) / 128 * 128; }
 
@@ -426,12 +533,14 @@ template <typename S, typename R, int FLUX, bool TMA>
 __device__ __forceinline__ void advect_tile(const AdvArgs<S> &a, int tile, unsigned char *adv_smem) {
     constexpr int HF = sizeof(S) == sizeof(R) ? 2 : 3;
     constexpr int NF = nf<R>();
-    R *A = reinterpret_cast<R *>(adv_smem);                            // [RING][MCOL][NF][32]
-    S *Hh = reinterpret_cast<S *>(A + RING * MCOL * NF * 32);           // [HRING][MT][HF][32]
+    constexpr bool PFR = adv_pfr<R, TMA>();
+    R *A = reinterpret_cast<R *>(adv_smem);                            // a_cells cells of [NF][32] (a_cell)
+    S *Hh = reinterpret_cast<S *>(A + a_cells<R, PFR>() * NF * 32);    // [HRING][MT][HF][32]
     R *Fr = reinterpret_cast<R *>(Hh + HRING * MT * HF * 32);           // [MT+1][5][32]
     double *geo = reinterpret_cast<double *>(Fr + (MT + 1) * 5 * 32);  // [MWARPS][2][GEO_N]: the row slots
     double *riv = geo + MWARPS * 2 * GEO_N;                             // [MT+1][5]: the r faces' intervals
-    constexpr size_t toff = adv_tma_off(adv_smem_base<S, R>());
+    double *rawp = riv + (MT + 1) * 5;                                  // PFR: [MT + 4][RAW_SLOT] raw slots
+    constexpr size_t toff = adv_tma_off(adv_smem_base<S, R, false>());
     S *raw = reinterpret_cast<S *>(adv_smem + toff);                                   // [3][MCOL][32]
     unsigned long long *bar = reinterpret_cast<unsigned long long *>(adv_smem + toff + raw_tile_bytes<S>());
     int *abort_flag = reinterpret_cast<int *>(bar + 1);
@@ -478,24 +587,41 @@ __device__ __forceinline__ void advect_tile(const AdvArgs<S> &a, int tile, unsig
         __syncthreads();
         if (threadIdx.x == 0 && j0 + 2 <= rlast) issue_row(j0 + 2);
     }
+    // PFR: the first row-ahead copies (the own column's row j0+2, warp 8's halo cells of row j0)
+    // go out before the prologue's own loads and are waited for at its end
+    S *rawo = reinterpret_cast<S *>(rawp + w * RAW_SLOT);   // own warps; halo cell q: slot MT + q
+    const int hl[4] = {0, 1, MT + 2, MT + 3};
+    if constexpr (PFR) {
+        if (own) {
+            const int r = j0 + 2;
+            if (r <= j1 + 1 && col <= v.nr + 1 && r <= v.nz + 1 && !(col >= v.nr && r >= v.nz))
+                raw_issue<S>(a, v, rawo, col, r, k, lane, kact);
+        } else if (j0 < j1) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int c2 = i0 - 2 + hl[q];
+                if (c2 <= v.nr + 1) raw_issue<S>(a, v, reinterpret_cast<S *>(rawp + (MT + q) * RAW_SLOT), c2, j0, k, lane, kact);
+            }
+        }
+        cp_async_commit();
+    }
     // prologue: own columns, rows j0-2 .. j0+1
     if (own && kact && col <= v.nr + 1) {
         for (int r = j0 - 2; r <= j0 + 1; r++) {
             bool gcol = col >= v.nr, grow = (r < 0 || r >= v.nz);
             if (r < -2 || r > v.nz + 1 || (gcol && grow)) continue;
-            stage_cell<S, R>(a, v, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps);
+            stage_cell<S, R, PFR>(a, v, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps);
         }
     }
     if constexpr (TMA) {
         // with bulk copies the halo columns of a row come with its copy, two rows before the
         // r faces read them: the prologue stages those of rows j0 and j0+1
         if (!own && kact) {
-            const int hl[4] = {0, 1, MT + 2, MT + 3};
             for (int r = j0; r <= j0 + 1 && r < j1 && r < v.nz; r++) {
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     int c2 = i0 - 2 + hl[q];
-                    if (c2 <= v.nr + 1) stage_cell<S, R>(a, v, A, Hh, r & (RING - 1), hl[q], c2, r, k, lane, jeps);
+                    if (c2 <= v.nr + 1) stage_cell<S, R, PFR>(a, v, A, Hh, r & (RING - 1), hl[q], c2, r, k, lane, jeps);
                 }
             }
         }
@@ -511,10 +637,11 @@ __device__ __forceinline__ void advect_tile(const AdvArgs<S> &a, int tile, unsig
         const int f = i0 + t / 5;
         riv[t] = f <= v.nr ? __ldg(a.rint + v.orint + 5 * f + t % 5) : 0.0;
     }
+    if constexpr (PFR) cp_async_wait<0>();
     __syncthreads();
     R zL[3] = {R(0), R(0), R(0)};
     if (own && kact && col < v.nr)
-        face_z_staged<S, R, FLUX>(a, v, A, w + 2, col, j0, k, lane, jeps, a.zint + v.ozint + 5 * j0,
+        face_z_staged<S, R, FLUX, PFR>(a, v, A, w + 2, col, j0, k, lane, jeps, a.zint + v.ozint + 5 * j0,
                                   a.u_Z_star + v.ozf + col + (long long)v.nr * j0, zL);   // face j0
 
     const double ctdt = v.ctdt;
@@ -548,14 +675,13 @@ __device__ __forceinline__ void advect_tile(const AdvArgs<S> &a, int tile, unsig
                     const bool grow = r >= v.nz;
                     if (own) {
                         if (col <= v.nr + 1 && !(col >= v.nr && grow))
-                            stage_from_raw<S, R>(a, v, raw, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps, i0);
+                            stage_from_raw<S, R, PFR>(a, v, raw, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps, i0);
                     } else if (!grow && r < j1) {
-                        const int hl[4] = {0, 1, MT + 2, MT + 3};
 #pragma unroll
                         for (int q = 0; q < 4; q++) {
                             int c2 = i0 - 2 + hl[q];
                             if (c2 <= v.nr + 1)
-                                stage_from_raw<S, R>(a, v, raw, A, Hh, r & (RING - 1), hl[q], c2, r, k, lane, jeps, i0);
+                                stage_from_raw<S, R, PFR>(a, v, raw, A, Hh, r & (RING - 1), hl[q], c2, r, k, lane, jeps, i0);
                         }
                     }
                 }
@@ -568,6 +694,38 @@ __device__ __forceinline__ void advect_tile(const AdvArgs<S> &a, int tile, unsig
             }
             // the raw tile is free again: fetch row j+3 while this row's faces and update run
             if (threadIdx.x == 0 && j + 3 <= rlast) issue_row(j + 3);
+        } else if constexpr (PFR) {
+            // (A) from the raw slots: the own column's row j+2 and warp 8's halo cells of row j,
+            // copied a row ago; then the copies of the next ones go out and land while this
+            // row's faces and update run (the wait at the end of the row)
+            if (own) {
+                const int r = j + 2;
+                if (kact && col <= v.nr + 1 && r <= v.nz + 1 && !(col >= v.nr && r >= v.nz))
+                    stage_raw<S, R, PFR>(a, v, rawo, A, Hh, r & (RING - 1), w + 2, col, r, lane, jeps);
+                __syncwarp();
+                const int rn = r + 1;
+                if (rn <= j1 + 1 && col <= v.nr + 1 && rn <= v.nz + 1 && !(col >= v.nr && rn >= v.nz))
+                    raw_issue<S>(a, v, rawo, col, rn, k, lane, kact);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const int c2 = i0 - 2 + hl[q];
+                    if (kact && c2 <= v.nr + 1)
+                        stage_raw<S, R, PFR>(a, v, reinterpret_cast<const S *>(rawp + (MT + q) * RAW_SLOT), A, Hh,
+                                             j & (RING - 1), hl[q], c2, j, lane, jeps);
+                }
+                __syncwarp();
+                if (j + 1 < j1) {
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const int c2 = i0 - 2 + hl[q];
+                        if (c2 <= v.nr + 1)
+                            raw_issue<S>(a, v, reinterpret_cast<S *>(rawp + (MT + q) * RAW_SLOT), c2, j + 1, k, lane, kact);
+                    }
+                }
+            }
+            cp_async_commit();
+            __syncthreads();
         } else {
             // (A) stage row j+2 of the own column; warp 8 stages the halo columns of row j (spread
             // over four warps instead, one halo cell each, the FP64 advection took 0.336 ms
@@ -577,14 +735,13 @@ __device__ __forceinline__ void advect_tile(const AdvArgs<S> &a, int tile, unsig
                     int r = j + 2;
                     bool gcol = col >= v.nr, grow = r >= v.nz;
                     if (col <= v.nr + 1 && r <= v.nz + 1 && !(gcol && grow))
-                        stage_cell<S, R>(a, v, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps);
+                        stage_cell<S, R, PFR>(a, v, A, Hh, r & (RING - 1), w + 2, col, r, k, lane, jeps);
                 } else {
-                    const int hl[4] = {0, 1, MT + 2, MT + 3};
 #pragma unroll
                     for (int q = 0; q < 4; q++) {
                         int c2 = i0 - 2 + hl[q];
                         if (c2 <= v.nr + 1)
-                            stage_cell<S, R>(a, v, A, Hh, j & (RING - 1), hl[q], c2, j, k, lane, jeps);
+                            stage_cell<S, R, PFR>(a, v, A, Hh, j & (RING - 1), hl[q], c2, j, k, lane, jeps);
                     }
                 }
             }
@@ -595,13 +752,13 @@ __device__ __forceinline__ void advect_tile(const AdvArgs<S> &a, int tile, unsig
         R zR[3] = {R(0), R(0), R(0)};
         if (kact && f <= v.nr) {
             R F[3], kL, kR;
-            face_r_staged<S, R, FLUX>(a, v, A, j & (RING - 1), w, f, j, k, lane, jeps, g + G_UR, riv + 5 * w, F,
+            face_r_staged<S, R, FLUX, PFR>(a, v, A, j & (RING - 1), w, f, j, k, lane, jeps, g + G_UR, riv + 5 * w, F,
                                       kL, kR);
             R *p = Fr + (w * 5) * 32 + lane;
             p[0] = F[0]; p[32] = F[1]; p[64] = F[2]; p[96] = kL; p[128] = kR;
         }
         if (own && kact && col < v.nr)
-            face_z_staged<S, R, FLUX>(a, v, A, w + 2, col, j + 1, k, lane, jeps, g + G_ZIV, g + G_UZ, zR);
+            face_z_staged<S, R, FLUX, PFR>(a, v, A, w + 2, col, j + 1, k, lane, jeps, g + G_ZIV, g + G_UZ, zR);
         __syncthreads();
         // (C) cell update, src/AdvectJandH.jl:1302-1382
         if (own && col < v.nr && k < a.nnu) {
@@ -613,7 +770,7 @@ __device__ __forceinline__ void advect_tile(const AdvArgs<S> &a, int tile, unsig
             } else {
                 const S *pH = Hh + ((hslot(j) * MT + w) * HF) * 32 + lane;
                 const S uHr = pH[0], uHZ = pH[32];
-                const S uJ = HF == 3 ? pH[64] : S(A[(((j & (RING - 1)) * MCOL + w + 2) * NF) * 32 + lane]);
+                const S uJ = HF == 3 ? pH[64] : S(a_cell<R, PFR>(A, j & (RING - 1), w + 2)[lane]);
                 const R sJ = R(uJ), sHr = R(uHr), sHZ = R(uHZ);
                 R Drr, DZZ, DrZ;
                 D_edd<R>(sHr, sHZ, sJ, jeps, R(a.heps2), Drr, DZZ, DrZ);
@@ -1698,8 +1855,8 @@ __global__ void __launch_bounds__(MTHREADS, 2) k_step_persistent(PersistArgs<S> 
 // ---- launch wrappers ----------------------------------------------------------------------
 template <typename S, typename R, bool TMA>
 static size_t adv_smem_bytes() {
-    if (!TMA) return adv_smem_base<S, R>();
-    return adv_tma_off(adv_smem_base<S, R>()) + raw_tile_bytes<S>() + 16;   // raw tile, mbarrier, abort flag
+    if (!TMA) return adv_smem_base<S, R, adv_pfr<R, TMA>()>();
+    return adv_tma_off(adv_smem_base<S, R, false>()) + raw_tile_bytes<S>() + 16;   // raw tile, mbarrier, abort flag
 }
 
 template <typename S, typename R, int FLUX, int MINB, bool TMA>

@@ -8,6 +8,8 @@
                                                   # 16 rows per advection tile, 4 CTAs/SM: 20 steps
     python -m lydion_b200.profile_cases step64    # the same cloud in FP64, 20 rows per tile,
                                                   # 3 CTAs/SM (the bench's tuned shape): 20 steps
+    python -m lydion_b200.profile_cases big64     # a 512x512x128 RHD snapshot in FP64 (33.5M
+                                                  # cell-bins, ~2 GB on the device, 15x L2): 6 steps
 """
 import sys
 
@@ -57,7 +59,19 @@ def step_case(fp64=False):
     return float(h[-1, 0])
 
 
+def big_case():
+    from . import workloads as W
+    from ._lib import PREC_FP64
+    from .m1 import context_for_cloud
+    cl = W.rhd_snapshot_cloud(n=512, n_nu=128, name="rhd_snapshot_512x512x128")
+    ctx = context_for_cloud(cl, precision=PREC_FP64)
+    ctx.set_tuning(20, 0, 0, 3)
+    h = ctx.static_steps(6, cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+    ctx.close()
+    return float(h[-1, 0])
+
+
 if __name__ == "__main__":
     case = sys.argv[1] if len(sys.argv) > 1 else "adjoint"
     print(case, {"adjoint": adjoint_case, "rhd": rhd_case, "step": step_case,
-                "step64": lambda: step_case(fp64=True)}[case]())
+                "step64": lambda: step_case(fp64=True), "big64": big_case}[case]())

@@ -61,6 +61,23 @@ def test_persistent_equals_three_launch_step_bitwise(n_nu, precision):
     per.close()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_persistent_hll_flux_bitwise(precision):
+    """The HLL flux (wave speeds from the closure's eigenvalues) through the persistent step."""
+    from lydion_b200.m1 import cloud_params
+    clouds = _clouds(64)
+    for c in clouds:
+        c.flux_method = W.FLUX_HLL
+    ref = _batch(clouds, precision, seed=23)
+    per = _batch(clouds, precision, seed=23)
+    h_ref = ref.batch_steps(5, cloud_params(clouds))
+    h_per = per.batch_steps(5, cloud_params(clouds), persistent=True)
+    np.testing.assert_array_equal(h_per, h_ref)
+    _same(ref, per, len(clouds))
+    ref.close()
+    per.close()
+
+
 def test_persistent_more_work_than_ctas():
     """A 128 x 160 cloud cut into 4-row tiles and 8-cell blocks: more tiles, items and
     reduction blocks than resident CTAs, so every CTA loops over several of each."""
