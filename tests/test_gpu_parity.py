@@ -314,6 +314,27 @@ def test_full_size_c2_steps_match_oracle(oracle_mod):
     assert w["escaping_flux"] < 1e-5, w["escaping_flux"]
 
 
+def test_c4_turbulent_cloud_200_steps_match_oracle(oracle_mod):
+    """The adjoint configuration's turbulent cloud (128 x 128 x 48: lognormal n_H, dust, a
+    50 km/s turbulent velocity field) over 200 fused steps against the oracle, with the bounds
+    of the headline cloud's test: every step's window and M_F; the final J, the flux fractions
+    and the edge-ring spectrum per element with a floor of 1e-6 of the maximum; the per-bin
+    escaping flux."""
+    cl = W.config_c4()
+    st, ctx = matched_pair(oracle_mod, cl)
+    n = 200
+    d_o = st.run(n)
+    d_g = ctx.static_steps(n, cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
+    np.testing.assert_array_equal(d_g[:, 5:7], d_o[:, 5:7])
+    assert max_rel(d_g[1:, 0], d_o[1:, 0]) < 1e-8
+    for f in ("J", "H_r", "H_Z"):
+        assert norm_err(ctx.download(f), getattr(st, f)) < 1e-8, f
+    w = wing_checks(ctx, st, cl)
+    for q in ("J", "H_r", "H_Z", "edge_spectrum"):
+        assert w[q] < 1e-8, (q, w[q])
+    assert w["escaping_flux"] < 1e-5, w["escaping_flux"]
+
+
 def test_c1_point_source_1000_steps_match_oracle(oracle_mod):
     """The plain-FP64 point-source cloud (64 x 64 x 64, tau0 = 1e6, recoil on) over the 1000
     steps it is specified with, against the oracle: the active window of every step, M_F, and
