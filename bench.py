@@ -255,7 +255,9 @@ def form_errors(cloud, local, precs, n_steps=2000):
 
 def e2e_form(ctx, cloud, args, barrier, stream_of, world):
     """End to end through the public API with host buffers: per step, J / H_r / H_Z up from
-    pinned host memory, one step with its diagnostics record, J / H_r / H_Z back."""
+    pinned host memory, one step with its diagnostics record, J / H_r / H_Z back into the same
+    pinned arrays. Through lyd_static_step_host, which pipelines the copies and the step over 8
+    row chunks; `serial` is the same loop as upload, one step, download calls."""
     import torch
     from lydion_b200 import sharding
     p = (cloud.c_tilde, cloud.dt, cloud.z_center, cloud.bc_r_right, cloud.bc_z_bot, cloud.bc_z_top)
@@ -267,7 +269,7 @@ def e2e_form(ctx, cloud, args, barrier, stream_of, world):
         a[...] = ctx.download(name)
     barrier(ctx)
 
-    def run(k):
+    def run_serial(k):
         for _ in range(k):
             for a, name in zip(pinned, names):
                 ctx.upload(name, a)
@@ -275,10 +277,19 @@ def e2e_form(ctx, cloud, args, barrier, stream_of, world):
             for a, name in zip(pinned, names):
                 ctx.download(name, out=a)
 
+    def run(k):
+        for _ in range(k):
+            ctx.static_step_host(pinned[0], pinned[1], pinned[2], *p, out=pinned, chunks=8)
+
+    ms_serial = sharding.max_over_ranks(_timed(ctx, run_serial, n, stream_of), device="cuda")
+    run(1)   # the first call decides the window from the uploaded state
     ms = sharding.max_over_ranks(_timed(ctx, run, n, stream_of), device="cuda")
     nbytes = 3 * cloud.cell_bins * 8
     return {"value": sharding.weak_scaling_throughput(n * cloud.cell_bins, world, ms), "unit": UNIT,
-            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes + 7 * 8, "steps": n}
+            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes + 7 * 8, "steps": n,
+            "ms_per_step": ms / n, "api": "lyd_static_step_host, 8 row chunks",
+            "serial": {"value": sharding.weak_scaling_throughput(n * cloud.cell_bins, world, ms_serial),
+                       "ms_per_step": ms_serial / n, "api": "lyd_upload x3, lyd_static_steps(1), lyd_download x3"}}
 
 
 def dropin_form(cloud, args, stream_of, local):

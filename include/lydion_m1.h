@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define LYD_ABI_VERSION 5
+#define LYD_ABI_VERSION 6
 
 /* status codes */
 #define LYD_OK              0
@@ -209,6 +209,21 @@ int  lyd_reset_dru(lyd_ctx *ctx);
  * per step; with diag_hist == NULL the call returns once the steps are enqueued and any
  * error is reported by the next synchronising call. */
 int  lyd_static_steps(lyd_ctx *ctx, const lyd_step_params *p, lyd_diag *diag_hist);
+/* One static-driver iteration on host state: J, H_r, H_Z (n_nu x n_r x n_z doubles each, the
+ * layout of lyd_upload) go up, the step runs, the new J, H_r, H_Z come back into the *_out
+ * arrays (which may be the inputs themselves) and diag receives its record (may be NULL).
+ * p->n_steps is ignored. The copies and the step are pipelined over `chunks` row chunks
+ * (1..16; 8 is a good choice): a chunk's rows advect once the next chunk has landed, its cells
+ * take the frequency step and go back down while later chunks still go up. For that the step
+ * uses the active window the previous step decided, and checks it against FindActiveBins of the
+ * uploaded J; when they differ (the caller changed J in between, or on the first call) the call
+ * steps again from the uploaded state, unpipelined. One cloud, the FP64 form (LYD_PREC_FP64,
+ * whose state is held in the caller's units), no Z slab; other contexts get LYD_ERR_STATE. The
+ * host arrays should be page-locked for the copies to overlap. The call returns when the
+ * outputs are written. */
+int  lyd_static_step_host(lyd_ctx *ctx, const lyd_step_params *p, const double *J, const double *H_r,
+                          const double *H_Z, double *J_out, double *H_r_out, double *H_Z_out, int32_t chunks,
+                          lyd_diag *diag);
 /* Per-kernel device time of the last lyd_static_steps call that had timing enabled:
  * ms[0] = advection kernel, ms[1] = frequency kernel, ms[2] = reductions (totals). */
 int  lyd_set_timing(lyd_ctx *ctx, int32_t enable);

@@ -131,6 +131,7 @@ SIGNATURES = {
     "lyd_edge_spectra_cloud": (C.c_int, [VP, I32, P, P, C.POINTER(I32), C.POINTER(I32)]),
     "lyd_batch_steps": (C.c_int, [VP, C.POINTER(CloudParams), I32, C.POINTER(Diag)]),
     "lyd_batch_steps_persistent": (C.c_int, [VP, C.POINTER(CloudParams), I32, C.c_int64, C.POINTER(Diag)]),
+    "lyd_static_step_host": (C.c_int, [VP, C.POINTER(StepParams), P, P, P, P, P, P, I32, C.POINTER(Diag)]),
     "lyd_persistent_info": (C.c_int, [VP, C.POINTER(I32)]),
     "lyd_set_tuning": (C.c_int, [VP, C.POINTER(Tuning)]),
     "lyd_get_tuning": (C.c_int, [VP, C.POINTER(Tuning)]),

@@ -104,6 +104,16 @@ struct lyd_ctx {
     cudaGraphExec_t gexec = nullptr;
     int gkey_cur = -1;
     long long gkey_polls = 0;          // 0: the three-launch step graph; else the persistent step's poll limit
+    // the host-state step (lyd_static_step_host): the state as uploaded, the window check, the
+    // work lists grouped by row chunk, its copy streams and events
+    double *hin = nullptr;             // [3][n3] J, H_r, H_Z as uploaded
+    double *part_chk = nullptr;        // FindActiveBins partials of the uploaded J
+    int *kwin_chk = nullptr;           // the window the step used, then the window of the uploaded J
+    int4 *ctiles = nullptr;            // advection tiles, chunk after chunk
+    std::vector<int> ct_off, it_off, row_off;
+    int hs_req = 0, hs_chunks = 0, hs_rows = 0, hs_cpb = 0, hs_pchk = 0;
+    cudaStream_t st_up = nullptr, st_dn = nullptr, st_fq = nullptr;
+    cudaEvent_t hs_ev[3 * 16 + 2] = {};
     unsigned *bar = nullptr;           // grid barrier of the persistent step: arrivals, generation
     int persist_graph = 0;             // persistent step replayed from a graph: 1 yes, -1 no (capture refused)
     bool timing = false;
@@ -459,13 +469,18 @@ int lyd_destroy(lyd_ctx *c) {
                   c->inv_dV, c->A_r, c->A_Z, c->inv_r_cell, c->rCoM, c->ZCoM, c->rint, c->zint, c->r_if, c->Z_if,
                   c->nu, c->nuC, c->dnu, c->inv_dnu, c->inv_nuC, c->partials, c->kwin, c->hist, c->step_ctr,
                   c->last, c->err, c->lut, c->stage, c->small, c->cl, c->tiles, c->items, c->adj_ws,
-                  c->red_cols, c->red_cnt, c->bar};
+                  c->red_cols, c->red_cnt, c->bar, c->hin, c->part_chk, c->kwin_chk, c->ctiles};
     for (void *p : ps) cudaFree(p);
     for (int q = 0; q < CF_N; q++) cudaFree(c->cellf[q]);
     cudaFree(c->dust_F);
     cudaFree(c->dd_cl);
     for (int q = 0; q < 8; q++)
         if (c->ev[q]) cudaEventDestroy(c->ev[q]);
+    for (cudaEvent_t e : c->hs_ev)
+        if (e) cudaEventDestroy(e);
+    if (c->st_up) cudaStreamDestroy(c->st_up);
+    if (c->st_dn) cudaStreamDestroy(c->st_dn);
+    if (c->st_fq) cudaStreamDestroy(c->st_fq);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
     return LYD_OK;
@@ -1235,6 +1250,185 @@ int lyd_static_steps(lyd_ctx *c, const lyd_step_params *p, lyd_diag *hist_out) {
     for (CloudDesc &d : c->desc) d.z_center = p->z_center;
     bcs_all(c, c->cfg.bc_r_left, p->bc_r_right, p->bc_z_bot, p->bc_z_top);
     return run_steps(c, p->n_steps, hist_out);
+}
+
+// ---- one step on host state, pipelined over row chunks -----------------------------------------
+constexpr int kMaxHostChunks = 16;
+
+// The work lists grouped by row chunk: chunk q covers the tile rows [q T / n, (q+1) T / n) of the
+// T tile rows, its advection tiles (every bin chunk of those rows), and the frequency items whose
+// cells all lie below the chunk's last row (the last chunk takes the rest).
+static int build_host_chunks(lyd_ctx *c, int chunks) {
+    const int rows = c->tune.rows_per_tile, nr = c->nr[0], nz = c->nz[0];
+    const int ntr = (nz + rows - 1) / rows, nkb = (c->nnu + 31) / 32, cpb = cells_per_block(c);
+    if (c->hs_req == chunks && c->hs_rows == rows && c->hs_cpb == cpb && c->ctiles) return LYD_OK;
+    c->hs_req = chunks;
+    if (chunks > ntr) chunks = ntr;
+    std::vector<int4> t;
+    c->ct_off.assign(chunks + 1, 0);
+    c->it_off.assign(chunks + 1, 0);
+    c->row_off.assign(chunks + 1, 0);
+    for (int q = 0; q < chunks; q++) {
+        const int tr0 = (int)((long long)q * ntr / chunks), tr1 = (int)((long long)(q + 1) * ntr / chunks);
+        c->ct_off[q] = (int)t.size();
+        for (int kb = 0; kb < nkb; kb++)
+            for (int tr = tr0; tr < tr1; tr++)
+                for (int i0 = 0; i0 < nr; i0 += kTileCols) t.push_back(make_int4(0, i0, tr * rows, 32 * kb));
+        c->row_off[q] = std::min(nz, tr0 * rows);
+        c->it_off[q] = (int)std::min<long long>(c->nitems, (long long)c->row_off[q] * nr / cpb);
+    }
+    c->ct_off[chunks] = (int)t.size();
+    c->row_off[chunks] = nz;
+    c->it_off[chunks] = c->nitems;
+    cudaFree(c->ctiles);
+    c->ctiles = nullptr;
+    LYD_TRY(dalloc(c, (void **)&c->ctiles, t.size() * sizeof(int4)));
+    LYD_CU(c, cudaMemcpyAsync(c->ctiles, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice, c->st));
+    LYD_CU(c, cudaStreamSynchronize(c->st));
+    c->hs_chunks = chunks;
+    c->hs_rows = rows;
+    c->hs_cpb = cpb;
+    return LYD_OK;
+}
+
+int lyd_static_step_host(lyd_ctx *c, const lyd_step_params *p, const double *J, const double *Hr, const double *HZ,
+                         double *J_out, double *Hr_out, double *HZ_out, int32_t chunks, lyd_diag *diag) {
+    if (!c || !p || !J || !Hr || !HZ || !J_out || !Hr_out || !HZ_out) return LYD_ERR_ARG;
+    LYD_TRY(single_cloud(c, "lyd_static_step_host"));
+    cudaSetDevice(c->dev);
+    if (chunks < 1 || chunks > kMaxHostChunks) return fail(c, LYD_ERR_ARG, "chunks outside 1..16");
+    if (c->prec != LYD_PREC_FP64 || c->jscale != 1.0)
+        return fail(c, LYD_ERR_STATE, "the host-state step runs the FP64 form (state in the caller's units)");
+    if (c->desc[0].j_own0 != 0 || c->desc[0].j_own1 != c->nz[0])
+        return fail(c, LYD_ERR_STATE, "the host-state step runs on a whole field, not a Z slab");
+    LYD_TRY(check_bcs(c, c->cfg.bc_r_left, p->bc_r_right, p->bc_z_bot, p->bc_z_top));
+    if (!(p->c_tilde > 0.0) || !(p->dt > 0.0)) return fail(c, LYD_ERR_ARG, "bad step parameters");
+    params_all(c, p->c_tilde, p->dt, p->c_tilde * p->dt);
+    c->desc[0].z_center = p->z_center;
+    bcs_all(c, c->cfg.bc_r_left, p->bc_r_right, p->bc_z_bot, p->bc_z_top);
+    LYD_TRY(need_inputs(c, true, true));
+    LYD_TRY(sync_desc(c));
+    const size_t n3 = c->n3, nnu = c->nnu, nr = c->nr[0];
+    if (!c->hin) LYD_TRY(dalloc(c, (void **)&c->hin, 3 * n3 * 8));
+    if (!c->kwin_chk) LYD_TRY(dalloc(c, (void **)&c->kwin_chk, 4 * sizeof(int)));
+    if (c->hs_pchk != c->nitems) {
+        cudaFree(c->part_chk);
+        c->part_chk = nullptr;
+        c->hs_pchk = 0;
+        LYD_TRY(dalloc(c, (void **)&c->part_chk, (size_t)c->nitems * (c->nnu + kExtraCols) * 8));
+        c->hs_pchk = c->nitems;
+    }
+    if (!c->st_up) {
+        LYD_CU(c, cudaStreamCreateWithFlags(&c->st_up, cudaStreamNonBlocking));
+        LYD_CU(c, cudaStreamCreateWithFlags(&c->st_dn, cudaStreamNonBlocking));
+        LYD_CU(c, cudaStreamCreateWithFlags(&c->st_fq, cudaStreamNonBlocking));
+        for (cudaEvent_t &e : c->hs_ev) LYD_CU(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    LYD_TRY(build_host_chunks(c, chunks));
+    const int nch = c->hs_chunks;
+    cudaEvent_t *ev_up = c->hs_ev, *ev_fq = c->hs_ev + kMaxHostChunks, *ev_adv = c->hs_ev + 2 * kMaxHostChunks;
+    cudaEvent_t ev_start = c->hs_ev[3 * kMaxHostChunks], ev_chk = c->hs_ev[3 * kMaxHostChunks + 1];
+    const double *src[3] = {J, Hr, HZ};
+    double *dst[3] = {J_out, Hr_out, HZ_out};
+    // whatever ran before on the context's stream is done with the reduction's counters first
+    LYD_CU(c, cudaEventRecord(ev_start, c->st));
+    LYD_CU(c, cudaStreamWaitEvent(c->st_up, ev_start, 0));
+    // the step keeps no Delta rho u between steps; the window it uses is the previous step's
+    const bool spec = c->active_valid;
+    LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_R], 0, c->ncell * 8, c->st));
+    LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_Z], 0, c->ncell * 8, c->st));
+    // uploads, chunk after chunk, then the window of the uploaded J (FindActiveBins) for the check
+    for (int q = 0; q < nch; q++) {
+        const size_t off = (size_t)c->row_off[q] * nr * nnu, len = (size_t)(c->row_off[q + 1] - c->row_off[q]) * nr * nnu;
+        for (int f = 0; f < 3; f++)
+            LYD_CU(c, cudaMemcpyAsync(c->hin + f * n3 + off, src[f] + off, len * 8, cudaMemcpyHostToDevice, c->st_up));
+        LYD_CU(c, cudaEventRecord(ev_up[q], c->st_up));
+    }
+    launch_find_active(0, c->hin, c->nnu, c->dnu, c->dV, c->cl, c->items, c->nitems, c->jeps_s, c->part_chk, c->st_up);
+    RedArgs rc = red_args(c, PART_ACTIVE);
+    rc.partials = c->part_chk;
+    rc.kwin = c->kwin_chk + 2;
+    rc.last = nullptr;
+    launch_reduce(rc, c->st_up);
+    LYD_CU(c, cudaEventRecord(ev_chk, c->st_up));
+    if (!spec) {
+        // no window yet: the step waits for that of the uploaded J
+        LYD_CU(c, cudaStreamWaitEvent(c->st, ev_chk, 0));
+        LYD_CU(c, cudaMemcpyAsync(c->kwin, c->kwin_chk + 2, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+    }
+    LYD_CU(c, cudaMemcpyAsync(c->kwin_chk, c->kwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+    // per chunk: the advection of its rows (once the next chunk, which holds their upper
+    // neighbours, has landed) from the uploaded state into the other buffer set, then on a
+    // second stream the frequency step of its items back into the state's set, then its rows
+    // down. A chunk's launches fill a fraction of the GPU, so the frequency step of chunk q runs
+    // beside the advection of chunk q+1 (they touch different rows).
+    const int A = c->cur, B = 1 - c->cur;
+    AdvArgs<double> aa;
+    fill_adv<double>(c, aa, A, B);
+    aa.J = c->hin; aa.Hr = c->hin + n3; aa.HZ = c->hin + 2 * n3;
+    aa.tmaps = nullptr;
+    FreqArgs<double> fa;
+    fill_freq<double>(c, fa, c->set[B][0], c->set[B][1], c->set[B][2], c->set[B][0], c->set[A][0], c->set[A][1],
+                      c->set[A][2]);
+    fa.do_emission = 1; fa.do_freq = 1; fa.update_ff = 1;
+    fa.parts = PART_ACTIVE | PART_DIAG;
+    fa.f_r = c->cellf[CF_F_R]; fa.f_Z = c->cellf[CF_F_Z];
+    fa.nitems_all = c->nitems;
+    for (int q = 0; q < nch; q++) {
+        LYD_CU(c, cudaStreamWaitEvent(c->st, ev_up[q + 1 < nch ? q + 1 : q], 0));
+        aa.tiles = c->ctiles + c->ct_off[q];
+        if (c->ct_off[q + 1] > c->ct_off[q])
+            launch_advect(c->prec, c->cfg.flux_method, &aa, c->ct_off[q + 1] - c->ct_off[q], c->tune.adv_ctas_per_sm,
+                          c->st);
+        LYD_CU(c, cudaEventRecord(ev_adv[q], c->st));
+        LYD_CU(c, cudaStreamWaitEvent(c->st_fq, ev_adv[q], 0));
+        fa.item0 = c->it_off[q];
+        if (c->it_off[q + 1] > c->it_off[q])
+            launch_freq(c->prec, &fa, c->nnu, c->it_off[q + 1] - c->it_off[q], c->st_fq);
+        LYD_CU(c, cudaEventRecord(ev_fq[q], c->st_fq));
+        LYD_CU(c, cudaStreamWaitEvent(c->st_dn, ev_fq[q], 0));
+        const size_t b0 = (size_t)c->it_off[q] * c->hs_cpb;
+        const size_t b1 = std::min<size_t>((size_t)c->it_off[q + 1] * c->hs_cpb, (size_t)c->ncell);
+        if (b1 > b0)
+            for (int f = 0; f < 3; f++)
+                LYD_CU(c, cudaMemcpyAsync(dst[f] + b0 * nnu, static_cast<const double *>(c->set[A][f]) + b0 * nnu,
+                                          (b1 - b0) * nnu * 8, cudaMemcpyDeviceToHost, c->st_dn));
+    }
+    LYD_CU(c, cudaGetLastError());
+    // the diagnostics and the next window, after the check (the two share the reduction's counters)
+    LYD_CU(c, cudaStreamWaitEvent(c->st, ev_fq[nch - 1], 0));
+    LYD_CU(c, cudaStreamWaitEvent(c->st, ev_chk, 0));
+    launch_reduce(red_args(c, PART_ACTIVE | PART_DIAG), c->st);
+    double rec[7];
+    int kw[4];
+    LYD_CU(c, cudaMemcpyAsync(rec, c->last, sizeof(rec), cudaMemcpyDeviceToHost, c->st));
+    LYD_CU(c, cudaMemcpyAsync(kw, c->kwin_chk, sizeof(kw), cudaMemcpyDeviceToHost, c->st));
+    LYD_CU(c, cudaStreamSynchronize(c->st_dn));
+    LYD_CU(c, cudaStreamSynchronize(c->st_up));
+    LYD_TRY(check_err(c));
+    c->old_alias = true;
+    c->active_valid = true;
+    if (kw[0] != kw[2] || kw[1] != kw[3]) {
+        // the uploaded J was not the state the previous step left: its window differs from the
+        // one the step used. Step again from the uploaded state with its own window, unpipelined.
+        for (int f = 0; f < 3; f++)
+            LYD_CU(c, cudaMemcpyAsync(c->set[A][f], c->hin + f * n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
+        LYD_CU(c, cudaMemcpyAsync(c->kwin, c->kwin_chk + 2, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+        LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_R], 0, c->ncell * 8, c->st));
+        LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_Z], 0, c->ncell * 8, c->st));
+        LYD_TRY(enqueue_step<double>(c, false, nullptr, nullptr, nullptr, nullptr, false));
+        launch_reduce(red_args(c, PART_ACTIVE | PART_DIAG), c->st);
+        for (int f = 0; f < 3; f++)
+            LYD_CU(c, cudaMemcpyAsync(dst[f], c->set[A][f], n3 * 8, cudaMemcpyDeviceToHost, c->st));
+        LYD_CU(c, cudaMemcpyAsync(rec, c->last, sizeof(rec), cudaMemcpyDeviceToHost, c->st));
+        LYD_TRY(check_err(c));
+    }
+    if (diag) {
+        diag->M_F = rec[0]; diag->M_F_radial_net = rec[1]; diag->M_F_radial_out = rec[2];
+        diag->L_tot = rec[3]; diag->f_esc = rec[4];
+        diag->kmin = (int32_t)rec[5]; diag->kmax = (int32_t)rec[6];
+    }
+    return LYD_OK;
 }
 
 // ---- Z-slab domain decomposition -------------------------------------------------------------

@@ -101,6 +101,7 @@ struct FreqArgs {
     int nnu;
     int solver;                  // SOLVER_*
     int vec16;                   // set by the launcher: rows move as whole 16-byte words
+    int item0, nitems_all;       // a launch over items item0 .. of a list of nitems_all (0: the grid's)
 };
 
 enum { SOLVER_PCR = 0, SOLVER_THOMAS = 1 };

@@ -1634,7 +1634,8 @@ __device__ __forceinline__ void freq_item(const FreqArgs<S> &a, int item, int ni
 template <typename S, typename R, int M, typename RC = R>
 __global__ void __launch_bounds__(FREQ_THREADS, M <= 4 ? 2 : 1) k_freq(FreqArgs<S> a) {
     extern __shared__ __align__(16) double fsm[];
-    freq_item<S, R, M, RC>(a, blockIdx.x, gridDim.x, fsm, blockDim.x >> 5);
+    freq_item<S, R, M, RC>(a, a.item0 + (int)blockIdx.x, a.nitems_all ? a.nitems_all : (int)gridDim.x, fsm,
+                           blockDim.x >> 5);
 }
 
 // FindActiveBins partials of the current J (src/UpdateLyaJandH.jl:47-97): one warp per cell,

@@ -166,6 +166,25 @@ class M1Context:
         self._ck(lib().lyd_static_steps(self._h, C.byref(p), None))
         return None
 
+    def static_step_host(self, J, H_r, H_Z, c_tilde, dt, z_center, bc_r_right=BC_OUTFLOW, bc_z_bot=BC_REFLECT,
+                         bc_z_top=BC_OUTFLOW, out=None, chunks=8):
+        """One static-driver iteration on host state (lyd_static_step_host): J, H_r, H_Z (float64,
+        C-contiguous, the lyd_upload layout) go up, the new state comes back into `out`
+        (three arrays; may be the inputs themselves; new arrays when None), pipelined over
+        `chunks` row chunks. Returns (J, H_r, H_Z, record) with the step's diagnostics record
+        (M_F, M_F_radial_net, M_F_radial_out, L_tot, f_esc, kmin, kmax)."""
+        ins = [np.ascontiguousarray(a, dtype=np.float64) for a in (J, H_r, H_Z)]
+        outs = list(out) if out is not None else [np.empty_like(a) for a in ins]
+        for a, b in zip(ins, outs):
+            if b.dtype != np.float64 or not b.flags.c_contiguous or b.size != a.size:
+                raise ValueError("outputs must be C-contiguous float64 arrays of the inputs' size")
+        p = _lib.StepParams(float(c_tilde), float(dt), float(z_center), bc_r_right, bc_z_bot, bc_z_top, 1)
+        d = _lib.Diag()
+        self._ck(lib().lyd_static_step_host(self._h, C.byref(p), _dp(ins[0]), _dp(ins[1]), _dp(ins[2]),
+                                             _dp(outs[0]), _dp(outs[1]), _dp(outs[2]), int(chunks), C.byref(d)))
+        rec = np.array([d.M_F, d.M_F_radial_net, d.M_F_radial_out, d.L_tot, d.f_esc, d.kmin, d.kmax])
+        return outs[0], outs[1], outs[2], rec
+
     def set_timing(self, on):
         self._ck(lib().lyd_set_timing(self._h, int(bool(on))))
 

@@ -29,7 +29,7 @@ def test_library_exports_every_declared_symbol():
 def test_abi_version_and_edge_count():
     from lydion_b200 import _lib
     L = _lib.lib()
-    assert L.lyd_abi_version() == 5
+    assert L.lyd_abi_version() == 6
     assert L.lyd_edge_count(64, 64) == 62 + 2 * 61
 
 
