@@ -161,6 +161,11 @@ int  lyd_abi_version(void);
  * closure chi(f) = (5 - 2 sqrt(4 - 3 f^2)) / 3 for f in [0, 1], 4: exp(x) for |x| <= 40 (the
  * table-driven form of the frequency factors). */
 int  lyd_math_check(int32_t fn, const double *x, double *y, size_t n);
+/* Page-locked host memory (cudaHostAlloc, portable to every context): copies between it and a
+ * context run at the link's rate instead of through a pageable staging buffer, and the
+ * host-state step's copies overlap. lyd_host_free releases it. */
+int  lyd_host_alloc(size_t bytes, void **out);
+int  lyd_host_free(void *p);
 int  lyd_set_geometry(lyd_ctx *ctx, const lyd_geometry *g);
 int  lyd_set_freq_grid(lyd_ctx *ctx, const lyd_freq_grid *f);
 int  lyd_upload(lyd_ctx *ctx, int32_t field, const double *host, size_t count);

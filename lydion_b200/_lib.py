@@ -104,6 +104,8 @@ SIGNATURES = {
     "lyd_last_error": (C.c_char_p, [VP]),
     "lyd_abi_version": (C.c_int, []),
     "lyd_math_check": (C.c_int, [I32, P, P, SZ]),
+    "lyd_host_alloc": (C.c_int, [SZ, C.POINTER(VP)]),
+    "lyd_host_free": (C.c_int, [VP]),
     "lyd_set_geometry": (C.c_int, [VP, C.POINTER(Geometry)]),
     "lyd_set_freq_grid": (C.c_int, [VP, C.POINTER(FreqGrid)]),
     "lyd_upload": (C.c_int, [VP, I32, P, SZ]),

@@ -339,6 +339,17 @@ const char *lyd_last_error(const lyd_ctx *c) { return c ? c->msg.c_str() : "null
 
 int lyd_edge_count(int32_t n_r, int32_t n_z) { return (n_z - 2) + 2 * (n_r - 3); }
 
+int lyd_host_alloc(size_t bytes, void **out) {
+    if (!out) return LYD_ERR_ARG;
+    *out = nullptr;
+    return cudaHostAlloc(out, bytes ? bytes : 16, cudaHostAllocPortable) == cudaSuccess ? LYD_OK : LYD_ERR_NOMEM;
+}
+
+int lyd_host_free(void *p) {
+    if (!p) return LYD_OK;
+    return cudaFreeHost(p) == cudaSuccess ? LYD_OK : LYD_ERR_CUDA;
+}
+
 int lyd_math_check(int32_t fn, const double *x, double *y, size_t n) {
     if (fn < 0 || fn > 4 || !x || !y) return LYD_ERR_ARG;
     if (n == 0) return LYD_OK;

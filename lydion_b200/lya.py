@@ -255,15 +255,22 @@ def generate_lya_arrays_from_saved(c_tilde, freq, geom, T, Hvoigt, phi_nu, recoi
     """GenerateLyaArrays_FromSaved (src/SetupLymanAlphaArrays.jl:244-393) for a frequency grid
     `freq` (grid.FreqGrid), geometry `geom` and temperature T [j, i]; H_voigt and phi_nu are
     supplied (the reference computes them with Update_Hvoigt!/Update_phi_nu!). Makes the
-    arrays' device twin."""
+    arrays' device twin. The cell-bin arrays are page-locked (m1.pinned_zeros), so the copies
+    of the copy mode run at the link's rate."""
+    from .m1 import pinned_zeros
     nz, nr = T.shape
     n = freq.n_nu
-    z3 = lambda: np.zeros((nz, nr, n))
+    z3 = lambda: pinned_zeros((nz, nr, n))
+
+    def pinned_copy(a):
+        out = pinned_zeros((nz, nr, n))
+        out[...] = a
+        return out
     z2 = lambda: np.zeros((nz, nr))
     from .grid import alpha_floor
     lya = LyaArrays(c_tilde=c_tilde, J=z3(), J_old=z3(), H_r=z3(), H_Z=z3(), H_r_old=z3(), H_Z_old=z3(),
-                    alpha=z2(), alpha_F=z3(), alpha_c=z2(), pd=z2(), js=z2(), Hvoigt=np.array(Hvoigt, dtype=float),
-                    phi_nu=np.array(phi_nu, dtype=float), nu=freq.nu, nuC=freq.nuC, dnu=freq.dnu,
+                    alpha=z2(), alpha_F=z3(), alpha_c=z2(), pd=z2(), js=z2(), Hvoigt=pinned_copy(Hvoigt),
+                    phi_nu=pinned_copy(phi_nu), nu=freq.nu, nuC=freq.nuC, dnu=freq.dnu,
                     inv_dnu=freq.inv_dnu, inv_nuC=freq.inv_nuC, kcore_min=freq.kcore_min,
                     kcore_max=freq.kcore_max, recoil=recoil, alpha_floor=alpha_floor(geom),
                     dru_r=z2(), dru_Z=z2(), f_r=z2(), f_Z=z2(), flux_method=FLUX_HLL if hll else FLUX_GLF)
