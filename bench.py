@@ -196,7 +196,8 @@ def measure_form(cloud, prec, args, barrier, stream_of, local, world, clk=None):
     if args.no_tune:
         tuning = ctx.tuning()
     else:
-        tuning = autotune.autotune(ctx, run, steps=10, device=local, reset=reset,
+        # 30 steps per candidate: neighbouring tile heights differ by ~1 %, less than 10 steps resolve
+        tuning = autotune.autotune(ctx, run, steps=30, device=local, reset=reset,
                                    cache=os.path.join(tempfile.gettempdir(), "lydion_bench_tuning.json"))
         reset()
     run(args.warmup)
