@@ -51,6 +51,22 @@ def test_host_step_equals_device_step_bitwise(flux, chunks):
     host.close()
 
 
+@pytest.mark.parametrize("bc_left", [W.BC_REFLECT, W.BC_OUTFLOW])
+def test_host_step_cartesian_bitwise(bc_left):
+    """A Cartesian grid (the first X interface reflecting or letting flow out), 6 chunks."""
+    cl = W.cartesian_cloud(nx=24, ny=64, n_nu=32, bc_left=bc_left)
+    dev, host, (J, Hr, HZ) = _pair(cl, seed=13)
+    p = _params(cl)
+    for _ in range(3):
+        rec_d = dev.static_steps(1, *p)[0]
+        J, Hr, HZ, rec_h = host.static_step_host(J, Hr, HZ, *p, out=(J, Hr, HZ), chunks=6)
+        np.testing.assert_array_equal(rec_h, rec_d)
+        np.testing.assert_array_equal(J, dev.download("J"))
+        np.testing.assert_array_equal(Hr, dev.download("H_r"))
+    dev.close()
+    host.close()
+
+
 def test_host_step_full_size_separate_outputs():
     """The 256 x 256 x 64 cloud, separate output arrays (the inputs stay as they were)."""
     cl = W.config_c2()
