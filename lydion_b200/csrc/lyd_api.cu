@@ -1302,6 +1302,18 @@ static int build_host_chunks(lyd_ctx *c, int chunks) {
     return LYD_OK;
 }
 
+// Drains the host-state step's streams when the step leaves early: no copy into or out of the
+// caller's arrays may still run after the call returns.
+struct HostStepDrain {
+    lyd_ctx *c;
+    bool armed = false;
+    ~HostStepDrain() {
+        if (!armed) return;
+        for (cudaStream_t s : {c->st_up, c->st_fq, c->st_dn, c->st})
+            if (s) cudaStreamSynchronize(s);
+    }
+};
+
 int lyd_static_step_host(lyd_ctx *c, const lyd_step_params *p, const double *J, const double *Hr, const double *HZ,
                          double *J_out, double *Hr_out, double *HZ_out, int32_t chunks, lyd_diag *diag) {
     if (!c || !p || !J || !Hr || !HZ || !J_out || !Hr_out || !HZ_out) return LYD_ERR_ARG;
@@ -1341,6 +1353,8 @@ int lyd_static_step_host(lyd_ctx *c, const lyd_step_params *p, const double *J, 
     cudaEvent_t ev_start = c->hs_ev[3 * kMaxHostChunks], ev_chk = c->hs_ev[3 * kMaxHostChunks + 1];
     const double *src[3] = {J, Hr, HZ};
     double *dst[3] = {J_out, Hr_out, HZ_out};
+    HostStepDrain drain{c};
+    drain.armed = true;
     // whatever ran before on the context's stream is done with the reduction's counters first
     LYD_CU(c, cudaEventRecord(ev_start, c->st));
     LYD_CU(c, cudaStreamWaitEvent(c->st_up, ev_start, 0));
