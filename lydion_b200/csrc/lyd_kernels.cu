@@ -187,7 +187,9 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const void *map, int x, i
 // cell values every face needs: J, the reduced fluxes H/max(J, Jeps) (so the reciprocal of J is
 // taken once per cell, not once per face) and alpha_F (formed once per cell, not at each of the
 // four face sides that read it); a ring of three rows holds the state of the own columns for
-// the cell update. The FP64 tile (74 KB) runs at three CTAs per SM. Warp w (0..7) owns
+// the cell update. With FP64 arithmetic and per-lane staging the halo columns keep one row and
+// every staged input comes a row ahead by cp.async (PFR below): the tile (76 KB) runs at three
+// CTAs per SM. Warp w (0..7) owns
 // column i0+w; warp 8 stages the halo columns and computes the tile's rightmost r face. Per row: stage row j+2 -> sync -> every warp
 // computes the r face on its left (warp 8: the right edge) into shared memory and its Z face
 // j+1/2 into registers -> sync -> the cell update of row j uses the two r faces from shared
@@ -729,7 +731,7 @@ __device__ __forceinline__ void advect_tile(const AdvArgs<S> &a, int tile, unsig
         } else {
             // (A) stage row j+2 of the own column; warp 8 stages the halo columns of row j (spread
             // over four warps instead, one halo cell each, the FP64 advection took 0.336 ms
-            // against 0.322 ms at 256^2 x 64)
+            // against 0.322 ms at 256^2 x 64, before the row-ahead copies)
             if (kact) {
                 if (own) {
                     int r = j + 2;
@@ -1886,7 +1888,7 @@ static void adv_occ(const void *args, int ntiles, cudaStream_t st, int ctas) {
 }
 
 int adv_ctas_per_sm(int prec, int want) {
-    if (prec == PREC_K_FP64) return (want == 2) ? 2 : 3;   // FP64: 74 KB of shared memory, 72 registers
+    if (prec == PREC_K_FP64) return (want == 2) ? 2 : 3;   // FP64: 76 KB of shared memory, 72 registers
     return (want >= 2 && want <= 4) ? want : 4;
 }
 
