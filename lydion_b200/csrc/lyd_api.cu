@@ -1266,9 +1266,11 @@ int lyd_static_steps(lyd_ctx *c, const lyd_step_params *p, lyd_diag *hist_out) {
 // ---- one step on host state, pipelined over row chunks -----------------------------------------
 constexpr int kMaxHostChunks = 16;
 
-// The work lists grouped by row chunk: chunk q covers the tile rows [q T / n, (q+1) T / n) of the
-// T tile rows, its advection tiles (every bin chunk of those rows), and the frequency items whose
-// cells all lie below the chunk's last row (the last chunk takes the rest).
+// The work lists grouped by row chunk: chunk q covers a run of the T tile rows, its advection
+// tiles (every bin chunk of those rows), and the frequency items whose cells all lie below the
+// chunk's last row (the last chunk takes the rest). The first and the last chunk get half the
+// rows of the others: the first chunk's upload runs before anything else can start, and the
+// last chunk's download after everything else has ended.
 static int build_host_chunks(lyd_ctx *c, int chunks) {
     const int rows = c->tune.rows_per_tile, nr = c->nr[0], nz = c->nz[0];
     const int ntr = (nz + rows - 1) / rows, nkb = (c->nnu + 31) / 32, cpb = cells_per_block(c);
@@ -1279,8 +1281,15 @@ static int build_host_chunks(lyd_ctx *c, int chunks) {
     c->ct_off.assign(chunks + 1, 0);
     c->it_off.assign(chunks + 1, 0);
     c->row_off.assign(chunks + 1, 0);
+    // boundary q (0 < q < n) at tile row T (q - 1/2) / (n - 1), rounded; at least one tile row each
+    auto bound = [&](int q) {
+        if (q <= 0) return 0;
+        if (q >= chunks) return ntr;
+        const int b = (int)(((long long)ntr * (2 * q - 1) + (chunks - 1)) / (2 * (chunks - 1)));
+        return std::min(std::max(b, q), ntr - (chunks - q));
+    };
     for (int q = 0; q < chunks; q++) {
-        const int tr0 = (int)((long long)q * ntr / chunks), tr1 = (int)((long long)(q + 1) * ntr / chunks);
+        const int tr0 = bound(q), tr1 = bound(q + 1);
         c->ct_off[q] = (int)t.size();
         for (int kb = 0; kb < nkb; kb++)
             for (int tr = tr0; tr < tr1; tr++)
@@ -1362,11 +1371,17 @@ int lyd_static_step_host(lyd_ctx *c, const lyd_step_params *p, const double *J, 
     const bool spec = c->active_valid;
     LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_R], 0, c->ncell * 8, c->st));
     LYD_CU(c, cudaMemsetAsync(c->cellf[CF_DRU_Z], 0, c->ncell * 8, c->st));
-    // uploads, chunk after chunk, then the window of the uploaded J (FindActiveBins) for the check
+    // uploads, chunk after chunk, then the window of the uploaded J (FindActiveBins) for the check.
+    // A chunk's advection reads two rows past its last row (the Z face of its last row reads rows
+    // up to one beyond, the reconstruction one more), so chunk q's upload ends two rows into
+    // chunk q+1 and the advection of q waits for q's upload alone.
+    const int nzr = c->nz[0];
+    auto up_row = [&](int q) { return q <= 0 ? 0 : q >= nch ? nzr : std::min(nzr, c->row_off[q] + 2); };
     for (int q = 0; q < nch; q++) {
-        const size_t off = (size_t)c->row_off[q] * nr * nnu, len = (size_t)(c->row_off[q + 1] - c->row_off[q]) * nr * nnu;
-        for (int f = 0; f < 3; f++)
-            LYD_CU(c, cudaMemcpyAsync(c->hin + f * n3 + off, src[f] + off, len * 8, cudaMemcpyHostToDevice, c->st_up));
+        const size_t off = (size_t)up_row(q) * nr * nnu, len = (size_t)(up_row(q + 1) - up_row(q)) * nr * nnu;
+        if (len > 0)
+            for (int f = 0; f < 3; f++)
+                LYD_CU(c, cudaMemcpyAsync(c->hin + f * n3 + off, src[f] + off, len * 8, cudaMemcpyHostToDevice, c->st_up));
         LYD_CU(c, cudaEventRecord(ev_up[q], c->st_up));
     }
     launch_find_active(0, c->hin, c->nnu, c->dnu, c->dV, c->cl, c->items, c->nitems, c->jeps_s, c->part_chk, c->st_up);
@@ -1382,8 +1397,8 @@ int lyd_static_step_host(lyd_ctx *c, const lyd_step_params *p, const double *J, 
         LYD_CU(c, cudaMemcpyAsync(c->kwin, c->kwin_chk + 2, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
     }
     LYD_CU(c, cudaMemcpyAsync(c->kwin_chk, c->kwin, 2 * sizeof(int), cudaMemcpyDeviceToDevice, c->st));
-    // per chunk: the advection of its rows (once the next chunk, which holds their upper
-    // neighbours, has landed) from the uploaded state into the other buffer set, then on a
+    // per chunk: the advection of its rows (once they and the two rows above them have landed)
+    // from the uploaded state into the other buffer set, then on a
     // second stream the frequency step of its items back into the state's set, then its rows
     // down. A chunk's launches fill a fraction of the GPU, so the frequency step of chunk q runs
     // beside the advection of chunk q+1 (they touch different rows).
@@ -1400,7 +1415,7 @@ int lyd_static_step_host(lyd_ctx *c, const lyd_step_params *p, const double *J, 
     fa.f_r = c->cellf[CF_F_R]; fa.f_Z = c->cellf[CF_F_Z];
     fa.nitems_all = c->nitems;
     for (int q = 0; q < nch; q++) {
-        LYD_CU(c, cudaStreamWaitEvent(c->st, ev_up[q + 1 < nch ? q + 1 : q], 0));
+        LYD_CU(c, cudaStreamWaitEvent(c->st, ev_up[q], 0));
         aa.tiles = c->ctiles + c->ct_off[q];
         if (c->ct_off[q + 1] > c->ct_off[q])
             launch_advect(c->prec, c->cfg.flux_method, &aa, c->ct_off[q + 1] - c->ct_off[q], c->tune.adv_ctas_per_sm,
