@@ -70,10 +70,11 @@ __device__ __forceinline__ float rsq(float x) {
 }
 
 // Reciprocal 1 / y. FP64: the hardware's approximate reciprocal (PTX rcp.approx.ftz.f64)
-// refined by two Newton-Raphson steps for 1/y, x <- x + x (1 - y x), each written as two
-// fused multiply-adds; every step squares the relative error (Markstein, IBM J. Res. Dev. 34
-// (1990) 111-119). No special-case branches: the callers divide by positive normal numbers
-// whose reciprocals are normal. FP32: the hardware's approximate reciprocal alone (PTX
+// refined by one third-order step of the Newton-Raphson family for 1/y: with e = 1 - y x,
+// 1/y = x / (1 - e) = x (1 + e + e^2 + ...), so x <- x + x (e + e^2) cubes the relative error
+// (Markstein, IBM J. Res. Dev. 34 (1990) 111-119), in three fused multiply-adds where two
+// quadratic steps take four. No special-case branches: the callers divide by positive normal
+// numbers whose reciprocals are normal. FP32: the hardware's approximate reciprocal alone (PTX
 // rcp.approx.ftz.f32, relative error within 2^-23 over the normal range, subnormals flushed),
 // one instruction in place of the IEEE division's refinement sequence; the FP32 arithmetic of
 // the mixed and FP32-storage forms already carries a 2^-24 rounding per operation.
@@ -81,10 +82,8 @@ template <typename R> __device__ __forceinline__ R rcp(R y);
 template <> __device__ __forceinline__ double rcp<double>(double y) {
     double x;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(x) : "d"(y));
-    double e = fma(-y, x, 1.0);
-    x = fma(x, e, x);
-    e = fma(-y, x, 1.0);
-    return fma(x, e, x);
+    const double e = fma(-y, x, 1.0);
+    return fma(x, fma(e, e, e), x);
 }
 template <> __device__ __forceinline__ float rcp<float>(float y) {
     float x;
@@ -93,19 +92,17 @@ template <> __device__ __forceinline__ float rcp<float>(float y) {
 }
 
 // Reciprocal square root 1 / sqrt(x) for FP64 arithmetic and x >= DBL_MIN: the hardware's
-// approximate reciprocal square root (PTX rsqrt.approx.ftz.f64) refined by two Newton-Raphson
-// steps for 1/sqrt(x), y <- y + y (1/2 - (x/2) y^2), each a multiply and two fused
-// multiply-adds; every step squares the relative error (Markstein, IBM J. Res. Dev. 34 (1990)
-// 111-119). x * rsqrt_nr(x) is then sqrt(x) to about an ulp, and one such root gives both a
+// approximate reciprocal square root (PTX rsqrt.approx.ftz.f64) refined by one third-order
+// step: with e = 1 - x y^2, 1/sqrt(x) = y (1 - e)^(-1/2) = y (1 + e/2 + 3 e^2/8 + ...), so
+// y <- y + y e (1/2 + 3 e / 8) cubes the relative error (Markstein, IBM J. Res. Dev. 34 (1990)
+// 111-119), in two multiplies and three fused multiply-adds where two quadratic steps take
+// seven operations. x * rsqrt_nr(x) is then sqrt(x) to about an ulp, and one such root gives both a
 // length and its reciprocal where the IEEE root needs a root and a reciprocal.
 __device__ __forceinline__ double rsqrt_nr(double x) {
     double y;
     asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    const double h = 0.5 * x;
-    double r = fma(-(h * y), y, 0.5);
-    y = fma(y, r, y);
-    r = fma(-(h * y), y, 0.5);
-    return fma(y, r, y);
+    const double e = fma(-(x * y), y, 1.0);
+    return fma(y, e * fma(e, 0.375, 0.5), y);
 }
 constexpr double kDblMinNormal = 2.2250738585072014e-308;
 
