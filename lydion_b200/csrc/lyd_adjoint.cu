@@ -147,24 +147,26 @@ __device__ __forceinline__ void cr_pcr2(RowA<2> &R_, int lane) {
     double eb = R_.b[0] + al * c_om + ga * R_.a[1];
     double ec = ga * R_.c[1];
     double ed = R_.d[0] + al * d_om + ga * R_.d[1];
+    // PCR over the even rows, each scaled to a unit diagonal (three values per neighbour)
+    double ib = rcp<double>(eb);
+    double na = ea * ib, nc = ec * ib, nd = ed * ib;
 #pragma unroll
     for (int s = 1; s < 32; s <<= 1) {
-        double ib = rcp<double>(eb);
-        double am = __shfl_up_sync(0xffffffffu, ea, s), cm = __shfl_up_sync(0xffffffffu, ec, s);
-        double dm = __shfl_up_sync(0xffffffffu, ed, s), ibm = __shfl_up_sync(0xffffffffu, ib, s);
-        double ap = __shfl_down_sync(0xffffffffu, ea, s), cp = __shfl_down_sync(0xffffffffu, ec, s);
-        double dp = __shfl_down_sync(0xffffffffu, ed, s), ibp = __shfl_down_sync(0xffffffffu, ib, s);
-        if (lane < s) { am = 0.0; cm = 0.0; dm = 0.0; ibm = 1.0; }
-        if (lane + s > 31) { ap = 0.0; cp = 0.0; dp = 0.0; ibp = 1.0; }
-        double a1 = -ea * ibm, g1 = -ec * ibp;
-        double nb = eb + a1 * cm + g1 * ap;
-        double nd = ed + a1 * dm + g1 * dp;
-        ea = a1 * am;
-        ec = g1 * cp;
-        eb = nb;
-        ed = nd;
+        double am = __shfl_up_sync(0xffffffffu, na, s), cm = __shfl_up_sync(0xffffffffu, nc, s);
+        double dm = __shfl_up_sync(0xffffffffu, nd, s);
+        double ap = __shfl_down_sync(0xffffffffu, na, s), cp = __shfl_down_sync(0xffffffffu, nc, s);
+        double dp = __shfl_down_sync(0xffffffffu, nd, s);
+        if (lane < s) { am = 0.0; cm = 0.0; dm = 0.0; }
+        if (lane + s > 31) { ap = 0.0; cp = 0.0; dp = 0.0; }
+        eb = fma(-na, cm, fma(-nc, ap, 1.0));
+        const double a2 = -na * am, c2 = -nc * cp;
+        const double d2 = fma(-na, dm, fma(-nc, dp, nd));
+        ib = rcp<double>(eb);
+        na = a2 * ib;
+        nc = c2 * ib;
+        nd = d2 * ib;
     }
-    const double xe = ed * rcp<double>(eb);
+    const double xe = nd;
     double xe2 = __shfl_down_sync(0xffffffffu, xe, 1);
     if (lane == 31) xe2 = 0.0;
     R_.d[0] = xe;

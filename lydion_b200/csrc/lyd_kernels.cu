@@ -984,25 +984,27 @@ __device__ __forceinline__ void cr_pcr_solve2(Row<2> &R_, int lane) {
     double eb = R_.b[0] + al * c_om + ga * R_.a[1];
     double ec = ga * R_.c[1];
     double ed = R_.d[0] + al * d_om + ga * R_.d[1];
-    // PCR over the 32 even rows (one per lane)
+    // PCR over the 32 even rows (one per lane), every row scaled to a unit diagonal so that a
+    // level fetches three values from each neighbour instead of four (and no reciprocal pivot)
+    double ib = rcp<double>(eb);
+    double na = ea * ib, nc = ec * ib, nd = ed * ib;
 #pragma unroll
     for (int s = 1; s < 32; s <<= 1) {
-        double ib = rcp<double>(eb);
-        double am = __shfl_up_sync(0xffffffffu, ea, s), cm = __shfl_up_sync(0xffffffffu, ec, s);
-        double dm = __shfl_up_sync(0xffffffffu, ed, s), ibm = __shfl_up_sync(0xffffffffu, ib, s);
-        double ap = __shfl_down_sync(0xffffffffu, ea, s), cp = __shfl_down_sync(0xffffffffu, ec, s);
-        double dp = __shfl_down_sync(0xffffffffu, ed, s), ibp = __shfl_down_sync(0xffffffffu, ib, s);
-        if (lane < s) { am = 0.0; cm = 0.0; dm = 0.0; ibm = 1.0; }
-        if (lane + s > 31) { ap = 0.0; cp = 0.0; dp = 0.0; ibp = 1.0; }
-        double a1 = -ea * ibm, g1 = -ec * ibp;
-        double nb = eb + a1 * cm + g1 * ap;
-        double nd = ed + a1 * dm + g1 * dp;
-        ea = a1 * am;
-        ec = g1 * cp;
-        eb = nb;
-        ed = nd;
+        double am = __shfl_up_sync(0xffffffffu, na, s), cm = __shfl_up_sync(0xffffffffu, nc, s);
+        double dm = __shfl_up_sync(0xffffffffu, nd, s);
+        double ap = __shfl_down_sync(0xffffffffu, na, s), cp = __shfl_down_sync(0xffffffffu, nc, s);
+        double dp = __shfl_down_sync(0xffffffffu, nd, s);
+        if (lane < s) { am = 0.0; cm = 0.0; dm = 0.0; }
+        if (lane + s > 31) { ap = 0.0; cp = 0.0; dp = 0.0; }
+        eb = fma(-na, cm, fma(-nc, ap, 1.0));
+        const double a2 = -na * am, c2 = -nc * cp;
+        const double d2 = fma(-na, dm, fma(-nc, dp, nd));
+        ib = rcp<double>(eb);
+        na = a2 * ib;
+        nc = c2 * ib;
+        nd = d2 * ib;
     }
-    const double xe = ed * rcp<double>(eb);
+    const double xe = nd;
     // odd rows: x_o = (d_o - a_o x_e - c_o x_{e+2}) / b_o
     double xe2 = __shfl_down_sync(0xffffffffu, xe, 1);
     if (lane == 31) xe2 = 0.0;
@@ -1011,26 +1013,31 @@ __device__ __forceinline__ void cr_pcr_solve2(Row<2> &R_, int lane) {
     R_.b[0] = eb;                      // the pivots, for the zero-pivot check (b[1] is b_o)
 }
 
-// PCR over one row per lane (lane l holds row l of a 32-row system coupled to lanes l +- s);
-// returns the reduced diagonal and right-hand side, x = ed / eb.
+// PCR over one row per lane (lane l holds row l of a 32-row system coupled to lanes l +- s),
+// every row scaled to a unit diagonal so that a level fetches three values from each neighbour;
+// returns the last level's diagonal (the pivot, before scaling) in eb and x in ed.
 __device__ __forceinline__ void pcr_lanes(double &ea, double &eb, double &ec, double &ed, int lane) {
+    double ib = rcp<double>(eb);
+    double na = ea * ib, nc = ec * ib, nd = ed * ib;
 #pragma unroll
     for (int s = 1; s < 32; s <<= 1) {
-        double ib = rcp<double>(eb);
-        double am = __shfl_up_sync(0xffffffffu, ea, s), cm = __shfl_up_sync(0xffffffffu, ec, s);
-        double dm = __shfl_up_sync(0xffffffffu, ed, s), ibm = __shfl_up_sync(0xffffffffu, ib, s);
-        double ap = __shfl_down_sync(0xffffffffu, ea, s), cp = __shfl_down_sync(0xffffffffu, ec, s);
-        double dp = __shfl_down_sync(0xffffffffu, ed, s), ibp = __shfl_down_sync(0xffffffffu, ib, s);
-        if (lane < s) { am = 0.0; cm = 0.0; dm = 0.0; ibm = 1.0; }
-        if (lane + s > 31) { ap = 0.0; cp = 0.0; dp = 0.0; ibp = 1.0; }
-        double a1 = -ea * ibm, g1 = -ec * ibp;
-        double nb = eb + a1 * cm + g1 * ap;
-        double nd = ed + a1 * dm + g1 * dp;
-        ea = a1 * am;
-        ec = g1 * cp;
-        eb = nb;
-        ed = nd;
+        double am = __shfl_up_sync(0xffffffffu, na, s), cm = __shfl_up_sync(0xffffffffu, nc, s);
+        double dm = __shfl_up_sync(0xffffffffu, nd, s);
+        double ap = __shfl_down_sync(0xffffffffu, na, s), cp = __shfl_down_sync(0xffffffffu, nc, s);
+        double dp = __shfl_down_sync(0xffffffffu, nd, s);
+        if (lane < s) { am = 0.0; cm = 0.0; dm = 0.0; }
+        if (lane + s > 31) { ap = 0.0; cp = 0.0; dp = 0.0; }
+        eb = fma(-na, cm, fma(-nc, ap, 1.0));
+        const double a2 = -na * am, c2 = -nc * cp;
+        const double d2 = fma(-na, dm, fma(-nc, dp, nd));
+        ib = rcp<double>(eb);
+        na = a2 * ib;
+        nc = c2 * ib;
+        nd = d2 * ib;
     }
+    ea = na;
+    ec = nc;
+    ed = nd;
 }
 
 // Four rows per lane (rows 4l .. 4l+3): two cyclic-reduction steps (the odd rows, then rows
@@ -1058,7 +1065,7 @@ __device__ __forceinline__ void cr_pcr_solve4(Row<4> &R_, int lane) {
     ga = -c0 * ib2;
     double ea = al * a2p, eb = b0 + al * c2p + ga * a2, ec = ga * c2, ed = d0 + al * d2p + ga * d2;
     pcr_lanes(ea, eb, ec, ed, lane);
-    const double x0 = ed * rcp<double>(eb);
+    const double x0 = ed;
     double x4 = __shfl_down_sync(0xffffffffu, x0, 1);
     if (lane == 31) x4 = 0.0;
     const double x2 = (d2 - a2 * x0 - c2 * x4) * ib2;
