@@ -114,6 +114,9 @@ struct lyd_ctx {
     int hs_req = 0, hs_chunks = 0, hs_rows = 0, hs_cpb = 0, hs_pchk = 0;
     cudaStream_t st_up = nullptr, st_dn = nullptr, st_fq = nullptr;
     cudaEvent_t hs_ev[3 * 16 + 2] = {};
+    // the adjoint's recomputation stream, and its events: recomputed (2), reversed (2), start
+    cudaStream_t st_rec = nullptr;
+    cudaEvent_t adj_ev[5] = {};
     unsigned *bar = nullptr;           // grid barrier of the persistent step: arrivals, generation
     int persist_graph = 0;             // persistent step replayed from a graph: 1 yes, -1 no (capture refused)
     bool timing = false;
@@ -492,6 +495,9 @@ int lyd_destroy(lyd_ctx *c) {
     if (c->st_up) cudaStreamDestroy(c->st_up);
     if (c->st_dn) cudaStreamDestroy(c->st_dn);
     if (c->st_fq) cudaStreamDestroy(c->st_fq);
+    for (cudaEvent_t e : c->adj_ev)
+        if (e) cudaEventDestroy(e);
+    if (c->st_rec) cudaStreamDestroy(c->st_rec);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
     return LYD_OK;
@@ -1311,14 +1317,15 @@ static int build_host_chunks(lyd_ctx *c, int chunks) {
     return LYD_OK;
 }
 
-// Drains the host-state step's streams when the step leaves early: no copy into or out of the
-// caller's arrays may still run after the call returns.
-struct HostStepDrain {
+// Drains the context's streams when a call that spreads its work over several of them leaves
+// early: no copy into or out of the caller's arrays (the host-state step), and no recomputation
+// into the workspace (the adjoint), may still run after the call returns.
+struct StreamDrain {
     lyd_ctx *c;
     bool armed = false;
-    ~HostStepDrain() {
+    ~StreamDrain() {
         if (!armed) return;
-        for (cudaStream_t s : {c->st_up, c->st_fq, c->st_dn, c->st})
+        for (cudaStream_t s : {c->st_up, c->st_fq, c->st_dn, c->st_rec, c->st})
             if (s) cudaStreamSynchronize(s);
     }
 };
@@ -1362,7 +1369,7 @@ int lyd_static_step_host(lyd_ctx *c, const lyd_step_params *p, const double *J, 
     cudaEvent_t ev_start = c->hs_ev[3 * kMaxHostChunks], ev_chk = c->hs_ev[3 * kMaxHostChunks + 1];
     const double *src[3] = {J, Hr, HZ};
     double *dst[3] = {J_out, Hr_out, HZ_out};
-    HostStepDrain drain{c};
+    StreamDrain drain{c};
     drain.armed = true;
     // whatever ran before on the context's stream is done with the reduction's counters first
     LYD_CU(c, cudaEventRecord(ev_start, c->st));
@@ -1928,15 +1935,25 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     // all are kept, else of one segment, recorded while it is recomputed); the adjoints; and
     // the gradient accumulators (zeroed here).
     const size_t ntape = store_all ? (size_t)N : (size_t)K;
-    const size_t sizes[] = {(size_t)nseg * S * 8, store_all ? 0 : (size_t)K * S * 8, S * 8, ntape * 4 * n3 * 8,
-                            S * 8, S * 8, S * 8, S * 8, n3 * 8, n3 * 8, nc * 8, nc * 8, nc * 8, 5 * nc * 8,
-                            c->nrf * 8, c->nzf * 8, S * 8, (size_t)nnu * 8, 2 * (size_t)nnu * (nr + nz + 2 * nr) * 8,
-                            (size_t)N * 2 * sizeof(int) + 16, 16, keep_ff ? (size_t)N * 3 * n3 * 8 : 0};
-    constexpr int NB = sizeof(sizes) / sizeof(sizes[0]);
+    // With uniform segments and phase timing off, segment g-1 is recomputed on a second stream
+    // while segment g is reversed, into a second buffer of states and tapes (when it fits).
+    bool overlap = !binom && !store_all && nseg >= 2 && !c->timing;
+    constexpr int NB = 24;
     size_t offs[NB], total = 0;
-    for (int q = 0; q < NB; q++) {
-        offs[q] = total;
-        total += (sizes[q] + 255) / 256 * 256;
+    for (;;) {
+        const size_t ov = overlap ? 1 : 0;
+        const size_t sizes[NB] = {(size_t)nseg * S * 8, store_all ? 0 : (size_t)K * S * 8, S * 8, ntape * 4 * n3 * 8,
+                                  S * 8, S * 8, S * 8, S * 8, n3 * 8, n3 * 8, nc * 8, nc * 8, nc * 8, 5 * nc * 8,
+                                  c->nrf * 8, c->nzf * 8, S * 8, (size_t)nnu * 8,
+                                  2 * (size_t)nnu * (nr + nz + 2 * nr) * 8, (size_t)N * 2 * sizeof(int) + 16, 16,
+                                  keep_ff ? (size_t)N * 3 * n3 * 8 : 0, ov * K * S * 8, ov * K * 4 * n3 * 8};
+        total = 0;
+        for (int q = 0; q < NB; q++) {
+            offs[q] = total;
+            total += (sizes[q] + 255) / 256 * 256;
+        }
+        if (!overlap || total + margin <= avail) break;
+        overlap = false;
     }
     if (total > c->adj_ws_bytes) {
         LYD_CU(c, cudaStreamSynchronize(c->st));
@@ -1958,17 +1975,18 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     int *win = reinterpret_cast<int *>(W_(19));
     int *finwin = reinterpret_cast<int *>(W_(20));
     double *ffs = keep_ff ? W_(21) : nullptr;
+    double *segB[2] = {seg, overlap ? W_(22) : nullptr}, *segTB[2] = {segT, overlap ? W_(23) : nullptr};
     // lambda and the accumulators start at zero (buffers 4 and 8..15 are contiguous in order)
     LYD_CU(c, cudaMemsetAsync(lam, 0, S * 8, c->st));
     LYD_CU(c, cudaMemsetAsync(gaF, 0, offs[16] - offs[8], c->st));
-    auto copy_state = [&](double *dst, int set) -> int {
+    auto copy_state = [&](double *dst, int set, cudaStream_t s = nullptr) -> int {
         for (int q = 0; q < 3; q++)
-            LYD_CU(c, cudaMemcpyAsync(dst + q * n3, c->set[set][q], n3 * 8, cudaMemcpyDeviceToDevice, c->st));
+            LYD_CU(c, cudaMemcpyAsync(dst + q * n3, c->set[set][q], n3 * 8, cudaMemcpyDeviceToDevice, s ? s : c->st));
         return LYD_OK;
     };
-    auto load_state = [&](const double *src, int set) -> int {
+    auto load_state = [&](const double *src, int set, cudaStream_t s = nullptr) -> int {
         for (int q = 0; q < 3; q++)
-            LYD_CU(c, cudaMemcpyAsync(c->set[set][q], src + q * n3, n3 * 8, cudaMemcpyDeviceToDevice, c->st));
+            LYD_CU(c, cudaMemcpyAsync(c->set[set][q], src + q * n3, n3 * 8, cudaMemcpyDeviceToDevice, s ? s : c->st));
         return LYD_OK;
     };
     // phase timing (lyd_set_timing): events around the forward sweep and every reverse phase
@@ -2047,13 +2065,14 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     // One step forward from the state in the context's current set (or from `sn`, which then
     // receives a copy of it), in the forward sweep's window of step n: the advection into x_A,
     // with its tape when `tape` is given, then (with `freq`) emission + frequency step x_A -> the
-    // current set.
-    auto forward_step = [&](int n, double *sn, double *tape, bool freq) -> int {
+    // current set. On stream `s` (the context's stream when null).
+    auto forward_step = [&](int n, double *sn, double *tape, bool freq, cudaStream_t s = nullptr) -> int {
+        if (!s) s = c->st;
         double *xA = segA;
         AdvArgs<double> aa;
         fill_adv<double>(c, aa, c->cur, B);
         if (sn) {
-            LYD_TRY(copy_state(sn, c->cur));
+            LYD_TRY(copy_state(sn, c->cur, s));
             aa.J = sn; aa.Hr = sn + n3; aa.HZ = sn + 2 * n3;
             aa.tmaps = nullptr;     // the maps cover the context's buffer sets, not the workspace
         }
@@ -2061,14 +2080,14 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
         aa.kwin = win + 2 * n;
         aa.tape = tape;
         aa.tape_stride = (long long)n3;
-        launch_advect(LYD_PREC_FP64, c->cfg.flux_method, &aa, c->ntiles, 2, c->st);
+        launch_advect(LYD_PREC_FP64, c->cfg.flux_method, &aa, c->ntiles, 2, s);
         if (freq) {
             FreqArgs<double> fq;
             fill_freq<double>(c, fq, xA, xA + n3, xA + 2 * n3, xA, c->set[c->cur][0], c->set[c->cur][1],
                               c->set[c->cur][2]);
             fq.do_emission = 1; fq.do_freq = 1; fq.update_ff = 1;
             fq.parts = 0;
-            launch_freq(LYD_PREC_FP64, &fq, nnu, c->nitems, c->st);
+            launch_freq(LYD_PREC_FP64, &fq, nnu, c->nitems, s);
         }
         LYD_CU(c, cudaGetLastError());
         return LYD_OK;
@@ -2137,7 +2156,44 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
         lamN = t;
         return LYD_OK;
     };
-    if (!binom) {
+    if (!binom && overlap) {
+        // segment g's states and tapes go to buffer g & 1, recomputed on the recomputation stream:
+        // reversal g waits for recomputation g, and recomputation g - 2 (into the same buffer)
+        // for reversal g, so recomputation g - 1 runs beside reversal g
+        if (!c->st_rec) {
+            LYD_CU(c, cudaStreamCreateWithFlags(&c->st_rec, cudaStreamNonBlocking));
+            for (cudaEvent_t &e : c->adj_ev) LYD_CU(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        }
+        cudaEvent_t *ev_rec = c->adj_ev, *ev_rev = c->adj_ev + 2;
+        StreamDrain drain{c};
+        drain.armed = true;
+        LYD_CU(c, cudaEventRecord(c->adj_ev[4], c->st));
+        LYD_CU(c, cudaStreamWaitEvent(c->st_rec, c->adj_ev[4], 0));
+        auto recompute = [&](int g) -> int {
+            const int n0 = g * K, n1 = (n0 + K < N) ? n0 + K : N;
+            double *sb = segB[g & 1], *tb = segTB[g & 1];
+            LYD_TRY(load_state(ck + (size_t)g * S, c->cur, c->st_rec));
+            for (int n = n0; n < n1; n++)
+                LYD_TRY(forward_step(n, sb + (size_t)(n - n0) * S, tb + (size_t)(n - n0) * 4 * n3, n + 1 < n1,
+                                     c->st_rec));
+            LYD_CU(c, cudaEventRecord(ev_rec[g & 1], c->st_rec));
+            return LYD_OK;
+        };
+        LYD_TRY(recompute(nseg - 1));
+        LYD_TRY(recompute(nseg - 2));
+        for (int g = nseg - 1; g >= 0; g--) {
+            const int n0 = g * K, n1 = (n0 + K < N) ? n0 + K : N;
+            LYD_CU(c, cudaStreamWaitEvent(c->st, ev_rec[g & 1], 0));
+            for (int n = n1 - 1; n >= n0; n--)
+                LYD_TRY(reverse_step(n, segB[g & 1] + (size_t)(n - n0) * S, segTB[g & 1] + (size_t)(n - n0) * 4 * n3));
+            if (g >= 2) {
+                LYD_CU(c, cudaEventRecord(ev_rev[g & 1], c->st));
+                LYD_CU(c, cudaStreamWaitEvent(c->st_rec, ev_rev[g & 1], 0));
+                LYD_TRY(recompute(g - 2));
+            }
+        }
+        drain.armed = false;
+    } else if (!binom) {
         for (int g = nseg - 1; g >= 0; g--) {
             const int n0 = g * K, n1 = (n0 + K < N) ? n0 + K : N;
             if (!store_all) {
