@@ -303,7 +303,9 @@ int  lyd_get_tuning(lyd_ctx *ctx, lyd_tuning *t);
  * (7 doubles per cell-bin per step), the forward sweep keeps every step's state and advection
  * tape, plus its frequency factors when 10 doubles per cell-bin per step fit, and nothing is
  * recomputed; with checkpoint_every = K > 1 (0 otherwise: 100)
- * it stores the state every K steps and the reverse sweep recomputes each segment once; with
+ * it stores the state every K steps and the reverse sweep recomputes each segment once (with
+ * timing off, and when the room is there, into a second buffer of K states and tapes on a
+ * second stream while the segment after it is reversed); with
  * checkpoint_every < 0 it keeps `snapshots` + 1 states in Griewank's binomial (Revolve)
  * schedule, advancing no step more than r times, r the least with C(snapshots + 1 + r, r) >=
  * n_steps, and records each step's tape right before its reverse. The
