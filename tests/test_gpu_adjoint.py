@@ -151,6 +151,26 @@ def test_checkpoint_spacing_does_not_change_gradients(prob):
             np.testing.assert_allclose(g2[k], g[k], rtol=1e-10, atol=1e-11 * np.abs(g[k]).max())
 
 
+def test_overlapped_recomputation_matches_the_serial_order():
+    """With uniform checkpoints and phase timing off, the next segment is recomputed on a second
+    stream while the current one is reversed; with timing on the segments run one after the
+    other. 30 steps in segments of 4 (8 segments, both state buffers reused several times) give
+    the same gradients and the same final state either way."""
+    P = Problem(30)
+    out, fin = [], []
+    for timing in (False, True):
+        ctx = P.ctx()
+        ctx.set_timing(timing)
+        out.append(ctx.adjoint(P.n, *P.p, w_MF=1.0, w_spec=SS * P.w, checkpoint_every=4))
+        ctx.set_timing(False)
+        fin.append(ctx.download("J"))
+        ctx.close()
+    assert out[0]["objective"] == out[1]["objective"]
+    np.testing.assert_array_equal(fin[0], fin[1])
+    for k in ("grad_alpha", "grad_alpha_c", "grad_T", "grad_J0", "grad_H_r0", "grad_u_r_star", "grad_u_Z_star"):
+        np.testing.assert_allclose(out[0][k], out[1][k], rtol=1e-10, atol=1e-11 * np.abs(out[1][k]).max())
+
+
 def test_binomial_schedule_on_a_longer_run():
     """40 steps with 3 extra snapshots (no step advanced more than 4 times) give the gradients of
     the run that keeps every step."""
