@@ -1935,9 +1935,11 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
     // all are kept, else of one segment, recorded while it is recomputed); the adjoints; and
     // the gradient accumulators (zeroed here).
     const size_t ntape = store_all ? (size_t)N : (size_t)K;
-    // With uniform segments and phase timing off, segment g-1 is recomputed on a second stream
-    // while segment g is reversed, into a second buffer of states and tapes (when it fits).
-    bool overlap = !binom && !store_all && nseg >= 2 && !c->timing;
+    // With phase timing off, the recomputation runs on a second stream beside the reverse
+    // sweep, into a second buffer of states and tapes (when it fits): with uniform segments
+    // segment g-1 is recomputed while segment g is reversed; in the binomial schedule every
+    // advance and record runs ahead of the reversals, one step's record per buffer.
+    bool overlap = !store_all && (binom || nseg >= 2) && !c->timing;
     constexpr int NB = 24;
     size_t offs[NB], total = 0;
     for (;;) {
@@ -2156,19 +2158,24 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
         lamN = t;
         return LYD_OK;
     };
+    // the recomputation stream starts once the forward sweep and the seeds are done
+    if (overlap && !c->st_rec) {
+        LYD_CU(c, cudaStreamCreateWithFlags(&c->st_rec, cudaStreamNonBlocking));
+        for (cudaEvent_t &e : c->adj_ev) LYD_CU(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    cudaEvent_t *ev_rec = c->adj_ev, *ev_rev = c->adj_ev + 2;
+    StreamDrain drain{c};
+    if (overlap) {
+        drain.armed = true;
+        LYD_CU(c, cudaEventRecord(c->adj_ev[4], c->st));
+        LYD_CU(c, cudaStreamWaitEvent(c->st_rec, c->adj_ev[4], 0));
+    }
+    // the stream of the forward work of the reverse sweep (advances, snapshots, records)
+    cudaStream_t fs = overlap ? c->st_rec : c->st;
     if (!binom && overlap) {
         // segment g's states and tapes go to buffer g & 1, recomputed on the recomputation stream:
         // reversal g waits for recomputation g, and recomputation g - 2 (into the same buffer)
         // for reversal g, so recomputation g - 1 runs beside reversal g
-        if (!c->st_rec) {
-            LYD_CU(c, cudaStreamCreateWithFlags(&c->st_rec, cudaStreamNonBlocking));
-            for (cudaEvent_t &e : c->adj_ev) LYD_CU(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        }
-        cudaEvent_t *ev_rec = c->adj_ev, *ev_rev = c->adj_ev + 2;
-        StreamDrain drain{c};
-        drain.armed = true;
-        LYD_CU(c, cudaEventRecord(c->adj_ev[4], c->st));
-        LYD_CU(c, cudaStreamWaitEvent(c->st_rec, c->adj_ev[4], 0));
         auto recompute = [&](int g) -> int {
             const int n0 = g * K, n1 = (n0 + K < N) ? n0 + K : N;
             double *sb = segB[g & 1], *tb = segTB[g & 1];
@@ -2192,7 +2199,6 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
                 LYD_TRY(recompute(g - 2));
             }
         }
-        drain.armed = false;
     } else if (!binom) {
         for (int g = nseg - 1; g >= 0; g--) {
             const int n0 = g * K, n1 = (n0 + K < N) ? n0 + K : N;
@@ -2220,20 +2226,31 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
         // (advanced once to place it) with the same snapshots and r - 1, so no step is advanced
         // more than r times. Each step is recorded (its input state and tape) right before its
         // reverse.
+        // Advances, snapshot copies and records go to `fs`. Overlapped, step n records into
+        // buffer n & 1 once reversal n + 2 (its last reader) is done, and reversal n waits for
+        // that record: the advances and records of the next steps run beside the reversals.
         auto advance = [&](int slot, int i0, int n_to) -> int {
             tick(0);
-            LYD_TRY(load_state(ck + (size_t)slot * S, c->cur));
-            for (int n = i0; n < n_to; n++) LYD_TRY(forward_step(n, nullptr, nullptr, true));
+            LYD_TRY(load_state(ck + (size_t)slot * S, c->cur, fs));
+            for (int n = i0; n < n_to; n++) LYD_TRY(forward_step(n, nullptr, nullptr, true, fs));
             tick(1);
             tock(0, 1, 1);
             return LYD_OK;
         };
         auto record_and_reverse = [&](int n) -> int {
+            double *sb = segB[overlap ? (n & 1) : 0], *tb = segTB[overlap ? (n & 1) : 0];
             tick(0);
-            LYD_TRY(forward_step(n, seg, segT, false));
+            if (overlap) LYD_CU(c, cudaStreamWaitEvent(fs, ev_rev[n & 1], 0));
+            LYD_TRY(forward_step(n, sb, tb, false, fs));
+            if (overlap) {
+                LYD_CU(c, cudaEventRecord(ev_rec[n & 1], fs));
+                LYD_CU(c, cudaStreamWaitEvent(c->st, ev_rec[n & 1], 0));
+            }
             tick(1);
             tock(0, 1, 1);
-            return reverse_step(n, seg, segT);
+            LYD_TRY(reverse_step(n, sb, tb));
+            if (overlap) LYD_CU(c, cudaEventRecord(ev_rev[n & 1], c->st));
+            return LYD_OK;
         };
         std::function<int(int, int, int, int)> rev = [&](int i0, int i1, int slot, int nfree) -> int {
             const int l = i1 - i0;
@@ -2253,12 +2270,13 @@ int lyd_adjoint_run(lyd_ctx *c, const lyd_adjoint_cfg *cfg, lyd_adjoint_out *out
             int t = l - (int)std::min((double)(l - 1), binomial_reach(nfree, r));
             if (t < 1) t = 1;
             LYD_TRY(advance(slot, i0, i0 + t));
-            LYD_TRY(copy_state(ck + (size_t)(slot + 1) * S, c->cur));
+            LYD_TRY(copy_state(ck + (size_t)(slot + 1) * S, c->cur, fs));
             LYD_TRY(rev(i0 + t, i1, slot + 1, nfree - 1));
             return rev(i0, i0 + t, slot, nfree);
         };
         LYD_TRY(rev(0, N, 0, snaps));
     }
+    drain.armed = false;
     // alpha_F = alpha H_voigt ; H_voigt(T) when it was computed on the device
     launch_af_params(gaF, c->cellf[CF_ALPHA], (const double *)c->Hv, nnu, (long long)nc, g_alpha, gHv, c->st);
     if (c->hv_from_T && c->lut)
