@@ -308,7 +308,8 @@ int  lyd_get_tuning(lyd_ctx *ctx, lyd_tuning *t);
  * second stream while the segment after it is reversed); with
  * checkpoint_every < 0 it keeps `snapshots` + 1 states in Griewank's binomial (Revolve)
  * schedule, advancing no step more than r times, r the least with C(snapshots + 1 + r, r) >=
- * n_steps, and records each step's tape right before its reverse. The
+ * n_steps, and records each step's tape right before its reverse (with timing off, the advances
+ * and records run on a second stream ahead of the reversals, two steps' records in flight). The
  * reverse sweep runs hand-written adjoint kernels of the step (advection, emission/absorption,
  * frequency factors, transposed tridiagonal solve, flux correction). The active window of every step is the forward's.
  * Non-smooth points (MinMod, floors, clamps, limiters) take the derivative of the branch the
