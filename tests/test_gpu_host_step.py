@@ -51,6 +51,24 @@ def test_host_step_equals_device_step_bitwise(flux, chunks):
     host.close()
 
 
+@pytest.mark.parametrize("chunks", [2, 3, 6])
+def test_host_step_ragged_last_tile_row_bitwise(chunks):
+    """41 rows in tiles of 8: the last tile row holds one row, so the last chunk's upload (which
+    starts two rows into it) is empty and the chunk before brings every remaining row."""
+    cl = W.static_cloud(nr=20, nz=41, n_nu=32, tau0=1e6, T0=1e4, umax_kms=100.0, rs=0.5, tau_abs=0.5)
+    dev, host, (J, Hr, HZ) = _pair(cl)
+    p = _params(cl)
+    for step in range(3):
+        rec_d = dev.static_steps(1, *p)[0]
+        J, Hr, HZ, rec_h = host.static_step_host(J, Hr, HZ, *p, out=(J, Hr, HZ), chunks=chunks)
+        np.testing.assert_array_equal(rec_h, rec_d, err_msg=f"step {step}")
+        np.testing.assert_array_equal(J, dev.download("J"), err_msg=f"step {step}")
+        np.testing.assert_array_equal(Hr, dev.download("H_r"))
+        np.testing.assert_array_equal(HZ, dev.download("H_Z"))
+    dev.close()
+    host.close()
+
+
 @pytest.mark.parametrize("bc_left", [W.BC_REFLECT, W.BC_OUTFLOW])
 def test_host_step_cartesian_bitwise(bc_left):
     """A Cartesian grid (the first X interface reflecting or letting flow out), 6 chunks."""
