@@ -6,7 +6,7 @@
                                                   # then 4 absorption sub-steps of 0.1 t_abs
     python -m lydion_b200.profile_cases step      # the dusty-outflow 256x256x64 cloud, mixed form,
                                                   # 16 rows per advection tile, 4 CTAs/SM: 20 steps
-    python -m lydion_b200.profile_cases step64    # the same cloud in FP64, 20 rows per tile,
+    python -m lydion_b200.profile_cases step64    # the same cloud in FP64, 16 rows per tile,
                                                   # 3 CTAs/SM (the bench's tuned shape): 20 steps
     python -m lydion_b200.profile_cases big64     # a 512x512x128 RHD snapshot in FP64 (33.5M
                                                   # cell-bins, ~2 GB on the device, 15x L2): 6 steps
@@ -53,7 +53,7 @@ def step_case(fp64=False):
     from .m1 import context_for_cloud
     cl = W.config_c2()
     ctx = context_for_cloud(cl, precision=PREC_FP64 if fp64 else PREC_MIXED)
-    ctx.set_tuning(*((20, 0, 0, 3) if fp64 else (16, 0, 0, 4)))
+    ctx.set_tuning(*((16, 0, 0, 3) if fp64 else (16, 0, 0, 4)))
     h = ctx.static_steps(20, cl.c_tilde, cl.dt, cl.z_center, cl.bc_r_right, cl.bc_z_bot, cl.bc_z_top)
     ctx.close()
     return float(h[-1, 0])
